@@ -1,0 +1,327 @@
+/*
+ * xdem_gpu.h — C-ABI of the B200 (sm_100a) implementation of xDEM's
+ * per-timestep hot path.
+ *
+ * One opaque world handle owns the device copy of a particle system (SoA
+ * arrays in HBM), its contact history (per-owner sorted slots) and its world
+ * scalars (box, Lees-Edwards shift, control-law state).  Every entry point
+ * below replaces one method of the reference's C++ class hierarchy; the cited
+ * file:line is the reference method whose argument meaning, sequencing and
+ * side effects the entry point reproduces.  Where the reference prints and
+ * calls exit(), these entry points return an XDEM_ERR_* bit set instead and
+ * leave the handle usable.
+ *
+ * Conventions
+ *   - particle ids equal indices 0..n-1 (the reference relies on this in
+ *     BaseWorld.cpp:72-74);
+ *   - a contact is keyed by (id_i, id_j) with id_i < id_j and its history is
+ *     owned by id_i (PeriodicBoundaryWorld.cpp:118, BaseParticle.cpp:36-95);
+ *   - all arrays are host pointers unless a name says otherwise; every call is
+ *     serialised on the handle's CUDA stream;
+ *   - return value: 0 (XDEM_OK) or an OR of XDEM_ERR_* bits.
+ */
+#ifndef XDEM_GPU_H
+#define XDEM_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define XDEM_ABI_VERSION 1
+
+/* Status bits.  Device kernels OR them into a per-world status word. */
+enum xdem_status_bits {
+  XDEM_OK = 0,
+  /* candidate list of one particle reached 200 entries
+     (PeriodicBoundaryWorld.cpp:75-78 exits with -2), or a particle ran out of
+     history slots (no reference counterpart: its hash map grows) */
+  XDEM_ERR_CAPACITY = 1 << 0,
+  /* closest-approach Newton iteration hit its cap (EllipticParticle.cpp:621
+     has no cap and can loop forever) */
+  XDEM_ERR_NEWTON = 1 << 1,
+  /* non-finite position/velocity/force detected */
+  XDEM_ERR_NONFINITE = 1 << 2,
+  /* pair of shapes without a contact law, e.g. circle-ellipse
+     (CircularParticle.cpp:38, EllipticParticle.cpp:30 exit with -1) */
+  XDEM_ERR_UNSUPPORTED_PAIR = 1 << 3,
+  /* normalisation of a zero-length vector (MathVector.h:180-190 exits) */
+  XDEM_ERR_ZERO_VECTOR = 1 << 4,
+  /* a CUDA runtime call failed */
+  XDEM_ERR_CUDA = 1 << 5,
+  /* bad argument, unknown enum, or call not valid for this world kind */
+  XDEM_ERR_ARGUMENT = 1 << 6,
+  /* cell grid has fewer than 3 cells along an axis (the reference's 3x3
+     neighbour scan would visit a cell twice) */
+  XDEM_ERR_GRID = 1 << 7
+};
+
+/* World kinds: PeriodicBoundaryWorld.h:8, PeriodicControlWorld.h:5,
+   LeesEdwardsBoundaryWorld.h:5 */
+enum xdem_world_kind {
+  XDEM_WORLD_PERIODIC = 0,
+  XDEM_WORLD_PERIODIC_CONTROL = 1,
+  XDEM_WORLD_LEES_EDWARDS = 2
+};
+
+/* Particle shapes: CircularParticle.h:10, EllipticParticle.h:10,
+   GluedParticle.h:5 */
+enum xdem_shape {
+  XDEM_SHAPE_CIRCLE = 0,
+  XDEM_SHAPE_ELLIPSE = 1,
+  XDEM_SHAPE_CLUMP = 2
+};
+
+/* SETTING bit flags, same values as BaseParticle.h:19-24 */
+enum xdem_setting {
+  XDEM_SETTING_NONE = 0,
+  XDEM_SKIP_TIME_INTEGRAL = 1 << 0,
+  XDEM_SKIP_CONTACT_DETECTION = 1 << 1,
+  XDEM_SKIP_MACRO_SUM = 1 << 2
+};
+
+/* Ellipse-ellipse contact law.  CLOSEST_APPROACH is the Zheng and
+   Palffy-Muhoray quartic solved by Newton (EllipticParticle.cpp:34-285, the
+   one the reference dispatches at :27); INTERSECTION is Strobach's fast
+   quartic solver on the intersection quartic (EllipticParticle.cpp:288-484). */
+enum xdem_ellipse_method {
+  XDEM_ELLIPSE_CLOSEST_APPROACH = 0,
+  XDEM_ELLIPSE_INTERSECTION = 1
+};
+
+/* Arithmetic of contact geometry and forces.  State, history and the
+   Lees-Edwards shift are FP64 in both modes. */
+enum xdem_precision {
+  XDEM_PRECISION_FP64 = 0,
+  XDEM_PRECISION_MIXED = 1
+};
+
+/* Box-control laws of PeriodicControlWorld (PeriodicControlWorld.cpp:124-237) */
+enum xdem_box_law {
+  XDEM_BOX_NONE = 0,
+  XDEM_BOX_STRAIN = 1,                 /* updatePeriodicBoundary_strainControl(p0, p1) */
+  XDEM_BOX_STRESS_XY = 2,              /* stressControlX(p0) then stressControlY(p0) */
+  XDEM_BOX_STRESS_UNIFORM = 3,         /* updatePeriodicBoundary_stressControlUniform(p0) */
+  XDEM_BOX_STRESS_UNIFORM_LIMIT = 4    /* ..._stressControlUniform_strainLimit(p0) */
+};
+
+/* Step sequences */
+enum xdem_sequence {
+  /* the world kind's own takeTimeStep(): PeriodicBoundaryWorld.cpp:119-127,
+     PeriodicControlWorld.cpp:114-122, LeesEdwardsBoundaryWorld.cpp:21-31 */
+  XDEM_SEQ_TAKE_TIME_STEP = 0,
+  /* the driver-composed compression loop of mainIsoCircPack_WCCM.cpp:117-126:
+     modifyParticlePosition, findPossibleContacts, updateContacts,
+     collectForceAndTorque, takeTimeIntegral (no rattler reset) */
+  XDEM_SEQ_SUBSTEPS = 1
+};
+
+/* Construction parameters: BaseWorld(dt, particles, model) (BaseWorld.h:44-56),
+   setWorldBoundary (BaseWorld.cpp:3-11), the contact model constructor
+   (ContactModel_LinearDissipativeFrictional.h:11-24), _GlobalDamping_
+   (BaseParticle.cpp:9) and setShiftStrainRate (LeesEdwardsBoundaryWorld.cpp:485). */
+typedef struct xdem_params {
+  int32_t world_kind;        /* enum xdem_world_kind */
+  int32_t ellipse_method;    /* enum xdem_ellipse_method */
+  int32_t precision;         /* enum xdem_precision */
+  int32_t max_contacts;      /* history slots per particle (<= 32), 0 = default (16) */
+  double dt;
+  double xmin, xmax, ymin, ymax;
+  double normal_stiffness, shear_stiffness, restitution_coeff, frictional_coeff;
+  double global_damping;
+  double shift_strain_rate;  /* Lees-Edwards only */
+  /* cell size; 0 = 2.01 * max outer radius (BaseWorld.cpp:201-219).  Any value
+     >= 2 * max outer radius gives the same contact set. */
+  double max_particle_size;
+} xdem_params;
+
+/* Per-step extras of xdem_run, matching what the reference drivers do around
+   the step (mainIsoCircPack_WCCM.cpp:76-85,115-126,
+   mainIsoElpsPackTestEntropy.cpp:171). */
+typedef struct xdem_control {
+  int32_t sequence;            /* enum xdem_sequence */
+  int32_t scale_rattlers;      /* 1: scaleVelocityOfRattlers(rattler_scale) before the step */
+  int32_t reset_rattlers;      /* 1: resetVelocityOfRattlers() after the step */
+  int32_t update_stress;       /* 1: updateTotalStress() after the step */
+  int32_t box_law;             /* enum xdem_box_law, applied after the stress update */
+  int32_t stop_on_pressure;    /* 1: stop once trace(stress)/2 >= stop_pressure (checked on device) */
+  double rattler_scale;
+  double p0, p1;               /* box-law arguments */
+  double stop_pressure;
+} xdem_control;
+
+/* Particle arrays (length n).  For xdem_set_particles every pointer must be
+   non-NULL except num_sub/branch_x/branch_y (NULL = no clumps) and
+   is_rattler (NULL = all rattlers, as before the first collect).  For
+   xdem_get_particles, NULL pointers are skipped. */
+typedef struct xdem_particles {
+  int32_t n;
+  int32_t *shape, *up_level, *setting, *is_rattler;
+  double *outer_radius;      /* BaseParticle::_outerRadius */
+  double *radius;            /* circle radius / ellipse semi-major axis a */
+  double *aspect_ratio;      /* a/b for ellipses, 1 otherwise */
+  double *x, *y, *vx, *vy, *rot, *rot_vel;
+  double *volume, *mass, *inv_mass, *inertia, *inv_inertia;
+  int32_t *num_sub;          /* clump: number of sub-particles whose ids follow it */
+  double *branch_x, *branch_y; /* sub-particle: GluedParticle::_branchVectors entry */
+} xdem_particles;
+
+/* Contact records, sorted by (id_i, id_j); the fields of ContactInformation
+   (ContactInformation.h:14-29).  branch = p_i - (p_j + offset)
+   (BaseParticle.cpp:85); force = fn + ft; torque_i/j = torqueOnP1/P2. */
+typedef struct xdem_contacts {
+  int64_t count;             /* in: records to upload; out: records present */
+  int64_t capacity;          /* out-calls: array length available */
+  int32_t *id_i, *id_j;
+  double *normal_x, *normal_y, *point_x, *point_y, *branch_x, *branch_y;
+  double *bv1_x, *bv1_y, *bv2_x, *bv2_y;
+  double *shear_x, *shear_y;
+  double *fn_x, *fn_y, *ft_x, *ft_y;
+  double *torque_i, *torque_j, *damping;
+} xdem_contacts;
+
+typedef struct xdem_world_s* xdem_world;
+
+/* ---- library ---------------------------------------------------------- */
+int32_t xdem_abi_version(void);
+const char* xdem_status_string(int32_t status_bit);
+/* sets *out to the number of CUDA devices; returns XDEM_ERR_CUDA if none */
+int32_t xdem_device_count(int32_t* out);
+
+/* ---- lifetime ---------------------------------------------------------- */
+/* BaseWorld::BaseWorld (BaseWorld.h:44-56) + setWorldBoundary (BaseWorld.cpp:3-11).
+   The world is created empty; xdem_set_particles sizes it. */
+int32_t xdem_create(const xdem_params* params, xdem_world* out);
+int32_t xdem_destroy(xdem_world w);
+/* run this world's work on a caller-owned cudaStream_t (NULL = own stream) */
+int32_t xdem_set_stream(xdem_world w, void* cuda_stream);
+
+/* ---- state exchange ----------------------------------------------------- */
+/* upload: vector<BaseParticle*> handed to the world constructor (BaseWorld.h:44);
+   also runs updateMaximumParticleSize (BaseWorld.cpp:201-219) and
+   updateTotalParticleVolume (BaseWorld.cpp:188-199) */
+int32_t xdem_set_particles(xdem_world w, const xdem_particles* p);
+/* download: the BaseParticle getters (BaseParticle.h:109-127) */
+int32_t xdem_get_particles(xdem_world w, xdem_particles* p);
+/* upload a contact history: the per-particle _contactInfo maps
+   (BaseParticle.h:46; read4File_particle BaseParticle.cpp:172-186) */
+int32_t xdem_set_contacts(xdem_world w, const xdem_contacts* c);
+/* download contacts: getContactInfo() of every particle (BaseParticle.h:125).
+   With capacity < count only count is written (returns XDEM_ERR_CAPACITY). */
+int32_t xdem_get_contacts(xdem_world w, xdem_contacts* c);
+/* _totalForce/_totalTorque/_numContactPerParticle after collectForceAndTorque
+   (BaseWorld.cpp:17-57) */
+int32_t xdem_get_force_and_torque(xdem_world w, double* fx, double* fy, double* torque,
+                                  int32_t* num_contacts);
+/* countActucalContacts (BaseWorld.cpp:262-269) */
+int32_t xdem_count_contacts(xdem_world w, int64_t* out);
+
+/* ---- world scalars ------------------------------------------------------ */
+/* getXmin/getXmax/getYmin/getYmax (BaseWorld.h:75-78) */
+int32_t xdem_get_boundary(xdem_world w, double box[4]);
+/* setWorldBoundary (BaseWorld.cpp:3-11) */
+int32_t xdem_set_boundary(xdem_world w, const double box[4]);
+/* getStress after updateTotalStress (BaseWorld.h:89): xx, xy, yx, yy */
+int32_t xdem_get_stress(xdem_world w, double stress[4]);
+/* getTotalShift, shift velocity, getTotalStrain, shift strain rate
+   (LeesEdwardsBoundaryWorld.h:39-40) */
+int32_t xdem_get_lees_edwards(xdem_world w, double out[4]);
+int32_t xdem_set_lees_edwards(xdem_world w, const double in[4]);
+/* setShiftStrainRate (LeesEdwardsBoundaryWorld.cpp:485-489) */
+int32_t xdem_set_shift_strain_rate(xdem_world w, double rate);
+/* setTimeIncrement (BaseWorld.cpp:178-181) */
+int32_t xdem_set_time_increment(xdem_world w, double dt);
+/* BaseParticle::_GlobalDamping_ (BaseParticle.cpp:9) */
+int32_t xdem_set_global_damping(xdem_world w, double damping);
+/* setFriction/setRestitutionCoeff/recalculateFactor
+   (ContactModel_LinearDissipativeFrictional.cpp:56-71); the damping constant
+   of an existing contact is kept, as in the reference */
+int32_t xdem_set_contact_model(xdem_world w, double kn, double kt, double restitution,
+                               double friction);
+/* setVirtualBoundaryMass() / (mass) and setMaxStrainRate
+   (PeriodicControlWorld.cpp:58-71) */
+int32_t xdem_set_virtual_boundary_mass(xdem_world w, double mass /* <0: from particles */);
+int32_t xdem_set_max_strain_rate(xdem_world w, double rate);
+/* kinetic energy (BaseWorld.cpp:302-310) */
+int32_t xdem_get_kinetic_energy(xdem_world w, double* out);
+
+/* ---- sub-steps (each one reference method) ----------------------------- */
+/* PeriodicBoundaryWorld::modifyParticlePosition (PeriodicBoundaryWorld.cpp:129-142)
+   or LeesEdwardsBoundaryWorld::modifyParticlePosition (LeesEdwardsBoundaryWorld.cpp:304-333) */
+int32_t xdem_modify_particle_position(xdem_world w);
+/* LeesEdwardsBoundaryWorld::apply/removeBackgroudVelocity (:508-530) */
+int32_t xdem_apply_background_velocity(xdem_world w);
+int32_t xdem_remove_background_velocity(xdem_world w);
+/* findPossibleContacts: the cell grid (PeriodicBoundaryWorld.cpp:12-85,
+   LeesEdwardsBoundaryWorld.cpp:34-205).  Candidates are generated from it
+   inside xdem_update_contacts; the set is the same. */
+int32_t xdem_find_possible_contacts(xdem_world w);
+/* updateContacts: per candidate pair geometry, force and history
+   (PeriodicBoundaryWorld.cpp:87-107, LeesEdwardsBoundaryWorld.cpp:207-283,
+   BaseParticle.cpp:27-98) */
+int32_t xdem_update_contacts(xdem_world w);
+/* BaseWorld::collectForceAndTorque (BaseWorld.cpp:17-57) */
+int32_t xdem_collect_force_and_torque(xdem_world w);
+/* BaseWorld::takeTimeIntegral (BaseWorld.cpp:59-77, BaseParticle.cpp:107-118,
+   GluedParticle.cpp:91-125) */
+int32_t xdem_take_time_integral(xdem_world w);
+/* BaseWorld::resetVelocityOfRattlers / scaleVelocityOfRattlers (BaseWorld.cpp:79-106) */
+int32_t xdem_reset_velocity_of_rattlers(xdem_world w);
+int32_t xdem_scale_velocity_of_rattlers(xdem_world w, double scale);
+/* BaseWorld::updateTotalStress (BaseWorld.cpp:158-176); stress may be NULL */
+int32_t xdem_update_total_stress(xdem_world w, double stress[4]);
+/* PeriodicControlWorld box laws (PeriodicControlWorld.cpp:124-237) */
+int32_t xdem_update_boundary(xdem_world w, int32_t box_law, double p0, double p1);
+/* LeesEdwardsBoundaryWorld::updateLeesEdwardBoundary (:285-296) */
+int32_t xdem_update_lees_edwards_boundary(xdem_world w);
+/* scaleBoundarySizeToGivenSolidFraction (PeriodicBoundaryWorld.cpp:276-284) */
+int32_t xdem_scale_boundary_to_solid_fraction(xdem_world w, double solid_fraction);
+
+/* ---- whole steps -------------------------------------------------------- */
+/* the world kind's takeTimeStep() */
+int32_t xdem_take_time_step(xdem_world w);
+/* nsteps iterations of ctl's sequence with fused kernels, captured in a CUDA
+   graph; *steps_done (may be NULL) receives the number of steps executed.
+   Returns the OR of all status bits raised (synchronises once at the end). */
+int32_t xdem_run(xdem_world w, int32_t nsteps, const xdem_control* ctl, int32_t* steps_done);
+/* wait for the handle's stream; returns and clears the device status word */
+int32_t xdem_synchronize(xdem_world w);
+
+/* ---- single-pair geometry (known-answer tests) ------------------------- */
+/* BaseParticle::calculateContactGeometry for one pair on the device.
+   pi/pj: {shape, radius, aspect_ratio, x, y, vx, vy, rot, rot_vel};
+   out: {contacted, nx, ny, cpx, cpy, bv1x, bv1y, bv2x, bv2y, overlap,
+         rvx, rvy, nrvx, nrvy, srvx, srvy, newton_iterations} per pair. */
+int32_t xdem_pair_geometry(int32_t npairs, int32_t ellipse_method, int32_t precision,
+                           const double* pi /* npairs*9 */, const double* pj /* npairs*9 */,
+                           const double* offset /* npairs*4: ox, oy, ovx, ovy */,
+                           double* out /* npairs*17 */);
+
+/* ---- packing generation (host only, no GPU) ------------------------------ */
+/* Random sequential addition of discs of the given bounding radii into the
+   box [xmin,xmax]x[ymin,ymax] without overlap; seeded, deterministic.
+   Returns XDEM_ERR_CAPACITY if max_attempts proposals for one disc fail. */
+int32_t xdem_rsa_positions(int32_t n, const double* radius, const double box[4], uint64_t seed,
+                           int64_t max_attempts, double* x, double* y);
+
+/* CircularParticle/EllipticParticle::calculateParticleProperties(density)
+   (CircularParticle.cpp:16-23, EllipticParticle.cpp:7-14) */
+int32_t xdem_particle_properties(int32_t n, const int32_t* shape, const double* radius,
+                                 const double* aspect_ratio, double density, double* volume,
+                                 double* mass, double* inv_mass, double* inertia,
+                                 double* inv_inertia);
+/* GluedParticle::calculateParticleProperties(density) (GluedParticle.cpp:7-80)
+   for one clump of nsub sub-particles; out_clump = {x, y, volume, mass,
+   inv_mass, inertia, inv_inertia}; branch_x/y receive each sub-particle's
+   branch vector.  The sub-particles take the clump's mass and inertia. */
+int32_t xdem_clump_properties(int32_t nsub, const int32_t* sub_shape, const double* sub_radius,
+                              const double* sub_aspect_ratio, const double* sub_x,
+                              const double* sub_y, const double* sub_rot, double density,
+                              double* out_clump, double* branch_x, double* branch_y);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* XDEM_GPU_H */

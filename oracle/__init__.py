@@ -1,0 +1,236 @@
+"""TEST INFRASTRUCTURE ONLY — the CPU checkers of the CUDA path.
+
+Two checkers share the reference-named interface of xdem_b200.world.WorldBase:
+  PortWorld  the C restatement in oracle/xdem_oracle.c (liboracle.so), built
+             by `make -C oracle` (and by __graft_entry__.build());
+  RefWorld   the unmodified reference sources compiled with
+             oracle/ref_harness.cpp into oracle/_ref/libxdem_ref.so.  It is only
+             present where the reference sources were available at build time.
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg may use
+this package; the product never imports it.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+from xdem_b200 import abi
+from xdem_b200.world import WorldBase
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PORT_LIB = os.path.join(HERE, "liboracle.so")
+REF_LIB = os.path.join(HERE, "_ref", "libxdem_ref.so")
+
+_d = C.POINTER(C.c_double)
+_i = C.POINTER(C.c_int32)
+_port = None
+_ref = None
+
+
+def build(ref_src="/root/reference/src"):
+    """make -C oracle (the restatement always; the reference when its sources exist)."""
+    subprocess.run(["make", "-s", "-C", HERE, f"REF_SRC={ref_src}"], check=True)
+
+
+def ref_available():
+    return os.path.exists(REF_LIB)
+
+
+def _bind(lib, prefix):
+    P = C.POINTER
+    V = C.c_void_p
+    sig = {
+        "create": (V, [P(abi.Params), C.c_int32]),
+        "destroy": (None, [V]),
+        "set_particles": (C.c_int32, [V, P(abi.Particles)]),
+        "get_particles": (C.c_int32, [V, P(abi.Particles)]),
+        "set_contacts": (C.c_int32, [V, P(abi.Contacts)]),
+        "get_contacts": (C.c_int32, [V, P(abi.Contacts)]),
+        "get_force_and_torque": (C.c_int32, [V, _d, _d, _d, _i]),
+        "get_boundary": (None, [V, _d]),
+        "get_stress": (None, [V, _d]),
+        "get_lees_edwards": (None, [V, _d]),
+        "set_lees_edwards": (None, [V, _d]),
+        "set_virtual_boundary_mass": (None, [V, C.c_double]),
+        "set_max_strain_rate": (None, [V, C.c_double]),
+        "kinetic_energy": (C.c_double, [V]),
+        "count_contacts": (C.c_int64, [V]),
+        "call": (C.c_int32, [V, C.c_int32, C.c_double, C.c_double, C.c_double]),
+        "run": (C.c_int32, [V, C.c_int32, P(abi.Control), P(C.c_int32)]),
+        "quadron_z_phi": (None, [V, _d]),
+        "pair_geometry": (C.c_int32, [C.c_int32, C.c_int32, _d, _d, _d, _d]),
+    }
+    fns = {}
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, prefix + name)
+        fn.restype = res
+        fn.argtypes = args
+        fns[name] = fn
+    return fns
+
+
+def port_lib():
+    global _port
+    if _port is None:
+        if not os.path.exists(PORT_LIB):
+            raise ImportError(f"{PORT_LIB} missing: run `make -C oracle`")
+        lib = C.CDLL(PORT_LIB)
+        _port = _bind(lib, "xo_")
+        lib.xo_status.restype = C.c_uint32
+        lib.xo_status.argtypes = [C.c_void_p]
+        lib.xo_newton_quartic.restype = C.c_double
+        lib.xo_newton_quartic.argtypes = [C.c_double] * 6 + [_i]
+        _port["status"] = lib.xo_status
+        _port["newton_quartic"] = lib.xo_newton_quartic
+    return _port
+
+
+def ref_lib():
+    global _ref
+    if _ref is None:
+        if not ref_available():
+            raise ImportError(f"{REF_LIB} missing: the reference was not compiled here")
+        lib = C.CDLL(REF_LIB)
+        _ref = _bind(lib, "refh_")
+        lib.refh_particle_properties.restype = None
+        lib.refh_particle_properties.argtypes = [C.c_int32, _i, _d, _d, C.c_double] + [_d] * 5
+        lib.refh_clump_properties.restype = None
+        lib.refh_clump_properties.argtypes = [C.c_int32, _i, _d, _d, _d, _d, _d, C.c_double, _d,
+                                              _d, _d]
+        lib.refh_set_threads.restype = None
+        lib.refh_set_threads.argtypes = [C.c_void_p, C.c_int32]
+        lib.refh_get_control_mass.restype = C.c_double
+        lib.refh_get_control_mass.argtypes = [C.c_void_p]
+        _ref["particle_properties"] = lib.refh_particle_properties
+        _ref["clump_properties"] = lib.refh_clump_properties
+        _ref["set_threads"] = lib.refh_set_threads
+        _ref["control_mass"] = lib.refh_get_control_mass
+    return _ref
+
+
+class _CpuWorld(WorldBase):
+    def __init__(self, fns, params, threads=1):
+        self.f = fns
+        self.params = params
+        self.h = fns["create"](C.byref(params), threads)
+        self.n = 0
+
+    def close(self):
+        if self.h:
+            self.f["destroy"](self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _set_particles(self, s):
+        return self.f["set_particles"](self.h, C.byref(s))
+
+    def _get_state(self, s):
+        return self.f["get_particles"](self.h, C.byref(s))
+
+    def _set_contacts(self, s):
+        return self.f["set_contacts"](self.h, C.byref(s))
+
+    def _get_contacts(self, s):
+        return self.f["get_contacts"](self.h, C.byref(s))
+
+    def _forces(self, fx, fy, t, nc):
+        return self.f["get_force_and_torque"](self.h, fx, fy, t, nc)
+
+    def count_contacts(self):
+        return int(self.f["count_contacts"](self.h))
+
+    def _call(self, which, a=0.0, b=0.0, c=0.0):
+        return self._status(self.f["call"](self.h, which, a, b, c))
+
+    def _run(self, nsteps, ctl, done):
+        return self._status(self.f["run"](self.h, nsteps, C.byref(ctl), C.byref(done)))
+
+    def _status(self, st):
+        return st
+
+    def _boundary(self, p):
+        self.f["get_boundary"](self.h, p)
+
+    def _stress(self, p):
+        self.f["get_stress"](self.h, p)
+
+    def _le(self, p):
+        self.f["get_lees_edwards"](self.h, p)
+
+    def _set_le(self, p):
+        self.f["set_lees_edwards"](self.h, p)
+
+    def _ke(self):
+        return float(self.f["kinetic_energy"](self.h))
+
+    def setVirtualBoundaryMass(self, mass=-1.0):
+        self.f["set_virtual_boundary_mass"](self.h, mass)
+
+    def setMaxStrainRate(self, rate):
+        self.f["set_max_strain_rate"](self.h, rate)
+
+    def quadron_z_phi(self):
+        out = np.zeros(2)
+        self.f["quadron_z_phi"](self.h, out.ctypes.data_as(_d))
+        return out
+
+
+class PortWorld(_CpuWorld):
+    """The C restatement."""
+
+    def __init__(self, params, threads=1):
+        super().__init__(port_lib(), params, threads)
+
+    def _status(self, st):
+        # status bits accumulate in the world; read and clear them
+        return int(self.f["status"](self.h))
+
+
+class RefWorld(_CpuWorld):
+    """The compiled reference."""
+
+    def __init__(self, params, threads=1):
+        super().__init__(ref_lib(), params, threads)
+
+    def set_threads(self, threads):
+        self.f["set_threads"](self.h, threads)
+
+    def control_mass(self):
+        return float(self.f["control_mass"](self.h))
+
+
+def pair_geometry(pi, pj, off, method=abi.ELLIPSE_CLOSEST_APPROACH, which="port"):
+    fns = port_lib() if which == "port" else ref_lib()
+    pi = np.ascontiguousarray(pi, np.float64)
+    pj = np.ascontiguousarray(pj, np.float64)
+    off = np.ascontiguousarray(off, np.float64)
+    out = np.zeros((pi.shape[0], 17))
+    st = fns["pair_geometry"](pi.shape[0], method, pi.ctypes.data_as(_d), pj.ctypes.data_as(_d),
+                              off.ctypes.data_as(_d), out.ctypes.data_as(_d))
+    return out, st
+
+
+def ref_particle_properties(shape, radius, aspect, density=1.0):
+    fns = ref_lib()
+    n = len(radius)
+    shape = np.ascontiguousarray(shape, np.int32)
+    radius = np.ascontiguousarray(radius, np.float64)
+    aspect = np.ascontiguousarray(aspect, np.float64)
+    out = {k: np.zeros(n) for k in ("volume", "mass", "inv_mass", "inertia", "inv_inertia")}
+    fns["particle_properties"](n, shape.ctypes.data_as(_i), radius.ctypes.data_as(_d),
+                               aspect.ctypes.data_as(_d), density,
+                               *[out[k].ctypes.data_as(_d) for k in
+                                 ("volume", "mass", "inv_mass", "inertia", "inv_inertia")])
+    return out
+
+
+def newton_quartic(A, B, Cc, D, E, init):
+    it = C.c_int32(0)
+    r = port_lib()["newton_quartic"](A, B, Cc, D, E, init, C.byref(it))
+    return r, it.value

@@ -1,0 +1,948 @@
+// api.cu — the C-ABI of include/xdem_gpu.h: world lifetime, host<->device
+// transfers, and the launch sequences of each reference step.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "../../include/xdem_gpu.h"
+#include "kernels.cuh"
+
+using namespace xdem;
+
+namespace {
+
+constexpr int kBlock = 128;
+constexpr int kDefaultSlots = 16;
+constexpr double kPi = 3.14159265358979323846;
+
+inline int blocks_for(int n, int b) { return (n + b - 1) / b; }
+
+struct DeviceBuffers {
+  std::vector<void*> ptrs;
+  template <class T>
+  cudaError_t alloc(T** p, size_t count) {
+    void* q = nullptr;
+    cudaError_t e = cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(T));
+    if (e != cudaSuccess) return e;
+    ptrs.push_back(q);
+    *p = static_cast<T*>(q);
+    return cudaSuccess;
+  }
+  void release() {
+    for (void* p : ptrs) cudaFree(p);
+    ptrs.clear();
+  }
+};
+
+}  // namespace
+
+struct xdem_world_s {
+  xdem_params prm{};
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  DevWorld dw{};
+  DeviceBuffers particle_bufs;
+  WorldScalars* ws = nullptr;
+  uint32_t* status = nullptr;
+  int par = 0;            // slot set holding the latest contacts
+  int nx_cap = 0, ny_cap = 0;
+  int partial_blocks = 0;
+  uint32_t host_status = 0;
+  double total_volume = 0.0;
+  double control_mass = 0.0;
+};
+
+namespace {
+
+inline uint32_t cuda_check(xdem_world_s* w, cudaError_t e) {
+  if (e == cudaSuccess) return 0;
+  if (w) w->host_status |= XDEM_ERR_CUDA;
+  return XDEM_ERR_CUDA;
+}
+
+#define CK(w, call)                                    \
+  do {                                                 \
+    if (uint32_t _s = cuda_check((w), (call))) return (int32_t)_s; \
+  } while (0)
+
+double factor_of(double kn, double e) {
+  // ContactModel_LinearDissipativeFrictioanl ctor (…Frictional.h:18-23)
+  double lg = std::log(e);
+  return 2.0 * std::sqrt(kn) * std::fabs(lg) / std::sqrt(kPi * kPi + lg * lg);
+}
+
+cudaError_t read_scalars(xdem_world_s* w, WorldScalars* out) {
+  cudaError_t e = cudaMemcpyAsync(out, w->ws, sizeof(WorldScalars), cudaMemcpyDeviceToHost, w->stream);
+  if (e != cudaSuccess) return e;
+  return cudaStreamSynchronize(w->stream);
+}
+
+cudaError_t write_scalars(xdem_world_s* w, const WorldScalars* in) {
+  cudaError_t e = cudaMemcpyAsync(w->ws, in, sizeof(WorldScalars), cudaMemcpyHostToDevice, w->stream);
+  if (e != cudaSuccess) return e;
+  return cudaStreamSynchronize(w->stream);
+}
+
+template <class T>
+cudaError_t upload(T* dst, const T* src, size_t count, cudaStream_t s) {
+  return cudaMemcpyAsync(dst, src, count * sizeof(T), cudaMemcpyHostToDevice, s);
+}
+template <class T>
+cudaError_t download(T* dst, const T* src, size_t count, cudaStream_t s) {
+  return cudaMemcpyAsync(dst, src, count * sizeof(T), cudaMemcpyDeviceToHost, s);
+}
+
+// ---- launch helpers -------------------------------------------------------
+void launch_modify(xdem_world_s* w) {
+  int n = w->dw.n;
+  k_modify_position<<<blocks_for(n, kBlock), kBlock, 0, w->stream>>>(w->dw);
+}
+
+void launch_find(xdem_world_s* w) {
+  int n = w->dw.n;
+  k_bin<<<blocks_for(n, kBlock), kBlock, 0, w->stream>>>(w->dw);
+  k_scan<<<1, 1024, 0, w->stream>>>(w->dw);
+  int cells = w->nx_cap * w->ny_cap + 2 * w->nx_cap;
+  int nb = std::max(blocks_for(n, kBlock), std::min(blocks_for(cells, kBlock), 1184));
+  k_scatter<<<nb, kBlock, 0, w->stream>>>(w->dw);
+}
+
+void launch_update(xdem_world_s* w, bool fold_bg, int record) {
+  int n = w->dw.n;
+  if (fold_bg)
+    k_update_contacts<true><<<blocks_for(n, 128), 128, 0, w->stream>>>(w->dw, w->par, record);
+  else
+    k_update_contacts<false><<<blocks_for(n, 128), 128, 0, w->stream>>>(w->dw, w->par, record);
+  w->par ^= 1;
+}
+
+void launch_collect(xdem_world_s* w) {
+  int n = w->dw.n;
+  k_collect<<<blocks_for(n, 128), 128, 0, w->stream>>>(w->dw, w->par);
+}
+
+void launch_integrate(xdem_world_s* w, bool fold_bg, int reset) {
+  int n = w->dw.n;
+  if (fold_bg)
+    k_integrate<true><<<blocks_for(n, kBlock), kBlock, 0, w->stream>>>(w->dw, reset);
+  else
+    k_integrate<false><<<blocks_for(n, kBlock), kBlock, 0, w->stream>>>(w->dw, reset);
+}
+
+void launch_stress(xdem_world_s* w) {
+  int nb = blocks_for(w->dw.n, kReduceBlock);
+  k_stress_partial<<<nb, kReduceBlock, 0, w->stream>>>(w->dw, w->par);
+  k_stress_final<<<1, 1024, 0, w->stream>>>(w->dw, nb);
+}
+
+void launch_rattlers(xdem_world_s* w, int reset, double scale) {
+  int n = w->dw.n;
+  k_rattlers<<<blocks_for(n, kBlock), kBlock, 0, w->stream>>>(w->dw, reset, scale);
+}
+
+void launch_end_of_step(xdem_world_s* w, int law, double p0, double p1, int le_update, int stop_on,
+                        double stop_p) {
+  k_end_of_step<<<1, 1, 0, w->stream>>>(w->dw, law, p0, p1, le_update, stop_on, stop_p);
+  if (law != BOX_NONE)
+    k_scale_positions<<<blocks_for(w->dw.n, kBlock), kBlock, 0, w->stream>>>(w->dw);
+}
+
+// one step of a control sequence; record: store the full contact record
+void enqueue_step(xdem_world_s* w, const xdem_control* ctl, int record) {
+  int kind = w->prm.world_kind;
+  bool own = ctl->sequence == XDEM_SEQ_TAKE_TIME_STEP;
+  bool le = own && kind == XDEM_WORLD_LEES_EDWARDS;
+  if (ctl->scale_rattlers) launch_rattlers(w, 0, ctl->rattler_scale);
+  launch_modify(w);
+  launch_find(w);
+  launch_update(w, le, record);
+  launch_collect(w);
+  launch_integrate(w, le, own && kind == XDEM_WORLD_PERIODIC_CONTROL);
+  if (ctl->reset_rattlers) launch_rattlers(w, 1, 0.0);
+  if (ctl->update_stress) launch_stress(w);
+  launch_end_of_step(w, ctl->box_law, ctl->p0, ctl->p1, le ? 1 : 0, ctl->stop_on_pressure,
+                     ctl->stop_pressure);
+}
+
+uint32_t fetch_status(xdem_world_s* w) {
+  uint32_t s = 0;
+  cudaError_t e = cudaMemcpyAsync(&s, w->status, sizeof(uint32_t), cudaMemcpyDeviceToHost, w->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(w->status, 0, sizeof(uint32_t), w->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(w->stream);
+  if (e != cudaSuccess) w->host_status |= XDEM_ERR_CUDA;
+  s |= w->host_status;
+  w->host_status = 0;
+  return s;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t xdem_abi_version(void) { return XDEM_ABI_VERSION; }
+
+const char* xdem_status_string(int32_t bit) {
+  switch (bit) {
+    case XDEM_OK: return "ok";
+    case XDEM_ERR_CAPACITY: return "capacity exceeded (candidate list or contact slots)";
+    case XDEM_ERR_NEWTON: return "closest-approach Newton iteration did not converge";
+    case XDEM_ERR_NONFINITE: return "non-finite value";
+    case XDEM_ERR_UNSUPPORTED_PAIR: return "no contact law for this pair of shapes";
+    case XDEM_ERR_ZERO_VECTOR: return "normalisation of a zero-length vector";
+    case XDEM_ERR_CUDA: return "CUDA runtime error";
+    case XDEM_ERR_ARGUMENT: return "invalid argument";
+    case XDEM_ERR_GRID: return "cell grid has fewer than 3 cells along an axis";
+    default: return "unknown status";
+  }
+}
+
+int32_t xdem_device_count(int32_t* out) {
+  int c = 0;
+  cudaError_t e = cudaGetDeviceCount(&c);
+  if (out) *out = (e == cudaSuccess) ? c : 0;
+  return (e == cudaSuccess && c > 0) ? XDEM_OK : XDEM_ERR_CUDA;
+}
+
+int32_t xdem_create(const xdem_params* prm, xdem_world* out) {
+  if (!prm || !out) return XDEM_ERR_ARGUMENT;
+  *out = nullptr;
+  if (prm->world_kind < 0 || prm->world_kind > 2 || prm->ellipse_method < 0 ||
+      prm->ellipse_method > 1 || prm->precision < 0 || prm->precision > 1 ||
+      prm->max_contacts < 0 || prm->max_contacts > kMaxSlots || !(prm->dt > 0.0))
+    return XDEM_ERR_ARGUMENT;
+  xdem_world_s* w = new (std::nothrow) xdem_world_s();
+  if (!w) return XDEM_ERR_ARGUMENT;
+  w->prm = *prm;
+  if (cudaStreamCreateWithFlags(&w->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete w;
+    return XDEM_ERR_CUDA;
+  }
+  w->own_stream = true;
+  if (cudaMalloc(&w->ws, sizeof(WorldScalars)) != cudaSuccess ||
+      cudaMalloc(&w->status, sizeof(uint32_t)) != cudaSuccess) {
+    xdem_destroy(w);
+    return XDEM_ERR_CUDA;
+  }
+  WorldScalars s{};
+  s.xmin = prm->xmin;
+  s.xmax = prm->xmax;
+  s.ymin = prm->ymin;
+  s.ymax = prm->ymax;
+  s.xlen = s.xmax - s.xmin;
+  s.ylen = s.ymax - s.ymin;
+  s.shift_rate = prm->shift_strain_rate;
+  s.shift_vel = s.shift_rate * s.ylen;  // setShiftStrainRate (LeesEdwardsBoundaryWorld.cpp:485-489)
+  s.dt = prm->dt;
+  s.g = prm->global_damping;
+  s.kn = prm->normal_stiffness;
+  s.kt = prm->shear_stiffness;
+  s.mu = prm->frictional_coeff;
+  s.factor = factor_of(prm->normal_stiffness, prm->restitution_coeff);
+  s.scale_x = s.scale_y = 1.0;
+  if (write_scalars(w, &s) != cudaSuccess || cudaMemset(w->status, 0, sizeof(uint32_t)) != cudaSuccess) {
+    xdem_destroy(w);
+    return XDEM_ERR_CUDA;
+  }
+  w->dw.ws = w->ws;
+  w->dw.status = w->status;
+  w->dw.kind = prm->world_kind;
+  w->dw.method = prm->ellipse_method;
+  w->dw.precision = prm->precision;
+  w->dw.K = prm->max_contacts > 0 ? prm->max_contacts : kDefaultSlots;
+  *out = w;
+  return XDEM_OK;
+}
+
+int32_t xdem_destroy(xdem_world w) {
+  if (!w) return XDEM_OK;
+  if (w->stream) cudaStreamSynchronize(w->stream);
+  w->particle_bufs.release();
+  if (w->ws) cudaFree(w->ws);
+  if (w->status) cudaFree(w->status);
+  if (w->own_stream && w->stream) cudaStreamDestroy(w->stream);
+  delete w;
+  return XDEM_OK;
+}
+
+int32_t xdem_set_stream(xdem_world w, void* s) {
+  if (!w) return XDEM_ERR_ARGUMENT;
+  cudaStreamSynchronize(w->stream);
+  if (w->own_stream) cudaStreamDestroy(w->stream);
+  if (s) {
+    w->stream = static_cast<cudaStream_t>(s);
+    w->own_stream = false;
+  } else {
+    CK(w, cudaStreamCreateWithFlags(&w->stream, cudaStreamNonBlocking));
+    w->own_stream = true;
+  }
+  return XDEM_OK;
+}
+
+int32_t xdem_set_particles(xdem_world w, const xdem_particles* P) {
+  if (!w || !P || P->n <= 0) return XDEM_ERR_ARGUMENT;
+  const int n = P->n;
+  if ((int64_t)n * w->dw.K >= (int64_t)1 << 31) return XDEM_ERR_ARGUMENT;
+  if (!P->shape || !P->up_level || !P->setting || !P->outer_radius || !P->radius ||
+      !P->aspect_ratio || !P->x || !P->y || !P->vx || !P->vy || !P->rot || !P->rot_vel ||
+      !P->volume || !P->mass || !P->inv_mass || !P->inertia || !P->inv_inertia)
+    return XDEM_ERR_ARGUMENT;
+  cudaStreamSynchronize(w->stream);
+  w->particle_bufs.release();
+  DevWorld& d = w->dw;
+  d.n = n;
+  const int K = d.K;
+  DeviceBuffers& B = w->particle_bufs;
+  int32_t *shape, *up, *setting, *num_sub;
+  double *orad, *rad, *asp, *mass, *im, *I, *iI, *vol;
+  CK(w, B.alloc(&shape, n));
+  CK(w, B.alloc(&up, n));
+  CK(w, B.alloc(&setting, n));
+  CK(w, B.alloc(&num_sub, n));
+  CK(w, B.alloc(&orad, n));
+  CK(w, B.alloc(&rad, n));
+  CK(w, B.alloc(&asp, n));
+  CK(w, B.alloc(&mass, n));
+  CK(w, B.alloc(&im, n));
+  CK(w, B.alloc(&I, n));
+  CK(w, B.alloc(&iI, n));
+  CK(w, B.alloc(&vol, n));
+  CK(w, B.alloc(&d.pos, n));
+  CK(w, B.alloc(&d.vel, n));
+  CK(w, B.alloc(&d.rot, n));
+  CK(w, B.alloc(&d.w, n));
+  CK(w, B.alloc(&d.branch, n));
+  CK(w, B.alloc(&d.rattler, n));
+  CK(w, B.alloc(&d.force, n));
+  CK(w, B.alloc(&d.torque, n));
+  CK(w, B.alloc(&d.ncp, n));
+  d.shape = shape;
+  d.up = up;
+  d.setting = setting;
+  d.num_sub = num_sub;
+  d.orad = orad;
+  d.rad = rad;
+  d.asp = asp;
+  d.mass = mass;
+  d.im = im;
+  d.I = I;
+  d.iI = iI;
+  d.vol = vol;
+  // host-side derived data
+  std::vector<double2> pos(n), vel(n), br(n);
+  std::vector<int32_t> ns(n, 0), rat(n, 0);
+  double maxr = 0.0, volsum = 0.0, msum = 0.0;
+  for (int i = 0; i < n; ++i) {
+    pos[i] = make_double2(P->x[i], P->y[i]);
+    vel[i] = make_double2(P->vx[i], P->vy[i]);
+    br[i] = make_double2(P->branch_x ? P->branch_x[i] : 0.0, P->branch_y ? P->branch_y[i] : 0.0);
+    if (P->num_sub) ns[i] = P->num_sub[i];
+    if (P->is_rattler) rat[i] = P->is_rattler[i];
+    if (P->shape[i] < 0 || P->shape[i] > 2) return XDEM_ERR_ARGUMENT;
+    if (P->shape[i] == XDEM_SHAPE_CLUMP && (ns[i] < 0 || i + ns[i] >= n)) return XDEM_ERR_ARGUMENT;
+    if (P->outer_radius[i] > maxr) maxr = P->outer_radius[i];  // BaseWorld.cpp:201-219
+    if (!(P->setting[i] & XDEM_SKIP_MACRO_SUM)) {
+      volsum += P->volume[i];  // BaseWorld.cpp:188-199
+      msum += P->mass[i];
+    }
+  }
+  cudaStream_t s = w->stream;
+  CK(w, upload(shape, P->shape, n, s));
+  CK(w, upload(up, P->up_level, n, s));
+  CK(w, upload(setting, P->setting, n, s));
+  CK(w, upload(num_sub, ns.data(), n, s));
+  CK(w, upload(orad, P->outer_radius, n, s));
+  CK(w, upload(rad, P->radius, n, s));
+  CK(w, upload(asp, P->aspect_ratio, n, s));
+  CK(w, upload(mass, P->mass, n, s));
+  CK(w, upload(im, P->inv_mass, n, s));
+  CK(w, upload(I, P->inertia, n, s));
+  CK(w, upload(iI, P->inv_inertia, n, s));
+  CK(w, upload(vol, P->volume, n, s));
+  CK(w, upload(d.pos, pos.data(), n, s));
+  CK(w, upload(d.vel, vel.data(), n, s));
+  CK(w, upload(d.rot, P->rot, n, s));
+  CK(w, upload(d.w, P->rot_vel, n, s));
+  CK(w, upload(d.branch, br.data(), n, s));
+  CK(w, upload(d.rattler, rat.data(), n, s));
+  CK(w, cudaMemsetAsync(d.force, 0, sizeof(double2) * n, s));
+  CK(w, cudaMemsetAsync(d.torque, 0, sizeof(double) * n, s));
+  CK(w, cudaMemsetAsync(d.ncp, 0, sizeof(int32_t) * n, s));
+  w->total_volume = volsum;
+  w->control_mass = msum / ((double)n * 10.0);  // setVirtualBoundaryMass (PeriodicControlWorld.cpp:58-66)
+  WorldScalars ws;
+  CK(w, read_scalars(w, &ws));
+  ws.maxsize = w->prm.max_particle_size > 0 ? w->prm.max_particle_size : maxr * 2.01;
+  // grid capacity: twice the starting grid per axis, so a growing box keeps
+  // its cell size for a while and then coarsens
+  int nx0 = (int)std::floor(ws.xlen / ws.maxsize), ny0 = (int)std::floor(ws.ylen / ws.maxsize);
+  w->nx_cap = std::max(3, 2 * nx0 + 4);
+  w->ny_cap = std::max(3, 2 * ny0 + 4);
+  d.nx_cap = w->nx_cap;
+  d.ny_cap = w->ny_cap;
+  CK(w, write_scalars(w, &ws));
+  size_t cells = (size_t)w->nx_cap * w->ny_cap + 2 * (size_t)w->nx_cap;
+  CK(w, B.alloc(&d.cell_count, cells + 1));
+  CK(w, B.alloc(&d.cell_start, cells + 1));
+  CK(w, B.alloc(&d.cell_mem, 2 * (size_t)n));
+  CK(w, B.alloc(&d.pcell, n));
+  CK(w, B.alloc(&d.prank, n));
+  CK(w, B.alloc(&d.gcell, n));
+  CK(w, B.alloc(&d.grank, n));
+  CK(w, cudaMemsetAsync(d.cell_count, 0, sizeof(int32_t) * (cells + 1), s));
+  size_t ks = (size_t)K * n;
+  for (int b = 0; b < 2; ++b) {
+    Slots& S = d.slots[b];
+    CK(w, B.alloc(&S.count, n));
+    CK(w, B.alloc(&S.partner, ks));
+    CK(w, B.alloc(&S.n, ks));
+    CK(w, B.alloc(&S.s, ks));
+    CK(w, B.alloc(&S.damp, ks));
+    CK(w, B.alloc(&S.f, ks));
+    CK(w, B.alloc(&S.t1, ks));
+    CK(w, B.alloc(&S.t2, ks));
+    CK(w, B.alloc(&S.b, ks));
+    CK(w, B.alloc(&S.cp, ks));
+    CK(w, B.alloc(&S.bv1, ks));
+    CK(w, B.alloc(&S.bv2, ks));
+    CK(w, B.alloc(&S.fn, ks));
+    CK(w, B.alloc(&S.ft, ks));
+    CK(w, cudaMemsetAsync(S.count, 0, sizeof(int32_t) * n, s));
+  }
+  CK(w, B.alloc(&d.incnt, n));
+  CK(w, B.alloc(&d.inref, ks));
+  CK(w, cudaMemsetAsync(d.incnt, 0, sizeof(int32_t) * n, s));
+  w->partial_blocks = blocks_for(n, kReduceBlock);
+  CK(w, B.alloc(&d.partials, 4 * (size_t)w->partial_blocks + 4));
+  w->par = 0;
+  CK(w, cudaStreamSynchronize(s));
+  return XDEM_OK;
+}
+
+int32_t xdem_get_particles(xdem_world w, xdem_particles* P) {
+  if (!w || !P || w->dw.n <= 0) return XDEM_ERR_ARGUMENT;
+  const int n = w->dw.n;
+  const DevWorld& d = w->dw;
+  cudaStream_t s = w->stream;
+  std::vector<double2> pos(n), vel(n), br(n);
+  CK(w, download(pos.data(), d.pos, n, s));
+  CK(w, download(vel.data(), d.vel, n, s));
+  CK(w, download(br.data(), d.branch, n, s));
+  if (P->rot) CK(w, download(P->rot, d.rot, n, s));
+  if (P->rot_vel) CK(w, download(P->rot_vel, d.w, n, s));
+  if (P->is_rattler) CK(w, download(P->is_rattler, d.rattler, n, s));
+  if (P->mass) CK(w, download(P->mass, d.mass, n, s));
+  if (P->inertia) CK(w, download(P->inertia, d.I, n, s));
+  if (P->shape) CK(w, download(P->shape, d.shape, n, s));
+  if (P->setting) CK(w, download(P->setting, d.setting, n, s));
+  if (P->up_level) CK(w, download(P->up_level, d.up, n, s));
+  CK(w, cudaStreamSynchronize(s));
+  P->n = n;
+  for (int i = 0; i < n; ++i) {
+    if (P->x) P->x[i] = pos[i].x;
+    if (P->y) P->y[i] = pos[i].y;
+    if (P->vx) P->vx[i] = vel[i].x;
+    if (P->vy) P->vy[i] = vel[i].y;
+    if (P->branch_x) P->branch_x[i] = br[i].x;
+    if (P->branch_y) P->branch_y[i] = br[i].y;
+  }
+  return XDEM_OK;
+}
+
+int32_t xdem_set_contacts(xdem_world w, const xdem_contacts* C) {
+  if (!w || !C || w->dw.n <= 0 || C->count < 0) return XDEM_ERR_ARGUMENT;
+  const int n = w->dw.n, K = w->dw.K;
+  const size_t ks = (size_t)K * n;
+  std::vector<int32_t> cnt(n, 0), partner(ks, 0);
+  std::vector<double2> nn(ks), sh(ks), f(ks), b(ks), cp(ks), bv1(ks), bv2(ks), fn(ks), ft(ks);
+  std::vector<double> damp(ks), t1(ks), t2(ks);
+  uint32_t st = 0;
+  for (int64_t k = 0; k < C->count; ++k) {
+    int i = C->id_i[k], j = C->id_j[k];
+    if (i < 0 || i >= n || j < 0 || j >= n || i >= j) return XDEM_ERR_ARGUMENT;
+    int s = cnt[i];
+    if (s >= K) {
+      st |= XDEM_ERR_CAPACITY;
+      continue;
+    }
+    cnt[i]++;
+    size_t ci = (size_t)s * n + i;
+    partner[ci] = j;
+    nn[ci] = make_double2(C->normal_x[k], C->normal_y[k]);
+    sh[ci] = make_double2(C->shear_x[k], C->shear_y[k]);
+    damp[ci] = C->damping[k];
+    double2 Fn = make_double2(C->fn_x[k], C->fn_y[k]);
+    double2 Ft = make_double2(C->ft_x[k], C->ft_y[k]);
+    f[ci] = make_double2(Fn.x + Ft.x, Fn.y + Ft.y);  // ContactInformation.h:63
+    t1[ci] = C->torque_i[k];
+    t2[ci] = C->torque_j[k];
+    b[ci] = make_double2(C->branch_x[k], C->branch_y[k]);
+    cp[ci] = make_double2(C->point_x[k], C->point_y[k]);
+    bv1[ci] = make_double2(C->bv1_x[k], C->bv1_y[k]);
+    bv2[ci] = make_double2(C->bv2_x[k], C->bv2_y[k]);
+    fn[ci] = Fn;
+    ft[ci] = Ft;
+  }
+  // incoming references, ascending owner, so a collect without an update
+  // sums these contacts as the reference would
+  std::vector<int32_t> inc(n, 0);
+  std::vector<uint32_t> inref(ks, 0);
+  for (int i = 0; i < n; ++i)
+    for (int s = 0; s < cnt[i]; ++s) {
+      int j = partner[(size_t)s * n + i];
+      if (inc[j] < K) inref[(size_t)inc[j] * n + j] = (uint32_t)i * K + s;
+      else st |= XDEM_ERR_CAPACITY;
+      inc[j]++;
+    }
+  const Slots& S = w->dw.slots[w->par];
+  cudaStream_t q = w->stream;
+  CK(w, upload(S.count, cnt.data(), n, q));
+  CK(w, upload(S.partner, partner.data(), ks, q));
+  CK(w, upload(S.n, nn.data(), ks, q));
+  CK(w, upload(S.s, sh.data(), ks, q));
+  CK(w, upload(S.damp, damp.data(), ks, q));
+  CK(w, upload(S.f, f.data(), ks, q));
+  CK(w, upload(S.t1, t1.data(), ks, q));
+  CK(w, upload(S.t2, t2.data(), ks, q));
+  CK(w, upload(S.b, b.data(), ks, q));
+  CK(w, upload(S.cp, cp.data(), ks, q));
+  CK(w, upload(S.bv1, bv1.data(), ks, q));
+  CK(w, upload(S.bv2, bv2.data(), ks, q));
+  CK(w, upload(S.fn, fn.data(), ks, q));
+  CK(w, upload(S.ft, ft.data(), ks, q));
+  for (int i = 0; i < n; ++i) inc[i] = std::min(inc[i], K);
+  CK(w, upload(w->dw.incnt, inc.data(), n, q));
+  CK(w, upload(w->dw.inref, inref.data(), ks, q));
+  CK(w, cudaStreamSynchronize(q));
+  return (int32_t)st;
+}
+
+int32_t xdem_get_contacts(xdem_world w, xdem_contacts* C) {
+  if (!w || !C || w->dw.n <= 0) return XDEM_ERR_ARGUMENT;
+  const int n = w->dw.n, K = w->dw.K;
+  const size_t ks = (size_t)K * n;
+  const Slots& S = w->dw.slots[w->par];
+  cudaStream_t q = w->stream;
+  std::vector<int32_t> cnt(n), partner(ks);
+  CK(w, download(cnt.data(), S.count, n, q));
+  CK(w, download(partner.data(), S.partner, ks, q));
+  CK(w, cudaStreamSynchronize(q));
+  int64_t total = 0;
+  for (int i = 0; i < n; ++i) total += std::min(cnt[i], K);
+  C->count = total;
+  if (C->capacity < total) return XDEM_ERR_CAPACITY;
+  std::vector<double2> nn(ks), sh(ks), b(ks), cp(ks), bv1(ks), bv2(ks), fn(ks), ft(ks);
+  std::vector<double> damp(ks), t1(ks), t2(ks);
+  CK(w, download(nn.data(), S.n, ks, q));
+  CK(w, download(sh.data(), S.s, ks, q));
+  CK(w, download(b.data(), S.b, ks, q));
+  CK(w, download(cp.data(), S.cp, ks, q));
+  CK(w, download(bv1.data(), S.bv1, ks, q));
+  CK(w, download(bv2.data(), S.bv2, ks, q));
+  CK(w, download(fn.data(), S.fn, ks, q));
+  CK(w, download(ft.data(), S.ft, ks, q));
+  CK(w, download(damp.data(), S.damp, ks, q));
+  CK(w, download(t1.data(), S.t1, ks, q));
+  CK(w, download(t2.data(), S.t2, ks, q));
+  CK(w, cudaStreamSynchronize(q));
+  int64_t k = 0;
+  std::vector<std::pair<int32_t, int32_t>> order;
+  for (int i = 0; i < n; ++i) {
+    int m = std::min(cnt[i], K);
+    order.clear();
+    for (int s = 0; s < m; ++s) order.push_back({partner[(size_t)s * n + i], s});
+    std::sort(order.begin(), order.end());
+    for (auto& o : order) {
+      size_t ci = (size_t)o.second * n + i;
+      C->id_i[k] = i;
+      C->id_j[k] = o.first;
+      C->normal_x[k] = nn[ci].x;
+      C->normal_y[k] = nn[ci].y;
+      C->point_x[k] = cp[ci].x;
+      C->point_y[k] = cp[ci].y;
+      C->branch_x[k] = b[ci].x;
+      C->branch_y[k] = b[ci].y;
+      C->bv1_x[k] = bv1[ci].x;
+      C->bv1_y[k] = bv1[ci].y;
+      C->bv2_x[k] = bv2[ci].x;
+      C->bv2_y[k] = bv2[ci].y;
+      C->shear_x[k] = sh[ci].x;
+      C->shear_y[k] = sh[ci].y;
+      C->fn_x[k] = fn[ci].x;
+      C->fn_y[k] = fn[ci].y;
+      C->ft_x[k] = ft[ci].x;
+      C->ft_y[k] = ft[ci].y;
+      C->torque_i[k] = t1[ci];
+      C->torque_j[k] = t2[ci];
+      C->damping[k] = damp[ci];
+      ++k;
+    }
+  }
+  return XDEM_OK;
+}
+
+int32_t xdem_get_force_and_torque(xdem_world w, double* fx, double* fy, double* t, int32_t* nc) {
+  if (!w || w->dw.n <= 0) return XDEM_ERR_ARGUMENT;
+  const int n = w->dw.n;
+  std::vector<double2> f(n);
+  CK(w, download(f.data(), w->dw.force, n, w->stream));
+  if (t) CK(w, download(t, w->dw.torque, n, w->stream));
+  if (nc) CK(w, download(nc, w->dw.ncp, n, w->stream));
+  CK(w, cudaStreamSynchronize(w->stream));
+  for (int i = 0; i < n; ++i) {
+    if (fx) fx[i] = f[i].x;
+    if (fy) fy[i] = f[i].y;
+  }
+  return XDEM_OK;
+}
+
+int32_t xdem_count_contacts(xdem_world w, int64_t* out) {
+  if (!w || !out || w->dw.n <= 0) return XDEM_ERR_ARGUMENT;
+  std::vector<int32_t> cnt(w->dw.n);
+  CK(w, download(cnt.data(), w->dw.slots[w->par].count, w->dw.n, w->stream));
+  CK(w, cudaStreamSynchronize(w->stream));
+  int64_t t = 0;
+  for (int c : cnt) t += std::min(c, w->dw.K);
+  *out = t;
+  return XDEM_OK;
+}
+
+// ---- world scalars -------------------------------------------------------
+int32_t xdem_get_boundary(xdem_world w, double box[4]) {
+  if (!w || !box) return XDEM_ERR_ARGUMENT;
+  WorldScalars s;
+  CK(w, read_scalars(w, &s));
+  box[0] = s.xmin;
+  box[1] = s.xmax;
+  box[2] = s.ymin;
+  box[3] = s.ymax;
+  return XDEM_OK;
+}
+
+int32_t xdem_set_boundary(xdem_world w, const double box[4]) {
+  if (!w || !box) return XDEM_ERR_ARGUMENT;
+  WorldScalars s;
+  CK(w, read_scalars(w, &s));
+  s.xmin = box[0];
+  s.xmax = box[1];
+  s.ymin = box[2];
+  s.ymax = box[3];
+  s.xlen = s.xmax - s.xmin;
+  s.ylen = s.ymax - s.ymin;
+  CK(w, write_scalars(w, &s));
+  return XDEM_OK;
+}
+
+int32_t xdem_get_stress(xdem_world w, double stress[4]) {
+  if (!w || !stress) return XDEM_ERR_ARGUMENT;
+  WorldScalars s;
+  CK(w, read_scalars(w, &s));
+  for (int c = 0; c < 4; ++c) stress[c] = s.stress[c];
+  return XDEM_OK;
+}
+
+int32_t xdem_get_lees_edwards(xdem_world w, double out[4]) {
+  if (!w || !out) return XDEM_ERR_ARGUMENT;
+  WorldScalars s;
+  CK(w, read_scalars(w, &s));
+  out[0] = s.shift;
+  out[1] = s.shift_vel;
+  out[2] = s.strain;
+  out[3] = s.shift_rate;
+  return XDEM_OK;
+}
+
+int32_t xdem_set_lees_edwards(xdem_world w, const double in[4]) {
+  if (!w || !in) return XDEM_ERR_ARGUMENT;
+  WorldScalars s;
+  CK(w, read_scalars(w, &s));
+  s.shift = in[0];
+  s.shift_vel = in[1];
+  s.strain = in[2];
+  s.shift_rate = in[3];
+  CK(w, write_scalars(w, &s));
+  return XDEM_OK;
+}
+
+int32_t xdem_set_shift_strain_rate(xdem_world w, double rate) {
+  if (!w) return XDEM_ERR_ARGUMENT;
+  WorldScalars s;
+  CK(w, read_scalars(w, &s));
+  s.shift_rate = rate;
+  s.shift_vel = rate * s.ylen;
+  CK(w, write_scalars(w, &s));
+  return XDEM_OK;
+}
+
+int32_t xdem_set_time_increment(xdem_world w, double dt) {
+  if (!w || !(dt > 0.0)) return XDEM_ERR_ARGUMENT;
+  WorldScalars s;
+  CK(w, read_scalars(w, &s));
+  s.dt = dt;
+  w->prm.dt = dt;
+  CK(w, write_scalars(w, &s));
+  return XDEM_OK;
+}
+
+int32_t xdem_set_global_damping(xdem_world w, double g) {
+  if (!w) return XDEM_ERR_ARGUMENT;
+  WorldScalars s;
+  CK(w, read_scalars(w, &s));
+  s.g = g;
+  CK(w, write_scalars(w, &s));
+  return XDEM_OK;
+}
+
+int32_t xdem_set_contact_model(xdem_world w, double kn, double kt, double e, double mu) {
+  if (!w) return XDEM_ERR_ARGUMENT;
+  WorldScalars s;
+  CK(w, read_scalars(w, &s));
+  s.kn = kn;
+  s.kt = kt;
+  s.mu = mu;
+  s.factor = factor_of(kn, e);
+  CK(w, write_scalars(w, &s));
+  return XDEM_OK;
+}
+
+int32_t xdem_set_virtual_boundary_mass(xdem_world w, double mass) {
+  if (!w) return XDEM_ERR_ARGUMENT;
+  WorldScalars s;
+  CK(w, read_scalars(w, &s));
+  s.vmass = mass >= 0 ? mass : w->control_mass;
+  CK(w, write_scalars(w, &s));
+  return XDEM_OK;
+}
+
+int32_t xdem_set_max_strain_rate(xdem_world w, double r) {
+  if (!w) return XDEM_ERR_ARGUMENT;
+  WorldScalars s;
+  CK(w, read_scalars(w, &s));
+  s.max_strain_rate = r;
+  CK(w, write_scalars(w, &s));
+  return XDEM_OK;
+}
+
+int32_t xdem_get_kinetic_energy(xdem_world w, double* out) {
+  if (!w || !out || w->dw.n <= 0) return XDEM_ERR_ARGUMENT;
+  int nb = blocks_for(w->dw.n, kReduceBlock);
+  k_ke_partial<<<nb, kReduceBlock, 0, w->stream>>>(w->dw);
+  k_ke_final<<<1, 1024, 0, w->stream>>>(w->dw, nb);
+  CK(w, cudaGetLastError());
+  WorldScalars s;
+  CK(w, read_scalars(w, &s));
+  *out = s.ke;
+  return XDEM_OK;
+}
+
+// ---- sub-steps ---------------------------------------------------------------
+#define SUBSTEP_BEGIN                                   \
+  if (!w || w->dw.n <= 0) return XDEM_ERR_ARGUMENT;     \
+  do {                                                  \
+  } while (0)
+#define SUBSTEP_END                  \
+  CK(w, cudaGetLastError());         \
+  return (int32_t)fetch_status(w)
+
+int32_t xdem_modify_particle_position(xdem_world w) {
+  SUBSTEP_BEGIN;
+  launch_modify(w);
+  SUBSTEP_END;
+}
+
+int32_t xdem_apply_background_velocity(xdem_world w) {
+  SUBSTEP_BEGIN;
+  k_background_velocity<<<blocks_for(w->dw.n, kBlock), kBlock, 0, w->stream>>>(w->dw, 1);
+  SUBSTEP_END;
+}
+
+int32_t xdem_remove_background_velocity(xdem_world w) {
+  SUBSTEP_BEGIN;
+  k_background_velocity<<<blocks_for(w->dw.n, kBlock), kBlock, 0, w->stream>>>(w->dw, 0);
+  SUBSTEP_END;
+}
+
+int32_t xdem_find_possible_contacts(xdem_world w) {
+  SUBSTEP_BEGIN;
+  launch_find(w);
+  SUBSTEP_END;
+}
+
+int32_t xdem_update_contacts(xdem_world w) {
+  SUBSTEP_BEGIN;
+  CK(w, cudaMemsetAsync(w->dw.incnt, 0, sizeof(int32_t) * w->dw.n, w->stream));
+  launch_update(w, false, 1);
+  SUBSTEP_END;
+}
+
+int32_t xdem_collect_force_and_torque(xdem_world w) {
+  SUBSTEP_BEGIN;
+  launch_collect(w);
+  SUBSTEP_END;
+}
+
+int32_t xdem_take_time_integral(xdem_world w) {
+  SUBSTEP_BEGIN;
+  launch_integrate(w, false, 0);
+  SUBSTEP_END;
+}
+
+int32_t xdem_reset_velocity_of_rattlers(xdem_world w) {
+  SUBSTEP_BEGIN;
+  launch_rattlers(w, 1, 0.0);
+  SUBSTEP_END;
+}
+
+int32_t xdem_scale_velocity_of_rattlers(xdem_world w, double scale) {
+  SUBSTEP_BEGIN;
+  launch_rattlers(w, 0, scale);
+  SUBSTEP_END;
+}
+
+int32_t xdem_update_total_stress(xdem_world w, double stress[4]) {
+  SUBSTEP_BEGIN;
+  launch_stress(w);
+  CK(w, cudaGetLastError());
+  int32_t st = (int32_t)fetch_status(w);
+  if (stress) {
+    int32_t e = xdem_get_stress(w, stress);
+    if (e) return st | e;
+  }
+  return st;
+}
+
+int32_t xdem_update_boundary(xdem_world w, int32_t law, double p0, double p1) {
+  SUBSTEP_BEGIN;
+  if (law < 0 || law > 4) return XDEM_ERR_ARGUMENT;
+  k_end_of_step<<<1, 1, 0, w->stream>>>(w->dw, law, p0, p1, 0, 0, 0.0);
+  if (law != BOX_NONE)
+    k_scale_positions<<<blocks_for(w->dw.n, kBlock), kBlock, 0, w->stream>>>(w->dw);
+  SUBSTEP_END;
+}
+
+int32_t xdem_update_lees_edwards_boundary(xdem_world w) {
+  SUBSTEP_BEGIN;
+  k_end_of_step<<<1, 1, 0, w->stream>>>(w->dw, BOX_NONE, 0.0, 0.0, 1, 0, 0.0);
+  SUBSTEP_END;
+}
+
+int32_t xdem_scale_boundary_to_solid_fraction(xdem_world w, double phi) {
+  // scaleBoundarySizeToGivenSolidFraction (PeriodicBoundaryWorld.cpp:276-284)
+  SUBSTEP_BEGIN;
+  if (!(phi > 0.0)) return XDEM_ERR_ARGUMENT;
+  WorldScalars s;
+  CK(w, read_scalars(w, &s));
+  double cur = w->total_volume / (s.xlen * s.ylen);
+  double scale = std::sqrt(cur / phi);
+  s.scale_x = scale;
+  s.scale_y = scale;
+  s.xmin *= scale;
+  s.xmax *= scale;
+  s.ymin *= scale;
+  s.ymax *= scale;
+  s.xlen = s.xmax - s.xmin;
+  s.ylen = s.ymax - s.ymin;
+  CK(w, write_scalars(w, &s));
+  k_scale_positions<<<blocks_for(w->dw.n, kBlock), kBlock, 0, w->stream>>>(w->dw);
+  SUBSTEP_END;
+}
+
+// ---- whole steps -------------------------------------------------------------
+int32_t xdem_take_time_step(xdem_world w) {
+  SUBSTEP_BEGIN;
+  xdem_control ctl{};
+  ctl.sequence = XDEM_SEQ_TAKE_TIME_STEP;
+  enqueue_step(w, &ctl, 1);
+  SUBSTEP_END;
+}
+
+int32_t xdem_run(xdem_world w, int32_t nsteps, const xdem_control* ctl, int32_t* steps_done) {
+  SUBSTEP_BEGIN;
+  if (!ctl || nsteps < 0 || ctl->sequence < 0 || ctl->sequence > 1 || ctl->box_law < 0 ||
+      ctl->box_law > 4)
+    return XDEM_ERR_ARGUMENT;
+  if (steps_done) *steps_done = 0;
+  if (nsteps == 0) return XDEM_OK;
+  WorldScalars s;
+  CK(w, read_scalars(w, &s));
+  s.stop = 0;
+  s.steps_done = 0;
+  CK(w, write_scalars(w, &s));
+  const int start_par = w->par;
+  // every step but the last skips the recorded contact fields unless the run
+  // may stop early
+  const int rec_all = ctl->stop_on_pressure ? 1 : 0;
+  int body = nsteps - 1;
+  const int kGraphSteps = 2;
+  if (body >= 8) {
+    // capture two steps (one per slot-set parity) and replay the graph
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    CK(w, cudaStreamBeginCapture(w->stream, cudaStreamCaptureModeThreadLocal));
+    for (int k = 0; k < kGraphSteps; ++k) enqueue_step(w, ctl, rec_all);
+    cudaError_t e = cudaStreamEndCapture(w->stream, &graph);
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
+    if (e != cudaSuccess) {
+      if (graph) cudaGraphDestroy(graph);
+      return (int32_t)(cuda_check(w, e) | fetch_status(w));
+    }
+    w->par = start_par;  // capture toggled the parity kGraphSteps times
+    int reps = body / kGraphSteps;
+    for (int r = 0; r < reps && e == cudaSuccess; ++r) e = cudaGraphLaunch(exec, w->stream);
+    body -= reps * kGraphSteps;
+    cudaGraphExecDestroy(exec);
+    cudaGraphDestroy(graph);
+    CK(w, e);
+  }
+  for (int k = 0; k < body; ++k) enqueue_step(w, ctl, rec_all);
+  enqueue_step(w, ctl, 1);
+  CK(w, cudaGetLastError());
+  uint32_t st = fetch_status(w);
+  CK(w, read_scalars(w, &s));
+  if (steps_done) *steps_done = s.steps_done;
+  w->par = start_par ^ (s.steps_done & 1);
+  return (int32_t)st;
+}
+
+int32_t xdem_synchronize(xdem_world w) {
+  if (!w) return XDEM_ERR_ARGUMENT;
+  return (int32_t)fetch_status(w);
+}
+
+// ---- single-pair geometry ------------------------------------------------------
+int32_t xdem_pair_geometry(int32_t npairs, int32_t method, int32_t precision, const double* pi,
+                           const double* pj, const double* off, double* out) {
+  (void)precision;
+  if (npairs <= 0 || !pi || !pj || !off || !out) return XDEM_ERR_ARGUMENT;
+  double *dpi = nullptr, *dpj = nullptr, *doff = nullptr, *dout = nullptr;
+  uint32_t* dst = nullptr;
+  uint32_t st = 0;
+  cudaError_t e = cudaMalloc(&dpi, sizeof(double) * 9 * npairs);
+  if (e == cudaSuccess) e = cudaMalloc(&dpj, sizeof(double) * 9 * npairs);
+  if (e == cudaSuccess) e = cudaMalloc(&doff, sizeof(double) * 4 * npairs);
+  if (e == cudaSuccess) e = cudaMalloc(&dout, sizeof(double) * 17 * npairs);
+  if (e == cudaSuccess) e = cudaMalloc(&dst, sizeof(uint32_t));
+  if (e == cudaSuccess) e = cudaMemset(dst, 0, sizeof(uint32_t));
+  if (e == cudaSuccess) e = cudaMemcpy(dpi, pi, sizeof(double) * 9 * npairs, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(dpj, pj, sizeof(double) * 9 * npairs, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(doff, off, sizeof(double) * 4 * npairs, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    k_pair_geometry<<<blocks_for(npairs, 128), 128>>>(npairs, method, dpi, dpj, doff, dout, dst);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpy(out, dout, sizeof(double) * 17 * npairs, cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(&st, dst, sizeof(uint32_t), cudaMemcpyDeviceToHost);
+  cudaFree(dpi);
+  cudaFree(dpj);
+  cudaFree(doff);
+  cudaFree(dout);
+  cudaFree(dst);
+  if (e != cudaSuccess) st |= XDEM_ERR_CUDA;
+  return (int32_t)st;
+}
+
+}  // extern "C"

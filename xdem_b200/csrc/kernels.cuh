@@ -1,0 +1,855 @@
+// kernels.cuh — the per-timestep kernels (FP64 path).
+//
+// Step of a PeriodicBoundaryWorld (PeriodicBoundaryWorld.cpp:119-127):
+//   k_modify_position       wrap into the box                     (a2)
+//   k_bin / k_scan / k_scatter   counting sort of particles by cell (a3)
+//   k_update_contacts       3x3 cell scan, geometry, force, history (a5-a15)
+//   k_collect               deterministic per-particle sums         (a16)
+//   k_integrate             semi-implicit Euler (+ clumps, rattlers)(a17-a19)
+// plus k_stress_* (a21), k_box_law/k_scale_positions (a20) and
+// k_le_boundary (a22).
+#pragma once
+#include "geometry.cuh"
+#include "world.cuh"
+
+namespace xdem {
+
+enum : int { WORLD_PERIODIC = 0, WORLD_CONTROL = 1, WORLD_LE = 2 };
+enum : int { SKIP_TIME_INTEGRAL = 1, SKIP_CONTACT_DETECTION = 2, SKIP_MACRO_SUM = 4 };
+enum : int { CAND_REGULAR = 0, CAND_TOP = 1, CAND_BOTTOM = 2 };
+
+constexpr int kCandidateCap = 200;  // MAXIMUM_POSSIBLE_CONTACT_LIST_SIZE (BaseWorld.h:11)
+
+struct Grid {
+  int nx, ny, ncell;
+  double lx, ly;
+};
+
+// Grid of PeriodicBoundaryWorld::findPossibleContacts (PeriodicBoundaryWorld.cpp:17-22):
+// nx = floor(xlen / (2.01 r_max)); clamped to the allocated capacity, which
+// only makes cells larger and leaves the contact set unchanged.
+__device__ __forceinline__ Grid grid_of(const WorldScalars& ws, int nx_cap, int ny_cap) {
+  Grid g;
+  double xlen = ws.xmax - ws.xmin, ylen = ws.ymax - ws.ymin;
+  g.nx = (int)floor(xlen / ws.maxsize);
+  g.ny = (int)floor(ylen / ws.maxsize);
+  if (g.nx > nx_cap) g.nx = nx_cap;
+  if (g.ny > ny_cap) g.ny = ny_cap;
+  g.ncell = g.nx * g.ny;
+  g.lx = xlen / g.nx;
+  g.ly = ylen / g.ny;
+  return g;
+}
+
+// cell of a coordinate; the reference's floor() can reach numGrid at the upper
+// edge (an out-of-range bin there), clamped here
+__device__ __forceinline__ int cell_of(double v, double vmin, double len, int ng) {
+  int c = (int)floor((v - vmin) / len);
+  return c < 0 ? 0 : (c > ng - 1 ? ng - 1 : c);
+}
+
+__device__ __forceinline__ void raise(uint32_t* status, uint32_t bits) {
+  if (bits) atomicOr(status, bits);
+}
+
+// ---------------------------------------------------------------------------
+// a2: modifyParticlePosition (PeriodicBoundaryWorld.cpp:129-142,
+//     LeesEdwardsBoundaryWorld.cpp:304-333), optionally preceded by the
+//     pending affine scale of a box law (scaleAllParticlePosition,
+//     BaseWorld.cpp:119-124).
+// ---------------------------------------------------------------------------
+__global__ void k_modify_position(DevWorld w) {
+  const WorldScalars& ws = *w.ws;
+  if (ws.stop) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= w.n) return;
+  double2 p = w.pos[i];
+  if (w.kind == WORLD_LE) {
+    if (p.y < ws.ymin) {
+      p.y += ws.ylen;
+      p.x += ws.shift;
+    } else if (p.y > ws.ymax) {
+      p.y += -ws.ylen;
+      p.x += -ws.shift;
+    }
+    if (p.x < ws.xmin) p.x += ws.xlen;
+    else if (p.x > ws.xmax) p.x += -ws.xlen;
+  } else {
+    if (p.x < ws.xmin) p.x += ws.xlen;
+    else if (p.x > ws.xmax) p.x += -ws.xlen;
+    if (p.y < ws.ymin) p.y += ws.ylen;
+    else if (p.y > ws.ymax) p.y += -ws.ylen;
+  }
+  w.pos[i] = p;
+}
+
+// scaleAllParticlePosition(scale_x, scale_y) (BaseWorld.cpp:119-124); after a
+// run's stop the scales are 1 and the pass leaves positions unchanged
+__global__ void k_scale_positions(DevWorld w) {
+  const WorldScalars& ws = *w.ws;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= w.n) return;
+  double2 p = w.pos[i];
+  p.x *= ws.scale_x;
+  p.y *= ws.scale_y;
+  w.pos[i] = p;
+}
+
+// a6: LeesEdwardsBoundaryWorld::apply/removeBackgroudVelocity (:508-530)
+__global__ void k_background_velocity(DevWorld w, int apply) {
+  const WorldScalars& ws = *w.ws;
+  if (ws.stop) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= w.n) return;
+  double2 v = w.vel[i];
+  double y = w.pos[i].y;
+  if (apply) v.x = v.x + ws.shift_rate * y;
+  else v.x = v.x - ws.shift_rate * y;
+  w.vel[i] = v;
+}
+
+// ---------------------------------------------------------------------------
+// a3/a4: cell binning.  Counting sort: per-cell counts by atomics, an
+// exclusive scan, and a scatter.  Ghost rows after the regular cells hold the
+// Lees-Edwards images: row ncell+[0,nx) takes bottom-row particles shifted by
+// +shift (boxLE_top, LeesEdwardsBoundaryWorld.cpp:75-81), row
+// ncell+nx+[0,nx) top-row particles shifted by -shift (boxLE_bottom, :82-88).
+// The order inside a cell is not fixed; nothing downstream depends on it.
+// ---------------------------------------------------------------------------
+__global__ void k_bin(DevWorld w) {
+  const WorldScalars& ws = *w.ws;
+  if (ws.stop) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  Grid G = grid_of(ws, w.nx_cap, w.ny_cap);
+  if (i == 0 && (G.nx < 3 || G.ny < 3)) raise(w.status, ST_GRID);
+  if (i >= w.n) return;
+  w.incnt[i] = 0;  // incoming-contact counters of this step's update
+  if (G.nx < 3 || G.ny < 3) return;
+  double2 p = w.pos[i];
+  int ix = cell_of(p.x, ws.xmin, G.lx, G.nx);
+  int iy = cell_of(p.y, ws.ymin, G.ly, G.ny);
+  int c = iy * G.nx + ix;
+  w.pcell[i] = c;
+  w.prank[i] = atomicAdd(&w.cell_count[c], 1);
+  int gc = -1;
+  if (w.kind == WORLD_LE) {
+    if (iy == 0) {
+      double t = p.x + ws.shift;
+      if (t < ws.xmin) t += ws.xlen;
+      else if (t > ws.xmax) t -= ws.xlen;
+      gc = G.ncell + cell_of(t, ws.xmin, G.lx, G.nx);
+    } else if (iy == G.ny - 1) {
+      double t = p.x - ws.shift;
+      if (t < ws.xmin) t += ws.xlen;
+      else if (t > ws.xmax) t -= ws.xlen;
+      gc = G.ncell + G.nx + cell_of(t, ws.xmin, G.lx, G.nx);
+    }
+  }
+  w.gcell[i] = gc;
+  if (gc >= 0) w.grank[i] = atomicAdd(&w.cell_count[gc], 1);
+}
+
+// exclusive scan of cell_count[0 .. ncell + 2nx) into cell_start (one block)
+__global__ void k_scan(DevWorld w) {
+  const WorldScalars& ws = *w.ws;
+  if (ws.stop) return;
+  Grid G = grid_of(ws, w.nx_cap, w.ny_cap);
+  int total = G.ncell + 2 * G.nx;
+  __shared__ int32_t sh[1024];
+  int t = threadIdx.x;
+  int per = (total + blockDim.x - 1) / blockDim.x;
+  int beg = t * per, end = min(beg + per, total);
+  int32_t local = 0;
+  for (int k = beg; k < end; ++k) local += w.cell_count[k];
+  sh[t] = local;
+  __syncthreads();
+  for (int off = 1; off < (int)blockDim.x; off <<= 1) {
+    int32_t v = (t >= off) ? sh[t - off] : 0;
+    __syncthreads();
+    sh[t] += v;
+    __syncthreads();
+  }
+  int32_t run = sh[t] - local;
+  for (int k = beg; k < end; ++k) {
+    w.cell_start[k] = run;
+    run += w.cell_count[k];
+  }
+  if (t == blockDim.x - 1) w.cell_start[total] = sh[t];
+}
+
+// also clears cell_count (already consumed by k_scan) for the next binning
+__global__ void k_scatter(DevWorld w) {
+  const WorldScalars& ws = *w.ws;
+  if (ws.stop) return;
+  Grid G = grid_of(ws, w.nx_cap, w.ny_cap);
+  int total = G.ncell + 2 * G.nx;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < total; c += gridDim.x * blockDim.x)
+    w.cell_count[c] = 0;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= w.n) return;
+  if (G.nx < 3 || G.ny < 3) return;
+  w.cell_mem[w.cell_start[w.pcell[i]] + w.prank[i]] = i;
+  int gc = w.gcell[i];
+  if (gc >= 0) w.cell_mem[w.cell_start[gc] + w.grank[i]] = i;
+}
+
+// ---------------------------------------------------------------------------
+// a5-a15: updateContacts.  One thread per owner particle i scans the 3x3
+// neighbourhood (PeriodicBoundaryWorld.cpp:47-84, LeesEdwardsBoundaryWorld.cpp:
+// 128-204), evaluates every candidate j > i at its image offset
+// (PeriodicBoundaryWorld.cpp:97-101, LeesEdwardsBoundaryWorld.cpp:233-279),
+// and writes the contacts into its slots of the new slot set:
+//   - new contact: initial shear overlap and damping constant (BaseParticle.cpp:38-65)
+//   - old contact: shear overlap rotated with the normal (BaseParticle.cpp:67-82)
+//   - candidate not in contact: dropped (BaseParticle.cpp:95)
+//   - history of a pair that is no longer a candidate: carried over unchanged,
+//     as the reference's map entry is.
+// FOLD_BG adds the Lees-Edwards background velocity on the fly, bit for bit the
+// value applyBackgroudVelocity would have stored.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double damping_constant(const DevWorld& w, double factor, int i, int j) {
+  // calculateDampingConstact (ContactModel_LinearDissipativeFrictional.cpp:73-82)
+  // selected by SKIP_TIME_INTEGRAL (BaseParticle.cpp:53-64)
+  int si = w.setting[i] & SKIP_TIME_INTEGRAL, sj = w.setting[j] & SKIP_TIME_INTEGRAL;
+  double mi = w.mass[i], mj = w.mass[j];
+  if (!si && sj) return sqrt(mi) * factor;
+  if (si && !sj) return sqrt(mj) * factor;
+  return sqrt((mi * mj) / (mi + mj)) * factor;
+}
+
+template <bool FOLD_BG>
+__device__ __forceinline__ PState load_state(const DevWorld& w, const WorldScalars& ws, int i) {
+  PState p;
+  p.shape = w.shape[i];
+  p.r = w.rad[i];
+  p.asp = w.asp[i];
+  double2 q = w.pos[i];
+  double2 v = w.vel[i];
+  p.x = q.x;
+  p.y = q.y;
+  p.vx = FOLD_BG ? v.x + ws.shift_rate * q.y : v.x;
+  p.vy = v.y;
+  p.rot = w.rot[i];
+  p.w = w.w[i];
+  return p;
+}
+
+template <bool FOLD_BG>
+__global__ void __launch_bounds__(128) k_update_contacts(DevWorld w, int par, int record) {
+  const WorldScalars& ws = *w.ws;
+  if (ws.stop) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= w.n) return;
+  const int n = w.n, K = w.K;
+  const Slots& old = w.slots[par];
+  const Slots& cur = w.slots[par ^ 1];
+  uint32_t st = 0;
+  Grid G = grid_of(ws, w.nx_cap, w.ny_cap);
+  bool grid_ok = (G.nx >= 3 && G.ny >= 3);
+
+  // previous history of i
+  int nold = old.count[i];
+  if (nold > K) nold = K;
+  int opart[kMaxSlots];
+  for (int o = 0; o < nold; ++o) opart[o] = old.partner[(size_t)o * n + i];
+  uint32_t seen = 0;
+  int k = 0;
+
+  const double dt = ws.dt, kn = ws.kn, kt = ws.kt, mu = ws.mu, factor = ws.factor;
+  if (grid_ok && !(w.setting[i] & SKIP_CONTACT_DETECTION)) {
+    PState a = load_state<FOLD_BG>(w, ws, i);
+    double2 csa = make_double2(0.0, 0.0);
+    if (a.shape == SHAPE_ELLIPSE) csa = make_double2(cos(a.rot), sin(a.rot));
+    int up_i = w.up[i];
+    double orad_i = w.orad[i];
+    int ix = cell_of(a.x, ws.xmin, G.lx, G.nx);
+    int iy = cell_of(a.y, ws.ymin, G.ly, G.ny);
+    int ncand[3] = {0, 0, 0};
+    for (int dx = -1; dx <= 1; ++dx) {
+      int jx = ix + dx;
+      if (jx == -1) jx = G.nx - 1;
+      else if (jx == G.nx) jx = 0;
+      for (int dy = -1; dy <= 1; ++dy) {
+        int jy = iy + dy;
+        int c, kind = CAND_REGULAR;
+        if (w.kind == WORLD_LE && (jy == -1 || jy == G.ny)) {
+          if (jy == -1) {
+            c = G.ncell + G.nx + jx;
+            kind = CAND_BOTTOM;
+          } else {
+            c = G.ncell + jx;
+            kind = CAND_TOP;
+          }
+        } else {
+          if (jy == -1) jy = G.ny - 1;
+          else if (jy == G.ny) jy = 0;
+          c = jy * G.nx + jx;
+        }
+        int q0 = w.cell_start[c], q1 = w.cell_start[c + 1];
+        for (int q = q0; q < q1; ++q) {
+          int j = w.cell_mem[q];
+          if (j <= i) continue;
+          if (w.setting[j] & SKIP_CONTACT_DETECTION) continue;
+          if (w.up[j] == up_i) continue;
+          if (ncand[kind] + 1 >= kCandidateCap) {
+            st |= ST_CAPACITY;
+            continue;
+          }
+          ncand[kind]++;
+          // offset of the image of j
+          double2 pj = w.pos[j];
+          vec2<double> off, ovel = V(0.0, 0.0);
+          if (kind == CAND_REGULAR) {
+            double ox = 0.0, oy = 0.0;
+            if (pj.x - a.x > ws.xlen / 2.0) ox = -ws.xlen;
+            else if (pj.x - a.x < -ws.xlen / 2.0) ox = ws.xlen;
+            if (pj.y - a.y > ws.ylen / 2.0) oy = -ws.ylen;
+            else if (pj.y - a.y < -ws.ylen / 2.0) oy = ws.ylen;
+            off = V(ox, oy);
+          } else {
+            off = (kind == CAND_TOP) ? V(ws.shift, ws.ylen) : V(-ws.shift, -ws.ylen);
+            double t = off.x + pj.x;
+            if (t < ws.xmin) {
+              off.x += ws.xlen;
+              t += ws.xlen;
+            } else if (t > ws.xmax) {
+              off.x += -ws.xlen;
+              t -= ws.xlen;
+            }
+            if (t - a.x > ws.xlen / 2.0) off.x += -ws.xlen;
+            else if (t - a.x < -ws.xlen / 2.0) off.x += ws.xlen;
+            ovel = V((kind == CAND_TOP) ? ws.shift_vel : -ws.shift_vel, 0.0);
+          }
+          // history slot of (i, j), if any
+          int o = -1;
+          for (int z = 0; z < nold; ++z)
+            if (opart[z] == j) {
+              o = z;
+              break;
+            }
+          if (o >= 0) seen |= 1u << o;
+          PState b = load_state<FOLD_BG>(w, ws, j);
+          double2 csb = make_double2(0.0, 0.0);
+          if (b.shape == SHAPE_ELLIPSE && a.shape == SHAPE_ELLIPSE)
+            csb = make_double2(cos(b.rot), sin(b.rot));
+          Geom g;
+          if (!contact_geometry(w.method, a, b, orad_i, w.orad[j], off, ovel, csa, csb, g, st))
+            continue;
+          if (k >= K) {
+            st |= ST_CAPACITY;
+            continue;
+          }
+          // BaseParticle::calculateContactForceAndTorque (BaseParticle.cpp:27-98)
+          vec2<double> sh, nn = g.n;
+          double damp;
+          if (o < 0) {
+            double rvn = dot(g.rv, g.n);
+            if (!is_normal(rvn)) sh = g.srv * dt;
+            else sh = g.srv * std_min(dt, g.overlap / rvn);
+            damp = damping_constant(w, factor, i, j);
+          } else {
+            size_t oi = (size_t)o * n + i;
+            double2 on = old.n[oi], os = old.s[oi];
+            damp = old.damp[oi];
+            vec2<double> no = V(on.x, on.y);
+            double dd = dot(no, nn);
+            double de = cross(no, nn);
+            double angle = atan2(de, dd);
+            double ca = cos(angle), sa = sin(angle);
+            mat2<double> R = M(ca, -sa, sa, ca);
+            sh = R * V(os.x, os.y);
+            sh = sh + g.srv * dt;
+          }
+          vec2<double> br = V(a.x, a.y) - (V(pj.x, pj.y) + off);
+          // ContactModel_LinearDissipativeFrictioanl (…Frictional.cpp:3-46)
+          vec2<double> fn = ((-nn) * kn) * g.overlap + (-g.nrv) * damp;
+          double maxFs = len(fn) * mu;
+          vec2<double> el = (-sh) * kt;
+          vec2<double> di = (-g.srv) * damp;
+          vec2<double> fs = el + di;
+          if (len(fs) > maxFs) {
+            fs = unit(fs) * maxFs;
+            if (len(el) > maxFs) sh = (-fs) / kt;
+            else sh = (-el) / kt;
+          }
+          // ContactInformation::calculateTotalForceAndTorque (ContactInformation.h:62-68)
+          vec2<double> F = fn + fs;
+          double t1 = cross(g.bv1, F);
+          double t2 = cross(g.bv2, -F);
+          size_t ci = (size_t)k * n + i;
+          cur.partner[ci] = j;
+          cur.n[ci] = make_double2(nn.x, nn.y);
+          cur.s[ci] = make_double2(sh.x, sh.y);
+          cur.damp[ci] = damp;
+          cur.f[ci] = make_double2(F.x, F.y);
+          cur.t1[ci] = t1;
+          cur.t2[ci] = t2;
+          cur.b[ci] = make_double2(br.x, br.y);
+          if (record) {
+            cur.cp[ci] = make_double2(g.cp.x, g.cp.y);
+            cur.bv1[ci] = make_double2(g.bv1.x, g.bv1.y);
+            cur.bv2[ci] = make_double2(g.bv2.x, g.bv2.y);
+            cur.fn[ci] = make_double2(fn.x, fn.y);
+            cur.ft[ci] = make_double2(fs.x, fs.y);
+          }
+          ++k;
+        }
+      }
+    }
+  }
+  // history of pairs that were not candidates survives unchanged
+  for (int o = 0; o < nold; ++o) {
+    if (seen & (1u << o)) continue;
+    if (k >= K) {
+      st |= ST_CAPACITY;
+      break;
+    }
+    size_t oi = (size_t)o * n + i, ci = (size_t)k * n + i;
+    cur.partner[ci] = opart[o];
+    cur.n[ci] = old.n[oi];
+    cur.s[ci] = old.s[oi];
+    cur.damp[ci] = old.damp[oi];
+    cur.f[ci] = old.f[oi];
+    cur.t1[ci] = old.t1[oi];
+    cur.t2[ci] = old.t2[oi];
+    cur.b[ci] = old.b[oi];
+    cur.cp[ci] = old.cp[oi];
+    cur.bv1[ci] = old.bv1[oi];
+    cur.bv2[ci] = old.bv2[oi];
+    cur.fn[ci] = old.fn[oi];
+    cur.ft[ci] = old.ft[oi];
+    ++k;
+  }
+  cur.count[i] = k;
+  // register each contact with its partner for the partner's force sum
+  for (int s = 0; s < k; ++s) {
+    int j = cur.partner[(size_t)s * n + i];
+    int pos = atomicAdd(&w.incnt[j], 1);
+    if (pos < K) w.inref[(size_t)pos * n + j] = (uint32_t)i * (uint32_t)K + (uint32_t)s;
+    else st |= ST_CAPACITY;
+  }
+  raise(w.status, st);
+}
+
+// small insertion sort of (key, value) pairs held in local arrays
+__device__ __forceinline__ void isort(uint32_t* key, int m) {
+  for (int a = 1; a < m; ++a) {
+    uint32_t x = key[a];
+    int b = a - 1;
+    while (b >= 0 && key[b] > x) {
+      key[b + 1] = key[b];
+      --b;
+    }
+    key[b + 1] = x;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// a16: collectForceAndTorque (BaseWorld.cpp:17-57).  Each particle sums, in a
+// fixed order, the contacts owned by lower ids (ascending owner; -F and
+// torqueOnP2) and then its own contacts (ascending partner; F and
+// torqueOnP1), starting from zero as the reference's per-thread arrays do.
+// Particles with no contact are rattlers (BaseWorld.cpp:25,44-45).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_collect(DevWorld w, int par) {
+  const WorldScalars& ws = *w.ws;
+  if (ws.stop) return;
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= w.n) return;
+  const int n = w.n, K = w.K;
+  const Slots& cur = w.slots[par];
+  int nown = min(cur.count[p], K);
+  int ninc = min(w.incnt[p], K);
+  uint32_t key[kMaxSlots];
+  double fx = 0.0, fy = 0.0, t = 0.0;
+  for (int a = 0; a < ninc; ++a) key[a] = w.inref[(size_t)a * n + p];
+  isort(key, ninc);
+  for (int a = 0; a < ninc; ++a) {
+    uint32_t owner = key[a] / K, slot = key[a] % K;
+    size_t ci = (size_t)slot * n + owner;
+    double2 F = cur.f[ci];
+    fx += -F.x;
+    fy += -F.y;
+    t += cur.t2[ci];
+  }
+  for (int a = 0; a < nown; ++a) key[a] = ((uint32_t)cur.partner[(size_t)a * n + p] << 5) | a;
+  isort(key, nown);
+  for (int a = 0; a < nown; ++a) {
+    size_t ci = (size_t)(key[a] & 31u) * n + p;
+    double2 F = cur.f[ci];
+    fx += F.x;
+    fy += F.y;
+    t += cur.t1[ci];
+  }
+  w.force[p] = make_double2(fx, fy);
+  w.torque[p] = t;
+  w.ncp[p] = nown + ninc;
+  w.rattler[p] = (nown + ninc) == 0 ? 1 : 0;
+}
+
+// GluedParticle::isRattlerParticle (GluedParticle.cpp:141-147)
+__device__ __forceinline__ bool is_rattler(const DevWorld& w, int i) {
+  if (w.shape[i] == SHAPE_CLUMP) {
+    int ns = w.num_sub[i];
+    for (int k = 1; k <= ns; ++k)
+      if (!w.rattler[i + k]) return false;
+    return true;
+  }
+  return w.rattler[i] != 0;
+}
+
+// ---------------------------------------------------------------------------
+// a17/a18/a19: takeTimeIntegral (BaseWorld.cpp:59-77; BaseParticle.cpp:107-118;
+// GluedParticle.cpp:91-125), then optionally resetVelocityOfRattlers
+// (BaseWorld.cpp:79-92).  FOLD_BG first removes the Lees-Edwards background
+// velocity exactly as removeBackgroudVelocity would after applyBackgroudVelocity.
+// ---------------------------------------------------------------------------
+template <bool FOLD_BG>
+__global__ void k_integrate(DevWorld w, int reset_rattlers) {
+  const WorldScalars& ws = *w.ws;
+  if (ws.stop) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= w.n) return;
+  const double dt = ws.dt, g = ws.g;
+  int set = w.setting[i];
+  double2 v = w.vel[i];
+  if (FOLD_BG) {
+    double y = w.pos[i].y;
+    v.x = (v.x + ws.shift_rate * y) - ws.shift_rate * y;
+  }
+  if (set & SKIP_TIME_INTEGRAL) {
+    // a sub-particle's velocity is rewritten by its clump below
+    if (FOLD_BG && w.up[i] == i) w.vel[i] = v;
+    if (reset_rattlers && !(set & SKIP_MACRO_SUM) && w.up[i] == i && is_rattler(w, i)) {
+      w.vel[i] = make_double2(0.0, 0.0);
+      w.w[i] = 0.0;
+    }
+    return;
+  }
+  double2 p = w.pos[i];
+  double om = w.w[i];
+  if (w.shape[i] == SHAPE_CLUMP) {
+    vec2<double> F = V(0.0, 0.0);
+    double T = 0.0;
+    int ns = w.num_sub[i];
+    for (int k = 1; k <= ns; ++k) {
+      double2 fk = w.force[i + k];
+      double2 bk = w.branch[i + k];
+      F = F + V(fk.x, fk.y);
+      T += w.torque[i + k];
+      T += cross(V(bk.x, bk.y), V(fk.x, fk.y));
+    }
+    vec2<double> vv = (V(v.x, v.y) * (1.0 - g * dt) + (F * w.im[i]) * dt) / (1.0 + g * dt);
+    p.x += vv.x * dt;
+    p.y += vv.y * dt;
+    om = (om * (1.0 - g * dt) + T * w.iI[i] * dt) / (1.0 + g * dt);
+    double rot = w.rot[i] + om * dt;
+    double angle = om * dt;
+    double ca = cos(angle), sa = sin(angle);
+    mat2<double> R = M(ca, -sa, sa, ca);
+    for (int k = 1; k <= ns; ++k) {
+      double2 bk = w.branch[i + k];
+      vec2<double> b = R * V(bk.x, bk.y);
+      w.branch[i + k] = make_double2(b.x, b.y);
+      vec2<double> sv = vv + crossw(b, om);
+      w.vel[i + k] = make_double2(sv.x, sv.y);
+      w.pos[i + k] = make_double2(p.x + b.x, p.y + b.y);
+      w.w[i + k] = om;
+      w.rot[i + k] += angle;
+    }
+    w.pos[i] = p;
+    w.rot[i] = rot;
+    if (reset_rattlers && !(set & SKIP_MACRO_SUM) && is_rattler(w, i)) {
+      w.vel[i] = make_double2(0.0, 0.0);
+      w.w[i] = 0.0;
+    } else {
+      w.vel[i] = make_double2(vv.x, vv.y);
+      w.w[i] = om;
+    }
+    return;
+  }
+  double2 F = w.force[i];
+  double im = w.im[i];
+  vec2<double> vv = (V(v.x, v.y) * (1.0 - g * dt) + (V(F.x, F.y) * im) * dt) / (1.0 + g * dt);
+  p.x += vv.x * dt;
+  p.y += vv.y * dt;
+  om = (om * (1.0 - g * dt) + w.torque[i] * w.iI[i] * dt) / (1.0 + g * dt);
+  w.pos[i] = p;
+  w.rot[i] = w.rot[i] + om * dt;
+  if (reset_rattlers && !(set & SKIP_MACRO_SUM) && w.rattler[i]) {
+    w.vel[i] = make_double2(0.0, 0.0);
+    w.w[i] = 0.0;
+  } else {
+    w.vel[i] = make_double2(vv.x, vv.y);
+    w.w[i] = om;
+  }
+}
+
+// BaseWorld::resetVelocityOfRattlers / scaleVelocityOfRattlers (BaseWorld.cpp:79-106)
+__global__ void k_rattlers(DevWorld w, int reset, double scale) {
+  const WorldScalars& ws = *w.ws;
+  if (ws.stop) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= w.n) return;
+  if (w.setting[i] & SKIP_MACRO_SUM) return;
+  if (!is_rattler(w, i)) return;
+  if (reset) {
+    w.vel[i] = make_double2(0.0, 0.0);
+    w.w[i] = 0.0;
+  } else {
+    double2 v = w.vel[i];
+    w.vel[i] = make_double2(v.x * scale, v.y * scale);
+    w.w[i] = w.w[i] * scale;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// a21: updateTotalStress (BaseWorld.cpp:158-176) with getStressFromContactList
+// of BaseParticle (BaseParticle.cpp:143-151) and GluedParticle
+// (GluedParticle.cpp:127-139).  Per-particle sums in ascending partner order,
+// then a fixed tree over particles: deterministic run to run.
+// ---------------------------------------------------------------------------
+constexpr int kReduceBlock = 256;
+
+__device__ __forceinline__ void own_stress(const DevWorld& w, const Slots& cur, int p,
+                                           bool sub, double2 bvo, mat2<double>& s) {
+  const int n = w.n, K = w.K;
+  int m = min(cur.count[p], K);
+  uint32_t key[kMaxSlots];
+  for (int a = 0; a < m; ++a) key[a] = ((uint32_t)cur.partner[(size_t)a * n + p] << 5) | a;
+  isort(key, m);
+  for (int a = 0; a < m; ++a) {
+    size_t ci = (size_t)(key[a] & 31u) * n + p;
+    double2 F = cur.f[ci], b = cur.b[ci];
+    vec2<double> bb = V(b.x, b.y);
+    if (sub) bb = bb + V(bvo.x, bvo.y);
+    s = s + dyad(V(F.x, F.y), bb);
+  }
+}
+
+__global__ void __launch_bounds__(kReduceBlock) k_stress_partial(DevWorld w, int par) {
+  const WorldScalars& ws = *w.ws;
+  if (ws.stop) return;
+  __shared__ double sh[4][kReduceBlock];
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  mat2<double> s = M(0.0, 0.0, 0.0, 0.0);
+  if (p < w.n && !(w.setting[p] & SKIP_MACRO_SUM)) {
+    const Slots& cur = w.slots[par];
+    if (w.shape[p] == SHAPE_CLUMP) {
+      // one running sum over all sub-particles (GluedParticle.cpp:128-137)
+      for (int k = 1; k <= w.num_sub[p]; ++k) own_stress(w, cur, p + k, true, w.branch[p + k], s);
+    } else {
+      own_stress(w, cur, p, false, make_double2(0.0, 0.0), s);
+    }
+  }
+  int t = threadIdx.x;
+  sh[0][t] = s.xx;
+  sh[1][t] = s.xy;
+  sh[2][t] = s.yx;
+  sh[3][t] = s.yy;
+  __syncthreads();
+  for (int off = kReduceBlock / 2; off > 0; off >>= 1) {
+    if (t < off)
+      for (int c = 0; c < 4; ++c) sh[c][t] += sh[c][t + off];
+    __syncthreads();
+  }
+  if (t == 0)
+    for (int c = 0; c < 4; ++c) w.partials[(size_t)c * gridDim.x + blockIdx.x] = sh[c][0];
+}
+
+// sums nblocks partials in a fixed tree; divides by the box area
+__global__ void k_stress_final(DevWorld w, int nblocks) {
+  WorldScalars& ws = *w.ws;
+  if (ws.stop) return;
+  __shared__ double sh[4][1024];
+  int t = threadIdx.x;
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int b = t; b < nblocks; b += blockDim.x)
+    for (int c = 0; c < 4; ++c) acc[c] += w.partials[(size_t)c * nblocks + b];
+  for (int c = 0; c < 4; ++c) sh[c][t] = acc[c];
+  __syncthreads();
+  for (int off = blockDim.x / 2; off > 0; off >>= 1) {
+    if (t < off)
+      for (int c = 0; c < 4; ++c) sh[c][t] += sh[c][t + off];
+    __syncthreads();
+  }
+  if (t == 0) {
+    double area = ws.xlen * ws.ylen;
+    for (int c = 0; c < 4; ++c) ws.stress[c] = sh[c][0] / area;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// a20: PeriodicControlWorld box laws (PeriodicControlWorld.cpp:124-237).  One
+// thread updates the box and leaves the affine scale for k_scale_positions.
+// Also counts the step and evaluates a run's stop condition.
+// ---------------------------------------------------------------------------
+enum : int { BOX_NONE = 0, BOX_STRAIN = 1, BOX_STRESS_XY = 2, BOX_STRESS_UNIFORM = 3,
+             BOX_STRESS_UNIFORM_LIMIT = 4 };
+
+__device__ __forceinline__ void box_law(WorldScalars& ws, int law, double p0, double p1) {
+  const double dt = ws.dt;
+  const double kMaxScaleRate = 100000000.0;
+  ws.scale_x = 1.0;
+  ws.scale_y = 1.0;
+  if (law == BOX_STRAIN) {
+    double sx = 1.0 + p0 * ws.xlen * dt;
+    double sy = 1.0 + p1 * ws.ylen * dt;
+    ws.xmin *= sx;
+    ws.xmax *= sx;
+    ws.ymin *= sy;
+    ws.ymax *= sy;
+    ws.xlen = ws.xmax - ws.xmin;
+    ws.ylen = ws.ymax - ws.ymin;
+    ws.scale_x = sx;
+    ws.scale_y = sy;
+  } else if (law == BOX_STRESS_UNIFORM) {
+    double hydro = (ws.stress[0] + ws.stress[3]) / 2.0;
+    double dv = (p0 - hydro) * ws.xlen * dt;
+    ws.velX += dv;
+    ws.velY = ws.velX;
+    double scale = (ws.xmin + dv * dt) / ws.xmin;
+    ws.xmin += dv * dt;
+    ws.xmax = -ws.xmin;
+    ws.xlen = ws.xmax - ws.xmin;
+    ws.ymin += dv * dt;
+    ws.ymax = -ws.ymin;
+    ws.ylen = ws.ymax - ws.ymin;
+    ws.scale_x = scale;
+    ws.scale_y = scale;
+  } else if (law == BOX_STRESS_XY) {
+    // stressControlX then stressControlY; the two scales compose into one
+    // pass because each multiplies a different coordinate
+    double pre = ws.xmin;
+    double sxx = ws.stress[0];
+    if (fabs(sxx) < p0) ws.velX *= (1.0 - dt * 1.0);
+    double dv = (p0 - sxx) * ws.xlen / ws.vmass * dt;
+    ws.velX = dv;
+    if (fabs(ws.velX) / ws.xlen > kMaxScaleRate * dt) ws.velX = kMaxScaleRate * dt * ws.xlen;
+    ws.xmin += ws.velX * dt;
+    ws.xmax = -ws.xmin;
+    ws.xlen = ws.xmax - ws.xmin;
+    ws.scale_x = ws.xmin / pre;
+    pre = ws.ymin;
+    double syy = ws.stress[3];
+    if (fabs(syy) < p0) ws.velY *= (1.0 - dt * 1.0);
+    dv = (p0 - syy) * ws.ylen / ws.vmass * dt;
+    ws.velY = dv;
+    if (fabs(ws.velY) / ws.ylen > kMaxScaleRate * dt) ws.velY = kMaxScaleRate * dt * ws.ylen;
+    ws.ymin += ws.velY * dt;
+    ws.ymax = -ws.ymin;
+    ws.ylen = ws.ymax - ws.ymin;
+    ws.scale_y = ws.ymin / pre;
+  } else if (law == BOX_STRESS_UNIFORM_LIMIT) {
+    double prex = ws.xmin;
+    double hydro = (ws.stress[0] + ws.stress[3]) / 2.0;
+    double dv = (p0 - hydro) * ws.xlen * dt;
+    ws.velX += dv;
+    if ((fabs(ws.velX) / (ws.xlen / 2.0)) > ws.max_strain_rate)
+      ws.velX = fabs(ws.velX) / ws.velX * (ws.xlen / 2.0) * ws.max_strain_rate;
+    ws.velY = ws.velX;
+    ws.xmin += ws.velX * dt;
+    ws.xmax = -ws.xmin;
+    ws.xlen = ws.xmax - ws.xmin;
+    ws.ymin += ws.velY * dt;
+    ws.ymax = -ws.ymin;
+    ws.ylen = ws.ymax - ws.ymin;
+    double scale = ws.xmin / prex;
+    ws.scale_x = scale;
+    ws.scale_y = scale;
+  }
+}
+
+// end-of-step scalar work: box law, Lees-Edwards update
+// (LeesEdwardsBoundaryWorld.cpp:285-296), step count and stop test
+__global__ void k_end_of_step(DevWorld w, int law, double p0, double p1, int le_update,
+                              int stop_on_pressure, double stop_pressure) {
+  WorldScalars& ws = *w.ws;
+  if (ws.stop) {
+    ws.scale_x = 1.0;
+    ws.scale_y = 1.0;
+    return;
+  }
+  if (law != BOX_NONE) box_law(ws, law, p0, p1);
+  if (le_update) {
+    ws.shift_vel = ws.shift_rate * ws.ylen;
+    ws.strain += ws.shift_rate * ws.dt;
+    ws.shift += ws.shift_vel * ws.dt;
+    if (ws.shift > ws.xmax) ws.shift -= ws.xlen;
+    else if (ws.shift < ws.xmin) ws.shift += ws.xlen;
+  }
+  ws.steps_done += 1;
+  if (stop_on_pressure && (ws.stress[0] + ws.stress[3]) / 2.0 >= stop_pressure) ws.stop = 1;
+}
+
+// kinetic energy (BaseWorld.cpp:302-310), fixed-tree sum
+__global__ void __launch_bounds__(kReduceBlock) k_ke_partial(DevWorld w) {
+  __shared__ double sh[kReduceBlock];
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  double e = 0.0;
+  if (p < w.n) {
+    double2 v = w.vel[p];
+    double om = w.w[p];
+    e = 0.5 * (w.mass[p] * (v.x * v.x + v.y * v.y) + w.I[p] * om * om);
+  }
+  int t = threadIdx.x;
+  sh[t] = e;
+  __syncthreads();
+  for (int off = kReduceBlock / 2; off > 0; off >>= 1) {
+    if (t < off) sh[t] += sh[t + off];
+    __syncthreads();
+  }
+  if (t == 0) w.partials[blockIdx.x] = sh[0];
+}
+
+__global__ void k_ke_final(DevWorld w, int nblocks) {
+  __shared__ double sh[1024];
+  int t = threadIdx.x;
+  double acc = 0.0;
+  for (int b = t; b < nblocks; b += blockDim.x) acc += w.partials[b];
+  sh[t] = acc;
+  __syncthreads();
+  for (int off = blockDim.x / 2; off > 0; off >>= 1) {
+    if (t < off) sh[t] += sh[t + off];
+    __syncthreads();
+  }
+  if (t == 0) w.ws->ke = sh[0];
+}
+
+// single-pair geometry for known-answer tests (xdem_pair_geometry)
+__global__ void k_pair_geometry(int npairs, int method, const double* pi, const double* pj,
+                                const double* off, double* out, uint32_t* status) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= npairs) return;
+  const double* a = pi + 9 * k;
+  const double* b = pj + 9 * k;
+  PState A{(int)a[0], a[1], a[2], a[3], a[4], a[5], a[6], a[7], a[8]};
+  PState B{(int)b[0], b[1], b[2], b[3], b[4], b[5], b[6], b[7], b[8]};
+  double2 csa = make_double2(cos(A.rot), sin(A.rot));
+  double2 csb = make_double2(cos(B.rot), sin(B.rot));
+  Geom g;
+  uint32_t st = 0;
+  bool c = contact_geometry(method, A, B, a[1], b[1], V(off[4 * k], off[4 * k + 1]),
+                            V(off[4 * k + 2], off[4 * k + 3]), csa, csb, g, st);
+  double* o = out + 17 * k;
+  o[0] = c ? 1.0 : 0.0;
+  o[1] = g.n.x;
+  o[2] = g.n.y;
+  o[3] = g.cp.x;
+  o[4] = g.cp.y;
+  o[5] = g.bv1.x;
+  o[6] = g.bv1.y;
+  o[7] = g.bv2.x;
+  o[8] = g.bv2.y;
+  o[9] = g.overlap;
+  o[10] = g.rv.x;
+  o[11] = g.rv.y;
+  o[12] = g.nrv.x;
+  o[13] = g.nrv.y;
+  o[14] = g.srv.x;
+  o[15] = g.srv.y;
+  o[16] = (double)g.iters;
+  if (st) atomicOr(status, st);
+}
+
+}  // namespace xdem

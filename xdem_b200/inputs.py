@@ -1,0 +1,155 @@
+"""Seeded synthetic inputs with the shapes, sizes and distributions of the
+benchmark configurations (there is no dataset: every input is generated).
+
+Positions come from random sequential addition (RSA) of bounding discs
+without overlap; a packing denser than RSA can reach is then made by the
+reference's own recipe, an affine scale of box and positions
+(scaleBoundarySizeToGivenSolidFraction, PeriodicBoundaryWorld.cpp:276-284),
+optionally followed by relaxation or controlled compression on the GPU.
+"""
+import ctypes as C
+import math
+
+import numpy as np
+
+from . import abi
+
+KN = 1.0e4
+KT = 0.5 * KN
+FRICTION = 0.5
+DAMPING_RATIO = 0.3
+# restitution coefficient with normal damping ratio 0.3:
+# e = exp(-zeta*pi/sqrt(1-zeta^2)); the reference's damping factor is then 2*sqrt(kn)*zeta
+RESTITUTION = math.exp(-DAMPING_RATIO * math.pi / math.sqrt(1.0 - DAMPING_RATIO ** 2))
+
+
+def particle_properties(shape, radius, aspect, density=1.0):
+    lib = abi.load_library()
+    n = len(radius)
+    shape = np.ascontiguousarray(shape, np.int32)
+    radius = np.ascontiguousarray(radius, np.float64)
+    aspect = np.ascontiguousarray(aspect, np.float64)
+    out = {k: np.zeros(n) for k in ("volume", "mass", "inv_mass", "inertia", "inv_inertia")}
+    d = C.POINTER(C.c_double)
+    st = lib.xdem_particle_properties(
+        n, shape.ctypes.data_as(C.POINTER(C.c_int32)), radius.ctypes.data_as(d),
+        aspect.ctypes.data_as(d), density, *[out[k].ctypes.data_as(d) for k in
+                                             ("volume", "mass", "inv_mass", "inertia", "inv_inertia")])
+    if st:
+        raise abi.XdemError(st, "xdem_particle_properties")
+    return out
+
+
+def rsa_positions(bound_radius, box, seed, max_attempts=100000):
+    lib = abi.load_library()
+    n = len(bound_radius)
+    r = np.ascontiguousarray(bound_radius, np.float64)
+    b = np.ascontiguousarray(box, np.float64)
+    x = np.zeros(n)
+    y = np.zeros(n)
+    d = C.POINTER(C.c_double)
+    st = lib.xdem_rsa_positions(n, r.ctypes.data_as(d), b.ctypes.data_as(d), C.c_uint64(seed),
+                                max_attempts, x.ctypes.data_as(d), y.ctypes.data_as(d))
+    if st:
+        raise abi.XdemError(st, "xdem_rsa_positions")
+    return x, y
+
+
+def assemble(shape, radius, aspect, x, y, vx, vy, rot, rot_vel, density=1.0):
+    n = len(radius)
+    props = particle_properties(shape, radius, aspect, density)
+    p = {
+        "shape": np.ascontiguousarray(shape, np.int32),
+        "up_level": np.arange(n, dtype=np.int32),
+        "setting": np.zeros(n, np.int32),
+        "is_rattler": np.zeros(n, np.int32),
+        "outer_radius": np.ascontiguousarray(radius, np.float64),
+        "radius": np.ascontiguousarray(radius, np.float64),
+        "aspect_ratio": np.ascontiguousarray(aspect, np.float64),
+        "x": np.ascontiguousarray(x, np.float64), "y": np.ascontiguousarray(y, np.float64),
+        "vx": np.ascontiguousarray(vx, np.float64), "vy": np.ascontiguousarray(vy, np.float64),
+        "rot": np.ascontiguousarray(rot, np.float64),
+        "rot_vel": np.ascontiguousarray(rot_vel, np.float64),
+        "num_sub": np.zeros(n, np.int32),
+        "branch_x": np.zeros(n), "branch_y": np.zeros(n),
+    }
+    p.update(props)
+    return p
+
+
+def box_for(area, phi):
+    half = 0.5 * math.sqrt(area / phi)
+    return np.array([-half, half, -half, half])
+
+
+def scale_to_fraction(p, box, volume_sum, phi):
+    """scaleBoundarySizeToGivenSolidFraction (PeriodicBoundaryWorld.cpp:276-284)"""
+    cur = volume_sum / ((box[1] - box[0]) * (box[3] - box[2]))
+    s = math.sqrt(cur / phi)
+    p["x"] = p["x"] * s
+    p["y"] = p["y"] * s
+    return box * s
+
+
+def disc_system(n, radii=(0.5, 0.7), phi_rsa=0.5, phi=0.70, seed=0, vel_sigma=0.01,
+                density=1.0):
+    """Bidisperse discs, 50:50 (config: 1,024 discs, r 0.5/0.7, phi 0.70)."""
+    rng = np.random.default_rng(seed)
+    r = np.where(rng.permutation(n) < n // 2, radii[0], radii[1]).astype(np.float64)
+    area = float(np.sum(np.pi * r * r))
+    box = box_for(area, phi_rsa)
+    x, y = rsa_positions(r, box, seed + 1)
+    vx = rng.normal(0.0, vel_sigma, n)
+    vy = rng.normal(0.0, vel_sigma, n)
+    p = assemble(np.zeros(n, np.int32), r, np.ones(n), x, y, vx, vy, np.zeros(n), np.zeros(n),
+                 density)
+    if phi is not None and phi != phi_rsa:
+        box = scale_to_fraction(p, box, float(np.sum(p["volume"])), phi)
+    return p, box
+
+
+def ellipse_system(n, b=None, aspect=None, phi_rsa_circle=0.45, phi=None, seed=0, vel_sigma=0.0,
+                   density=1.0, rng_kind="bidisperse"):
+    """Ellipses with semi-axes (a, b), a = aspect*b, orientations U[0, pi).
+    `b` and `aspect` are arrays, or callables rng -> array."""
+    rng = np.random.default_rng(seed)
+    bb = b(rng, n) if callable(b) else np.asarray(b, np.float64)
+    asp = aspect(rng, n) if callable(aspect) else np.asarray(aspect, np.float64)
+    a = asp * bb
+    area_circle = float(np.sum(np.pi * a * a))
+    box = box_for(area_circle, phi_rsa_circle)
+    x, y = rsa_positions(a, box, seed + 1)
+    rot = rng.uniform(0.0, np.pi, n)
+    vx = rng.normal(0.0, vel_sigma, n) if vel_sigma > 0 else np.zeros(n)
+    vy = rng.normal(0.0, vel_sigma, n) if vel_sigma > 0 else np.zeros(n)
+    p = assemble(np.ones(n, np.int32), a, asp, x, y, vx, vy, rot, np.zeros(n), density)
+    if phi is not None:
+        box = scale_to_fraction(p, box, float(np.sum(p["volume"])), phi)
+    return p, box
+
+
+def time_step(p, kn=KN, factor=0.02):
+    """dt = 0.02 * sqrt(m_min / kn)"""
+    return factor * math.sqrt(float(np.min(p["mass"][p["shape"] != abi.SHAPE_CLUMP])) / kn)
+
+
+# ---- configuration-shaped generators ------------------------------------------
+
+def c1_b(rng, n):
+    return rng.uniform(0.4, 0.6, n)
+
+
+def c1_aspect(rng, n):
+    return np.full(n, 1.5)
+
+
+def c2_b(rng, n):
+    return np.where(rng.permutation(n) < n // 2, 0.5, 0.7).astype(np.float64)
+
+
+def c2_aspect(rng, n):
+    return rng.uniform(1.0, 2.0, n)
+
+
+def c4_aspect(rng, n):
+    return rng.uniform(1.0, 3.0, n)
