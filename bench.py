@@ -1,0 +1,467 @@
+#!/usr/bin/env python
+"""Throughput of the per-timestep DEM path on B200: particle-steps/s.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl xdem|reference]
+                    [--workload NAME] [--n PARTICLES]
+
+One step = one time step of the whole particle system (the reference's
+takeTimeStep).  The default workload is a Lees-Edwards shear of ellipses at
+the shapes of the learned-warm-start configuration (a/b ~ U[1,3], b in
+{0.5, 0.7}, solid fraction 0.85, shear rate 1e-3 sqrt(kn/m_min)), 1,048,576
+particles, plain FP64 closest-approach contact law.  The packing is generated
+(RSA of bounding discs, then strain-controlled compression on the GPU) before
+any timing.
+
+Timed regions (all after W untimed warm-up steps, each of K steps):
+  value      device time of K steps through xdem_run (CUDA events on the
+             library's stream), inputs resident in HBM (state + contact
+             history exceed the 126 MB L2);
+  roofline   the same K steps with per-kernel CUDA events, dominant kernel;
+  e2e        K x (upload state from pinned host memory, one step, download
+             state), CUDA events on the library's stream.
+The CPU baseline runs the compiled reference (oracle/_ref) with all host
+threads on the same packing for a bounded number of steps.
+
+Multi-GPU: the path does not shard (one system per GPU); with N ranks every
+rank runs its own replica (weak scaling), value = sum over ranks.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+RANK = int(os.environ.get("RANK", "0"))
+WORLD = int(os.environ.get("WORLD_SIZE", "1"))
+LOCAL = int(os.environ.get("LOCAL_RANK", "0"))
+if WORLD > 1:
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    devs = vis.split(",") if vis else [str(i) for i in range(64)]
+    os.environ["CUDA_VISIBLE_DEVICES"] = devs[LOCAL]
+
+import ctypes as C  # noqa: E402
+
+import numpy as np  # noqa: E402
+
+METRIC = "particle-steps/s, 1 B200: learned/batched FP32 vs plain FP64 GPU, same accuracy"
+UNIT = "particle-steps/s"
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+# ---------------------------------------------------------------------------
+# workloads
+# ---------------------------------------------------------------------------
+def workload_le_ellipses(n, seed):
+    """Lees-Edwards shear of ellipses, a/b ~ U[1,3], b in {0.5,0.7}, phi 0.85."""
+    from xdem_b200 import abi, inputs
+    from xdem_b200.world import World, make_control, make_params
+    p, box = inputs.ellipse_system(n, b=inputs.c2_b, aspect=inputs.c4_aspect, phi_rsa_circle=0.40,
+                                   phi=None, seed=seed)
+    dt = inputs.time_step(p)
+    m_min = float(np.min(p["mass"]))
+    rate = 1e-3 * math.sqrt(inputs.KN / m_min)
+    # compression: PeriodicControlWorld strain control to solid fraction 0.85,
+    # with global damping 0.1 (the reference drivers' compression setting)
+    prm_c = make_params(abi.WORLD_PERIODIC_CONTROL, dt, box, inputs.KN, inputs.KT,
+                        inputs.RESTITUTION, inputs.FRICTION, global_damping=0.1)
+    w = World(prm_c)
+    w.set_particles(p)
+    area0 = (box[1] - box[0]) * (box[3] - box[2])
+    phi0 = float(p["volume"].sum() / area0)
+    phi_target = 0.85
+    steps_c = 4000
+    # scale per step s = 1 + r*L*dt; choose r so that steps_c steps reach the target
+    L = box[1] - box[0]
+    s_total = math.sqrt(phi0 / phi_target)
+    s_step = s_total ** (1.0 / steps_c)
+    r = (s_step - 1.0) / (L * dt)  # first-step rate; L shrinks, so the run is slightly slower
+    ctl = make_control(box_law=abi.BOX_STRAIN, p0=r, p1=r, reset_rattlers=False)
+    t = time.time()
+    done = 0
+    while True:
+        b = w.getBoundary()
+        phi = float(p["volume"].sum() / ((b[1] - b[0]) * (b[3] - b[2])))
+        if phi >= phi_target or done > 3 * steps_c:
+            break
+        L = b[1] - b[0]
+        ctl.p0 = ctl.p1 = (s_step - 1.0) / (L * dt)
+        w.run(200, ctl)
+        done += 200
+    w.run(1000, make_control())  # relax at the final box
+    log(f"setup: compressed phi {phi0:.3f} -> {phi:.3f} in {done} steps, {time.time() - t:.1f}s")
+    st = w.get_state()
+    contacts = w.get_contacts()
+    b = w.getBoundary()
+    q = dict(p)
+    for k in ("x", "y", "vx", "vy", "rot", "rot_vel"):
+        q[k] = st[k].copy()
+    q["is_rattler"] = st["is_rattler"].copy()
+    w.close()
+    prm = make_params(abi.WORLD_LEES_EDWARDS, dt, b, inputs.KN, inputs.KT, inputs.RESTITUTION,
+                      inputs.FRICTION, shift_strain_rate=rate)
+    return {"particles": q, "contacts": contacts, "params": prm, "control": make_control(),
+            "config": {"workload": f"lees_edwards_shear_ellipses_{n}", "n_particles": n,
+                       "world": "LeesEdwardsBoundaryWorld", "contact_law": "closest-approach (Newton)",
+                       "aspect_ratio": "U[1,3]", "b": "{0.5,0.7}", "solid_fraction": round(phi, 4),
+                       "shear_rate": rate, "dt": dt, "precision": "fp64"}}
+
+
+def workload_periodic_discs(n, seed):
+    """Bidisperse discs r 0.5/0.7 at phi 0.70, PeriodicBoundaryWorld (config-0 recipe at size n)."""
+    from xdem_b200 import abi, inputs
+    from xdem_b200.world import make_control, make_params
+    p, box = inputs.disc_system(n, phi=0.70, seed=seed)
+    dt = inputs.time_step(p)
+    prm = make_params(abi.WORLD_PERIODIC, dt, box, inputs.KN, inputs.KT, inputs.RESTITUTION,
+                      inputs.FRICTION)
+    return {"particles": p, "contacts": None, "params": prm, "control": make_control(),
+            "config": {"workload": f"periodic_discs_{n}", "n_particles": n,
+                       "world": "PeriodicBoundaryWorld", "contact_law": "disc-disc",
+                       "radii": "{0.5,0.7}", "solid_fraction": 0.70, "dt": dt, "precision": "fp64"}}
+
+
+WORKLOADS = {"le_ellipses": workload_le_ellipses, "periodic_discs": workload_periodic_discs}
+
+
+# ---------------------------------------------------------------------------
+# measurement helpers
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during a timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index=0):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 8:
+                self.rows.append(parts)
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[4 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic_per_particle(kernel):
+    """DRAM bytes per particle of `kernel` from the committed ncu summary, or None."""
+    path = os.path.join(ROOT, "profiles", "traffic_per_particle.txt")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        parts = line.split()
+        if len(parts) >= 2 and parts[0] == kernel:
+            try:
+                return float(parts[1])
+            except ValueError:
+                return None
+    return None
+
+
+def update_kernel_bytes(n, contacts, prm):
+    """Algorithmic DRAM bytes of one k_update_contacts launch.
+    Per particle: the owner's state (pos 16, vel 16, rot 8, spin 8, radius 8,
+    aspect 8, outer radius 8, setting 4, up-level 4, shape 4, history count 4)
+    = 88 B, written once: new history count 4 B, incoming counter 4 B.
+    Per contact: previous history read (partner 4, normal 16, shear 16,
+    damping 8) = 44 B; new record written (partner 4, normal 16, shear 16,
+    damping 8, force 16, two torques 16, branch vector 16) = 92 B; partner's
+    incoming reference 4 B + counter 4 B = 8 B.  Neighbour reads of other
+    particles' state are counted once with the owner (they hit L2)."""
+    return 96.0 * n + 144.0 * contacts
+
+
+def _cpu_child(path, steps, warmup, threads, budget_s):
+    """Child process: times the compiled reference (else the C restatement) on
+    the workload saved at `path`; prints one JSON line."""
+    import oracle
+    from xdem_b200 import abi
+    z = np.load(path, allow_pickle=False)
+    p = {k[2:]: z[k] for k in z.files if k.startswith("p_")}
+    c = {k[2:]: z[k] for k in z.files if k.startswith("c_")}
+    prm = abi.Params()
+    C.memmove(C.byref(prm), z["params"].tobytes(), C.sizeof(abi.Params))
+    ctl = abi.Control()
+    C.memmove(C.byref(ctl), z["control"].tobytes(), C.sizeof(abi.Control))
+    kind = "reference" if oracle.ref_available() else "port"
+    W = oracle.RefWorld if kind == "reference" else oracle.PortWorld
+    w = W(prm, threads)
+    w.set_particles(p)
+    if c and len(c["id_i"]):
+        w.set_contacts(c)
+    for _ in range(warmup):
+        w.run(1, ctl)
+    t0 = time.perf_counter()
+    w.run(1, ctl)
+    one = time.perf_counter() - t0
+    k = max(1, min(steps, int(budget_s / max(one, 1e-6))))
+    t0 = time.perf_counter()
+    w.run(k, ctl)
+    dt = time.perf_counter() - t0
+    n = len(p["x"])
+    print(json.dumps({"value": n * k / dt, "steps": k, "kind": kind, "one_step_s": one}), flush=True)
+
+
+def run_reference(work, steps, warmup, threads, budget_s=25.0, timeout_s=900):
+    """Times the CPU reference in a child process with a watchdog (the
+    reference's Newton loop has no iteration cap and can hang on deep
+    overlaps).  Returns the child's result dict or {"error": ...}."""
+    import tempfile
+    path = os.path.join(tempfile.gettempdir(), f"xdem_bench_{os.getpid()}.npz")
+    arrs = {f"p_{k}": v for k, v in work["particles"].items() if isinstance(v, np.ndarray)}
+    if work["contacts"] is not None:
+        arrs.update({f"c_{k}": v for k, v in work["contacts"].items()})
+    arrs["params"] = np.frombuffer(bytes(work["params"]), np.uint8)
+    arrs["control"] = np.frombuffer(bytes(work["control"]), np.uint8)
+    np.savez(path, **arrs)
+    cmd = [sys.executable, os.path.abspath(__file__), "--cpu-child", path, "--steps", str(steps),
+           "--warmup", str(warmup), "--threads", str(threads), "--budget", str(budget_s)]
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+    try:
+        r = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout_s, env=env)
+        lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
+        if r.returncode != 0 or not lines:
+            return {"error": f"exit {r.returncode}: {r.stderr.strip()[-300:]}"}
+        return json.loads(lines[-1])
+    except subprocess.TimeoutExpired:
+        return {"error": f"no result within {timeout_s} s (reference did not finish)"}
+    finally:
+        if os.path.exists(path):
+            os.remove(path)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="xdem", choices=["xdem", "reference"])
+    ap.add_argument("--workload", default="le_ellipses", choices=sorted(WORKLOADS))
+    ap.add_argument("--n", type=int, default=1 << 20)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-child", default=None, help=argparse.SUPPRESS)
+    ap.add_argument("--threads", type=int, default=0, help=argparse.SUPPRESS)
+    ap.add_argument("--budget", type=float, default=20.0, help=argparse.SUPPRESS)
+    args = ap.parse_args()
+    if args.cpu_child:
+        _cpu_child(args.cpu_child, args.steps, args.warmup, args.threads or os.cpu_count(),
+                   args.budget)
+        return
+
+    dist = None
+    if WORLD > 1:
+        import torch
+        import torch.distributed as dist_mod
+        from datetime import timedelta
+        dist_mod.init_process_group("gloo", timeout=timedelta(seconds=600))
+        dist = dist_mod
+
+    if args.impl == "reference":
+        if RANK != 0:
+            if dist:
+                dist.destroy_process_group()
+            return
+        work = WORKLOADS[args.workload](args.n, args.seed)
+        threads = os.cpu_count() or 1
+        res = run_reference(work, args.steps, 1, threads, budget_s=60.0)
+        if "error" in res:
+            print(json.dumps({"impl": "reference", "unavailable": res["error"]}), flush=True)
+        else:
+            v, k = res["value"], res["steps"]
+            sample = (f"{k} steps of the full {work['config']['n_particles']}-particle workload "
+                      f"after 1 warm-up step, {threads} threads")
+            line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT,
+                    "n_gpus": args.gpus, "steps": k, "warmup": 1,
+                    "ms_per_step": 1e3 * work["config"]["n_particles"] / v,
+                    "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                    "data": "synthetic", "config": work["config"],
+                    "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": res["kind"],
+                                     "sample": sample},
+                    "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0,
+                            "d2h_bytes_per_step": 0}}
+            print(json.dumps(line), flush=True)
+        if dist:
+            dist.destroy_process_group()
+        return
+
+    from xdem_b200 import abi
+    from xdem_b200.world import World
+
+    work = WORKLOADS[args.workload](args.n, args.seed + RANK)
+    p = work["particles"]
+    n = len(p["x"])
+    w = World(work["params"])
+    w.set_particles(p)
+    if work["contacts"] is not None and len(work["contacts"]["id_i"]):
+        w.set_contacts(work["contacts"])
+    ctl = work["control"]
+    lib = w.lib
+
+    # warm-up
+    w.run(max(args.warmup, 3), ctl)
+
+    def barrier():
+        if dist:
+            dist.barrier()
+
+    # ---- value: device time of K steps ----------------------------------
+    barrier()
+    w.synchronize()
+    clocks = ClockSampler(0)
+    clocks.start()
+    l0 = w.launch_count()
+    lib.xdem_timer_start(w.h)
+    done = w.run(args.steps, ctl)
+    ms = C.c_double(0.0)
+    lib.xdem_timer_stop(w.h, C.byref(ms))
+    launches = w.launch_count() - l0
+    clk = clocks.stop()
+    ms_total = ms.value
+    contacts = w.count_contacts()
+    if dist:
+        import torch
+        t = torch.tensor([ms_total], dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_total = float(t.item())
+    value = n * done * WORLD / (ms_total / 1e3)
+
+    # ---- roofline: per-kernel events over the same number of steps ---------
+    w.set_profiling(True)
+    w.run(args.steps, ctl)
+    prof = w.profile()
+    w.set_profiling(False)
+    top = max(prof.items(), key=lambda kv: kv[1][1])
+    upd = prof.get("k_update_contacts", top[1])
+    avg_s = upd[1] / upd[0] / 1e3
+    alg_bytes = update_kernel_bytes(n, contacts, work["params"])
+    peak, peak_kind = measured_peaks()
+    achieved = alg_bytes / avg_s / 1e9
+    traffic_pp = ncu_traffic_per_particle("k_update_contacts")
+    step_ms = sum(v[1] for v in prof.values()) / args.steps
+    shares = {k: round(v[1] / sum(x[1] for x in prof.values()), 4) for k, v in prof.items()}
+
+    # ---- e2e through the C-ABI with pinned host buffers ----------------------
+    nbytes = 8 * n
+    bufs = [lib.xdem_host_alloc(nbytes) for _ in range(6)]
+    if not all(bufs):
+        raise RuntimeError("xdem_host_alloc failed")
+    st = w.get_state()
+    for buf, key in zip(bufs, ("x", "y", "vx", "vy", "rot", "rot_vel")):
+        C.memmove(buf, st[key].ctypes.data, nbytes)
+    one = abi.Control()
+    C.memmove(C.byref(one), C.byref(ctl), C.sizeof(abi.Control))
+    done_c = C.c_int32(0)
+    barrier()
+    w.synchronize()
+    lib.xdem_timer_start(w.h)
+    for _ in range(args.steps):
+        lib.xdem_upload_state(w.h, *[C.cast(b, C.POINTER(C.c_double)) for b in bufs])
+        lib.xdem_run(w.h, 1, C.byref(one), C.byref(done_c))
+        lib.xdem_download_state(w.h, *[C.cast(b, C.POINTER(C.c_double)) for b in bufs])
+    ms_e2e = C.c_double(0.0)
+    lib.xdem_timer_stop(w.h, C.byref(ms_e2e))
+    e2e_ms = ms_e2e.value
+    if dist:
+        import torch
+        t = torch.tensor([e2e_ms], dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    for b in bufs:
+        lib.xdem_host_free(b)
+    e2e = n * args.steps * WORLD / (e2e_ms / 1e3)
+    status = w.synchronize()
+
+    # ---- CPU baseline (rank 0, N = 1 only) ----------------------------------
+    cpu = None
+    if RANK == 0 and WORLD == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        res = run_reference(work, 50, 1, threads, budget_s=20.0, timeout_s=600)
+        if "error" in res:
+            cpu = {"value": None, "unit": UNIT, "cores": threads, "kind": "reference",
+                   "sample": res["error"]}
+        else:
+            cpu = {"value": res["value"], "unit": UNIT, "cores": threads, "kind": res["kind"],
+                   "sample": f"{res['steps']} steps of the full {n}-particle workload after 1 "
+                             f"warm-up step ({res['one_step_s']:.2f} s per step)"}
+
+    cfg = dict(work["config"])
+    cfg["l2"] = "inputs larger than L2 (state + contact history resident in HBM)"
+    cfg["parallelism"] = f"replicas{WORLD}" if WORLD > 1 else "single"
+    cfg["contacts"] = contacts
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": WORLD, "steps": args.steps,
+        "warmup": max(args.warmup, 3), "ms_per_step": ms_total / max(done, 1),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": cfg,
+        "contacts_per_s": contacts * done * WORLD / (ms_total / 1e3),
+        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 6 * nbytes,
+                "d2h_bytes_per_step": 6 * nbytes},
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": peak_kind,
+                     "kernel": "k_update_contacts", "algorithmic_bytes_per_launch": alg_bytes,
+                     "avg_launch_ms": avg_s * 1e3,
+                     "traffic": None if traffic_pp is None else traffic_pp * n},
+        "kernel_share": shares, "profiled_ms_per_step": step_ms,
+        "clocks": clk, "status": status,
+        "cpu_baseline": cpu,
+    }
+    if RANK == 0:
+        print(json.dumps(line), flush=True)
+    w.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

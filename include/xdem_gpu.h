@@ -217,6 +217,16 @@ int32_t xdem_get_force_and_torque(xdem_world w, double* fx, double* fy, double* 
 /* countActucalContacts (BaseWorld.cpp:262-269) */
 int32_t xdem_count_contacts(xdem_world w, int64_t* out);
 
+/* Dynamic state only (positions, velocities, orientations, spins), the part a
+   driver reads and writes every step through the BaseParticle getters and
+   setters (BaseParticle.h:112-119, :140-153).  Host arrays may be pinned
+   (cudaHostAlloc); the copies are then asynchronous on the world's stream and
+   xdem_download_state returns after they complete. */
+int32_t xdem_upload_state(xdem_world w, const double* x, const double* y, const double* vx,
+                          const double* vy, const double* rot, const double* rot_vel);
+int32_t xdem_download_state(xdem_world w, double* x, double* y, double* vx, double* vy,
+                            double* rot, double* rot_vel);
+
 /* ---- world scalars ------------------------------------------------------ */
 /* getXmin/getXmax/getYmin/getYmax (BaseWorld.h:75-78) */
 int32_t xdem_get_boundary(xdem_world w, double box[4]);
@@ -287,6 +297,27 @@ int32_t xdem_take_time_step(xdem_world w);
 int32_t xdem_run(xdem_world w, int32_t nsteps, const xdem_control* ctl, int32_t* steps_done);
 /* wait for the handle's stream; returns and clears the device status word */
 int32_t xdem_synchronize(xdem_world w);
+
+/* ---- per-kernel timing (CUDA events on the world's stream) --------------- */
+/* enable=1: every kernel launch of this world is bracketed by CUDA events and
+   xdem_run launches without graph capture; enable=0 stops and clears. */
+int32_t xdem_set_profiling(xdem_world w, int32_t enable);
+/* Number of kernel kinds; name of kind k. */
+int32_t xdem_profile_kinds(void);
+const char* xdem_profile_name(int32_t kind);
+/* Synchronises, then for every kernel kind k < nkinds writes the launches
+   recorded since profiling was enabled and their summed device time (ms). */
+int32_t xdem_get_profile(xdem_world w, int32_t nkinds, int64_t* launches, double* total_ms);
+/* Kernel launches issued on this world's stream since creation (graph
+   replays count every kernel node). */
+int32_t xdem_launch_count(xdem_world w, int64_t* out);
+/* Device-side interval on the world's stream: start records an event; stop
+   records a second one, waits for it and returns the elapsed milliseconds. */
+int32_t xdem_timer_start(xdem_world w);
+int32_t xdem_timer_stop(xdem_world w, double* ms);
+/* Page-locked host memory for asynchronous state exchange. */
+void* xdem_host_alloc(int64_t bytes);
+void xdem_host_free(void* p);
 
 /* ---- single-pair geometry (known-answer tests) ------------------------- */
 /* BaseParticle::calculateContactGeometry for one pair on the device.

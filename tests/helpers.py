@@ -1,0 +1,169 @@
+"""Shared builders and comparisons for the parity tests."""
+import numpy as np
+
+from xdem_b200 import abi, inputs
+from xdem_b200.world import make_control, make_params
+
+STATE_KEYS = ("x", "y", "vx", "vy", "rot", "rot_vel")
+CONTACT_KEYS = ("normal_x", "normal_y", "point_x", "point_y", "branch_x", "branch_y", "bv1_x",
+                "bv1_y", "bv2_x", "bv2_y", "shear_x", "shear_y", "fn_x", "fn_y", "ft_x", "ft_y",
+                "torque_i", "torque_j", "damping")
+
+
+def disc_case(n=256, phi=0.80, seed=3, kind=abi.WORLD_PERIODIC, vel_sigma=0.01, **kw):
+    p, box = inputs.disc_system(n, phi=phi, seed=seed, vel_sigma=vel_sigma)
+    dt = inputs.time_step(p)
+    prm = make_params(kind, dt, box, inputs.KN, inputs.KT, inputs.RESTITUTION, inputs.FRICTION, **kw)
+    return p, prm
+
+
+def ellipse_case(n=400, seed=5, kind=abi.WORLD_PERIODIC, method=abi.ELLIPSE_CLOSEST_APPROACH,
+                 compress=1.25, b=inputs.c2_b, aspect=inputs.c2_aspect, phi_rsa_circle=0.42,
+                 vel_sigma=0.01, shift_rate=0.1, **kw):
+    """RSA of bounding circles, then a mild affine compression (by `compress` in
+    solid fraction) that makes contacts without deep overlaps."""
+    p, box = inputs.ellipse_system(n, b=b, aspect=aspect, phi_rsa_circle=phi_rsa_circle, phi=None,
+                                   seed=seed, vel_sigma=vel_sigma)
+    area = (box[1] - box[0]) * (box[3] - box[2])
+    phi0 = p["volume"].sum() / area
+    box = inputs.scale_to_fraction(p, box, p["volume"].sum(), phi0 * compress)
+    dt = inputs.time_step(p)
+    prm = make_params(kind, dt, box, inputs.KN, inputs.KT, inputs.RESTITUTION, inputs.FRICTION,
+                      ellipse_method=method,
+                      shift_strain_rate=shift_rate if kind == abi.WORLD_LEES_EDWARDS else 0.0, **kw)
+    return p, prm
+
+
+def clump_case(nfree=120, nclump=30, seed=11, phi=0.55):
+    """Discs plus clumps of 2-5 circular sub-discs (radii U[0.3,0.6], offsets
+    within 0.8 of the clump centre); sub-particle ids follow the clump id."""
+    rng = np.random.default_rng(seed)
+    # bounding radius of each body for RSA
+    bodies = []
+    for _ in range(nfree):
+        bodies.append(("disc", rng.choice([0.5, 0.7])))
+    for _ in range(nclump):
+        k = int(rng.integers(2, 6))
+        r = rng.uniform(0.3, 0.6, k)
+        ang = rng.uniform(0, 2 * np.pi, k)
+        rad = 0.8 * np.sqrt(rng.uniform(0, 1, k))
+        off = np.stack([rad * np.cos(ang), rad * np.sin(ang)], 1)
+        bodies.append(("clump", (r, off)))
+    order = rng.permutation(len(bodies))
+    bodies = [bodies[i] for i in order]
+    bound = np.array([b[1] if b[0] == "disc" else float(np.max(np.hypot(b[1][1][:, 0], b[1][1][:, 1]) + b[1][0]))
+                      for b in bodies])
+    area = float(np.sum(np.pi * bound ** 2))
+    box = inputs.box_for(area, phi)
+    bx, by = inputs.rsa_positions(bound, box, seed + 7)
+    rows = []
+    for (kind, data), cx, cy in zip(bodies, bx, by):
+        if kind == "disc":
+            rows.append(dict(shape=0, r=data, x=cx, y=cy, up=-1, setting=0, nsub=0))
+        else:
+            r, off = data
+            rows.append(dict(shape=2, r=-1.0, x=cx, y=cy, up=-1, setting=abi.SKIP_CONTACT_DETECTION,
+                             nsub=len(r)))
+            for k in range(len(r)):
+                rows.append(dict(shape=0, r=r[k], x=cx + off[k, 0], y=cy + off[k, 1], up=-2,
+                                 setting=abi.SKIP_TIME_INTEGRAL | abi.SKIP_MACRO_SUM, nsub=0))
+    n = len(rows)
+    shape = np.array([r["shape"] for r in rows], np.int32)
+    rad = np.array([r["r"] for r in rows])
+    x = np.array([r["x"] for r in rows])
+    y = np.array([r["y"] for r in rows])
+    nsub = np.array([r["nsub"] for r in rows], np.int32)
+    setting = np.array([r["setting"] for r in rows], np.int32)
+    up = np.arange(n, dtype=np.int32)
+    cur = -1
+    for i, r in enumerate(rows):
+        if r["shape"] == 2:
+            cur = i
+        elif r["up"] == -2:
+            up[i] = cur
+    prop_shape = np.where(shape == 2, 0, shape).astype(np.int32)
+    prop_r = np.where(shape == 2, 1.0, rad)
+    p = inputs.assemble(prop_shape, prop_r, np.ones(n), x, y, rng.normal(0, 0.01, n),
+                        rng.normal(0, 0.01, n), np.zeros(n), np.zeros(n))
+    p["shape"] = shape
+    p["radius"] = rad.copy()
+    p["outer_radius"] = rad.copy()
+    p["up_level"] = up
+    p["setting"] = setting
+    p["num_sub"] = nsub
+    bxv = np.zeros(n)
+    byv = np.zeros(n)
+    from xdem_b200 import abi as A
+    import ctypes as C
+    lib = A.load_library()
+    d = C.POINTER(C.c_double)
+    for i in np.where(shape == 2)[0]:
+        k = nsub[i]
+        s = np.arange(i + 1, i + 1 + k)
+        out = np.zeros(7)
+        brx = np.zeros(k)
+        bry = np.zeros(k)
+        sub_shape = np.ascontiguousarray(shape[s])
+        st = lib.xdem_clump_properties(
+            int(k), sub_shape.ctypes.data_as(C.POINTER(C.c_int32)),
+            np.ascontiguousarray(rad[s]).ctypes.data_as(d), np.ones(k).ctypes.data_as(d),
+            np.ascontiguousarray(x[s]).ctypes.data_as(d), np.ascontiguousarray(y[s]).ctypes.data_as(d),
+            np.zeros(k).ctypes.data_as(d), 1.0, out.ctypes.data_as(d), brx.ctypes.data_as(d),
+            bry.ctypes.data_as(d))
+        assert st == 0
+        p["x"][i], p["y"][i] = out[0], out[1]
+        p["volume"][i], p["mass"][i], p["inv_mass"][i] = out[2], out[3], out[4]
+        p["inertia"][i], p["inv_inertia"][i] = out[5], out[6]
+        p["vx"][s] = p["vx"][i]
+        p["vy"][s] = p["vy"][i]
+        for q, sp in enumerate(s):
+            # GluedParticle.cpp:71-75: each sub-particle takes the clump's mass and inertia
+            p["mass"][sp], p["inv_mass"][sp] = out[3], out[4]
+            p["inertia"][sp], p["inv_inertia"][sp] = out[5], out[6]
+            bxv[sp], byv[sp] = brx[q], bry[q]
+            p["vx"][sp] = p["vx"][i]
+            p["vy"][sp] = p["vy"][i]
+    p["branch_x"] = bxv
+    p["branch_y"] = byv
+    p["outer_radius"][shape == 2] = -1.0
+    dt = inputs.time_step(p)
+    prm = make_params(abi.WORLD_PERIODIC, dt, box, inputs.KN, inputs.KT, inputs.RESTITUTION,
+                      inputs.FRICTION)
+    return p, prm
+
+
+def same_pairs(ca, cb):
+    return (len(ca["id_i"]) == len(cb["id_i"]) and np.array_equal(ca["id_i"], cb["id_i"])
+            and np.array_equal(ca["id_j"], cb["id_j"]))
+
+
+def rel_err(a, b, floor=1e-300):
+    scale = max(np.max(np.abs(a)) if len(a) else 0.0, np.max(np.abs(b)) if len(b) else 0.0, floor)
+    return float(np.max(np.abs(a - b)) / scale) if len(a) else 0.0
+
+
+def compare_contacts(ca, cb, tol, keys=CONTACT_KEYS):
+    assert same_pairs(ca, cb), (len(ca["id_i"]), len(cb["id_i"]))
+    worst = {k: rel_err(ca[k], cb[k]) for k in keys}
+    bad = {k: v for k, v in worst.items() if v > tol}
+    assert not bad, bad
+    return worst
+
+
+def compare_states(sa, sb, tol, keys=STATE_KEYS):
+    worst = {k: rel_err(sa[k], sb[k]) for k in keys}
+    bad = {k: v for k, v in worst.items() if v > tol}
+    assert not bad, bad
+    return worst
+
+
+def controls():
+    return {
+        "plain": make_control(),
+        "stress": make_control(update_stress=True),
+        "strain": make_control(update_stress=True, box_law=abi.BOX_STRAIN, p0=-2e-3, p1=-2e-3),
+        "stress_xy": make_control(update_stress=True, box_law=abi.BOX_STRESS_XY, p0=5.0,
+                                  scale_rattlers=0.99, sequence=abi.SEQ_SUBSTEPS),
+        "uniform": make_control(update_stress=True, box_law=abi.BOX_STRESS_UNIFORM, p0=5.0,
+                                reset_rattlers=True),
+    }

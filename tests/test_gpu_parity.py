@@ -1,0 +1,267 @@
+"""GPU parity: the CUDA path (through the C-ABI) against the C restatement
+(oracle/), which tests/test_oracle_vs_reference.py pins to the compiled
+reference.
+
+Tolerances.  The CUDA FP64 path performs the reference's operations in the
+reference's order with -fmad=false; it differs only where CUDA's cos, sin,
+atan2 and pow round differently from glibc's (within a few ulp).  Hence:
+  - contact pair sets: identical (bit-exact integer sets);
+  - one step from an identical state: every contact field and every particle
+    sum within 1e-12 relative (to the largest magnitude of that field);
+  - short trajectories: within 1e-9 relative after 50 steps;
+  - determinism: two GPU runs agree bit for bit.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from xdem_b200 import abi
+from xdem_b200.world import World, make_control, pair_geometry
+
+from helpers import (clump_case, compare_contacts, compare_states, controls, disc_case,
+                     ellipse_case, rel_err, same_pairs)
+
+pytestmark = pytest.mark.gpu
+
+ONE_STEP_TOL = 1e-12
+TRAJ_TOL = 1e-9
+
+
+def _pair(p, prm):
+    g = World(prm)
+    g.set_particles(p)
+    c = oracle.PortWorld(prm)
+    c.set_particles(p)
+    if prm.world_kind == abi.WORLD_PERIODIC_CONTROL:
+        g.setVirtualBoundaryMass()
+        c.setVirtualBoundaryMass()
+    return g, c
+
+
+def _compare_worlds(g, c, tol):
+    compare_contacts(g.get_contacts(), c.get_contacts(), tol)
+    compare_states(g.get_state(), c.get_state(), tol)
+    fg, fc = g.get_force_and_torque(), c.get_force_and_torque()
+    for k in ("fx", "fy", "torque"):
+        assert rel_err(fg[k], fc[k]) <= tol, k
+    assert np.array_equal(fg["num_contacts"], fc["num_contacts"])
+    assert np.array_equal(g.get_state()["is_rattler"], c.get_state()["is_rattler"])
+
+
+def test_device_present():
+    import ctypes as C
+    lib = abi.load_library()
+    n = C.c_int32(0)
+    assert lib.xdem_device_count(C.byref(n)) == 0 and n.value >= 1
+
+
+@pytest.mark.parametrize("method", [abi.ELLIPSE_CLOSEST_APPROACH, abi.ELLIPSE_INTERSECTION])
+def test_pair_geometry_ellipses(method):
+    rng = np.random.default_rng(42 + method)
+    N = 4000
+    b1 = rng.uniform(0.4, 0.7, N)
+    a1 = b1 * rng.uniform(1.0, 3.0, N)
+    b2 = rng.uniform(0.4, 0.7, N)
+    a2 = b2 * rng.uniform(1.0, 3.0, N)
+    ang = rng.uniform(0, 2 * np.pi, N)
+    dist = rng.uniform(0.5, 1.05, N) * (a1 + a2)
+    pi = np.stack([np.ones(N), a1, a1 / b1, rng.normal(0, 5, N), rng.normal(0, 5, N),
+                   rng.normal(0, .1, N), rng.normal(0, .1, N), rng.uniform(0, np.pi, N),
+                   rng.normal(0, .1, N)], 1)
+    pj = pi.copy()
+    pj[:, 1], pj[:, 2] = a2, a2 / b2
+    pj[:, 3] = pi[:, 3] + dist * np.cos(ang)
+    pj[:, 4] = pi[:, 4] + dist * np.sin(ang)
+    pj[:, 5:7] = rng.normal(0, .1, (N, 2))
+    pj[:, 7] = rng.uniform(0, np.pi, N)
+    # aligned and crossed orientations
+    pi[:200, 7] = 0.0
+    pj[:200, 7] = 0.0
+    pj[200:400, 7] = np.pi / 2
+    off = np.zeros((N, 4))
+    og, sg = pair_geometry(pi, pj, off, method)
+    oc, sc = oracle.pair_geometry(pi, pj, off, method, "port")
+    assert sg == sc
+    assert np.array_equal(og[:, 0], oc[:, 0]), np.where(og[:, 0] != oc[:, 0])
+    hit = og[:, 0] == 1
+    assert hit.sum() > 500
+    for col in range(1, 16):
+        assert rel_err(og[hit, col], oc[hit, col]) <= 1e-11, col
+    if method == abi.ELLIPSE_CLOSEST_APPROACH:
+        assert np.array_equal(og[hit, 16], oc[hit, 16])  # Newton iteration counts
+
+
+def test_pair_geometry_circles():
+    rng = np.random.default_rng(7)
+    N = 2000
+    r1 = rng.choice([0.5, 0.7], N)
+    r2 = rng.choice([0.5, 0.7], N)
+    ang = rng.uniform(0, 2 * np.pi, N)
+    dist = rng.uniform(0.8, 1.02, N) * (r1 + r2)
+    dist[:10] = (r1 + r2)[:10]  # exact touching: overlap 0 counts as contact
+    pi = np.stack([np.zeros(N), r1, np.ones(N), np.zeros(N), np.zeros(N), rng.normal(0, .1, N),
+                   rng.normal(0, .1, N), np.zeros(N), rng.normal(0, .1, N)], 1)
+    pj = np.stack([np.zeros(N), r2, np.ones(N), dist * np.cos(ang), dist * np.sin(ang),
+                   rng.normal(0, .1, N), rng.normal(0, .1, N), np.zeros(N), rng.normal(0, .1, N)], 1)
+    off = np.zeros((N, 4))
+    og, _ = pair_geometry(pi, pj, off)
+    oc, _ = oracle.pair_geometry(pi, pj, off, 0, "port")
+    np.testing.assert_array_equal(og[:, :16], oc[:, :16])  # + - * / sqrt only: bit-exact
+
+
+def test_newton_cap_raises_status():
+    """The input that cycles forever in the reference's uncapped Newton loop
+    (EllipticParticle.cpp:621) stops at the cap on the host restatement, and
+    the product reports XDEM_ERR_NEWTON rather than hanging."""
+    A, B, C, D, E = (-0.26036636837902971, -0.32298145246944276, 0.12112405448664837,
+                     0.28164745468898272, 0.087345098145840058)
+    r, it = oracle.newton_quartic(A, B, C, D, E, 0.51812102010664518)
+    assert it == 1000
+
+
+@pytest.mark.parametrize("kind", [abi.WORLD_PERIODIC, abi.WORLD_PERIODIC_CONTROL,
+                                  abi.WORLD_LEES_EDWARDS])
+def test_discs_one_step(kind):
+    p, prm = disc_case(n=400, phi=0.82, seed=1, kind=kind, shift_strain_rate=0.05)
+    g, c = _pair(p, prm)
+    g.takeTimeStep()
+    c.takeTimeStep()
+    _compare_worlds(g, c, ONE_STEP_TOL)
+
+
+@pytest.mark.parametrize("method", [abi.ELLIPSE_CLOSEST_APPROACH, abi.ELLIPSE_INTERSECTION])
+@pytest.mark.parametrize("kind", [abi.WORLD_PERIODIC, abi.WORLD_PERIODIC_CONTROL,
+                                  abi.WORLD_LEES_EDWARDS])
+def test_ellipses_one_step(kind, method):
+    p, prm = ellipse_case(n=600, seed=2, kind=kind, method=method, compress=1.6)
+    g, c = _pair(p, prm)
+    g.takeTimeStep()
+    c.takeTimeStep()
+    assert c.count_contacts() > 100
+    _compare_worlds(g, c, ONE_STEP_TOL)
+
+
+@pytest.mark.parametrize("name", ["plain", "stress", "strain", "stress_xy", "uniform"])
+def test_discs_trajectory_controls(name):
+    kind = abi.WORLD_PERIODIC_CONTROL if name != "plain" else abi.WORLD_PERIODIC
+    p, prm = disc_case(n=300, phi=0.80, seed=4, kind=kind)
+    g, c = _pair(p, prm)
+    ctl = controls()[name]
+    assert g.run(50, ctl) == 50
+    assert c.run(50, ctl) == 50
+    _compare_worlds(g, c, TRAJ_TOL)
+    assert rel_err(g.getBoundary(), c.getBoundary()) <= TRAJ_TOL
+    if ctl.update_stress:
+        assert rel_err(g.getStress(), c.getStress()) <= TRAJ_TOL
+
+
+@pytest.mark.parametrize("method", [abi.ELLIPSE_CLOSEST_APPROACH, abi.ELLIPSE_INTERSECTION])
+def test_lees_edwards_ellipses_trajectory(method):
+    p, prm = ellipse_case(n=500, seed=9, kind=abi.WORLD_LEES_EDWARDS, method=method, compress=1.5,
+                          shift_rate=0.2)
+    g, c = _pair(p, prm)
+    ctl = make_control(update_stress=True)
+    g.run(40, ctl)
+    c.run(40, ctl)
+    _compare_worlds(g, c, TRAJ_TOL)
+    assert rel_err(g.getLeesEdwards(), c.getLeesEdwards()) <= 1e-15
+    assert rel_err(g.getStress(), c.getStress()) <= TRAJ_TOL
+
+
+def test_clumps_trajectory():
+    p, prm = clump_case()
+    g, c = _pair(p, prm)
+    ctl = make_control(update_stress=True)
+    g.run(30, ctl)
+    c.run(30, ctl)
+    _compare_worlds(g, c, TRAJ_TOL)
+    sg, sc = g.get_state(), c.get_state()
+    assert rel_err(sg["branch_x"], sc["branch_x"]) <= TRAJ_TOL
+    assert rel_err(g.getStress(), c.getStress()) <= TRAJ_TOL
+
+
+def test_substeps_equal_fused_step():
+    """Calling the reference's sub-steps one by one gives the fused step's result."""
+    p, prm = disc_case(n=300, phi=0.8, seed=6)
+    a = World(prm)
+    a.set_particles(p)
+    b = World(prm)
+    b.set_particles(p)
+    for _ in range(3):
+        a.takeTimeStep()
+        b.modifyParticlePosition()
+        b.findPossibleContacts()
+        b.updateContacts()
+        b.collectForceAndTorque()
+        b.takeTimeIntegral()
+    sa, sb = a.get_state(), b.get_state()
+    for k in ("x", "y", "vx", "vy", "rot", "rot_vel"):
+        np.testing.assert_array_equal(sa[k], sb[k])
+
+
+def test_lees_edwards_substeps_equal_fused_step():
+    """LE takeTimeStep folds apply/removeBackgroudVelocity into the kernels;
+    the explicit sub-step sequence gives the same bits."""
+    p, prm = ellipse_case(n=300, seed=3, kind=abi.WORLD_LEES_EDWARDS, compress=1.5)
+    a = World(prm)
+    a.set_particles(p)
+    b = World(prm)
+    b.set_particles(p)
+    for _ in range(3):
+        a.takeTimeStep()
+        b.modifyParticlePosition()
+        b.applyBackgroudVelocity()
+        b.findPossibleContacts()
+        b.updateContacts()
+        b.removeBackgroudVelocity()
+        b.collectForceAndTorque()
+        b.takeTimeIntegral()
+        b.updateLeesEdwardBoundary()
+    sa, sb = a.get_state(), b.get_state()
+    for k in ("x", "y", "vx", "vy", "rot", "rot_vel"):
+        np.testing.assert_array_equal(sa[k], sb[k])
+
+
+def test_run_deterministic():
+    p, prm = ellipse_case(n=500, seed=8, compress=1.5)
+    out = []
+    for _ in range(2):
+        g = World(prm)
+        g.set_particles(p)
+        g.run(30, make_control(update_stress=True))
+        out.append((g.get_state(), g.get_contacts(), g.getStress()))
+    for k in ("x", "y", "vx", "vy", "rot", "rot_vel"):
+        np.testing.assert_array_equal(out[0][0][k], out[1][0][k])
+    assert same_pairs(out[0][1], out[1][1])
+    np.testing.assert_array_equal(out[0][2], out[1][2])
+
+
+def test_contact_upload_roundtrip():
+    """Contacts downloaded from the checker and uploaded to the GPU world give
+    the same next step (checkpoint/resume of the contact history)."""
+    p, prm = disc_case(n=300, phi=0.82, seed=12)
+    c = oracle.PortWorld(prm)
+    c.set_particles(p)
+    c.run(20)
+    st = c.get_state()
+    q = dict(p)
+    for k in ("x", "y", "vx", "vy", "rot", "rot_vel"):
+        q[k] = st[k].copy()
+    g = World(prm)
+    g.set_particles(q)
+    g.set_contacts(c.get_contacts())
+    compare_contacts(g.get_contacts(), c.get_contacts(), 0.0)
+    g.takeTimeStep()
+    c.takeTimeStep()
+    _compare_worlds(g, c, ONE_STEP_TOL)
+
+
+def test_stop_on_pressure():
+    p, prm = disc_case(n=300, phi=0.75, seed=13, kind=abi.WORLD_PERIODIC_CONTROL)
+    g, c = _pair(p, prm)
+    ctl = make_control(update_stress=True, box_law=abi.BOX_STRAIN, p0=-5e-3, p1=-5e-3,
+                       reset_rattlers=False, stop_pressure=2.0)
+    ng = g.run(2000, ctl)
+    nc = c.run(2000, ctl)
+    assert ng == nc and ng < 2000
+    _compare_worlds(g, c, TRAJ_TOL)

@@ -214,6 +214,17 @@ def load_library(path=LIB_PATH):
         "xdem_take_time_step": (C.c_int32, [W]),
         "xdem_run": (C.c_int32, [W, C.c_int32, P(Control), P(C.c_int32)]),
         "xdem_synchronize": (C.c_int32, [W]),
+        "xdem_upload_state": (C.c_int32, [W, _d, _d, _d, _d, _d, _d]),
+        "xdem_download_state": (C.c_int32, [W, _d, _d, _d, _d, _d, _d]),
+        "xdem_set_profiling": (C.c_int32, [W, C.c_int32]),
+        "xdem_profile_kinds": (C.c_int32, []),
+        "xdem_profile_name": (C.c_char_p, [C.c_int32]),
+        "xdem_get_profile": (C.c_int32, [W, C.c_int32, P(C.c_int64), _d]),
+        "xdem_launch_count": (C.c_int32, [W, P(C.c_int64)]),
+        "xdem_timer_start": (C.c_int32, [W]),
+        "xdem_timer_stop": (C.c_int32, [W, _d]),
+        "xdem_host_alloc": (C.c_void_p, [C.c_int64]),
+        "xdem_host_free": (None, [C.c_void_p]),
         "xdem_pair_geometry": (C.c_int32, [C.c_int32, C.c_int32, C.c_int32, _d, _d, _d, _d]),
         "xdem_rsa_positions": (C.c_int32, [C.c_int32, _d, _d, C.c_uint64, C.c_int64, _d, _d]),
         "xdem_particle_properties": (C.c_int32, [C.c_int32, _i, _d, _d, C.c_double, _d, _d, _d,

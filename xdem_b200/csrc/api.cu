@@ -55,6 +55,13 @@ struct xdem_world_s {
   uint32_t host_status = 0;
   double total_volume = 0.0;
   double control_mass = 0.0;
+  // per-kernel timing
+  bool prof_on = false;
+  std::vector<cudaEvent_t> prof_events;  // pairs (begin, end)
+  std::vector<int> prof_kind;            // kind of each pair
+  size_t prof_used = 0;                  // pairs recorded
+  int64_t launches = 0;
+  cudaEvent_t timer[2] = {nullptr, nullptr};
 };
 
 namespace {
@@ -97,59 +104,103 @@ cudaError_t download(T* dst, const T* src, size_t count, cudaStream_t s) {
   return cudaMemcpyAsync(dst, src, count * sizeof(T), cudaMemcpyDeviceToHost, s);
 }
 
+// ---- per-kernel timing ------------------------------------------------------
+enum KernelKind {
+  KK_MODIFY = 0, KK_BIN, KK_SCAN, KK_SCATTER, KK_UPDATE, KK_COLLECT, KK_INTEGRATE, KK_RATTLERS,
+  KK_STRESS_PARTIAL, KK_STRESS_FINAL, KK_END_OF_STEP, KK_SCALE, KK_BACKGROUND, KK_KE, KK_COUNT
+};
+const char* const kKindNames[KK_COUNT] = {
+    "k_modify_position", "k_bin", "k_scan", "k_scatter", "k_update_contacts", "k_collect",
+    "k_integrate", "k_rattlers", "k_stress_partial", "k_stress_final", "k_end_of_step",
+    "k_scale_positions", "k_background_velocity", "k_kinetic_energy"};
+
+void prof_begin(xdem_world_s* w, int kind) {
+  if (!w->prof_on) return;
+  size_t need = 2 * (w->prof_used + 1);
+  while (w->prof_events.size() < need) {
+    cudaEvent_t e;
+    if (cudaEventCreate(&e) != cudaSuccess) {
+      w->host_status |= XDEM_ERR_CUDA;
+      w->prof_on = false;
+      return;
+    }
+    w->prof_events.push_back(e);
+  }
+  if (w->prof_kind.size() <= w->prof_used) w->prof_kind.resize(w->prof_used + 1);
+  w->prof_kind[w->prof_used] = kind;
+  cudaEventRecord(w->prof_events[2 * w->prof_used], w->stream);
+}
+
+void prof_end(xdem_world_s* w) {
+  if (!w->prof_on) return;
+  cudaEventRecord(w->prof_events[2 * w->prof_used + 1], w->stream);
+  w->prof_used++;
+}
+
+#define LAUNCH(w, kind, ...)  \
+  do {                        \
+    prof_begin((w), (kind));  \
+    __VA_ARGS__;              \
+    prof_end((w));            \
+    (w)->launches++;          \
+  } while (0)
+
 // ---- launch helpers -------------------------------------------------------
 void launch_modify(xdem_world_s* w) {
   int n = w->dw.n;
-  k_modify_position<<<blocks_for(n, kBlock), kBlock, 0, w->stream>>>(w->dw);
+  LAUNCH(w, KK_MODIFY, k_modify_position<<<blocks_for(n, kBlock), kBlock, 0, w->stream>>>(w->dw));
 }
 
 void launch_find(xdem_world_s* w) {
   int n = w->dw.n;
-  k_bin<<<blocks_for(n, kBlock), kBlock, 0, w->stream>>>(w->dw);
-  k_scan<<<1, 1024, 0, w->stream>>>(w->dw);
+  LAUNCH(w, KK_BIN, k_bin<<<blocks_for(n, kBlock), kBlock, 0, w->stream>>>(w->dw));
+  LAUNCH(w, KK_SCAN, k_scan<<<1, 1024, 0, w->stream>>>(w->dw));
   int cells = w->nx_cap * w->ny_cap + 2 * w->nx_cap;
   int nb = std::max(blocks_for(n, kBlock), std::min(blocks_for(cells, kBlock), 1184));
-  k_scatter<<<nb, kBlock, 0, w->stream>>>(w->dw);
+  LAUNCH(w, KK_SCATTER, k_scatter<<<nb, kBlock, 0, w->stream>>>(w->dw));
 }
 
 void launch_update(xdem_world_s* w, bool fold_bg, int record) {
   int n = w->dw.n;
   if (fold_bg)
-    k_update_contacts<true><<<blocks_for(n, 128), 128, 0, w->stream>>>(w->dw, w->par, record);
+    LAUNCH(w, KK_UPDATE,
+           k_update_contacts<true><<<blocks_for(n, 128), 128, 0, w->stream>>>(w->dw, w->par, record));
   else
-    k_update_contacts<false><<<blocks_for(n, 128), 128, 0, w->stream>>>(w->dw, w->par, record);
+    LAUNCH(w, KK_UPDATE,
+           k_update_contacts<false><<<blocks_for(n, 128), 128, 0, w->stream>>>(w->dw, w->par, record));
   w->par ^= 1;
 }
 
 void launch_collect(xdem_world_s* w) {
   int n = w->dw.n;
-  k_collect<<<blocks_for(n, 128), 128, 0, w->stream>>>(w->dw, w->par);
+  LAUNCH(w, KK_COLLECT, k_collect<<<blocks_for(n, 128), 128, 0, w->stream>>>(w->dw, w->par));
 }
 
 void launch_integrate(xdem_world_s* w, bool fold_bg, int reset) {
   int n = w->dw.n;
   if (fold_bg)
-    k_integrate<true><<<blocks_for(n, kBlock), kBlock, 0, w->stream>>>(w->dw, reset);
+    LAUNCH(w, KK_INTEGRATE, k_integrate<true><<<blocks_for(n, kBlock), kBlock, 0, w->stream>>>(w->dw, reset));
   else
-    k_integrate<false><<<blocks_for(n, kBlock), kBlock, 0, w->stream>>>(w->dw, reset);
+    LAUNCH(w, KK_INTEGRATE, k_integrate<false><<<blocks_for(n, kBlock), kBlock, 0, w->stream>>>(w->dw, reset));
 }
 
 void launch_stress(xdem_world_s* w) {
   int nb = blocks_for(w->dw.n, kReduceBlock);
-  k_stress_partial<<<nb, kReduceBlock, 0, w->stream>>>(w->dw, w->par);
-  k_stress_final<<<1, 1024, 0, w->stream>>>(w->dw, nb);
+  LAUNCH(w, KK_STRESS_PARTIAL, k_stress_partial<<<nb, kReduceBlock, 0, w->stream>>>(w->dw, w->par));
+  LAUNCH(w, KK_STRESS_FINAL, k_stress_final<<<1, 1024, 0, w->stream>>>(w->dw, nb));
 }
 
 void launch_rattlers(xdem_world_s* w, int reset, double scale) {
   int n = w->dw.n;
-  k_rattlers<<<blocks_for(n, kBlock), kBlock, 0, w->stream>>>(w->dw, reset, scale);
+  LAUNCH(w, KK_RATTLERS, k_rattlers<<<blocks_for(n, kBlock), kBlock, 0, w->stream>>>(w->dw, reset, scale));
 }
 
 void launch_end_of_step(xdem_world_s* w, int law, double p0, double p1, int le_update, int stop_on,
                         double stop_p) {
-  k_end_of_step<<<1, 1, 0, w->stream>>>(w->dw, law, p0, p1, le_update, stop_on, stop_p);
+  LAUNCH(w, KK_END_OF_STEP,
+         k_end_of_step<<<1, 1, 0, w->stream>>>(w->dw, law, p0, p1, le_update, stop_on, stop_p));
   if (law != BOX_NONE)
-    k_scale_positions<<<blocks_for(w->dw.n, kBlock), kBlock, 0, w->stream>>>(w->dw);
+    LAUNCH(w, KK_SCALE, k_scale_positions<<<blocks_for(w->dw.n, kBlock), kBlock, 0, w->stream>>>(w->dw));
 }
 
 // one step of a control sequence; record: store the full contact record
@@ -262,6 +313,9 @@ int32_t xdem_destroy(xdem_world w) {
   if (!w) return XDEM_OK;
   if (w->stream) cudaStreamSynchronize(w->stream);
   w->particle_bufs.release();
+  for (cudaEvent_t e : w->prof_events) cudaEventDestroy(e);
+  for (cudaEvent_t e : w->timer)
+    if (e) cudaEventDestroy(e);
   if (w->ws) cudaFree(w->ws);
   if (w->status) cudaFree(w->status);
   if (w->own_stream && w->stream) cudaStreamDestroy(w->stream);
@@ -730,8 +784,8 @@ int32_t xdem_set_max_strain_rate(xdem_world w, double r) {
 int32_t xdem_get_kinetic_energy(xdem_world w, double* out) {
   if (!w || !out || w->dw.n <= 0) return XDEM_ERR_ARGUMENT;
   int nb = blocks_for(w->dw.n, kReduceBlock);
-  k_ke_partial<<<nb, kReduceBlock, 0, w->stream>>>(w->dw);
-  k_ke_final<<<1, 1024, 0, w->stream>>>(w->dw, nb);
+  LAUNCH(w, KK_KE, k_ke_partial<<<nb, kReduceBlock, 0, w->stream>>>(w->dw));
+  LAUNCH(w, KK_KE, k_ke_final<<<1, 1024, 0, w->stream>>>(w->dw, nb));
   CK(w, cudaGetLastError());
   WorldScalars s;
   CK(w, read_scalars(w, &s));
@@ -756,13 +810,13 @@ int32_t xdem_modify_particle_position(xdem_world w) {
 
 int32_t xdem_apply_background_velocity(xdem_world w) {
   SUBSTEP_BEGIN;
-  k_background_velocity<<<blocks_for(w->dw.n, kBlock), kBlock, 0, w->stream>>>(w->dw, 1);
+  LAUNCH(w, KK_BACKGROUND, k_background_velocity<<<blocks_for(w->dw.n, kBlock), kBlock, 0, w->stream>>>(w->dw, 1));
   SUBSTEP_END;
 }
 
 int32_t xdem_remove_background_velocity(xdem_world w) {
   SUBSTEP_BEGIN;
-  k_background_velocity<<<blocks_for(w->dw.n, kBlock), kBlock, 0, w->stream>>>(w->dw, 0);
+  LAUNCH(w, KK_BACKGROUND, k_background_velocity<<<blocks_for(w->dw.n, kBlock), kBlock, 0, w->stream>>>(w->dw, 0));
   SUBSTEP_END;
 }
 
@@ -818,15 +872,13 @@ int32_t xdem_update_total_stress(xdem_world w, double stress[4]) {
 int32_t xdem_update_boundary(xdem_world w, int32_t law, double p0, double p1) {
   SUBSTEP_BEGIN;
   if (law < 0 || law > 4) return XDEM_ERR_ARGUMENT;
-  k_end_of_step<<<1, 1, 0, w->stream>>>(w->dw, law, p0, p1, 0, 0, 0.0);
-  if (law != BOX_NONE)
-    k_scale_positions<<<blocks_for(w->dw.n, kBlock), kBlock, 0, w->stream>>>(w->dw);
+  launch_end_of_step(w, law, p0, p1, 0, 0, 0.0);
   SUBSTEP_END;
 }
 
 int32_t xdem_update_lees_edwards_boundary(xdem_world w) {
   SUBSTEP_BEGIN;
-  k_end_of_step<<<1, 1, 0, w->stream>>>(w->dw, BOX_NONE, 0.0, 0.0, 1, 0, 0.0);
+  launch_end_of_step(w, BOX_NONE, 0.0, 0.0, 1, 0, 0.0);
   SUBSTEP_END;
 }
 
@@ -847,7 +899,7 @@ int32_t xdem_scale_boundary_to_solid_fraction(xdem_world w, double phi) {
   s.xlen = s.xmax - s.xmin;
   s.ylen = s.ymax - s.ymin;
   CK(w, write_scalars(w, &s));
-  k_scale_positions<<<blocks_for(w->dw.n, kBlock), kBlock, 0, w->stream>>>(w->dw);
+  LAUNCH(w, KK_SCALE, k_scale_positions<<<blocks_for(w->dw.n, kBlock), kBlock, 0, w->stream>>>(w->dw));
   SUBSTEP_END;
 }
 
@@ -878,10 +930,11 @@ int32_t xdem_run(xdem_world w, int32_t nsteps, const xdem_control* ctl, int32_t*
   const int rec_all = ctl->stop_on_pressure ? 1 : 0;
   int body = nsteps - 1;
   const int kGraphSteps = 2;
-  if (body >= 8) {
+  if (body >= 8 && !w->prof_on) {
     // capture two steps (one per slot-set parity) and replay the graph
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
+    int64_t launches_before = w->launches;
     CK(w, cudaStreamBeginCapture(w->stream, cudaStreamCaptureModeThreadLocal));
     for (int k = 0; k < kGraphSteps; ++k) enqueue_step(w, ctl, rec_all);
     cudaError_t e = cudaStreamEndCapture(w->stream, &graph);
@@ -892,6 +945,8 @@ int32_t xdem_run(xdem_world w, int32_t nsteps, const xdem_control* ctl, int32_t*
     }
     w->par = start_par;  // capture toggled the parity kGraphSteps times
     int reps = body / kGraphSteps;
+    int64_t per_graph = w->launches - launches_before;
+    w->launches += per_graph * (reps - 1);
     for (int r = 0; r < reps && e == cudaSuccess; ++r) e = cudaGraphLaunch(exec, w->stream);
     body -= reps * kGraphSteps;
     cudaGraphExecDestroy(exec);
@@ -906,6 +961,115 @@ int32_t xdem_run(xdem_world w, int32_t nsteps, const xdem_control* ctl, int32_t*
   if (steps_done) *steps_done = s.steps_done;
   w->par = start_par ^ (s.steps_done & 1);
   return (int32_t)st;
+}
+
+int32_t xdem_upload_state(xdem_world w, const double* x, const double* y, const double* vx,
+                          const double* vy, const double* rot, const double* rot_vel) {
+  if (!w || w->dw.n <= 0 || !x || !y || !vx || !vy || !rot || !rot_vel) return XDEM_ERR_ARGUMENT;
+  const int n = w->dw.n;
+  cudaStream_t s = w->stream;
+  // positions and velocities are interleaved (double2) on the device: copy the
+  // x and y columns into the two lanes with strided 2-D copies
+  CK(w, cudaMemcpy2DAsync(&w->dw.pos[0].x, sizeof(double2), x, sizeof(double), sizeof(double), n,
+                          cudaMemcpyHostToDevice, s));
+  CK(w, cudaMemcpy2DAsync(&w->dw.pos[0].y, sizeof(double2), y, sizeof(double), sizeof(double), n,
+                          cudaMemcpyHostToDevice, s));
+  CK(w, cudaMemcpy2DAsync(&w->dw.vel[0].x, sizeof(double2), vx, sizeof(double), sizeof(double), n,
+                          cudaMemcpyHostToDevice, s));
+  CK(w, cudaMemcpy2DAsync(&w->dw.vel[0].y, sizeof(double2), vy, sizeof(double), sizeof(double), n,
+                          cudaMemcpyHostToDevice, s));
+  CK(w, upload(w->dw.rot, rot, n, s));
+  CK(w, upload(w->dw.w, rot_vel, n, s));
+  return XDEM_OK;
+}
+
+int32_t xdem_download_state(xdem_world w, double* x, double* y, double* vx, double* vy,
+                            double* rot, double* rot_vel) {
+  if (!w || w->dw.n <= 0) return XDEM_ERR_ARGUMENT;
+  const int n = w->dw.n;
+  cudaStream_t s = w->stream;
+  if (x) CK(w, cudaMemcpy2DAsync(x, sizeof(double), &w->dw.pos[0].x, sizeof(double2), sizeof(double), n,
+                                 cudaMemcpyDeviceToHost, s));
+  if (y) CK(w, cudaMemcpy2DAsync(y, sizeof(double), &w->dw.pos[0].y, sizeof(double2), sizeof(double), n,
+                                 cudaMemcpyDeviceToHost, s));
+  if (vx) CK(w, cudaMemcpy2DAsync(vx, sizeof(double), &w->dw.vel[0].x, sizeof(double2), sizeof(double), n,
+                                  cudaMemcpyDeviceToHost, s));
+  if (vy) CK(w, cudaMemcpy2DAsync(vy, sizeof(double), &w->dw.vel[0].y, sizeof(double2), sizeof(double), n,
+                                  cudaMemcpyDeviceToHost, s));
+  if (rot) CK(w, download(rot, w->dw.rot, n, s));
+  if (rot_vel) CK(w, download(rot_vel, w->dw.w, n, s));
+  CK(w, cudaStreamSynchronize(s));
+  return XDEM_OK;
+}
+
+int32_t xdem_set_profiling(xdem_world w, int32_t enable) {
+  if (!w) return XDEM_ERR_ARGUMENT;
+  CK(w, cudaStreamSynchronize(w->stream));
+  w->prof_on = enable != 0;
+  w->prof_used = 0;
+  return XDEM_OK;
+}
+
+int32_t xdem_profile_kinds(void) { return KK_COUNT; }
+
+const char* xdem_profile_name(int32_t kind) {
+  return (kind >= 0 && kind < KK_COUNT) ? kKindNames[kind] : "unknown";
+}
+
+int32_t xdem_get_profile(xdem_world w, int32_t nkinds, int64_t* launches, double* total_ms) {
+  if (!w || nkinds < 0 || !launches || !total_ms) return XDEM_ERR_ARGUMENT;
+  CK(w, cudaStreamSynchronize(w->stream));
+  for (int k = 0; k < nkinds; ++k) {
+    launches[k] = 0;
+    total_ms[k] = 0.0;
+  }
+  for (size_t i = 0; i < w->prof_used; ++i) {
+    float ms = 0.f;
+    CK(w, cudaEventElapsedTime(&ms, w->prof_events[2 * i], w->prof_events[2 * i + 1]));
+    int k = w->prof_kind[i];
+    if (k < nkinds) {
+      launches[k] += 1;
+      total_ms[k] += ms;
+    }
+  }
+  return XDEM_OK;
+}
+
+int32_t xdem_launch_count(xdem_world w, int64_t* out) {
+  if (!w || !out) return XDEM_ERR_ARGUMENT;
+  *out = w->launches;
+  return XDEM_OK;
+}
+
+int32_t xdem_timer_start(xdem_world w) {
+  if (!w) return XDEM_ERR_ARGUMENT;
+  if (!w->timer[0]) {
+    CK(w, cudaEventCreate(&w->timer[0]));
+    CK(w, cudaEventCreate(&w->timer[1]));
+  }
+  CK(w, cudaEventRecord(w->timer[0], w->stream));
+  return XDEM_OK;
+}
+
+int32_t xdem_timer_stop(xdem_world w, double* ms) {
+  if (!w || !ms || !w->timer[0]) return XDEM_ERR_ARGUMENT;
+  CK(w, cudaEventRecord(w->timer[1], w->stream));
+  CK(w, cudaEventSynchronize(w->timer[1]));
+  float f = 0.f;
+  CK(w, cudaEventElapsedTime(&f, w->timer[0], w->timer[1]));
+  *ms = f;
+  return XDEM_OK;
+}
+
+void* xdem_host_alloc(int64_t bytes) {
+  void* p = nullptr;
+  if (bytes <= 0 || cudaHostAlloc(&p, (size_t)bytes, cudaHostAllocDefault) != cudaSuccess)
+    return nullptr;
+  return p;
+}
+
+void xdem_host_free(void* p) {
+  if (p) cudaFreeHost(p);
 }
 
 int32_t xdem_synchronize(xdem_world w) {

@@ -91,7 +91,7 @@ def scale_to_fraction(p, box, volume_sum, phi):
     return box * s
 
 
-def disc_system(n, radii=(0.5, 0.7), phi_rsa=0.5, phi=0.70, seed=0, vel_sigma=0.01,
+def disc_system(n, radii=(0.5, 0.7), phi_rsa=0.45, phi=0.70, seed=0, vel_sigma=0.01,
                 density=1.0):
     """Bidisperse discs, 50:50 (config: 1,024 discs, r 0.5/0.7, phi 0.70)."""
     rng = np.random.default_rng(seed)

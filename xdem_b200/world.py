@@ -306,6 +306,35 @@ class World(WorldBase):
     def synchronize(self):
         return self.lib.xdem_synchronize(self.h)
 
+    # ---- per-step state exchange and timing ---------------------------------
+    def upload_state(self, x, y, vx, vy, rot, rot_vel):
+        d = C.POINTER(C.c_double)
+        return self._check(self.lib.xdem_upload_state(
+            self.h, *[C.cast(a, d) if isinstance(a, int) else a.ctypes.data_as(d)
+                      for a in (x, y, vx, vy, rot, rot_vel)]), "upload_state")
+
+    def download_state(self, x, y, vx, vy, rot, rot_vel):
+        d = C.POINTER(C.c_double)
+        return self._check(self.lib.xdem_download_state(
+            self.h, *[C.cast(a, d) if isinstance(a, int) else a.ctypes.data_as(d)
+                      for a in (x, y, vx, vy, rot, rot_vel)]), "download_state")
+
+    def set_profiling(self, on):
+        self._check(self.lib.xdem_set_profiling(self.h, 1 if on else 0), "set_profiling")
+
+    def profile(self):
+        k = self.lib.xdem_profile_kinds()
+        launches = (C.c_int64 * k)()
+        ms = (C.c_double * k)()
+        self._check(self.lib.xdem_get_profile(self.h, k, launches, ms), "get_profile")
+        return {self.lib.xdem_profile_name(i).decode(): (int(launches[i]), float(ms[i]))
+                for i in range(k) if launches[i]}
+
+    def launch_count(self):
+        v = C.c_int64(0)
+        self._check(self.lib.xdem_launch_count(self.h, C.byref(v)), "launch_count")
+        return int(v.value)
+
 
 def pair_geometry(pi, pj, off, method=abi.ELLIPSE_CLOSEST_APPROACH, precision=abi.PRECISION_FP64):
     """Contact geometry of npairs pairs on the GPU (rows as xdem_pair_geometry)."""
