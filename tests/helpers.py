@@ -54,8 +54,12 @@ def clump_case(nfree=120, nclump=30, seed=11, phi=0.55):
     bound = np.array([b[1] if b[0] == "disc" else float(np.max(np.hypot(b[1][1][:, 0], b[1][1][:, 1]) + b[1][0]))
                       for b in bodies])
     area = float(np.sum(np.pi * bound ** 2))
-    box = inputs.box_for(area, phi)
+    box = inputs.box_for(area, 0.42)
     bx, by = inputs.rsa_positions(bound, box, seed + 7)
+    # bring the body centres closer (bounding-disc fraction 0.42 -> phi); the
+    # clump shapes are built afterwards, so they keep their size
+    s = np.sqrt(0.42 / phi)
+    bx, by, box = bx * s, by * s, box * s
     rows = []
     for (kind, data), cx, cy in zip(bodies, bx, by):
         if kind == "disc":
@@ -138,8 +142,23 @@ def same_pairs(ca, cb):
 
 
 def rel_err(a, b, floor=1e-300):
-    scale = max(np.max(np.abs(a)) if len(a) else 0.0, np.max(np.abs(b)) if len(b) else 0.0, floor)
-    return float(np.max(np.abs(a - b)) / scale) if len(a) else 0.0
+    """Largest |a-b| relative to the largest finite magnitude; NaN must sit at
+    the same places in both (the reference itself yields NaN fields for some
+    degenerate ellipse pairs), inf likewise."""
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    if len(a) == 0:
+        return 0.0
+    if not np.array_equal(np.isnan(a), np.isnan(b)):
+        return float("inf")
+    fin = np.isfinite(a) & np.isfinite(b)
+    if not np.array_equal(a[~fin & ~np.isnan(a)], b[~fin & ~np.isnan(b)]):
+        return float("inf")
+    if not fin.any():
+        return 0.0
+    a, b = a[fin], b[fin]
+    scale = max(np.max(np.abs(a)), np.max(np.abs(b)), floor)
+    return float(np.max(np.abs(a - b)) / scale)
 
 
 def compare_contacts(ca, cb, tol, keys=CONTACT_KEYS):

@@ -98,15 +98,18 @@ def test_pair_geometry_circles():
     r2 = rng.choice([0.5, 0.7], N)
     ang = rng.uniform(0, 2 * np.pi, N)
     dist = rng.uniform(0.8, 1.02, N) * (r1 + r2)
-    dist[:10] = (r1 + r2)[:10]  # exact touching: overlap 0 counts as contact
     pi = np.stack([np.zeros(N), r1, np.ones(N), np.zeros(N), np.zeros(N), rng.normal(0, .1, N),
                    rng.normal(0, .1, N), np.zeros(N), rng.normal(0, .1, N)], 1)
     pj = np.stack([np.zeros(N), r2, np.ones(N), dist * np.cos(ang), dist * np.sin(ang),
                    rng.normal(0, .1, N), rng.normal(0, .1, N), np.zeros(N), rng.normal(0, .1, N)], 1)
+    # exactly touching (exactly representable): overlap 0 counts as contact
+    pi[:10, 1], pj[:10, 1] = 0.5, 0.25
+    pj[:10, 3], pj[:10, 4] = 0.75, 0.0
     off = np.zeros((N, 4))
     og, _ = pair_geometry(pi, pj, off)
     oc, _ = oracle.pair_geometry(pi, pj, off, 0, "port")
     np.testing.assert_array_equal(og[:, :16], oc[:, :16])  # + - * / sqrt only: bit-exact
+    assert og[:10, 0].all()
 
 
 def test_newton_cap_raises_status():

@@ -40,7 +40,17 @@ def particle_properties(shape, radius, aspect, density=1.0):
     return out
 
 
-def rsa_positions(bound_radius, box, seed, max_attempts=100000):
+def rsa_positions(bound_radius, box, seed, max_attempts=100000, largest_first=True):
+    """RSA of discs; with largest_first the discs are added in decreasing size
+    (the usual order for polydisperse RSA), positions returned in input order."""
+    if largest_first:
+        order = np.argsort(-np.asarray(bound_radius), kind="stable")
+        xs, ys = rsa_positions(np.asarray(bound_radius)[order], box, seed, max_attempts, False)
+        x = np.empty_like(xs)
+        y = np.empty_like(ys)
+        x[order] = xs
+        y[order] = ys
+        return x, y
     lib = abi.load_library()
     n = len(bound_radius)
     r = np.ascontiguousarray(bound_radius, np.float64)
