@@ -161,6 +161,44 @@ def rel_err(a, b, floor=1e-300):
     return float(np.max(np.abs(a - b)) / scale)
 
 
+def compare_pair_geometry(og, oc, pi, pj, off, method, tol=1e-10):
+    """GPU pair geometry `og` against the checker's `oc` (rows as
+    xdem_pair_geometry).  Conditioning: the orientations are perturbed by one
+    ulp (the size of the cos/sin differences between CUDA and glibc) and the
+    checker's own outputs move by `spread`; the GPU may differ by a few times
+    that, and by at most `tol` of the field's scale on the well-conditioned
+    pairs (all but the near-tangent ones of the intersection quartic, whose
+    near-double root turns an ulp into ~sqrt(ulp))."""
+    import oracle
+    hit = oc[:, 0] == 1
+    spread = np.zeros_like(oc)
+    for sgn in (-1.0, 1.0):
+        qi, qj = pi.copy(), pj.copy()
+        qi[:, 7] = np.nextafter(pi[:, 7], sgn * np.inf)
+        qj[:, 7] = np.nextafter(pj[:, 7], -sgn * np.inf)
+        op, _ = oracle.pair_geometry(qi, qj, off, method, "port")
+        both = (op[:, 0] == 1) & hit
+        d = np.where(both[:, None], np.abs(np.nan_to_num(op - oc)), 0.0)
+        spread = np.maximum(spread, d)
+    for col in range(1, 16):
+        a, b = og[hit, col], oc[hit, col]
+        assert np.array_equal(np.isnan(a), np.isnan(b)), col
+        fin = np.isfinite(a)
+        if not fin.any():
+            continue
+        scale = np.max(np.abs(b[fin]))
+        err = np.abs(a[fin] - b[fin])
+        allowed = tol * scale + 8.0 * spread[hit, col][fin]
+        assert np.all(err <= allowed), (col, float(np.max(err / allowed)))
+    # pairs whose outputs move by at most 1e-12 of scale under a 1-ulp
+    # perturbation (condition number below ~5e3) must also meet `tol` alone
+    well = hit & (spread[:, 9] <= 1e-12 * np.max(oc[hit, 9]))
+    assert well.sum() >= 0.75 * hit.sum(), (well.sum(), hit.sum())
+    for col in range(1, 16):
+        assert rel_err(og[well, col], oc[well, col]) <= tol, col
+    return int(hit.sum() - well.sum())
+
+
 def compare_contacts(ca, cb, tol, keys=CONTACT_KEYS):
     assert same_pairs(ca, cb), (len(ca["id_i"]), len(cb["id_i"]))
     worst = {k: rel_err(ca[k], cb[k]) for k in keys}

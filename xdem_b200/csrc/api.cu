@@ -11,6 +11,7 @@
 
 #include "../../include/xdem_gpu.h"
 #include "kernels.cuh"
+#include "resort.cuh"
 
 using namespace xdem;
 
@@ -18,6 +19,9 @@ namespace {
 
 constexpr int kBlock = 128;
 constexpr int kDefaultSlots = 16;
+// steps between memory-order refreshes; odd, so that a captured chunk (one
+// re-sort + kResortEvery steps) swaps the slot sets an even number of times
+constexpr int kResortEvery = 31;
 constexpr double kPi = 3.14159265358979323846;
 
 inline int blocks_for(int n, int b) { return (n + b - 1) / b; }
@@ -62,6 +66,8 @@ struct xdem_world_s {
   size_t prof_used = 0;                  // pairs recorded
   int64_t launches = 0;
   cudaEvent_t timer[2] = {nullptr, nullptr};
+  int since_resort = kResortEvery;  // steps since the memory order was refreshed
+  PermList perm{};                  // particle arrays moved by a re-sort
 };
 
 namespace {
@@ -107,12 +113,13 @@ cudaError_t download(T* dst, const T* src, size_t count, cudaStream_t s) {
 // ---- per-kernel timing ------------------------------------------------------
 enum KernelKind {
   KK_MODIFY = 0, KK_BIN, KK_SCAN, KK_SCATTER, KK_UPDATE, KK_COLLECT, KK_INTEGRATE, KK_RATTLERS,
-  KK_STRESS_PARTIAL, KK_STRESS_FINAL, KK_END_OF_STEP, KK_SCALE, KK_BACKGROUND, KK_KE, KK_COUNT
+  KK_STRESS_PARTIAL, KK_STRESS_FINAL, KK_END_OF_STEP, KK_SCALE, KK_BACKGROUND, KK_KE, KK_RESORT,
+  KK_STAGE, KK_COUNT
 };
 const char* const kKindNames[KK_COUNT] = {
     "k_modify_position", "k_bin", "k_scan", "k_scatter", "k_update_contacts", "k_collect",
     "k_integrate", "k_rattlers", "k_stress_partial", "k_stress_final", "k_end_of_step",
-    "k_scale_positions", "k_background_velocity", "k_kinetic_energy"};
+    "k_scale_positions", "k_background_velocity", "k_kinetic_energy", "k_resort", "k_stage"};
 
 void prof_begin(xdem_world_s* w, int kind) {
   if (!w->prof_on) return;
@@ -154,8 +161,11 @@ void launch_modify(xdem_world_s* w) {
 void launch_find(xdem_world_s* w) {
   int n = w->dw.n;
   LAUNCH(w, KK_BIN, k_bin<<<blocks_for(n, kBlock), kBlock, 0, w->stream>>>(w->dw));
-  LAUNCH(w, KK_SCAN, k_scan<<<1, 1024, 0, w->stream>>>(w->dw));
   int cells = w->nx_cap * w->ny_cap + 2 * w->nx_cap;
+  int tiles = std::min(blocks_for(cells, kScanTile), 2 * 148 * 8);
+  LAUNCH(w, KK_SCAN, k_scan_tiles<<<tiles, kScanThreads, 0, w->stream>>>(w->dw));
+  LAUNCH(w, KK_SCAN, k_scan_sums<<<1, kScanThreads, 0, w->stream>>>(w->dw));
+  LAUNCH(w, KK_SCAN, k_scan_apply<<<tiles, kScanThreads, 0, w->stream>>>(w->dw));
   int nb = std::max(blocks_for(n, kBlock), std::min(blocks_for(cells, kBlock), 1184));
   LAUNCH(w, KK_SCATTER, k_scatter<<<nb, kBlock, 0, w->stream>>>(w->dw));
 }
@@ -196,28 +206,73 @@ void launch_rattlers(xdem_world_s* w, int reset, double scale) {
 }
 
 void launch_end_of_step(xdem_world_s* w, int law, double p0, double p1, int le_update, int stop_on,
-                        double stop_p) {
-  LAUNCH(w, KK_END_OF_STEP,
-         k_end_of_step<<<1, 1, 0, w->stream>>>(w->dw, law, p0, p1, le_update, stop_on, stop_p));
+                        double stop_p, int count_step) {
+  LAUNCH(w, KK_END_OF_STEP, k_end_of_step<<<1, 1, 0, w->stream>>>(w->dw, law, p0, p1, le_update,
+                                                                 stop_on, stop_p, count_step));
   if (law != BOX_NONE)
     LAUNCH(w, KK_SCALE, k_scale_positions<<<blocks_for(w->dw.n, kBlock), kBlock, 0, w->stream>>>(w->dw));
 }
 
-// one step of a control sequence; record: store the full contact record
-void enqueue_step(xdem_world_s* w, const xdem_control* ctl, int record) {
+// refresh of the memory order (resort.cuh), after a step's binning
+void launch_resort(xdem_world_s* w) {
+  int n = w->dw.n;
+  int cells = w->nx_cap * w->ny_cap;
+  int cb = std::min(blocks_for(cells, kBlock), 148 * 16);
+  LAUNCH(w, KK_RESORT, k_sort_cells<<<cb, kBlock, 0, w->stream>>>(w->dw));
+  LAUNCH(w, KK_RESORT, k_permute<<<blocks_for(n, kBlock), kBlock, 0, w->stream>>>(w->dw, w->perm));
+  LAUNCH(w, KK_RESORT, k_copy_back<<<blocks_for(n, kBlock), kBlock, 0, w->stream>>>(w->dw, w->perm));
+  LAUNCH(w, KK_RESORT,
+         k_permute_history<<<blocks_for(n, kBlock), kBlock, 0, w->stream>>>(w->dw, w->par));
+  w->par ^= 1;
+  LAUNCH(w, KK_RESORT, k_remap_cells<<<std::min(blocks_for(2 * n, kBlock), 148 * 16), kBlock, 0,
+                                       w->stream>>>(w->dw));
+}
+
+// one step of a control sequence; record: store the full contact record;
+// resort: refresh the memory order after the binning
+void enqueue_step(xdem_world_s* w, const xdem_control* ctl, int record, bool resort = false) {
   int kind = w->prm.world_kind;
   bool own = ctl->sequence == XDEM_SEQ_TAKE_TIME_STEP;
   bool le = own && kind == XDEM_WORLD_LEES_EDWARDS;
   if (ctl->scale_rattlers) launch_rattlers(w, 0, ctl->rattler_scale);
   launch_modify(w);
   launch_find(w);
+  if (resort) launch_resort(w);
   launch_update(w, le, record);
   launch_collect(w);
   launch_integrate(w, le, own && kind == XDEM_WORLD_PERIODIC_CONTROL);
   if (ctl->reset_rattlers) launch_rattlers(w, 1, 0.0);
   if (ctl->update_stress) launch_stress(w);
   launch_end_of_step(w, ctl->box_law, ctl->p0, ctl->p1, le ? 1 : 0, ctl->stop_on_pressure,
-                     ctl->stop_pressure);
+                     ctl->stop_pressure, 1);
+}
+
+// a step with the re-sort policy: the memory order is refreshed every
+// kResortEvery steps
+void policy_step(xdem_world_s* w, const xdem_control* ctl, int record) {
+  bool resort = w->since_resort >= kResortEvery;
+  if (resort) w->since_resort = 0;
+  enqueue_step(w, ctl, record, resort);
+  w->since_resort++;
+}
+
+// host arrays in id order from device arrays in memory order
+template <class T>
+cudaError_t download_by_id(xdem_world_s* w, T* dst, const T* src, const std::vector<int32_t>& id_of) {
+  const int n = w->dw.n;
+  std::vector<T> tmp(n);
+  cudaError_t e = download(tmp.data(), src, n, w->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(w->stream);
+  if (e != cudaSuccess) return e;
+  for (int m = 0; m < n; ++m) dst[id_of[m]] = tmp[m];
+  return cudaSuccess;
+}
+
+cudaError_t fetch_id_of(xdem_world_s* w, std::vector<int32_t>& id_of) {
+  id_of.resize(w->dw.n);
+  cudaError_t e = download(id_of.data(), w->dw.id_of, w->dw.n, w->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(w->stream);
+  return e;
 }
 
 uint32_t fetch_status(xdem_world_s* w) {
@@ -442,6 +497,7 @@ int32_t xdem_set_particles(xdem_world w, const xdem_particles* P) {
   size_t cells = (size_t)w->nx_cap * w->ny_cap + 2 * (size_t)w->nx_cap;
   CK(w, B.alloc(&d.cell_count, cells + 1));
   CK(w, B.alloc(&d.cell_start, cells + 1));
+  CK(w, B.alloc(&d.tile_sum, cells / kScanTile + 2));
   CK(w, B.alloc(&d.cell_mem, 2 * (size_t)n));
   CK(w, B.alloc(&d.pcell, n));
   CK(w, B.alloc(&d.prank, n));
@@ -472,7 +528,54 @@ int32_t xdem_set_particles(xdem_world w, const xdem_particles* P) {
   CK(w, cudaMemsetAsync(d.incnt, 0, sizeof(int32_t) * n, s));
   w->partial_blocks = blocks_for(n, kReduceBlock);
   CK(w, B.alloc(&d.partials, 4 * (size_t)w->partial_blocks + 4));
+  // memory order starts as id order
+  std::vector<int32_t> ident(n);
+  for (int i = 0; i < n; ++i) ident[i] = i;
+  CK(w, B.alloc(&d.id_of, n));
+  CK(w, B.alloc(&d.mpos, n));
+  CK(w, B.alloc(&d.newpos, n));
+  CK(w, B.alloc(&d.stage, 6 * (size_t)n));
+  CK(w, upload(d.id_of, ident.data(), n, s));
+  CK(w, upload(d.mpos, ident.data(), n, s));
+  // arrays moved by a re-sort, each with a slab of the scratch buffer
+  PermList& L = w->perm;
+  L = PermList{};
+  auto add = [&](void* p, int esize) {
+    L.base[L.count] = p;
+    L.esize[L.count] = esize;
+    L.count++;
+  };
+  add(d.id_of, 4);
+  add(shape, 4);
+  add(up, 4);
+  add(setting, 4);
+  add(num_sub, 4);
+  add(d.rattler, 4);
+  add(d.ncp, 4);
+  add(orad, 8);
+  add(rad, 8);
+  add(asp, 8);
+  add(mass, 8);
+  add(im, 8);
+  add(I, 8);
+  add(iI, 8);
+  add(vol, 8);
+  add(d.rot, 8);
+  add(d.w, 8);
+  add(d.torque, 8);
+  add(d.pos, 16);
+  add(d.vel, 16);
+  add(d.branch, 16);
+  add(d.force, 16);
+  size_t off = 0;
+  for (int a = 0; a < L.count; ++a) {
+    L.offset[a] = off;
+    off += (size_t)L.esize[a] * n;
+    off = (off + 255) & ~(size_t)255;
+  }
+  CK(w, B.alloc(&d.scratch, off));
   w->par = 0;
+  w->since_resort = kResortEvery;
   CK(w, cudaStreamSynchronize(s));
   return XDEM_OK;
 }
@@ -481,20 +584,20 @@ int32_t xdem_get_particles(xdem_world w, xdem_particles* P) {
   if (!w || !P || w->dw.n <= 0) return XDEM_ERR_ARGUMENT;
   const int n = w->dw.n;
   const DevWorld& d = w->dw;
-  cudaStream_t s = w->stream;
+  std::vector<int32_t> id_of;
+  CK(w, fetch_id_of(w, id_of));
   std::vector<double2> pos(n), vel(n), br(n);
-  CK(w, download(pos.data(), d.pos, n, s));
-  CK(w, download(vel.data(), d.vel, n, s));
-  CK(w, download(br.data(), d.branch, n, s));
-  if (P->rot) CK(w, download(P->rot, d.rot, n, s));
-  if (P->rot_vel) CK(w, download(P->rot_vel, d.w, n, s));
-  if (P->is_rattler) CK(w, download(P->is_rattler, d.rattler, n, s));
-  if (P->mass) CK(w, download(P->mass, d.mass, n, s));
-  if (P->inertia) CK(w, download(P->inertia, d.I, n, s));
-  if (P->shape) CK(w, download(P->shape, d.shape, n, s));
-  if (P->setting) CK(w, download(P->setting, d.setting, n, s));
-  if (P->up_level) CK(w, download(P->up_level, d.up, n, s));
-  CK(w, cudaStreamSynchronize(s));
+  CK(w, download_by_id(w, pos.data(), d.pos, id_of));
+  CK(w, download_by_id(w, vel.data(), d.vel, id_of));
+  CK(w, download_by_id(w, br.data(), d.branch, id_of));
+  if (P->rot) CK(w, download_by_id(w, P->rot, d.rot, id_of));
+  if (P->rot_vel) CK(w, download_by_id(w, P->rot_vel, d.w, id_of));
+  if (P->is_rattler) CK(w, download_by_id(w, P->is_rattler, d.rattler, id_of));
+  if (P->mass) CK(w, download_by_id(w, P->mass, (const double*)d.mass, id_of));
+  if (P->inertia) CK(w, download_by_id(w, P->inertia, (const double*)d.I, id_of));
+  if (P->shape) CK(w, download_by_id(w, P->shape, (const int32_t*)d.shape, id_of));
+  if (P->setting) CK(w, download_by_id(w, P->setting, (const int32_t*)d.setting, id_of));
+  if (P->up_level) CK(w, download_by_id(w, P->up_level, (const int32_t*)d.up, id_of));
   P->n = n;
   for (int i = 0; i < n; ++i) {
     if (P->x) P->x[i] = pos[i].x;
@@ -511,6 +614,9 @@ int32_t xdem_set_contacts(xdem_world w, const xdem_contacts* C) {
   if (!w || !C || w->dw.n <= 0 || C->count < 0) return XDEM_ERR_ARGUMENT;
   const int n = w->dw.n, K = w->dw.K;
   const size_t ks = (size_t)K * n;
+  std::vector<int32_t> mpos(n);
+  CK(w, download(mpos.data(), w->dw.mpos, n, w->stream));
+  CK(w, cudaStreamSynchronize(w->stream));
   std::vector<int32_t> cnt(n, 0), partner(ks, 0);
   std::vector<double2> nn(ks), sh(ks), f(ks), b(ks), cp(ks), bv1(ks), bv2(ks), fn(ks), ft(ks);
   std::vector<double> damp(ks), t1(ks), t2(ks);
@@ -518,13 +624,14 @@ int32_t xdem_set_contacts(xdem_world w, const xdem_contacts* C) {
   for (int64_t k = 0; k < C->count; ++k) {
     int i = C->id_i[k], j = C->id_j[k];
     if (i < 0 || i >= n || j < 0 || j >= n || i >= j) return XDEM_ERR_ARGUMENT;
-    int s = cnt[i];
+    int m = mpos[i];
+    int s = cnt[m];
     if (s >= K) {
       st |= XDEM_ERR_CAPACITY;
       continue;
     }
-    cnt[i]++;
-    size_t ci = (size_t)s * n + i;
+    cnt[m]++;
+    size_t ci = (size_t)s * n + m;
     partner[ci] = j;
     nn[ci] = make_double2(C->normal_x[k], C->normal_y[k]);
     sh[ci] = make_double2(C->shear_x[k], C->shear_y[k]);
@@ -541,16 +648,16 @@ int32_t xdem_set_contacts(xdem_world w, const xdem_contacts* C) {
     fn[ci] = Fn;
     ft[ci] = Ft;
   }
-  // incoming references, ascending owner, so a collect without an update
-  // sums these contacts as the reference would
+  // incoming references, so that a collect without an update sums these
+  // contacts as the reference would
   std::vector<int32_t> inc(n, 0);
   std::vector<uint32_t> inref(ks, 0);
-  for (int i = 0; i < n; ++i)
-    for (int s = 0; s < cnt[i]; ++s) {
-      int j = partner[(size_t)s * n + i];
-      if (inc[j] < K) inref[(size_t)inc[j] * n + j] = (uint32_t)i * K + s;
+  for (int m = 0; m < n; ++m)
+    for (int s = 0; s < cnt[m]; ++s) {
+      int mj = mpos[partner[(size_t)s * n + m]];
+      if (inc[mj] < K) inref[(size_t)inc[mj] * n + mj] = (uint32_t)m * K + s;
       else st |= XDEM_ERR_CAPACITY;
-      inc[j]++;
+      inc[mj]++;
     }
   const Slots& S = w->dw.slots[w->par];
   cudaStream_t q = w->stream;
@@ -581,12 +688,14 @@ int32_t xdem_get_contacts(xdem_world w, xdem_contacts* C) {
   const size_t ks = (size_t)K * n;
   const Slots& S = w->dw.slots[w->par];
   cudaStream_t q = w->stream;
-  std::vector<int32_t> cnt(n), partner(ks);
+  std::vector<int32_t> cnt(n), partner(ks), id_of(n), mpos(n);
   CK(w, download(cnt.data(), S.count, n, q));
   CK(w, download(partner.data(), S.partner, ks, q));
+  CK(w, download(id_of.data(), w->dw.id_of, n, q));
+  CK(w, download(mpos.data(), w->dw.mpos, n, q));
   CK(w, cudaStreamSynchronize(q));
   int64_t total = 0;
-  for (int i = 0; i < n; ++i) total += std::min(cnt[i], K);
+  for (int m = 0; m < n; ++m) total += std::min(cnt[m], K);
   C->count = total;
   if (C->capacity < total) return XDEM_ERR_CAPACITY;
   std::vector<double2> nn(ks), sh(ks), b(ks), cp(ks), bv1(ks), bv2(ks), fn(ks), ft(ks);
@@ -605,13 +714,14 @@ int32_t xdem_get_contacts(xdem_world w, xdem_contacts* C) {
   CK(w, cudaStreamSynchronize(q));
   int64_t k = 0;
   std::vector<std::pair<int32_t, int32_t>> order;
-  for (int i = 0; i < n; ++i) {
-    int m = std::min(cnt[i], K);
+  for (int i = 0; i < n; ++i) {  // owners in id order
+    const int m = mpos[i];
+    const int c = std::min(cnt[m], K);
     order.clear();
-    for (int s = 0; s < m; ++s) order.push_back({partner[(size_t)s * n + i], s});
+    for (int s = 0; s < c; ++s) order.push_back({partner[(size_t)s * n + m], s});
     std::sort(order.begin(), order.end());
     for (auto& o : order) {
-      size_t ci = (size_t)o.second * n + i;
+      size_t ci = (size_t)o.second * n + m;
       C->id_i[k] = i;
       C->id_j[k] = o.first;
       C->normal_x[k] = nn[ci].x;
@@ -636,17 +746,19 @@ int32_t xdem_get_contacts(xdem_world w, xdem_contacts* C) {
       ++k;
     }
   }
+  (void)id_of;
   return XDEM_OK;
 }
 
 int32_t xdem_get_force_and_torque(xdem_world w, double* fx, double* fy, double* t, int32_t* nc) {
   if (!w || w->dw.n <= 0) return XDEM_ERR_ARGUMENT;
   const int n = w->dw.n;
+  std::vector<int32_t> id_of;
+  CK(w, fetch_id_of(w, id_of));
   std::vector<double2> f(n);
-  CK(w, download(f.data(), w->dw.force, n, w->stream));
-  if (t) CK(w, download(t, w->dw.torque, n, w->stream));
-  if (nc) CK(w, download(nc, w->dw.ncp, n, w->stream));
-  CK(w, cudaStreamSynchronize(w->stream));
+  CK(w, download_by_id(w, f.data(), w->dw.force, id_of));
+  if (t) CK(w, download_by_id(w, t, w->dw.torque, id_of));
+  if (nc) CK(w, download_by_id(w, nc, w->dw.ncp, id_of));
   for (int i = 0; i < n; ++i) {
     if (fx) fx[i] = f[i].x;
     if (fy) fy[i] = f[i].y;
@@ -872,13 +984,13 @@ int32_t xdem_update_total_stress(xdem_world w, double stress[4]) {
 int32_t xdem_update_boundary(xdem_world w, int32_t law, double p0, double p1) {
   SUBSTEP_BEGIN;
   if (law < 0 || law > 4) return XDEM_ERR_ARGUMENT;
-  launch_end_of_step(w, law, p0, p1, 0, 0, 0.0);
+  launch_end_of_step(w, law, p0, p1, 0, 0, 0.0, 0);
   SUBSTEP_END;
 }
 
 int32_t xdem_update_lees_edwards_boundary(xdem_world w) {
   SUBSTEP_BEGIN;
-  launch_end_of_step(w, BOX_NONE, 0.0, 0.0, 1, 0, 0.0);
+  launch_end_of_step(w, BOX_NONE, 0.0, 0.0, 1, 0, 0.0, 0);
   SUBSTEP_END;
 }
 
@@ -908,7 +1020,7 @@ int32_t xdem_take_time_step(xdem_world w) {
   SUBSTEP_BEGIN;
   xdem_control ctl{};
   ctl.sequence = XDEM_SEQ_TAKE_TIME_STEP;
-  enqueue_step(w, &ctl, 1);
+  policy_step(w, &ctl, 1);
   SUBSTEP_END;
 }
 
@@ -923,44 +1035,57 @@ int32_t xdem_run(xdem_world w, int32_t nsteps, const xdem_control* ctl, int32_t*
   CK(w, read_scalars(w, &s));
   s.stop = 0;
   s.steps_done = 0;
+  s.flips = 0;
   CK(w, write_scalars(w, &s));
   const int start_par = w->par;
   // every step but the last skips the recorded contact fields unless the run
   // may stop early
   const int rec_all = ctl->stop_on_pressure ? 1 : 0;
   int body = nsteps - 1;
-  const int kGraphSteps = 2;
-  if (body >= 8 && !w->prof_on) {
-    // capture two steps (one per slot-set parity) and replay the graph
+  // direct steps until a re-sort is due, then whole chunks (one re-sort and
+  // kResortEvery steps) captured once in a CUDA graph and replayed
+  while (body > 0 && w->since_resort < kResortEvery) {
+    policy_step(w, ctl, rec_all);
+    --body;
+  }
+  if (body >= kResortEvery && !w->prof_on) {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
-    int64_t launches_before = w->launches;
+    const int par0 = w->par;
+    const int64_t launches_before = w->launches;
     CK(w, cudaStreamBeginCapture(w->stream, cudaStreamCaptureModeThreadLocal));
-    for (int k = 0; k < kGraphSteps; ++k) enqueue_step(w, ctl, rec_all);
+    for (int k = 0; k < kResortEvery; ++k) policy_step(w, ctl, rec_all);
     cudaError_t e = cudaStreamEndCapture(w->stream, &graph);
     if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
     if (e != cudaSuccess) {
       if (graph) cudaGraphDestroy(graph);
       return (int32_t)(cuda_check(w, e) | fetch_status(w));
     }
-    w->par = start_par;  // capture toggled the parity kGraphSteps times
-    int reps = body / kGraphSteps;
-    int64_t per_graph = w->launches - launches_before;
-    w->launches += per_graph * (reps - 1);
+    // a chunk swaps the slot sets an even number of times: parity unchanged
+    w->par = par0;
+    const int reps = body / kResortEvery;
+    const int64_t per_chunk = w->launches - launches_before;
+    w->launches += per_chunk * (reps - 1);
     for (int r = 0; r < reps && e == cudaSuccess; ++r) e = cudaGraphLaunch(exec, w->stream);
-    body -= reps * kGraphSteps;
+    body -= reps * kResortEvery;
     cudaGraphExecDestroy(exec);
     cudaGraphDestroy(graph);
     CK(w, e);
   }
-  for (int k = 0; k < body; ++k) enqueue_step(w, ctl, rec_all);
-  enqueue_step(w, ctl, 1);
+  for (; body > 0; --body) policy_step(w, ctl, rec_all);
+  policy_step(w, ctl, 1);
   CK(w, cudaGetLastError());
   uint32_t st = fetch_status(w);
   CK(w, read_scalars(w, &s));
   if (steps_done) *steps_done = s.steps_done;
-  w->par = start_par ^ (s.steps_done & 1);
+  // slot-set swaps that actually ran (none after a stop)
+  w->par = start_par ^ (s.flips & 1);
   return (int32_t)st;
+}
+
+int32_t xdem_synchronize(xdem_world w) {
+  if (!w) return XDEM_ERR_ARGUMENT;
+  return (int32_t)fetch_status(w);
 }
 
 int32_t xdem_upload_state(xdem_world w, const double* x, const double* y, const double* vx,
@@ -968,18 +1093,11 @@ int32_t xdem_upload_state(xdem_world w, const double* x, const double* y, const 
   if (!w || w->dw.n <= 0 || !x || !y || !vx || !vy || !rot || !rot_vel) return XDEM_ERR_ARGUMENT;
   const int n = w->dw.n;
   cudaStream_t s = w->stream;
-  // positions and velocities are interleaved (double2) on the device: copy the
-  // x and y columns into the two lanes with strided 2-D copies
-  CK(w, cudaMemcpy2DAsync(&w->dw.pos[0].x, sizeof(double2), x, sizeof(double), sizeof(double), n,
-                          cudaMemcpyHostToDevice, s));
-  CK(w, cudaMemcpy2DAsync(&w->dw.pos[0].y, sizeof(double2), y, sizeof(double), sizeof(double), n,
-                          cudaMemcpyHostToDevice, s));
-  CK(w, cudaMemcpy2DAsync(&w->dw.vel[0].x, sizeof(double2), vx, sizeof(double), sizeof(double), n,
-                          cudaMemcpyHostToDevice, s));
-  CK(w, cudaMemcpy2DAsync(&w->dw.vel[0].y, sizeof(double2), vy, sizeof(double), sizeof(double), n,
-                          cudaMemcpyHostToDevice, s));
-  CK(w, upload(w->dw.rot, rot, n, s));
-  CK(w, upload(w->dw.w, rot_vel, n, s));
+  double* st = w->dw.stage;
+  const double* src[6] = {x, y, vx, vy, rot, rot_vel};
+  for (int k = 0; k < 6; ++k) CK(w, upload(st + (size_t)k * n, src[k], n, s));
+  LAUNCH(w, KK_STAGE, k_stage<<<blocks_for(n, kBlock), kBlock, 0, s>>>(w->dw, 1));
+  CK(w, cudaGetLastError());
   return XDEM_OK;
 }
 
@@ -988,16 +1106,11 @@ int32_t xdem_download_state(xdem_world w, double* x, double* y, double* vx, doub
   if (!w || w->dw.n <= 0) return XDEM_ERR_ARGUMENT;
   const int n = w->dw.n;
   cudaStream_t s = w->stream;
-  if (x) CK(w, cudaMemcpy2DAsync(x, sizeof(double), &w->dw.pos[0].x, sizeof(double2), sizeof(double), n,
-                                 cudaMemcpyDeviceToHost, s));
-  if (y) CK(w, cudaMemcpy2DAsync(y, sizeof(double), &w->dw.pos[0].y, sizeof(double2), sizeof(double), n,
-                                 cudaMemcpyDeviceToHost, s));
-  if (vx) CK(w, cudaMemcpy2DAsync(vx, sizeof(double), &w->dw.vel[0].x, sizeof(double2), sizeof(double), n,
-                                  cudaMemcpyDeviceToHost, s));
-  if (vy) CK(w, cudaMemcpy2DAsync(vy, sizeof(double), &w->dw.vel[0].y, sizeof(double2), sizeof(double), n,
-                                  cudaMemcpyDeviceToHost, s));
-  if (rot) CK(w, download(rot, w->dw.rot, n, s));
-  if (rot_vel) CK(w, download(rot_vel, w->dw.w, n, s));
+  LAUNCH(w, KK_STAGE, k_stage<<<blocks_for(n, kBlock), kBlock, 0, s>>>(w->dw, 0));
+  const double* st = w->dw.stage;
+  double* dst[6] = {x, y, vx, vy, rot, rot_vel};
+  for (int k = 0; k < 6; ++k)
+    if (dst[k]) CK(w, download(dst[k], st + (size_t)k * n, n, s));
   CK(w, cudaStreamSynchronize(s));
   return XDEM_OK;
 }
@@ -1072,10 +1185,6 @@ void xdem_host_free(void* p) {
   if (p) cudaFreeHost(p);
 }
 
-int32_t xdem_synchronize(xdem_world w) {
-  if (!w) return XDEM_ERR_ARGUMENT;
-  return (int32_t)fetch_status(w);
-}
 
 // ---- single-pair geometry ------------------------------------------------------
 int32_t xdem_pair_geometry(int32_t npairs, int32_t method, int32_t precision, const double* pi,

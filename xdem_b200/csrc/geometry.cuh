@@ -409,8 +409,7 @@ __device__ __forceinline__ bool contact_geometry(int method, const PState& a, co
                                                  double orad_a, double orad_b, vec2<double> off,
                                                  vec2<double> ovel, double2 cs_a, double2 cs_b,
                                                  Geom& g, uint32_t& st) {
-  g.contacted = 0;
-  g.iters = 0;
+  g = Geom{};
   if (a.shape == SHAPE_CLUMP || b.shape == SHAPE_CLUMP) return false;
   if (a.shape == SHAPE_CIRCLE) {
     if (b.shape != SHAPE_CIRCLE) {

@@ -1,13 +1,13 @@
 // kernels.cuh — the per-timestep kernels (FP64 path).
 //
 // Step of a PeriodicBoundaryWorld (PeriodicBoundaryWorld.cpp:119-127):
-//   k_modify_position       wrap into the box                     (a2)
-//   k_bin / k_scan / k_scatter   counting sort of particles by cell (a3)
-//   k_update_contacts       3x3 cell scan, geometry, force, history (a5-a15)
-//   k_collect               deterministic per-particle sums         (a16)
-//   k_integrate             semi-implicit Euler (+ clumps, rattlers)(a17-a19)
-// plus k_stress_* (a21), k_box_law/k_scale_positions (a20) and
-// k_le_boundary (a22).
+//   k_modify_position           wrap into the box                     (a2)
+//   k_bin / k_scan_* / k_scatter  counting sort of particles by cell   (a3, a4)
+//   k_update_contacts           3x3 cell scan, geometry, force, history (a5-a15)
+//   k_collect                   deterministic per-particle sums         (a16)
+//   k_integrate                 semi-implicit Euler, clumps, rattlers (a17-a19)
+// plus k_stress_* (a21), k_end_of_step / k_scale_positions (a20, a22).
+// Every thread works on memory position m (world.cuh); ids come from id_of.
 #pragma once
 #include "geometry.cuh"
 #include "world.cuh"
@@ -54,9 +54,7 @@ __device__ __forceinline__ void raise(uint32_t* status, uint32_t bits) {
 
 // ---------------------------------------------------------------------------
 // a2: modifyParticlePosition (PeriodicBoundaryWorld.cpp:129-142,
-//     LeesEdwardsBoundaryWorld.cpp:304-333), optionally preceded by the
-//     pending affine scale of a box law (scaleAllParticlePosition,
-//     BaseWorld.cpp:119-124).
+//     LeesEdwardsBoundaryWorld.cpp:304-333)
 // ---------------------------------------------------------------------------
 __global__ void k_modify_position(DevWorld w) {
   const WorldScalars& ws = *w.ws;
@@ -149,35 +147,106 @@ __global__ void k_bin(DevWorld w) {
   if (gc >= 0) w.grank[i] = atomicAdd(&w.cell_count[gc], 1);
 }
 
-// exclusive scan of cell_count[0 .. ncell + 2nx) into cell_start (one block)
-__global__ void k_scan(DevWorld w) {
+// Exclusive scan of cell_count[0 .. ncell + 2nx) into cell_start, in three
+// passes over tiles of kScanTile cells: tile sums, a scan of the tile sums
+// (one block), and the per-tile exclusive prefixes.
+constexpr int kScanThreads = 256;
+constexpr int kScanPer = 8;
+constexpr int kScanTile = kScanThreads * kScanPer;
+
+// block-wide inclusive scan of one value per thread (kScanThreads threads)
+__device__ __forceinline__ int32_t block_inclusive_scan(int32_t v, int32_t* sh_warp) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int32_t u = __shfl_up_sync(0xffffffffu, v, o);
+    if (lane >= o) v += u;
+  }
+  if (lane == 31) sh_warp[warp] = v;
+  __syncthreads();
+  if (warp == 0) {
+    int32_t s = (lane < kScanThreads / 32) ? sh_warp[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int32_t u = __shfl_up_sync(0xffffffffu, s, o);
+      if (lane >= o) s += u;
+    }
+    if (lane < kScanThreads / 32) sh_warp[lane] = s;
+  }
+  __syncthreads();
+  if (warp > 0) v += sh_warp[warp - 1];
+  return v;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_tiles(DevWorld w) {
   const WorldScalars& ws = *w.ws;
   if (ws.stop) return;
   Grid G = grid_of(ws, w.nx_cap, w.ny_cap);
   int total = G.ncell + 2 * G.nx;
-  __shared__ int32_t sh[1024];
-  int t = threadIdx.x;
-  int per = (total + blockDim.x - 1) / blockDim.x;
-  int beg = t * per, end = min(beg + per, total);
-  int32_t local = 0;
-  for (int k = beg; k < end; ++k) local += w.cell_count[k];
-  sh[t] = local;
-  __syncthreads();
-  for (int off = 1; off < (int)blockDim.x; off <<= 1) {
-    int32_t v = (t >= off) ? sh[t - off] : 0;
-    __syncthreads();
-    sh[t] += v;
+  int ntiles = (total + kScanTile - 1) / kScanTile;
+  __shared__ int32_t sh_warp[kScanThreads / 32];
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    int base = tile * kScanTile + threadIdx.x * kScanPer;
+    int32_t s = 0;
+#pragma unroll
+    for (int k = 0; k < kScanPer; ++k)
+      if (base + k < total) s += w.cell_count[base + k];
+    int32_t inc = block_inclusive_scan(s, sh_warp);
+    if (threadIdx.x == kScanThreads - 1) w.tile_sum[tile] = inc;
     __syncthreads();
   }
-  int32_t run = sh[t] - local;
-  for (int k = beg; k < end; ++k) {
-    w.cell_start[k] = run;
-    run += w.cell_count[k];
-  }
-  if (t == blockDim.x - 1) w.cell_start[total] = sh[t];
 }
 
-// also clears cell_count (already consumed by k_scan) for the next binning
+// exclusive scan of the tile sums (one block); cell_start[total] = total count
+__global__ void __launch_bounds__(kScanThreads) k_scan_sums(DevWorld w) {
+  const WorldScalars& ws = *w.ws;
+  if (ws.stop) return;
+  Grid G = grid_of(ws, w.nx_cap, w.ny_cap);
+  int total = G.ncell + 2 * G.nx;
+  int ntiles = (total + kScanTile - 1) / kScanTile;
+  __shared__ int32_t sh_warp[kScanThreads / 32];
+  int32_t carry = 0;
+  for (int base = 0; base < ntiles; base += kScanThreads) {
+    int t = base + threadIdx.x;
+    int32_t v = t < ntiles ? w.tile_sum[t] : 0;
+    int32_t inc = block_inclusive_scan(v, sh_warp);
+    if (t < ntiles) w.tile_sum[t] = carry + inc - v;
+    __syncthreads();
+    if (threadIdx.x == kScanThreads - 1) sh_warp[0] = inc;
+    __syncthreads();
+    carry += sh_warp[0];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) w.cell_start[total] = carry;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_apply(DevWorld w) {
+  const WorldScalars& ws = *w.ws;
+  if (ws.stop) return;
+  Grid G = grid_of(ws, w.nx_cap, w.ny_cap);
+  int total = G.ncell + 2 * G.nx;
+  int ntiles = (total + kScanTile - 1) / kScanTile;
+  __shared__ int32_t sh_warp[kScanThreads / 32];
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    int base = tile * kScanTile + threadIdx.x * kScanPer;
+    int32_t c[kScanPer];
+    int32_t s = 0;
+#pragma unroll
+    for (int k = 0; k < kScanPer; ++k) {
+      c[k] = (base + k < total) ? w.cell_count[base + k] : 0;
+      s += c[k];
+    }
+    int32_t run = block_inclusive_scan(s, sh_warp) - s + w.tile_sum[tile];
+#pragma unroll
+    for (int k = 0; k < kScanPer; ++k) {
+      if (base + k < total) w.cell_start[base + k] = run;
+      run += c[k];
+    }
+    __syncthreads();
+  }
+}
+
+// also clears cell_count (already consumed by the scan) for the next binning
 __global__ void k_scatter(DevWorld w) {
   const WorldScalars& ws = *w.ws;
   if (ws.stop) return;
@@ -194,11 +263,12 @@ __global__ void k_scatter(DevWorld w) {
 }
 
 // ---------------------------------------------------------------------------
-// a5-a15: updateContacts.  One thread per owner particle i scans the 3x3
-// neighbourhood (PeriodicBoundaryWorld.cpp:47-84, LeesEdwardsBoundaryWorld.cpp:
-// 128-204), evaluates every candidate j > i at its image offset
-// (PeriodicBoundaryWorld.cpp:97-101, LeesEdwardsBoundaryWorld.cpp:233-279),
-// and writes the contacts into its slots of the new slot set:
+// a5-a15: updateContacts.  One thread per owner (memory position m) scans the
+// 3x3 neighbourhood (PeriodicBoundaryWorld.cpp:47-84,
+// LeesEdwardsBoundaryWorld.cpp:128-204), evaluates every candidate with a
+// larger id at its image offset (PeriodicBoundaryWorld.cpp:97-101,
+// LeesEdwardsBoundaryWorld.cpp:233-279), and writes the contacts into its
+// slots of the new slot set:
 //   - new contact: initial shear overlap and damping constant (BaseParticle.cpp:38-65)
 //   - old contact: shear overlap rotated with the normal (BaseParticle.cpp:67-82)
 //   - candidate not in contact: dropped (BaseParticle.cpp:95)
@@ -207,30 +277,30 @@ __global__ void k_scatter(DevWorld w) {
 // FOLD_BG adds the Lees-Edwards background velocity on the fly, bit for bit the
 // value applyBackgroudVelocity would have stored.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ double damping_constant(const DevWorld& w, double factor, int i, int j) {
+__device__ __forceinline__ double damping_constant(const DevWorld& w, double factor, int mi, int mj) {
   // calculateDampingConstact (ContactModel_LinearDissipativeFrictional.cpp:73-82)
   // selected by SKIP_TIME_INTEGRAL (BaseParticle.cpp:53-64)
-  int si = w.setting[i] & SKIP_TIME_INTEGRAL, sj = w.setting[j] & SKIP_TIME_INTEGRAL;
-  double mi = w.mass[i], mj = w.mass[j];
-  if (!si && sj) return sqrt(mi) * factor;
-  if (si && !sj) return sqrt(mj) * factor;
-  return sqrt((mi * mj) / (mi + mj)) * factor;
+  int si = w.setting[mi] & SKIP_TIME_INTEGRAL, sj = w.setting[mj] & SKIP_TIME_INTEGRAL;
+  double a = w.mass[mi], b = w.mass[mj];
+  if (!si && sj) return sqrt(a) * factor;
+  if (si && !sj) return sqrt(b) * factor;
+  return sqrt((a * b) / (a + b)) * factor;
 }
 
 template <bool FOLD_BG>
-__device__ __forceinline__ PState load_state(const DevWorld& w, const WorldScalars& ws, int i) {
+__device__ __forceinline__ PState load_state(const DevWorld& w, const WorldScalars& ws, int m) {
   PState p;
-  p.shape = w.shape[i];
-  p.r = w.rad[i];
-  p.asp = w.asp[i];
-  double2 q = w.pos[i];
-  double2 v = w.vel[i];
+  p.shape = w.shape[m];
+  p.r = w.rad[m];
+  p.asp = w.asp[m];
+  double2 q = w.pos[m];
+  double2 v = w.vel[m];
   p.x = q.x;
   p.y = q.y;
   p.vx = FOLD_BG ? v.x + ws.shift_rate * q.y : v.x;
   p.vy = v.y;
-  p.rot = w.rot[i];
-  p.w = w.w[i];
+  p.rot = w.rot[m];
+  p.w = w.w[m];
   return p;
 }
 
@@ -238,30 +308,31 @@ template <bool FOLD_BG>
 __global__ void __launch_bounds__(128) k_update_contacts(DevWorld w, int par, int record) {
   const WorldScalars& ws = *w.ws;
   if (ws.stop) return;
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= w.n) return;
+  int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= w.n) return;
   const int n = w.n, K = w.K;
   const Slots& old = w.slots[par];
   const Slots& cur = w.slots[par ^ 1];
   uint32_t st = 0;
   Grid G = grid_of(ws, w.nx_cap, w.ny_cap);
   bool grid_ok = (G.nx >= 3 && G.ny >= 3);
+  const int id_i = w.id_of[m];
 
-  // previous history of i
-  int nold = old.count[i];
+  // previous history of this owner
+  int nold = old.count[m];
   if (nold > K) nold = K;
   int opart[kMaxSlots];
-  for (int o = 0; o < nold; ++o) opart[o] = old.partner[(size_t)o * n + i];
+  for (int o = 0; o < nold; ++o) opart[o] = old.partner[(size_t)o * n + m];
   uint32_t seen = 0;
   int k = 0;
 
   const double dt = ws.dt, kn = ws.kn, kt = ws.kt, mu = ws.mu, factor = ws.factor;
-  if (grid_ok && !(w.setting[i] & SKIP_CONTACT_DETECTION)) {
-    PState a = load_state<FOLD_BG>(w, ws, i);
+  if (grid_ok && !(w.setting[m] & SKIP_CONTACT_DETECTION)) {
+    PState a = load_state<FOLD_BG>(w, ws, m);
     double2 csa = make_double2(0.0, 0.0);
     if (a.shape == SHAPE_ELLIPSE) csa = make_double2(cos(a.rot), sin(a.rot));
-    int up_i = w.up[i];
-    double orad_i = w.orad[i];
+    const int up_i = w.up[m];
+    const double orad_i = w.orad[m];
     int ix = cell_of(a.x, ws.xmin, G.lx, G.nx);
     int iy = cell_of(a.y, ws.ymin, G.ly, G.ny);
     int ncand[3] = {0, 0, 0};
@@ -287,17 +358,18 @@ __global__ void __launch_bounds__(128) k_update_contacts(DevWorld w, int par, in
         }
         int q0 = w.cell_start[c], q1 = w.cell_start[c + 1];
         for (int q = q0; q < q1; ++q) {
-          int j = w.cell_mem[q];
-          if (j <= i) continue;
-          if (w.setting[j] & SKIP_CONTACT_DETECTION) continue;
-          if (w.up[j] == up_i) continue;
+          int mj = w.cell_mem[q];
+          int id_j = w.id_of[mj];
+          if (id_j <= id_i) continue;
+          if (w.setting[mj] & SKIP_CONTACT_DETECTION) continue;
+          if (w.up[mj] == up_i) continue;
           if (ncand[kind] + 1 >= kCandidateCap) {
             st |= ST_CAPACITY;
             continue;
           }
           ncand[kind]++;
           // offset of the image of j
-          double2 pj = w.pos[j];
+          double2 pj = w.pos[mj];
           vec2<double> off, ovel = V(0.0, 0.0);
           if (kind == CAND_REGULAR) {
             double ox = 0.0, oy = 0.0;
@@ -323,17 +395,17 @@ __global__ void __launch_bounds__(128) k_update_contacts(DevWorld w, int par, in
           // history slot of (i, j), if any
           int o = -1;
           for (int z = 0; z < nold; ++z)
-            if (opart[z] == j) {
+            if (opart[z] == id_j) {
               o = z;
               break;
             }
           if (o >= 0) seen |= 1u << o;
-          PState b = load_state<FOLD_BG>(w, ws, j);
+          PState b = load_state<FOLD_BG>(w, ws, mj);
           double2 csb = make_double2(0.0, 0.0);
           if (b.shape == SHAPE_ELLIPSE && a.shape == SHAPE_ELLIPSE)
             csb = make_double2(cos(b.rot), sin(b.rot));
           Geom g;
-          if (!contact_geometry(w.method, a, b, orad_i, w.orad[j], off, ovel, csa, csb, g, st))
+          if (!contact_geometry(w.method, a, b, orad_i, w.orad[mj], off, ovel, csa, csb, g, st))
             continue;
           if (k >= K) {
             st |= ST_CAPACITY;
@@ -346,9 +418,9 @@ __global__ void __launch_bounds__(128) k_update_contacts(DevWorld w, int par, in
             double rvn = dot(g.rv, g.n);
             if (!is_normal(rvn)) sh = g.srv * dt;
             else sh = g.srv * std_min(dt, g.overlap / rvn);
-            damp = damping_constant(w, factor, i, j);
+            damp = damping_constant(w, factor, m, mj);
           } else {
-            size_t oi = (size_t)o * n + i;
+            size_t oi = (size_t)o * n + m;
             double2 on = old.n[oi], os = old.s[oi];
             damp = old.damp[oi];
             vec2<double> no = V(on.x, on.y);
@@ -376,8 +448,8 @@ __global__ void __launch_bounds__(128) k_update_contacts(DevWorld w, int par, in
           vec2<double> F = fn + fs;
           double t1 = cross(g.bv1, F);
           double t2 = cross(g.bv2, -F);
-          size_t ci = (size_t)k * n + i;
-          cur.partner[ci] = j;
+          size_t ci = (size_t)k * n + m;
+          cur.partner[ci] = id_j;
           cur.n[ci] = make_double2(nn.x, nn.y);
           cur.s[ci] = make_double2(sh.x, sh.y);
           cur.damp[ci] = damp;
@@ -392,6 +464,10 @@ __global__ void __launch_bounds__(128) k_update_contacts(DevWorld w, int par, in
             cur.fn[ci] = make_double2(fn.x, fn.y);
             cur.ft[ci] = make_double2(fs.x, fs.y);
           }
+          // register with the partner for its force sum
+          int pos = atomicAdd(&w.incnt[mj], 1);
+          if (pos < K) w.inref[(size_t)pos * n + mj] = (uint32_t)m * (uint32_t)K + (uint32_t)k;
+          else st |= ST_CAPACITY;
           ++k;
         }
       }
@@ -404,7 +480,7 @@ __global__ void __launch_bounds__(128) k_update_contacts(DevWorld w, int par, in
       st |= ST_CAPACITY;
       break;
     }
-    size_t oi = (size_t)o * n + i, ci = (size_t)k * n + i;
+    size_t oi = (size_t)o * n + m, ci = (size_t)k * n + m;
     cur.partner[ci] = opart[o];
     cur.n[ci] = old.n[oi];
     cur.s[ci] = old.s[oi];
@@ -418,23 +494,21 @@ __global__ void __launch_bounds__(128) k_update_contacts(DevWorld w, int par, in
     cur.bv2[ci] = old.bv2[oi];
     cur.fn[ci] = old.fn[oi];
     cur.ft[ci] = old.ft[oi];
+    int mj = w.mpos[opart[o]];
+    int pos = atomicAdd(&w.incnt[mj], 1);
+    if (pos < K) w.inref[(size_t)pos * n + mj] = (uint32_t)m * (uint32_t)K + (uint32_t)k;
+    else st |= ST_CAPACITY;
     ++k;
   }
-  cur.count[i] = k;
-  // register each contact with its partner for the partner's force sum
-  for (int s = 0; s < k; ++s) {
-    int j = cur.partner[(size_t)s * n + i];
-    int pos = atomicAdd(&w.incnt[j], 1);
-    if (pos < K) w.inref[(size_t)pos * n + j] = (uint32_t)i * (uint32_t)K + (uint32_t)s;
-    else st |= ST_CAPACITY;
-  }
+  cur.count[m] = k;
   raise(w.status, st);
 }
 
-// small insertion sort of (key, value) pairs held in local arrays
-__device__ __forceinline__ void isort(uint32_t* key, int m) {
-  for (int a = 1; a < m; ++a) {
-    uint32_t x = key[a];
+// small insertion sorts of keys held in local arrays
+template <class T>
+__device__ __forceinline__ void isort(T* key, int cnt) {
+  for (int a = 1; a < cnt; ++a) {
+    T x = key[a];
     int b = a - 1;
     while (b >= 0 && key[b] > x) {
       key[b + 1] = key[b];
@@ -446,8 +520,8 @@ __device__ __forceinline__ void isort(uint32_t* key, int m) {
 
 // ---------------------------------------------------------------------------
 // a16: collectForceAndTorque (BaseWorld.cpp:17-57).  Each particle sums, in a
-// fixed order, the contacts owned by lower ids (ascending owner; -F and
-// torqueOnP2) and then its own contacts (ascending partner; F and
+// fixed order, the contacts owned by lower ids (ascending owner id; -F and
+// torqueOnP2) and then its own contacts (ascending partner id; F and
 // torqueOnP1), starting from zero as the reference's per-thread arrays do.
 // Particles with no contact are rattlers (BaseWorld.cpp:25,44-45).
 // ---------------------------------------------------------------------------
@@ -460,26 +534,34 @@ __global__ void __launch_bounds__(128) k_collect(DevWorld w, int par) {
   const Slots& cur = w.slots[par];
   int nown = min(cur.count[p], K);
   int ninc = min(w.incnt[p], K);
-  uint32_t key[kMaxSlots];
   double fx = 0.0, fy = 0.0, t = 0.0;
-  for (int a = 0; a < ninc; ++a) key[a] = w.inref[(size_t)a * n + p];
-  isort(key, ninc);
-  for (int a = 0; a < ninc; ++a) {
-    uint32_t owner = key[a] / K, slot = key[a] % K;
-    size_t ci = (size_t)slot * n + owner;
-    double2 F = cur.f[ci];
-    fx += -F.x;
-    fy += -F.y;
-    t += cur.t2[ci];
+  {
+    uint64_t key[kMaxSlots];  // owner id << 32 | reference
+    for (int a = 0; a < ninc; ++a) {
+      uint32_t ref = w.inref[(size_t)a * n + p];
+      key[a] = ((uint64_t)(uint32_t)w.id_of[ref / K] << 32) | ref;
+    }
+    isort(key, ninc);
+    for (int a = 0; a < ninc; ++a) {
+      uint32_t ref = (uint32_t)key[a];
+      size_t ci = (size_t)(ref % K) * n + ref / K;
+      double2 F = cur.f[ci];
+      fx += -F.x;
+      fy += -F.y;
+      t += cur.t2[ci];
+    }
   }
-  for (int a = 0; a < nown; ++a) key[a] = ((uint32_t)cur.partner[(size_t)a * n + p] << 5) | a;
-  isort(key, nown);
-  for (int a = 0; a < nown; ++a) {
-    size_t ci = (size_t)(key[a] & 31u) * n + p;
-    double2 F = cur.f[ci];
-    fx += F.x;
-    fy += F.y;
-    t += cur.t1[ci];
+  {
+    uint32_t key[kMaxSlots];  // partner id << 5 | slot
+    for (int a = 0; a < nown; ++a) key[a] = ((uint32_t)cur.partner[(size_t)a * n + p] << 5) | a;
+    isort(key, nown);
+    for (int a = 0; a < nown; ++a) {
+      size_t ci = (size_t)(key[a] & 31u) * n + p;
+      double2 F = cur.f[ci];
+      fx += F.x;
+      fy += F.y;
+      t += cur.t1[ci];
+    }
   }
   w.force[p] = make_double2(fx, fy);
   w.torque[p] = t;
@@ -488,14 +570,14 @@ __global__ void __launch_bounds__(128) k_collect(DevWorld w, int par) {
 }
 
 // GluedParticle::isRattlerParticle (GluedParticle.cpp:141-147)
-__device__ __forceinline__ bool is_rattler(const DevWorld& w, int i) {
-  if (w.shape[i] == SHAPE_CLUMP) {
-    int ns = w.num_sub[i];
+__device__ __forceinline__ bool is_rattler(const DevWorld& w, int m) {
+  if (w.shape[m] == SHAPE_CLUMP) {
+    int ns = w.num_sub[m], id = w.id_of[m];
     for (int k = 1; k <= ns; ++k)
-      if (!w.rattler[i + k]) return false;
+      if (!w.rattler[w.mpos[id + k]]) return false;
     return true;
   }
-  return w.rattler[i] != 0;
+  return w.rattler[m] != 0;
 }
 
 // ---------------------------------------------------------------------------
@@ -511,7 +593,8 @@ __global__ void k_integrate(DevWorld w, int reset_rattlers) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= w.n) return;
   const double dt = ws.dt, g = ws.g;
-  int set = w.setting[i];
+  const int set = w.setting[i];
+  const int id = w.id_of[i];
   double2 v = w.vel[i];
   if (FOLD_BG) {
     double y = w.pos[i].y;
@@ -519,8 +602,8 @@ __global__ void k_integrate(DevWorld w, int reset_rattlers) {
   }
   if (set & SKIP_TIME_INTEGRAL) {
     // a sub-particle's velocity is rewritten by its clump below
-    if (FOLD_BG && w.up[i] == i) w.vel[i] = v;
-    if (reset_rattlers && !(set & SKIP_MACRO_SUM) && w.up[i] == i && is_rattler(w, i)) {
+    if (FOLD_BG && w.up[i] == id) w.vel[i] = v;
+    if (reset_rattlers && !(set & SKIP_MACRO_SUM) && w.up[i] == id && is_rattler(w, i)) {
       w.vel[i] = make_double2(0.0, 0.0);
       w.w[i] = 0.0;
     }
@@ -531,12 +614,13 @@ __global__ void k_integrate(DevWorld w, int reset_rattlers) {
   if (w.shape[i] == SHAPE_CLUMP) {
     vec2<double> F = V(0.0, 0.0);
     double T = 0.0;
-    int ns = w.num_sub[i];
+    const int ns = w.num_sub[i];
     for (int k = 1; k <= ns; ++k) {
-      double2 fk = w.force[i + k];
-      double2 bk = w.branch[i + k];
+      int sk = w.mpos[id + k];
+      double2 fk = w.force[sk];
+      double2 bk = w.branch[sk];
       F = F + V(fk.x, fk.y);
-      T += w.torque[i + k];
+      T += w.torque[sk];
       T += cross(V(bk.x, bk.y), V(fk.x, fk.y));
     }
     vec2<double> vv = (V(v.x, v.y) * (1.0 - g * dt) + (F * w.im[i]) * dt) / (1.0 + g * dt);
@@ -548,14 +632,15 @@ __global__ void k_integrate(DevWorld w, int reset_rattlers) {
     double ca = cos(angle), sa = sin(angle);
     mat2<double> R = M(ca, -sa, sa, ca);
     for (int k = 1; k <= ns; ++k) {
-      double2 bk = w.branch[i + k];
+      int sk = w.mpos[id + k];
+      double2 bk = w.branch[sk];
       vec2<double> b = R * V(bk.x, bk.y);
-      w.branch[i + k] = make_double2(b.x, b.y);
+      w.branch[sk] = make_double2(b.x, b.y);
       vec2<double> sv = vv + crossw(b, om);
-      w.vel[i + k] = make_double2(sv.x, sv.y);
-      w.pos[i + k] = make_double2(p.x + b.x, p.y + b.y);
-      w.w[i + k] = om;
-      w.rot[i + k] += angle;
+      w.vel[sk] = make_double2(sv.x, sv.y);
+      w.pos[sk] = make_double2(p.x + b.x, p.y + b.y);
+      w.w[sk] = om;
+      w.rot[sk] += angle;
     }
     w.pos[i] = p;
     w.rot[i] = rot;
@@ -607,18 +692,19 @@ __global__ void k_rattlers(DevWorld w, int reset, double scale) {
 // a21: updateTotalStress (BaseWorld.cpp:158-176) with getStressFromContactList
 // of BaseParticle (BaseParticle.cpp:143-151) and GluedParticle
 // (GluedParticle.cpp:127-139).  Per-particle sums in ascending partner order,
-// then a fixed tree over particles: deterministic run to run.
+// then a fixed tree over the memory order, which is a deterministic function
+// of the state: deterministic run to run.
 // ---------------------------------------------------------------------------
 constexpr int kReduceBlock = 256;
 
-__device__ __forceinline__ void own_stress(const DevWorld& w, const Slots& cur, int p,
-                                           bool sub, double2 bvo, mat2<double>& s) {
+__device__ __forceinline__ void own_stress(const DevWorld& w, const Slots& cur, int p, bool sub,
+                                           double2 bvo, mat2<double>& s) {
   const int n = w.n, K = w.K;
-  int m = min(cur.count[p], K);
+  int cnt = min(cur.count[p], K);
   uint32_t key[kMaxSlots];
-  for (int a = 0; a < m; ++a) key[a] = ((uint32_t)cur.partner[(size_t)a * n + p] << 5) | a;
-  isort(key, m);
-  for (int a = 0; a < m; ++a) {
+  for (int a = 0; a < cnt; ++a) key[a] = ((uint32_t)cur.partner[(size_t)a * n + p] << 5) | a;
+  isort(key, cnt);
+  for (int a = 0; a < cnt; ++a) {
     size_t ci = (size_t)(key[a] & 31u) * n + p;
     double2 F = cur.f[ci], b = cur.b[ci];
     vec2<double> bb = V(b.x, b.y);
@@ -637,7 +723,11 @@ __global__ void __launch_bounds__(kReduceBlock) k_stress_partial(DevWorld w, int
     const Slots& cur = w.slots[par];
     if (w.shape[p] == SHAPE_CLUMP) {
       // one running sum over all sub-particles (GluedParticle.cpp:128-137)
-      for (int k = 1; k <= w.num_sub[p]; ++k) own_stress(w, cur, p + k, true, w.branch[p + k], s);
+      int id = w.id_of[p];
+      for (int k = 1; k <= w.num_sub[p]; ++k) {
+        int sk = w.mpos[id + k];
+        own_stress(w, cur, sk, true, w.branch[sk], s);
+      }
     } else {
       own_stress(w, cur, p, false, make_double2(0.0, 0.0), s);
     }
@@ -682,7 +772,6 @@ __global__ void k_stress_final(DevWorld w, int nblocks) {
 // ---------------------------------------------------------------------------
 // a20: PeriodicControlWorld box laws (PeriodicControlWorld.cpp:124-237).  One
 // thread updates the box and leaves the affine scale for k_scale_positions.
-// Also counts the step and evaluates a run's stop condition.
 // ---------------------------------------------------------------------------
 enum : int { BOX_NONE = 0, BOX_STRAIN = 1, BOX_STRESS_XY = 2, BOX_STRESS_UNIFORM = 3,
              BOX_STRESS_UNIFORM_LIMIT = 4 };
@@ -760,17 +849,17 @@ __device__ __forceinline__ void box_law(WorldScalars& ws, int law, double p0, do
   }
 }
 
-// end-of-step scalar work: box law, Lees-Edwards update
-// (LeesEdwardsBoundaryWorld.cpp:285-296), step count and stop test
+// End-of-step scalar work: Lees-Edwards update (LeesEdwardsBoundaryWorld.cpp:
+// 285-296, part of its takeTimeStep), then the driver's box law, the step
+// count and the stop test.  After a stop the scales are 1.
 __global__ void k_end_of_step(DevWorld w, int law, double p0, double p1, int le_update,
-                              int stop_on_pressure, double stop_pressure) {
+                              int stop_on_pressure, double stop_pressure, int count_step) {
   WorldScalars& ws = *w.ws;
   if (ws.stop) {
     ws.scale_x = 1.0;
     ws.scale_y = 1.0;
     return;
   }
-  if (law != BOX_NONE) box_law(ws, law, p0, p1);
   if (le_update) {
     ws.shift_vel = ws.shift_rate * ws.ylen;
     ws.strain += ws.shift_rate * ws.dt;
@@ -778,7 +867,11 @@ __global__ void k_end_of_step(DevWorld w, int law, double p0, double p1, int le_
     if (ws.shift > ws.xmax) ws.shift -= ws.xlen;
     else if (ws.shift < ws.xmin) ws.shift += ws.xlen;
   }
-  ws.steps_done += 1;
+  if (law != BOX_NONE) box_law(ws, law, p0, p1);
+  if (count_step) {
+    ws.steps_done += 1;
+    ws.flips += 1;
+  }
   if (stop_on_pressure && (ws.stress[0] + ws.stress[3]) / 2.0 >= stop_pressure) ws.stop = 1;
 }
 
@@ -814,6 +907,30 @@ __global__ void k_ke_final(DevWorld w, int nblocks) {
     __syncthreads();
   }
   if (t == 0) w.ws->ke = sh[0];
+}
+
+// id-ordered staging of the dynamic state (x, y, vx, vy, rot, rot_vel blocks
+// of n doubles each) <-> memory order
+__global__ void k_stage(DevWorld w, int to_world) {
+  int id = blockIdx.x * blockDim.x + threadIdx.x;
+  if (id >= w.n) return;
+  const int n = w.n;
+  const int m = w.mpos[id];
+  double* s = w.stage;
+  if (to_world) {
+    w.pos[m] = make_double2(s[id], s[n + id]);
+    w.vel[m] = make_double2(s[2 * n + id], s[3 * n + id]);
+    w.rot[m] = s[4 * n + id];
+    w.w[m] = s[5 * n + id];
+  } else {
+    double2 p = w.pos[m], v = w.vel[m];
+    s[id] = p.x;
+    s[n + id] = p.y;
+    s[2 * n + id] = v.x;
+    s[3 * n + id] = v.y;
+    s[4 * n + id] = w.rot[m];
+    s[5 * n + id] = w.w[m];
+  }
 }
 
 // single-pair geometry for known-answer tests (xdem_pair_geometry)

@@ -1,0 +1,149 @@
+// resort.cuh — refreshes the memory order of a world (world.cuh).
+//
+// Runs after a step's binning: particles are ordered by regular cell, ties by
+// id (k_sort_cells, deterministic), every particle array is moved to its new
+// position through a scratch slab and copied back (array addresses stay fixed,
+// so captured graphs stay valid), the contact history moves into the other
+// slot set (which the next update overwrites anyway), and the cell lists are
+// renumbered.  Nothing the reference computes depends on the memory order.
+#pragma once
+#include "kernels.cuh"
+
+namespace xdem {
+
+constexpr int kMaxPermArrays = 24;
+
+struct PermList {
+  void* base[kMaxPermArrays];
+  size_t offset[kMaxPermArrays];  // byte offset of the array's slab in scratch
+  int esize[kMaxPermArrays];      // 4, 8 or 16 bytes
+  int count;
+};
+
+// members of each regular cell in ascending id; newpos = the sorted index
+__global__ void k_sort_cells(DevWorld w) {
+  const WorldScalars& ws = *w.ws;
+  if (ws.stop) return;
+  Grid G = grid_of(ws, w.nx_cap, w.ny_cap);
+  if (G.nx < 3 || G.ny < 3) return;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < G.ncell; c += gridDim.x * blockDim.x) {
+    int q0 = w.cell_start[c], q1 = w.cell_start[c + 1];
+    for (int a = q0 + 1; a < q1; ++a) {
+      int x = w.cell_mem[a];
+      int kx = w.id_of[x];
+      int b = a - 1;
+      while (b >= q0 && w.id_of[w.cell_mem[b]] > kx) {
+        w.cell_mem[b + 1] = w.cell_mem[b];
+        --b;
+      }
+      w.cell_mem[b + 1] = x;
+    }
+    for (int q = q0; q < q1; ++q) w.newpos[w.cell_mem[q]] = q;
+  }
+}
+
+template <int E>
+struct Elem;
+template <>
+struct Elem<4> {
+  using T = int32_t;
+};
+template <>
+struct Elem<8> {
+  using T = double;
+};
+template <>
+struct Elem<16> {
+  using T = double2;
+};
+
+template <int E>
+__device__ __forceinline__ void move_elem(void* src, int si, void* dst, int di) {
+  using T = typename Elem<E>::T;
+  static_cast<T*>(dst)[di] = static_cast<const T*>(src)[si];
+}
+
+// every array element m -> scratch slab at newpos[m]; mpos follows
+__global__ void k_permute(DevWorld w, PermList L) {
+  const WorldScalars& ws = *w.ws;
+  if (ws.stop) return;
+  Grid G = grid_of(ws, w.nx_cap, w.ny_cap);
+  if (G.nx < 3 || G.ny < 3) return;
+  int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= w.n) return;
+  int t = w.newpos[m];
+  w.mpos[w.id_of[m]] = t;
+  for (int a = 0; a < L.count; ++a) {
+    void* dst = w.scratch + L.offset[a];
+    switch (L.esize[a]) {
+      case 4: move_elem<4>(L.base[a], m, dst, t); break;
+      case 8: move_elem<8>(L.base[a], m, dst, t); break;
+      default: move_elem<16>(L.base[a], m, dst, t); break;
+    }
+  }
+}
+
+__global__ void k_copy_back(DevWorld w, PermList L) {
+  const WorldScalars& ws = *w.ws;
+  if (ws.stop) return;
+  Grid G = grid_of(ws, w.nx_cap, w.ny_cap);
+  if (G.nx < 3 || G.ny < 3) return;
+  int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= w.n) return;
+  for (int a = 0; a < L.count; ++a) {
+    void* src = w.scratch + L.offset[a];
+    switch (L.esize[a]) {
+      case 4: move_elem<4>(src, m, L.base[a], m); break;
+      case 8: move_elem<8>(src, m, L.base[a], m); break;
+      default: move_elem<16>(src, m, L.base[a], m); break;
+    }
+  }
+}
+
+// history of the owner at m -> slot set par^1 at newpos[m]; counts one swap.
+// With an invalid grid the particles did not move and the history is copied
+// in place, so that the slot-set parity stays what the host expects.
+__global__ void k_permute_history(DevWorld w, int par) {
+  WorldScalars& ws = *w.ws;
+  if (ws.stop) return;
+  Grid G = grid_of(ws, w.nx_cap, w.ny_cap);
+  const bool moved = G.nx >= 3 && G.ny >= 3;
+  int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m == 0) ws.flips += 1;
+  if (m >= w.n) return;
+  const int n = w.n, K = w.K;
+  const Slots& src = w.slots[par];
+  const Slots& dst = w.slots[par ^ 1];
+  int t = moved ? w.newpos[m] : m;
+  int c = min(src.count[m], K);
+  dst.count[t] = c;
+  for (int s = 0; s < c; ++s) {
+    size_t a = (size_t)s * n + m, b = (size_t)s * n + t;
+    dst.partner[b] = src.partner[a];
+    dst.n[b] = src.n[a];
+    dst.s[b] = src.s[a];
+    dst.damp[b] = src.damp[a];
+    dst.f[b] = src.f[a];
+    dst.t1[b] = src.t1[a];
+    dst.t2[b] = src.t2[a];
+    dst.b[b] = src.b[a];
+    dst.cp[b] = src.cp[a];
+    dst.bv1[b] = src.bv1[a];
+    dst.bv2[b] = src.bv2[a];
+    dst.fn[b] = src.fn[a];
+    dst.ft[b] = src.ft[a];
+  }
+}
+
+// cell lists hold positions: renumber them
+__global__ void k_remap_cells(DevWorld w) {
+  const WorldScalars& ws = *w.ws;
+  if (ws.stop) return;
+  Grid G = grid_of(ws, w.nx_cap, w.ny_cap);
+  if (G.nx < 3 || G.ny < 3) return;
+  int total = w.cell_start[G.ncell + 2 * G.nx];
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < total; q += gridDim.x * blockDim.x)
+    w.cell_mem[q] = w.newpos[w.cell_mem[q]];
+}
+
+}  // namespace xdem

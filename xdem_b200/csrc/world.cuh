@@ -1,11 +1,19 @@
 // world.cuh — device-side layout of one DEM world.
 //
-// Particles are SoA in id order (ids equal indices, as the reference assumes).
-// Contact history lives in per-owner slots: slot s of particle i is element
-// s*n + i of each slot array (slot-major, so consecutive particles touch
-// consecutive addresses), owner = lower id as in the reference's per-particle
-// maps.  Two slot sets alternate between steps: one holds the previous step's
-// history, the other receives this step's contacts.
+// Memory order.  Every per-particle array is stored in a memory order m that
+// follows the cell grid: particles of one cell are contiguous, cells in
+// row-major order, ties broken by particle id.  The order is refreshed every
+// few steps (resort.cuh), so that the 3x3 neighbourhood of a warp's particles
+// is a handful of contiguous address ranges.  id_of[m] is the reference's
+// particle id at position m and mpos[id] its inverse; everything the reference
+// orders by id (contact ownership, force-sum order, clump sub-particles) is
+// ordered by id here too, so results do not depend on the memory order.
+//
+// Contact history lives in per-owner slots: slot s of the particle at m is
+// element s*n + m of each slot array (slot-major, so consecutive particles
+// touch consecutive addresses); the owner is the lower id, as in the
+// reference's per-particle maps.  Two slot sets alternate: one holds the
+// previous history while the other receives the new contacts.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -15,8 +23,8 @@ namespace xdem {
 constexpr int kMaxSlots = 32;  // upper bound of history slots per particle
 
 struct Slots {
-  int32_t* count;    // [n] contacts owned by particle i
-  int32_t* partner;  // [K*n] partner id j (> i)
+  int32_t* count;    // [n] contacts owned by the particle at m
+  int32_t* partner;  // [K*n] partner id j (> owner id)
   double2* n;        // contact normal
   double2* s;        // tangential spring (shear overlap)
   double* damp;      // damping constant, fixed at creation
@@ -44,6 +52,7 @@ struct WorldScalars {
   double ke;
   int32_t stop;        // set once a run's stop condition is met
   int32_t steps_done;  // steps completed in the current run
+  int32_t flips;       // slot-set swaps executed in the current run
 };
 
 struct DevWorld {
@@ -53,20 +62,21 @@ struct DevWorld {
   int method;
   int precision;
   int nx_cap, ny_cap;  // cell-grid capacity
-  // static particle data
-  const int32_t* shape;
-  const int32_t* up;
-  const int32_t* setting;
-  const int32_t* num_sub;
-  const double* orad;
-  const double* rad;
-  const double* asp;
-  const double* mass;
-  const double* im;
-  const double* I;
-  const double* iI;
-  const double* vol;
-  // dynamic particle data
+  // particle arrays, memory order
+  int32_t* id_of;  // id at position m
+  int32_t* mpos;   // [id] position of id
+  int32_t* shape;
+  int32_t* up;
+  int32_t* setting;
+  int32_t* num_sub;
+  double* orad;
+  double* rad;
+  double* asp;
+  double* mass;
+  double* im;
+  double* I;
+  double* iI;
+  double* vol;
   double2* pos;
   double2* vel;
   double* rot;
@@ -76,22 +86,27 @@ struct DevWorld {
   double2* force;
   double* torque;
   int32_t* ncp;
-  // cell grid: regular cells, then two ghost rows of nx (Lees-Edwards images)
+  // cell grid: regular cells, then two ghost rows of nx (Lees-Edwards images);
+  // cell_mem holds memory positions
   int32_t* cell_count;
   int32_t* cell_start;
+  int32_t* tile_sum;  // scan tile sums
   int32_t* cell_mem;
-  int32_t* pcell;  // [n] regular cell of particle
+  int32_t* pcell;  // [n] regular cell of the particle at m
   int32_t* prank;  // [n] rank within the cell
   int32_t* gcell;  // [n] ghost cell or -1
   int32_t* grank;
+  int32_t* newpos;  // [n] destination of m in a re-sort
   // contacts
   Slots slots[2];
   int32_t* incnt;   // [n] contacts owned by lower ids
-  uint32_t* inref;  // [K*n] owner*K + slot of those contacts
+  uint32_t* inref;  // [K*n] owner position*K + slot of those contacts
   // scalars, status, scratch
   WorldScalars* ws;
   uint32_t* status;
   double* partials;  // block partial sums
+  char* scratch;     // re-sort staging, one slab per particle array
+  double* stage;     // [6n] id-ordered staging of the dynamic state
 };
 
 }  // namespace xdem
