@@ -75,6 +75,11 @@ def workload_le_ellipses(n, seed):
     prm_c = make_params(abi.WORLD_PERIODIC_CONTROL, dt, box, inputs.KN, inputs.KT,
                         inputs.RESTITUTION, inputs.FRICTION, global_damping=0.1)
     w = World(prm_c)
+    # during the fast compression a few deeply overlapping pairs send the
+    # closest-approach Newton iteration into a cycle (the reference's loop would
+    # never return there); the capped solver reports it and carries on
+    w.raise_mask = ~abi.ERR_NEWTON
+    newton_events = 0
     w.set_particles(p)
     area0 = (box[1] - box[0]) * (box[3] - box[2])
     phi0 = float(p["volume"].sum() / area0)
@@ -96,9 +101,12 @@ def workload_le_ellipses(n, seed):
         L = b[1] - b[0]
         ctl.p0 = ctl.p1 = (s_step - 1.0) / (L * dt)
         w.run(200, ctl)
+        newton_events += 1 if w.last_status & abi.ERR_NEWTON else 0
         done += 200
-    w.run(1000, make_control())  # relax at the final box
-    log(f"setup: compressed phi {phi0:.3f} -> {phi:.3f} in {done} steps, {time.time() - t:.1f}s")
+    w.run(2000, make_control())  # relax at the final box
+    newton_events += 1 if w.last_status & abi.ERR_NEWTON else 0
+    log(f"setup: compressed phi {phi0:.3f} -> {phi:.3f} in {done} steps, {time.time() - t:.1f}s, "
+        f"{newton_events} chunks with capped Newton iterations")
     st = w.get_state()
     contacts = w.get_contacts()
     b = w.getBoundary()

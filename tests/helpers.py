@@ -192,7 +192,7 @@ def compare_pair_geometry(og, oc, pi, pj, off, method, tol=1e-10):
         assert np.all(err <= allowed), (col, float(np.max(err / allowed)))
     # pairs whose outputs move by at most 1e-12 of scale under a 1-ulp
     # perturbation (condition number below ~5e3) must also meet `tol` alone
-    well = hit & (spread[:, 9] <= 1e-12 * np.max(oc[hit, 9]))
+    well = hit & (spread[:, 9] <= 1e-12 * np.nanmax(np.abs(oc[hit, 9])))
     assert well.sum() >= 0.75 * hit.sum(), (well.sum(), hit.sum())
     for col in range(1, 16):
         assert rel_err(og[well, col], oc[well, col]) <= tol, col

@@ -225,6 +225,24 @@ def test_lees_edwards_substeps_equal_fused_step():
         np.testing.assert_array_equal(sa[k], sb[k])
 
 
+def test_many_resorts_match_checker():
+    """Runs long enough for several memory-order refreshes (each captured chunk
+    starts with one), with state read back and written again in between."""
+    p, prm = disc_case(n=500, phi=0.80, seed=14)
+    g, c = _pair(p, prm)
+    ctl = make_control(update_stress=True)
+    for chunk in (70, 64, 1, 33):
+        g.run(chunk, ctl)
+        c.run(chunk, ctl)
+        _compare_worlds(g, c, TRAJ_TOL)
+    # a state round trip through the id-ordered boundary leaves the run unchanged
+    st = g.get_state()
+    g.upload_state(st["x"], st["y"], st["vx"], st["vy"], st["rot"], st["rot_vel"])
+    g.run(40, ctl)
+    c.run(40, ctl)
+    _compare_worlds(g, c, TRAJ_TOL)
+
+
 def test_run_deterministic():
     p, prm = ellipse_case(n=500, seed=8, compress=1.5)
     out = []

@@ -67,6 +67,7 @@ struct xdem_world_s {
   int64_t launches = 0;
   cudaEvent_t timer[2] = {nullptr, nullptr};
   int since_resort = kResortEvery;  // steps since the memory order was refreshed
+  int law = LAW_ANY;                // contact-kernel specialisation for the shapes present
   PermList perm{};                  // particle arrays moved by a re-sort
 };
 
@@ -170,14 +171,32 @@ void launch_find(xdem_world_s* w) {
   LAUNCH(w, KK_SCATTER, k_scatter<<<nb, kBlock, 0, w->stream>>>(w->dw));
 }
 
+template <bool FOLD_BG>
+void launch_update_law(xdem_world_s* w, int record) {
+  const int nb = blocks_for(w->dw.n, 128);
+  switch (w->law) {
+    case LAW_CIRCLE:
+      LAUNCH(w, KK_UPDATE, k_update_contacts<FOLD_BG, LAW_CIRCLE>
+                               <<<nb, 128, 0, w->stream>>>(w->dw, w->par, record));
+      break;
+    case LAW_CLOSEST:
+      LAUNCH(w, KK_UPDATE, k_update_contacts<FOLD_BG, LAW_CLOSEST>
+                               <<<nb, 128, 0, w->stream>>>(w->dw, w->par, record));
+      break;
+    case LAW_INTERSECTION:
+      LAUNCH(w, KK_UPDATE, k_update_contacts<FOLD_BG, LAW_INTERSECTION>
+                               <<<nb, 128, 0, w->stream>>>(w->dw, w->par, record));
+      break;
+    default:
+      LAUNCH(w, KK_UPDATE, k_update_contacts<FOLD_BG, LAW_ANY>
+                               <<<nb, 128, 0, w->stream>>>(w->dw, w->par, record));
+      break;
+  }
+}
+
 void launch_update(xdem_world_s* w, bool fold_bg, int record) {
-  int n = w->dw.n;
-  if (fold_bg)
-    LAUNCH(w, KK_UPDATE,
-           k_update_contacts<true><<<blocks_for(n, 128), 128, 0, w->stream>>>(w->dw, w->par, record));
-  else
-    LAUNCH(w, KK_UPDATE,
-           k_update_contacts<false><<<blocks_for(n, 128), 128, 0, w->stream>>>(w->dw, w->par, record));
+  if (fold_bg) launch_update_law<true>(w, record);
+  else launch_update_law<false>(w, record);
   w->par ^= 1;
 }
 
@@ -483,6 +502,16 @@ int32_t xdem_set_particles(xdem_world w, const xdem_particles* P) {
   CK(w, cudaMemsetAsync(d.ncp, 0, sizeof(int32_t) * n, s));
   w->total_volume = volsum;
   w->control_mass = msum / ((double)n * 10.0);  // setVirtualBoundaryMass (PeriodicControlWorld.cpp:58-66)
+  // one contact law for the whole world when every non-clump body has one shape
+  bool any_circle = false, any_ellipse = false;
+  for (int i = 0; i < n; ++i) {
+    any_circle |= P->shape[i] == XDEM_SHAPE_CIRCLE;
+    any_ellipse |= P->shape[i] == XDEM_SHAPE_ELLIPSE;
+  }
+  if (any_circle && any_ellipse) w->law = LAW_ANY;
+  else if (any_ellipse)
+    w->law = w->prm.ellipse_method == XDEM_ELLIPSE_INTERSECTION ? LAW_INTERSECTION : LAW_CLOSEST;
+  else w->law = LAW_CIRCLE;
   WorldScalars ws;
   CK(w, read_scalars(w, &ws));
   ws.maxsize = w->prm.max_particle_size > 0 ? w->prm.max_particle_size : maxr * 2.01;

@@ -304,8 +304,9 @@ __device__ __forceinline__ PState load_state(const DevWorld& w, const WorldScala
   return p;
 }
 
-template <bool FOLD_BG>
-__global__ void __launch_bounds__(128) k_update_contacts(DevWorld w, int par, int record) {
+template <bool FOLD_BG, int LAW>
+__global__ void __launch_bounds__(128, LAW == LAW_CIRCLE ? 4 : 1)
+    k_update_contacts(DevWorld w, int par, int record) {
   const WorldScalars& ws = *w.ws;
   if (ws.stop) return;
   int m = blockIdx.x * blockDim.x + threadIdx.x;
@@ -330,7 +331,7 @@ __global__ void __launch_bounds__(128) k_update_contacts(DevWorld w, int par, in
   if (grid_ok && !(w.setting[m] & SKIP_CONTACT_DETECTION)) {
     PState a = load_state<FOLD_BG>(w, ws, m);
     double2 csa = make_double2(0.0, 0.0);
-    if (a.shape == SHAPE_ELLIPSE) csa = make_double2(cos(a.rot), sin(a.rot));
+    if (LAW != LAW_CIRCLE && a.shape == SHAPE_ELLIPSE) csa = make_double2(cos(a.rot), sin(a.rot));
     const int up_i = w.up[m];
     const double orad_i = w.orad[m];
     int ix = cell_of(a.x, ws.xmin, G.lx, G.nx);
@@ -402,11 +403,15 @@ __global__ void __launch_bounds__(128) k_update_contacts(DevWorld w, int par, in
           if (o >= 0) seen |= 1u << o;
           PState b = load_state<FOLD_BG>(w, ws, mj);
           double2 csb = make_double2(0.0, 0.0);
-          if (b.shape == SHAPE_ELLIPSE && a.shape == SHAPE_ELLIPSE)
+          if (LAW != LAW_CIRCLE && b.shape == SHAPE_ELLIPSE && a.shape == SHAPE_ELLIPSE)
             csb = make_double2(cos(b.rot), sin(b.rot));
           Geom g;
-          if (!contact_geometry(w.method, a, b, orad_i, w.orad[mj], off, ovel, csa, csb, g, st))
-            continue;
+          bool touching;
+          if (LAW == LAW_ANY)
+            touching = contact_geometry(w.method, a, b, orad_i, w.orad[mj], off, ovel, csa, csb, g, st);
+          else
+            touching = contact_geometry_law<LAW>(a, b, orad_i, w.orad[mj], off, ovel, csa, csb, g, st);
+          if (!touching) continue;
           if (k >= K) {
             st |= ST_CAPACITY;
             continue;
