@@ -255,6 +255,11 @@ int32_t xdem_set_virtual_boundary_mass(xdem_world w, double mass /* <0: from par
 int32_t xdem_set_max_strain_rate(xdem_world w, double rate);
 /* kinetic energy (BaseWorld.cpp:302-310) */
 int32_t xdem_get_kinetic_energy(xdem_world w, double* out);
+/* closest-approach Newton statistics since creation or the last reset:
+   out = {solves, iterations, solves stopped by the iteration cap}
+   (NewtonRaphsonForQuartic, EllipticParticle.cpp:613-626) */
+int32_t xdem_get_newton_stats(xdem_world w, int64_t out[3]);
+int32_t xdem_reset_newton_stats(xdem_world w);
 
 /* ---- sub-steps (each one reference method) ----------------------------- */
 /* PeriodicBoundaryWorld::modifyParticlePosition (PeriodicBoundaryWorld.cpp:129-142)

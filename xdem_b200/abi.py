@@ -198,6 +198,8 @@ def load_library(path=LIB_PATH):
         "xdem_set_virtual_boundary_mass": (C.c_int32, [W, C.c_double]),
         "xdem_set_max_strain_rate": (C.c_int32, [W, C.c_double]),
         "xdem_get_kinetic_energy": (C.c_int32, [W, _d]),
+        "xdem_get_newton_stats": (C.c_int32, [W, P(C.c_int64)]),
+        "xdem_reset_newton_stats": (C.c_int32, [W]),
         "xdem_modify_particle_position": (C.c_int32, [W]),
         "xdem_apply_background_velocity": (C.c_int32, [W]),
         "xdem_remove_background_velocity": (C.c_int32, [W]),

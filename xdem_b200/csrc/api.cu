@@ -922,6 +922,25 @@ int32_t xdem_set_max_strain_rate(xdem_world w, double r) {
   return XDEM_OK;
 }
 
+int32_t xdem_get_newton_stats(xdem_world w, int64_t out[3]) {
+  if (!w || !out) return XDEM_ERR_ARGUMENT;
+  WorldScalars s;
+  CK(w, read_scalars(w, &s));
+  out[0] = (int64_t)s.newton_solves;
+  out[1] = (int64_t)s.newton_iters;
+  out[2] = (int64_t)s.newton_capped;
+  return XDEM_OK;
+}
+
+int32_t xdem_reset_newton_stats(xdem_world w) {
+  if (!w) return XDEM_ERR_ARGUMENT;
+  WorldScalars s;
+  CK(w, read_scalars(w, &s));
+  s.newton_solves = s.newton_iters = s.newton_capped = 0;
+  CK(w, write_scalars(w, &s));
+  return XDEM_OK;
+}
+
 int32_t xdem_get_kinetic_energy(xdem_world w, double* out) {
   if (!w || !out || w->dw.n <= 0) return XDEM_ERR_ARGUMENT;
   int nb = blocks_for(w->dw.n, kReduceBlock);

@@ -326,6 +326,7 @@ __global__ void __launch_bounds__(128, LAW == LAW_CIRCLE ? 4 : 1)
   for (int o = 0; o < nold; ++o) opart[o] = old.partner[(size_t)o * n + m];
   uint32_t seen = 0;
   int k = 0;
+  uint32_t n_solves = 0, n_iters = 0, n_capped = 0;
 
   const double dt = ws.dt, kn = ws.kn, kt = ws.kt, mu = ws.mu, factor = ws.factor;
   if (grid_ok && !(w.setting[m] & SKIP_CONTACT_DETECTION)) {
@@ -411,6 +412,11 @@ __global__ void __launch_bounds__(128, LAW == LAW_CIRCLE ? 4 : 1)
             touching = contact_geometry(w.method, a, b, orad_i, w.orad[mj], off, ovel, csa, csb, g, st);
           else
             touching = contact_geometry_law<LAW>(a, b, orad_i, w.orad[mj], off, ovel, csa, csb, g, st);
+          if (LAW != LAW_CIRCLE && g.iters > 0) {
+            n_solves++;
+            n_iters += g.iters;
+            n_capped += g.iters >= kNewtonCap ? 1u : 0u;
+          }
           if (!touching) continue;
           if (k >= K) {
             st |= ST_CAPACITY;
@@ -507,6 +513,12 @@ __global__ void __launch_bounds__(128, LAW == LAW_CIRCLE ? 4 : 1)
   }
   cur.count[m] = k;
   raise(w.status, st);
+  if (n_solves) {
+    WorldScalars* wsm = w.ws;
+    atomicAdd(&wsm->newton_solves, (unsigned long long)n_solves);
+    atomicAdd(&wsm->newton_iters, (unsigned long long)n_iters);
+    if (n_capped) atomicAdd(&wsm->newton_capped, (unsigned long long)n_capped);
+  }
 }
 
 // small insertion sorts of keys held in local arrays

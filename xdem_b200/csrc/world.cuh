@@ -53,6 +53,10 @@ struct WorldScalars {
   int32_t stop;        // set once a run's stop condition is met
   int32_t steps_done;  // steps completed in the current run
   int32_t flips;       // slot-set swaps executed in the current run
+  int32_t pad_;
+  // closest-approach Newton statistics since the last reset: solves,
+  // iterations, solves stopped by the iteration cap
+  unsigned long long newton_solves, newton_iters, newton_capped;
 };
 
 struct DevWorld {

@@ -330,6 +330,16 @@ class World(WorldBase):
         return {self.lib.xdem_profile_name(i).decode(): (int(launches[i]), float(ms[i]))
                 for i in range(k) if launches[i]}
 
+    def newton_stats(self):
+        """(solves, iterations, capped solves) of the closest-approach Newton
+        iteration since creation or the last reset."""
+        out = (C.c_int64 * 3)()
+        self._check(self.lib.xdem_get_newton_stats(self.h, out), "newton_stats")
+        return int(out[0]), int(out[1]), int(out[2])
+
+    def reset_newton_stats(self):
+        self._check(self.lib.xdem_reset_newton_stats(self.h), "reset_newton_stats")
+
     def launch_count(self):
         v = C.c_int64(0)
         self._check(self.lib.xdem_launch_count(self.h, C.byref(v)), "launch_count")
