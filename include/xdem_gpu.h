@@ -334,6 +334,26 @@ int32_t xdem_pair_geometry(int32_t npairs, int32_t ellipse_method, int32_t preci
                            const double* offset /* npairs*4: ox, oy, ovx, ovy */,
                            double* out /* npairs*17 */);
 
+/* ---- allocation-free stress ---------------------------------------------- */
+/* No counterpart in the reference.  For callers that cannot allocate device
+   memory (code inside a CUDA graph being captured, hosts that own a fixed
+   device budget, real-time loops that must not take allocator locks): the box
+   stress sum_c F_c (x) b_c / area (the sum of BaseWorld::updateTotalStress)
+   from per-contact force (fx, fy) and branch vector (bx, by) arrays the caller
+   holds on the device; stress receives xx, xy, yx, yy on the device.  All
+   pointers are device pointers; work is queued on cuda_stream (NULL = the
+   default stream) and is not waited for.  Uses no cudaMalloc: its partial sums
+   live in a fixed array of the library (128 KiB on every GPU that loads it,
+   held until exit), so at most xdem_total_stress_noalloc_max_contacts()
+   contacts per call (4,194,304; more returns XDEM_ERR_CAPACITY), and calls
+   that may overlap on the GPU race on that array and must be ordered by the
+   caller.  The first call on a device looks the array up for that device:
+   make it with the device current and before any stream capture begins. */
+int32_t xdem_total_stress_noalloc(int64_t ncontacts, const double* fx, const double* fy,
+                                  const double* bx, const double* by, double area,
+                                  double* stress, void* cuda_stream);
+int64_t xdem_total_stress_noalloc_max_contacts(void);
+
 /* ---- packing generation (host only, no GPU) ------------------------------ */
 /* Random sequential addition of discs of the given bounding radii into the
    box [xmin,xmax]x[ymin,ymax] without overlap; seeded, deterministic.

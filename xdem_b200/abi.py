@@ -225,6 +225,9 @@ def load_library(path=LIB_PATH):
         "xdem_launch_count": (C.c_int32, [W, P(C.c_int64)]),
         "xdem_timer_start": (C.c_int32, [W]),
         "xdem_timer_stop": (C.c_int32, [W, _d]),
+        "xdem_total_stress_noalloc": (C.c_int32, [C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,
+                                                  C.c_void_p, C.c_double, C.c_void_p, C.c_void_p]),
+        "xdem_total_stress_noalloc_max_contacts": (C.c_int64, []),
         "xdem_host_alloc": (C.c_void_p, [C.c_int64]),
         "xdem_host_free": (None, [C.c_void_p]),
         "xdem_pair_geometry": (C.c_int32, [C.c_int32, C.c_int32, C.c_int32, _d, _d, _d, _d]),
