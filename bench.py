@@ -220,17 +220,24 @@ def ncu_traffic_per_particle(kernel):
     return None
 
 
-def update_kernel_bytes(n, contacts, prm):
-    """Algorithmic DRAM bytes of one k_update_contacts launch.
-    Per particle: the owner's state (pos 16, vel 16, rot 8, spin 8, radius 8,
-    aspect 8, outer radius 8, setting 4, up-level 4, shape 4, history count 4)
-    = 88 B, written once: new history count 4 B, incoming counter 4 B.
-    Per contact: previous history read (partner 4, normal 16, shear 16,
-    damping 8) = 44 B; new record written (partner 4, normal 16, shear 16,
-    damping 8, force 16, two torques 16, branch vector 16) = 92 B; partner's
-    incoming reference 4 B + counter 4 B = 8 B.  Neighbour reads of other
-    particles' state are counted once with the owner (they hit L2)."""
-    return 96.0 * n + 144.0 * contacts
+def kernel_bytes(kernel, n, contacts, pairs):
+    """Algorithmic DRAM bytes of one launch of a contact-update kernel, with
+    every particle's data counted once (neighbour re-reads hit L2).
+    k_candidates: per particle the screening data (position 16, id 4,
+      setting 4, up-level 4, radius 8, outer radius 8) and the old history's
+      partner ids (4 per contact), written: slot count 4 + seen mask 4;
+      per listed pair a 16 B entry.
+    k_pair_forces: per particle the state the geometry reads (position 16,
+      velocity 16, orientation 8, spin 8, radius 8, aspect 8, outer radius 8,
+      shape 4, mass 8, setting 4, id 4) = 92 B; per listed pair its entry 16 B;
+      per contact the previous history (partner 4, normal 16, shear 16,
+      damping 8 = 44 B), the new record (partner 4, normal 16, shear 16,
+      damping 8, force 16, torques 16, branch vector 16 = 92 B) and the
+      partner's incoming reference and counter (8 B); per listed pair that
+      does not touch, an empty-slot mark (4 B)."""
+    if kernel == "k_candidates":
+        return 44.0 * n + 4.0 * contacts + 16.0 * pairs
+    return 92.0 * n + 16.0 * pairs + 144.0 * contacts + 4.0 * max(pairs - contacts, 0)
 
 
 def _cpu_child(path, steps, warmup, threads, budget_s):
@@ -399,13 +406,15 @@ def main():
     w.run(args.steps, ctl)
     prof = w.profile()
     w.set_profiling(False)
-    top = max(prof.items(), key=lambda kv: kv[1][1])
-    upd = prof.get("k_update_contacts", top[1])
+    # the dominant contact-update kernel
+    pairs = w.pair_count()
+    kname = max(("k_candidates", "k_pair_forces"), key=lambda k: prof.get(k, (1, 0.0))[1])
+    upd = prof[kname]
     avg_s = upd[1] / upd[0] / 1e3
-    alg_bytes = update_kernel_bytes(n, contacts, work["params"])
+    alg_bytes = kernel_bytes(kname, n, contacts, pairs)
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / avg_s / 1e9
-    traffic_pp = ncu_traffic_per_particle("k_update_contacts")
+    traffic_pp = ncu_traffic_per_particle(kname)
     step_ms = sum(v[1] for v in prof.values()) / args.steps
     shares = {k: round(v[1] / sum(x[1] for x in prof.values()), 4) for k, v in prof.items()}
 
@@ -468,7 +477,8 @@ def main():
         "gpu_launches": int(launches),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_kind,
-                     "kernel": "k_update_contacts", "algorithmic_bytes_per_launch": alg_bytes,
+                     "kernel": kname, "algorithmic_bytes_per_launch": alg_bytes,
+                     "pairs_per_step": pairs,
                      "avg_launch_ms": avg_s * 1e3,
                      "traffic": None if traffic_pp is None else traffic_pp * n},
         "kernel_share": shares, "profiled_ms_per_step": step_ms,

@@ -125,7 +125,7 @@ typedef struct xdem_params {
   int32_t world_kind;        /* enum xdem_world_kind */
   int32_t ellipse_method;    /* enum xdem_ellipse_method */
   int32_t precision;         /* enum xdem_precision */
-  int32_t max_contacts;      /* history slots per particle (<= 32), 0 = default (16) */
+  int32_t max_contacts;      /* history slots per particle (<= 32), 0 = default (24) */
   double dt;
   double xmin, xmax, ymin, ymax;
   double normal_stiffness, shear_stiffness, restitution_coeff, frictional_coeff;
@@ -260,6 +260,9 @@ int32_t xdem_get_kinetic_energy(xdem_world w, double* out);
    (NewtonRaphsonForQuartic, EllipticParticle.cpp:613-626) */
 int32_t xdem_get_newton_stats(xdem_world w, int64_t out[3]);
 int32_t xdem_reset_newton_stats(xdem_world w);
+/* pairs that passed the last candidate scan's coarse test (the pairs whose
+   geometry was evaluated) */
+int32_t xdem_get_pair_count(xdem_world w, int64_t* out);
 
 /* ---- sub-steps (each one reference method) ----------------------------- */
 /* PeriodicBoundaryWorld::modifyParticlePosition (PeriodicBoundaryWorld.cpp:129-142)

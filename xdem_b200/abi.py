@@ -200,6 +200,7 @@ def load_library(path=LIB_PATH):
         "xdem_get_kinetic_energy": (C.c_int32, [W, _d]),
         "xdem_get_newton_stats": (C.c_int32, [W, P(C.c_int64)]),
         "xdem_reset_newton_stats": (C.c_int32, [W]),
+        "xdem_get_pair_count": (C.c_int32, [W, P(C.c_int64)]),
         "xdem_modify_particle_position": (C.c_int32, [W]),
         "xdem_apply_background_velocity": (C.c_int32, [W]),
         "xdem_remove_background_velocity": (C.c_int32, [W]),

@@ -11,6 +11,7 @@
 
 #include "../../include/xdem_gpu.h"
 #include "kernels.cuh"
+#include "pairs.cuh"
 #include "resort.cuh"
 
 using namespace xdem;
@@ -18,7 +19,7 @@ using namespace xdem;
 namespace {
 
 constexpr int kBlock = 128;
-constexpr int kDefaultSlots = 16;
+constexpr int kDefaultSlots = 24;
 // steps between memory-order refreshes; odd, so that a captured chunk (one
 // re-sort + kResortEvery steps) swaps the slot sets an even number of times
 constexpr int kResortEvery = 31;
@@ -113,14 +114,15 @@ cudaError_t download(T* dst, const T* src, size_t count, cudaStream_t s) {
 
 // ---- per-kernel timing ------------------------------------------------------
 enum KernelKind {
-  KK_MODIFY = 0, KK_BIN, KK_SCAN, KK_SCATTER, KK_UPDATE, KK_COLLECT, KK_INTEGRATE, KK_RATTLERS,
-  KK_STRESS_PARTIAL, KK_STRESS_FINAL, KK_END_OF_STEP, KK_SCALE, KK_BACKGROUND, KK_KE, KK_RESORT,
-  KK_STAGE, KK_COUNT
+  KK_MODIFY = 0, KK_BIN, KK_SCAN, KK_SCATTER, KK_CANDIDATES, KK_PAIRS, KK_FINISH, KK_COLLECT,
+  KK_INTEGRATE, KK_RATTLERS, KK_STRESS_PARTIAL, KK_STRESS_FINAL, KK_END_OF_STEP, KK_SCALE,
+  KK_BACKGROUND, KK_KE, KK_RESORT, KK_STAGE, KK_COUNT
 };
 const char* const kKindNames[KK_COUNT] = {
-    "k_modify_position", "k_bin", "k_scan", "k_scatter", "k_update_contacts", "k_collect",
-    "k_integrate", "k_rattlers", "k_stress_partial", "k_stress_final", "k_end_of_step",
-    "k_scale_positions", "k_background_velocity", "k_kinetic_energy", "k_resort", "k_stage"};
+    "k_modify_position", "k_bin", "k_scan", "k_scatter", "k_candidates", "k_pair_forces",
+    "k_finish_slots", "k_collect", "k_integrate", "k_rattlers", "k_stress_partial",
+    "k_stress_final", "k_end_of_step", "k_scale_positions", "k_background_velocity",
+    "k_kinetic_energy", "k_resort", "k_stage"};
 
 void prof_begin(xdem_world_s* w, int kind) {
   if (!w->prof_on) return;
@@ -171,26 +173,25 @@ void launch_find(xdem_world_s* w) {
   LAUNCH(w, KK_SCATTER, k_scatter<<<nb, kBlock, 0, w->stream>>>(w->dw));
 }
 
+// updateContacts as candidate scan, per-pair forces, and history carry-over
+// (pairs.cuh); the pair kernel runs a grid-stride loop over the listed pairs
+template <bool FOLD_BG, int LAW>
+void launch_update_phases(xdem_world_s* w, int record) {
+  const int nb = blocks_for(w->dw.n, 128);
+  const int pb = 148 * 16;
+  LAUNCH(w, KK_CANDIDATES, k_candidates<LAW><<<nb, 128, 0, w->stream>>>(w->dw, w->par));
+  LAUNCH(w, KK_PAIRS,
+         k_pair_forces<FOLD_BG, LAW><<<pb, 128, 0, w->stream>>>(w->dw, w->par, record));
+  LAUNCH(w, KK_FINISH, k_finish_slots<<<nb, 128, 0, w->stream>>>(w->dw, w->par));
+}
+
 template <bool FOLD_BG>
 void launch_update_law(xdem_world_s* w, int record) {
-  const int nb = blocks_for(w->dw.n, 128);
   switch (w->law) {
-    case LAW_CIRCLE:
-      LAUNCH(w, KK_UPDATE, k_update_contacts<FOLD_BG, LAW_CIRCLE>
-                               <<<nb, 128, 0, w->stream>>>(w->dw, w->par, record));
-      break;
-    case LAW_CLOSEST:
-      LAUNCH(w, KK_UPDATE, k_update_contacts<FOLD_BG, LAW_CLOSEST>
-                               <<<nb, 128, 0, w->stream>>>(w->dw, w->par, record));
-      break;
-    case LAW_INTERSECTION:
-      LAUNCH(w, KK_UPDATE, k_update_contacts<FOLD_BG, LAW_INTERSECTION>
-                               <<<nb, 128, 0, w->stream>>>(w->dw, w->par, record));
-      break;
-    default:
-      LAUNCH(w, KK_UPDATE, k_update_contacts<FOLD_BG, LAW_ANY>
-                               <<<nb, 128, 0, w->stream>>>(w->dw, w->par, record));
-      break;
+    case LAW_CIRCLE: launch_update_phases<FOLD_BG, LAW_CIRCLE>(w, record); break;
+    case LAW_CLOSEST: launch_update_phases<FOLD_BG, LAW_CLOSEST>(w, record); break;
+    case LAW_INTERSECTION: launch_update_phases<FOLD_BG, LAW_INTERSECTION>(w, record); break;
+    default: launch_update_phases<FOLD_BG, LAW_ANY>(w, record); break;
   }
 }
 
@@ -555,6 +556,10 @@ int32_t xdem_set_particles(xdem_world w, const xdem_particles* P) {
   CK(w, B.alloc(&d.incnt, n));
   CK(w, B.alloc(&d.inref, ks));
   CK(w, cudaMemsetAsync(d.incnt, 0, sizeof(int32_t) * n, s));
+  CK(w, B.alloc(&d.seen, n));
+  CK(w, B.alloc(&d.pairs, ks));
+  CK(w, B.alloc(&d.npairs, 1));
+  CK(w, cudaMemsetAsync(d.npairs, 0, sizeof(int32_t), s));
   w->partial_blocks = blocks_for(n, kReduceBlock);
   CK(w, B.alloc(&d.partials, 4 * (size_t)w->partial_blocks + 4));
   // memory order starts as id order
@@ -724,7 +729,8 @@ int32_t xdem_get_contacts(xdem_world w, xdem_contacts* C) {
   CK(w, download(mpos.data(), w->dw.mpos, n, q));
   CK(w, cudaStreamSynchronize(q));
   int64_t total = 0;
-  for (int m = 0; m < n; ++m) total += std::min(cnt[m], K);
+  for (int m = 0; m < n; ++m)
+    for (int s = 0; s < std::min(cnt[m], K); ++s) total += partner[(size_t)s * n + m] >= 0;
   C->count = total;
   if (C->capacity < total) return XDEM_ERR_CAPACITY;
   std::vector<double2> nn(ks), sh(ks), b(ks), cp(ks), bv1(ks), bv2(ks), fn(ks), ft(ks);
@@ -747,7 +753,8 @@ int32_t xdem_get_contacts(xdem_world w, xdem_contacts* C) {
     const int m = mpos[i];
     const int c = std::min(cnt[m], K);
     order.clear();
-    for (int s = 0; s < c; ++s) order.push_back({partner[(size_t)s * n + m], s});
+    for (int s = 0; s < c; ++s)
+      if (partner[(size_t)s * n + m] >= 0) order.push_back({partner[(size_t)s * n + m], s});
     std::sort(order.begin(), order.end());
     for (auto& o : order) {
       size_t ci = (size_t)o.second * n + m;
@@ -797,11 +804,14 @@ int32_t xdem_get_force_and_torque(xdem_world w, double* fx, double* fy, double* 
 
 int32_t xdem_count_contacts(xdem_world w, int64_t* out) {
   if (!w || !out || w->dw.n <= 0) return XDEM_ERR_ARGUMENT;
-  std::vector<int32_t> cnt(w->dw.n);
-  CK(w, download(cnt.data(), w->dw.slots[w->par].count, w->dw.n, w->stream));
+  const int n = w->dw.n, K = w->dw.K;
+  std::vector<int32_t> cnt(n), partner((size_t)K * n);
+  CK(w, download(cnt.data(), w->dw.slots[w->par].count, n, w->stream));
+  CK(w, download(partner.data(), w->dw.slots[w->par].partner, (size_t)K * n, w->stream));
   CK(w, cudaStreamSynchronize(w->stream));
   int64_t t = 0;
-  for (int c : cnt) t += std::min(c, w->dw.K);
+  for (int m = 0; m < n; ++m)
+    for (int s = 0; s < std::min(cnt[m], K); ++s) t += partner[(size_t)s * n + m] >= 0;
   *out = t;
   return XDEM_OK;
 }
@@ -929,6 +939,14 @@ int32_t xdem_get_newton_stats(xdem_world w, int64_t out[3]) {
   out[0] = (int64_t)s.newton_solves;
   out[1] = (int64_t)s.newton_iters;
   out[2] = (int64_t)s.newton_capped;
+  return XDEM_OK;
+}
+
+int32_t xdem_get_pair_count(xdem_world w, int64_t* out) {
+  if (!w || !out) return XDEM_ERR_ARGUMENT;
+  WorldScalars s;
+  CK(w, read_scalars(w, &s));
+  *out = s.last_pairs;
   return XDEM_OK;
 }
 

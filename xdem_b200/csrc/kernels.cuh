@@ -304,223 +304,6 @@ __device__ __forceinline__ PState load_state(const DevWorld& w, const WorldScala
   return p;
 }
 
-template <bool FOLD_BG, int LAW>
-__global__ void __launch_bounds__(128, LAW == LAW_CIRCLE ? 4 : 1)
-    k_update_contacts(DevWorld w, int par, int record) {
-  const WorldScalars& ws = *w.ws;
-  if (ws.stop) return;
-  int m = blockIdx.x * blockDim.x + threadIdx.x;
-  if (m >= w.n) return;
-  const int n = w.n, K = w.K;
-  const Slots& old = w.slots[par];
-  const Slots& cur = w.slots[par ^ 1];
-  uint32_t st = 0;
-  Grid G = grid_of(ws, w.nx_cap, w.ny_cap);
-  bool grid_ok = (G.nx >= 3 && G.ny >= 3);
-  const int id_i = w.id_of[m];
-
-  // previous history of this owner
-  int nold = old.count[m];
-  if (nold > K) nold = K;
-  int opart[kMaxSlots];
-  for (int o = 0; o < nold; ++o) opart[o] = old.partner[(size_t)o * n + m];
-  uint32_t seen = 0;
-  int k = 0;
-  uint32_t n_solves = 0, n_iters = 0, n_capped = 0;
-
-  const double dt = ws.dt, kn = ws.kn, kt = ws.kt, mu = ws.mu, factor = ws.factor;
-  if (grid_ok && !(w.setting[m] & SKIP_CONTACT_DETECTION)) {
-    PState a = load_state<FOLD_BG>(w, ws, m);
-    double2 csa = make_double2(0.0, 0.0);
-    if (LAW != LAW_CIRCLE && a.shape == SHAPE_ELLIPSE) csa = make_double2(cos(a.rot), sin(a.rot));
-    const int up_i = w.up[m];
-    const double orad_i = w.orad[m];
-    int ix = cell_of(a.x, ws.xmin, G.lx, G.nx);
-    int iy = cell_of(a.y, ws.ymin, G.ly, G.ny);
-    int ncand[3] = {0, 0, 0};
-    for (int dx = -1; dx <= 1; ++dx) {
-      int jx = ix + dx;
-      if (jx == -1) jx = G.nx - 1;
-      else if (jx == G.nx) jx = 0;
-      for (int dy = -1; dy <= 1; ++dy) {
-        int jy = iy + dy;
-        int c, kind = CAND_REGULAR;
-        if (w.kind == WORLD_LE && (jy == -1 || jy == G.ny)) {
-          if (jy == -1) {
-            c = G.ncell + G.nx + jx;
-            kind = CAND_BOTTOM;
-          } else {
-            c = G.ncell + jx;
-            kind = CAND_TOP;
-          }
-        } else {
-          if (jy == -1) jy = G.ny - 1;
-          else if (jy == G.ny) jy = 0;
-          c = jy * G.nx + jx;
-        }
-        int q0 = w.cell_start[c], q1 = w.cell_start[c + 1];
-        for (int q = q0; q < q1; ++q) {
-          int mj = w.cell_mem[q];
-          int id_j = w.id_of[mj];
-          if (id_j <= id_i) continue;
-          if (w.setting[mj] & SKIP_CONTACT_DETECTION) continue;
-          if (w.up[mj] == up_i) continue;
-          if (ncand[kind] + 1 >= kCandidateCap) {
-            st |= ST_CAPACITY;
-            continue;
-          }
-          ncand[kind]++;
-          // offset of the image of j
-          double2 pj = w.pos[mj];
-          vec2<double> off, ovel = V(0.0, 0.0);
-          if (kind == CAND_REGULAR) {
-            double ox = 0.0, oy = 0.0;
-            if (pj.x - a.x > ws.xlen / 2.0) ox = -ws.xlen;
-            else if (pj.x - a.x < -ws.xlen / 2.0) ox = ws.xlen;
-            if (pj.y - a.y > ws.ylen / 2.0) oy = -ws.ylen;
-            else if (pj.y - a.y < -ws.ylen / 2.0) oy = ws.ylen;
-            off = V(ox, oy);
-          } else {
-            off = (kind == CAND_TOP) ? V(ws.shift, ws.ylen) : V(-ws.shift, -ws.ylen);
-            double t = off.x + pj.x;
-            if (t < ws.xmin) {
-              off.x += ws.xlen;
-              t += ws.xlen;
-            } else if (t > ws.xmax) {
-              off.x += -ws.xlen;
-              t -= ws.xlen;
-            }
-            if (t - a.x > ws.xlen / 2.0) off.x += -ws.xlen;
-            else if (t - a.x < -ws.xlen / 2.0) off.x += ws.xlen;
-            ovel = V((kind == CAND_TOP) ? ws.shift_vel : -ws.shift_vel, 0.0);
-          }
-          // history slot of (i, j), if any
-          int o = -1;
-          for (int z = 0; z < nold; ++z)
-            if (opart[z] == id_j) {
-              o = z;
-              break;
-            }
-          if (o >= 0) seen |= 1u << o;
-          PState b = load_state<FOLD_BG>(w, ws, mj);
-          double2 csb = make_double2(0.0, 0.0);
-          if (LAW != LAW_CIRCLE && b.shape == SHAPE_ELLIPSE && a.shape == SHAPE_ELLIPSE)
-            csb = make_double2(cos(b.rot), sin(b.rot));
-          Geom g;
-          bool touching;
-          if (LAW == LAW_ANY)
-            touching = contact_geometry(w.method, a, b, orad_i, w.orad[mj], off, ovel, csa, csb, g, st);
-          else
-            touching = contact_geometry_law<LAW>(a, b, orad_i, w.orad[mj], off, ovel, csa, csb, g, st);
-          if (LAW != LAW_CIRCLE && g.iters > 0) {
-            n_solves++;
-            n_iters += g.iters;
-            n_capped += g.iters >= kNewtonCap ? 1u : 0u;
-          }
-          if (!touching) continue;
-          if (k >= K) {
-            st |= ST_CAPACITY;
-            continue;
-          }
-          // BaseParticle::calculateContactForceAndTorque (BaseParticle.cpp:27-98)
-          vec2<double> sh, nn = g.n;
-          double damp;
-          if (o < 0) {
-            double rvn = dot(g.rv, g.n);
-            if (!is_normal(rvn)) sh = g.srv * dt;
-            else sh = g.srv * std_min(dt, g.overlap / rvn);
-            damp = damping_constant(w, factor, m, mj);
-          } else {
-            size_t oi = (size_t)o * n + m;
-            double2 on = old.n[oi], os = old.s[oi];
-            damp = old.damp[oi];
-            vec2<double> no = V(on.x, on.y);
-            double dd = dot(no, nn);
-            double de = cross(no, nn);
-            double angle = atan2(de, dd);
-            double ca = cos(angle), sa = sin(angle);
-            mat2<double> R = M(ca, -sa, sa, ca);
-            sh = R * V(os.x, os.y);
-            sh = sh + g.srv * dt;
-          }
-          vec2<double> br = V(a.x, a.y) - (V(pj.x, pj.y) + off);
-          // ContactModel_LinearDissipativeFrictioanl (…Frictional.cpp:3-46)
-          vec2<double> fn = ((-nn) * kn) * g.overlap + (-g.nrv) * damp;
-          double maxFs = len(fn) * mu;
-          vec2<double> el = (-sh) * kt;
-          vec2<double> di = (-g.srv) * damp;
-          vec2<double> fs = el + di;
-          if (len(fs) > maxFs) {
-            fs = unit(fs) * maxFs;
-            if (len(el) > maxFs) sh = (-fs) / kt;
-            else sh = (-el) / kt;
-          }
-          // ContactInformation::calculateTotalForceAndTorque (ContactInformation.h:62-68)
-          vec2<double> F = fn + fs;
-          double t1 = cross(g.bv1, F);
-          double t2 = cross(g.bv2, -F);
-          size_t ci = (size_t)k * n + m;
-          cur.partner[ci] = id_j;
-          cur.n[ci] = make_double2(nn.x, nn.y);
-          cur.s[ci] = make_double2(sh.x, sh.y);
-          cur.damp[ci] = damp;
-          cur.f[ci] = make_double2(F.x, F.y);
-          cur.t1[ci] = t1;
-          cur.t2[ci] = t2;
-          cur.b[ci] = make_double2(br.x, br.y);
-          if (record) {
-            cur.cp[ci] = make_double2(g.cp.x, g.cp.y);
-            cur.bv1[ci] = make_double2(g.bv1.x, g.bv1.y);
-            cur.bv2[ci] = make_double2(g.bv2.x, g.bv2.y);
-            cur.fn[ci] = make_double2(fn.x, fn.y);
-            cur.ft[ci] = make_double2(fs.x, fs.y);
-          }
-          // register with the partner for its force sum
-          int pos = atomicAdd(&w.incnt[mj], 1);
-          if (pos < K) w.inref[(size_t)pos * n + mj] = (uint32_t)m * (uint32_t)K + (uint32_t)k;
-          else st |= ST_CAPACITY;
-          ++k;
-        }
-      }
-    }
-  }
-  // history of pairs that were not candidates survives unchanged
-  for (int o = 0; o < nold; ++o) {
-    if (seen & (1u << o)) continue;
-    if (k >= K) {
-      st |= ST_CAPACITY;
-      break;
-    }
-    size_t oi = (size_t)o * n + m, ci = (size_t)k * n + m;
-    cur.partner[ci] = opart[o];
-    cur.n[ci] = old.n[oi];
-    cur.s[ci] = old.s[oi];
-    cur.damp[ci] = old.damp[oi];
-    cur.f[ci] = old.f[oi];
-    cur.t1[ci] = old.t1[oi];
-    cur.t2[ci] = old.t2[oi];
-    cur.b[ci] = old.b[oi];
-    cur.cp[ci] = old.cp[oi];
-    cur.bv1[ci] = old.bv1[oi];
-    cur.bv2[ci] = old.bv2[oi];
-    cur.fn[ci] = old.fn[oi];
-    cur.ft[ci] = old.ft[oi];
-    int mj = w.mpos[opart[o]];
-    int pos = atomicAdd(&w.incnt[mj], 1);
-    if (pos < K) w.inref[(size_t)pos * n + mj] = (uint32_t)m * (uint32_t)K + (uint32_t)k;
-    else st |= ST_CAPACITY;
-    ++k;
-  }
-  cur.count[m] = k;
-  raise(w.status, st);
-  if (n_solves) {
-    WorldScalars* wsm = w.ws;
-    atomicAdd(&wsm->newton_solves, (unsigned long long)n_solves);
-    atomicAdd(&wsm->newton_iters, (unsigned long long)n_iters);
-    if (n_capped) atomicAdd(&wsm->newton_capped, (unsigned long long)n_capped);
-  }
-}
-
 // small insertion sorts of keys held in local arrays
 template <class T>
 __device__ __forceinline__ void isort(T* key, int cnt) {
@@ -569,8 +352,13 @@ __global__ void __launch_bounds__(128) k_collect(DevWorld w, int par) {
     }
   }
   {
-    uint32_t key[kMaxSlots];  // partner id << 5 | slot
-    for (int a = 0; a < nown; ++a) key[a] = ((uint32_t)cur.partner[(size_t)a * n + p] << 5) | a;
+    uint32_t key[kMaxSlots];  // partner id << 5 | slot; empty slots skipped
+    int nk = 0;
+    for (int a = 0; a < nown; ++a) {
+      int partner = cur.partner[(size_t)a * n + p];
+      if (partner >= 0) key[nk++] = ((uint32_t)partner << 5) | a;
+    }
+    nown = nk;
     isort(key, nown);
     for (int a = 0; a < nown; ++a) {
       size_t ci = (size_t)(key[a] & 31u) * n + p;
@@ -717,9 +505,12 @@ constexpr int kReduceBlock = 256;
 __device__ __forceinline__ void own_stress(const DevWorld& w, const Slots& cur, int p, bool sub,
                                            double2 bvo, mat2<double>& s) {
   const int n = w.n, K = w.K;
-  int cnt = min(cur.count[p], K);
+  int c0 = min(cur.count[p], K), cnt = 0;
   uint32_t key[kMaxSlots];
-  for (int a = 0; a < cnt; ++a) key[a] = ((uint32_t)cur.partner[(size_t)a * n + p] << 5) | a;
+  for (int a = 0; a < c0; ++a) {
+    int partner = cur.partner[(size_t)a * n + p];
+    if (partner >= 0) key[cnt++] = ((uint32_t)partner << 5) | a;
+  }
   isort(key, cnt);
   for (int a = 0; a < cnt; ++a) {
     size_t ci = (size_t)(key[a] & 31u) * n + p;

@@ -1,0 +1,336 @@
+// pairs.cuh — updateContacts in three phases (rows a3-a15).
+//
+//   k_candidates    one thread per owner: the reference's 3x3 candidate scan
+//                   (PeriodicBoundaryWorld.cpp:47-84, LeesEdwardsBoundaryWorld.cpp:
+//                   128-204) with its filters and 200-candidate cap, a cheap
+//                   coarse test, and a compact list of the pairs that pass;
+//   k_pair_forces   one thread per listed pair: image offset, contact geometry,
+//                   history, contact force and torques (BaseParticle.cpp:27-98),
+//                   written to the owner's slot for that pair;
+//   k_finish_slots  one thread per owner: carries over the history of pairs
+//                   that were not candidates this step, as the reference's map
+//                   entries survive.
+// Splitting the light scan from the heavy geometry keeps warps full on the
+// FP64 ellipse solvers.  A candidate rejected by the coarse test is still a
+// candidate: its history is dropped, as the reference erases it
+// (BaseParticle.cpp:95).  A listed pair that turns out not to touch leaves an
+// empty slot (partner -1) that every reader skips.
+#pragma once
+#include "kernels.cuh"
+
+namespace xdem {
+
+// image offset of candidate j (PeriodicBoundaryWorld.cpp:97-101,
+// LeesEdwardsBoundaryWorld.cpp:233-279)
+__device__ __forceinline__ void image_offset(const WorldScalars& ws, int kind, double2 pi,
+                                             double2 pj, vec2<double>& off, vec2<double>& ovel) {
+  ovel = V(0.0, 0.0);
+  if (kind == CAND_REGULAR) {
+    double ox = 0.0, oy = 0.0;
+    if (pj.x - pi.x > ws.xlen / 2.0) ox = -ws.xlen;
+    else if (pj.x - pi.x < -ws.xlen / 2.0) ox = ws.xlen;
+    if (pj.y - pi.y > ws.ylen / 2.0) oy = -ws.ylen;
+    else if (pj.y - pi.y < -ws.ylen / 2.0) oy = ws.ylen;
+    off = V(ox, oy);
+    return;
+  }
+  off = (kind == CAND_TOP) ? V(ws.shift, ws.ylen) : V(-ws.shift, -ws.ylen);
+  double t = off.x + pj.x;
+  if (t < ws.xmin) {
+    off.x += ws.xlen;
+    t += ws.xlen;
+  } else if (t > ws.xmax) {
+    off.x += -ws.xlen;
+    t -= ws.xlen;
+  }
+  if (t - pi.x > ws.xlen / 2.0) off.x += -ws.xlen;
+  else if (t - pi.x < -ws.xlen / 2.0) off.x += ws.xlen;
+  ovel = V((kind == CAND_TOP) ? ws.shift_vel : -ws.shift_vel, 0.0);
+}
+
+// Cheap test that every contact passes: the full overlap test for two circles
+// (CircularParticle.cpp:73-77, same operations), the bounding-circle test for
+// two ellipses (takeCoarseDetection, BaseParticle.h:131-132).  Other pairs
+// (mixed shapes, clumps) go on to the dispatcher, which rejects or flags them.
+template <int LAW>
+__device__ __forceinline__ bool coarse_pass(int shape_i, int shape_j, double r_i, double r_j,
+                                            double orad_i, double orad_j, double2 pi, double2 pj,
+                                            vec2<double> off) {
+  vec2<double> pa = V(pi.x, pi.y);
+  vec2<double> pb = V(pj.x, pj.y) + off;
+  bool circles = LAW == LAW_CIRCLE || (shape_i == SHAPE_CIRCLE && shape_j == SHAPE_CIRCLE);
+  bool ellipses = LAW == LAW_CLOSEST || LAW == LAW_INTERSECTION ||
+                  (shape_i == SHAPE_ELLIPSE && shape_j == SHAPE_ELLIPSE);
+  if (circles) {
+    double distance = len(pb - pa);
+    return !((r_i + r_j) - distance < 0.0);
+  }
+  if (ellipses) return (orad_i + orad_j) > sqrt(len2(pa - pb));
+  return true;
+}
+
+// ---- phase A --------------------------------------------------------------------
+template <int LAW>
+__global__ void __launch_bounds__(128) k_candidates(DevWorld w, int par) {
+  const WorldScalars& ws = *w.ws;
+  if (ws.stop) return;
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool valid = m < w.n;
+  const int n = w.n, K = w.K;
+  const Slots& old = w.slots[par];
+  const Slots& cur = w.slots[par ^ 1];
+  uint32_t st = 0;
+  int nlist = 0;
+  int32_t list_mj[kMaxSlots];
+  int8_t list_kind[kMaxSlots];
+  if (valid) {
+    Grid G = grid_of(ws, w.nx_cap, w.ny_cap);
+    const int id_i = w.id_of[m];
+    int nold = min(old.count[m], K);
+    int32_t opart[kMaxSlots];
+    for (int o = 0; o < nold; ++o) opart[o] = old.partner[(size_t)o * n + m];
+    uint32_t seen = 0;
+    if (G.nx >= 3 && G.ny >= 3 && !(w.setting[m] & SKIP_CONTACT_DETECTION)) {
+      const double2 pi = w.pos[m];
+      const int up_i = w.up[m];
+      const int shape_i = (LAW == LAW_ANY) ? w.shape[m] : 0;
+      const double r_i = w.rad[m], orad_i = w.orad[m];
+      int ix = cell_of(pi.x, ws.xmin, G.lx, G.nx);
+      int iy = cell_of(pi.y, ws.ymin, G.ly, G.ny);
+      int ncand[3] = {0, 0, 0};
+      for (int dx = -1; dx <= 1; ++dx) {
+        int jx = ix + dx;
+        if (jx == -1) jx = G.nx - 1;
+        else if (jx == G.nx) jx = 0;
+        for (int dy = -1; dy <= 1; ++dy) {
+          int jy = iy + dy;
+          int c, kind = CAND_REGULAR;
+          if (w.kind == WORLD_LE && (jy == -1 || jy == G.ny)) {
+            if (jy == -1) {
+              c = G.ncell + G.nx + jx;
+              kind = CAND_BOTTOM;
+            } else {
+              c = G.ncell + jx;
+              kind = CAND_TOP;
+            }
+          } else {
+            if (jy == -1) jy = G.ny - 1;
+            else if (jy == G.ny) jy = 0;
+            c = jy * G.nx + jx;
+          }
+          const int q0 = w.cell_start[c], q1 = w.cell_start[c + 1];
+          for (int q = q0; q < q1; ++q) {
+            const int mj = w.cell_mem[q];
+            const int id_j = w.id_of[mj];
+            if (id_j <= id_i) continue;
+            if (w.setting[mj] & SKIP_CONTACT_DETECTION) continue;
+            if (w.up[mj] == up_i) continue;
+            if (ncand[kind] + 1 >= kCandidateCap) {
+              st |= ST_CAPACITY;
+              continue;
+            }
+            ncand[kind]++;
+            for (int z = 0; z < nold; ++z)
+              if (opart[z] == id_j) seen |= 1u << z;
+            const double2 pj = w.pos[mj];
+            vec2<double> off, ovel;
+            image_offset(ws, kind, pi, pj, off, ovel);
+            const int shape_j = (LAW == LAW_ANY) ? w.shape[mj] : 0;
+            const double r_j = (LAW == LAW_CIRCLE || LAW == LAW_ANY) ? w.rad[mj] : 0.0;
+            const double orad_j = (LAW == LAW_CIRCLE) ? 0.0 : w.orad[mj];
+            if (!coarse_pass<LAW>(shape_i, shape_j, r_i, r_j, orad_i, orad_j, pi, pj, off)) continue;
+            if (nlist >= K) {
+              st |= ST_CAPACITY;
+              continue;
+            }
+            list_mj[nlist] = mj;
+            list_kind[nlist] = (int8_t)kind;
+            ++nlist;
+          }
+        }
+      }
+    }
+    cur.count[m] = nlist;
+    w.seen[m] = seen;
+  }
+  // reserve room in the pair list for the whole warp at once
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  int incl = nlist;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int v = __shfl_up_sync(full, incl, o);
+    if (lane >= o) incl += v;
+  }
+  int total = __shfl_sync(full, incl, 31);
+  int base = 0;
+  if (lane == 31 && total > 0) base = atomicAdd(w.npairs, total);
+  base = __shfl_sync(full, base, 31);
+  int at = base + incl - nlist;
+  for (int s = 0; s < nlist; ++s) w.pairs[at + s] = PairEntry{m, list_mj[s], list_kind[s], s};
+  raise(w.status, st);
+}
+
+// ---- phase B --------------------------------------------------------------------
+template <bool FOLD_BG, int LAW>
+__global__ void __launch_bounds__(128) k_pair_forces(DevWorld w, int par, int record) {
+  const WorldScalars& ws = *w.ws;
+  if (ws.stop) return;
+  const int n = w.n, K = w.K;
+  const Slots& old = w.slots[par];
+  const Slots& cur = w.slots[par ^ 1];
+  const int npairs = *w.npairs;
+  const double dt = ws.dt, kn = ws.kn, kt = ws.kt, mu = ws.mu, factor = ws.factor;
+  uint32_t st = 0;
+  uint32_t n_solves = 0, n_iters = 0, n_capped = 0;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < npairs; t += gridDim.x * blockDim.x) {
+    const PairEntry e = w.pairs[t];
+    const int m = e.m, mj = e.mj;
+    const size_t ci = (size_t)e.slot * n + m;
+    PState a = load_state<FOLD_BG>(w, ws, m);
+    PState b = load_state<FOLD_BG>(w, ws, mj);
+    vec2<double> off, ovel;
+    image_offset(ws, e.kind, make_double2(a.x, a.y), make_double2(b.x, b.y), off, ovel);
+    double2 csa = make_double2(0.0, 0.0), csb = make_double2(0.0, 0.0);
+    if (LAW != LAW_CIRCLE && a.shape == SHAPE_ELLIPSE && b.shape == SHAPE_ELLIPSE) {
+      csa = make_double2(cos(a.rot), sin(a.rot));
+      csb = make_double2(cos(b.rot), sin(b.rot));
+    }
+    Geom g;
+    bool touching;
+    if (LAW == LAW_ANY)
+      touching = contact_geometry(w.method, a, b, w.orad[m], w.orad[mj], off, ovel, csa, csb, g, st);
+    else
+      touching = contact_geometry_law<LAW>(a, b, w.orad[m], w.orad[mj], off, ovel, csa, csb, g, st);
+    if (LAW != LAW_CIRCLE && g.iters > 0) {
+      n_solves++;
+      n_iters += g.iters;
+      n_capped += g.iters >= kNewtonCap ? 1u : 0u;
+    }
+    if (!touching) {
+      cur.partner[ci] = -1;
+      continue;
+    }
+    const int id_j = w.id_of[mj];
+    // history slot of the pair, if any
+    const int nold = min(old.count[m], K);
+    int o = -1;
+    for (int z = 0; z < nold; ++z)
+      if (old.partner[(size_t)z * n + m] == id_j) {
+        o = z;
+        break;
+      }
+    // BaseParticle::calculateContactForceAndTorque (BaseParticle.cpp:27-98)
+    vec2<double> sh, nn = g.n;
+    double damp;
+    if (o < 0) {
+      double rvn = dot(g.rv, g.n);
+      if (!is_normal(rvn)) sh = g.srv * dt;
+      else sh = g.srv * std_min(dt, g.overlap / rvn);
+      damp = damping_constant(w, factor, m, mj);
+    } else {
+      size_t oi = (size_t)o * n + m;
+      double2 on = old.n[oi], os = old.s[oi];
+      damp = old.damp[oi];
+      vec2<double> no = V(on.x, on.y);
+      double dd = dot(no, nn);
+      double de = cross(no, nn);
+      double angle = atan2(de, dd);
+      double ca = cos(angle), sa = sin(angle);
+      mat2<double> R = M(ca, -sa, sa, ca);
+      sh = R * V(os.x, os.y);
+      sh = sh + g.srv * dt;
+    }
+    vec2<double> br = V(a.x, a.y) - (V(b.x, b.y) + off);
+    // ContactModel_LinearDissipativeFrictioanl (…Frictional.cpp:3-46)
+    vec2<double> fn = ((-nn) * kn) * g.overlap + (-g.nrv) * damp;
+    double maxFs = len(fn) * mu;
+    vec2<double> el = (-sh) * kt;
+    vec2<double> di = (-g.srv) * damp;
+    vec2<double> fs = el + di;
+    if (len(fs) > maxFs) {
+      fs = unit(fs) * maxFs;
+      if (len(el) > maxFs) sh = (-fs) / kt;
+      else sh = (-el) / kt;
+    }
+    // ContactInformation::calculateTotalForceAndTorque (ContactInformation.h:62-68)
+    vec2<double> F = fn + fs;
+    cur.partner[ci] = id_j;
+    cur.n[ci] = make_double2(nn.x, nn.y);
+    cur.s[ci] = make_double2(sh.x, sh.y);
+    cur.damp[ci] = damp;
+    cur.f[ci] = make_double2(F.x, F.y);
+    cur.t1[ci] = cross(g.bv1, F);
+    cur.t2[ci] = cross(g.bv2, -F);
+    cur.b[ci] = make_double2(br.x, br.y);
+    if (record) {
+      cur.cp[ci] = make_double2(g.cp.x, g.cp.y);
+      cur.bv1[ci] = make_double2(g.bv1.x, g.bv1.y);
+      cur.bv2[ci] = make_double2(g.bv2.x, g.bv2.y);
+      cur.fn[ci] = make_double2(fn.x, fn.y);
+      cur.ft[ci] = make_double2(fs.x, fs.y);
+    }
+    // register with the partner for its force sum
+    int pos = atomicAdd(&w.incnt[mj], 1);
+    if (pos < K) w.inref[(size_t)pos * n + mj] = (uint32_t)m * (uint32_t)K + (uint32_t)e.slot;
+    else st |= ST_CAPACITY;
+  }
+  raise(w.status, st);
+  if (n_solves) {
+    WorldScalars* wsm = w.ws;
+    atomicAdd(&wsm->newton_solves, (unsigned long long)n_solves);
+    atomicAdd(&wsm->newton_iters, (unsigned long long)n_iters);
+    if (n_capped) atomicAdd(&wsm->newton_capped, (unsigned long long)n_capped);
+  }
+}
+
+// ---- phase C --------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_finish_slots(DevWorld w, int par) {
+  const WorldScalars& ws = *w.ws;
+  if (ws.stop) return;
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m == 0) {  // phase B has consumed the list
+    w.ws->last_pairs = *w.npairs;
+    *w.npairs = 0;
+  }
+  if (m >= w.n) return;
+  const int n = w.n, K = w.K;
+  const Slots& old = w.slots[par];
+  const Slots& cur = w.slots[par ^ 1];
+  uint32_t st = 0;
+  const uint32_t seen = w.seen[m];
+  const int nold = min(old.count[m], K);
+  int k = cur.count[m];
+  for (int o = 0; o < nold; ++o) {
+    size_t oi = (size_t)o * n + m;
+    int partner = old.partner[oi];
+    if (partner < 0 || (seen & (1u << o))) continue;
+    if (k >= K) {
+      st |= ST_CAPACITY;
+      break;
+    }
+    size_t ci = (size_t)k * n + m;
+    cur.partner[ci] = partner;
+    cur.n[ci] = old.n[oi];
+    cur.s[ci] = old.s[oi];
+    cur.damp[ci] = old.damp[oi];
+    cur.f[ci] = old.f[oi];
+    cur.t1[ci] = old.t1[oi];
+    cur.t2[ci] = old.t2[oi];
+    cur.b[ci] = old.b[oi];
+    cur.cp[ci] = old.cp[oi];
+    cur.bv1[ci] = old.bv1[oi];
+    cur.bv2[ci] = old.bv2[oi];
+    cur.fn[ci] = old.fn[oi];
+    cur.ft[ci] = old.ft[oi];
+    int mj = w.mpos[partner];
+    int pos = atomicAdd(&w.incnt[mj], 1);
+    if (pos < K) w.inref[(size_t)pos * n + mj] = (uint32_t)m * (uint32_t)K + (uint32_t)k;
+    else st |= ST_CAPACITY;
+    ++k;
+  }
+  cur.count[m] = k;
+  raise(w.status, st);
+}
+
+}  // namespace xdem

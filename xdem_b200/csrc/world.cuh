@@ -53,10 +53,16 @@ struct WorldScalars {
   int32_t stop;        // set once a run's stop condition is met
   int32_t steps_done;  // steps completed in the current run
   int32_t flips;       // slot-set swaps executed in the current run
-  int32_t pad_;
+  int32_t last_pairs;  // pairs listed by the last candidate scan
   // closest-approach Newton statistics since the last reset: solves,
   // iterations, solves stopped by the iteration cap
   unsigned long long newton_solves, newton_iters, newton_capped;
+};
+
+// one pair listed by the candidate scan: owner position, partner position,
+// image kind and the owner's slot for it
+struct PairEntry {
+  int32_t m, mj, kind, slot;
 };
 
 struct DevWorld {
@@ -105,6 +111,9 @@ struct DevWorld {
   Slots slots[2];
   int32_t* incnt;   // [n] contacts owned by lower ids
   uint32_t* inref;  // [K*n] owner position*K + slot of those contacts
+  uint32_t* seen;   // [n] old slots whose pair was a candidate this step
+  PairEntry* pairs; // [K*n] pairs that passed the candidate scan
+  int32_t* npairs;  // number of listed pairs
   // scalars, status, scratch
   WorldScalars* ws;
   uint32_t* status;

@@ -337,6 +337,12 @@ class World(WorldBase):
         self._check(self.lib.xdem_get_newton_stats(self.h, out), "newton_stats")
         return int(out[0]), int(out[1]), int(out[2])
 
+    def pair_count(self):
+        """Pairs that passed the last candidate scan (geometry evaluated)."""
+        v = C.c_int64(0)
+        self._check(self.lib.xdem_get_pair_count(self.h, C.byref(v)), "pair_count")
+        return int(v.value)
+
     def reset_newton_stats(self):
         self._check(self.lib.xdem_reset_newton_stats(self.h), "reset_newton_stats")
 
