@@ -58,9 +58,11 @@ __device__ __forceinline__ bool coarse_pass(int shape_i, int shape_j, double r_i
                                             vec2<double> off) {
   vec2<double> pa = V(pi.x, pi.y);
   vec2<double> pb = V(pj.x, pj.y) + off;
-  bool circles = LAW == LAW_CIRCLE || (shape_i == SHAPE_CIRCLE && shape_j == SHAPE_CIRCLE);
-  bool ellipses = LAW == LAW_CLOSEST || LAW == LAW_INTERSECTION ||
-                  (shape_i == SHAPE_ELLIPSE && shape_j == SHAPE_ELLIPSE);
+  // a world-wide law decides; only a mixed world looks at the two shapes
+  const bool circles =
+      LAW == LAW_CIRCLE || (LAW == LAW_ANY && shape_i == SHAPE_CIRCLE && shape_j == SHAPE_CIRCLE);
+  const bool ellipses = LAW == LAW_CLOSEST || LAW == LAW_INTERSECTION ||
+                        (LAW == LAW_ANY && shape_i == SHAPE_ELLIPSE && shape_j == SHAPE_ELLIPSE);
   if (circles) {
     double distance = len(pb - pa);
     return !((r_i + r_j) - distance < 0.0);
