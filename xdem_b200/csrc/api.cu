@@ -529,6 +529,10 @@ int32_t xdem_set_particles(xdem_world w, const xdem_particles* P) {
   CK(w, B.alloc(&d.cell_start, cells + 1));
   CK(w, B.alloc(&d.tile_sum, cells / kScanTile + 2));
   CK(w, B.alloc(&d.cell_mem, 2 * (size_t)n));
+  CK(w, B.alloc(&d.cell_pos, 2 * (size_t)n));
+  CK(w, B.alloc(&d.cell_rec, 2 * (size_t)n));
+  CK(w, B.alloc(&d.cs, n));
+  d.screen_r = w->law == LAW_CIRCLE ? d.rad : d.orad;
   CK(w, B.alloc(&d.pcell, n));
   CK(w, B.alloc(&d.prank, n));
   CK(w, B.alloc(&d.gcell, n));
@@ -575,6 +579,7 @@ int32_t xdem_set_particles(xdem_world w, const xdem_particles* P) {
   PermList& L = w->perm;
   L = PermList{};
   auto add = [&](void* p, int esize) {
+    if (L.count >= kMaxPermArrays) return;  // sized for the arrays listed below
     L.base[L.count] = p;
     L.esize[L.count] = esize;
     L.count++;
@@ -601,6 +606,8 @@ int32_t xdem_set_particles(xdem_world w, const xdem_particles* P) {
   add(d.vel, 16);
   add(d.branch, 16);
   add(d.force, 16);
+  add(d.pcell, 4);  // read by the candidate scan's history test after a re-sort
+  add(d.gcell, 4);
   size_t off = 0;
   for (int a = 0; a < L.count; ++a) {
     L.offset[a] = off;

@@ -408,7 +408,8 @@ enum : int { LAW_CIRCLE = 0, LAW_CLOSEST = 1, LAW_INTERSECTION = 2, LAW_ANY = 3 
 
 // calculateContactGeometry for a world whose bodies all have one shape; the
 // clump test stays (a clump's geometry is never a contact, GluedParticle.cpp:133-140)
-template <int LAW>
+// (SCREENED: the caller has already applied the bounding-circle test)
+template <int LAW, bool SCREENED = false>
 __device__ __forceinline__ bool contact_geometry_law(const PState& a, const PState& b,
                                                      double orad_a, double orad_b,
                                                      vec2<double> off, vec2<double> ovel,
@@ -418,8 +419,10 @@ __device__ __forceinline__ bool contact_geometry_law(const PState& a, const PSta
   if (a.shape == SHAPE_CLUMP || b.shape == SHAPE_CLUMP) return false;
   if (LAW == LAW_CIRCLE) return circle_circle(a, b, off, ovel, g);
   // EllipticParticle::calculateContactGeometry (EllipticParticle.cpp:16-32)
-  vec2<double> dd = V(a.x, a.y) - (V(b.x, b.y) + off);
-  if (!((orad_a + orad_b) > sqrt(len2(dd)))) return false;
+  if (!SCREENED) {
+    vec2<double> dd = V(a.x, a.y) - (V(b.x, b.y) + off);
+    if (!((orad_a + orad_b) > sqrt(len2(dd)))) return false;
+  }
   if (LAW == LAW_INTERSECTION)
     return ellipse_intersection(a, b, off, ovel, cs_a.x, cs_a.y, cs_b.x, cs_b.y, g);
   return ellipse_closest(a, b, off, ovel, cs_a.x, cs_a.y, cs_b.x, cs_b.y, g, st);

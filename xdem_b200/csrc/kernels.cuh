@@ -257,9 +257,22 @@ __global__ void k_scatter(DevWorld w) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= w.n) return;
   if (G.nx < 3 || G.ny < 3) return;
-  w.cell_mem[w.cell_start[w.pcell[i]] + w.prank[i]] = i;
+  const double2 p = w.pos[i];
+  ScreenRec r;
+  r.r = w.screen_r[i];
+  r.id = (w.setting[i] & SKIP_CONTACT_DETECTION) ? -1 : w.id_of[i];
+  r.up = w.up[i];
+  int q = w.cell_start[w.pcell[i]] + w.prank[i];
+  w.cell_mem[q] = i;
+  w.cell_pos[q] = p;
+  w.cell_rec[q] = r;
   int gc = w.gcell[i];
-  if (gc >= 0) w.cell_mem[w.cell_start[gc] + w.grank[i]] = i;
+  if (gc >= 0) {
+    q = w.cell_start[gc] + w.grank[i];
+    w.cell_mem[q] = i;
+    w.cell_pos[q] = p;
+    w.cell_rec[q] = r;
+  }
 }
 
 // ---------------------------------------------------------------------------

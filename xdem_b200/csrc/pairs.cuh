@@ -72,6 +72,49 @@ __device__ __forceinline__ bool coarse_pass(int shape_i, int shape_j, double r_i
 }
 
 // ---- phase A --------------------------------------------------------------------
+// The nine cells of the reference's scan, in its order, with the image kind
+// of each (LeesEdwardsBoundaryWorld.cpp:128-204 for the ghost rows).
+struct Neighbourhood {
+  int cell[9];
+  int kind[9];
+};
+
+__device__ __forceinline__ Neighbourhood neighbourhood(const Grid& G, int world_kind, int ix,
+                                                       int iy) {
+  Neighbourhood nb;
+  int k = 0;
+  for (int dx = -1; dx <= 1; ++dx) {
+    int jx = ix + dx;
+    if (jx == -1) jx = G.nx - 1;
+    else if (jx == G.nx) jx = 0;
+    for (int dy = -1; dy <= 1; ++dy, ++k) {
+      int jy = iy + dy;
+      if (world_kind == WORLD_LE && (jy == -1 || jy == G.ny)) {
+        if (jy == -1) {
+          nb.cell[k] = G.ncell + G.nx + jx;
+          nb.kind[k] = CAND_BOTTOM;
+        } else {
+          nb.cell[k] = G.ncell + jx;
+          nb.kind[k] = CAND_TOP;
+        }
+      } else {
+        if (jy == -1) jy = G.ny - 1;
+        else if (jy == G.ny) jy = 0;
+        nb.cell[k] = jy * G.nx + jx;
+        nb.kind[k] = CAND_REGULAR;
+      }
+    }
+  }
+  return nb;
+}
+
+// One thread per owner m.  Cell entries are read from the cell-ordered
+// screening copies (cell_rec, cell_pos), so a neighbour cell is one
+// contiguous run of records.  Old slots whose partner sits in one of the nine
+// cells (and passes the same filters) are marked seen: such a pair was a
+// candidate, so its history is replaced or dropped rather than carried over.
+// For an all-ellipse world the thread also leaves (cos, sin) of its
+// orientation for the pair kernel, computed once per body instead of per pair.
 template <int LAW>
 __global__ void __launch_bounds__(128) k_candidates(DevWorld w, int par) {
   const WorldScalars& ws = *w.ws;
@@ -83,73 +126,75 @@ __global__ void __launch_bounds__(128) k_candidates(DevWorld w, int par) {
   const Slots& cur = w.slots[par ^ 1];
   uint32_t st = 0;
   int nlist = 0;
-  int32_t list_mj[kMaxSlots];
-  int8_t list_kind[kMaxSlots];
+  int32_t list_q[kMaxSlots];
+  int32_t list_code[kMaxSlots];
   if (valid) {
+    if (LAW == LAW_CLOSEST || LAW == LAW_INTERSECTION) {
+      const double r = w.rot[m];
+      w.cs[m] = make_double2(cos(r), sin(r));
+    }
     Grid G = grid_of(ws, w.nx_cap, w.ny_cap);
     const int id_i = w.id_of[m];
-    int nold = min(old.count[m], K);
-    int32_t opart[kMaxSlots];
-    for (int o = 0; o < nold; ++o) opart[o] = old.partner[(size_t)o * n + m];
+    const int nold = min(old.count[m], K);
     uint32_t seen = 0;
     if (G.nx >= 3 && G.ny >= 3 && !(w.setting[m] & SKIP_CONTACT_DETECTION)) {
       const double2 pi = w.pos[m];
       const int up_i = w.up[m];
       const int shape_i = (LAW == LAW_ANY) ? w.shape[m] : 0;
       const double r_i = w.rad[m], orad_i = w.orad[m];
-      int ix = cell_of(pi.x, ws.xmin, G.lx, G.nx);
-      int iy = cell_of(pi.y, ws.ymin, G.ly, G.ny);
+      const int ix = cell_of(pi.x, ws.xmin, G.lx, G.nx);
+      const int iy = cell_of(pi.y, ws.ymin, G.ly, G.ny);
+      const Neighbourhood nb = neighbourhood(G, w.kind, ix, iy);
       int ncand[3] = {0, 0, 0};
-      for (int dx = -1; dx <= 1; ++dx) {
-        int jx = ix + dx;
-        if (jx == -1) jx = G.nx - 1;
-        else if (jx == G.nx) jx = 0;
-        for (int dy = -1; dy <= 1; ++dy) {
-          int jy = iy + dy;
-          int c, kind = CAND_REGULAR;
-          if (w.kind == WORLD_LE && (jy == -1 || jy == G.ny)) {
-            if (jy == -1) {
-              c = G.ncell + G.nx + jx;
-              kind = CAND_BOTTOM;
-            } else {
-              c = G.ncell + jx;
-              kind = CAND_TOP;
-            }
-          } else {
-            if (jy == -1) jy = G.ny - 1;
-            else if (jy == G.ny) jy = 0;
-            c = jy * G.nx + jx;
+#pragma unroll 1
+      for (int k = 0; k < 9; ++k) {
+        const int c = nb.cell[k], kind = nb.kind[k];
+        const int q0 = w.cell_start[c], q1 = w.cell_start[c + 1];
+        for (int q = q0; q < q1; ++q) {
+          const ScreenRec rj = w.cell_rec[q];
+          if (rj.id <= id_i) continue;  // also drops SKIP_CONTACT_DETECTION
+          if (rj.up == up_i) continue;
+          if (ncand[kind] + 1 >= kCandidateCap) {
+            st |= ST_CAPACITY;
+            continue;
           }
-          const int q0 = w.cell_start[c], q1 = w.cell_start[c + 1];
-          for (int q = q0; q < q1; ++q) {
+          ncand[kind]++;
+          const double2 pj = w.cell_pos[q];
+          vec2<double> off, ovel;
+          image_offset(ws, kind, pi, pj, off, ovel);
+          bool pass;
+          if (LAW == LAW_ANY) {
             const int mj = w.cell_mem[q];
-            const int id_j = w.id_of[mj];
-            if (id_j <= id_i) continue;
-            if (w.setting[mj] & SKIP_CONTACT_DETECTION) continue;
-            if (w.up[mj] == up_i) continue;
-            if (ncand[kind] + 1 >= kCandidateCap) {
-              st |= ST_CAPACITY;
-              continue;
-            }
-            ncand[kind]++;
-            for (int z = 0; z < nold; ++z)
-              if (opart[z] == id_j) seen |= 1u << z;
-            const double2 pj = w.pos[mj];
-            vec2<double> off, ovel;
-            image_offset(ws, kind, pi, pj, off, ovel);
-            const int shape_j = (LAW == LAW_ANY) ? w.shape[mj] : 0;
-            const double r_j = (LAW == LAW_CIRCLE || LAW == LAW_ANY) ? w.rad[mj] : 0.0;
-            const double orad_j = (LAW == LAW_CIRCLE) ? 0.0 : w.orad[mj];
-            if (!coarse_pass<LAW>(shape_i, shape_j, r_i, r_j, orad_i, orad_j, pi, pj, off)) continue;
-            if (nlist >= K) {
-              st |= ST_CAPACITY;
-              continue;
-            }
-            list_mj[nlist] = mj;
-            list_kind[nlist] = (int8_t)kind;
-            ++nlist;
+            pass = coarse_pass<LAW>(shape_i, w.shape[mj], r_i, w.rad[mj], orad_i, w.orad[mj], pi,
+                                    pj, off);
+          } else {
+            pass = coarse_pass<LAW>(0, 0, r_i, rj.r, orad_i, rj.r, pi, pj, off);
           }
+          if (!pass) continue;
+          if (nlist >= K) {
+            st |= ST_CAPACITY;
+            continue;
+          }
+          int oslot = kNoOldSlot;
+          for (int z = 0; z < nold; ++z)
+            if (old.partner[(size_t)z * n + m] == rj.id) oslot = z;
+          list_q[nlist] = q;
+          list_code[nlist] = kind | (nlist << 8) | (oslot << 16);
+          ++nlist;
         }
+      }
+      // old partners among the candidates
+      for (int z = 0; z < nold; ++z) {
+        const int p = old.partner[(size_t)z * n + m];
+        if (p < 0) continue;
+        const int mj = w.mpos[p];
+        if (w.setting[mj] & SKIP_CONTACT_DETECTION) continue;
+        if (w.up[mj] == up_i) continue;
+        const int cr = w.pcell[mj], cg = w.gcell[mj];
+        bool hit = false;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) hit |= nb.cell[k] == cr || nb.cell[k] == cg;
+        if (hit) seen |= 1u << z;
       }
     }
     cur.count[m] = nlist;
@@ -169,13 +214,13 @@ __global__ void __launch_bounds__(128) k_candidates(DevWorld w, int par) {
   if (lane == 31 && total > 0) base = atomicAdd(w.npairs, total);
   base = __shfl_sync(full, base, 31);
   int at = base + incl - nlist;
-  for (int s = 0; s < nlist; ++s) w.pairs[at + s] = PairEntry{m, list_mj[s], list_kind[s], s};
+  for (int s = 0; s < nlist; ++s) w.pairs[at + s] = PairEntry{m, w.cell_mem[list_q[s]], list_code[s], 0};
   raise(w.status, st);
 }
 
 // ---- phase B --------------------------------------------------------------------
 template <bool FOLD_BG, int LAW>
-__global__ void __launch_bounds__(128) k_pair_forces(DevWorld w, int par, int record) {
+__global__ void __launch_bounds__(128, 4) k_pair_forces(DevWorld w, int par, int record) {
   const WorldScalars& ws = *w.ws;
   if (ws.stop) return;
   const int n = w.n, K = w.K;
@@ -188,22 +233,30 @@ __global__ void __launch_bounds__(128) k_pair_forces(DevWorld w, int par, int re
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < npairs; t += gridDim.x * blockDim.x) {
     const PairEntry e = w.pairs[t];
     const int m = e.m, mj = e.mj;
-    const size_t ci = (size_t)e.slot * n + m;
+    const int kind = e.code & 0xff, slot = (e.code >> 8) & 0xff, o = (e.code >> 16) & 0xff;
+    const size_t ci = (size_t)slot * n + m;
     PState a = load_state<FOLD_BG>(w, ws, m);
     PState b = load_state<FOLD_BG>(w, ws, mj);
     vec2<double> off, ovel;
-    image_offset(ws, e.kind, make_double2(a.x, a.y), make_double2(b.x, b.y), off, ovel);
-    double2 csa = make_double2(0.0, 0.0), csb = make_double2(0.0, 0.0);
-    if (LAW != LAW_CIRCLE && a.shape == SHAPE_ELLIPSE && b.shape == SHAPE_ELLIPSE) {
-      csa = make_double2(cos(a.rot), sin(a.rot));
-      csb = make_double2(cos(b.rot), sin(b.rot));
-    }
+    image_offset(ws, kind, make_double2(a.x, a.y), make_double2(b.x, b.y), off, ovel);
     Geom g;
     bool touching;
-    if (LAW == LAW_ANY)
+    if (LAW == LAW_ANY) {
+      double2 csa = make_double2(0.0, 0.0), csb = make_double2(0.0, 0.0);
+      if (a.shape == SHAPE_ELLIPSE && b.shape == SHAPE_ELLIPSE) {
+        csa = make_double2(cos(a.rot), sin(a.rot));
+        csb = make_double2(cos(b.rot), sin(b.rot));
+      }
       touching = contact_geometry(w.method, a, b, w.orad[m], w.orad[mj], off, ovel, csa, csb, g, st);
-    else
-      touching = contact_geometry_law<LAW>(a, b, w.orad[m], w.orad[mj], off, ovel, csa, csb, g, st);
+    } else {
+      // the scan has applied the coarse test of this pair
+      double2 csa = make_double2(0.0, 0.0), csb = make_double2(0.0, 0.0);
+      if (LAW != LAW_CIRCLE) {
+        csa = w.cs[m];
+        csb = w.cs[mj];
+      }
+      touching = contact_geometry_law<LAW, true>(a, b, 0.0, 0.0, off, ovel, csa, csb, g, st);
+    }
     if (LAW != LAW_CIRCLE && g.iters > 0) {
       n_solves++;
       n_iters += g.iters;
@@ -214,18 +267,10 @@ __global__ void __launch_bounds__(128) k_pair_forces(DevWorld w, int par, int re
       continue;
     }
     const int id_j = w.id_of[mj];
-    // history slot of the pair, if any
-    const int nold = min(old.count[m], K);
-    int o = -1;
-    for (int z = 0; z < nold; ++z)
-      if (old.partner[(size_t)z * n + m] == id_j) {
-        o = z;
-        break;
-      }
     // BaseParticle::calculateContactForceAndTorque (BaseParticle.cpp:27-98)
     vec2<double> sh, nn = g.n;
     double damp;
-    if (o < 0) {
+    if (o == kNoOldSlot) {
       double rvn = dot(g.rv, g.n);
       if (!is_normal(rvn)) sh = g.srv * dt;
       else sh = g.srv * std_min(dt, g.overlap / rvn);
@@ -274,7 +319,7 @@ __global__ void __launch_bounds__(128) k_pair_forces(DevWorld w, int par, int re
     }
     // register with the partner for its force sum
     int pos = atomicAdd(&w.incnt[mj], 1);
-    if (pos < K) w.inref[(size_t)pos * n + mj] = (uint32_t)m * (uint32_t)K + (uint32_t)e.slot;
+    if (pos < K) w.inref[(size_t)pos * n + mj] = (uint32_t)m * (uint32_t)K + (uint32_t)slot;
     else st |= ST_CAPACITY;
   }
   raise(w.status, st);

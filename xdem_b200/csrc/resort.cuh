@@ -11,7 +11,7 @@
 
 namespace xdem {
 
-constexpr int kMaxPermArrays = 24;
+constexpr int kMaxPermArrays = 28;
 
 struct PermList {
   void* base[kMaxPermArrays];
@@ -20,7 +20,8 @@ struct PermList {
   int count;
 };
 
-// members of each regular cell in ascending id; newpos = the sorted index
+// members of each regular cell in ascending id, their screening copies moved
+// along; newpos = the sorted index
 __global__ void k_sort_cells(DevWorld w) {
   const WorldScalars& ws = *w.ws;
   if (ws.stop) return;
@@ -29,14 +30,20 @@ __global__ void k_sort_cells(DevWorld w) {
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < G.ncell; c += gridDim.x * blockDim.x) {
     int q0 = w.cell_start[c], q1 = w.cell_start[c + 1];
     for (int a = q0 + 1; a < q1; ++a) {
-      int x = w.cell_mem[a];
-      int kx = w.id_of[x];
+      const int x = w.cell_mem[a];
+      const double2 px = w.cell_pos[a];
+      const ScreenRec rx = w.cell_rec[a];
+      const int kx = w.id_of[x];
       int b = a - 1;
       while (b >= q0 && w.id_of[w.cell_mem[b]] > kx) {
         w.cell_mem[b + 1] = w.cell_mem[b];
+        w.cell_pos[b + 1] = w.cell_pos[b];
+        w.cell_rec[b + 1] = w.cell_rec[b];
         --b;
       }
       w.cell_mem[b + 1] = x;
+      w.cell_pos[b + 1] = px;
+      w.cell_rec[b + 1] = rx;
     }
     for (int q = q0; q < q1; ++q) w.newpos[w.cell_mem[q]] = q;
   }

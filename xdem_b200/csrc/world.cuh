@@ -60,9 +60,20 @@ struct WorldScalars {
 };
 
 // one pair listed by the candidate scan: owner position, partner position,
-// image kind and the owner's slot for it
+// and packed in `code` the image kind (bits 0-7), the owner's new slot for the
+// pair (bits 8-15) and its slot in the old set, 255 when the pair is new
+// (bits 16-23)
 struct PairEntry {
-  int32_t m, mj, kind, slot;
+  int32_t m, mj, code, pad;
+};
+constexpr int kNoOldSlot = 255;
+
+// screening record of a cell entry, written in cell order by the scatter:
+// the radius of the coarse test, the id (negative when the particle skips
+// contact detection, so that one comparison applies both filters) and upLevel
+struct ScreenRec {
+  double r;
+  int32_t id, up;
 };
 
 struct DevWorld {
@@ -102,6 +113,10 @@ struct DevWorld {
   int32_t* cell_start;
   int32_t* tile_sum;  // scan tile sums
   int32_t* cell_mem;
+  double2* cell_pos;      // [2n] position of each cell entry, cell order
+  ScreenRec* cell_rec;    // [2n] screening record of each cell entry
+  double2* cs;            // [n] (cos, sin) of the orientation, this step
+  const double* screen_r; // rad for an all-circle world, orad otherwise
   int32_t* pcell;  // [n] regular cell of the particle at m
   int32_t* prank;  // [n] rank within the cell
   int32_t* gcell;  // [n] ghost cell or -1
