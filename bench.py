@@ -123,6 +123,13 @@ def workload_le_ellipses(n, seed):
     prm = make_params(abi.WORLD_LEES_EDWARDS, dt, b, inputs.KN, inputs.KT, inputs.RESTITUTION,
                       inputs.FRICTION, shift_strain_rate=rate)
     return {"particles": q, "contacts": contacts, "params": prm, "control": make_control(),
+            # the compiled reference's Newton loop (EllipticParticle.cpp:621) has no
+            # iteration cap and never returns on the few deeply overlapping pairs of
+            # this packing that cycle (the GPU run counts them as capped solves), so
+            # the CPU leg runs the C restatement, identical but for that cap
+            "cpu_kind": "port",
+            "cpu_note": "C restatement of the reference (capped Newton; the compiled reference "
+                        "does not return on this packing's cycling Newton pairs)",
             "config": {"workload": f"lees_edwards_shear_ellipses_{n}", "n_particles": n,
                        "world": "LeesEdwardsBoundaryWorld", "contact_law": "closest-approach (Newton)",
                        "aspect_ratio": "U[1,3]", "b": "{0.5,0.7}", "solid_fraction": round(phi, 4),
@@ -138,6 +145,7 @@ def workload_periodic_discs(n, seed):
     prm = make_params(abi.WORLD_PERIODIC, dt, box, inputs.KN, inputs.KT, inputs.RESTITUTION,
                       inputs.FRICTION)
     return {"particles": p, "contacts": None, "params": prm, "control": make_control(),
+            "cpu_kind": "reference", "cpu_note": "compiled reference sources (oracle/_ref)",
             "config": {"workload": f"periodic_discs_{n}", "n_particles": n,
                        "world": "PeriodicBoundaryWorld", "contact_law": "disc-disc",
                        "radii": "{0.5,0.7}", "solid_fraction": 0.70, "dt": dt, "precision": "fp64"}}
@@ -240,9 +248,10 @@ def kernel_bytes(kernel, n, contacts, pairs):
     return 92.0 * n + 16.0 * pairs + 144.0 * contacts + 4.0 * max(pairs - contacts, 0)
 
 
-def _cpu_child(path, steps, warmup, threads, budget_s):
-    """Child process: times the compiled reference (else the C restatement) on
-    the workload saved at `path`; prints one JSON line."""
+def _cpu_child(path, steps, warmup, threads, budget_s, kind):
+    """Child process: times the compiled reference (kind "reference") or the
+    C restatement (kind "port") on the workload saved at `path`; prints one
+    JSON line."""
     import oracle
     from xdem_b200 import abi
     z = np.load(path, allow_pickle=False)
@@ -250,9 +259,11 @@ def _cpu_child(path, steps, warmup, threads, budget_s):
     c = {k[2:]: z[k] for k in z.files if k.startswith("c_")}
     prm = abi.Params()
     C.memmove(C.byref(prm), z["params"].tobytes(), C.sizeof(abi.Params))
+    prm.precision = abi.PRECISION_FP64
     ctl = abi.Control()
     C.memmove(C.byref(ctl), z["control"].tobytes(), C.sizeof(abi.Control))
-    kind = "reference" if oracle.ref_available() else "port"
+    if kind == "reference" and not oracle.ref_available():
+        kind = "port"
     W = oracle.RefWorld if kind == "reference" else oracle.PortWorld
     w = W(prm, threads)
     w.set_particles(p)
@@ -271,10 +282,9 @@ def _cpu_child(path, steps, warmup, threads, budget_s):
     print(json.dumps({"value": n * k / dt, "steps": k, "kind": kind, "one_step_s": one}), flush=True)
 
 
-def run_reference(work, steps, warmup, threads, budget_s=25.0, timeout_s=900):
-    """Times the CPU reference in a child process with a watchdog (the
-    reference's Newton loop has no iteration cap and can hang on deep
-    overlaps).  Returns the child's result dict or {"error": ...}."""
+def run_cpu(work, steps, warmup, threads, budget_s=25.0, timeout_s=300):
+    """Times the CPU implementation named by work["cpu_kind"] in a child
+    process with a watchdog.  Returns the child's result dict or {"error": ...}."""
     import tempfile
     path = os.path.join(tempfile.gettempdir(), f"xdem_bench_{os.getpid()}.npz")
     arrs = {f"p_{k}": v for k, v in work["particles"].items() if isinstance(v, np.ndarray)}
@@ -284,7 +294,8 @@ def run_reference(work, steps, warmup, threads, budget_s=25.0, timeout_s=900):
     arrs["control"] = np.frombuffer(bytes(work["control"]), np.uint8)
     np.savez(path, **arrs)
     cmd = [sys.executable, os.path.abspath(__file__), "--cpu-child", path, "--steps", str(steps),
-           "--warmup", str(warmup), "--threads", str(threads), "--budget", str(budget_s)]
+           "--warmup", str(warmup), "--threads", str(threads), "--budget", str(budget_s),
+           "--cpu-kind", work["cpu_kind"]]
     env = dict(os.environ, OMP_NUM_THREADS=str(threads))
     try:
         r = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout_s, env=env)
@@ -293,74 +304,24 @@ def run_reference(work, steps, warmup, threads, budget_s=25.0, timeout_s=900):
             return {"error": f"exit {r.returncode}: {r.stderr.strip()[-300:]}"}
         return json.loads(lines[-1])
     except subprocess.TimeoutExpired:
-        return {"error": f"no result within {timeout_s} s (reference did not finish)"}
+        return {"error": f"no result within {timeout_s} s"}
     finally:
         if os.path.exists(path):
             os.remove(path)
 
 
-def main():
-    ap = argparse.ArgumentParser()
-    ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
-    ap.add_argument("--warmup", type=int, default=5)
-    ap.add_argument("--impl", default="xdem", choices=["xdem", "reference"])
-    ap.add_argument("--workload", default="le_ellipses", choices=sorted(WORKLOADS))
-    ap.add_argument("--n", type=int, default=1 << 20)
-    ap.add_argument("--seed", type=int, default=0)
-    ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--cpu-child", default=None, help=argparse.SUPPRESS)
-    ap.add_argument("--threads", type=int, default=0, help=argparse.SUPPRESS)
-    ap.add_argument("--budget", type=float, default=20.0, help=argparse.SUPPRESS)
-    args = ap.parse_args()
-    if args.cpu_child:
-        _cpu_child(args.cpu_child, args.steps, args.warmup, args.threads or os.cpu_count(),
-                   args.budget)
-        return
-
-    dist = None
-    if WORLD > 1:
-        import torch
-        import torch.distributed as dist_mod
-        from datetime import timedelta
-        dist_mod.init_process_group("gloo", timeout=timedelta(seconds=600))
-        dist = dist_mod
-
-    if args.impl == "reference":
-        if RANK != 0:
-            if dist:
-                dist.destroy_process_group()
-            return
-        work = WORKLOADS[args.workload](args.n, args.seed)
-        threads = os.cpu_count() or 1
-        res = run_reference(work, args.steps, 1, threads, budget_s=60.0)
-        if "error" in res:
-            print(json.dumps({"impl": "reference", "unavailable": res["error"]}), flush=True)
-        else:
-            v, k = res["value"], res["steps"]
-            sample = (f"{k} steps of the full {work['config']['n_particles']}-particle workload "
-                      f"after 1 warm-up step, {threads} threads")
-            line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT,
-                    "n_gpus": args.gpus, "steps": k, "warmup": 1,
-                    "ms_per_step": 1e3 * work["config"]["n_particles"] / v,
-                    "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-                    "data": "synthetic", "config": work["config"],
-                    "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": res["kind"],
-                                     "sample": sample},
-                    "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0,
-                            "d2h_bytes_per_step": 0}}
-            print(json.dumps(line), flush=True)
-        if dist:
-            dist.destroy_process_group()
-        return
-
+def measure(work, precision, args, dist, full=True):
+    """Times `args.steps` steps of the workload at the given precision.
+    full: also the per-kernel roofline pass and the end-to-end pass."""
     from xdem_b200 import abi
     from xdem_b200.world import World
 
-    work = WORKLOADS[args.workload](args.n, args.seed + RANK)
+    prm = abi.Params()
+    C.memmove(C.byref(prm), C.byref(work["params"]), C.sizeof(abi.Params))
+    prm.precision = precision
     p = work["particles"]
     n = len(p["x"])
-    w = World(work["params"])
+    w = World(prm)
     # capped Newton solves are counted and reported, not raised
     w.raise_mask = ~abi.ERR_NEWTON
     w.set_particles(p)
@@ -369,12 +330,19 @@ def main():
     ctl = work["control"]
     lib = w.lib
 
-    # warm-up
-    w.run(max(args.warmup, 3), ctl)
-
     def barrier():
         if dist:
             dist.barrier()
+
+    def max_over_ranks(v):
+        if not dist:
+            return v
+        import torch
+        t = torch.tensor([v], dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    w.run(max(args.warmup, 3), ctl)
 
     # ---- value: device time of K steps ----------------------------------
     barrier()
@@ -383,30 +351,31 @@ def main():
     w.reset_newton_stats()
     clocks.start()
     l0 = w.launch_count()
+    lib.xdem_range_push(b"bench_value")
     lib.xdem_timer_start(w.h)
     done = w.run(args.steps, ctl)
     ms = C.c_double(0.0)
     lib.xdem_timer_stop(w.h, C.byref(ms))
+    lib.xdem_range_pop()
     launches = w.launch_count() - l0
     clk = clocks.stop()
-    ms_total = ms.value
+    ms_total = max_over_ranks(ms.value)
     contacts = w.count_contacts()
     solves, iters, capped = w.newton_stats()
-    newton = {"solves_per_step": solves / max(done, 1),
-              "iterations_per_solve": iters / max(solves, 1), "capped_solves": capped}
-    if dist:
-        import torch
-        t = torch.tensor([ms_total], dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_total = float(t.item())
-    value = n * done * WORLD / (ms_total / 1e3)
+    out = {"value": n * done * WORLD / (ms_total / 1e3), "ms_per_step": ms_total / max(done, 1),
+           "done": done, "contacts": contacts, "launches": int(launches), "clocks": clk,
+           "newton": {"solves_per_step": solves / max(done, 1),
+                      "iterations_per_solve": iters / max(solves, 1), "capped_solves": capped}}
+    if not full:
+        out["status"] = w.synchronize()
+        w.close()
+        return out
 
     # ---- roofline: per-kernel events over the same number of steps ---------
     w.set_profiling(True)
     w.run(args.steps, ctl)
     prof = w.profile()
     w.set_profiling(False)
-    # the dominant contact-update kernel
     pairs = w.pair_count()
     kname = max(("k_candidates", "k_pair_forces"), key=lambda k: prof.get(k, (1, 0.0))[1])
     upd = prof[kname]
@@ -415,8 +384,15 @@ def main():
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / avg_s / 1e9
     traffic_pp = ncu_traffic_per_particle(kname)
-    step_ms = sum(v[1] for v in prof.values()) / args.steps
-    shares = {k: round(v[1] / sum(x[1] for x in prof.values()), 4) for k, v in prof.items()}
+    total = sum(x[1] for x in prof.values())
+    out["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                       "frac": achieved / peak, "peak_source": peak_kind,
+                       "kernel": kname, "algorithmic_bytes_per_launch": alg_bytes,
+                       "pairs_per_step": pairs, "avg_launch_ms": avg_s * 1e3,
+                       "traffic": None if traffic_pp is None else traffic_pp * n}
+    out["kernel_share"] = {k: round(v[1] / total, 4) for k, v in prof.items()}
+    out["kernel_ms_per_step"] = {k: round(v[1] / args.steps, 5) for k, v in prof.items()}
+    out["profiled_ms_per_step"] = total / args.steps
 
     # ---- e2e through the C-ABI with pinned host buffers ----------------------
     nbytes = 8 * n
@@ -438,56 +414,123 @@ def main():
         lib.xdem_download_state(w.h, *[C.cast(b, C.POINTER(C.c_double)) for b in bufs])
     ms_e2e = C.c_double(0.0)
     lib.xdem_timer_stop(w.h, C.byref(ms_e2e))
-    e2e_ms = ms_e2e.value
-    if dist:
-        import torch
-        t = torch.tensor([e2e_ms], dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(ms_e2e.value)
     for b in bufs:
         lib.xdem_host_free(b)
-    e2e = n * args.steps * WORLD / (e2e_ms / 1e3)
-    status = w.synchronize()
+    out["e2e"] = {"value": n * args.steps * WORLD / (e2e_ms / 1e3), "unit": UNIT,
+                  "h2d_bytes_per_step": 6 * nbytes, "d2h_bytes_per_step": 6 * nbytes}
+    out["status"] = w.synchronize()
+    w.close()
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="xdem", choices=["xdem", "reference"])
+    ap.add_argument("--workload", default="le_ellipses", choices=sorted(WORKLOADS))
+    ap.add_argument("--n", type=int, default=1 << 20)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"],
+                    help="arithmetic of the headline path (the other one is timed beside it)")
+    ap.add_argument("--no-compare", action="store_true", help="skip the second precision")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-child", default=None, help=argparse.SUPPRESS)
+    ap.add_argument("--cpu-kind", default="port", help=argparse.SUPPRESS)
+    ap.add_argument("--threads", type=int, default=0, help=argparse.SUPPRESS)
+    ap.add_argument("--budget", type=float, default=20.0, help=argparse.SUPPRESS)
+    args = ap.parse_args()
+    if args.cpu_child:
+        _cpu_child(args.cpu_child, args.steps, args.warmup, args.threads or os.cpu_count(),
+                   args.budget, args.cpu_kind)
+        return
+
+    dist = None
+    if WORLD > 1:
+        import torch
+        import torch.distributed as dist_mod
+        from datetime import timedelta
+        dist_mod.init_process_group("gloo", timeout=timedelta(seconds=600))
+        dist = dist_mod
+
+    if args.impl == "reference":
+        if RANK != 0:
+            if dist:
+                dist.destroy_process_group()
+            return
+        work = WORKLOADS[args.workload](args.n, args.seed)
+        threads = os.cpu_count() or 1
+        res = run_cpu(work, args.steps, 1, threads, budget_s=60.0)
+        if "error" in res:
+            print(json.dumps({"impl": "reference", "unavailable": res["error"]}), flush=True)
+        else:
+            v, k = res["value"], res["steps"]
+            sample = (f"{k} steps of the full {work['config']['n_particles']}-particle workload "
+                      f"after 1 warm-up step, {threads} threads; {work['cpu_note']}")
+            line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT,
+                    "n_gpus": args.gpus, "steps": k, "warmup": 1,
+                    "ms_per_step": 1e3 * work["config"]["n_particles"] / v,
+                    "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                    "data": "synthetic", "config": work["config"],
+                    "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": res["kind"],
+                                     "sample": sample},
+                    "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0,
+                            "d2h_bytes_per_step": 0}}
+            print(json.dumps(line), flush=True)
+        if dist:
+            dist.destroy_process_group()
+        return
+
+    from xdem_b200 import abi
+    prec = {"mixed": abi.PRECISION_MIXED, "fp64": abi.PRECISION_FP64}
+    other = "fp64" if args.precision == "mixed" else "mixed"
+
+    work = WORKLOADS[args.workload](args.n, args.seed + RANK)
+    n = len(work["particles"]["x"])
+    head = measure(work, prec[args.precision], args, dist, full=True)
+    cmp_ = None if args.no_compare else measure(work, prec[other], args, dist, full=False)
 
     # ---- CPU baseline (rank 0, N = 1 only) ----------------------------------
     cpu = None
     if RANK == 0 and WORLD == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        res = run_reference(work, 50, 1, threads, budget_s=20.0, timeout_s=600)
+        res = run_cpu(work, 50, 1, threads, budget_s=20.0)
         if "error" in res:
-            cpu = {"value": None, "unit": UNIT, "cores": threads, "kind": "reference",
+            cpu = {"value": None, "unit": UNIT, "cores": threads, "kind": work["cpu_kind"],
                    "sample": res["error"]}
         else:
             cpu = {"value": res["value"], "unit": UNIT, "cores": threads, "kind": res["kind"],
                    "sample": f"{res['steps']} steps of the full {n}-particle workload after 1 "
-                             f"warm-up step ({res['one_step_s']:.2f} s per step)"}
+                             f"warm-up step ({res['one_step_s']:.2f} s per step); "
+                             f"{work['cpu_note']}"}
 
     cfg = dict(work["config"])
+    cfg["precision"] = args.precision
     cfg["l2"] = "inputs larger than L2 (state + contact history resident in HBM)"
     cfg["parallelism"] = f"replicas{WORLD}" if WORLD > 1 else "single"
-    cfg["contacts"] = contacts
+    cfg["contacts"] = head["contacts"]
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": WORLD, "steps": args.steps,
-        "warmup": max(args.warmup, 3), "ms_per_step": ms_total / max(done, 1),
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": WORLD,
+        "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": head["ms_per_step"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32+f64" if args.precision == "mixed" else "f64",
         "data": "synthetic", "config": cfg,
-        "contacts_per_s": contacts * done * WORLD / (ms_total / 1e3),
-        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 6 * nbytes,
-                "d2h_bytes_per_step": 6 * nbytes},
-        "gpu_launches": int(launches),
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "peak_source": peak_kind,
-                     "kernel": kname, "algorithmic_bytes_per_launch": alg_bytes,
-                     "pairs_per_step": pairs,
-                     "avg_launch_ms": avg_s * 1e3,
-                     "traffic": None if traffic_pp is None else traffic_pp * n},
-        "kernel_share": shares, "profiled_ms_per_step": step_ms,
-        "clocks": clk, "status": status, "newton": newton,
+        "contacts_per_s": head["contacts"] * head["done"] * WORLD / (head["ms_per_step"] * head["done"] / 1e3),
+        "e2e": head["e2e"], "gpu_launches": head["launches"], "roofline": head["roofline"],
+        "kernel_share": head["kernel_share"], "kernel_ms_per_step": head["kernel_ms_per_step"],
+        "profiled_ms_per_step": head["profiled_ms_per_step"],
+        "clocks": head["clocks"], "status": head["status"], "newton": head["newton"],
         "cpu_baseline": cpu,
     }
+    if cmp_ is not None:
+        line[other] = {"value": cmp_["value"], "ms_per_step": cmp_["ms_per_step"],
+                       "contacts": cmp_["contacts"], "newton": cmp_["newton"],
+                       "clocks": cmp_["clocks"], "status": cmp_["status"]}
+        line[f"speedup_vs_{other}"] = head["value"] / cmp_["value"]
     if RANK == 0:
         print(json.dumps(line), flush=True)
-    w.close()
     if dist:
         dist.destroy_process_group()
 

@@ -323,6 +323,10 @@ int32_t xdem_launch_count(xdem_world w, int64_t* out);
    records a second one, waits for it and returns the elapsed milliseconds. */
 int32_t xdem_timer_start(xdem_world w);
 int32_t xdem_timer_stop(xdem_world w, double* ms);
+/* NVTX range around the calls in between (for profilers: ncu --nvtx
+   --nvtx-include "<name>/"); no effect without a tool attached. */
+int32_t xdem_range_push(const char* name);
+int32_t xdem_range_pop(void);
 /* Page-locked host memory for asynchronous state exchange. */
 void* xdem_host_alloc(int64_t bytes);
 void xdem_host_free(void* p);

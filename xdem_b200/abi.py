@@ -230,6 +230,8 @@ def load_library(path=LIB_PATH):
                                                   C.c_void_p, C.c_double, C.c_void_p, C.c_void_p]),
         "xdem_total_stress_noalloc_max_contacts": (C.c_int64, []),
         "xdem_host_alloc": (C.c_void_p, [C.c_int64]),
+        "xdem_range_push": (C.c_int32, [C.c_char_p]),
+        "xdem_range_pop": (C.c_int32, []),
         "xdem_host_free": (None, [C.c_void_p]),
         "xdem_pair_geometry": (C.c_int32, [C.c_int32, C.c_int32, C.c_int32, _d, _d, _d, _d]),
         "xdem_rsa_positions": (C.c_int32, [C.c_int32, _d, _d, C.c_uint64, C.c_int64, _d, _d]),

@@ -12,6 +12,7 @@
 #include "../../include/xdem_gpu.h"
 #include "kernels.cuh"
 #include "pairs.cuh"
+#include "pairs_mixed.cuh"
 #include "resort.cuh"
 
 using namespace xdem;
@@ -116,13 +117,13 @@ cudaError_t download(T* dst, const T* src, size_t count, cudaStream_t s) {
 enum KernelKind {
   KK_MODIFY = 0, KK_BIN, KK_SCAN, KK_SCATTER, KK_CANDIDATES, KK_PAIRS, KK_FINISH, KK_COLLECT,
   KK_INTEGRATE, KK_RATTLERS, KK_STRESS_PARTIAL, KK_STRESS_FINAL, KK_END_OF_STEP, KK_SCALE,
-  KK_BACKGROUND, KK_KE, KK_RESORT, KK_STAGE, KK_COUNT
+  KK_BACKGROUND, KK_KE, KK_RESORT, KK_STAGE, KK_FALLBACK, KK_COUNT
 };
 const char* const kKindNames[KK_COUNT] = {
     "k_modify_position", "k_bin", "k_scan", "k_scatter", "k_candidates", "k_pair_forces",
     "k_finish_slots", "k_collect", "k_integrate", "k_rattlers", "k_stress_partial",
     "k_stress_final", "k_end_of_step", "k_scale_positions", "k_background_velocity",
-    "k_kinetic_energy", "k_resort", "k_stage"};
+    "k_kinetic_energy", "k_resort", "k_stage", "k_pair_fallback"};
 
 void prof_begin(xdem_world_s* w, int kind) {
   if (!w->prof_on) return;
@@ -180,8 +181,16 @@ void launch_update_phases(xdem_world_s* w, int record) {
   const int nb = blocks_for(w->dw.n, 128);
   const int pb = 148 * 16;
   LAUNCH(w, KK_CANDIDATES, k_candidates<LAW><<<nb, 128, 0, w->stream>>>(w->dw, w->par));
-  LAUNCH(w, KK_PAIRS,
-         k_pair_forces<FOLD_BG, LAW><<<pb, 128, 0, w->stream>>>(w->dw, w->par, record));
+  if (w->prm.precision == XDEM_PRECISION_MIXED) {
+    LAUNCH(w, KK_PAIRS,
+           k_pair_forces_m<FOLD_BG, LAW><<<pb, 128, 0, w->stream>>>(w->dw, w->par, record));
+    if (LAW == LAW_CLOSEST || LAW == LAW_ANY)
+      LAUNCH(w, KK_FALLBACK, k_pair_fallback_m<FOLD_BG, LAW><<<148 * 4, 128, 0, w->stream>>>(
+                                 w->dw, w->par, record));
+  } else {
+    LAUNCH(w, KK_PAIRS,
+           k_pair_forces<FOLD_BG, LAW><<<pb, 128, 0, w->stream>>>(w->dw, w->par, record));
+  }
   LAUNCH(w, KK_FINISH, k_finish_slots<<<nb, 128, 0, w->stream>>>(w->dw, w->par));
 }
 
@@ -564,6 +573,9 @@ int32_t xdem_set_particles(xdem_world w, const xdem_particles* P) {
   CK(w, B.alloc(&d.pairs, ks));
   CK(w, B.alloc(&d.npairs, 1));
   CK(w, cudaMemsetAsync(d.npairs, 0, sizeof(int32_t), s));
+  CK(w, B.alloc(&d.fallback, w->prm.precision == XDEM_PRECISION_MIXED ? ks : 1));
+  CK(w, B.alloc(&d.nfallback, 1));
+  CK(w, cudaMemsetAsync(d.nfallback, 0, sizeof(int32_t), s));
   w->partial_blocks = blocks_for(n, kReduceBlock);
   CK(w, B.alloc(&d.partials, 4 * (size_t)w->partial_blocks + 4));
   // memory order starts as id order
@@ -1262,8 +1274,8 @@ void xdem_host_free(void* p) {
 // ---- single-pair geometry ------------------------------------------------------
 int32_t xdem_pair_geometry(int32_t npairs, int32_t method, int32_t precision, const double* pi,
                            const double* pj, const double* off, double* out) {
-  (void)precision;
-  if (npairs <= 0 || !pi || !pj || !off || !out) return XDEM_ERR_ARGUMENT;
+  if (npairs <= 0 || !pi || !pj || !off || !out || precision < 0 || precision > 1)
+    return XDEM_ERR_ARGUMENT;
   double *dpi = nullptr, *dpj = nullptr, *doff = nullptr, *dout = nullptr;
   uint32_t* dst = nullptr;
   uint32_t st = 0;
@@ -1277,7 +1289,10 @@ int32_t xdem_pair_geometry(int32_t npairs, int32_t method, int32_t precision, co
   if (e == cudaSuccess) e = cudaMemcpy(dpj, pj, sizeof(double) * 9 * npairs, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(doff, off, sizeof(double) * 4 * npairs, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) {
-    k_pair_geometry<<<blocks_for(npairs, 128), 128>>>(npairs, method, dpi, dpj, doff, dout, dst);
+    if (precision == XDEM_PRECISION_MIXED)
+      k_pair_geometry_m<<<blocks_for(npairs, 128), 128>>>(npairs, method, dpi, dpj, doff, dout, dst);
+    else
+      k_pair_geometry<<<blocks_for(npairs, 128), 128>>>(npairs, method, dpi, dpj, doff, dout, dst);
     e = cudaGetLastError();
   }
   if (e == cudaSuccess) e = cudaMemcpy(out, dout, sizeof(double) * 17 * npairs, cudaMemcpyDeviceToHost);

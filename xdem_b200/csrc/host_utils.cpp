@@ -5,6 +5,8 @@
 #include <cstdint>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/xdem_gpu.h"
 
 namespace {
@@ -193,6 +195,16 @@ int32_t xdem_clump_properties(int32_t nsub, const int32_t* sub_shape, const doub
     branch_x[k] = sub_x[k] - mcx;
     branch_y[k] = sub_y[k] - mcy;
   }
+  return XDEM_OK;
+}
+
+// named ranges for profilers (NVTX; no effect unless a tool is attached)
+int32_t xdem_range_push(const char* name) {
+  nvtxRangePushA(name ? name : "");
+  return XDEM_OK;
+}
+int32_t xdem_range_pop(void) {
+  nvtxRangePop();
   return XDEM_OK;
 }
 

@@ -336,9 +336,10 @@ __global__ void __launch_bounds__(128) k_finish_slots(DevWorld w, int par) {
   const WorldScalars& ws = *w.ws;
   if (ws.stop) return;
   const int m = blockIdx.x * blockDim.x + threadIdx.x;
-  if (m == 0) {  // phase B has consumed the list
+  if (m == 0) {  // phase B has consumed the lists
     w.ws->last_pairs = *w.npairs;
     *w.npairs = 0;
+    *w.nfallback = 0;
   }
   if (m >= w.n) return;
   const int n = w.n, K = w.K;

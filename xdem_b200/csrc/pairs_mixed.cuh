@@ -1,0 +1,297 @@
+// pairs_mixed.cuh — phase B of updateContacts for the mixed-precision path
+// (XDEM_PRECISION_MIXED).  Same candidate list, slots and history carry-over
+// as the FP64 path (pairs.cuh); per listed pair:
+//   geometry   geometry_mixed.cuh (FP32 with the FP64 overlap);
+//   history    the tangential spring stays FP64: its rotation with the normal
+//              (BaseParticle.cpp:67-82) takes cos/sin of the turn angle as
+//              (n_old·n, n_old×n)/|…| instead of atan2 followed by cos and sin
+//              (the same numbers, without the transcendental calls), and the
+//              increment v_t dt is added in FP64;
+//   force      ContactModel_LinearDissipativeFrictioanl (…Frictional.cpp:3-46)
+//              in FP32, written to the FP64 slot arrays.
+// Closest-approach pairs that need the reference's FP64 construction (see
+// geometry_mixed.cuh) are appended to a fallback list and evaluated by
+// k_pair_fallback_m after the main pass, so that both passes run converged
+// warps.
+#pragma once
+#include "geometry_mixed.cuh"
+#include "pairs.cuh"
+
+namespace xdem {
+
+__device__ __forceinline__ bool is_normal_f(float x) {
+  const float a = fabsf(x);
+  return a >= 1.17549435e-38f && a <= 3.40282347e38f;
+}
+
+// history, force and torques of one touching pair, written to its slot
+__device__ __forceinline__ void write_contact_m(const DevWorld& w, const WorldScalars& ws,
+                                                const PairEntry& e, const PState& a,
+                                                const PState& b, vec2<double> off,
+                                                const GeomM& g, int par, int record,
+                                                uint32_t& st) {
+  const int n = w.n, K = w.K;
+  const Slots& old = w.slots[par];
+  const Slots& cur = w.slots[par ^ 1];
+  const int m = e.m, mj = e.mj;
+  const int slot = (e.code >> 8) & 0xff, o = (e.code >> 16) & 0xff;
+  const size_t ci = (size_t)slot * n + m;
+  const double dt = ws.dt;
+  double sx, sy, damp;
+  if (o == kNoOldSlot) {
+    // new contact (BaseParticle.cpp:38-65)
+    const float rvn = g.rv.x * g.n.x + g.rv.y * g.n.y;
+    double tt = dt;
+    if (is_normal_f(rvn)) tt = std_min(dt, g.overlap / (double)rvn);
+    sx = (double)g.srv.x * tt;
+    sy = (double)g.srv.y * tt;
+    damp = damping_constant(w, ws.factor, m, mj);
+  } else {
+    const size_t oi = (size_t)o * n + m;
+    const double2 on = old.n[oi], os = old.s[oi];
+    damp = old.damp[oi];
+    const float nox = (float)on.x, noy = (float)on.y;
+    const float dd = nox * g.n.x + noy * g.n.y;
+    const float de = nox * g.n.y - noy * g.n.x;
+    const float r2 = dd * dd + de * de;
+    float ca = 1.0f, sa = 0.0f;
+    if (r2 > 0.0f) {
+      const float ir = rsqrtf(r2);
+      ca = dd * ir;
+      sa = de * ir;
+    }
+    sx = (double)ca * os.x - (double)sa * os.y + (double)g.srv.x * dt;
+    sy = (double)sa * os.x + (double)ca * os.y + (double)g.srv.y * dt;
+  }
+  const float kt = (float)ws.kt, mu = (float)ws.mu, fd = (float)damp;
+  const float kov = (float)(ws.kn * g.overlap);
+  float fnx = -g.n.x * kov - g.nrv.x * fd;
+  float fny = -g.n.y * kov - g.nrv.y * fd;
+  const float maxFs = sqrtf(fnx * fnx + fny * fny) * mu;
+  const float elx = (float)(-sx) * kt, ely = (float)(-sy) * kt;
+  float fsx = elx - g.srv.x * fd, fsy = ely - g.srv.y * fd;
+  const float fsl = sqrtf(fsx * fsx + fsy * fsy);
+  if (fsl > maxFs) {
+    const float sc = maxFs / fsl;
+    fsx *= sc;
+    fsy *= sc;
+    if (sqrtf(elx * elx + ely * ely) > maxFs) {
+      sx = (double)(-fsx) / ws.kt;
+      sy = (double)(-fsy) / ws.kt;
+    }
+  }
+  const float Fx = fnx + fsx, Fy = fny + fsy;
+  const int id_j = w.id_of[mj];
+  cur.partner[ci] = id_j;
+  cur.n[ci] = make_double2((double)g.n.x, (double)g.n.y);
+  cur.s[ci] = make_double2(sx, sy);
+  cur.damp[ci] = damp;
+  cur.f[ci] = make_double2((double)Fx, (double)Fy);
+  cur.t1[ci] = (double)(g.bv1.x * Fy - g.bv1.y * Fx);
+  cur.t2[ci] = (double)(-(g.bv2.x * Fy - g.bv2.y * Fx));
+  cur.b[ci] = make_double2(a.x - (b.x + off.x), a.y - (b.y + off.y));
+  if (record) {
+    cur.cp[ci] = make_double2(a.x + (double)g.cpo.x, a.y + (double)g.cpo.y);
+    cur.bv1[ci] = make_double2((double)g.bv1.x, (double)g.bv1.y);
+    cur.bv2[ci] = make_double2((double)g.bv2.x, (double)g.bv2.y);
+    cur.fn[ci] = make_double2((double)fnx, (double)fny);
+    cur.ft[ci] = make_double2((double)fsx, (double)fsy);
+  }
+  // register with the partner for its force sum
+  const int pos = atomicAdd(&w.incnt[mj], 1);
+  if (pos < K) w.inref[(size_t)pos * n + mj] = (uint32_t)m * (uint32_t)K + (uint32_t)slot;
+  else st |= ST_CAPACITY;
+}
+
+__device__ __forceinline__ void count_solve(uint32_t it, uint32_t& n_solves, uint32_t& n_iters) {
+  if (it > 0) {
+    n_solves++;
+    n_iters += it;
+  }
+}
+
+__device__ __forceinline__ void flush_stats(const DevWorld& w, uint32_t st, uint32_t n_solves,
+                                            uint32_t n_iters, uint32_t n_capped) {
+  raise(w.status, st);
+  if (n_solves) {
+    WorldScalars* wsm = w.ws;
+    atomicAdd(&wsm->newton_solves, (unsigned long long)n_solves);
+    atomicAdd(&wsm->newton_iters, (unsigned long long)n_iters);
+    if (n_capped) atomicAdd(&wsm->newton_capped, (unsigned long long)n_capped);
+  }
+}
+
+template <bool FOLD_BG, int LAW>
+__global__ void __launch_bounds__(128, 4) k_pair_forces_m(DevWorld w, int par, int record) {
+  const WorldScalars& ws = *w.ws;
+  if (ws.stop) return;
+  const int n = w.n;
+  const Slots& cur = w.slots[par ^ 1];
+  const int npairs = *w.npairs;
+  uint32_t st = 0, n_solves = 0, n_iters = 0, n_capped = 0;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < npairs; t += gridDim.x * blockDim.x) {
+    const PairEntry e = w.pairs[t];
+    const int m = e.m, mj = e.mj;
+    const int kind = e.code & 0xff, slot = (e.code >> 8) & 0xff;
+    const size_t ci = (size_t)slot * n + m;
+    const PState a = load_state<FOLD_BG>(w, ws, m);
+    const PState b = load_state<FOLD_BG>(w, ws, mj);
+    vec2<double> off, ovel;
+    image_offset(ws, kind, make_double2(a.x, a.y), make_double2(b.x, b.y), off, ovel);
+    GeomM g;
+    int res = PW_NONE;
+    const bool circles = LAW == LAW_CIRCLE ||
+                         (LAW == LAW_ANY && a.shape == SHAPE_CIRCLE && b.shape == SHAPE_CIRCLE);
+    const bool closest = LAW == LAW_CLOSEST ||
+                         (LAW == LAW_ANY && w.method == ELLIPSE_CLOSEST &&
+                          a.shape == SHAPE_ELLIPSE && b.shape == SHAPE_ELLIPSE);
+    if (circles) {
+      res = circle_circle_m(a, b, off, ovel, g) ? PW_CONTACT : PW_NONE;
+    } else if (closest) {
+      double2 csa, csb;
+      if (LAW == LAW_CLOSEST) {
+        csa = w.cs[m];
+        csb = w.cs[mj];
+      } else {
+        csa = make_double2(cos(a.rot), sin(a.rot));
+        csb = make_double2(cos(b.rot), sin(b.rot));
+      }
+      res = ellipse_closest_m(a, b, off, ovel, csa, csb, g);
+      if (res == PW_FALLBACK) {
+        w.fallback[atomicAdd(w.nfallback, 1)] = t;
+        continue;
+      }
+      count_solve(g.iters, n_solves, n_iters);
+    } else {
+      // intersection law (kept FP64: near tangency its quartic has a near
+      // double root), clumps and unsupported pairs: the FP64 dispatcher
+      double2 csa = make_double2(0.0, 0.0), csb = make_double2(0.0, 0.0);
+      if (LAW == LAW_INTERSECTION) {
+        csa = w.cs[m];
+        csb = w.cs[mj];
+      } else if (a.shape == SHAPE_ELLIPSE && b.shape == SHAPE_ELLIPSE) {
+        csa = make_double2(cos(a.rot), sin(a.rot));
+        csb = make_double2(cos(b.rot), sin(b.rot));
+      }
+      Geom gd;
+      bool touching;
+      if (LAW == LAW_INTERSECTION)
+        touching = contact_geometry_law<LAW_INTERSECTION, true>(a, b, 0.0, 0.0, off, ovel, csa, csb, gd, st);
+      else
+        touching = contact_geometry(w.method, a, b, w.orad[m], w.orad[mj], off, ovel, csa, csb, gd, st);
+      if (touching) geom_to_m(gd, a, g);
+      res = touching ? PW_CONTACT : PW_NONE;
+    }
+    if (res != PW_CONTACT) {
+      cur.partner[ci] = -1;
+      continue;
+    }
+    write_contact_m(w, ws, e, a, b, off, g, par, record, st);
+  }
+  flush_stats(w, st, n_solves, n_iters, n_capped);
+}
+
+// the closest-approach pairs deferred by k_pair_forces_m: the reference's FP64
+// construction (EllipticParticle.cpp:34-285), then the mixed force
+template <bool FOLD_BG, int LAW>
+__global__ void __launch_bounds__(128) k_pair_fallback_m(DevWorld w, int par, int record) {
+  const WorldScalars& ws = *w.ws;
+  if (ws.stop) return;
+  const int n = w.n;
+  const Slots& cur = w.slots[par ^ 1];
+  const int nfb = *w.nfallback;
+  uint32_t st = 0, n_solves = 0, n_iters = 0, n_capped = 0;
+  for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < nfb; f += gridDim.x * blockDim.x) {
+    const PairEntry e = w.pairs[w.fallback[f]];
+    const int m = e.m, mj = e.mj;
+    const int kind = e.code & 0xff, slot = (e.code >> 8) & 0xff;
+    const size_t ci = (size_t)slot * n + m;
+    const PState a = load_state<FOLD_BG>(w, ws, m);
+    const PState b = load_state<FOLD_BG>(w, ws, mj);
+    vec2<double> off, ovel;
+    image_offset(ws, kind, make_double2(a.x, a.y), make_double2(b.x, b.y), off, ovel);
+    double2 csa, csb;
+    if (LAW == LAW_CLOSEST) {
+      csa = w.cs[m];
+      csb = w.cs[mj];
+    } else {
+      csa = make_double2(cos(a.rot), sin(a.rot));
+      csb = make_double2(cos(b.rot), sin(b.rot));
+    }
+    Geom gd = Geom{};
+    const bool touching =
+        ellipse_closest(a, b, off, ovel, csa.x, csa.y, csb.x, csb.y, gd, st);
+    if (gd.iters > 0) {
+      n_solves++;
+      n_iters += gd.iters;
+      n_capped += gd.iters >= kNewtonCap ? 1u : 0u;
+    }
+    if (!touching) {
+      cur.partner[ci] = -1;
+      continue;
+    }
+    GeomM g;
+    geom_to_m(gd, a, g);
+    write_contact_m(w, ws, e, a, b, off, g, par, record, st);
+  }
+  flush_stats(w, st, n_solves, n_iters, n_capped);
+}
+
+// single pairs through the mixed geometry (xdem_pair_geometry with
+// XDEM_PRECISION_MIXED); same output layout as k_pair_geometry
+__global__ void k_pair_geometry_m(int npairs, int method, const double* pi, const double* pj,
+                                  const double* off, double* out, uint32_t* status) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= npairs) return;
+  const double* a = pi + 9 * k;
+  const double* b = pj + 9 * k;
+  PState A{(int)a[0], a[1], a[2], a[3], a[4], a[5], a[6], a[7], a[8]};
+  PState B{(int)b[0], b[1], b[2], b[3], b[4], b[5], b[6], b[7], b[8]};
+  const double2 csa = make_double2(cos(A.rot), sin(A.rot));
+  const double2 csb = make_double2(cos(B.rot), sin(B.rot));
+  const vec2<double> of = V(off[4 * k], off[4 * k + 1]), ov = V(off[4 * k + 2], off[4 * k + 3]);
+  uint32_t st = 0;
+  GeomM g{};
+  int res = PW_NONE;
+  if (A.shape == SHAPE_CIRCLE && B.shape == SHAPE_CIRCLE) {
+    res = circle_circle_m(A, B, of, ov, g) ? PW_CONTACT : PW_NONE;
+  } else if (method == ELLIPSE_CLOSEST && A.shape == SHAPE_ELLIPSE && B.shape == SHAPE_ELLIPSE) {
+    vec2<double> dd = V(A.x, A.y) - (V(B.x, B.y) + of);
+    if ((a[1] + b[1]) > sqrt(len2(dd))) {
+      res = ellipse_closest_m(A, B, of, ov, csa, csb, g);
+      if (res == PW_FALLBACK) {
+        Geom gd = Geom{};
+        res = ellipse_closest(A, B, of, ov, csa.x, csa.y, csb.x, csb.y, gd, st) ? PW_CONTACT : PW_NONE;
+        if (res == PW_CONTACT) geom_to_m(gd, A, g);
+      }
+    }
+  } else {
+    Geom gd = Geom{};
+    res = contact_geometry(method, A, B, a[1], b[1], of, ov, csa, csb, gd, st) ? PW_CONTACT : PW_NONE;
+    if (res == PW_CONTACT) geom_to_m(gd, A, g);
+  }
+  double* o = out + 17 * k;
+  for (int z = 0; z < 17; ++z) o[z] = 0.0;
+  o[0] = res == PW_CONTACT ? 1.0 : 0.0;
+  if (res == PW_CONTACT) {
+    o[1] = g.n.x;
+    o[2] = g.n.y;
+    o[3] = A.x + (double)g.cpo.x;
+    o[4] = A.y + (double)g.cpo.y;
+    o[5] = g.bv1.x;
+    o[6] = g.bv1.y;
+    o[7] = g.bv2.x;
+    o[8] = g.bv2.y;
+    o[9] = g.overlap;
+    o[10] = g.rv.x;
+    o[11] = g.rv.y;
+    o[12] = g.nrv.x;
+    o[13] = g.nrv.y;
+    o[14] = g.srv.x;
+    o[15] = g.srv.y;
+    o[16] = (double)g.iters;
+  }
+  if (st) atomicOr(status, st);
+}
+
+}  // namespace xdem

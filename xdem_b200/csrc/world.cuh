@@ -129,6 +129,8 @@ struct DevWorld {
   uint32_t* seen;   // [n] old slots whose pair was a candidate this step
   PairEntry* pairs; // [K*n] pairs that passed the candidate scan
   int32_t* npairs;  // number of listed pairs
+  int32_t* fallback;   // [K*n] mixed precision: listed pairs deferred to the FP64 construction
+  int32_t* nfallback;  // number of deferred pairs
   // scalars, status, scratch
   WorldScalars* ws;
   uint32_t* status;
