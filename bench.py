@@ -63,63 +63,18 @@ def log(*a):
 # ---------------------------------------------------------------------------
 def workload_le_ellipses(n, seed):
     """Lees-Edwards shear of ellipses, a/b ~ U[1,3], b in {0.5,0.7}, phi 0.85."""
-    from xdem_b200 import abi, inputs
-    from xdem_b200.world import World, make_control, make_params
+    from xdem_b200 import abi, inputs, packing
+    from xdem_b200.world import make_control, make_params
     p, box = inputs.ellipse_system(n, b=inputs.c2_b, aspect=inputs.c4_aspect, phi_rsa_circle=0.40,
                                    phi=None, seed=seed)
     dt = inputs.time_step(p)
     m_min = float(np.min(p["mass"]))
     rate = 1e-3 * math.sqrt(inputs.KN / m_min)
-    # compression: PeriodicControlWorld strain control to solid fraction 0.85,
-    # with global damping 0.1 (the reference drivers' compression setting)
-    prm_c = make_params(abi.WORLD_PERIODIC_CONTROL, dt, box, inputs.KN, inputs.KT,
-                        inputs.RESTITUTION, inputs.FRICTION, global_damping=0.1)
-    w = World(prm_c)
-    # during the fast compression a few deeply overlapping pairs send the
-    # closest-approach Newton iteration into a cycle (the reference's loop would
-    # never return there); the capped solver reports it and carries on
-    w.raise_mask = ~abi.ERR_NEWTON
-    newton_events = 0
-    w.set_particles(p)
-    area0 = (box[1] - box[0]) * (box[3] - box[2])
-    vol = float(p["volume"].sum())
-    phi0 = vol / area0
-    phi_target = 0.85
-    steps_c = 4000
-    # strain control scales the box by s = 1 + r*L*dt per step
-    # (PeriodicControlWorld.cpp:124-135); the rate is set chunk by chunk so that
-    # the compression reaches phi_target from below in about steps_c steps
-    s_step = math.sqrt(phi0 / phi_target) ** (1.0 / steps_c)
-    ctl = make_control(box_law=abi.BOX_STRAIN, reset_rattlers=False)
     t = time.time()
-    done = 0
-    while done < 3 * steps_c:
-        b = w.getBoundary()
-        L = b[1] - b[0]
-        phi = vol / (L * (b[3] - b[2]))
-        s_rem = math.sqrt(phi / phi_target)  # < 1 while below the target
-        if s_rem >= 1.0 - 1e-7:
-            break
-        left = max(1, int(math.ceil(math.log(s_rem) / math.log(s_step))))
-        chunk = min(200, left)
-        per = s_rem ** (1.0 / chunk) if chunk == left else s_step
-        ctl.p0 = ctl.p1 = (per - 1.0) / (L * dt)
-        w.run(chunk, ctl)
-        done += chunk
-    b = w.getBoundary()
-    phi = vol / ((b[1] - b[0]) * (b[3] - b[2]))
-    w.run(2000, make_control())  # relax at the final box
-    capped = w.newton_stats()[2]
-    log(f"setup: compressed phi {phi0:.3f} -> {phi:.4f} in {done} steps + 2000 relaxation steps, "
-        f"{time.time() - t:.1f}s, {capped} capped Newton solves")
-    st = w.get_state()
-    contacts = w.get_contacts()
-    b = w.getBoundary()
-    q = dict(p)
-    for k in ("x", "y", "vx", "vy", "rot", "rot_vel"):
-        q[k] = st[k].copy()
-    q["is_rattler"] = st["is_rattler"].copy()
-    w.close()
+    q, contacts, b, info = packing.compress(p, box, 0.85, dt, steps=4000, relax=2000)
+    log(f"setup: compressed phi {info['phi0']:.3f} -> {info['phi']:.4f} in {info['steps']} steps "
+        f"+ {info['relax']} relaxation steps, {time.time() - t:.1f}s, "
+        f"{info['capped_newton']} capped Newton solves")
     prm = make_params(abi.WORLD_LEES_EDWARDS, dt, b, inputs.KN, inputs.KT, inputs.RESTITUTION,
                       inputs.FRICTION, shift_strain_rate=rate)
     return {"particles": q, "contacts": contacts, "params": prm, "control": make_control(),
@@ -131,9 +86,10 @@ def workload_le_ellipses(n, seed):
             "cpu_note": "C restatement of the reference (capped Newton; the compiled reference "
                         "does not return on this packing's cycling Newton pairs)",
             "config": {"workload": f"lees_edwards_shear_ellipses_{n}", "n_particles": n,
-                       "world": "LeesEdwardsBoundaryWorld", "contact_law": "closest-approach (Newton)",
-                       "aspect_ratio": "U[1,3]", "b": "{0.5,0.7}", "solid_fraction": round(phi, 4),
-                       "shear_rate": rate, "dt": dt, "precision": "fp64"}}
+                       "world": "LeesEdwardsBoundaryWorld",
+                       "contact_law": "closest approach (Zheng-Palffy-Muhoray quartic, Newton)",
+                       "aspect_ratio": "U[1,3]", "b": "{0.5,0.7}",
+                       "solid_fraction": round(info["phi"], 4), "shear_rate": rate, "dt": dt}}
 
 
 def workload_periodic_discs(n, seed):
@@ -148,10 +104,54 @@ def workload_periodic_discs(n, seed):
             "cpu_kind": "reference", "cpu_note": "compiled reference sources (oracle/_ref)",
             "config": {"workload": f"periodic_discs_{n}", "n_particles": n,
                        "world": "PeriodicBoundaryWorld", "contact_law": "disc-disc",
-                       "radii": "{0.5,0.7}", "solid_fraction": 0.70, "dt": dt, "precision": "fp64"}}
+                       "radii": "{0.5,0.7}", "solid_fraction": 0.70, "dt": dt}}
 
 
-WORKLOADS = {"le_ellipses": workload_le_ellipses, "periodic_discs": workload_periodic_discs}
+def workload_batch_ensemble(n_systems, seed):
+    """Batched uneven ensemble: n_systems independent PeriodicBoundaryWorld
+    packings, N log-uniform in [1,000, 50,000] particles, solid fraction
+    U[0.6, 0.8]; 40 % bidisperse discs (r 0.5/0.7), 40 % ellipses (a/b ~
+    U[1,2], b in {0.5, 0.7}), 20 % clumps of 2-5 sub-discs.  Each packing is
+    made by RSA and strain-controlled compression on the GPU."""
+    from xdem_b200 import abi, inputs, packing
+    from xdem_b200.world import make_control, make_params
+    rng = np.random.default_rng(seed)
+    kinds = (["disc"] * int(round(0.4 * n_systems)) + ["ellipse"] * int(round(0.4 * n_systems)))
+    kinds += ["clump"] * (n_systems - len(kinds))
+    kinds = [kinds[i] for i in rng.permutation(n_systems)]
+    systems = []
+    t = time.time()
+    for s, kind in enumerate(kinds):
+        N = int(round(math.exp(rng.uniform(math.log(1000), math.log(50000)))))
+        phi = float(rng.uniform(0.6, 0.8))
+        if kind == "disc":
+            p, box = inputs.disc_system(N, phi_rsa=0.45, phi=None, seed=seed * 1000 + s)
+        elif kind == "ellipse":
+            p, box = inputs.ellipse_system(N, b=inputs.c2_b, aspect=inputs.c2_aspect,
+                                           phi_rsa_circle=0.40, phi=None, seed=seed * 1000 + s,
+                                           vel_sigma=0.01)
+        else:
+            p, box = inputs.clump_system(max(2, int(N / 4.5)), seed=seed * 1000 + s)
+        dt = inputs.time_step(p)
+        q, contacts, b, info = packing.compress(p, box, phi, dt, steps=1500, relax=500)
+        systems.append({"particles": q, "contacts": contacts, "box": b, "dt": dt, "kind": kind,
+                        "phi": info["phi"]})
+    n = sum(len(sy["particles"]["x"]) for sy in systems)
+    log(f"setup: {n_systems} systems, {n} particles, compressed in {time.time() - t:.1f}s")
+    prm = make_params(abi.WORLD_PERIODIC, systems[0]["dt"], systems[0]["box"], inputs.KN, inputs.KT,
+                      inputs.RESTITUTION, inputs.FRICTION)
+    counts = {k: kinds.count(k) for k in ("disc", "ellipse", "clump")}
+    return {"systems": systems, "params": prm, "control": make_control(),
+            "cpu_kind": "reference",
+            "cpu_note": "compiled reference sources (oracle/_ref) on the first systems of the batch",
+            "config": {"workload": f"batch_ensemble_{n_systems}x", "n_systems": n_systems,
+                       "n_particles": n, "world": "PeriodicBoundaryWorld (batched)",
+                       "system_kinds": counts, "particles_per_system": "log-uniform [1000, 50000]",
+                       "solid_fraction": "U[0.6, 0.8]"}}
+
+
+WORKLOADS = {"le_ellipses": workload_le_ellipses, "periodic_discs": workload_periodic_discs,
+             "batch_ensemble": workload_batch_ensemble}
 
 
 # ---------------------------------------------------------------------------
@@ -248,51 +248,84 @@ def kernel_bytes(kernel, n, contacts, pairs):
     return 92.0 * n + 16.0 * pairs + 144.0 * contacts + 4.0 * max(pairs - contacts, 0)
 
 
-def _cpu_child(path, steps, warmup, threads, budget_s, kind):
+def _cpu_child(paths, steps, warmup, threads, budget_s, kind):
     """Child process: times the compiled reference (kind "reference") or the
-    C restatement (kind "port") on the workload saved at `path`; prints one
-    JSON line."""
+    C restatement (kind "port") on the systems saved at `paths` (each stepped
+    in turn, the same number of steps); prints one JSON line."""
     import oracle
     from xdem_b200 import abi
-    z = np.load(path, allow_pickle=False)
-    p = {k[2:]: z[k] for k in z.files if k.startswith("p_")}
-    c = {k[2:]: z[k] for k in z.files if k.startswith("c_")}
-    prm = abi.Params()
-    C.memmove(C.byref(prm), z["params"].tobytes(), C.sizeof(abi.Params))
-    prm.precision = abi.PRECISION_FP64
-    ctl = abi.Control()
-    C.memmove(C.byref(ctl), z["control"].tobytes(), C.sizeof(abi.Control))
     if kind == "reference" and not oracle.ref_available():
         kind = "port"
     W = oracle.RefWorld if kind == "reference" else oracle.PortWorld
-    w = W(prm, threads)
-    w.set_particles(p)
-    if c and len(c["id_i"]):
-        w.set_contacts(c)
+    worlds, sizes = [], []
+    ctl = abi.Control()
+    for path in paths.split(","):
+        z = np.load(path, allow_pickle=False)
+        p = {k[2:]: z[k] for k in z.files if k.startswith("p_")}
+        c = {k[2:]: z[k] for k in z.files if k.startswith("c_")}
+        prm = abi.Params()
+        C.memmove(C.byref(prm), z["params"].tobytes(), C.sizeof(abi.Params))
+        prm.precision = abi.PRECISION_FP64
+        C.memmove(C.byref(ctl), z["control"].tobytes(), C.sizeof(abi.Control))
+        w = W(prm, threads)
+        w.raise_mask = ~abi.ERR_NEWTON
+        w.set_particles(p)
+        if c and len(c["id_i"]):
+            w.set_contacts(c)
+        worlds.append(w)
+        sizes.append(len(p["x"]))
     for _ in range(warmup):
-        w.run(1, ctl)
+        for w in worlds:
+            w.run(1, ctl)
     t0 = time.perf_counter()
-    w.run(1, ctl)
+    for w in worlds:
+        w.run(1, ctl)
     one = time.perf_counter() - t0
     k = max(1, min(steps, int(budget_s / max(one, 1e-6))))
     t0 = time.perf_counter()
-    w.run(k, ctl)
+    for w in worlds:
+        w.run(k, ctl)
     dt = time.perf_counter() - t0
-    n = len(p["x"])
-    print(json.dumps({"value": n * k / dt, "steps": k, "kind": kind, "one_step_s": one}), flush=True)
+    n = sum(sizes)
+    print(json.dumps({"value": n * k / dt, "steps": k, "kind": kind, "one_step_s": one,
+                      "systems": len(worlds), "particles": n}), flush=True)
 
 
-def run_cpu(work, steps, warmup, threads, budget_s=25.0, timeout_s=300):
+def _system_params(work, sy):
+    """World parameters of one system of a batch workload."""
+    from xdem_b200 import abi
+    prm = abi.Params()
+    C.memmove(C.byref(prm), C.byref(work["params"]), C.sizeof(abi.Params))
+    prm.xmin, prm.xmax, prm.ymin, prm.ymax = (float(v) for v in sy["box"])
+    prm.dt = sy["dt"]
+    return prm
+
+
+def run_cpu(work, steps, warmup, threads, budget_s=25.0, timeout_s=300, max_particles=150000):
     """Times the CPU implementation named by work["cpu_kind"] in a child
-    process with a watchdog.  Returns the child's result dict or {"error": ...}."""
+    process with a watchdog (a batch: its first systems, up to max_particles).
+    Returns the child's result dict or {"error": ...}."""
     import tempfile
-    path = os.path.join(tempfile.gettempdir(), f"xdem_bench_{os.getpid()}.npz")
-    arrs = {f"p_{k}": v for k, v in work["particles"].items() if isinstance(v, np.ndarray)}
-    if work["contacts"] is not None:
-        arrs.update({f"c_{k}": v for k, v in work["contacts"].items()})
-    arrs["params"] = np.frombuffer(bytes(work["params"]), np.uint8)
-    arrs["control"] = np.frombuffer(bytes(work["control"]), np.uint8)
-    np.savez(path, **arrs)
+    if "systems" in work:
+        items, total = [], 0
+        for sy in work["systems"]:
+            if items and total + len(sy["particles"]["x"]) > max_particles:
+                break
+            items.append((sy["particles"], sy["contacts"], _system_params(work, sy)))
+            total += len(sy["particles"]["x"])
+    else:
+        items = [(work["particles"], work["contacts"], work["params"])]
+    paths = []
+    for k, (p, c, prm) in enumerate(items):
+        path = os.path.join(tempfile.gettempdir(), f"xdem_bench_{os.getpid()}_{k}.npz")
+        arrs = {f"p_{key}": v for key, v in p.items() if isinstance(v, np.ndarray)}
+        if c is not None:
+            arrs.update({f"c_{key}": v for key, v in c.items()})
+        arrs["params"] = np.frombuffer(bytes(prm), np.uint8)
+        arrs["control"] = np.frombuffer(bytes(work["control"]), np.uint8)
+        np.savez(path, **arrs)
+        paths.append(path)
+    path = ",".join(paths)
     cmd = [sys.executable, os.path.abspath(__file__), "--cpu-child", path, "--steps", str(steps),
            "--warmup", str(warmup), "--threads", str(threads), "--budget", str(budget_s),
            "--cpu-kind", work["cpu_kind"]]
@@ -306,8 +339,58 @@ def run_cpu(work, steps, warmup, threads, budget_s=25.0, timeout_s=300):
     except subprocess.TimeoutExpired:
         return {"error": f"no result within {timeout_s} s"}
     finally:
-        if os.path.exists(path):
-            os.remove(path)
+        for p_ in paths:
+            if os.path.exists(p_):
+                os.remove(p_)
+
+
+def batch_contacts(systems, first):
+    """The systems' contact histories with ids made global."""
+    keys = systems[0]["contacts"].keys()
+    out = {}
+    for key in keys:
+        parts = []
+        for sy, f in zip(systems, first):
+            v = sy["contacts"][key]
+            parts.append(v + f if key in ("id_i", "id_j") else v)
+        out[key] = np.ascontiguousarray(np.concatenate(parts))
+    return out
+
+
+def measure_loop(work, precision, args):
+    """The batch workload as a per-system loop: one world per system on one
+    stream, each run for the K steps in turn (CUDA events around the loop)."""
+    from xdem_b200 import abi
+    from xdem_b200.world import World
+    worlds = []
+    for sy in work["systems"]:
+        prm = _system_params(work, sy)
+        prm.precision = precision
+        w = World(prm)
+        w.raise_mask = ~abi.ERR_NEWTON
+        w.set_particles(sy["particles"])
+        w.set_contacts(sy["contacts"])
+        worlds.append(w)
+    lib = worlds[0].lib
+    stream = C.c_void_p(0)
+    lib.xdem_get_stream(worlds[0].h, C.byref(stream))
+    for w in worlds[1:]:
+        lib.xdem_set_stream(w.h, stream)
+    ctl = work["control"]
+    for w in worlds:
+        w.run(max(args.warmup, 3), ctl)
+    n = sum(len(sy["particles"]["x"]) for sy in work["systems"])
+    worlds[0].synchronize()
+    lib.xdem_timer_start(worlds[0].h)
+    for w in worlds:
+        w.run(args.steps, ctl)
+    ms = C.c_double(0.0)
+    lib.xdem_timer_stop(worlds[0].h, C.byref(ms))
+    for w in worlds[1:]:
+        lib.xdem_set_stream(w.h, None)
+    for w in reversed(worlds):
+        w.close()
+    return {"value": n * args.steps / (ms.value / 1e3), "ms_per_step": ms.value / args.steps}
 
 
 def measure(work, precision, args, dist, full=True):
@@ -319,14 +402,22 @@ def measure(work, precision, args, dist, full=True):
     prm = abi.Params()
     C.memmove(C.byref(prm), C.byref(work["params"]), C.sizeof(abi.Params))
     prm.precision = precision
-    p = work["particles"]
-    n = len(p["x"])
     w = World(prm)
     # capped Newton solves are counted and reported, not raised
     w.raise_mask = ~abi.ERR_NEWTON
-    w.set_particles(p)
-    if work["contacts"] is not None and len(work["contacts"]["id_i"]):
-        w.set_contacts(work["contacts"])
+    if "systems" in work:
+        systems = work["systems"]
+        w.set_batch([sy["particles"] for sy in systems], [sy["box"] for sy in systems],
+                    [sy["dt"] for sy in systems])
+        _, first = w.batch_info()
+        w.set_contacts(batch_contacts(systems, first))
+        n = int(first[-1])
+    else:
+        p = work["particles"]
+        n = len(p["x"])
+        w.set_particles(p)
+        if work["contacts"] is not None and len(work["contacts"]["id_i"]):
+            w.set_contacts(work["contacts"])
     ctl = work["control"]
     lib = w.lib
 
@@ -432,6 +523,7 @@ def main():
     ap.add_argument("--impl", default="xdem", choices=["xdem", "reference"])
     ap.add_argument("--workload", default="le_ellipses", choices=sorted(WORKLOADS))
     ap.add_argument("--n", type=int, default=1 << 20)
+    ap.add_argument("--systems", type=int, default=128, help="batch_ensemble: number of systems")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"],
                     help="arithmetic of the headline path (the other one is timed beside it)")
@@ -460,14 +552,15 @@ def main():
             if dist:
                 dist.destroy_process_group()
             return
-        work = WORKLOADS[args.workload](args.n, args.seed)
+        size = args.n if args.workload != "batch_ensemble" else args.systems
+        work = WORKLOADS[args.workload](size, args.seed)
         threads = os.cpu_count() or 1
         res = run_cpu(work, args.steps, 1, threads, budget_s=60.0)
         if "error" in res:
             print(json.dumps({"impl": "reference", "unavailable": res["error"]}), flush=True)
         else:
             v, k = res["value"], res["steps"]
-            sample = (f"{k} steps of the full {work['config']['n_particles']}-particle workload "
+            sample = (f"{k} steps of {res['particles']} particles in {res['systems']} system(s) "
                       f"after 1 warm-up step, {threads} threads; {work['cpu_note']}")
             line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT,
                     "n_gpus": args.gpus, "steps": k, "warmup": 1,
@@ -487,10 +580,14 @@ def main():
     prec = {"mixed": abi.PRECISION_MIXED, "fp64": abi.PRECISION_FP64}
     other = "fp64" if args.precision == "mixed" else "mixed"
 
-    work = WORKLOADS[args.workload](args.n, args.seed + RANK)
-    n = len(work["particles"]["x"])
+    size = args.n if args.workload != "batch_ensemble" else args.systems
+    work = WORKLOADS[args.workload](size, args.seed + RANK)
+    n = work["config"]["n_particles"]
     head = measure(work, prec[args.precision], args, dist, full=True)
     cmp_ = None if args.no_compare else measure(work, prec[other], args, dist, full=False)
+    loop = None
+    if "systems" in work:
+        loop = measure_loop(work, prec[args.precision], args)
 
     # ---- CPU baseline (rank 0, N = 1 only) ----------------------------------
     cpu = None
@@ -502,9 +599,9 @@ def main():
                    "sample": res["error"]}
         else:
             cpu = {"value": res["value"], "unit": UNIT, "cores": threads, "kind": res["kind"],
-                   "sample": f"{res['steps']} steps of the full {n}-particle workload after 1 "
-                             f"warm-up step ({res['one_step_s']:.2f} s per step); "
-                             f"{work['cpu_note']}"}
+                   "sample": f"{res['steps']} steps of {res['particles']} particles in "
+                             f"{res['systems']} system(s) after 1 warm-up step "
+                             f"({res['one_step_s']:.2f} s per step); {work['cpu_note']}"}
 
     cfg = dict(work["config"])
     cfg["precision"] = args.precision
@@ -524,6 +621,11 @@ def main():
         "clocks": head["clocks"], "status": head["status"], "newton": head["newton"],
         "cpu_baseline": cpu,
     }
+    if loop is not None:
+        line["per_system_loop"] = {"value": loop["value"], "ms_per_step": loop["ms_per_step"],
+                                   "what": "one world per system, each run for the K steps in "
+                                           "turn on one stream"}
+        line["speedup_vs_per_system_loop"] = head["value"] / loop["value"]
     if cmp_ is not None:
         line[other] = {"value": cmp_["value"], "ms_per_step": cmp_["ms_per_step"],
                        "contacts": cmp_["contacts"], "newton": cmp_["newton"],

@@ -196,6 +196,36 @@ int32_t xdem_create(const xdem_params* params, xdem_world* out);
 int32_t xdem_destroy(xdem_world w);
 /* run this world's work on a caller-owned cudaStream_t (NULL = own stream) */
 int32_t xdem_set_stream(xdem_world w, void* cuda_stream);
+/* the cudaStream_t this world's work runs on */
+int32_t xdem_get_stream(xdem_world w, void** cuda_stream);
+
+/* ---- batched systems ----------------------------------------------------- */
+/* No counterpart in the reference, which runs one world per process.  Puts
+   nsys independent systems of this world's kind into one handle, so that each
+   kernel of a step covers all of them and xdem_run replays one captured graph
+   for the whole batch.  systems[s] holds system s with local ids 0..n_s-1
+   (up_level local too); in the world its particles take the ids first_s + id,
+   first_s = n_0 + ... + n_{s-1}, and every other entry point addresses that
+   concatenation (contacts, state, particles).  boxes: xmin, xmax, ymin, ymax
+   per system; dts: time step per system (NULL = the world's).  The contact
+   model, precision, ellipse method and slot count are the world's.  Replaces
+   xdem_set_particles.  Per-system results come from the xdem_batch_get_*
+   calls; xdem_get_boundary, xdem_get_stress and xdem_get_lees_edwards report
+   system 0; xdem_set_boundary, xdem_set_lees_edwards and
+   xdem_scale_boundary_to_solid_fraction, and xdem_run with stop_on_pressure,
+   return XDEM_ERR_ARGUMENT on a batch; the other setters apply to every
+   system. */
+int32_t xdem_batch_set_particles(xdem_world w, int32_t nsys, const xdem_particles* systems,
+                                 const double* boxes, const double* dts);
+/* *nsys = systems in the world; first (may be NULL): nsys + 1 entries, the
+   first id of each system and then n */
+int32_t xdem_batch_info(xdem_world w, int32_t* nsys, int32_t* first);
+/* updateTotalStress result of each system (xx, xy, yx, yy per system) */
+int32_t xdem_batch_get_stress(xdem_world w, double* stress);
+/* box of each system (xmin, xmax, ymin, ymax per system) */
+int32_t xdem_batch_get_boundaries(xdem_world w, double* boxes);
+/* countActucalContacts of each system */
+int32_t xdem_batch_count_contacts(xdem_world w, int64_t* counts);
 
 /* ---- state exchange ----------------------------------------------------- */
 /* upload: vector<BaseParticle*> handed to the world constructor (BaseWorld.h:44);

@@ -224,3 +224,17 @@ def controls():
         "uniform": make_control(update_stress=True, box_law=abi.BOX_STRESS_UNIFORM, p0=5.0,
                                 reset_rattlers=True),
     }
+
+
+def dense_ellipse_case(n=3000, seed=21, kind=abi.WORLD_LEES_EDWARDS, phi=0.85, aspect=inputs.c4_aspect,
+                       shift_rate=0.1, steps=1500, relax=300):
+    """An ellipse packing compressed on the GPU (FP64) to solid fraction phi;
+    returns (particles, contacts, params) for a world of the given kind."""
+    from xdem_b200 import packing
+    p, box = inputs.ellipse_system(n, b=inputs.c2_b, aspect=aspect, phi_rsa_circle=0.40, phi=None,
+                                   seed=seed, vel_sigma=0.01)
+    dt = inputs.time_step(p)
+    q, contacts, b, _ = packing.compress(p, box, phi, dt, steps=steps, relax=relax)
+    prm = make_params(kind, dt, b, inputs.KN, inputs.KT, inputs.RESTITUTION, inputs.FRICTION,
+                      shift_strain_rate=shift_rate if kind == abi.WORLD_LEES_EDWARDS else 0.0)
+    return q, contacts, prm

@@ -14,7 +14,14 @@ the stated error of the mixed path:
   - forces after one step from an identical state: within 1e-5 of the
     largest contact force, per contact (the force tolerance the mixed mode
     promises), torques likewise;
-  - mean shear stress of a Lees-Edwards shear run: within 0.5 %.
+  - mean shear stress of a Lees-Edwards shear run: within 0.5 %, or within
+    the spread that a 1e-12 perturbation of the initial state produces in
+    the FP64 path itself, whichever is larger (a short run of a small system
+    is chaotic enough for the two to be comparable).
+Pairs whose FP64 closest-approach Newton iteration does not converge (the
+reference's loop never returns on them, EllipticParticle.cpp:621; the
+checker stops it at its cap) have no FP64 answer to compare with and are
+left out of the force comparison; the mixed path solves them.
 """
 import numpy as np
 import pytest
@@ -23,7 +30,7 @@ import oracle
 from xdem_b200 import abi, inputs
 from xdem_b200.world import World, make_control, pair_geometry
 
-from helpers import disc_case, ellipse_case, same_pairs
+from helpers import dense_ellipse_case, disc_case, same_pairs
 
 pytestmark = pytest.mark.gpu
 
@@ -91,78 +98,113 @@ def test_mixed_pair_geometry_circles_overlap_is_fp64():
     assert np.max(np.abs(om[c][:, 1:3] - oc[c][:, 1:3])) <= 2e-6
 
 
-def _one_step_pair(p, prm_fp64, prm_mixed):
-    c = oracle.PortWorld(prm_fp64)
+def _mixed(prm):
+    from ctypes import sizeof, memmove, byref
+    pm = abi.Params()
+    memmove(byref(pm), byref(prm), sizeof(abi.Params))
+    pm.precision = abi.PRECISION_MIXED
+    return pm
+
+
+def _one_step_pair(p, prm, contacts=None):
+    """One step of the FP64 checker and of the mixed GPU path from the same
+    state and history."""
+    c = oracle.PortWorld(prm)
+    c.raise_mask = ~abi.ERR_NEWTON
     c.set_particles(p)
-    g = World(prm_mixed)
+    g = World(_mixed(prm))
+    g.raise_mask = ~abi.ERR_NEWTON
     g.set_particles(p)
+    if contacts is not None and len(contacts["id_i"]):
+        c.set_contacts(contacts)
+        g.set_contacts(contacts)
     c.takeTimeStep()
     g.takeTimeStep()
     return g.get_contacts(), c.get_contacts()
 
 
-def _force_err(cm, cc):
-    f_m = np.hypot(cm["fn_x"] + cm["ft_x"], cm["fn_y"] + cm["ft_y"])
-    scale = np.max(np.hypot(cc["fn_x"] + cc["ft_x"], cc["fn_y"] + cc["ft_y"]))
+def _converged(p, cc, prm):
+    """Mask of the contacts whose FP64 closest-approach Newton iteration
+    converged, from the pre-step state p and the contacts' branch vectors
+    b = p_i - (p_j + offset)."""
+    i, j = cc["id_i"], cc["id_j"]
+    if prm.ellipse_method != abi.ELLIPSE_CLOSEST_APPROACH or not np.any(p["shape"] == 1):
+        return np.ones(len(i), bool)
+
+    def rows(k):
+        return np.stack([p["shape"][k], p["radius"][k], p["aspect_ratio"][k], p["x"][k], p["y"][k],
+                         p["vx"][k], p["vy"][k], p["rot"][k], p["rot_vel"][k]], 1).astype(np.float64)
+    off = np.zeros((len(i), 4))
+    off[:, 0] = p["x"][i] - p["x"][j] - cc["branch_x"]
+    off[:, 1] = p["y"][i] - p["y"][j] - cc["branch_y"]
+    out, _ = oracle.pair_geometry(rows(i), rows(j), off, abi.ELLIPSE_CLOSEST_APPROACH, "port")
+    return out[:, 16] < 1000
+
+
+def _force_err(cm, cc, keep=None):
+    """largest per-contact force difference over the largest contact force"""
+    keep = np.ones(len(cc["id_i"]), bool) if keep is None else keep
+    scale = np.max(np.hypot(cc["fn_x"] + cc["ft_x"], cc["fn_y"] + cc["ft_y"])[keep])
     dfx = (cm["fn_x"] + cm["ft_x"]) - (cc["fn_x"] + cc["ft_x"])
     dfy = (cm["fn_y"] + cm["ft_y"]) - (cc["fn_y"] + cc["ft_y"])
-    del f_m
-    return np.max(np.hypot(dfx, dfy)) / scale
+    return np.max(np.hypot(dfx, dfy)[keep]) / scale
 
 
 @pytest.mark.parametrize("kind", [abi.WORLD_PERIODIC, abi.WORLD_LEES_EDWARDS])
 def test_mixed_ellipse_world_one_step_forces(kind):
-    from ctypes import sizeof, memmove, byref
-    p, prm = ellipse_case(n=3000, seed=21, kind=kind, aspect=inputs.c4_aspect, compress=1.3)
-    pm = abi.Params()
-    memmove(byref(pm), byref(prm), sizeof(abi.Params))
-    pm.precision = abi.PRECISION_MIXED
-    cm, cc = _one_step_pair(p, prm, pm)
+    p, contacts, prm = dense_ellipse_case(n=3000, seed=21, kind=kind)
+    cm, cc = _one_step_pair(p, prm, contacts)
     assert same_pairs(cm, cc)
-    assert len(cc["id_i"]) > 1000
-    assert _force_err(cm, cc) <= FORCE_TOL
-    tscale = max(np.max(np.abs(cc["torque_i"])), 1e-300)
-    assert np.max(np.abs(cm["torque_i"] - cc["torque_i"])) <= FORCE_TOL * tscale
-    assert np.max(np.abs(cm["normal_x"] - cc["normal_x"])) <= 2e-6
+    assert len(cc["id_i"]) > 3000
+    keep = _converged(p, cc, prm)
+    assert keep.sum() >= len(keep) - 10
+    assert _force_err(cm, cc, keep) <= FORCE_TOL
+    tscale = np.max(np.abs(cc["torque_i"][keep]))
+    assert np.max(np.abs(cm["torque_i"] - cc["torque_i"])[keep]) <= FORCE_TOL * tscale
+    assert np.max(np.abs(cm["normal_x"] - cc["normal_x"])[keep]) <= 2e-6
+    # the tangential springs carried over from the history
+    sscale = np.max(np.hypot(cc["shear_x"], cc["shear_y"])[keep])
+    assert np.max(np.abs(cm["shear_x"] - cc["shear_x"])[keep]) <= FORCE_TOL * sscale
 
 
 def test_mixed_disc_world_one_step_forces():
-    from ctypes import sizeof, memmove, byref
-    p, prm = disc_case(n=2000, phi=0.82, seed=4, kind=abi.WORLD_LEES_EDWARDS, shift_strain_rate=0.05)
-    pm = abi.Params()
-    memmove(byref(pm), byref(prm), sizeof(abi.Params))
-    pm.precision = abi.PRECISION_MIXED
-    cm, cc = _one_step_pair(p, prm, pm)
+    p, prm = disc_case(n=2000, phi=0.84, seed=4, kind=abi.WORLD_LEES_EDWARDS, shift_strain_rate=0.05)
+    cm, cc = _one_step_pair(p, prm)
     assert same_pairs(cm, cc)
+    assert len(cc["id_i"]) > 1000
     assert _force_err(cm, cc) <= FORCE_TOL
 
 
 def test_mixed_lees_edwards_history_and_mean_shear_stress():
-    """Several hundred steps of shear: the contact history carries over in
-    both runs, and the time-averaged shear stress agrees within 0.5 %."""
-    from ctypes import sizeof, memmove, byref
-    p, prm = ellipse_case(n=4000, seed=33, kind=abi.WORLD_LEES_EDWARDS, aspect=inputs.c4_aspect,
-                          compress=1.35, shift_rate=0.1)
-    pm = abi.Params()
-    memmove(byref(pm), byref(prm), sizeof(abi.Params))
-    pm.precision = abi.PRECISION_MIXED
-    g64, gmx = World(prm), World(pm)
-    for w in (g64, gmx):
+    """Shear of a dense packing: the time-averaged shear stress of the mixed
+    path agrees with the FP64 path's within 0.5 % or within the FP64 path's
+    own spread under a 1e-12 perturbation of the initial positions, and the
+    contact sets stay nearly the same."""
+    p, contacts, prm = dense_ellipse_case(n=4000, seed=33, kind=abi.WORLD_LEES_EDWARDS,
+                                          shift_rate=0.1)
+    q = dict(p)
+    q["x"] = p["x"] * (1.0 + 1e-12)
+    worlds = [World(prm), World(prm), World(_mixed(prm))]
+    for w, state in zip(worlds, (p, q, p)):
         w.raise_mask = ~abi.ERR_NEWTON
-        w.set_particles(p)
+        w.set_particles(state)
+        w.set_contacts(contacts)
     ctl = make_control(update_stress=True)
-    s64, smx = [], []
+    series = [[], [], []]
     for _ in range(40):
-        g64.run(20, ctl)
-        gmx.run(20, ctl)
-        s64.append(g64.getStress()[1])
-        smx.append(gmx.getStress()[1])
-    m64, mmx = np.mean(s64), np.mean(smx)
+        for w, s in zip(worlds, series):
+            w.run(25, ctl)
+            s.append(w.getStress()[1])
+    m64, m64p, mmx = (float(np.mean(s)) for s in series)
     assert abs(m64) > 0
-    assert abs(mmx - m64) <= 5e-3 * abs(m64), (m64, mmx)
-    assert g64.count_contacts() > 2000
-    # the contact set after 800 steps is still nearly the same
-    c64, cmx = g64.get_contacts(), gmx.get_contacts()
-    k64 = set(zip(c64["id_i"].tolist(), c64["id_j"].tolist()))
-    kmx = set(zip(cmx["id_i"].tolist(), cmx["id_j"].tolist()))
-    assert len(k64 ^ kmx) <= 0.01 * len(k64)
+    spread = abs(m64p - m64)
+    assert abs(mmx - m64) <= max(5e-3 * abs(m64), 4.0 * spread), (m64, m64p, mmx)
+    assert worlds[0].count_contacts() > 4000
+    keys = []
+    for w in worlds:
+        c = w.get_contacts()
+        keys.append(set(zip(c["id_i"].tolist(), c["id_j"].tolist())))
+    # the contact sets drift apart no faster than the FP64 path's own under
+    # the perturbation
+    own = len(keys[0] ^ keys[1])
+    assert len(keys[0] ^ keys[2]) <= max(0.01 * len(keys[0]), 2.0 * own), (own, len(keys[0] ^ keys[2]))

@@ -180,7 +180,13 @@ def load_library(path=LIB_PATH):
         "xdem_create": (C.c_int32, [P(Params), P(W)]),
         "xdem_destroy": (C.c_int32, [W]),
         "xdem_set_stream": (C.c_int32, [W, C.c_void_p]),
+        "xdem_get_stream": (C.c_int32, [W, P(C.c_void_p)]),
         "xdem_set_particles": (C.c_int32, [W, P(Particles)]),
+        "xdem_batch_set_particles": (C.c_int32, [W, C.c_int32, P(Particles), _d, _d]),
+        "xdem_batch_info": (C.c_int32, [W, P(C.c_int32), P(C.c_int32)]),
+        "xdem_batch_get_stress": (C.c_int32, [W, _d]),
+        "xdem_batch_get_boundaries": (C.c_int32, [W, _d]),
+        "xdem_batch_count_contacts": (C.c_int32, [W, P(C.c_int64)]),
         "xdem_get_particles": (C.c_int32, [W, P(Particles)]),
         "xdem_set_contacts": (C.c_int32, [W, P(Contacts)]),
         "xdem_get_contacts": (C.c_int32, [W, P(Contacts)]),

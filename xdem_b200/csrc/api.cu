@@ -56,11 +56,11 @@ struct xdem_world_s {
   WorldScalars* ws = nullptr;
   uint32_t* status = nullptr;
   int par = 0;            // slot set holding the latest contacts
-  int nx_cap = 0, ny_cap = 0;
+  int nsys = 1;           // systems (batched worlds: more than one)
   int partial_blocks = 0;
   uint32_t host_status = 0;
   double total_volume = 0.0;
-  double control_mass = 0.0;
+  std::vector<double> control_mass{0.0};  // per system
   // per-kernel timing
   bool prof_on = false;
   std::vector<cudaEvent_t> prof_events;  // pairs (begin, end)
@@ -100,6 +100,21 @@ cudaError_t read_scalars(xdem_world_s* w, WorldScalars* out) {
 
 cudaError_t write_scalars(xdem_world_s* w, const WorldScalars* in) {
   cudaError_t e = cudaMemcpyAsync(w->ws, in, sizeof(WorldScalars), cudaMemcpyHostToDevice, w->stream);
+  if (e != cudaSuccess) return e;
+  return cudaStreamSynchronize(w->stream);
+}
+
+// applies f to the scalars of every system of the world
+template <class F>
+cudaError_t modify_all(xdem_world_s* w, F f) {
+  std::vector<WorldScalars> all(w->nsys);
+  cudaError_t e = cudaMemcpyAsync(all.data(), w->ws, sizeof(WorldScalars) * w->nsys,
+                                  cudaMemcpyDeviceToHost, w->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(w->stream);
+  if (e != cudaSuccess) return e;
+  for (int s = 0; s < w->nsys; ++s) f(all[s], s);
+  e = cudaMemcpyAsync(w->ws, all.data(), sizeof(WorldScalars) * w->nsys, cudaMemcpyHostToDevice,
+                      w->stream);
   if (e != cudaSuccess) return e;
   return cudaStreamSynchronize(w->stream);
 }
@@ -165,7 +180,7 @@ void launch_modify(xdem_world_s* w) {
 void launch_find(xdem_world_s* w) {
   int n = w->dw.n;
   LAUNCH(w, KK_BIN, k_bin<<<blocks_for(n, kBlock), kBlock, 0, w->stream>>>(w->dw));
-  int cells = w->nx_cap * w->ny_cap + 2 * w->nx_cap;
+  int cells = w->dw.ncell_total;
   int tiles = std::min(blocks_for(cells, kScanTile), 2 * 148 * 8);
   LAUNCH(w, KK_SCAN, k_scan_tiles<<<tiles, kScanThreads, 0, w->stream>>>(w->dw));
   LAUNCH(w, KK_SCAN, k_scan_sums<<<1, kScanThreads, 0, w->stream>>>(w->dw));
@@ -224,6 +239,11 @@ void launch_integrate(xdem_world_s* w, bool fold_bg, int reset) {
 }
 
 void launch_stress(xdem_world_s* w) {
+  if (w->nsys > 1) {
+    LAUNCH(w, KK_STRESS_PARTIAL,
+           k_stress_systems<<<w->nsys, kReduceBlock, 0, w->stream>>>(w->dw, w->par));
+    return;
+  }
   int nb = blocks_for(w->dw.n, kReduceBlock);
   LAUNCH(w, KK_STRESS_PARTIAL, k_stress_partial<<<nb, kReduceBlock, 0, w->stream>>>(w->dw, w->par));
   LAUNCH(w, KK_STRESS_FINAL, k_stress_final<<<1, 1024, 0, w->stream>>>(w->dw, nb));
@@ -236,8 +256,9 @@ void launch_rattlers(xdem_world_s* w, int reset, double scale) {
 
 void launch_end_of_step(xdem_world_s* w, int law, double p0, double p1, int le_update, int stop_on,
                         double stop_p, int count_step) {
-  LAUNCH(w, KK_END_OF_STEP, k_end_of_step<<<1, 1, 0, w->stream>>>(w->dw, law, p0, p1, le_update,
-                                                                 stop_on, stop_p, count_step));
+  LAUNCH(w, KK_END_OF_STEP,
+         k_end_of_step<<<blocks_for(w->nsys, 128), 128, 0, w->stream>>>(
+             w->dw, law, p0, p1, le_update, stop_on, stop_p, count_step));
   if (law != BOX_NONE)
     LAUNCH(w, KK_SCALE, k_scale_positions<<<blocks_for(w->dw.n, kBlock), kBlock, 0, w->stream>>>(w->dw));
 }
@@ -245,7 +266,7 @@ void launch_end_of_step(xdem_world_s* w, int law, double p0, double p1, int le_u
 // refresh of the memory order (resort.cuh), after a step's binning
 void launch_resort(xdem_world_s* w) {
   int n = w->dw.n;
-  int cells = w->nx_cap * w->ny_cap;
+  int cells = w->dw.ncell_total;
   int cb = std::min(blocks_for(cells, kBlock), 148 * 16);
   LAUNCH(w, KK_RESORT, k_sort_cells<<<cb, kBlock, 0, w->stream>>>(w->dw));
   LAUNCH(w, KK_RESORT, k_permute<<<blocks_for(n, kBlock), kBlock, 0, w->stream>>>(w->dw, w->perm));
@@ -384,6 +405,7 @@ int32_t xdem_create(const xdem_params* prm, xdem_world* out) {
     return XDEM_ERR_CUDA;
   }
   w->dw.ws = w->ws;
+  w->dw.nsys = 1;
   w->dw.status = w->status;
   w->dw.kind = prm->world_kind;
   w->dw.method = prm->ellipse_method;
@@ -407,6 +429,12 @@ int32_t xdem_destroy(xdem_world w) {
   return XDEM_OK;
 }
 
+int32_t xdem_get_stream(xdem_world w, void** s) {
+  if (!w || !s) return XDEM_ERR_ARGUMENT;
+  *s = static_cast<void*>(w->stream);
+  return XDEM_OK;
+}
+
 int32_t xdem_set_stream(xdem_world w, void* s) {
   if (!w) return XDEM_ERR_ARGUMENT;
   cudaStreamSynchronize(w->stream);
@@ -421,8 +449,22 @@ int32_t xdem_set_stream(xdem_world w, void* s) {
   return XDEM_OK;
 }
 
-int32_t xdem_set_particles(xdem_world w, const xdem_particles* P) {
-  if (!w || !P || P->n <= 0) return XDEM_ERR_ARGUMENT;
+}  // extern "C"
+
+namespace {
+
+// One system of a world: particles [first, first + count), its box, time step.
+struct SysDesc {
+  int first, count;
+  double box[4];
+  double dt;
+};
+
+// Uploads the particles P (all systems, ids global) and sizes every device
+// array; sys lists the systems in id order (one entry for a single world,
+// whose box and time step are then taken from its current scalars).
+int32_t set_particles_impl(xdem_world_s* w, const xdem_particles* P, const std::vector<SysDesc>& sys) {
+  if (!w || !P || P->n <= 0 || sys.empty()) return XDEM_ERR_ARGUMENT;
   const int n = P->n;
   if ((int64_t)n * w->dw.K >= (int64_t)1 << 31) return XDEM_ERR_ARGUMENT;
   if (!P->shape || !P->up_level || !P->setting || !P->outer_radius || !P->radius ||
@@ -473,7 +515,6 @@ int32_t xdem_set_particles(xdem_world w, const xdem_particles* P) {
   // host-side derived data
   std::vector<double2> pos(n), vel(n), br(n);
   std::vector<int32_t> ns(n, 0), rat(n, 0);
-  double maxr = 0.0, volsum = 0.0, msum = 0.0;
   for (int i = 0; i < n; ++i) {
     pos[i] = make_double2(P->x[i], P->y[i]);
     vel[i] = make_double2(P->vx[i], P->vy[i]);
@@ -482,10 +523,26 @@ int32_t xdem_set_particles(xdem_world w, const xdem_particles* P) {
     if (P->is_rattler) rat[i] = P->is_rattler[i];
     if (P->shape[i] < 0 || P->shape[i] > 2) return XDEM_ERR_ARGUMENT;
     if (P->shape[i] == XDEM_SHAPE_CLUMP && (ns[i] < 0 || i + ns[i] >= n)) return XDEM_ERR_ARGUMENT;
-    if (P->outer_radius[i] > maxr) maxr = P->outer_radius[i];  // BaseWorld.cpp:201-219
-    if (!(P->setting[i] & XDEM_SKIP_MACRO_SUM)) {
-      volsum += P->volume[i];  // BaseWorld.cpp:188-199
-      msum += P->mass[i];
+  }
+  // per system: largest outer radius (updateMaximumParticleSize,
+  // BaseWorld.cpp:201-219), particle volume (updateTotalParticleVolume,
+  // BaseWorld.cpp:188-199) and mass
+  const int nsys = (int)sys.size();
+  std::vector<double> sys_maxr(nsys, 0.0), sys_vol(nsys, 0.0), sys_mass(nsys, 0.0);
+  std::vector<int32_t> sys_of(n, 0);
+  for (int k = 0; k < nsys; ++k) {
+    if (sys[k].first < 0 || sys[k].count <= 0 || sys[k].first + sys[k].count > n)
+      return XDEM_ERR_ARGUMENT;
+    for (int i = sys[k].first; i < sys[k].first + sys[k].count; ++i) {
+      sys_of[i] = k;
+      // a clump's sub-particles belong to its system
+      if (P->shape[i] == XDEM_SHAPE_CLUMP && i + ns[i] >= sys[k].first + sys[k].count)
+        return XDEM_ERR_ARGUMENT;
+      if (P->outer_radius[i] > sys_maxr[k]) sys_maxr[k] = P->outer_radius[i];
+      if (!(P->setting[i] & XDEM_SKIP_MACRO_SUM)) {
+        sys_vol[k] += P->volume[i];
+        sys_mass[k] += P->mass[i];
+      }
     }
   }
   cudaStream_t s = w->stream;
@@ -510,8 +567,10 @@ int32_t xdem_set_particles(xdem_world w, const xdem_particles* P) {
   CK(w, cudaMemsetAsync(d.force, 0, sizeof(double2) * n, s));
   CK(w, cudaMemsetAsync(d.torque, 0, sizeof(double) * n, s));
   CK(w, cudaMemsetAsync(d.ncp, 0, sizeof(int32_t) * n, s));
-  w->total_volume = volsum;
-  w->control_mass = msum / ((double)n * 10.0);  // setVirtualBoundaryMass (PeriodicControlWorld.cpp:58-66)
+  w->total_volume = sys_vol[0];
+  w->control_mass.assign(nsys, 0.0);
+  for (int k = 0; k < nsys; ++k)  // setVirtualBoundaryMass (PeriodicControlWorld.cpp:58-66)
+    w->control_mass[k] = sys_mass[k] / ((double)sys[k].count * 10.0);
   // one contact law for the whole world when every non-clump body has one shape
   bool any_circle = false, any_ellipse = false;
   for (int i = 0; i < n; ++i) {
@@ -522,18 +581,62 @@ int32_t xdem_set_particles(xdem_world w, const xdem_particles* P) {
   else if (any_ellipse)
     w->law = w->prm.ellipse_method == XDEM_ELLIPSE_INTERSECTION ? LAW_INTERSECTION : LAW_CLOSEST;
   else w->law = LAW_CIRCLE;
-  WorldScalars ws;
-  CK(w, read_scalars(w, &ws));
-  ws.maxsize = w->prm.max_particle_size > 0 ? w->prm.max_particle_size : maxr * 2.01;
-  // grid capacity: twice the starting grid per axis, so a growing box keeps
-  // its cell size for a while and then coarsens
-  int nx0 = (int)std::floor(ws.xlen / ws.maxsize), ny0 = (int)std::floor(ws.ylen / ws.maxsize);
-  w->nx_cap = std::max(3, 2 * nx0 + 4);
-  w->ny_cap = std::max(3, 2 * ny0 + 4);
-  d.nx_cap = w->nx_cap;
-  d.ny_cap = w->ny_cap;
-  CK(w, write_scalars(w, &ws));
-  size_t cells = (size_t)w->nx_cap * w->ny_cap + 2 * (size_t)w->nx_cap;
+  // scalars of every system: the single world keeps its current ones; a batch
+  // takes the contact model and run settings of the world's and its own box
+  // and time step
+  WorldScalars tmpl;
+  CK(w, read_scalars(w, &tmpl));
+  if (nsys != w->nsys) {
+    WorldScalars* nws = nullptr;
+    CK(w, cudaMalloc(&nws, sizeof(WorldScalars) * nsys));
+    cudaFree(w->ws);
+    w->ws = nws;
+    w->dw.ws = nws;
+    w->nsys = nsys;
+  }
+  d.nsys = nsys;
+  std::vector<WorldScalars> all(nsys, tmpl);
+  std::vector<int32_t> cell_base(nsys + 1, 0);
+  size_t cells = 0;
+  for (int k = 0; k < nsys; ++k) {
+    WorldScalars& ws = all[k];
+    if (nsys > 1) {
+      ws.xmin = sys[k].box[0];
+      ws.xmax = sys[k].box[1];
+      ws.ymin = sys[k].box[2];
+      ws.ymax = sys[k].box[3];
+      ws.xlen = ws.xmax - ws.xmin;
+      ws.ylen = ws.ymax - ws.ymin;
+      ws.shift_vel = ws.shift_rate * ws.ylen;
+      ws.dt = sys[k].dt;
+      ws.shift = ws.strain = ws.velX = ws.velY = 0.0;
+      for (int c = 0; c < 4; ++c) ws.stress[c] = 0.0;
+      if (!(ws.xlen > 0.0) || !(ws.ylen > 0.0) || !(ws.dt > 0.0)) return XDEM_ERR_ARGUMENT;
+    }
+    ws.maxsize = w->prm.max_particle_size > 0 ? w->prm.max_particle_size : sys_maxr[k] * 2.01;
+    // grid capacity: twice the starting grid per axis, so a growing box keeps
+    // its cell size for a while and then coarsens
+    int nx0 = (int)std::floor(ws.xlen / ws.maxsize), ny0 = (int)std::floor(ws.ylen / ws.maxsize);
+    ws.nx_cap = std::max(3, 2 * nx0 + 4);
+    ws.ny_cap = std::max(3, 2 * ny0 + 4);
+    ws.cell_base = (int32_t)cells;
+    ws.first = sys[k].first;
+    ws.count = sys[k].count;
+    cell_base[k] = (int32_t)cells;
+    cells += (size_t)ws.nx_cap * ws.ny_cap + 2 * (size_t)ws.nx_cap;
+    if (cells >= ((size_t)1 << 31) - 2) return XDEM_ERR_ARGUMENT;
+  }
+  cell_base[nsys] = (int32_t)cells;
+  d.ncell_total = (int)cells;
+  CK(w, cudaMemcpyAsync(w->ws, all.data(), sizeof(WorldScalars) * nsys, cudaMemcpyHostToDevice, s));
+  CK(w, B.alloc(&d.sys_cell_base, nsys + 1));
+  CK(w, upload(d.sys_cell_base, cell_base.data(), nsys + 1, s));
+  d.sys_of = nullptr;
+  if (nsys > 1) {
+    // a system keeps its memory range through re-sorts, so sys_of never moves
+    CK(w, B.alloc(&d.sys_of, n));
+    CK(w, upload(d.sys_of, sys_of.data(), n, s));
+  }
   CK(w, B.alloc(&d.cell_count, cells + 1));
   CK(w, B.alloc(&d.cell_start, cells + 1));
   CK(w, B.alloc(&d.tile_sum, cells / kScanTile + 2));
@@ -632,6 +735,165 @@ int32_t xdem_set_particles(xdem_world w, const xdem_particles* P) {
   CK(w, cudaStreamSynchronize(s));
   return XDEM_OK;
 }
+
+}  // namespace
+
+extern "C" {
+
+int32_t xdem_set_particles(xdem_world w, const xdem_particles* P) {
+  if (!w || !P || P->n <= 0) return XDEM_ERR_ARGUMENT;
+  std::vector<SysDesc> sys(1);
+  sys[0].first = 0;
+  sys[0].count = P->n;
+  return set_particles_impl(w, P, sys);
+}
+
+// ---- batched systems ------------------------------------------------------------
+int32_t xdem_batch_set_particles(xdem_world w, int32_t nsys, const xdem_particles* systems,
+                                 const double* boxes, const double* dts) {
+  if (!w || nsys <= 0 || !systems || !boxes) return XDEM_ERR_ARGUMENT;
+  std::vector<SysDesc> sys(nsys);
+  int64_t total = 0;
+  for (int k = 0; k < nsys; ++k) {
+    const xdem_particles& Q = systems[k];
+    if (Q.n <= 0 || !Q.shape || !Q.up_level || !Q.setting || !Q.outer_radius || !Q.radius ||
+        !Q.aspect_ratio || !Q.x || !Q.y || !Q.vx || !Q.vy || !Q.rot || !Q.rot_vel || !Q.volume ||
+        !Q.mass || !Q.inv_mass || !Q.inertia || !Q.inv_inertia)
+      return XDEM_ERR_ARGUMENT;
+    sys[k].first = (int)total;
+    sys[k].count = Q.n;
+    for (int c = 0; c < 4; ++c) sys[k].box[c] = boxes[4 * k + c];
+    sys[k].dt = dts ? dts[k] : w->prm.dt;
+    total += Q.n;
+  }
+  if (total >= ((int64_t)1 << 31) / kMaxSlots) return XDEM_ERR_ARGUMENT;
+  const int n = (int)total;
+  // the concatenation, ids made global
+  std::vector<int32_t> shape(n), up(n), setting(n), rattler(n, 0), num_sub(n, 0);
+  std::vector<double> orad(n), rad(n), asp(n), x(n), y(n), vx(n), vy(n), rot(n), rv(n), vol(n),
+      mass(n), im(n), I(n), iI(n), bx(n, 0.0), by(n, 0.0);
+  bool clumps = false, rattlers = false;
+  for (int k = 0; k < nsys; ++k) {
+    const xdem_particles& Q = systems[k];
+    const int f = sys[k].first;
+    for (int i = 0; i < Q.n; ++i) {
+      const int g = f + i;
+      shape[g] = Q.shape[i];
+      if (Q.up_level[i] < 0 || Q.up_level[i] >= Q.n) return XDEM_ERR_ARGUMENT;
+      up[g] = f + Q.up_level[i];
+      setting[g] = Q.setting[i];
+      if (Q.is_rattler) {
+        rattler[g] = Q.is_rattler[i];
+        rattlers = true;
+      }
+      if (Q.num_sub) {
+        num_sub[g] = Q.num_sub[i];
+        clumps = true;
+      }
+      orad[g] = Q.outer_radius[i];
+      rad[g] = Q.radius[i];
+      asp[g] = Q.aspect_ratio[i];
+      x[g] = Q.x[i];
+      y[g] = Q.y[i];
+      vx[g] = Q.vx[i];
+      vy[g] = Q.vy[i];
+      rot[g] = Q.rot[i];
+      rv[g] = Q.rot_vel[i];
+      vol[g] = Q.volume[i];
+      mass[g] = Q.mass[i];
+      im[g] = Q.inv_mass[i];
+      I[g] = Q.inertia[i];
+      iI[g] = Q.inv_inertia[i];
+      if (Q.branch_x) bx[g] = Q.branch_x[i];
+      if (Q.branch_y) by[g] = Q.branch_y[i];
+    }
+  }
+  xdem_particles P{};
+  P.n = n;
+  P.shape = shape.data();
+  P.up_level = up.data();
+  P.setting = setting.data();
+  P.is_rattler = rattlers ? rattler.data() : nullptr;
+  P.outer_radius = orad.data();
+  P.radius = rad.data();
+  P.aspect_ratio = asp.data();
+  P.x = x.data();
+  P.y = y.data();
+  P.vx = vx.data();
+  P.vy = vy.data();
+  P.rot = rot.data();
+  P.rot_vel = rv.data();
+  P.volume = vol.data();
+  P.mass = mass.data();
+  P.inv_mass = im.data();
+  P.inertia = I.data();
+  P.inv_inertia = iI.data();
+  P.num_sub = clumps ? num_sub.data() : nullptr;
+  P.branch_x = clumps ? bx.data() : nullptr;
+  P.branch_y = clumps ? by.data() : nullptr;
+  return set_particles_impl(w, &P, sys);
+}
+
+int32_t xdem_batch_info(xdem_world w, int32_t* nsys, int32_t* first) {
+  if (!w || !nsys) return XDEM_ERR_ARGUMENT;
+  *nsys = w->nsys;
+  if (first) {
+    std::vector<WorldScalars> all(w->nsys);
+    CK(w, cudaMemcpyAsync(all.data(), w->ws, sizeof(WorldScalars) * w->nsys, cudaMemcpyDeviceToHost,
+                          w->stream));
+    CK(w, cudaStreamSynchronize(w->stream));
+    for (int k = 0; k < w->nsys; ++k) first[k] = all[k].first;
+    first[w->nsys] = w->dw.n;
+  }
+  return XDEM_OK;
+}
+
+int32_t xdem_batch_get_stress(xdem_world w, double* stress) {
+  if (!w || !stress) return XDEM_ERR_ARGUMENT;
+  std::vector<WorldScalars> all(w->nsys);
+  CK(w, cudaMemcpyAsync(all.data(), w->ws, sizeof(WorldScalars) * w->nsys, cudaMemcpyDeviceToHost,
+                        w->stream));
+  CK(w, cudaStreamSynchronize(w->stream));
+  for (int k = 0; k < w->nsys; ++k)
+    for (int c = 0; c < 4; ++c) stress[4 * k + c] = all[k].stress[c];
+  return XDEM_OK;
+}
+
+int32_t xdem_batch_get_boundaries(xdem_world w, double* boxes) {
+  if (!w || !boxes) return XDEM_ERR_ARGUMENT;
+  std::vector<WorldScalars> all(w->nsys);
+  CK(w, cudaMemcpyAsync(all.data(), w->ws, sizeof(WorldScalars) * w->nsys, cudaMemcpyDeviceToHost,
+                        w->stream));
+  CK(w, cudaStreamSynchronize(w->stream));
+  for (int k = 0; k < w->nsys; ++k) {
+    boxes[4 * k + 0] = all[k].xmin;
+    boxes[4 * k + 1] = all[k].xmax;
+    boxes[4 * k + 2] = all[k].ymin;
+    boxes[4 * k + 3] = all[k].ymax;
+  }
+  return XDEM_OK;
+}
+
+int32_t xdem_batch_count_contacts(xdem_world w, int64_t* counts) {
+  if (!w || !counts || w->dw.n <= 0) return XDEM_ERR_ARGUMENT;
+  const int n = w->dw.n, K = w->dw.K;
+  std::vector<WorldScalars> all(w->nsys);
+  std::vector<int32_t> cnt(n), partner((size_t)K * n);
+  CK(w, cudaMemcpyAsync(all.data(), w->ws, sizeof(WorldScalars) * w->nsys, cudaMemcpyDeviceToHost,
+                        w->stream));
+  CK(w, download(cnt.data(), w->dw.slots[w->par].count, n, w->stream));
+  CK(w, download(partner.data(), w->dw.slots[w->par].partner, (size_t)K * n, w->stream));
+  CK(w, cudaStreamSynchronize(w->stream));
+  // a system's particles keep its memory range [first, first + count)
+  for (int k = 0; k < w->nsys; ++k) {
+    int64_t t = 0;
+    for (int m = all[k].first; m < all[k].first + all[k].count; ++m)
+      for (int s = 0; s < std::min(cnt[m], K); ++s) t += partner[(size_t)s * n + m] >= 0;
+    counts[k] = t;
+  }
+  return XDEM_OK;
+}
+
 
 int32_t xdem_get_particles(xdem_world w, xdem_particles* P) {
   if (!w || !P || w->dw.n <= 0) return XDEM_ERR_ARGUMENT;
@@ -848,7 +1110,7 @@ int32_t xdem_get_boundary(xdem_world w, double box[4]) {
 }
 
 int32_t xdem_set_boundary(xdem_world w, const double box[4]) {
-  if (!w || !box) return XDEM_ERR_ARGUMENT;
+  if (!w || !box || w->nsys > 1) return XDEM_ERR_ARGUMENT;
   WorldScalars s;
   CK(w, read_scalars(w, &s));
   s.xmin = box[0];
@@ -881,7 +1143,7 @@ int32_t xdem_get_lees_edwards(xdem_world w, double out[4]) {
 }
 
 int32_t xdem_set_lees_edwards(xdem_world w, const double in[4]) {
-  if (!w || !in) return XDEM_ERR_ARGUMENT;
+  if (!w || !in || w->nsys > 1) return XDEM_ERR_ARGUMENT;
   WorldScalars s;
   CK(w, read_scalars(w, &s));
   s.shift = in[0];
@@ -894,60 +1156,49 @@ int32_t xdem_set_lees_edwards(xdem_world w, const double in[4]) {
 
 int32_t xdem_set_shift_strain_rate(xdem_world w, double rate) {
   if (!w) return XDEM_ERR_ARGUMENT;
-  WorldScalars s;
-  CK(w, read_scalars(w, &s));
-  s.shift_rate = rate;
-  s.shift_vel = rate * s.ylen;
-  CK(w, write_scalars(w, &s));
+  CK(w, modify_all(w, [&](WorldScalars& s, int) {
+       s.shift_rate = rate;
+       s.shift_vel = rate * s.ylen;
+     }));
   return XDEM_OK;
 }
 
 int32_t xdem_set_time_increment(xdem_world w, double dt) {
   if (!w || !(dt > 0.0)) return XDEM_ERR_ARGUMENT;
-  WorldScalars s;
-  CK(w, read_scalars(w, &s));
-  s.dt = dt;
   w->prm.dt = dt;
-  CK(w, write_scalars(w, &s));
+  CK(w, modify_all(w, [&](WorldScalars& s, int) { s.dt = dt; }));
   return XDEM_OK;
 }
 
 int32_t xdem_set_global_damping(xdem_world w, double g) {
   if (!w) return XDEM_ERR_ARGUMENT;
-  WorldScalars s;
-  CK(w, read_scalars(w, &s));
-  s.g = g;
-  CK(w, write_scalars(w, &s));
+  CK(w, modify_all(w, [&](WorldScalars& s, int) { s.g = g; }));
   return XDEM_OK;
 }
 
 int32_t xdem_set_contact_model(xdem_world w, double kn, double kt, double e, double mu) {
   if (!w) return XDEM_ERR_ARGUMENT;
-  WorldScalars s;
-  CK(w, read_scalars(w, &s));
-  s.kn = kn;
-  s.kt = kt;
-  s.mu = mu;
-  s.factor = factor_of(kn, e);
-  CK(w, write_scalars(w, &s));
+  const double factor = factor_of(kn, e);
+  CK(w, modify_all(w, [&](WorldScalars& s, int) {
+       s.kn = kn;
+       s.kt = kt;
+       s.mu = mu;
+       s.factor = factor;
+     }));
   return XDEM_OK;
 }
 
 int32_t xdem_set_virtual_boundary_mass(xdem_world w, double mass) {
   if (!w) return XDEM_ERR_ARGUMENT;
-  WorldScalars s;
-  CK(w, read_scalars(w, &s));
-  s.vmass = mass >= 0 ? mass : w->control_mass;
-  CK(w, write_scalars(w, &s));
+  CK(w, modify_all(w, [&](WorldScalars& s, int k) {
+       s.vmass = mass >= 0 ? mass : w->control_mass[k];
+     }));
   return XDEM_OK;
 }
 
 int32_t xdem_set_max_strain_rate(xdem_world w, double r) {
   if (!w) return XDEM_ERR_ARGUMENT;
-  WorldScalars s;
-  CK(w, read_scalars(w, &s));
-  s.max_strain_rate = r;
-  CK(w, write_scalars(w, &s));
+  CK(w, modify_all(w, [&](WorldScalars& s, int) { s.max_strain_rate = r; }));
   return XDEM_OK;
 }
 
@@ -1082,7 +1333,7 @@ int32_t xdem_update_lees_edwards_boundary(xdem_world w) {
 int32_t xdem_scale_boundary_to_solid_fraction(xdem_world w, double phi) {
   // scaleBoundarySizeToGivenSolidFraction (PeriodicBoundaryWorld.cpp:276-284)
   SUBSTEP_BEGIN;
-  if (!(phi > 0.0)) return XDEM_ERR_ARGUMENT;
+  if (!(phi > 0.0) || w->nsys > 1) return XDEM_ERR_ARGUMENT;
   WorldScalars s;
   CK(w, read_scalars(w, &s));
   double cur = w->total_volume / (s.xlen * s.ylen);
@@ -1114,6 +1365,8 @@ int32_t xdem_run(xdem_world w, int32_t nsteps, const xdem_control* ctl, int32_t*
   if (!ctl || nsteps < 0 || ctl->sequence < 0 || ctl->sequence > 1 || ctl->box_law < 0 ||
       ctl->box_law > 4)
     return XDEM_ERR_ARGUMENT;
+  // a batch steps all its systems together (one slot-set parity)
+  if (w->nsys > 1 && ctl->stop_on_pressure) return XDEM_ERR_ARGUMENT;
   if (steps_done) *steps_done = 0;
   if (nsteps == 0) return XDEM_OK;
   WorldScalars s;

@@ -22,23 +22,47 @@ constexpr int kCandidateCap = 200;  // MAXIMUM_POSSIBLE_CONTACT_LIST_SIZE (BaseW
 
 struct Grid {
   int nx, ny, ncell;
+  int base;  // first cell of the system in the cell arrays
   double lx, ly;
 };
 
+// system of the particle at memory position m
+__device__ __forceinline__ int sys_at(const DevWorld& w, int m) {
+  return w.nsys > 1 ? w.sys_of[m] : 0;
+}
+
+// run-level stop flag (set by a stop condition; ends the kernels of a run)
+__device__ __forceinline__ bool stopped(const DevWorld& w) { return w.ws->stop != 0; }
+
 // Grid of PeriodicBoundaryWorld::findPossibleContacts (PeriodicBoundaryWorld.cpp:17-22):
 // nx = floor(xlen / (2.01 r_max)); clamped to the allocated capacity, which
-// only makes cells larger and leaves the contact set unchanged.
-__device__ __forceinline__ Grid grid_of(const WorldScalars& ws, int nx_cap, int ny_cap) {
+// only makes cells larger and leaves the contact set unchanged.  Regular cell
+// (ix, iy) is base + iy*nx + ix; the Lees-Edwards ghost rows follow at
+// base + ncell.
+__device__ __forceinline__ Grid grid_of(const WorldScalars& ws) {
   Grid g;
   double xlen = ws.xmax - ws.xmin, ylen = ws.ymax - ws.ymin;
   g.nx = (int)floor(xlen / ws.maxsize);
   g.ny = (int)floor(ylen / ws.maxsize);
-  if (g.nx > nx_cap) g.nx = nx_cap;
-  if (g.ny > ny_cap) g.ny = ny_cap;
+  if (g.nx > ws.nx_cap) g.nx = ws.nx_cap;
+  if (g.ny > ws.ny_cap) g.ny = ws.ny_cap;
   g.ncell = g.nx * g.ny;
+  g.base = ws.cell_base;
   g.lx = xlen / g.nx;
   g.ly = ylen / g.ny;
   return g;
+}
+
+// system owning cell c (binary search over the systems' first cells)
+__device__ __forceinline__ int sys_of_cell(const DevWorld& w, int c) {
+  if (w.nsys <= 1) return 0;
+  int lo = 0, hi = w.nsys - 1;
+  while (lo < hi) {
+    int mid = (lo + hi + 1) >> 1;
+    if (w.sys_cell_base[mid] <= c) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
 }
 
 // cell of a coordinate; the reference's floor() can reach numGrid at the upper
@@ -52,15 +76,37 @@ __device__ __forceinline__ void raise(uint32_t* status, uint32_t bits) {
   if (bits) atomicOr(status, bits);
 }
 
+// A thread's status bits and closest-approach Newton counts, combined over
+// its warp and added by one lane: the counters are single addresses shared by
+// the whole grid, where one atomic per thread would serialise.  Every lane of
+// the warp must call it.
+__device__ __forceinline__ void flush_warp(const DevWorld& w, uint32_t st, uint32_t solves,
+                                           uint32_t iters, uint32_t capped) {
+  const unsigned full = 0xffffffffu;
+  st = __reduce_or_sync(full, st);
+  solves = __reduce_add_sync(full, solves);
+  iters = __reduce_add_sync(full, iters);
+  capped = __reduce_add_sync(full, capped);
+  if ((threadIdx.x & 31) == 0) {
+    if (st) atomicOr(w.status, st);
+    if (solves) {
+      WorldScalars* wsm = w.ws;
+      atomicAdd(&wsm->newton_solves, (unsigned long long)solves);
+      atomicAdd(&wsm->newton_iters, (unsigned long long)iters);
+      if (capped) atomicAdd(&wsm->newton_capped, (unsigned long long)capped);
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // a2: modifyParticlePosition (PeriodicBoundaryWorld.cpp:129-142,
 //     LeesEdwardsBoundaryWorld.cpp:304-333)
 // ---------------------------------------------------------------------------
 __global__ void k_modify_position(DevWorld w) {
-  const WorldScalars& ws = *w.ws;
-  if (ws.stop) return;
+  if (stopped(w)) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= w.n) return;
+  const WorldScalars& ws = w.ws[sys_at(w, i)];
   double2 p = w.pos[i];
   if (w.kind == WORLD_LE) {
     if (p.y < ws.ymin) {
@@ -84,9 +130,9 @@ __global__ void k_modify_position(DevWorld w) {
 // scaleAllParticlePosition(scale_x, scale_y) (BaseWorld.cpp:119-124); after a
 // run's stop the scales are 1 and the pass leaves positions unchanged
 __global__ void k_scale_positions(DevWorld w) {
-  const WorldScalars& ws = *w.ws;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= w.n) return;
+  const WorldScalars& ws = w.ws[sys_at(w, i)];
   double2 p = w.pos[i];
   p.x *= ws.scale_x;
   p.y *= ws.scale_y;
@@ -95,10 +141,10 @@ __global__ void k_scale_positions(DevWorld w) {
 
 // a6: LeesEdwardsBoundaryWorld::apply/removeBackgroudVelocity (:508-530)
 __global__ void k_background_velocity(DevWorld w, int apply) {
-  const WorldScalars& ws = *w.ws;
-  if (ws.stop) return;
+  if (stopped(w)) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= w.n) return;
+  const WorldScalars& ws = w.ws[sys_at(w, i)];
   double2 v = w.vel[i];
   double y = w.pos[i].y;
   if (apply) v.x = v.x + ws.shift_rate * y;
@@ -115,18 +161,20 @@ __global__ void k_background_velocity(DevWorld w, int apply) {
 // The order inside a cell is not fixed; nothing downstream depends on it.
 // ---------------------------------------------------------------------------
 __global__ void k_bin(DevWorld w) {
-  const WorldScalars& ws = *w.ws;
-  if (ws.stop) return;
+  if (stopped(w)) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
-  Grid G = grid_of(ws, w.nx_cap, w.ny_cap);
-  if (i == 0 && (G.nx < 3 || G.ny < 3)) raise(w.status, ST_GRID);
   if (i >= w.n) return;
+  const WorldScalars& ws = w.ws[sys_at(w, i)];
+  Grid G = grid_of(ws);
   w.incnt[i] = 0;  // incoming-contact counters of this step's update
-  if (G.nx < 3 || G.ny < 3) return;
+  if (G.nx < 3 || G.ny < 3) {
+    if (i == ws.first) raise(w.status, ST_GRID);
+    return;
+  }
   double2 p = w.pos[i];
   int ix = cell_of(p.x, ws.xmin, G.lx, G.nx);
   int iy = cell_of(p.y, ws.ymin, G.ly, G.ny);
-  int c = iy * G.nx + ix;
+  int c = G.base + iy * G.nx + ix;
   w.pcell[i] = c;
   w.prank[i] = atomicAdd(&w.cell_count[c], 1);
   int gc = -1;
@@ -135,12 +183,12 @@ __global__ void k_bin(DevWorld w) {
       double t = p.x + ws.shift;
       if (t < ws.xmin) t += ws.xlen;
       else if (t > ws.xmax) t -= ws.xlen;
-      gc = G.ncell + cell_of(t, ws.xmin, G.lx, G.nx);
+      gc = G.base + G.ncell + cell_of(t, ws.xmin, G.lx, G.nx);
     } else if (iy == G.ny - 1) {
       double t = p.x - ws.shift;
       if (t < ws.xmin) t += ws.xlen;
       else if (t > ws.xmax) t -= ws.xlen;
-      gc = G.ncell + G.nx + cell_of(t, ws.xmin, G.lx, G.nx);
+      gc = G.base + G.ncell + G.nx + cell_of(t, ws.xmin, G.lx, G.nx);
     }
   }
   w.gcell[i] = gc;
@@ -179,10 +227,8 @@ __device__ __forceinline__ int32_t block_inclusive_scan(int32_t v, int32_t* sh_w
 }
 
 __global__ void __launch_bounds__(kScanThreads) k_scan_tiles(DevWorld w) {
-  const WorldScalars& ws = *w.ws;
-  if (ws.stop) return;
-  Grid G = grid_of(ws, w.nx_cap, w.ny_cap);
-  int total = G.ncell + 2 * G.nx;
+  if (stopped(w)) return;
+  const int total = w.ncell_total;
   int ntiles = (total + kScanTile - 1) / kScanTile;
   __shared__ int32_t sh_warp[kScanThreads / 32];
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
@@ -199,10 +245,8 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_tiles(DevWorld w) {
 
 // exclusive scan of the tile sums (one block); cell_start[total] = total count
 __global__ void __launch_bounds__(kScanThreads) k_scan_sums(DevWorld w) {
-  const WorldScalars& ws = *w.ws;
-  if (ws.stop) return;
-  Grid G = grid_of(ws, w.nx_cap, w.ny_cap);
-  int total = G.ncell + 2 * G.nx;
+  if (stopped(w)) return;
+  const int total = w.ncell_total;
   int ntiles = (total + kScanTile - 1) / kScanTile;
   __shared__ int32_t sh_warp[kScanThreads / 32];
   int32_t carry = 0;
@@ -221,10 +265,8 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_sums(DevWorld w) {
 }
 
 __global__ void __launch_bounds__(kScanThreads) k_scan_apply(DevWorld w) {
-  const WorldScalars& ws = *w.ws;
-  if (ws.stop) return;
-  Grid G = grid_of(ws, w.nx_cap, w.ny_cap);
-  int total = G.ncell + 2 * G.nx;
+  if (stopped(w)) return;
+  const int total = w.ncell_total;
   int ntiles = (total + kScanTile - 1) / kScanTile;
   __shared__ int32_t sh_warp[kScanThreads / 32];
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
@@ -248,14 +290,13 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_apply(DevWorld w) {
 
 // also clears cell_count (already consumed by the scan) for the next binning
 __global__ void k_scatter(DevWorld w) {
-  const WorldScalars& ws = *w.ws;
-  if (ws.stop) return;
-  Grid G = grid_of(ws, w.nx_cap, w.ny_cap);
-  int total = G.ncell + 2 * G.nx;
+  if (stopped(w)) return;
+  const int total = w.ncell_total;
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < total; c += gridDim.x * blockDim.x)
     w.cell_count[c] = 0;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= w.n) return;
+  const Grid G = grid_of(w.ws[sys_at(w, i)]);
   if (G.nx < 3 || G.ny < 3) return;
   const double2 p = w.pos[i];
   ScreenRec r;
@@ -339,8 +380,7 @@ __device__ __forceinline__ void isort(T* key, int cnt) {
 // Particles with no contact are rattlers (BaseWorld.cpp:25,44-45).
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(128) k_collect(DevWorld w, int par) {
-  const WorldScalars& ws = *w.ws;
-  if (ws.stop) return;
+  if (stopped(w)) return;
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= w.n) return;
   const int n = w.n, K = w.K;
@@ -406,10 +446,10 @@ __device__ __forceinline__ bool is_rattler(const DevWorld& w, int m) {
 // ---------------------------------------------------------------------------
 template <bool FOLD_BG>
 __global__ void k_integrate(DevWorld w, int reset_rattlers) {
-  const WorldScalars& ws = *w.ws;
-  if (ws.stop) return;
+  if (stopped(w)) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= w.n) return;
+  const WorldScalars& ws = w.ws[sys_at(w, i)];
   const double dt = ws.dt, g = ws.g;
   const int set = w.setting[i];
   const int id = w.id_of[i];
@@ -490,8 +530,7 @@ __global__ void k_integrate(DevWorld w, int reset_rattlers) {
 
 // BaseWorld::resetVelocityOfRattlers / scaleVelocityOfRattlers (BaseWorld.cpp:79-106)
 __global__ void k_rattlers(DevWorld w, int reset, double scale) {
-  const WorldScalars& ws = *w.ws;
-  if (ws.stop) return;
+  if (stopped(w)) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= w.n) return;
   if (w.setting[i] & SKIP_MACRO_SUM) return;
@@ -534,25 +573,55 @@ __device__ __forceinline__ void own_stress(const DevWorld& w, const Slots& cur, 
   }
 }
 
+// the stress contribution of the body at memory position p
+__device__ __forceinline__ mat2<double> body_stress(const DevWorld& w, const Slots& cur, int p) {
+  mat2<double> s = M(0.0, 0.0, 0.0, 0.0);
+  if (w.setting[p] & SKIP_MACRO_SUM) return s;
+  if (w.shape[p] == SHAPE_CLUMP) {
+    // one running sum over all sub-particles (GluedParticle.cpp:128-137)
+    int id = w.id_of[p];
+    for (int k = 1; k <= w.num_sub[p]; ++k) {
+      int sk = w.mpos[id + k];
+      own_stress(w, cur, sk, true, w.branch[sk], s);
+    }
+  } else {
+    own_stress(w, cur, p, false, make_double2(0.0, 0.0), s);
+  }
+  return s;
+}
+
+// batched worlds: one block per system sums the system's bodies (its memory
+// range) in a fixed tree and divides by its box area
+__global__ void __launch_bounds__(kReduceBlock) k_stress_systems(DevWorld w, int par) {
+  if (stopped(w)) return;
+  __shared__ double sh[4][kReduceBlock];
+  WorldScalars& ws = w.ws[blockIdx.x];
+  const Slots& cur = w.slots[par];
+  const int t = threadIdx.x;
+  mat2<double> s = M(0.0, 0.0, 0.0, 0.0);
+  for (int p = ws.first + t; p < ws.first + ws.count; p += kReduceBlock) s = s + body_stress(w, cur, p);
+  sh[0][t] = s.xx;
+  sh[1][t] = s.xy;
+  sh[2][t] = s.yx;
+  sh[3][t] = s.yy;
+  __syncthreads();
+  for (int off = kReduceBlock / 2; off > 0; off >>= 1) {
+    if (t < off)
+      for (int c = 0; c < 4; ++c) sh[c][t] += sh[c][t + off];
+    __syncthreads();
+  }
+  if (t == 0) {
+    double area = ws.xlen * ws.ylen;
+    for (int c = 0; c < 4; ++c) ws.stress[c] = sh[c][0] / area;
+  }
+}
+
 __global__ void __launch_bounds__(kReduceBlock) k_stress_partial(DevWorld w, int par) {
-  const WorldScalars& ws = *w.ws;
-  if (ws.stop) return;
+  if (stopped(w)) return;
   __shared__ double sh[4][kReduceBlock];
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   mat2<double> s = M(0.0, 0.0, 0.0, 0.0);
-  if (p < w.n && !(w.setting[p] & SKIP_MACRO_SUM)) {
-    const Slots& cur = w.slots[par];
-    if (w.shape[p] == SHAPE_CLUMP) {
-      // one running sum over all sub-particles (GluedParticle.cpp:128-137)
-      int id = w.id_of[p];
-      for (int k = 1; k <= w.num_sub[p]; ++k) {
-        int sk = w.mpos[id + k];
-        own_stress(w, cur, sk, true, w.branch[sk], s);
-      }
-    } else {
-      own_stress(w, cur, p, false, make_double2(0.0, 0.0), s);
-    }
-  }
+  if (p < w.n) s = body_stress(w, w.slots[par], p);
   int t = threadIdx.x;
   sh[0][t] = s.xx;
   sh[1][t] = s.xy;
@@ -571,7 +640,7 @@ __global__ void __launch_bounds__(kReduceBlock) k_stress_partial(DevWorld w, int
 // sums nblocks partials in a fixed tree; divides by the box area
 __global__ void k_stress_final(DevWorld w, int nblocks) {
   WorldScalars& ws = *w.ws;
-  if (ws.stop) return;
+  if (ws.stop) return;  // single-system worlds only
   __shared__ double sh[4][1024];
   int t = threadIdx.x;
   double acc[4] = {0.0, 0.0, 0.0, 0.0};
@@ -673,10 +742,14 @@ __device__ __forceinline__ void box_law(WorldScalars& ws, int law, double p0, do
 // End-of-step scalar work: Lees-Edwards update (LeesEdwardsBoundaryWorld.cpp:
 // 285-296, part of its takeTimeStep), then the driver's box law, the step
 // count and the stop test.  After a stop the scales are 1.
+// One thread per system; the run-level counters and the stop test (single
+// systems only) belong to system 0.
 __global__ void k_end_of_step(DevWorld w, int law, double p0, double p1, int le_update,
                               int stop_on_pressure, double stop_pressure, int count_step) {
-  WorldScalars& ws = *w.ws;
-  if (ws.stop) {
+  const int sys = blockIdx.x * blockDim.x + threadIdx.x;
+  if (sys >= w.nsys) return;
+  WorldScalars& ws = w.ws[sys];
+  if (stopped(w)) {
     ws.scale_x = 1.0;
     ws.scale_y = 1.0;
     return;
@@ -689,6 +762,7 @@ __global__ void k_end_of_step(DevWorld w, int law, double p0, double p1, int le_
     else if (ws.shift < ws.xmin) ws.shift += ws.xlen;
   }
   if (law != BOX_NONE) box_law(ws, law, p0, p1);
+  if (sys != 0) return;
   if (count_step) {
     ws.steps_done += 1;
     ws.flips += 1;

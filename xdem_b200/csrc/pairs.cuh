@@ -63,11 +63,23 @@ __device__ __forceinline__ bool coarse_pass(int shape_i, int shape_j, double r_i
       LAW == LAW_CIRCLE || (LAW == LAW_ANY && shape_i == SHAPE_CIRCLE && shape_j == SHAPE_CIRCLE);
   const bool ellipses = LAW == LAW_CLOSEST || LAW == LAW_INTERSECTION ||
                         (LAW == LAW_ANY && shape_i == SHAPE_ELLIPSE && shape_j == SHAPE_ELLIPSE);
+  // the squared distance decides unless it lies within 1e-14 (relative) of
+  // the squared radius sum, where the reference's expression (with its
+  // correctly rounded sqrt) is evaluated as written
   if (circles) {
-    double distance = len(pb - pa);
-    return !((r_i + r_j) - distance < 0.0);
+    const vec2<double> dv = pb - pa;
+    const double R = r_i + r_j, d2 = len2(dv), R2 = R * R;
+    if (d2 < R2 * (1.0 - 1e-14)) return true;
+    if (d2 > R2 * (1.0 + 1e-14)) return false;
+    double distance = len(dv);
+    return !(R - distance < 0.0);
   }
-  if (ellipses) return (orad_i + orad_j) > sqrt(len2(pa - pb));
+  if (ellipses) {
+    const double R = orad_i + orad_j, d2 = len2(pa - pb), R2 = R * R;
+    if (d2 < R2 * (1.0 - 1e-14)) return true;
+    if (d2 > R2 * (1.0 + 1e-14)) return false;
+    return R > sqrt(len2(pa - pb));
+  }
   return true;
 }
 
@@ -91,16 +103,16 @@ __device__ __forceinline__ Neighbourhood neighbourhood(const Grid& G, int world_
       int jy = iy + dy;
       if (world_kind == WORLD_LE && (jy == -1 || jy == G.ny)) {
         if (jy == -1) {
-          nb.cell[k] = G.ncell + G.nx + jx;
+          nb.cell[k] = G.base + G.ncell + G.nx + jx;
           nb.kind[k] = CAND_BOTTOM;
         } else {
-          nb.cell[k] = G.ncell + jx;
+          nb.cell[k] = G.base + G.ncell + jx;
           nb.kind[k] = CAND_TOP;
         }
       } else {
         if (jy == -1) jy = G.ny - 1;
         else if (jy == G.ny) jy = 0;
-        nb.cell[k] = jy * G.nx + jx;
+        nb.cell[k] = G.base + jy * G.nx + jx;
         nb.kind[k] = CAND_REGULAR;
       }
     }
@@ -117,10 +129,10 @@ __device__ __forceinline__ Neighbourhood neighbourhood(const Grid& G, int world_
 // orientation for the pair kernel, computed once per body instead of per pair.
 template <int LAW>
 __global__ void __launch_bounds__(128) k_candidates(DevWorld w, int par) {
-  const WorldScalars& ws = *w.ws;
-  if (ws.stop) return;
+  if (stopped(w)) return;
   const int m = blockIdx.x * blockDim.x + threadIdx.x;
   const bool valid = m < w.n;
+  const WorldScalars& ws = w.ws[valid ? sys_at(w, m) : 0];
   const int n = w.n, K = w.K;
   const Slots& old = w.slots[par];
   const Slots& cur = w.slots[par ^ 1];
@@ -133,7 +145,7 @@ __global__ void __launch_bounds__(128) k_candidates(DevWorld w, int par) {
       const double r = w.rot[m];
       w.cs[m] = make_double2(cos(r), sin(r));
     }
-    Grid G = grid_of(ws, w.nx_cap, w.ny_cap);
+    Grid G = grid_of(ws);
     const int id_i = w.id_of[m];
     const int nold = min(old.count[m], K);
     uint32_t seen = 0;
@@ -200,19 +212,26 @@ __global__ void __launch_bounds__(128) k_candidates(DevWorld w, int par) {
     cur.count[m] = nlist;
     w.seen[m] = seen;
   }
-  // reserve room in the pair list for the whole warp at once
+  // reserve room in the pair list for the whole block at once (one atomic
+  // per block on the shared counter)
   const unsigned full = 0xffffffffu;
-  const int lane = threadIdx.x & 31;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   int incl = nlist;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
     int v = __shfl_up_sync(full, incl, o);
     if (lane >= o) incl += v;
   }
-  int total = __shfl_sync(full, incl, 31);
-  int base = 0;
-  if (lane == 31 && total > 0) base = atomicAdd(w.npairs, total);
-  base = __shfl_sync(full, base, 31);
+  __shared__ int warp_total[4], block_base;
+  if (lane == 31) warp_total[warp] = incl;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const int tot = warp_total[0] + warp_total[1] + warp_total[2] + warp_total[3];
+    block_base = tot > 0 ? atomicAdd(w.npairs, tot) : 0;
+  }
+  __syncthreads();
+  int base = block_base;
+  for (int k = 0; k < warp; ++k) base += warp_total[k];
   int at = base + incl - nlist;
   for (int s = 0; s < nlist; ++s) w.pairs[at + s] = PairEntry{m, w.cell_mem[list_q[s]], list_code[s], 0};
   raise(w.status, st);
@@ -221,18 +240,18 @@ __global__ void __launch_bounds__(128) k_candidates(DevWorld w, int par) {
 // ---- phase B --------------------------------------------------------------------
 template <bool FOLD_BG, int LAW>
 __global__ void __launch_bounds__(128, 4) k_pair_forces(DevWorld w, int par, int record) {
-  const WorldScalars& ws = *w.ws;
-  if (ws.stop) return;
+  if (stopped(w)) return;
   const int n = w.n, K = w.K;
   const Slots& old = w.slots[par];
   const Slots& cur = w.slots[par ^ 1];
   const int npairs = *w.npairs;
-  const double dt = ws.dt, kn = ws.kn, kt = ws.kt, mu = ws.mu, factor = ws.factor;
   uint32_t st = 0;
   uint32_t n_solves = 0, n_iters = 0, n_capped = 0;
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < npairs; t += gridDim.x * blockDim.x) {
     const PairEntry e = w.pairs[t];
     const int m = e.m, mj = e.mj;
+    const WorldScalars& ws = w.ws[sys_at(w, m)];
+    const double dt = ws.dt, kn = ws.kn, kt = ws.kt, mu = ws.mu, factor = ws.factor;
     const int kind = e.code & 0xff, slot = (e.code >> 8) & 0xff, o = (e.code >> 16) & 0xff;
     const size_t ci = (size_t)slot * n + m;
     PState a = load_state<FOLD_BG>(w, ws, m);
@@ -322,19 +341,12 @@ __global__ void __launch_bounds__(128, 4) k_pair_forces(DevWorld w, int par, int
     if (pos < K) w.inref[(size_t)pos * n + mj] = (uint32_t)m * (uint32_t)K + (uint32_t)slot;
     else st |= ST_CAPACITY;
   }
-  raise(w.status, st);
-  if (n_solves) {
-    WorldScalars* wsm = w.ws;
-    atomicAdd(&wsm->newton_solves, (unsigned long long)n_solves);
-    atomicAdd(&wsm->newton_iters, (unsigned long long)n_iters);
-    if (n_capped) atomicAdd(&wsm->newton_capped, (unsigned long long)n_capped);
-  }
+  flush_warp(w, st, n_solves, n_iters, n_capped);
 }
 
 // ---- phase C --------------------------------------------------------------------
 __global__ void __launch_bounds__(128) k_finish_slots(DevWorld w, int par) {
-  const WorldScalars& ws = *w.ws;
-  if (ws.stop) return;
+  if (stopped(w)) return;
   const int m = blockIdx.x * blockDim.x + threadIdx.x;
   if (m == 0) {  // phase B has consumed the lists
     w.ws->last_pairs = *w.npairs;

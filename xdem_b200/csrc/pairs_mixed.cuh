@@ -110,21 +110,10 @@ __device__ __forceinline__ void count_solve(uint32_t it, uint32_t& n_solves, uin
   }
 }
 
-__device__ __forceinline__ void flush_stats(const DevWorld& w, uint32_t st, uint32_t n_solves,
-                                            uint32_t n_iters, uint32_t n_capped) {
-  raise(w.status, st);
-  if (n_solves) {
-    WorldScalars* wsm = w.ws;
-    atomicAdd(&wsm->newton_solves, (unsigned long long)n_solves);
-    atomicAdd(&wsm->newton_iters, (unsigned long long)n_iters);
-    if (n_capped) atomicAdd(&wsm->newton_capped, (unsigned long long)n_capped);
-  }
-}
 
 template <bool FOLD_BG, int LAW>
 __global__ void __launch_bounds__(128, 4) k_pair_forces_m(DevWorld w, int par, int record) {
-  const WorldScalars& ws = *w.ws;
-  if (ws.stop) return;
+  if (stopped(w)) return;
   const int n = w.n;
   const Slots& cur = w.slots[par ^ 1];
   const int npairs = *w.npairs;
@@ -132,6 +121,7 @@ __global__ void __launch_bounds__(128, 4) k_pair_forces_m(DevWorld w, int par, i
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < npairs; t += gridDim.x * blockDim.x) {
     const PairEntry e = w.pairs[t];
     const int m = e.m, mj = e.mj;
+    const WorldScalars& ws = w.ws[sys_at(w, m)];
     const int kind = e.code & 0xff, slot = (e.code >> 8) & 0xff;
     const size_t ci = (size_t)slot * n + m;
     const PState a = load_state<FOLD_BG>(w, ws, m);
@@ -157,8 +147,15 @@ __global__ void __launch_bounds__(128, 4) k_pair_forces_m(DevWorld w, int par, i
         csb = make_double2(cos(b.rot), sin(b.rot));
       }
       res = ellipse_closest_m(a, b, off, ovel, csa, csb, g);
+      // deferred pairs take consecutive list entries, one atomic per warp
+      const unsigned act = __activemask();
+      const unsigned defer = __ballot_sync(act, res == PW_FALLBACK);
       if (res == PW_FALLBACK) {
-        w.fallback[atomicAdd(w.nfallback, 1)] = t;
+        const int lane = threadIdx.x & 31, leader = __ffs(defer) - 1;
+        int base = 0;
+        if (lane == leader) base = atomicAdd(w.nfallback, __popc(defer));
+        base = __shfl_sync(defer, base, leader);
+        w.fallback[base + __popc(defer & ((1u << lane) - 1u))] = t;
         continue;
       }
       count_solve(g.iters, n_solves, n_iters);
@@ -188,15 +185,14 @@ __global__ void __launch_bounds__(128, 4) k_pair_forces_m(DevWorld w, int par, i
     }
     write_contact_m(w, ws, e, a, b, off, g, par, record, st);
   }
-  flush_stats(w, st, n_solves, n_iters, n_capped);
+  flush_warp(w, st, n_solves, n_iters, n_capped);
 }
 
 // the closest-approach pairs deferred by k_pair_forces_m: the reference's FP64
 // construction (EllipticParticle.cpp:34-285), then the mixed force
 template <bool FOLD_BG, int LAW>
 __global__ void __launch_bounds__(128) k_pair_fallback_m(DevWorld w, int par, int record) {
-  const WorldScalars& ws = *w.ws;
-  if (ws.stop) return;
+  if (stopped(w)) return;
   const int n = w.n;
   const Slots& cur = w.slots[par ^ 1];
   const int nfb = *w.nfallback;
@@ -204,6 +200,7 @@ __global__ void __launch_bounds__(128) k_pair_fallback_m(DevWorld w, int par, in
   for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < nfb; f += gridDim.x * blockDim.x) {
     const PairEntry e = w.pairs[w.fallback[f]];
     const int m = e.m, mj = e.mj;
+    const WorldScalars& ws = w.ws[sys_at(w, m)];
     const int kind = e.code & 0xff, slot = (e.code >> 8) & 0xff;
     const size_t ci = (size_t)slot * n + m;
     const PState a = load_state<FOLD_BG>(w, ws, m);
@@ -234,7 +231,7 @@ __global__ void __launch_bounds__(128) k_pair_fallback_m(DevWorld w, int par, in
     geom_to_m(gd, a, g);
     write_contact_m(w, ws, e, a, b, off, g, par, record, st);
   }
-  flush_stats(w, st, n_solves, n_iters, n_capped);
+  flush_warp(w, st, n_solves, n_iters, n_capped);
 }
 
 // single pairs through the mixed geometry (xdem_pair_geometry with

@@ -23,11 +23,12 @@ struct PermList {
 // members of each regular cell in ascending id, their screening copies moved
 // along; newpos = the sorted index
 __global__ void k_sort_cells(DevWorld w) {
-  const WorldScalars& ws = *w.ws;
-  if (ws.stop) return;
-  Grid G = grid_of(ws, w.nx_cap, w.ny_cap);
-  if (G.nx < 3 || G.ny < 3) return;
-  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < G.ncell; c += gridDim.x * blockDim.x) {
+  if (stopped(w)) return;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < w.ncell_total;
+       c += gridDim.x * blockDim.x) {
+    const Grid G = grid_of(w.ws[sys_of_cell(w, c)]);
+    // regular cells of a valid grid only (ghost rows hold images)
+    if (G.nx < 3 || G.ny < 3 || c - G.base >= G.ncell) continue;
     int q0 = w.cell_start[c], q1 = w.cell_start[c + 1];
     for (int a = q0 + 1; a < q1; ++a) {
       const int x = w.cell_mem[a];
@@ -72,12 +73,11 @@ __device__ __forceinline__ void move_elem(void* src, int si, void* dst, int di) 
 
 // every array element m -> scratch slab at newpos[m]; mpos follows
 __global__ void k_permute(DevWorld w, PermList L) {
-  const WorldScalars& ws = *w.ws;
-  if (ws.stop) return;
-  Grid G = grid_of(ws, w.nx_cap, w.ny_cap);
-  if (G.nx < 3 || G.ny < 3) return;
+  if (stopped(w)) return;
   int m = blockIdx.x * blockDim.x + threadIdx.x;
   if (m >= w.n) return;
+  const Grid G = grid_of(w.ws[sys_at(w, m)]);
+  if (G.nx < 3 || G.ny < 3) return;
   int t = w.newpos[m];
   w.mpos[w.id_of[m]] = t;
   for (int a = 0; a < L.count; ++a) {
@@ -91,12 +91,13 @@ __global__ void k_permute(DevWorld w, PermList L) {
 }
 
 __global__ void k_copy_back(DevWorld w, PermList L) {
-  const WorldScalars& ws = *w.ws;
-  if (ws.stop) return;
-  Grid G = grid_of(ws, w.nx_cap, w.ny_cap);
-  if (G.nx < 3 || G.ny < 3) return;
+  if (stopped(w)) return;
   int m = blockIdx.x * blockDim.x + threadIdx.x;
   if (m >= w.n) return;
+  // a system keeps its memory range, so the slab entry at m was written by a
+  // particle of the same system
+  const Grid G = grid_of(w.ws[sys_at(w, m)]);
+  if (G.nx < 3 || G.ny < 3) return;
   for (int a = 0; a < L.count; ++a) {
     void* src = w.scratch + L.offset[a];
     switch (L.esize[a]) {
@@ -111,13 +112,12 @@ __global__ void k_copy_back(DevWorld w, PermList L) {
 // With an invalid grid the particles did not move and the history is copied
 // in place, so that the slot-set parity stays what the host expects.
 __global__ void k_permute_history(DevWorld w, int par) {
-  WorldScalars& ws = *w.ws;
-  if (ws.stop) return;
-  Grid G = grid_of(ws, w.nx_cap, w.ny_cap);
-  const bool moved = G.nx >= 3 && G.ny >= 3;
+  if (stopped(w)) return;
   int m = blockIdx.x * blockDim.x + threadIdx.x;
-  if (m == 0) ws.flips += 1;
+  if (m == 0) w.ws->flips += 1;
   if (m >= w.n) return;
+  const Grid G = grid_of(w.ws[sys_at(w, m)]);
+  const bool moved = G.nx >= 3 && G.ny >= 3;
   const int n = w.n, K = w.K;
   const Slots& src = w.slots[par];
   const Slots& dst = w.slots[par ^ 1];
@@ -144,11 +144,8 @@ __global__ void k_permute_history(DevWorld w, int par) {
 
 // cell lists hold positions: renumber them
 __global__ void k_remap_cells(DevWorld w) {
-  const WorldScalars& ws = *w.ws;
-  if (ws.stop) return;
-  Grid G = grid_of(ws, w.nx_cap, w.ny_cap);
-  if (G.nx < 3 || G.ny < 3) return;
-  int total = w.cell_start[G.ncell + 2 * G.nx];
+  if (stopped(w)) return;
+  int total = w.cell_start[w.ncell_total];
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < total; q += gridDim.x * blockDim.x)
     w.cell_mem[q] = w.newpos[w.cell_mem[q]];
 }

@@ -54,6 +54,9 @@ struct WorldScalars {
   int32_t steps_done;  // steps completed in the current run
   int32_t flips;       // slot-set swaps executed in the current run
   int32_t last_pairs;  // pairs listed by the last candidate scan
+  // cell grid of this system: capacity per axis and first cell in the cell
+  // arrays; particles (ids and memory positions) [first, first + count)
+  int32_t nx_cap, ny_cap, cell_base, first, count, pad_;
   // closest-approach Newton statistics since the last reset: solves,
   // iterations, solves stopped by the iteration cap
   unsigned long long newton_solves, newton_iters, newton_capped;
@@ -76,13 +79,22 @@ struct ScreenRec {
   int32_t id, up;
 };
 
+// A world holds one system or, batched, nsys independent systems of the same
+// world kind side by side: system s owns the particles (ids and memory
+// positions) [ws[s].first, ws[s].first + ws[s].count), its own block of
+// cells, and its own scalars ws[s]; ids are global, so contacts, slots and
+// the pair list need no system index.  The run-level counters and the stop
+// flag live in ws[0].
 struct DevWorld {
   int n;
   int K;  // slots per particle
   int kind;
   int method;
   int precision;
-  int nx_cap, ny_cap;  // cell-grid capacity
+  int nsys;         // systems in this world
+  int ncell_total;  // cells of all systems (regular + Lees-Edwards ghost rows, at capacity)
+  int32_t* sys_of;  // [n] system of the particle at m (NULL when nsys == 1)
+  int32_t* sys_cell_base;  // [nsys + 1] first cell of each system, then ncell_total
   // particle arrays, memory order
   int32_t* id_of;  // id at position m
   int32_t* mpos;   // [id] position of id
@@ -131,7 +143,7 @@ struct DevWorld {
   int32_t* npairs;  // number of listed pairs
   int32_t* fallback;   // [K*n] mixed precision: listed pairs deferred to the FP64 construction
   int32_t* nfallback;  // number of deferred pairs
-  // scalars, status, scratch
+  // scalars (one per system), status, scratch
   WorldScalars* ws;
   uint32_t* status;
   double* partials;  // block partial sums

@@ -163,3 +163,86 @@ def c2_aspect(rng, n):
 
 def c4_aspect(rng, n):
     return rng.uniform(1.0, 3.0, n)
+
+
+def clump_system(nclump, phi_rsa=0.42, seed=0, vel_sigma=0.01, density=1.0):
+    """GluedParticle clumps of 2-5 circular sub-discs (radii U[0.3,0.6], offsets
+    uniform within radius 0.8 of the clump centre), placed by RSA of their
+    bounding discs at fraction phi_rsa.  Each clump is a row of shape CLUMP
+    (SKIP_CONTACT_DETECTION, the GluedParticle) followed by its sub-discs
+    (SKIP_TIME_INTEGRAL | SKIP_MACRO_SUM, up_level = the clump's id), whose
+    branch vectors and the clump's mass and inertia come from
+    xdem_clump_properties (GluedParticle::calculateParticleProperties)."""
+    rng = np.random.default_rng(seed)
+    k = rng.integers(2, 6, nclump)
+    sub_r = [rng.uniform(0.3, 0.6, kk) for kk in k]
+    sub_off = []
+    bound = np.zeros(nclump)
+    for c in range(nclump):
+        ang = rng.uniform(0.0, 2.0 * np.pi, k[c])
+        rad = 0.8 * np.sqrt(rng.uniform(0.0, 1.0, k[c]))
+        off = np.stack([rad * np.cos(ang), rad * np.sin(ang)], 1)
+        sub_off.append(off)
+        bound[c] = float(np.max(np.hypot(off[:, 0], off[:, 1]) + sub_r[c]))
+    box = box_for(float(np.sum(np.pi * bound ** 2)), phi_rsa)
+    cx, cy = rsa_positions(bound, box, seed + 1)
+    n = int(nclump + k.sum())
+    shape = np.zeros(n, np.int32)
+    radius = np.zeros(n)
+    x = np.zeros(n)
+    y = np.zeros(n)
+    up = np.arange(n, dtype=np.int32)
+    setting = np.zeros(n, np.int32)
+    num_sub = np.zeros(n, np.int32)
+    parent = np.zeros(nclump, np.int64)
+    i = 0
+    for c in range(nclump):
+        parent[c] = i
+        shape[i] = abi.SHAPE_CLUMP
+        radius[i] = 1.0
+        setting[i] = abi.SKIP_CONTACT_DETECTION
+        num_sub[i] = k[c]
+        s = slice(i + 1, i + 1 + k[c])
+        radius[s] = sub_r[c]
+        x[s] = cx[c] + sub_off[c][:, 0]
+        y[s] = cy[c] + sub_off[c][:, 1]
+        up[s] = i
+        setting[s] = abi.SKIP_TIME_INTEGRAL | abi.SKIP_MACRO_SUM
+        i += 1 + k[c]
+    prop_shape = np.where(shape == abi.SHAPE_CLUMP, abi.SHAPE_CIRCLE, shape).astype(np.int32)
+    vx = rng.normal(0.0, vel_sigma, n)
+    vy = rng.normal(0.0, vel_sigma, n)
+    p = assemble(prop_shape, radius, np.ones(n), x, y, vx, vy, np.zeros(n), np.zeros(n), density)
+    p["shape"] = shape
+    p["up_level"] = up
+    p["setting"] = setting
+    p["num_sub"] = num_sub
+    lib = abi.load_library()
+    d = C.POINTER(C.c_double)
+    for c in range(nclump):
+        i = int(parent[c])
+        kk = int(k[c])
+        s = np.arange(i + 1, i + 1 + kk)
+        out = np.zeros(7)
+        brx = np.zeros(kk)
+        bry = np.zeros(kk)
+        st = lib.xdem_clump_properties(
+            kk, np.ascontiguousarray(shape[s]).ctypes.data_as(C.POINTER(C.c_int32)),
+            np.ascontiguousarray(radius[s]).ctypes.data_as(d), np.ones(kk).ctypes.data_as(d),
+            np.ascontiguousarray(x[s]).ctypes.data_as(d), np.ascontiguousarray(y[s]).ctypes.data_as(d),
+            np.zeros(kk).ctypes.data_as(d), density, out.ctypes.data_as(d), brx.ctypes.data_as(d),
+            bry.ctypes.data_as(d))
+        if st:
+            raise abi.XdemError(st, "xdem_clump_properties")
+        p["x"][i], p["y"][i] = out[0], out[1]
+        p["volume"][i], p["mass"][i], p["inv_mass"][i] = out[2], out[3], out[4]
+        p["inertia"][i], p["inv_inertia"][i] = out[5], out[6]
+        # GluedParticle.cpp:71-75: each sub-particle takes the clump's mass and inertia
+        p["mass"][s], p["inv_mass"][s] = out[3], out[4]
+        p["inertia"][s], p["inv_inertia"][s] = out[5], out[6]
+        p["branch_x"][s], p["branch_y"][s] = brx, bry
+        p["vx"][s] = p["vx"][i]
+        p["vy"][s] = p["vy"][i]
+    p["radius"][shape == abi.SHAPE_CLUMP] = -1.0
+    p["outer_radius"] = p["radius"].copy()
+    return p, box

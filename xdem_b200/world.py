@@ -218,6 +218,55 @@ class World(WorldBase):
     def _set_particles(self, s):
         return self.lib.xdem_set_particles(self.h, C.byref(s))
 
+    # ---- batched systems (one handle, many independent systems) ------------
+    def set_batch(self, systems, boxes, dts=None):
+        """Places the systems (particle dicts with local ids) side by side in
+        this world: system s takes the ids first_s + id (xdem_batch_set_particles)."""
+        nsys = len(systems)
+        arr = (abi.Particles * nsys)()
+        for k, p in enumerate(systems):
+            arr[k] = abi.particles_struct(p)
+        self._batch_keep = (systems, arr)
+        boxes = np.ascontiguousarray(np.asarray(boxes, np.float64).reshape(nsys, 4))
+        d = C.POINTER(C.c_double)
+        dts_p = None
+        if dts is not None:
+            dts = np.ascontiguousarray(np.asarray(dts, np.float64))
+            dts_p = dts.ctypes.data_as(d)
+        self.n = int(sum(len(p["x"]) for p in systems))
+        self._check(self.lib.xdem_batch_set_particles(self.h, nsys, arr, boxes.ctypes.data_as(d),
+                                                      dts_p), "batch_set_particles")
+
+    def batch_info(self):
+        """(number of systems, first id of each system followed by n)"""
+        k = C.c_int32(0)
+        self._check(self.lib.xdem_batch_info(self.h, C.byref(k), None), "batch_info")
+        first = np.zeros(k.value + 1, np.int32)
+        self._check(self.lib.xdem_batch_info(self.h, C.byref(k),
+                                             first.ctypes.data_as(C.POINTER(C.c_int32))), "batch_info")
+        return k.value, first
+
+    def batch_stress(self):
+        k, _ = self.batch_info()
+        out = np.zeros((k, 4))
+        self._check(self.lib.xdem_batch_get_stress(self.h, out.ctypes.data_as(C.POINTER(C.c_double))),
+                    "batch_get_stress")
+        return out
+
+    def batch_boundaries(self):
+        k, _ = self.batch_info()
+        out = np.zeros((k, 4))
+        self._check(self.lib.xdem_batch_get_boundaries(
+            self.h, out.ctypes.data_as(C.POINTER(C.c_double))), "batch_get_boundaries")
+        return out
+
+    def batch_count_contacts(self):
+        k, _ = self.batch_info()
+        out = np.zeros(k, np.int64)
+        self._check(self.lib.xdem_batch_count_contacts(
+            self.h, out.ctypes.data_as(C.POINTER(C.c_int64))), "batch_count_contacts")
+        return out
+
     def _get_state(self, s):
         return self.lib.xdem_get_particles(self.h, C.byref(s))
 
