@@ -92,6 +92,45 @@ def workload_le_ellipses(n, seed):
                        "solid_fraction": round(info["phi"], 4), "shear_rate": rate, "dt": dt}}
 
 
+def train_warm_start(seed, n=262144, target_pairs=10_000_000, epochs=3):
+    """The warm-start network of the learned configuration: pairs harvested
+    from a Lees-Edwards shear of n ellipses with a/b ~ U[1,2], b in {0.5, 0.7},
+    solid fraction 0.85 and shear rate 1e-3 sqrt(kn/m_min), trained on the GPU
+    by the library's own kernels."""
+    from xdem_b200 import abi, inputs, packing
+    from xdem_b200.learned import Mlp
+    from xdem_b200.world import World, make_control, make_params
+    t0 = time.time()
+    p, box = inputs.ellipse_system(n, b=inputs.c2_b, aspect=inputs.c2_aspect, phi_rsa_circle=0.40,
+                                   phi=None, seed=seed + 100)
+    dt = inputs.time_step(p)
+    rate = 1e-3 * math.sqrt(inputs.KN / float(np.min(p["mass"])))
+    q, contacts, b, _ = packing.compress(p, box, 0.85, dt, steps=4000, relax=1000)
+    prm = make_params(abi.WORLD_LEES_EDWARDS, dt, b, inputs.KN, inputs.KT, inputs.RESTITUTION,
+                      inputs.FRICTION, shift_strain_rate=rate)
+    w = World(prm)
+    w.raise_mask = ~abi.ERR_NEWTON
+    w.set_particles(q)
+    w.set_contacts(contacts)
+    net = Mlp(seed=seed + 7)
+    steps = 0
+    while net.dataset_size() < target_pairs and steps < 2000:
+        w.run(10, make_control())
+        steps += 10
+        net.harvest(w, stride=1, max_new=target_pairs - net.dataset_size())
+    w.close()
+    t1 = time.time()
+    losses = net.train(epochs, batch=4096, lr=1e-3, seed=seed)
+    t2 = time.time()
+    info = {"harvest": f"LeesEdwardsBoundaryWorld shear of {n} ellipses, a/b U[1,2], phi 0.85, "
+                       f"{steps} steps",
+            "pairs": net.dataset_size(), "epochs": epochs, "batch": 4096,
+            "loss_first_epoch": float(losses[0]), "loss_last_epoch": float(losses[-1]),
+            "harvest_s": round(t1 - t0, 1), "train_s": round(t2 - t1, 1)}
+    log(f"warm start: {info}")
+    return net, info
+
+
 def workload_periodic_discs(n, seed):
     """Bidisperse discs r 0.5/0.7 at phi 0.70, PeriodicBoundaryWorld (config-0 recipe at size n)."""
     from xdem_b200 import abi, inputs
@@ -393,10 +432,12 @@ def measure_loop(work, precision, args):
     return {"value": n * args.steps / (ms.value / 1e3), "ms_per_step": ms.value / args.steps}
 
 
-def measure(work, precision, args, dist, full=True):
+def measure(work, precision, args, dist, full=True, net=None):
     """Times `args.steps` steps of the workload at the given precision.
-    full: also the per-kernel roofline pass and the end-to-end pass."""
+    full: also the per-kernel roofline pass and the end-to-end pass;
+    net: the learned warm start to attach."""
     from xdem_b200 import abi
+    from xdem_b200.learned import warm_stats
     from xdem_b200.world import World
 
     prm = abi.Params()
@@ -420,6 +461,8 @@ def measure(work, precision, args, dist, full=True):
             w.set_contacts(work["contacts"])
     ctl = work["control"]
     lib = w.lib
+    if net is not None:
+        net.attach(w)
 
     def barrier():
         if dist:
@@ -457,6 +500,13 @@ def measure(work, precision, args, dist, full=True):
            "done": done, "contacts": contacts, "launches": int(launches), "clocks": clk,
            "newton": {"solves_per_step": solves / max(done, 1),
                       "iterations_per_solve": iters / max(solves, 1), "capped_solves": capped}}
+    if net is not None:
+        ws = warm_stats(w)
+        off = max(ws["offered"], 1)
+        out["warm_start"] = {"offered_per_step": ws["offered"] / max(done, 1),
+                             "used_fraction": ws["used"] / off,
+                             "fallback_fraction": (ws["rejected"] + ws["restarted"]) / off,
+                             "contact_logit_accuracy": ws["logit_right"] / off}
     if not full:
         out["status"] = w.synchronize()
         w.close()
@@ -528,6 +578,8 @@ def main():
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"],
                     help="arithmetic of the headline path (the other one is timed beside it)")
     ap.add_argument("--no-compare", action="store_true", help="skip the second precision")
+    ap.add_argument("--no-learned", action="store_true",
+                    help="skip training and timing the learned warm start")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-child", default=None, help=argparse.SUPPRESS)
     ap.add_argument("--cpu-kind", default="port", help=argparse.SUPPRESS)
@@ -588,6 +640,16 @@ def main():
     loop = None
     if "systems" in work:
         loop = measure_loop(work, prec[args.precision], args)
+    learned = None
+    if args.workload == "le_ellipses" and not args.no_learned and not args.no_compare:
+        net, tinfo = train_warm_start(args.seed)
+        learned = {"training": tinfo}
+        for name, pr in (("fp64_warm", abi.PRECISION_FP64), ("mixed_warm", abi.PRECISION_MIXED)):
+            r = measure(work, pr, args, dist, full=False, net=net)
+            learned[name] = {"value": r["value"], "ms_per_step": r["ms_per_step"],
+                             "newton": r["newton"], "warm_start": r["warm_start"],
+                             "status": r["status"], "clocks": r["clocks"]}
+        net.close()
 
     # ---- CPU baseline (rank 0, N = 1 only) ----------------------------------
     cpu = None
@@ -626,6 +688,8 @@ def main():
                                    "what": "one world per system, each run for the K steps in "
                                            "turn on one stream"}
         line["speedup_vs_per_system_loop"] = head["value"] / loop["value"]
+    if learned is not None:
+        line["learned"] = learned
     if cmp_ is not None:
         line[other] = {"value": cmp_["value"], "ms_per_step": cmp_["ms_per_step"],
                        "contacts": cmp_["contacts"], "newton": cmp_["newton"],

@@ -182,6 +182,7 @@ typedef struct xdem_contacts {
 } xdem_contacts;
 
 typedef struct xdem_world_s* xdem_world;
+typedef struct xdem_mlp_s* xdem_mlp;
 
 /* ---- library ---------------------------------------------------------- */
 int32_t xdem_abi_version(void);
@@ -370,6 +371,58 @@ int32_t xdem_pair_geometry(int32_t npairs, int32_t ellipse_method, int32_t preci
                            const double* pi /* npairs*9 */, const double* pj /* npairs*9 */,
                            const double* offset /* npairs*4: ox, oy, ovx, ovy */,
                            double* out /* npairs*17 */);
+
+/* ---- learned warm start of the closest-approach Newton iteration ---------- */
+/* No counterpart in the reference.  A network (7 inputs: the centre offset in
+   ellipse i's frame over b_i, cos and sin of θ_j - θ_i, a_i/b_i, a_j/b_i,
+   b_j/b_i; three hidden layers of 64 with SiLU; outputs: the root of the
+   reference's quartic (EllipticParticle.cpp:92-100, 163) as a fraction of
+   Newton's analytic start sqrt(δ+1), and a contact logit), BF16 weights with
+   FP32 accumulation on the tensor cores, trained on pairs harvested from a
+   world.  With xdem_set_warm_start a closest-approach world starts Newton
+   from the prediction when its first step is small, keeps the plain start
+   otherwise, and iterates to the reference's tolerance either way, so the
+   result is the plain solver's; xdem_get_warm_stats counts what happened. */
+int32_t xdem_mlp_create(uint64_t seed, xdem_mlp* out);
+int32_t xdem_mlp_destroy(xdem_mlp m);
+/* number of FP32 parameters: W1[64][16], b1[64], W2[64][64], b2[64],
+   W3[64][64], b3[64], W4[8][64], b4[8] (input columns 7..15 of W1 and
+   output rows 2..7 of W4 are padding and stay zero) */
+int32_t xdem_mlp_param_count(void);
+/* parameters (host arrays of xdem_mlp_param_count floats) and the 7 input
+   scales (each feature is multiplied by its scale); either may be NULL */
+int32_t xdem_mlp_get_params(xdem_mlp m, float* theta, float* scale);
+int32_t xdem_mlp_set_params(xdem_mlp m, const float* theta, const float* scale);
+/* forward pass of n rows of 7 features (host arrays; y: 2 per row) */
+int32_t xdem_mlp_forward(xdem_mlp m, int64_t n, const float* x, float* y);
+/* gradient of the mean loss over n samples (host arrays: x 7 per row,
+   target root fraction or NaN where no root exists, contact 0/1):
+   (y0 - target)^2 where the target exists + 0.1 * BCE(y1, contact) */
+int32_t xdem_mlp_gradient(xdem_mlp m, int64_t n, const float* x, const float* target,
+                          const float* contact, float* grad, float* loss);
+/* the network's training set: append host samples, read it back (arrays
+   may be NULL; *size receives the count), clear it */
+int32_t xdem_mlp_add_samples(xdem_mlp m, int64_t n, const float* x, const float* target,
+                             const float* contact);
+int32_t xdem_mlp_dataset(xdem_mlp m, int64_t* size, float* x, float* target, float* contact);
+int32_t xdem_mlp_clear_dataset(xdem_mlp m);
+/* Adam over the training set (first max_samples, 0 = all): epochs passes of
+   shuffled mini-batches (batch >= 64); epoch_loss (may be NULL) receives the
+   mean loss of each epoch */
+int32_t xdem_mlp_train(xdem_mlp m, int32_t epochs, int32_t batch, float lr, uint64_t seed,
+                       int64_t max_samples, float* epoch_loss);
+/* appends to m's training set every stride-th ellipse pair of the world's
+   last candidate list (features, the plain Newton root as a fraction of its
+   start or NaN, contact flag); at most max_new, *added receives the count */
+int32_t xdem_harvest_pairs(xdem_world w, xdem_mlp m, int32_t stride, int64_t max_new,
+                           int64_t* added);
+/* m (NULL: off) gives the closest-approach Newton iteration of this world its
+   warm start from the next step on; m must outlive the setting */
+int32_t xdem_set_warm_start(xdem_world w, xdem_mlp m);
+/* since the last xdem_reset_newton_stats: {starts offered, used, rejected by
+   the residual test, used but overruled by the plain start, contact logits
+   that matched the outcome} */
+int32_t xdem_get_warm_stats(xdem_world w, int64_t out[5]);
 
 /* ---- allocation-free stress ---------------------------------------------- */
 /* No counterpart in the reference.  For callers that cannot allocate device

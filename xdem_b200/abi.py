@@ -50,6 +50,7 @@ class XdemError(RuntimeError):
 
 _d = C.POINTER(C.c_double)
 _i = C.POINTER(C.c_int32)
+_f = C.POINTER(C.c_float)
 
 
 class Params(C.Structure):
@@ -237,6 +238,20 @@ def load_library(path=LIB_PATH):
         "xdem_total_stress_noalloc_max_contacts": (C.c_int64, []),
         "xdem_host_alloc": (C.c_void_p, [C.c_int64]),
         "xdem_range_push": (C.c_int32, [C.c_char_p]),
+        "xdem_mlp_create": (C.c_int32, [C.c_uint64, P(W)]),
+        "xdem_mlp_destroy": (C.c_int32, [W]),
+        "xdem_mlp_param_count": (C.c_int32, []),
+        "xdem_mlp_get_params": (C.c_int32, [W, _f, _f]),
+        "xdem_mlp_set_params": (C.c_int32, [W, _f, _f]),
+        "xdem_mlp_forward": (C.c_int32, [W, C.c_int64, _f, _f]),
+        "xdem_mlp_gradient": (C.c_int32, [W, C.c_int64, _f, _f, _f, _f, _f]),
+        "xdem_mlp_add_samples": (C.c_int32, [W, C.c_int64, _f, _f, _f]),
+        "xdem_mlp_dataset": (C.c_int32, [W, P(C.c_int64), _f, _f, _f]),
+        "xdem_mlp_clear_dataset": (C.c_int32, [W]),
+        "xdem_mlp_train": (C.c_int32, [W, C.c_int32, C.c_int32, C.c_float, C.c_uint64, C.c_int64, _f]),
+        "xdem_harvest_pairs": (C.c_int32, [W, W, C.c_int32, C.c_int64, P(C.c_int64)]),
+        "xdem_set_warm_start": (C.c_int32, [W, W]),
+        "xdem_get_warm_stats": (C.c_int32, [W, P(C.c_int64)]),
         "xdem_range_pop": (C.c_int32, []),
         "xdem_host_free": (None, [C.c_void_p]),
         "xdem_pair_geometry": (C.c_int32, [C.c_int32, C.c_int32, C.c_int32, _d, _d, _d, _d]),

@@ -19,7 +19,7 @@ NVCC_FLAGS = [
     "-Xcompiler", "-fPIC,-O2", "-shared",
     "-I", os.path.join(ROOT, "include"),
 ]
-SOURCES = ["api.cu", "noalloc.cu", "host_utils.cpp"]
+SOURCES = ["api.cu", "learn.cu", "noalloc.cu", "host_utils.cpp"]
 
 
 def _nvcc():

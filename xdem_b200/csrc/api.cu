@@ -13,6 +13,8 @@
 #include "kernels.cuh"
 #include "pairs.cuh"
 #include "pairs_mixed.cuh"
+#include "learned.cuh"
+#include "mlp_host.h"
 #include "resort.cuh"
 
 using namespace xdem;
@@ -70,6 +72,7 @@ struct xdem_world_s {
   cudaEvent_t timer[2] = {nullptr, nullptr};
   int since_resort = kResortEvery;  // steps since the memory order was refreshed
   int law = LAW_ANY;                // contact-kernel specialisation for the shapes present
+  xdem_mlp_s* mlp = nullptr;        // learned warm start of the closest-approach Newton iteration
   PermList perm{};                  // particle arrays moved by a re-sort
 };
 
@@ -132,13 +135,13 @@ cudaError_t download(T* dst, const T* src, size_t count, cudaStream_t s) {
 enum KernelKind {
   KK_MODIFY = 0, KK_BIN, KK_SCAN, KK_SCATTER, KK_CANDIDATES, KK_PAIRS, KK_FINISH, KK_COLLECT,
   KK_INTEGRATE, KK_RATTLERS, KK_STRESS_PARTIAL, KK_STRESS_FINAL, KK_END_OF_STEP, KK_SCALE,
-  KK_BACKGROUND, KK_KE, KK_RESORT, KK_STAGE, KK_FALLBACK, KK_COUNT
+  KK_BACKGROUND, KK_KE, KK_RESORT, KK_STAGE, KK_FALLBACK, KK_WARM, KK_COUNT
 };
 const char* const kKindNames[KK_COUNT] = {
     "k_modify_position", "k_bin", "k_scan", "k_scatter", "k_candidates", "k_pair_forces",
     "k_finish_slots", "k_collect", "k_integrate", "k_rattlers", "k_stress_partial",
     "k_stress_final", "k_end_of_step", "k_scale_positions", "k_background_velocity",
-    "k_kinetic_energy", "k_resort", "k_stage", "k_pair_fallback"};
+    "k_kinetic_energy", "k_resort", "k_stage", "k_pair_fallback", "k_mlp_warm"};
 
 void prof_begin(xdem_world_s* w, int kind) {
   if (!w->prof_on) return;
@@ -195,13 +198,28 @@ template <bool FOLD_BG, int LAW>
 void launch_update_phases(xdem_world_s* w, int record) {
   const int nb = blocks_for(w->dw.n, 128);
   const int pb = 148 * 16;
+  // the learned warm start applies to closest-approach worlds
+  const bool warm = w->mlp != nullptr && w->dw.warm != nullptr && LAW == LAW_CLOSEST;
   LAUNCH(w, KK_CANDIDATES, k_candidates<LAW><<<nb, 128, 0, w->stream>>>(w->dw, w->par));
   if (w->prm.precision == XDEM_PRECISION_MIXED) {
     LAUNCH(w, KK_PAIRS,
            k_pair_forces_m<FOLD_BG, LAW><<<pb, 128, 0, w->stream>>>(w->dw, w->par, record));
-    if (LAW == LAW_CLOSEST || LAW == LAW_ANY)
-      LAUNCH(w, KK_FALLBACK, k_pair_fallback_m<FOLD_BG, LAW><<<148 * 4, 128, 0, w->stream>>>(
-                                 w->dw, w->par, record));
+    if (LAW == LAW_CLOSEST || LAW == LAW_ANY) {
+      if (warm) {
+        LAUNCH(w, KK_WARM, k_mlp_warm<LAW><<<148 * 4, 128, 0, w->stream>>>(
+                               w->dw, w->mlp->dev(), w->dw.nfallback, w->dw.fallback));
+        LAUNCH(w, KK_FALLBACK, k_pair_fallback_m<FOLD_BG, LAW, true><<<148 * 4, 128, 0, w->stream>>>(
+                                   w->dw, w->par, record));
+      } else {
+        LAUNCH(w, KK_FALLBACK, k_pair_fallback_m<FOLD_BG, LAW><<<148 * 4, 128, 0, w->stream>>>(
+                                   w->dw, w->par, record));
+      }
+    }
+  } else if (warm) {
+    LAUNCH(w, KK_WARM,
+           k_mlp_warm<LAW><<<148 * 8, 128, 0, w->stream>>>(w->dw, w->mlp->dev(), w->dw.npairs, nullptr));
+    LAUNCH(w, KK_PAIRS,
+           k_pair_forces<FOLD_BG, LAW, true><<<pb, 128, 0, w->stream>>>(w->dw, w->par, record));
   } else {
     LAUNCH(w, KK_PAIRS,
            k_pair_forces<FOLD_BG, LAW><<<pb, 128, 0, w->stream>>>(w->dw, w->par, record));
@@ -679,6 +697,8 @@ int32_t set_particles_impl(xdem_world_s* w, const xdem_particles* P, const std::
   CK(w, B.alloc(&d.fallback, w->prm.precision == XDEM_PRECISION_MIXED ? ks : 1));
   CK(w, B.alloc(&d.nfallback, 1));
   CK(w, cudaMemsetAsync(d.nfallback, 0, sizeof(int32_t), s));
+  d.warm = nullptr;
+  if (w->mlp) CK(w, B.alloc(&d.warm, ks));
   w->partial_blocks = blocks_for(n, kReduceBlock);
   CK(w, B.alloc(&d.partials, 4 * (size_t)w->partial_blocks + 4));
   // memory order starts as id order
@@ -1225,7 +1245,55 @@ int32_t xdem_reset_newton_stats(xdem_world w) {
   WorldScalars s;
   CK(w, read_scalars(w, &s));
   s.newton_solves = s.newton_iters = s.newton_capped = 0;
+  s.warm_offered = s.warm_used = s.warm_rejected = s.warm_restarted = s.logit_right = 0;
   CK(w, write_scalars(w, &s));
+  return XDEM_OK;
+}
+
+// ---- learned warm start ------------------------------------------------------
+int32_t xdem_set_warm_start(xdem_world w, xdem_mlp m) {
+  if (!w) return XDEM_ERR_ARGUMENT;
+  cudaStreamSynchronize(w->stream);
+  w->mlp = m;
+  if (m && w->dw.n > 0 && !w->dw.warm)
+    CK(w, w->particle_bufs.alloc(&w->dw.warm, (size_t)w->dw.K * w->dw.n));
+  if (!m) w->dw.warm = nullptr;
+  return XDEM_OK;
+}
+
+int32_t xdem_get_warm_stats(xdem_world w, int64_t out[5]) {
+  if (!w || !out) return XDEM_ERR_ARGUMENT;
+  WorldScalars s;
+  CK(w, read_scalars(w, &s));
+  out[0] = (int64_t)s.warm_offered;
+  out[1] = (int64_t)s.warm_used;
+  out[2] = (int64_t)s.warm_rejected;
+  out[3] = (int64_t)s.warm_restarted;
+  out[4] = (int64_t)s.logit_right;
+  return XDEM_OK;
+}
+
+int32_t xdem_harvest_pairs(xdem_world w, xdem_mlp m, int32_t stride, int64_t max_new, int64_t* added) {
+  if (!w || !m || stride <= 0 || max_new <= 0 || w->dw.n <= 0) return XDEM_ERR_ARGUMENT;
+  if (added) *added = 0;
+  CK(w, cudaStreamSynchronize(m->stream));
+  CK(w, mlp_reserve(m, m->size + max_new));
+  unsigned long long* dcount = nullptr;
+  CK(w, cudaMalloc(&dcount, sizeof(unsigned long long)));
+  cudaError_t e = cudaMemsetAsync(dcount, 0, sizeof(unsigned long long), w->stream);
+  if (e == cudaSuccess) {
+    k_harvest<<<148 * 8, 128, 0, w->stream>>>(w->dw, m->dev(), stride, m->x, m->target, m->contact,
+                                              m->size, m->size + max_new, dcount);
+    e = cudaGetLastError();
+  }
+  unsigned long long got = 0;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&got, dcount, sizeof(got), cudaMemcpyDeviceToHost, w->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(w->stream);
+  cudaFree(dcount);
+  CK(w, e);
+  const int64_t n = std::min<int64_t>((int64_t)got, max_new);
+  m->size += n;
+  if (added) *added = n;
   return XDEM_OK;
 }
 

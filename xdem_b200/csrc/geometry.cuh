@@ -32,9 +32,12 @@ struct PState {
 struct Geom {
   int contacted;
   int iters;
+  int warm;  // learned warm start: 0 not offered, 1 used, 2 rejected by the residual test,
+             // 3 used but the root left its interval (the plain start decided)
   vec2<double> cp, n, bv1, bv2;
   double overlap;
   vec2<double> rv, nrv, srv;
+  double q, q_start;  // closest approach: the quartic's root and Newton's analytic start
 };
 
 // BaseParticle::calculateRelativeVelocityAtContactPoint (BaseParticle.cpp:11-25)
@@ -95,12 +98,25 @@ __device__ __forceinline__ double newton_quartic(double A, double B, double C, d
   return r0;
 }
 
+// Largest Newton step accepted at a learned warm start, relative to the start
+constexpr double kWarmResidual = 0.05;
+
 // EllipticParticle::contactWithEllipticParticle, closest approach
 // (Zheng & Palffy-Muhoray), EllipticParticle.cpp:34-285.  (k1x, k1y) and
 // (k2x, k2y) are cos/sin of the two orientations.
+//
+// WARM: `warm` is a predicted root as a fraction of the analytic start
+// sqrt(δ+1) (mlp.cuh).  It is clamped to [min(1, s), max(1, s)], s = sqrt(δ+1),
+// the interval that holds the root the plain start converges to (the quartic
+// has one positive root there); it is used only when the first Newton step
+// from it is below kWarmResidual of it, and a root that leaves the interval is
+// discarded for the plain iteration from s.  Newton then stops at the same
+// tolerance, so the answer is the plain solver's.
+template <bool WARM = false>
 __device__ __forceinline__ bool ellipse_closest(const PState& a, const PState& b, vec2<double> off,
                                                 vec2<double> ovel, double k1x, double k1y,
-                                                double k2x, double k2y, Geom& g, uint32_t& st) {
+                                                double k2x, double k2y, Geom& g, uint32_t& st,
+                                                float warm = 0.0f) {
   double a1 = a.r, a2 = b.r;
   double b1 = a1 / a.asp, b2 = a2 / b.asp;
   vec2<double> pa = V(a.x, a.y);
@@ -161,8 +177,34 @@ __device__ __forceinline__ bool ellipse_closest(const PState& a, const PState& b
   double D = 2.0 * (1.0 + tanPhi2) * (1.0 + delta) / b2p;
   double E = (1.0 + tanPhi2 + delta) * (1.0 + delta);
   int it = 0;
-  double q = newton_quartic(A, B, C, D, E, sqrt(delta + 1.0), it);
+  const double start = sqrt(delta + 1.0);
+  double init = start;
+  double lo = 0.0, hi = 0.0;
+  if (WARM) {
+    lo = fmin(1.0, start);
+    hi = fmax(1.0, start);
+    g.warm = 2;
+    double q0 = (double)warm * start;
+    if (isfinite(q0)) {
+      q0 = fmin(fmax(q0, lo), hi);
+      const double f = A * q0 * q0 * q0 * q0 + B * q0 * q0 * q0 + C * q0 * q0 + D * q0 + E;
+      const double fp = 4.0 * A * q0 * q0 * q0 + 3.0 * B * q0 * q0 + 2.0 * C * q0 + D;
+      if (fabs(f) <= kWarmResidual * q0 * fabs(fp)) {
+        init = q0;
+        g.warm = 1;
+      }
+    }
+  }
+  double q = newton_quartic(A, B, C, D, E, init, it);
+  if (WARM && g.warm == 1 && !(q >= lo * (1.0 - 1e-9) && q <= hi * (1.0 + 1e-9))) {
+    int it2 = 0;
+    q = newton_quartic(A, B, C, D, E, start, it2);
+    it += it2;
+    g.warm = 3;
+  }
   g.iters = it;
+  g.q = q;
+  g.q_start = start;
   if (it >= kNewtonCap) st |= ST_NEWTON;
   double temp = (q * q - 1.0) / delta;
   double d_prime = 0.0;
@@ -409,12 +451,12 @@ enum : int { LAW_CIRCLE = 0, LAW_CLOSEST = 1, LAW_INTERSECTION = 2, LAW_ANY = 3 
 // calculateContactGeometry for a world whose bodies all have one shape; the
 // clump test stays (a clump's geometry is never a contact, GluedParticle.cpp:133-140)
 // (SCREENED: the caller has already applied the bounding-circle test)
-template <int LAW, bool SCREENED = false>
+template <int LAW, bool SCREENED = false, bool WARM = false>
 __device__ __forceinline__ bool contact_geometry_law(const PState& a, const PState& b,
                                                      double orad_a, double orad_b,
                                                      vec2<double> off, vec2<double> ovel,
                                                      double2 cs_a, double2 cs_b, Geom& g,
-                                                     uint32_t& st) {
+                                                     uint32_t& st, float warm = 0.0f) {
   g = Geom{};
   if (a.shape == SHAPE_CLUMP || b.shape == SHAPE_CLUMP) return false;
   if (LAW == LAW_CIRCLE) return circle_circle(a, b, off, ovel, g);
@@ -425,7 +467,7 @@ __device__ __forceinline__ bool contact_geometry_law(const PState& a, const PSta
   }
   if (LAW == LAW_INTERSECTION)
     return ellipse_intersection(a, b, off, ovel, cs_a.x, cs_a.y, cs_b.x, cs_b.y, g);
-  return ellipse_closest(a, b, off, ovel, cs_a.x, cs_a.y, cs_b.x, cs_b.y, g, st);
+  return ellipse_closest<WARM>(a, b, off, ovel, cs_a.x, cs_a.y, cs_b.x, cs_b.y, g, st, warm);
 }
 
 // BaseParticle::calculateContactGeometry dispatch (CircularParticle.cpp:25-40,

@@ -9,7 +9,9 @@
 //                   written to the owner's slot for that pair;
 //   k_finish_slots  one thread per owner: carries over the history of pairs
 //                   that were not candidates this step, as the reference's map
-//                   entries survive.
+//                   entries survive, and registers every contact with its
+//                   partner for the partner's force sum (kept out of the heavy
+//                   pair kernel, whose warps would otherwise wait on the atomic).
 // Splitting the light scan from the heavy geometry keeps warps full on the
 // FP64 ellipse solvers.  A candidate rejected by the coarse test is still a
 // candidate: its history is dropped, as the reference erases it
@@ -238,20 +240,45 @@ __global__ void __launch_bounds__(128) k_candidates(DevWorld w, int par) {
 }
 
 // ---- phase B --------------------------------------------------------------------
-template <bool FOLD_BG, int LAW>
+// learned warm-start counters of a thread, combined over its warp (every lane
+// must call)
+__device__ __forceinline__ void flush_warm(const DevWorld& w, uint32_t offered, uint32_t used,
+                                           uint32_t rejected, uint32_t restarted, uint32_t right) {
+  const unsigned full = 0xffffffffu;
+  offered = __reduce_add_sync(full, offered);
+  used = __reduce_add_sync(full, used);
+  rejected = __reduce_add_sync(full, rejected);
+  restarted = __reduce_add_sync(full, restarted);
+  right = __reduce_add_sync(full, right);
+  if ((threadIdx.x & 31) == 0 && offered) {
+    WorldScalars* wsm = w.ws;
+    atomicAdd(&wsm->warm_offered, (unsigned long long)offered);
+    atomicAdd(&wsm->warm_used, (unsigned long long)used);
+    atomicAdd(&wsm->warm_rejected, (unsigned long long)rejected);
+    atomicAdd(&wsm->warm_restarted, (unsigned long long)restarted);
+    atomicAdd(&wsm->logit_right, (unsigned long long)right);
+  }
+}
+
+// WARM: closest-approach pairs start Newton from the learned warm start of
+// their list entry (w.warm, written by k_mlp_warm)
+template <bool FOLD_BG, int LAW, bool WARM = false>
 __global__ void __launch_bounds__(128, 4) k_pair_forces(DevWorld w, int par, int record) {
   if (stopped(w)) return;
-  const int n = w.n, K = w.K;
+  const int n = w.n;
   const Slots& old = w.slots[par];
   const Slots& cur = w.slots[par ^ 1];
   const int npairs = *w.npairs;
   uint32_t st = 0;
   uint32_t n_solves = 0, n_iters = 0, n_capped = 0;
+  uint32_t w_off = 0, w_used = 0, w_rej = 0, w_rest = 0, w_right = 0;
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < npairs; t += gridDim.x * blockDim.x) {
     const PairEntry e = w.pairs[t];
     const int m = e.m, mj = e.mj;
     const WorldScalars& ws = w.ws[sys_at(w, m)];
     const double dt = ws.dt, kn = ws.kn, kt = ws.kt, mu = ws.mu, factor = ws.factor;
+    float2 wp = make_float2(0.0f, 0.0f);
+    if (WARM && LAW == LAW_CLOSEST) wp = w.warm[t];
     const int kind = e.code & 0xff, slot = (e.code >> 8) & 0xff, o = (e.code >> 16) & 0xff;
     const size_t ci = (size_t)slot * n + m;
     PState a = load_state<FOLD_BG>(w, ws, m);
@@ -274,7 +301,15 @@ __global__ void __launch_bounds__(128, 4) k_pair_forces(DevWorld w, int par, int
         csa = w.cs[m];
         csb = w.cs[mj];
       }
-      touching = contact_geometry_law<LAW, true>(a, b, 0.0, 0.0, off, ovel, csa, csb, g, st);
+      touching = contact_geometry_law<LAW, true, WARM && LAW == LAW_CLOSEST>(
+          a, b, 0.0, 0.0, off, ovel, csa, csb, g, st, wp.x);
+    }
+    if (WARM && LAW == LAW_CLOSEST && g.warm) {
+      w_off++;
+      w_used += g.warm == 1 || g.warm == 3;
+      w_rej += g.warm == 2;
+      w_rest += g.warm == 3;
+      w_right += (wp.y > 0.0f) == touching;
     }
     if (LAW != LAW_CIRCLE && g.iters > 0) {
       n_solves++;
@@ -336,12 +371,9 @@ __global__ void __launch_bounds__(128, 4) k_pair_forces(DevWorld w, int par, int
       cur.fn[ci] = make_double2(fn.x, fn.y);
       cur.ft[ci] = make_double2(fs.x, fs.y);
     }
-    // register with the partner for its force sum
-    int pos = atomicAdd(&w.incnt[mj], 1);
-    if (pos < K) w.inref[(size_t)pos * n + mj] = (uint32_t)m * (uint32_t)K + (uint32_t)slot;
-    else st |= ST_CAPACITY;
   }
   flush_warp(w, st, n_solves, n_iters, n_capped);
+  if (WARM) flush_warm(w, w_off, w_used, w_rej, w_rest, w_right);
 }
 
 // ---- phase C --------------------------------------------------------------------
@@ -361,6 +393,15 @@ __global__ void __launch_bounds__(128) k_finish_slots(DevWorld w, int par) {
   const uint32_t seen = w.seen[m];
   const int nold = min(old.count[m], K);
   int k = cur.count[m];
+  // the contacts listed this step
+  for (int s = 0; s < k; ++s) {
+    const int partner = cur.partner[(size_t)s * n + m];
+    if (partner < 0) continue;
+    const int mj = w.mpos[partner];
+    const int pos = atomicAdd(&w.incnt[mj], 1);
+    if (pos < K) w.inref[(size_t)pos * n + mj] = (uint32_t)m * (uint32_t)K + (uint32_t)s;
+    else st |= ST_CAPACITY;
+  }
   for (int o = 0; o < nold; ++o) {
     size_t oi = (size_t)o * n + m;
     int partner = old.partner[oi];

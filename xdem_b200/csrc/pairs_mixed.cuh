@@ -30,7 +30,7 @@ __device__ __forceinline__ void write_contact_m(const DevWorld& w, const WorldSc
                                                 const PState& b, vec2<double> off,
                                                 const GeomM& g, int par, int record,
                                                 uint32_t& st) {
-  const int n = w.n, K = w.K;
+  const int n = w.n;
   const Slots& old = w.slots[par];
   const Slots& cur = w.slots[par ^ 1];
   const int m = e.m, mj = e.mj;
@@ -97,10 +97,7 @@ __device__ __forceinline__ void write_contact_m(const DevWorld& w, const WorldSc
     cur.fn[ci] = make_double2((double)fnx, (double)fny);
     cur.ft[ci] = make_double2((double)fsx, (double)fsy);
   }
-  // register with the partner for its force sum
-  const int pos = atomicAdd(&w.incnt[mj], 1);
-  if (pos < K) w.inref[(size_t)pos * n + mj] = (uint32_t)m * (uint32_t)K + (uint32_t)slot;
-  else st |= ST_CAPACITY;
+  (void)st;
 }
 
 __device__ __forceinline__ void count_solve(uint32_t it, uint32_t& n_solves, uint32_t& n_iters) {
@@ -190,13 +187,14 @@ __global__ void __launch_bounds__(128, 4) k_pair_forces_m(DevWorld w, int par, i
 
 // the closest-approach pairs deferred by k_pair_forces_m: the reference's FP64
 // construction (EllipticParticle.cpp:34-285), then the mixed force
-template <bool FOLD_BG, int LAW>
+template <bool FOLD_BG, int LAW, bool WARM = false>
 __global__ void __launch_bounds__(128) k_pair_fallback_m(DevWorld w, int par, int record) {
   if (stopped(w)) return;
   const int n = w.n;
   const Slots& cur = w.slots[par ^ 1];
   const int nfb = *w.nfallback;
   uint32_t st = 0, n_solves = 0, n_iters = 0, n_capped = 0;
+  uint32_t w_off = 0, w_used = 0, w_rej = 0, w_rest = 0, w_right = 0;
   for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < nfb; f += gridDim.x * blockDim.x) {
     const PairEntry e = w.pairs[w.fallback[f]];
     const int m = e.m, mj = e.mj;
@@ -216,8 +214,16 @@ __global__ void __launch_bounds__(128) k_pair_fallback_m(DevWorld w, int par, in
       csb = make_double2(cos(b.rot), sin(b.rot));
     }
     Geom gd = Geom{};
+    const float2 wp = WARM ? w.warm[f] : make_float2(0.0f, 0.0f);
     const bool touching =
-        ellipse_closest(a, b, off, ovel, csa.x, csa.y, csb.x, csb.y, gd, st);
+        ellipse_closest<WARM>(a, b, off, ovel, csa.x, csa.y, csb.x, csb.y, gd, st, wp.x);
+    if (WARM && gd.warm) {
+      w_off++;
+      w_used += gd.warm == 1 || gd.warm == 3;
+      w_rej += gd.warm == 2;
+      w_rest += gd.warm == 3;
+      w_right += (wp.y > 0.0f) == touching;
+    }
     if (gd.iters > 0) {
       n_solves++;
       n_iters += gd.iters;
@@ -232,6 +238,7 @@ __global__ void __launch_bounds__(128) k_pair_fallback_m(DevWorld w, int par, in
     write_contact_m(w, ws, e, a, b, off, g, par, record, st);
   }
   flush_warp(w, st, n_solves, n_iters, n_capped);
+  if (WARM) flush_warm(w, w_off, w_used, w_rej, w_rest, w_right);
 }
 
 // single pairs through the mixed geometry (xdem_pair_geometry with

@@ -60,6 +60,10 @@ struct WorldScalars {
   // closest-approach Newton statistics since the last reset: solves,
   // iterations, solves stopped by the iteration cap
   unsigned long long newton_solves, newton_iters, newton_capped;
+  // learned warm start since the last reset: starts offered, used, rejected by
+  // the residual test, used but overruled by the plain start; contact logits
+  // that matched the outcome
+  unsigned long long warm_offered, warm_used, warm_rejected, warm_restarted, logit_right;
 };
 
 // one pair listed by the candidate scan: owner position, partner position,
@@ -143,6 +147,7 @@ struct DevWorld {
   int32_t* npairs;  // number of listed pairs
   int32_t* fallback;   // [K*n] mixed precision: listed pairs deferred to the FP64 construction
   int32_t* nfallback;  // number of deferred pairs
+  float2* warm;        // [K*n] learned warm start of each listed pair: (root fraction, contact logit)
   // scalars (one per system), status, scratch
   WorldScalars* ws;
   uint32_t* status;
