@@ -24,12 +24,17 @@
 //
 //    The reference orders the two eigenvalues of its matrix A' by their
 //    truncated integer magnitudes (int abs on a double, MathMatrix2d.h:122),
-//    which exchanges them whenever both share an integer part; its rejection
-//    tests then discard some pairs that touch (EllipticParticle.cpp:77-84).
-//    Those pairs, and pairs whose eigenvalues are within FP32 error of an
-//    integer, are handed to the reference's FP64 construction (a separate
-//    pass, so that warps stay converged), which keeps the contact set the
-//    FP64 path's.
+//    which exchanges them whenever both share an integer part; its two
+//    rejection tests (EllipticParticle.cpp:77-84) then discard some pairs that
+//    touch, and deep overlaps come out differently.  For such pairs the two
+//    tests are evaluated here in FP32 with the exchanged semi-axes: a pair
+//    they reject has no contact, as in the reference; a pair they pass, if
+//    its overlap is below a tenth of the contact distance, has the reference's
+//    geometry, which the contact function reproduces.  A pair within FP32
+//    error of a test's threshold or of an integer eigenvalue, or overlapping
+//    deeper, is handed to the reference's FP64 construction (a separate pass,
+//    so that warps stay converged), which keeps the contact set the FP64
+//    path's.
 #pragma once
 #include "geometry.cuh"
 
@@ -100,21 +105,25 @@ __device__ __forceinline__ int ellipse_closest_m(const PState& a, const PState& 
 
   // ---- reference eigenvalue ordering, FP32 -----------------------------
   // A' = (b1²/b2²) P Q P with P = I + η k1k1ᵀ, Q = I - e2² k2k2ᵀ
-  // (EllipticParticle.cpp:59-71); only its trace and determinant are needed:
-  //   det A' = (a1 b1 / (a2 b2))²,
-  //   tr(PQP) = tr(P²) - e2² k2ᵀ P² k2,  P² = I + (2η + η²) k1k1ᵀ
+  // (EllipticParticle.cpp:59-71); its eigenvalues from the trace and
+  // det A' = (a1 b1 / (a2 b2))²
   const float c1 = (float)csa.x, s1 = (float)csa.y, c2 = (float)csb.x, s2 = (float)csb.y;
+  bool exchanged;
   {
     const float fa1 = (float)a1, fb1 = (float)b1, fa2 = (float)a2, fb2 = (float)b2;
     const float eta = fa1 / fb1 - 1.0f;
-    const float p2 = eta * (2.0f + eta);
     const float e22 = 1.0f - (fb2 * fb2) / (fa2 * fa2);
-    const float k12 = c1 * c2 + s1 * s2;
-    const float trPQP = (2.0f + p2) - e22 * (1.0f + p2 * k12 * k12);
     const float sc = (fb1 * fb1) / (fb2 * fb2);
-    const float tr = sc * trPQP;
+    // A' = sc P Q P, P = I + η k1k1ᵀ, Q = I - e2² k2k2ᵀ (symmetric)
+    const float Pxx = 1.0f + eta * c1 * c1, Pxy = eta * c1 * s1, Pyy = 1.0f + eta * s1 * s1;
+    const float Qxx = 1.0f - e22 * c2 * c2, Qxy = -e22 * c2 * s2, Qyy = 1.0f - e22 * s2 * s2;
+    const float Mxx = Pxx * Qxx + Pxy * Qxy, Mxy = Pxx * Qxy + Pxy * Qyy;
+    const float Myx = Pxy * Qxx + Pyy * Qxy, Myy = Pxy * Qxy + Pyy * Qyy;
+    const float Axx = sc * (Mxx * Pxx + Mxy * Pxy), Axy = sc * (Mxx * Pxy + Mxy * Pyy);
+    const float Ayy = sc * (Myx * Pxy + Myy * Pyy);
+    const float tr = Axx + Ayy;
     const float rt = (fa1 * fb1) / (fa2 * fb2);
-    const float dt_ = rt * rt;
+    const float dt_ = rt * rt;  // det A' = (a1 b1 / (a2 b2))²
     float disc = tr * tr - 4.0f * dt_;
     disc = disc > 0.0f ? sqrtf(disc) : 0.0f;
     const float ev1 = 0.5f * (tr + disc), ev2 = 0.5f * (tr - disc);
@@ -123,7 +132,30 @@ __device__ __forceinline__ int ellipse_closest_m(const PState& a, const PState& 
     const float f1lo = floorf(ev1 - tol), f1hi = floorf(ev1 + tol);
     const float f2lo = floorf(ev2 - tol), f2hi = floorf(ev2 + tol);
     if (f1lo != f1hi || f2lo != f2hi) return PW_FALLBACK;  // ambiguous in FP32
-    if (f1lo == f2lo) return PW_FALLBACK;                   // exchanged by the reference
+    exchanged = f1lo == f2lo;
+    if (exchanged) {
+      // the reference's rejection tests with its exchanged axes
+      // (EllipticParticle.cpp:73-84): lx = ev2, ly = ev1
+      if (fabsf(Axy) < 1e-4f * tr) return PW_FALLBACK;  // ill-conditioned eigenvector
+      const float lx = ev2, ly = ev1;
+      const float a2p = rsqrtf(ly), b2p = rsqrtf(lx);
+      float kx = 1.0f, ky = (lx - Axx) / Axy;
+      const float ik = rsqrtf(kx * kx + ky * ky);
+      kx *= ik;
+      ky *= ik;
+      const float fdx = (float)dx, fdy = (float)dy;
+      const float k1d = c1 * fdx + s1 * fdy, g1 = fb1 / fa1 - 1.0f;
+      const float px = (fdx + c1 * k1d * g1) / fb1, py = (fdy + s1 * k1d * g1) / fb1;
+      const float dn = sqrtf(px * px + py * py);
+      const float r1 = dn - (1.0f + a2p);
+      const float r2 = fabsf(px * kx + py * ky) - (1.0f + b2p);
+      const float rtol = 2e-5f * (1.0f + dn);
+      if (fabsf(r1) <= rtol || fabsf(r2) <= rtol) return PW_FALLBACK;
+      if (r1 > 0.0f || r2 > 0.0f) {
+        g.iters = 0;
+        return PW_NONE;
+      }
+    }
   }
 
   // ---- λ* by Newton on d/dλ log F, FP32 ----------------------------------
@@ -187,6 +219,8 @@ __device__ __forceinline__ int ellipse_closest_m(const PState& a, const PState& 
   const double overlap0 = sigma - dlen;
   g.iters = it;
   if (!(overlap0 >= 0.0)) return PW_NONE;
+  // deep overlaps of exchanged pairs: the reference's construction decides
+  if (exchanged && overlap0 > 0.1 * sigma) return PW_FALLBACK;
 
   // ---- normal, tangent point, relative velocity, FP32 ----------------------
   {
