@@ -660,7 +660,8 @@ int32_t set_particles_impl(xdem_world_s* w, const xdem_particles* P, const std::
   CK(w, B.alloc(&d.tile_sum, cells / kScanTile + 2));
   CK(w, B.alloc(&d.cell_mem, 2 * (size_t)n));
   CK(w, B.alloc(&d.cell_pos, 2 * (size_t)n));
-  CK(w, B.alloc(&d.cell_rec, 2 * (size_t)n));
+  CK(w, B.alloc(&d.cell_scr, 2 * (size_t)n));
+  CK(w, B.alloc(&d.cell_up, 2 * (size_t)n));
   CK(w, B.alloc(&d.cs, n));
   d.screen_r = w->law == LAW_CIRCLE ? d.rad : d.orad;
   CK(w, B.alloc(&d.pcell, n));

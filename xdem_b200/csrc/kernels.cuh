@@ -298,21 +298,33 @@ __global__ void k_scatter(DevWorld w) {
   if (i >= w.n) return;
   const Grid G = grid_of(w.ws[sys_at(w, i)]);
   if (G.nx < 3 || G.ny < 3) return;
+  const WorldScalars& ws = w.ws[sys_at(w, i)];
   const double2 p = w.pos[i];
-  ScreenRec r;
-  r.r = w.screen_r[i];
-  r.id = (w.setting[i] & SKIP_CONTACT_DETECTION) ? -1 : w.id_of[i];
-  r.up = w.up[i];
-  int q = w.cell_start[w.pcell[i]] + w.prank[i];
+  const int pc = w.pcell[i], local = pc - G.base;
+  const int ix = local % G.nx, iy = local / G.nx;
+  // position relative to the cell's corner; y is the same in a ghost row
+  const float ry = (float)(p.y - (ws.ymin + iy * G.ly));
+  const float sr = (float)w.screen_r[i];
+  const float idb = __int_as_float((w.setting[i] & SKIP_CONTACT_DETECTION) ? -1 : w.id_of[i]);
+  const int up = w.up[i];
+  int q = w.cell_start[pc] + w.prank[i];
   w.cell_mem[q] = i;
   w.cell_pos[q] = p;
-  w.cell_rec[q] = r;
+  w.cell_scr[q] = make_float4((float)(p.x - (ws.xmin + ix * G.lx)), ry, sr, idb);
+  w.cell_up[q] = up;
   int gc = w.gcell[i];
   if (gc >= 0) {
+    // the image's x as k_bin placed it: shifted by +shift (bottom row, into
+    // the ghost row above the top) or -shift (top row), wrapped into the box
+    double t = iy == 0 ? p.x + ws.shift : p.x - ws.shift;
+    if (t < ws.xmin) t += ws.xlen;
+    else if (t > ws.xmax) t -= ws.xlen;
+    const int gx = gc - G.base - G.ncell - (iy == 0 ? 0 : G.nx);
     q = w.cell_start[gc] + w.grank[i];
     w.cell_mem[q] = i;
     w.cell_pos[q] = p;
-    w.cell_rec[q] = r;
+    w.cell_scr[q] = make_float4((float)(t - (ws.xmin + gx * G.lx)), ry, sr, idb);
+    w.cell_up[q] = up;
   }
 }
 

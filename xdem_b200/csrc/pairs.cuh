@@ -86,45 +86,31 @@ __device__ __forceinline__ bool coarse_pass(int shape_i, int shape_j, double r_i
 }
 
 // ---- phase A --------------------------------------------------------------------
-// The nine cells of the reference's scan, in its order, with the image kind
-// of each (LeesEdwardsBoundaryWorld.cpp:128-204 for the ghost rows).
-struct Neighbourhood {
-  int cell[9];
-  int kind[9];
-};
-
-__device__ __forceinline__ Neighbourhood neighbourhood(const Grid& G, int world_kind, int ix,
-                                                       int iy) {
-  Neighbourhood nb;
-  int k = 0;
-  for (int dx = -1; dx <= 1; ++dx) {
-    int jx = ix + dx;
-    if (jx == -1) jx = G.nx - 1;
-    else if (jx == G.nx) jx = 0;
-    for (int dy = -1; dy <= 1; ++dy, ++k) {
-      int jy = iy + dy;
-      if (world_kind == WORLD_LE && (jy == -1 || jy == G.ny)) {
-        if (jy == -1) {
-          nb.cell[k] = G.base + G.ncell + G.nx + jx;
-          nb.kind[k] = CAND_BOTTOM;
-        } else {
-          nb.cell[k] = G.base + G.ncell + jx;
-          nb.kind[k] = CAND_TOP;
-        }
-      } else {
-        if (jy == -1) jy = G.ny - 1;
-        else if (jy == G.ny) jy = 0;
-        nb.cell[k] = G.base + jy * G.nx + jx;
-        nb.kind[k] = CAND_REGULAR;
-      }
-    }
+// Cell (ix+dx, iy+dy) of the reference's 3x3 scan with its image kind
+// (PeriodicBoundaryWorld.cpp:47-84; LeesEdwardsBoundaryWorld.cpp:128-204 for
+// the ghost rows beyond the top and bottom edges).  The scan order does not
+// matter: the pair list, slots and force sums are order independent.
+__device__ __forceinline__ int neighbour_cell(const Grid& G, int world_kind, int ix, int iy, int dx,
+                                              int dy, int& kind) {
+  int jx = ix + dx;
+  if (jx == -1) jx = G.nx - 1;
+  else if (jx == G.nx) jx = 0;
+  int jy = iy + dy;
+  if (world_kind == WORLD_LE && (jy == -1 || jy == G.ny)) {
+    kind = jy == -1 ? CAND_BOTTOM : CAND_TOP;
+    return jy == -1 ? G.base + G.ncell + G.nx + jx : G.base + G.ncell + jx;
   }
-  return nb;
+  if (jy == -1) jy = G.ny - 1;
+  else if (jy == G.ny) jy = 0;
+  kind = CAND_REGULAR;
+  return G.base + jy * G.nx + jx;
 }
 
 // One thread per owner m.  Cell entries are read from the cell-ordered
-// screening copies (cell_rec, cell_pos), so a neighbour cell is one
-// contiguous run of records.  Old slots whose partner sits in one of the nine
+// screening records (cell_scr, cell_up), so a neighbour cell is one
+// contiguous run of 20-byte records; the distance screen runs in FP32 on
+// positions relative to the cell corners, and only candidates within its
+// rounding margin of the threshold take the reference's FP64 test.  Old slots whose partner sits in one of the nine
 // cells (and passes the same filters) are marked seen: such a pair was a
 // candidate, so its history is replaced or dropped rather than carried over.
 // For an all-ellipse world the thread also leaves (cos, sin) of its
@@ -158,40 +144,57 @@ __global__ void __launch_bounds__(128) k_candidates(DevWorld w, int par) {
       const double r_i = w.rad[m], orad_i = w.orad[m];
       const int ix = cell_of(pi.x, ws.xmin, G.lx, G.nx);
       const int iy = cell_of(pi.y, ws.ymin, G.ly, G.ny);
-      const Neighbourhood nb = neighbourhood(G, w.kind, ix, iy);
-      int ncand[3] = {0, 0, 0};
+      // the owner relative to its cell's corner, in FP32 (see k_scatter)
+      const float rxi = (float)(pi.x - (ws.xmin + ix * G.lx));
+      const float ryi = (float)(pi.y - (ws.ymin + iy * G.ly));
+      const float flx = (float)G.lx, fly = (float)G.ly;
+      const float sr_i = (float)w.screen_r[m];
+      int ncand0 = 0, ncand1 = 0, ncand2 = 0;
 #pragma unroll 1
       for (int k = 0; k < 9; ++k) {
-        const int c = nb.cell[k], kind = nb.kind[k];
+        const int dx = k / 3 - 1, dy = k % 3 - 1;
+        int kind;
+        const int c = neighbour_cell(G, w.kind, ix, iy, dx, dy, kind);
         const int q0 = w.cell_start[c], q1 = w.cell_start[c + 1];
+        // the neighbour cell's corner relative to the owner's
+        const float ox = dx * flx - rxi, oy = dy * fly - ryi;
         for (int q = q0; q < q1; ++q) {
-          const ScreenRec rj = w.cell_rec[q];
-          if (rj.id <= id_i) continue;  // also drops SKIP_CONTACT_DETECTION
-          if (rj.up == up_i) continue;
-          if (ncand[kind] + 1 >= kCandidateCap) {
+          const float4 rj = w.cell_scr[q];
+          const int id_j = __float_as_int(rj.w);
+          if (id_j <= id_i) continue;  // also drops SKIP_CONTACT_DETECTION
+          if (w.cell_up[q] == up_i) continue;
+          int& nc = kind == CAND_REGULAR ? ncand0 : (kind == CAND_TOP ? ncand1 : ncand2);
+          if (nc + 1 >= kCandidateCap) {
             st |= ST_CAPACITY;
             continue;
           }
-          ncand[kind]++;
-          const double2 pj = w.cell_pos[q];
-          vec2<double> off, ovel;
-          image_offset(ws, kind, pi, pj, off, ovel);
-          bool pass;
-          if (LAW == LAW_ANY) {
+          nc++;
+          // FP32 screen with a margin well above its rounding error; the band
+          // around the threshold takes the reference's FP64 test
+          const float ddx = ox + rj.x, ddy = oy + rj.y;
+          const float d2 = ddx * ddx + ddy * ddy;
+          const float R = sr_i + rj.z, R2 = R * R;
+          if (d2 > R2 * (1.0f + 1e-4f) + 1e-4f) continue;
+          if (LAW == LAW_ANY || !(d2 < R2 * (1.0f - 1e-4f) - 1e-4f)) {
+            const double2 pj = w.cell_pos[q];
+            vec2<double> off, ovel;
+            image_offset(ws, kind, pi, pj, off, ovel);
             const int mj = w.cell_mem[q];
-            pass = coarse_pass<LAW>(shape_i, w.shape[mj], r_i, w.rad[mj], orad_i, w.orad[mj], pi,
-                                    pj, off);
-          } else {
-            pass = coarse_pass<LAW>(0, 0, r_i, rj.r, orad_i, rj.r, pi, pj, off);
+            bool pass;
+            if (LAW == LAW_ANY)
+              pass = coarse_pass<LAW>(shape_i, w.shape[mj], r_i, w.rad[mj], orad_i, w.orad[mj], pi,
+                                      pj, off);
+            else
+              pass = coarse_pass<LAW>(0, 0, r_i, w.screen_r[mj], orad_i, w.screen_r[mj], pi, pj, off);
+            if (!pass) continue;
           }
-          if (!pass) continue;
           if (nlist >= K) {
             st |= ST_CAPACITY;
             continue;
           }
           int oslot = kNoOldSlot;
           for (int z = 0; z < nold; ++z)
-            if (old.partner[(size_t)z * n + m] == rj.id) oslot = z;
+            if (old.partner[(size_t)z * n + m] == id_j) oslot = z;
           list_q[nlist] = q;
           list_code[nlist] = kind | (nlist << 8) | (oslot << 16);
           ++nlist;
@@ -207,7 +210,11 @@ __global__ void __launch_bounds__(128) k_candidates(DevWorld w, int par) {
         const int cr = w.pcell[mj], cg = w.gcell[mj];
         bool hit = false;
 #pragma unroll
-        for (int k = 0; k < 9; ++k) hit |= nb.cell[k] == cr || nb.cell[k] == cg;
+        for (int k = 0; k < 9; ++k) {
+          int kind;
+          const int c = neighbour_cell(G, w.kind, ix, iy, k / 3 - 1, k % 3 - 1, kind);
+          hit |= c == cr || c == cg;
+        }
         if (hit) seen |= 1u << z;
       }
     }

@@ -33,18 +33,21 @@ __global__ void k_sort_cells(DevWorld w) {
     for (int a = q0 + 1; a < q1; ++a) {
       const int x = w.cell_mem[a];
       const double2 px = w.cell_pos[a];
-      const ScreenRec rx = w.cell_rec[a];
+      const float4 rx = w.cell_scr[a];
+      const int ux = w.cell_up[a];
       const int kx = w.id_of[x];
       int b = a - 1;
       while (b >= q0 && w.id_of[w.cell_mem[b]] > kx) {
         w.cell_mem[b + 1] = w.cell_mem[b];
         w.cell_pos[b + 1] = w.cell_pos[b];
-        w.cell_rec[b + 1] = w.cell_rec[b];
+        w.cell_scr[b + 1] = w.cell_scr[b];
+        w.cell_up[b + 1] = w.cell_up[b];
         --b;
       }
       w.cell_mem[b + 1] = x;
       w.cell_pos[b + 1] = px;
-      w.cell_rec[b + 1] = rx;
+      w.cell_scr[b + 1] = rx;
+      w.cell_up[b + 1] = ux;
     }
     for (int q = q0; q < q1; ++q) w.newpos[w.cell_mem[q]] = q;
   }

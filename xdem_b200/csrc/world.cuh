@@ -75,13 +75,6 @@ struct PairEntry {
 };
 constexpr int kNoOldSlot = 255;
 
-// screening record of a cell entry, written in cell order by the scatter:
-// the radius of the coarse test, the id (negative when the particle skips
-// contact detection, so that one comparison applies both filters) and upLevel
-struct ScreenRec {
-  double r;
-  int32_t id, up;
-};
 
 // A world holds one system or, batched, nsys independent systems of the same
 // world kind side by side: system s owns the particles (ids and memory
@@ -130,7 +123,12 @@ struct DevWorld {
   int32_t* tile_sum;  // scan tile sums
   int32_t* cell_mem;
   double2* cell_pos;      // [2n] position of each cell entry, cell order
-  ScreenRec* cell_rec;    // [2n] screening record of each cell entry
+  // [2n] screening record of each cell entry, cell order: position relative
+  // to its cell's corner (FP32; magnitudes below a cell size), the radius of
+  // the coarse test, and the id as int bits (negative when the particle skips
+  // contact detection, so that one comparison applies both filters)
+  float4* cell_scr;
+  int32_t* cell_up;       // [2n] upLevel of each cell entry
   double2* cs;            // [n] (cos, sin) of the orientation, this step
   const double* screen_r; // rad for an all-circle world, orad otherwise
   int32_t* pcell;  // [n] regular cell of the particle at m
