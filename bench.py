@@ -274,21 +274,22 @@ def ncu_traffic_per_particle(kernel):
 def kernel_bytes(kernel, n, contacts, pairs):
     """Algorithmic DRAM bytes of one launch of a contact-update kernel, with
     every particle's data counted once (neighbour re-reads hit L2).
-    k_candidates: per particle the screening data (position 16, id 4,
-      setting 4, up-level 4, radius 8, outer radius 8) and the old history's
-      partner ids (4 per contact), written: slot count 4 + seen mask 4;
-      per listed pair a 16 B entry.
+    k_candidates: per particle the owner's data (position 16, id 4, setting 4,
+      up-level 4, radius 8, outer radius 8, screening radius 8, orientation 8,
+      old slot count 4) and its 20-byte screening record read by its
+      neighbours = 84 B, written: slot count 4, seen mask 4, orientation
+      cosines 16 = 24 B; per contact the old partner id 4 B; per listed pair a
+      16 B entry.
     k_pair_forces: per particle the state the geometry reads (position 16,
       velocity 16, orientation 8, spin 8, radius 8, aspect 8, outer radius 8,
       shape 4, mass 8, setting 4, id 4) = 92 B; per listed pair its entry 16 B;
       per contact the previous history (partner 4, normal 16, shear 16,
-      damping 8 = 44 B), the new record (partner 4, normal 16, shear 16,
-      damping 8, force 16, torques 16, branch vector 16 = 92 B) and the
-      partner's incoming reference and counter (8 B); per listed pair that
-      does not touch, an empty-slot mark (4 B)."""
+      damping 8 = 44 B) and the new record (partner 4, normal 16, shear 16,
+      damping 8, force 16, torques 16, branch vector 16 = 92 B); per listed
+      pair that does not touch, an empty-slot mark (4 B)."""
     if kernel == "k_candidates":
-        return 44.0 * n + 4.0 * contacts + 16.0 * pairs
-    return 92.0 * n + 16.0 * pairs + 144.0 * contacts + 4.0 * max(pairs - contacts, 0)
+        return 108.0 * n + 4.0 * contacts + 16.0 * pairs
+    return 92.0 * n + 16.0 * pairs + 136.0 * contacts + 4.0 * max(pairs - contacts, 0)
 
 
 def _cpu_child(paths, steps, warmup, threads, budget_s, kind):

@@ -8,7 +8,10 @@
 
 namespace xdem {
 
-constexpr int kNewtonCap = 1000;  // the reference loop (EllipticParticle.cpp:621) has no cap
+// The reference loop (EllipticParticle.cpp:621) has no cap and cycles forever
+// on some deeply overlapping pairs; converging pairs need at most ~120
+// iterations from the analytic start.
+constexpr int kNewtonCap = 256;
 
 enum : uint32_t {
   ST_CAPACITY = 1u << 0,
