@@ -362,6 +362,25 @@ int32_t xdem_range_pop(void);
 void* xdem_host_alloc(int64_t bytes);
 void xdem_host_free(void* p);
 
+/* ---- launch configuration and autotuning ---------------------------------- */
+/* No counterpart in the reference.  Results do not depend on these (the
+   contact set of any cell size >= 2 r_max is the same, and force sums run in
+   id order), only the speed does.  pair_blocks_per_sm: blocks of 128 threads
+   per SM of the pair kernels, whose grid-stride loop gives each thread
+   npairs / (148 * blocks * 128) pairs (default 16); cell_factor: cell size as
+   a multiple of 2.01 x the largest outer radius, in [1, 4] (default 1; a
+   larger cell meets the 200-candidate cap sooner). */
+int32_t xdem_set_launch_config(xdem_world w, int32_t pair_blocks_per_sm, double cell_factor);
+int32_t xdem_get_launch_config(xdem_world w, int32_t* pair_blocks_per_sm, double* cell_factor);
+/* Times steps_per_trial steps of ctl for each of 12 configurations
+   (blocks 4, 8, 16, 32 x cell factors 1, 1.2, 1.5; CUDA events on the
+   world's stream), keeps the fastest and returns the OR of the status bits of
+   the trials.  The trials are real steps: the world advances by
+   12 * (steps_per_trial + 1) steps.  trial_ms (may be NULL): 12 times,
+   factor-major. */
+int32_t xdem_autotune(xdem_world w, const xdem_control* ctl, int32_t steps_per_trial,
+                      double* trial_ms);
+
 /* ---- single-pair geometry (known-answer tests) ------------------------- */
 /* BaseParticle::calculateContactGeometry for one pair on the device.
    pi/pj: {shape, radius, aspect_ratio, x, y, vx, vy, rot, rot_vel};

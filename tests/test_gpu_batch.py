@@ -101,3 +101,38 @@ def test_batch_rejects_stop_on_pressure_and_box_setters():
     ctl = make_control(stop_pressure=1.0)
     done = C.c_int32(0)
     assert batch.lib.xdem_run(batch.h, 5, C.byref(ctl), C.byref(done)) == abi.ERR_ARGUMENT
+
+
+def test_launch_config_leaves_results_unchanged():
+    """Pair-kernel grid and cell size change the speed only: the contact set
+    of any cell size >= 2 r_max is the same and force sums run in id order."""
+    p, prm = ellipse_case(n=800, seed=12, kind=abi.WORLD_LEES_EDWARDS, compress=1.3)
+    a, b = World(prm), World(prm)
+    for w in (a, b):
+        w.raise_mask = ~abi.ERR_NEWTON
+        w.set_particles(p)
+    b.set_launch_config(4, 1.5)
+    assert b.launch_config() == (4, 1.5)
+    for w in (a, b):
+        w.run(70, make_control(update_stress=True))
+    sa, sb = a.get_state(), b.get_state()
+    for key in ("x", "y", "vx", "vy", "rot", "rot_vel"):
+        np.testing.assert_array_equal(sa[key], sb[key], err_msg=key)
+    ca, cb = a.get_contacts(), b.get_contacts()
+    for key in ca:
+        np.testing.assert_array_equal(ca[key], cb[key], err_msg=key)
+    ra, rb = np.asarray(a.getStress()), np.asarray(b.getStress())
+    assert np.max(np.abs(ra - rb)) <= 1e-12 * np.max(np.abs(ra))
+
+
+def test_autotune_picks_a_timed_configuration():
+    systems = _systems()
+    prm0 = systems[0][1]
+    batch = World(prm0)
+    batch.set_batch([p for p, _ in systems], [_box(prm) for _, prm in systems],
+                    [prm.dt for _, prm in systems])
+    blocks, factor, ms = batch.autotune(make_control(), steps_per_trial=5)
+    assert blocks in (4, 8, 16, 32) and factor in (1.0, 1.2, 1.5)
+    assert all(t > 0 for t in ms)
+    k = [1.0, 1.2, 1.5].index(factor) * 4 + [4, 8, 16, 32].index(blocks)
+    assert ms[k] == min(ms)

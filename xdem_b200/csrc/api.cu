@@ -74,6 +74,13 @@ struct xdem_world_s {
   int law = LAW_ANY;                // contact-kernel specialisation for the shapes present
   xdem_mlp_s* mlp = nullptr;        // learned warm start of the closest-approach Newton iteration
   PermList perm{};                  // particle arrays moved by a re-sort
+  // launch configuration (xdem_set_launch_config / xdem_autotune): blocks per
+  // SM of the pair kernels (their grid-stride loop gives each thread
+  // npairs / (blocks * 128) pairs) and the cell size as a multiple of each
+  // system's base cell size
+  int pair_blocks_per_sm = 16;
+  double cell_factor = 1.0;
+  std::vector<double> base_maxsize;
 };
 
 namespace {
@@ -197,7 +204,7 @@ void launch_find(xdem_world_s* w) {
 template <bool FOLD_BG, int LAW>
 void launch_update_phases(xdem_world_s* w, int record) {
   const int nb = blocks_for(w->dw.n, 128);
-  const int pb = 148 * 16;
+  const int pb = 148 * w->pair_blocks_per_sm;
   // the learned warm start applies to closest-approach worlds
   const bool warm = w->mlp != nullptr && w->dw.warm != nullptr && LAW == LAW_CLOSEST;
   LAUNCH(w, KK_CANDIDATES, k_candidates<LAW><<<nb, 128, 0, w->stream>>>(w->dw, w->par));
@@ -632,11 +639,14 @@ int32_t set_particles_impl(xdem_world_s* w, const xdem_particles* P, const std::
       if (!(ws.xlen > 0.0) || !(ws.ylen > 0.0) || !(ws.dt > 0.0)) return XDEM_ERR_ARGUMENT;
     }
     ws.maxsize = w->prm.max_particle_size > 0 ? w->prm.max_particle_size : sys_maxr[k] * 2.01;
-    // grid capacity: twice the starting grid per axis, so a growing box keeps
-    // its cell size for a while and then coarsens
+    w->base_maxsize.resize(nsys);
+    w->base_maxsize[k] = ws.maxsize;
+    // grid capacity: twice the starting grid of the base cell size per axis,
+    // so a growing box keeps its cell size for a while and then coarsens
     int nx0 = (int)std::floor(ws.xlen / ws.maxsize), ny0 = (int)std::floor(ws.ylen / ws.maxsize);
     ws.nx_cap = std::max(3, 2 * nx0 + 4);
     ws.ny_cap = std::max(3, 2 * ny0 + 4);
+    ws.maxsize *= w->cell_factor;
     ws.cell_base = (int32_t)cells;
     ws.first = sys[k].first;
     ws.count = sys[k].count;
@@ -1272,6 +1282,60 @@ int32_t xdem_get_warm_stats(xdem_world w, int64_t out[5]) {
   out[3] = (int64_t)s.warm_restarted;
   out[4] = (int64_t)s.logit_right;
   return XDEM_OK;
+}
+
+// ---- launch configuration and autotuning -----------------------------------------
+int32_t xdem_set_launch_config(xdem_world w, int32_t pair_blocks_per_sm, double cell_factor) {
+  if (!w || pair_blocks_per_sm < 1 || pair_blocks_per_sm > 64 || !(cell_factor >= 1.0) ||
+      cell_factor > 4.0)
+    return XDEM_ERR_ARGUMENT;
+  cudaStreamSynchronize(w->stream);
+  w->pair_blocks_per_sm = pair_blocks_per_sm;
+  w->cell_factor = cell_factor;
+  if (w->dw.n > 0 && !w->base_maxsize.empty()) {
+    // a coarser grid must still fit the cell blocks allocated for the base size
+    CK(w, modify_all(w, [&](WorldScalars& s, int k) { s.maxsize = w->base_maxsize[k] * cell_factor; }));
+  }
+  return XDEM_OK;
+}
+
+int32_t xdem_get_launch_config(xdem_world w, int32_t* pair_blocks_per_sm, double* cell_factor) {
+  if (!w) return XDEM_ERR_ARGUMENT;
+  if (pair_blocks_per_sm) *pair_blocks_per_sm = w->pair_blocks_per_sm;
+  if (cell_factor) *cell_factor = w->cell_factor;
+  return XDEM_OK;
+}
+
+int32_t xdem_autotune(xdem_world w, const xdem_control* ctl, int32_t steps_per_trial,
+                      double* trial_ms) {
+  if (!w || !ctl || steps_per_trial < 1 || w->dw.n <= 0 || ctl->stop_on_pressure)
+    return XDEM_ERR_ARGUMENT;
+  static const int kBlocks[4] = {4, 8, 16, 32};
+  static const double kFactors[3] = {1.0, 1.2, 1.5};
+  double best = 1e300;
+  int bb = w->pair_blocks_per_sm;
+  double bf = w->cell_factor;
+  uint32_t st_all = 0;
+  for (int fi = 0; fi < 3; ++fi)
+    for (int bi = 0; bi < 4; ++bi) {
+      int32_t s = xdem_set_launch_config(w, kBlocks[bi], kFactors[fi]);
+      if (s) return s;
+      // one untimed step settles the grid, then the timed trial
+      int32_t done = 0;
+      st_all |= (uint32_t)xdem_run(w, 1, ctl, &done);
+      CK(w, xdem_timer_start(w) == XDEM_OK ? cudaSuccess : cudaErrorUnknown);
+      st_all |= (uint32_t)xdem_run(w, steps_per_trial, ctl, &done);
+      double ms = 0.0;
+      CK(w, xdem_timer_stop(w, &ms) == XDEM_OK ? cudaSuccess : cudaErrorUnknown);
+      if (trial_ms) trial_ms[fi * 4 + bi] = ms;
+      if (ms < best) {
+        best = ms;
+        bb = kBlocks[bi];
+        bf = kFactors[fi];
+      }
+    }
+  int32_t s = xdem_set_launch_config(w, bb, bf);
+  return s ? s : (int32_t)st_all;
 }
 
 int32_t xdem_harvest_pairs(xdem_world w, xdem_mlp m, int32_t stride, int64_t max_new, int64_t* added) {

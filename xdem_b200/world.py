@@ -386,6 +386,26 @@ class World(WorldBase):
         self._check(self.lib.xdem_get_newton_stats(self.h, out), "newton_stats")
         return int(out[0]), int(out[1]), int(out[2])
 
+    def set_launch_config(self, pair_blocks_per_sm, cell_factor):
+        self._check(self.lib.xdem_set_launch_config(self.h, pair_blocks_per_sm, cell_factor),
+                    "set_launch_config")
+
+    def launch_config(self):
+        b = C.c_int32(0)
+        f = C.c_double(0.0)
+        self._check(self.lib.xdem_get_launch_config(self.h, C.byref(b), C.byref(f)), "launch_config")
+        return int(b.value), float(f.value)
+
+    def autotune(self, control=None, steps_per_trial=20):
+        """Picks the fastest launch configuration by timing real steps (the
+        world advances 12 * (steps_per_trial + 1) steps); returns
+        (blocks per SM, cell factor, 12 trial times in ms)."""
+        ctl = control if control is not None else make_control()
+        ms = (C.c_double * 12)()
+        self._check(self.lib.xdem_autotune(self.h, C.byref(ctl), steps_per_trial, ms), "autotune")
+        b, f = self.launch_config()
+        return b, f, [float(v) for v in ms]
+
     def pair_count(self):
         """Pairs that passed the last candidate scan (geometry evaluated)."""
         v = C.c_int64(0)
