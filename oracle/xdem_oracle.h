@@ -20,7 +20,7 @@
 #include <stdint.h>
 #include "../include/xdem_gpu.h"
 
-#define XO_NEWTON_CAP 256
+#define XO_NEWTON_CAP 1000
 #define XO_CANDIDATE_CAP 200
 
 typedef struct xo_world xo_world;

@@ -138,7 +138,7 @@ def _converged(p, cc, prm):
     off[:, 0] = p["x"][i] - p["x"][j] - cc["branch_x"]
     off[:, 1] = p["y"][i] - p["y"][j] - cc["branch_y"]
     out, _ = oracle.pair_geometry(rows(i), rows(j), off, abi.ELLIPSE_CLOSEST_APPROACH, "port")
-    return out[:, 16] < 256
+    return out[:, 16] < 1000
 
 
 def _force_err(cm, cc, keep=None):

@@ -9,9 +9,9 @@
 namespace xdem {
 
 // The reference loop (EllipticParticle.cpp:621) has no cap and cycles forever
-// on some deeply overlapping pairs; converging pairs need at most ~120
-// iterations from the analytic start.
-constexpr int kNewtonCap = 256;
+// on some deeply overlapping pairs; some converging pairs of dense packings
+// need several hundred iterations from the analytic start.
+constexpr int kNewtonCap = 1000;
 
 enum : uint32_t {
   ST_CAPACITY = 1u << 0,

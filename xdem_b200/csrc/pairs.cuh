@@ -116,7 +116,7 @@ __device__ __forceinline__ int neighbour_cell(const Grid& G, int world_kind, int
 // For an all-ellipse world the thread also leaves (cos, sin) of its
 // orientation for the pair kernel, computed once per body instead of per pair.
 template <int LAW>
-__global__ void __launch_bounds__(128, 7) k_candidates(DevWorld w, int par) {
+__global__ void __launch_bounds__(128) k_candidates(DevWorld w, int par) {
   if (stopped(w)) return;
   const int m = blockIdx.x * blockDim.x + threadIdx.x;
   const bool valid = m < w.n;
@@ -126,9 +126,8 @@ __global__ void __launch_bounds__(128, 7) k_candidates(DevWorld w, int par) {
   const Slots& cur = w.slots[par ^ 1];
   uint32_t st = 0;
   int nlist = 0;
-  // the thread's listed pairs (cell entry, code), slot-major so that a warp's
-  // writes fall in distinct banks
-  __shared__ int2 s_list[kMaxSlots * 128];
+  int32_t list_q[kMaxSlots];
+  int32_t list_code[kMaxSlots];
   if (valid) {
     if (LAW == LAW_CLOSEST || LAW == LAW_INTERSECTION) {
       const double r = w.rot[m];
@@ -159,18 +158,10 @@ __global__ void __launch_bounds__(128, 7) k_candidates(DevWorld w, int par) {
         const int q0 = w.cell_start[c], q1 = w.cell_start[c + 1];
         // the neighbour cell's corner relative to the owner's
         const float ox = dx * flx - rxi, oy = dy * fly - ryi;
-        // records four at a time, all loads issued before any is used
-        for (int qb = q0; qb < q1; qb += 4) {
-         float4 rr[4];
-#pragma unroll
-         for (int u = 0; u < 4; ++u)
-           rr[u] = qb + u < q1 ? w.cell_scr[qb + u] : make_float4(0.0f, 0.0f, 0.0f, __int_as_float(-1));
-#pragma unroll
-         for (int u = 0; u < 4; ++u) {
-          const int q = qb + u;
-          const float4 rj = rr[u];
+        for (int q = q0; q < q1; ++q) {
+          const float4 rj = w.cell_scr[q];
           const int id_j = __float_as_int(rj.w);
-          if (id_j <= id_i) continue;  // also drops SKIP_CONTACT_DETECTION (and the padding)
+          if (id_j <= id_i) continue;  // also drops SKIP_CONTACT_DETECTION
           if (w.cell_up[q] == up_i) continue;
           int& nc = kind == CAND_REGULAR ? ncand0 : (kind == CAND_TOP ? ncand1 : ncand2);
           if (nc + 1 >= kCandidateCap) {
@@ -204,9 +195,9 @@ __global__ void __launch_bounds__(128, 7) k_candidates(DevWorld w, int par) {
           int oslot = kNoOldSlot;
           for (int z = 0; z < nold; ++z)
             if (old.partner[(size_t)z * n + m] == id_j) oslot = z;
-          s_list[nlist * 128 + threadIdx.x] = make_int2(q, kind | (nlist << 8) | (oslot << 16));
+          list_q[nlist] = q;
+          list_code[nlist] = kind | (nlist << 8) | (oslot << 16);
           ++nlist;
-         }
         }
       }
       // old partners among the candidates
@@ -251,10 +242,7 @@ __global__ void __launch_bounds__(128, 7) k_candidates(DevWorld w, int par) {
   int base = block_base;
   for (int k = 0; k < warp; ++k) base += warp_total[k];
   int at = base + incl - nlist;
-  for (int s = 0; s < nlist; ++s) {
-    const int2 e = s_list[s * 128 + threadIdx.x];
-    w.pairs[at + s] = PairEntry{m, w.cell_mem[e.x], e.y, 0};
-  }
+  for (int s = 0; s < nlist; ++s) w.pairs[at + s] = PairEntry{m, w.cell_mem[list_q[s]], list_code[s], 0};
   raise(w.status, st);
 }
 
