@@ -372,6 +372,17 @@ void xdem_host_free(void* p);
    larger cell meets the 200-candidate cap sooner). */
 int32_t xdem_set_launch_config(xdem_world w, int32_t pair_blocks_per_sm, double cell_factor);
 int32_t xdem_get_launch_config(xdem_world w, int32_t* pair_blocks_per_sm, double* cell_factor);
+/* Candidate lists kept across steps (no counterpart in the reference, which
+   rescans the 3x3 cells every step, PeriodicBoundaryWorld.cpp:47-84): each
+   particle keeps the partners within its screening distance plus a skin
+   (skin_fraction x the cell size) found by the last full scan, and only those
+   are tested each step with the reference's tests; the lists are rebuilt when
+   particles, the Lees-Edwards shift or the box have moved enough to use up the
+   skin, after memory-order refreshes and after host changes.  The pairs found
+   are the full scan's.  capacity: partners kept per particle (0 = full scan
+   every step; default 48, more raises XDEM_ERR_CAPACITY); skin_fraction in
+   (0, 1] (default 0.1).  Call before xdem_set_particles. */
+int32_t xdem_set_candidate_lists(xdem_world w, int32_t capacity, double skin_fraction);
 /* Times steps_per_trial steps of ctl for each of 12 configurations
    (blocks 4, 8, 16, 32 x cell factors 1, 1.2, 1.5; CUDA events on the
    world's stream), keeps the fastest and returns the OR of the status bits of

@@ -14,6 +14,7 @@
 #include "pairs.cuh"
 #include "pairs_mixed.cuh"
 #include "learned.cuh"
+#include "verlet.cuh"
 #include "mlp_host.h"
 #include "resort.cuh"
 
@@ -81,6 +82,10 @@ struct xdem_world_s {
   int pair_blocks_per_sm = 16;
   double cell_factor = 1.0;
   std::vector<double> base_maxsize;
+  // candidate lists (verlet.cuh): entries per particle (0 = full scan every
+  // step) and the skin as a fraction of the smallest base cell size
+  int vl_capacity = 48;
+  double skin_fraction = 0.1;
 };
 
 namespace {
@@ -142,13 +147,15 @@ cudaError_t download(T* dst, const T* src, size_t count, cudaStream_t s) {
 enum KernelKind {
   KK_MODIFY = 0, KK_BIN, KK_SCAN, KK_SCATTER, KK_CANDIDATES, KK_PAIRS, KK_FINISH, KK_COLLECT,
   KK_INTEGRATE, KK_RATTLERS, KK_STRESS_PARTIAL, KK_STRESS_FINAL, KK_END_OF_STEP, KK_SCALE,
-  KK_BACKGROUND, KK_KE, KK_RESORT, KK_STAGE, KK_FALLBACK, KK_WARM, KK_COUNT
+  KK_BACKGROUND, KK_KE, KK_RESORT, KK_STAGE, KK_FALLBACK, KK_WARM, KK_VL_CHECK, KK_VL_BUILD,
+  KK_COUNT
 };
 const char* const kKindNames[KK_COUNT] = {
     "k_modify_position", "k_bin", "k_scan", "k_scatter", "k_candidates", "k_pair_forces",
     "k_finish_slots", "k_collect", "k_integrate", "k_rattlers", "k_stress_partial",
     "k_stress_final", "k_end_of_step", "k_scale_positions", "k_background_velocity",
-    "k_kinetic_energy", "k_resort", "k_stage", "k_pair_fallback", "k_mlp_warm"};
+    "k_kinetic_energy", "k_resort", "k_stage", "k_pair_fallback", "k_mlp_warm", "k_vl_check",
+    "k_vl_build"};
 
 void prof_begin(xdem_world_s* w, int kind) {
   if (!w->prof_on) return;
@@ -207,7 +214,15 @@ void launch_update_phases(xdem_world_s* w, int record) {
   const int pb = 148 * w->pair_blocks_per_sm;
   // the learned warm start applies to closest-approach worlds
   const bool warm = w->mlp != nullptr && w->dw.warm != nullptr && LAW == LAW_CLOSEST;
-  LAUNCH(w, KK_CANDIDATES, k_candidates<LAW><<<nb, 128, 0, w->stream>>>(w->dw, w->par));
+  if (w->dw.V > 0) {
+    const int vb = blocks_for(w->dw.n, kVlBlock);
+    LAUNCH(w, KK_VL_CHECK, k_vl_maxdisp<<<vb, kVlBlock, 0, w->stream>>>(w->dw));
+    LAUNCH(w, KK_VL_CHECK, k_vl_check<<<1, 1024, 0, w->stream>>>(w->dw, vb));
+    LAUNCH(w, KK_VL_BUILD, k_vl_build<LAW><<<nb, 128, 0, w->stream>>>(w->dw));
+    LAUNCH(w, KK_CANDIDATES, k_candidates_vl<LAW><<<nb, 128, 0, w->stream>>>(w->dw, w->par));
+  } else {
+    LAUNCH(w, KK_CANDIDATES, k_candidates<LAW><<<nb, 128, 0, w->stream>>>(w->dw, w->par));
+  }
   if (w->prm.precision == XDEM_PRECISION_MIXED) {
     LAUNCH(w, KK_PAIRS,
            k_pair_forces_m<FOLD_BG, LAW><<<pb, 128, 0, w->stream>>>(w->dw, w->par, record));
@@ -650,6 +665,8 @@ int32_t set_particles_impl(xdem_world_s* w, const xdem_particles* P, const std::
     ws.cell_base = (int32_t)cells;
     ws.first = sys[k].first;
     ws.count = sys[k].count;
+    ws.vl_valid = 0;  // the first step builds the candidate lists
+    ws.vl_travel = 0.0;
     cell_base[k] = (int32_t)cells;
     cells += (size_t)ws.nx_cap * ws.ny_cap + 2 * (size_t)ws.nx_cap;
     if (cells >= ((size_t)1 << 31) - 2) return XDEM_ERR_ARGUMENT;
@@ -710,6 +727,25 @@ int32_t set_particles_impl(xdem_world_s* w, const xdem_particles* P, const std::
   CK(w, cudaMemsetAsync(d.nfallback, 0, sizeof(int32_t), s));
   d.warm = nullptr;
   if (w->mlp) CK(w, B.alloc(&d.warm, ks));
+  // candidate lists: rebuilt by the first step (vl_valid starts at 0)
+  d.V = w->vl_capacity;
+  {
+    double smallest = 1e300;
+    for (double b : w->base_maxsize) smallest = std::min(smallest, b);
+    d.skin = w->skin_fraction * smallest;
+  }
+  d.vl = nullptr;
+  d.vl_cnt = nullptr;
+  d.vl_disp = nullptr;
+  d.vl_part = nullptr;
+  if (d.V > 0) {
+    CK(w, B.alloc(&d.vl, (size_t)d.V * n));
+    CK(w, B.alloc(&d.vl_cnt, n));
+    CK(w, B.alloc(&d.vl_disp, n));
+    CK(w, B.alloc(&d.vl_part, (size_t)blocks_for(n, kVlBlock) + 1));
+    CK(w, cudaMemsetAsync(d.vl_cnt, 0, sizeof(int32_t) * n, s));
+    CK(w, cudaMemsetAsync(d.vl_disp, 0, sizeof(double) * n, s));
+  }
   w->partial_blocks = blocks_for(n, kReduceBlock);
   CK(w, B.alloc(&d.partials, 4 * (size_t)w->partial_blocks + 4));
   // memory order starts as id order
@@ -1150,6 +1186,7 @@ int32_t xdem_set_boundary(xdem_world w, const double box[4]) {
   s.ymax = box[3];
   s.xlen = s.xmax - s.xmin;
   s.ylen = s.ymax - s.ymin;
+  s.vl_valid = 0;  // the candidate lists are rebuilt by the next step
   CK(w, write_scalars(w, &s));
   return XDEM_OK;
 }
@@ -1181,6 +1218,7 @@ int32_t xdem_set_lees_edwards(xdem_world w, const double in[4]) {
   s.shift_vel = in[1];
   s.strain = in[2];
   s.shift_rate = in[3];
+  s.vl_valid = 0;
   CK(w, write_scalars(w, &s));
   return XDEM_OK;
 }
@@ -1296,6 +1334,15 @@ int32_t xdem_set_launch_config(xdem_world w, int32_t pair_blocks_per_sm, double 
     // a coarser grid must still fit the cell blocks allocated for the base size
     CK(w, modify_all(w, [&](WorldScalars& s, int k) { s.maxsize = w->base_maxsize[k] * cell_factor; }));
   }
+  return XDEM_OK;
+}
+
+int32_t xdem_set_candidate_lists(xdem_world w, int32_t capacity, double skin_fraction) {
+  if (!w || capacity < 0 || capacity > 256 || !(skin_fraction > 0.0) || skin_fraction > 1.0)
+    return XDEM_ERR_ARGUMENT;
+  if (w->dw.n > 0) return XDEM_ERR_ARGUMENT;  // before xdem_set_particles
+  w->vl_capacity = capacity;
+  w->skin_fraction = skin_fraction;
   return XDEM_OK;
 }
 
@@ -1471,6 +1518,7 @@ int32_t xdem_scale_boundary_to_solid_fraction(xdem_world w, double phi) {
   CK(w, read_scalars(w, &s));
   double cur = w->total_volume / (s.xlen * s.ylen);
   double scale = std::sqrt(cur / phi);
+  s.vl_valid = 0;
   s.scale_x = scale;
   s.scale_y = scale;
   s.xmin *= scale;

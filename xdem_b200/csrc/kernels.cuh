@@ -112,9 +112,11 @@ __global__ void k_modify_position(DevWorld w) {
     if (p.y < ws.ymin) {
       p.y += ws.ylen;
       p.x += ws.shift;
+      if (w.V) w.ws->vl_valid = 0;  // its image kinds change: rebuild the candidate lists
     } else if (p.y > ws.ymax) {
       p.y += -ws.ylen;
       p.x += -ws.shift;
+      if (w.V) w.ws->vl_valid = 0;
     }
     if (p.x < ws.xmin) p.x += ws.xlen;
     else if (p.x > ws.xmax) p.x += -ws.xlen;
@@ -508,10 +510,16 @@ __global__ void k_integrate(DevWorld w, int reset_rattlers) {
       w.branch[sk] = make_double2(b.x, b.y);
       vec2<double> sv = vv + crossw(b, om);
       w.vel[sk] = make_double2(sv.x, sv.y);
+      if (w.V) {  // path length for the candidate lists
+        const double2 op = w.pos[sk];
+        const double ex = (p.x + b.x) - op.x, ey = (p.y + b.y) - op.y;
+        w.vl_disp[sk] += sqrt(ex * ex + ey * ey);
+      }
       w.pos[sk] = make_double2(p.x + b.x, p.y + b.y);
       w.w[sk] = om;
       w.rot[sk] += angle;
     }
+    if (w.V) w.vl_disp[i] += sqrt(vv.x * vv.x + vv.y * vv.y) * dt;
     w.pos[i] = p;
     w.rot[i] = rot;
     if (reset_rattlers && !(set & SKIP_MACRO_SUM) && is_rattler(w, i)) {
@@ -529,6 +537,7 @@ __global__ void k_integrate(DevWorld w, int reset_rattlers) {
   p.x += vv.x * dt;
   p.y += vv.y * dt;
   om = (om * (1.0 - g * dt) + w.torque[i] * w.iI[i] * dt) / (1.0 + g * dt);
+  if (w.V) w.vl_disp[i] += sqrt(vv.x * vv.x + vv.y * vv.y) * dt;  // for the candidate lists
   w.pos[i] = p;
   w.rot[i] = w.rot[i] + om * dt;
   if (reset_rattlers && !(set & SKIP_MACRO_SUM) && w.rattler[i]) {
@@ -772,8 +781,14 @@ __global__ void k_end_of_step(DevWorld w, int law, double p0, double p1, int le_
     ws.shift += ws.shift_vel * ws.dt;
     if (ws.shift > ws.xmax) ws.shift -= ws.xlen;
     else if (ws.shift < ws.xmin) ws.shift += ws.xlen;
+    // pairs across the sheared edge move apart by the shift travelled
+    ws.vl_travel += fabs(ws.shift_vel * ws.dt);
   }
-  if (law != BOX_NONE) box_law(ws, law, p0, p1);
+  if (law != BOX_NONE) {
+    box_law(ws, law, p0, p1);
+    // an affine scale s moves a pair at distance d by |s - 1| d
+    ws.vl_travel += fmax(fabs(ws.scale_x - 1.0), fabs(ws.scale_y - 1.0)) * (ws.maxsize + w.skin);
+  }
   if (sys != 0) return;
   if (count_step) {
     ws.steps_done += 1;
@@ -825,6 +840,11 @@ __global__ void k_stage(DevWorld w, int to_world) {
   const int m = w.mpos[id];
   double* s = w.stage;
   if (to_world) {
+    if (w.V) {  // the host's move counts toward the candidate lists' skin
+      const double2 op = w.pos[m];
+      const double ex = s[id] - op.x, ey = s[n + id] - op.y;
+      w.vl_disp[m] += sqrt(ex * ex + ey * ey);
+    }
     w.pos[m] = make_double2(s[id], s[n + id]);
     w.vel[m] = make_double2(s[2 * n + id], s[3 * n + id]);
     w.rot[m] = s[4 * n + id];

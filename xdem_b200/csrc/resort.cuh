@@ -24,6 +24,8 @@ struct PermList {
 // along; newpos = the sorted index
 __global__ void k_sort_cells(DevWorld w) {
   if (stopped(w)) return;
+  // memory positions move: the candidate lists hold them
+  if (blockIdx.x == 0 && threadIdx.x == 0) w.ws->vl_valid = 0;
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < w.ncell_total;
        c += gridDim.x * blockDim.x) {
     const Grid G = grid_of(w.ws[sys_of_cell(w, c)]);

@@ -50,13 +50,18 @@ struct WorldScalars {
   double dt, g, kn, kt, mu, factor;
   double maxsize;
   double ke;
+  double vl_travel;  // relative displacement budget used since the candidate lists were built
+                     // (Lees-Edwards shift travelled, affine box scaling)
   int32_t stop;        // set once a run's stop condition is met
   int32_t steps_done;  // steps completed in the current run
   int32_t flips;       // slot-set swaps executed in the current run
   int32_t last_pairs;  // pairs listed by the last candidate scan
   // cell grid of this system: capacity per axis and first cell in the cell
   // arrays; particles (ids and memory positions) [first, first + count)
-  int32_t nx_cap, ny_cap, cell_base, first, count, pad_;
+  int32_t nx_cap, ny_cap, cell_base, first, count;
+  // candidate lists (verlet.cuh), system 0: 0 once they must be rebuilt;
+  // 1 while the step's build kernel rebuilds them
+  int32_t vl_valid, vl_build, pad_;
   // closest-approach Newton statistics since the last reset: solves,
   // iterations, solves stopped by the iteration cap
   unsigned long long newton_solves, newton_iters, newton_capped;
@@ -146,6 +151,13 @@ struct DevWorld {
   int32_t* fallback;   // [K*n] mixed precision: listed pairs deferred to the FP64 construction
   int32_t* nfallback;  // number of deferred pairs
   float2* warm;        // [K*n] learned warm start of each listed pair: (root fraction, contact logit)
+  // candidate lists kept across steps (verlet.cuh); V == 0: full scan each step
+  int V;
+  double skin;
+  int32_t* vl;       // [V*n] entries (partner memory position << 2 | image kind), slot-major
+  int32_t* vl_cnt;   // [n]
+  double* vl_disp;   // [n] path length since the lists were built
+  double* vl_part;   // block maxima of vl_disp
   // scalars (one per system), status, scratch
   WorldScalars* ws;
   uint32_t* status;

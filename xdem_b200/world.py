@@ -390,6 +390,12 @@ class World(WorldBase):
         self._check(self.lib.xdem_set_launch_config(self.h, pair_blocks_per_sm, cell_factor),
                     "set_launch_config")
 
+    def set_candidate_lists(self, capacity, skin_fraction=0.1):
+        """Before set_particles: partners kept per particle (0 = full 3x3 scan
+        every step) and the skin as a fraction of the cell size."""
+        self._check(self.lib.xdem_set_candidate_lists(self.h, capacity, skin_fraction),
+                    "set_candidate_lists")
+
     def launch_config(self):
         b = C.c_int32(0)
         f = C.c_double(0.0)
