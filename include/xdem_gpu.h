@@ -383,6 +383,9 @@ int32_t xdem_get_launch_config(xdem_world w, int32_t* pair_blocks_per_sm, double
    every step; default 48, more raises XDEM_ERR_CAPACITY); skin_fraction in
    (0, 1] (default 0.1).  Call before xdem_set_particles. */
 int32_t xdem_set_candidate_lists(xdem_world w, int32_t capacity, double skin_fraction);
+/* out = {list rebuilds since the last xdem_reset_newton_stats, longest list,
+   total entries, capacity} */
+int32_t xdem_get_candidate_list_stats(xdem_world w, int64_t out[4]);
 /* Times steps_per_trial steps of ctl for each of 12 configurations
    (blocks 4, 8, 16, 32 x cell factors 1, 1.2, 1.5; CUDA events on the
    world's stream), keeps the fastest and returns the OR of the status bits of

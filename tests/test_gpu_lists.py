@@ -9,18 +9,20 @@ import pytest
 from xdem_b200 import abi
 from xdem_b200.world import World, make_control
 
-from helpers import clump_case, disc_case, ellipse_case
+from helpers import clump_case, dense_ellipse_case, disc_case
 
 pytestmark = pytest.mark.gpu
 
 
-def _pair_of_worlds(p, prm, skin=0.1):
+def _pair_of_worlds(p, prm, skin=0.1, contacts=None):
     a, b = World(prm), World(prm)
     a.set_candidate_lists(0)
     b.set_candidate_lists(48, skin)
     for w in (a, b):
         w.raise_mask = ~abi.ERR_NEWTON
         w.set_particles(p)
+        if contacts is not None:
+            w.set_contacts(contacts)
     return a, b
 
 
@@ -36,14 +38,15 @@ def _same(a, b):
 
 @pytest.mark.parametrize("precision", [abi.PRECISION_FP64, abi.PRECISION_MIXED])
 def test_lists_match_full_scan_lees_edwards(precision):
-    p, prm = ellipse_case(n=1500, seed=61, kind=abi.WORLD_LEES_EDWARDS, compress=1.3,
-                          shift_rate=2.0)
+    p, contacts, prm = dense_ellipse_case(n=2000, seed=61, kind=abi.WORLD_LEES_EDWARDS,
+                                          shift_rate=2.0)
     prm.precision = precision
-    a, b = _pair_of_worlds(p, prm, skin=0.05)
+    a, b = _pair_of_worlds(p, prm, skin=0.05, contacts=contacts)
     for w in (a, b):
         w.run(150, make_control(update_stress=True))
-    assert _same(a, b) > 500
+    assert _same(a, b) > 1500
     assert abs(a.getLeesEdwards()[0]) > 0
+    assert b.candidate_list_stats()["builds"] > 2
 
 
 def test_lists_match_full_scan_strain_control_and_uploads():

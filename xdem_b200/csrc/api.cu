@@ -1294,6 +1294,7 @@ int32_t xdem_reset_newton_stats(xdem_world w) {
   WorldScalars s;
   CK(w, read_scalars(w, &s));
   s.newton_solves = s.newton_iters = s.newton_capped = 0;
+  s.vl_builds = 0;
   s.warm_offered = s.warm_used = s.warm_rejected = s.warm_restarted = s.logit_right = 0;
   CK(w, write_scalars(w, &s));
   return XDEM_OK;
@@ -1343,6 +1344,28 @@ int32_t xdem_set_candidate_lists(xdem_world w, int32_t capacity, double skin_fra
   if (w->dw.n > 0) return XDEM_ERR_ARGUMENT;  // before xdem_set_particles
   w->vl_capacity = capacity;
   w->skin_fraction = skin_fraction;
+  return XDEM_OK;
+}
+
+int32_t xdem_get_candidate_list_stats(xdem_world w, int64_t out[4]) {
+  if (!w || !out) return XDEM_ERR_ARGUMENT;
+  WorldScalars s;
+  CK(w, read_scalars(w, &s));
+  out[0] = (int64_t)s.vl_builds;
+  out[1] = out[2] = 0;
+  out[3] = w->dw.V;
+  if (w->dw.V > 0 && w->dw.n > 0) {
+    std::vector<int32_t> cnt(w->dw.n);
+    CK(w, download(cnt.data(), w->dw.vl_cnt, w->dw.n, w->stream));
+    CK(w, cudaStreamSynchronize(w->stream));
+    int64_t tot = 0, mx = 0;
+    for (int32_t c : cnt) {
+      tot += c;
+      mx = std::max<int64_t>(mx, c);
+    }
+    out[1] = mx;
+    out[2] = tot;
+  }
   return XDEM_OK;
 }
 

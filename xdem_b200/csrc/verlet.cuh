@@ -61,6 +61,7 @@ __global__ void __launch_bounds__(1024) k_vl_check(DevWorld w, int nblocks) {
     if (rebuild) {
       for (int s = 0; s < w.nsys; ++s) ws[s].vl_travel = 0.0;
       ws[0].vl_valid = 1;
+      ws[0].vl_builds += 1;
     }
   }
 }

@@ -69,6 +69,7 @@ struct WorldScalars {
   // the residual test, used but overruled by the plain start; contact logits
   // that matched the outcome
   unsigned long long warm_offered, warm_used, warm_rejected, warm_restarted, logit_right;
+  unsigned long long vl_builds;  // candidate-list rebuilds since the last reset
 };
 
 // one pair listed by the candidate scan: owner position, partner position,

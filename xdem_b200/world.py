@@ -396,6 +396,12 @@ class World(WorldBase):
         self._check(self.lib.xdem_set_candidate_lists(self.h, capacity, skin_fraction),
                     "set_candidate_lists")
 
+    def candidate_list_stats(self):
+        """{builds, longest, entries, capacity} of the candidate lists"""
+        out = (C.c_int64 * 4)()
+        self._check(self.lib.xdem_get_candidate_list_stats(self.h, out), "candidate_list_stats")
+        return dict(zip(("builds", "longest", "entries", "capacity"), (int(v) for v in out)))
+
     def launch_config(self):
         b = C.c_int32(0)
         f = C.c_double(0.0)
