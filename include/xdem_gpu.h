@@ -380,7 +380,8 @@ int32_t xdem_get_launch_config(xdem_world w, int32_t* pair_blocks_per_sm, double
    particles, the Lees-Edwards shift or the box have moved enough to use up the
    skin, after memory-order refreshes and after host changes.  The pairs found
    are the full scan's.  capacity: partners kept per particle (0 = full scan
-   every step; default 48, more raises XDEM_ERR_CAPACITY); skin_fraction in
+   every step; default 48; a particle with more is scanned in full until the next
+   build); skin_fraction in
    (0, 1] (default 0.1).  Call before xdem_set_particles. */
 int32_t xdem_set_candidate_lists(xdem_world w, int32_t capacity, double skin_fraction);
 /* out = {list rebuilds since the last xdem_reset_newton_stats, longest list,

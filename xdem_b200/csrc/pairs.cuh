@@ -106,6 +106,77 @@ __device__ __forceinline__ int neighbour_cell(const Grid& G, int world_kind, int
   return G.base + jy * G.nx + jx;
 }
 
+// The reference's 3x3 scan for the owner at m (cell ix, iy): every candidate
+// j with a larger id and another upLevel, counted per image kind against the
+// 200-candidate cap, and the ones passing the coarse test appended to
+// (list_mj, list_code).  The distance screen runs in FP32 on positions
+// relative to the cell corners; only candidates within its rounding margin of
+// the threshold take the reference's FP64 test.
+template <int LAW>
+__device__ __forceinline__ void scan_cells(const DevWorld& w, const WorldScalars& ws, const Grid& G,
+                                           int m, int ix, int iy, double2 pi, int id_i, int up_i,
+                                           int shape_i, double r_i, double orad_i,
+                                           const Slots& old, int nold, int& nlist,
+                                           int32_t* list_mj, int32_t* list_code, uint32_t& st) {
+  const int n = w.n, K = w.K;
+  // the owner relative to its cell's corner, in FP32 (see k_scatter)
+  const float rxi = (float)(pi.x - (ws.xmin + ix * G.lx));
+  const float ryi = (float)(pi.y - (ws.ymin + iy * G.ly));
+  const float flx = (float)G.lx, fly = (float)G.ly;
+  const float sr_i = (float)w.screen_r[m];
+  int ncand0 = 0, ncand1 = 0, ncand2 = 0;
+#pragma unroll 1
+  for (int k = 0; k < 9; ++k) {
+    const int dx = k / 3 - 1, dy = k % 3 - 1;
+    int kind;
+    const int c = neighbour_cell(G, w.kind, ix, iy, dx, dy, kind);
+    const int q0 = w.cell_start[c], q1 = w.cell_start[c + 1];
+    // the neighbour cell's corner relative to the owner's
+    const float ox = dx * flx - rxi, oy = dy * fly - ryi;
+    for (int q = q0; q < q1; ++q) {
+      const float4 rj = w.cell_scr[q];
+      const int id_j = __float_as_int(rj.w);
+      if (id_j <= id_i) continue;  // also drops SKIP_CONTACT_DETECTION
+      if (w.cell_up[q] == up_i) continue;
+      int& nc = kind == CAND_REGULAR ? ncand0 : (kind == CAND_TOP ? ncand1 : ncand2);
+      if (nc + 1 >= kCandidateCap) {
+        st |= ST_CAPACITY;
+        continue;
+      }
+      nc++;
+      // FP32 screen with a margin well above its rounding error; the band
+      // around the threshold takes the reference's FP64 test
+      const float ddx = ox + rj.x, ddy = oy + rj.y;
+      const float d2 = ddx * ddx + ddy * ddy;
+      const float R = sr_i + rj.z, R2 = R * R;
+      if (d2 > R2 * (1.0f + 1e-4f) + 1e-4f) continue;
+      if (LAW == LAW_ANY || !(d2 < R2 * (1.0f - 1e-4f) - 1e-4f)) {
+        const double2 pj = w.cell_pos[q];
+        vec2<double> off, ovel;
+        image_offset(ws, kind, pi, pj, off, ovel);
+        const int mj = w.cell_mem[q];
+        bool pass;
+        if (LAW == LAW_ANY)
+          pass = coarse_pass<LAW>(shape_i, w.shape[mj], r_i, w.rad[mj], orad_i, w.orad[mj], pi,
+                                  pj, off);
+        else
+          pass = coarse_pass<LAW>(0, 0, r_i, w.screen_r[mj], orad_i, w.screen_r[mj], pi, pj, off);
+        if (!pass) continue;
+      }
+      if (nlist >= K) {
+        st |= ST_CAPACITY;
+        continue;
+      }
+      int oslot = kNoOldSlot;
+      for (int z = 0; z < nold; ++z)
+        if (old.partner[(size_t)z * n + m] == id_j) oslot = z;
+      list_mj[nlist] = w.cell_mem[q];
+      list_code[nlist] = kind | (nlist << 8) | (oslot << 16);
+      ++nlist;
+    }
+  }
+}
+
 // One thread per owner m.  Cell entries are read from the cell-ordered
 // screening records (cell_scr, cell_up), so a neighbour cell is one
 // contiguous run of 20-byte records; the distance screen runs in FP32 on
@@ -126,7 +197,7 @@ __global__ void __launch_bounds__(128) k_candidates(DevWorld w, int par) {
   const Slots& cur = w.slots[par ^ 1];
   uint32_t st = 0;
   int nlist = 0;
-  int32_t list_q[kMaxSlots];
+  int32_t list_mj[kMaxSlots];
   int32_t list_code[kMaxSlots];
   if (valid) {
     if (LAW == LAW_CLOSEST || LAW == LAW_INTERSECTION) {
@@ -144,62 +215,8 @@ __global__ void __launch_bounds__(128) k_candidates(DevWorld w, int par) {
       const double r_i = w.rad[m], orad_i = w.orad[m];
       const int ix = cell_of(pi.x, ws.xmin, G.lx, G.nx);
       const int iy = cell_of(pi.y, ws.ymin, G.ly, G.ny);
-      // the owner relative to its cell's corner, in FP32 (see k_scatter)
-      const float rxi = (float)(pi.x - (ws.xmin + ix * G.lx));
-      const float ryi = (float)(pi.y - (ws.ymin + iy * G.ly));
-      const float flx = (float)G.lx, fly = (float)G.ly;
-      const float sr_i = (float)w.screen_r[m];
-      int ncand0 = 0, ncand1 = 0, ncand2 = 0;
-#pragma unroll 1
-      for (int k = 0; k < 9; ++k) {
-        const int dx = k / 3 - 1, dy = k % 3 - 1;
-        int kind;
-        const int c = neighbour_cell(G, w.kind, ix, iy, dx, dy, kind);
-        const int q0 = w.cell_start[c], q1 = w.cell_start[c + 1];
-        // the neighbour cell's corner relative to the owner's
-        const float ox = dx * flx - rxi, oy = dy * fly - ryi;
-        for (int q = q0; q < q1; ++q) {
-          const float4 rj = w.cell_scr[q];
-          const int id_j = __float_as_int(rj.w);
-          if (id_j <= id_i) continue;  // also drops SKIP_CONTACT_DETECTION
-          if (w.cell_up[q] == up_i) continue;
-          int& nc = kind == CAND_REGULAR ? ncand0 : (kind == CAND_TOP ? ncand1 : ncand2);
-          if (nc + 1 >= kCandidateCap) {
-            st |= ST_CAPACITY;
-            continue;
-          }
-          nc++;
-          // FP32 screen with a margin well above its rounding error; the band
-          // around the threshold takes the reference's FP64 test
-          const float ddx = ox + rj.x, ddy = oy + rj.y;
-          const float d2 = ddx * ddx + ddy * ddy;
-          const float R = sr_i + rj.z, R2 = R * R;
-          if (d2 > R2 * (1.0f + 1e-4f) + 1e-4f) continue;
-          if (LAW == LAW_ANY || !(d2 < R2 * (1.0f - 1e-4f) - 1e-4f)) {
-            const double2 pj = w.cell_pos[q];
-            vec2<double> off, ovel;
-            image_offset(ws, kind, pi, pj, off, ovel);
-            const int mj = w.cell_mem[q];
-            bool pass;
-            if (LAW == LAW_ANY)
-              pass = coarse_pass<LAW>(shape_i, w.shape[mj], r_i, w.rad[mj], orad_i, w.orad[mj], pi,
-                                      pj, off);
-            else
-              pass = coarse_pass<LAW>(0, 0, r_i, w.screen_r[mj], orad_i, w.screen_r[mj], pi, pj, off);
-            if (!pass) continue;
-          }
-          if (nlist >= K) {
-            st |= ST_CAPACITY;
-            continue;
-          }
-          int oslot = kNoOldSlot;
-          for (int z = 0; z < nold; ++z)
-            if (old.partner[(size_t)z * n + m] == id_j) oslot = z;
-          list_q[nlist] = q;
-          list_code[nlist] = kind | (nlist << 8) | (oslot << 16);
-          ++nlist;
-        }
-      }
+      scan_cells<LAW>(w, ws, G, m, ix, iy, pi, id_i, up_i, shape_i, r_i, orad_i, old, nold, nlist,
+                      list_mj, list_code, st);
       // old partners among the candidates
       for (int z = 0; z < nold; ++z) {
         const int p = old.partner[(size_t)z * n + m];
@@ -242,7 +259,7 @@ __global__ void __launch_bounds__(128) k_candidates(DevWorld w, int par) {
   int base = block_base;
   for (int k = 0; k < warp; ++k) base += warp_total[k];
   int at = base + incl - nlist;
-  for (int s = 0; s < nlist; ++s) w.pairs[at + s] = PairEntry{m, w.cell_mem[list_q[s]], list_code[s], 0};
+  for (int s = 0; s < nlist; ++s) w.pairs[at + s] = PairEntry{m, list_mj[s], list_code[s], 0};
   raise(w.status, st);
 }
 

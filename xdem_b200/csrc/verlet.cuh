@@ -68,7 +68,9 @@ __global__ void __launch_bounds__(1024) k_vl_check(DevWorld w, int nblocks) {
 
 // One thread per owner: the full 3x3 scan with the reference's filters, the
 // partners within R + skin (an FP32 test with a margin that only widens the
-// list) kept as (memory position, image kind); the path lengths restart.
+// list) kept as (memory position, image kind); the path lengths restart.  An
+// owner with more partners than the list holds is marked (count -1) and
+// scanned in full every step until the next build.
 template <int LAW>
 __global__ void __launch_bounds__(128) k_vl_build(DevWorld w) {
   if (stopped(w) || !w.ws->vl_build) return;
@@ -78,7 +80,6 @@ __global__ void __launch_bounds__(128) k_vl_build(DevWorld w) {
   const WorldScalars& ws = w.ws[sys_at(w, m)];
   const int n = w.n;
   int cnt = 0;
-  uint32_t st = 0;
   const Grid G = grid_of(ws);
   if (G.nx >= 3 && G.ny >= 3 && !(w.setting[m] & SKIP_CONTACT_DETECTION)) {
     const double2 pi = w.pos[m];
@@ -104,16 +105,16 @@ __global__ void __launch_bounds__(128) k_vl_build(DevWorld w) {
         const float R = sr_i + rj.z;
         if (ddx * ddx + ddy * ddy > R * R * (1.0f + 1e-4f) + 1e-4f) continue;
         if (cnt >= w.V) {
-          st |= ST_CAPACITY;
-          continue;
+          cnt = -1;
+          break;
         }
         w.vl[(size_t)cnt * n + m] = (w.cell_mem[q] << 2) | kind;
         ++cnt;
       }
+      if (cnt < 0) break;
     }
   }
   w.vl_cnt[m] = cnt;
-  raise(w.status, st);
 }
 
 // k_candidates with the lists: same outputs (slot counts, seen masks, the
@@ -147,56 +148,63 @@ __global__ void __launch_bounds__(128) k_candidates_vl(DevWorld w, int par) {
       const double r_i = w.rad[m], orad_i = w.orad[m];
       const int ix = cell_of(pi.x, ws.xmin, G.lx, G.nx);
       const int iy = cell_of(pi.y, ws.ymin, G.ly, G.ny);
-      // the 200-candidate cap (PeriodicBoundaryWorld.cpp:75-78): the nine
-      // cells' record counts bound each kind's candidates; where a bound
-      // reaches the cap, the candidates are counted as the full scan does
-      int tot0 = 0, tot1 = 0, tot2 = 0;
+      const int cnt = w.vl_cnt[m];
+      if (cnt < 0) {  // the list overflowed at its build: the full scan
+        scan_cells<LAW>(w, ws, G, m, ix, iy, pi, id_i, up_i, shape_i, r_i, orad_i, old, nold,
+                        nlist, list_mj, list_code, st);
+      } else {
+        // the 200-candidate cap (PeriodicBoundaryWorld.cpp:75-78): the nine
+        // cells' record counts bound each kind's candidates; where a bound
+        // reaches the cap, the candidates are counted as the full scan does
+        int tot0 = 0, tot1 = 0, tot2 = 0;
 #pragma unroll
-      for (int k = 0; k < 9; ++k) {
-        int kind;
-        const int c = neighbour_cell(G, w.kind, ix, iy, k / 3 - 1, k % 3 - 1, kind);
-        const int cc = w.cell_start[c + 1] - w.cell_start[c];
-        tot0 += kind == CAND_REGULAR ? cc : 0;
-        tot1 += kind == CAND_TOP ? cc : 0;
-        tot2 += kind == CAND_BOTTOM ? cc : 0;
-      }
-      if (tot0 + 1 >= kCandidateCap || tot1 + 1 >= kCandidateCap || tot2 + 1 >= kCandidateCap) {
-        int c0 = 0, c1 = 0, c2 = 0;
         for (int k = 0; k < 9; ++k) {
           int kind;
           const int c = neighbour_cell(G, w.kind, ix, iy, k / 3 - 1, k % 3 - 1, kind);
-          for (int q = w.cell_start[c]; q < w.cell_start[c + 1]; ++q) {
-            if (__float_as_int(w.cell_scr[q].w) <= id_i || w.cell_up[q] == up_i) continue;
-            int& nc = kind == CAND_REGULAR ? c0 : (kind == CAND_TOP ? c1 : c2);
-            if (nc + 1 >= kCandidateCap) st |= ST_CAPACITY;
-            else nc++;
+          const int cc = w.cell_start[c + 1] - w.cell_start[c];
+          tot0 += kind == CAND_REGULAR ? cc : 0;
+          tot1 += kind == CAND_TOP ? cc : 0;
+          tot2 += kind == CAND_BOTTOM ? cc : 0;
+        }
+        if (tot0 + 1 >= kCandidateCap || tot1 + 1 >= kCandidateCap || tot2 + 1 >= kCandidateCap) {
+          int c0 = 0, c1 = 0, c2 = 0;
+          for (int k = 0; k < 9; ++k) {
+            int kind;
+            const int c = neighbour_cell(G, w.kind, ix, iy, k / 3 - 1, k % 3 - 1, kind);
+            for (int q = w.cell_start[c]; q < w.cell_start[c + 1]; ++q) {
+              if (__float_as_int(w.cell_scr[q].w) <= id_i || w.cell_up[q] == up_i) continue;
+              int& nc = kind == CAND_REGULAR ? c0 : (kind == CAND_TOP ? c1 : c2);
+              if (nc + 1 >= kCandidateCap) st |= ST_CAPACITY;
+              else nc++;
+            }
           }
         }
-      }
-      const int cnt = w.vl_cnt[m];
-      for (int v = 0; v < cnt; ++v) {
-        const int e = w.vl[(size_t)v * n + m];
-        const int mj = e >> 2, kind = e & 3;
-        const double2 pj = w.pos[mj];
-        vec2<double> off, ovel;
-        image_offset(ws, kind, pi, pj, off, ovel);
-        bool pass;
-        if (LAW == LAW_ANY)
-          pass = coarse_pass<LAW>(shape_i, w.shape[mj], r_i, w.rad[mj], orad_i, w.orad[mj], pi, pj, off);
-        else
-          pass = coarse_pass<LAW>(0, 0, r_i, w.screen_r[mj], orad_i, w.screen_r[mj], pi, pj, off);
-        if (!pass) continue;
-        if (nlist >= K) {
-          st |= ST_CAPACITY;
-          continue;
+        for (int v = 0; v < cnt; ++v) {
+          const int e = w.vl[(size_t)v * n + m];
+          const int mj = e >> 2, kind = e & 3;
+          const double2 pj = w.pos[mj];
+          vec2<double> off, ovel;
+          image_offset(ws, kind, pi, pj, off, ovel);
+          bool pass;
+          if (LAW == LAW_ANY)
+            pass = coarse_pass<LAW>(shape_i, w.shape[mj], r_i, w.rad[mj], orad_i, w.orad[mj], pi,
+                                    pj, off);
+          else
+            pass = coarse_pass<LAW>(0, 0, r_i, w.screen_r[mj], orad_i, w.screen_r[mj], pi, pj,
+                                    off);
+          if (!pass) continue;
+          if (nlist >= K) {
+            st |= ST_CAPACITY;
+            continue;
+          }
+          const int id_j = w.id_of[mj];
+          int oslot = kNoOldSlot;
+          for (int z = 0; z < nold; ++z)
+            if (old.partner[(size_t)z * n + m] == id_j) oslot = z;
+          list_mj[nlist] = mj;
+          list_code[nlist] = kind | (nlist << 8) | (oslot << 16);
+          ++nlist;
         }
-        const int id_j = w.id_of[mj];
-        int oslot = kNoOldSlot;
-        for (int z = 0; z < nold; ++z)
-          if (old.partner[(size_t)z * n + m] == id_j) oslot = z;
-        list_mj[nlist] = mj;
-        list_code[nlist] = kind | (nlist << 8) | (oslot << 16);
-        ++nlist;
       }
       // old partners among the candidates
       for (int z = 0; z < nold; ++z) {
