@@ -295,6 +295,16 @@ int32_t xdem_reset_newton_stats(xdem_world w);
    geometry was evaluated) */
 int32_t xdem_get_pair_count(xdem_world w, int64_t* out);
 
+/* ---- observables ---------------------------------------------------------- */
+/* QuadronAnalysis's rattler-free coordination number and solid fraction
+   (QuadronAnalysis.cpp:663-668,980-986,144-165,703-713,724-732) on the
+   device, from the current contacts: particles without contacts leave, then
+   repeatedly the particles left with one contact, with it; out = {Z = 2 x
+   remaining contacts / remaining particles, remaining volume / box area}.
+   The batch form writes two values per system. */
+int32_t xdem_quadron_z_phi(xdem_world w, double out[2]);
+int32_t xdem_batch_quadron_z_phi(xdem_world w, double* out);
+
 /* ---- sub-steps (each one reference method) ----------------------------- */
 /* PeriodicBoundaryWorld::modifyParticlePosition (PeriodicBoundaryWorld.cpp:129-142)
    or LeesEdwardsBoundaryWorld::modifyParticlePosition (LeesEdwardsBoundaryWorld.cpp:304-333) */

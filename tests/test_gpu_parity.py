@@ -286,3 +286,18 @@ def test_stop_on_pressure():
     nc = c.run(2000, ctl)
     assert ng == nc and ng < 2000
     _compare_worlds(g, c, TRAJ_TOL)
+
+
+@pytest.mark.parametrize("kind", [abi.WORLD_PERIODIC, abi.WORLD_LEES_EDWARDS])
+def test_quadron_z_phi_on_device(kind):
+    """QuadronAnalysis's rattler-free Z and solid fraction computed on the
+    device equal the checker's (pinned to the compiled reference) after a run."""
+    p, prm = disc_case(n=600, phi=0.80, seed=23, kind=kind, shift_strain_rate=0.05)
+    g, c = _pair(p, prm)
+    ctl = make_control()
+    g.run(60, ctl)
+    c.run(60, ctl)
+    zg, zc = g.quadron_z_phi(), c.quadron_z_phi()
+    assert zc[0] > 0
+    assert zg[0] == zc[0]
+    assert abs(zg[1] - zc[1]) <= 1e-12 * zc[1]

@@ -15,6 +15,7 @@
 #include "pairs_mixed.cuh"
 #include "learned.cuh"
 #include "verlet.cuh"
+#include "analysis.cuh"
 #include "mlp_host.h"
 #include "resort.cuh"
 
@@ -1320,6 +1321,78 @@ int32_t xdem_get_warm_stats(xdem_world w, int64_t out[5]) {
   out[2] = (int64_t)s.warm_rejected;
   out[3] = (int64_t)s.warm_restarted;
   out[4] = (int64_t)s.logit_right;
+  return XDEM_OK;
+}
+
+// ---- rattler-free coordination number and solid fraction --------------------------
+namespace {
+int32_t core_z_phi(xdem_world_s* w, std::vector<double>& res) {
+  const int n = w->dw.n, K = w->dw.K;
+  const int nsys = w->nsys;
+  int32_t *deg = nullptr, *changed = nullptr;
+  uint8_t *active = nullptr, *leave = nullptr, *eact = nullptr;
+  double* out = nullptr;
+  cudaStream_t s = w->stream;
+  cudaError_t e = cudaMalloc(&deg, sizeof(int32_t) * n);
+  if (e == cudaSuccess) e = cudaMalloc(&changed, sizeof(int32_t));
+  if (e == cudaSuccess) e = cudaMalloc(&active, n);
+  if (e == cudaSuccess) e = cudaMalloc(&leave, n);
+  if (e == cudaSuccess) e = cudaMalloc(&eact, (size_t)K * n);
+  if (e == cudaSuccess) e = cudaMalloc(&out, sizeof(double) * 3 * nsys);
+  const int nb = blocks_for(n, kBlock);
+  if (e == cudaSuccess) e = cudaMemsetAsync(deg, 0, sizeof(int32_t) * n, s);
+  if (e == cudaSuccess) {
+    k_core_init<<<nb, kBlock, 0, s>>>(w->dw, w->par, deg, eact);
+    k_core_active<<<nb, kBlock, 0, s>>>(w->dw, deg, active);
+    e = cudaGetLastError();
+  }
+  // parallel rounds until no particle leaves (at most n rounds)
+  for (int round = 0; round <= n && e == cudaSuccess; ++round) {
+    int32_t h = 0;
+    e = cudaMemsetAsync(changed, 0, sizeof(int32_t), s);
+    if (e != cudaSuccess) break;
+    k_core_mark<<<nb, kBlock, 0, s>>>(w->dw, deg, active, leave, changed);
+    k_core_edges<<<nb, kBlock, 0, s>>>(w->dw, w->par, deg, leave, eact);
+    e = cudaMemcpyAsync(&h, changed, sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (h == 0) break;
+  }
+  if (e == cudaSuccess) {
+    k_core_sums<<<nsys, 256, 0, s>>>(w->dw, active, eact, out);
+    e = cudaGetLastError();
+  }
+  res.assign(3 * (size_t)nsys, 0.0);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(res.data(), out, sizeof(double) * 3 * nsys, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  cudaFree(deg);
+  cudaFree(changed);
+  cudaFree(active);
+  cudaFree(leave);
+  cudaFree(eact);
+  cudaFree(out);
+  return e == cudaSuccess ? XDEM_OK : (int32_t)cuda_check(w, e);
+}
+}  // namespace
+
+int32_t xdem_quadron_z_phi(xdem_world w, double out[2]) {
+  if (!w || !out || w->dw.n <= 0) return XDEM_ERR_ARGUMENT;
+  std::vector<double> r;
+  int32_t st = core_z_phi(w, r);
+  if (st) return st;
+  out[0] = r[0];
+  out[1] = r[1];
+  return XDEM_OK;
+}
+
+int32_t xdem_batch_quadron_z_phi(xdem_world w, double* out) {
+  if (!w || !out || w->dw.n <= 0) return XDEM_ERR_ARGUMENT;
+  std::vector<double> r;
+  int32_t st = core_z_phi(w, r);
+  if (st) return st;
+  for (int k = 0; k < w->nsys; ++k) {
+    out[2 * k] = r[3 * k];
+    out[2 * k + 1] = r[3 * k + 1];
+  }
   return XDEM_OK;
 }
 

@@ -237,6 +237,20 @@ class World(WorldBase):
         self._check(self.lib.xdem_batch_set_particles(self.h, nsys, arr, boxes.ctypes.data_as(d),
                                                       dts_p), "batch_set_particles")
 
+    def quadron_z_phi(self):
+        """Rattler-free (Z, solid fraction) as QuadronAnalysis computes them."""
+        out = np.zeros(2)
+        self._check(self.lib.xdem_quadron_z_phi(self.h, out.ctypes.data_as(C.POINTER(C.c_double))),
+                    "quadron_z_phi")
+        return out
+
+    def batch_quadron_z_phi(self):
+        k, _ = self.batch_info()
+        out = np.zeros((k, 2))
+        self._check(self.lib.xdem_batch_quadron_z_phi(
+            self.h, out.ctypes.data_as(C.POINTER(C.c_double))), "batch_quadron_z_phi")
+        return out
+
     def batch_info(self):
         """(number of systems, first id of each system followed by n)"""
         k = C.c_int32(0)
