@@ -295,6 +295,19 @@ int32_t xdem_reset_newton_stats(xdem_world w);
    geometry was evaluated) */
 int32_t xdem_get_pair_count(xdem_world w, int64_t* out);
 
+/* ---- binary snapshots ----------------------------------------------------- */
+/* Checkpoint and resume (the reference writes text files,
+   BaseParticle.cpp:158-186, ContactInformation.h:51-60, and reads particles
+   back with read4File_particle): the whole world — every system's box, time
+   step, contact model, Lees-Edwards and box-law state, every particle field
+   and the full contact history — in one binary file, so that a loaded world
+   continues exactly as the saved one would have.  Loading needs a world of
+   the same kind (its precision, ellipse law and slot count stay its own) and
+   replaces its particles, contacts and scalars; the file is tied to the
+   library's build (native byte order, structure sizes checked). */
+int32_t xdem_save_snapshot(xdem_world w, const char* path);
+int32_t xdem_load_snapshot(xdem_world w, const char* path);
+
 /* ---- observables ---------------------------------------------------------- */
 /* QuadronAnalysis's rattler-free coordination number and solid fraction
    (QuadronAnalysis.cpp:663-668,980-986,144-165,703-713,724-732) on the

@@ -185,6 +185,8 @@ def load_library(path=LIB_PATH):
         "xdem_set_particles": (C.c_int32, [W, P(Particles)]),
         "xdem_batch_set_particles": (C.c_int32, [W, C.c_int32, P(Particles), _d, _d]),
         "xdem_quadron_z_phi": (C.c_int32, [W, _d]),
+        "xdem_save_snapshot": (C.c_int32, [W, C.c_char_p]),
+        "xdem_load_snapshot": (C.c_int32, [W, C.c_char_p]),
         "xdem_batch_quadron_z_phi": (C.c_int32, [W, _d]),
         "xdem_batch_info": (C.c_int32, [W, P(C.c_int32), P(C.c_int32)]),
         "xdem_batch_get_stress": (C.c_int32, [W, _d]),

@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdint>
 #include <cstring>
 #include <new>
 #include <vector>
@@ -1321,6 +1322,269 @@ int32_t xdem_get_warm_stats(xdem_world w, int64_t out[5]) {
   out[2] = (int64_t)s.warm_rejected;
   out[3] = (int64_t)s.warm_restarted;
   out[4] = (int64_t)s.logit_right;
+  return XDEM_OK;
+}
+
+// ---- binary snapshots ---------------------------------------------------------------
+}  // extern "C"
+namespace {
+
+// file layout (native byte order): SnapHeader, nsys WorldScalars, the
+// particles in id order (5 int32 arrays, then 16 double arrays), the memory
+// order (the id at each memory position), the contacts (id_i, id_j, then 19
+// double arrays, in xdem_contacts field order).  The memory order and the
+// steps since the last re-sort come along because block sums (the stress)
+// run in memory order: with both restored, a loaded world repeats the saved
+// one bit for bit.
+struct SnapHeader {
+  char magic[8];
+  uint32_t version, nsys;
+  int32_t n, K;
+  int64_t ncontacts;
+  uint32_t scalars_bytes, params_bytes;
+  int32_t since_resort, pad_;
+  xdem_params prm;
+};
+constexpr char kSnapMagic[8] = {'X', 'D', 'E', 'M', 'S', 'N', 'P', '1'};
+
+struct FileCloser {
+  FILE* f;
+  ~FileCloser() {
+    if (f) fclose(f);
+  }
+};
+
+template <class T>
+bool put(FILE* f, const T* p, size_t count) {
+  return fwrite(p, sizeof(T), count, f) == count;
+}
+template <class T>
+bool get(FILE* f, T* p, size_t count) {
+  return fread(p, sizeof(T), count, f) == count;
+}
+
+// a device array in memory order, downloaded in id order
+template <class T>
+cudaError_t by_id(xdem_world_s* w, const T* src, const std::vector<int32_t>& id_of, std::vector<T>& out) {
+  out.resize(w->dw.n);
+  return download_by_id(w, out.data(), src, id_of);
+}
+
+}  // namespace
+extern "C" {
+
+int32_t xdem_save_snapshot(xdem_world w, const char* path) {
+  if (!w || !path || w->dw.n <= 0) return XDEM_ERR_ARGUMENT;
+  const int n = w->dw.n;
+  const DevWorld& d = w->dw;
+  std::vector<WorldScalars> all(w->nsys);
+  CK(w, cudaMemcpyAsync(all.data(), w->ws, sizeof(WorldScalars) * w->nsys, cudaMemcpyDeviceToHost,
+                        w->stream));
+  CK(w, cudaStreamSynchronize(w->stream));
+  std::vector<int32_t> id_of;
+  CK(w, fetch_id_of(w, id_of));
+  // particles
+  std::vector<int32_t> ints[5];
+  const int32_t* isrc[5] = {d.shape, d.up, d.setting, d.rattler, d.num_sub};
+  for (int k = 0; k < 5; ++k) CK(w, by_id(w, isrc[k], id_of, ints[k]));
+  std::vector<double> dbl[16];
+  std::vector<double2> v2;
+  CK(w, by_id(w, d.pos, id_of, v2));
+  dbl[3].resize(n);
+  dbl[4].resize(n);
+  for (int i = 0; i < n; ++i) {
+    dbl[3][i] = v2[i].x;
+    dbl[4][i] = v2[i].y;
+  }
+  CK(w, by_id(w, d.vel, id_of, v2));
+  dbl[5].resize(n);
+  dbl[6].resize(n);
+  for (int i = 0; i < n; ++i) {
+    dbl[5][i] = v2[i].x;
+    dbl[6][i] = v2[i].y;
+  }
+  CK(w, by_id(w, d.branch, id_of, v2));
+  dbl[14].resize(n);
+  dbl[15].resize(n);
+  for (int i = 0; i < n; ++i) {
+    dbl[14][i] = v2[i].x;
+    dbl[15][i] = v2[i].y;
+  }
+  const double* dsrc[16] = {d.orad, d.rad, d.asp, nullptr, nullptr, nullptr, nullptr, d.rot,
+                            d.w,    d.vol, d.mass, d.im,   d.I,     d.iI,    nullptr, nullptr};
+  for (int k = 0; k < 16; ++k)
+    if (dsrc[k]) CK(w, by_id(w, dsrc[k], id_of, dbl[k]));
+  // contacts
+  xdem_contacts c{};
+  c.capacity = 0;
+  int32_t st = xdem_get_contacts(w, &c);
+  if (st && st != XDEM_ERR_CAPACITY) return st;
+  const int64_t nc = c.count;
+  std::vector<int32_t> ci(nc), cj(nc);
+  std::vector<std::vector<double>> cd(19, std::vector<double>(nc));
+  c.capacity = nc;
+  c.id_i = ci.data();
+  c.id_j = cj.data();
+  double** fields[19] = {&c.normal_x, &c.normal_y, &c.point_x, &c.point_y, &c.branch_x,
+                         &c.branch_y, &c.bv1_x,    &c.bv1_y,   &c.bv2_x,   &c.bv2_y,
+                         &c.shear_x,  &c.shear_y,  &c.fn_x,    &c.fn_y,    &c.ft_x,
+                         &c.ft_y,     &c.torque_i, &c.torque_j, &c.damping};
+  for (int k = 0; k < 19; ++k) *fields[k] = cd[k].data();
+  if (nc > 0) {
+    st = xdem_get_contacts(w, &c);
+    if (st) return st;
+  }
+  FileCloser fc{fopen(path, "wb")};
+  if (!fc.f) return XDEM_ERR_ARGUMENT;
+  SnapHeader h{};
+  std::memcpy(h.magic, kSnapMagic, 8);
+  h.version = 1;
+  h.nsys = (uint32_t)w->nsys;
+  h.n = n;
+  h.K = d.K;
+  h.ncontacts = nc;
+  h.scalars_bytes = sizeof(WorldScalars);
+  h.params_bytes = sizeof(xdem_params);
+  h.since_resort = w->since_resort;
+  h.prm = w->prm;
+  bool ok = put(fc.f, &h, 1) && put(fc.f, all.data(), all.size());
+  for (int k = 0; k < 5 && ok; ++k) ok = put(fc.f, ints[k].data(), n);
+  for (int k = 0; k < 16 && ok; ++k) ok = put(fc.f, dbl[k].data(), n);
+  ok = ok && put(fc.f, id_of.data(), n);
+  ok = ok && put(fc.f, ci.data(), nc) && put(fc.f, cj.data(), nc);
+  for (int k = 0; k < 19 && ok; ++k) ok = put(fc.f, cd[k].data(), nc);
+  return ok ? XDEM_OK : XDEM_ERR_ARGUMENT;
+}
+
+int32_t xdem_load_snapshot(xdem_world w, const char* path) {
+  if (!w || !path) return XDEM_ERR_ARGUMENT;
+  FileCloser fc{fopen(path, "rb")};
+  if (!fc.f) return XDEM_ERR_ARGUMENT;
+  SnapHeader h{};
+  if (!get(fc.f, &h, 1) || std::memcmp(h.magic, kSnapMagic, 8) != 0 || h.version != 1 ||
+      h.scalars_bytes != sizeof(WorldScalars) || h.params_bytes != sizeof(xdem_params) ||
+      h.n <= 0 || h.nsys == 0 || h.ncontacts < 0 || h.prm.world_kind != w->prm.world_kind)
+    return XDEM_ERR_ARGUMENT;
+  const int n = h.n;
+  const int nsys = (int)h.nsys;
+  std::vector<WorldScalars> all(nsys);
+  std::vector<int32_t> ints[5];
+  std::vector<double> dbl[16];
+  bool ok = get(fc.f, all.data(), nsys);
+  for (int k = 0; k < 5 && ok; ++k) {
+    ints[k].resize(n);
+    ok = get(fc.f, ints[k].data(), n);
+  }
+  for (int k = 0; k < 16 && ok; ++k) {
+    dbl[k].resize(n);
+    ok = get(fc.f, dbl[k].data(), n);
+  }
+  std::vector<int32_t> mem_id(n);
+  ok = ok && get(fc.f, mem_id.data(), n);
+  const int64_t nc = h.ncontacts;
+  std::vector<int32_t> ci(nc), cj(nc);
+  std::vector<std::vector<double>> cd(19, std::vector<double>(nc));
+  ok = ok && get(fc.f, ci.data(), nc) && get(fc.f, cj.data(), nc);
+  for (int k = 0; k < 19 && ok; ++k) ok = get(fc.f, cd[k].data(), nc);
+  if (!ok) return XDEM_ERR_ARGUMENT;
+  // the particles (the snapshot's contact-model and run settings are restored
+  // below; its precision, ellipse law and slot count are the world's own)
+  w->prm.dt = h.prm.dt;
+  xdem_particles P{};
+  P.n = n;
+  P.shape = ints[0].data();
+  P.up_level = ints[1].data();
+  P.setting = ints[2].data();
+  P.is_rattler = ints[3].data();
+  P.num_sub = ints[4].data();
+  P.outer_radius = dbl[0].data();
+  P.radius = dbl[1].data();
+  P.aspect_ratio = dbl[2].data();
+  P.x = dbl[3].data();
+  P.y = dbl[4].data();
+  P.vx = dbl[5].data();
+  P.vy = dbl[6].data();
+  P.rot = dbl[7].data();
+  P.rot_vel = dbl[8].data();
+  P.volume = dbl[9].data();
+  P.mass = dbl[10].data();
+  P.inv_mass = dbl[11].data();
+  P.inertia = dbl[12].data();
+  P.inv_inertia = dbl[13].data();
+  P.branch_x = dbl[14].data();
+  P.branch_y = dbl[15].data();
+  std::vector<SysDesc> sys(nsys);
+  for (int k = 0; k < nsys; ++k) {
+    sys[k].first = all[k].first;
+    sys[k].count = all[k].count;
+    sys[k].box[0] = all[k].xmin;
+    sys[k].box[1] = all[k].xmax;
+    sys[k].box[2] = all[k].ymin;
+    sys[k].box[3] = all[k].ymax;
+    sys[k].dt = all[k].dt;
+  }
+  // the memory order: a permutation keeping every system in its id range
+  std::vector<int32_t> newpos(n, -1);
+  for (int k = 0; k < nsys; ++k)
+    for (int m = sys[k].first; m < sys[k].first + sys[k].count; ++m) {
+      const int id = mem_id[m];
+      if (id < sys[k].first || id >= sys[k].first + sys[k].count || newpos[id] >= 0)
+        return XDEM_ERR_ARGUMENT;
+      newpos[id] = m;
+    }
+  int32_t st = set_particles_impl(w, &P, sys);
+  if (st) return st;
+  // set_particles leaves memory order = id order: move every particle array
+  // to the saved order (the history is uploaded afterwards, into that order)
+  CK(w, upload(w->dw.newpos, newpos.data(), n, w->stream));
+  k_permute<<<blocks_for(n, kBlock), kBlock, 0, w->stream>>>(w->dw, w->perm);
+  CK(w, cudaGetLastError());
+  k_copy_back<<<blocks_for(n, kBlock), kBlock, 0, w->stream>>>(w->dw, w->perm);
+  CK(w, cudaGetLastError());
+  w->since_resort = std::max(0, std::min(h.since_resort, kResortEvery));
+  // the world scalars of every system: box, time step, contact model,
+  // Lees-Edwards and box-law state, the last stress
+  CK(w, modify_all(w, [&](WorldScalars& s, int k) {
+       const WorldScalars& o = all[k];
+       s.xmin = o.xmin;
+       s.xmax = o.xmax;
+       s.ymin = o.ymin;
+       s.ymax = o.ymax;
+       s.xlen = o.xlen;
+       s.ylen = o.ylen;
+       s.shift = o.shift;
+       s.shift_vel = o.shift_vel;
+       s.strain = o.strain;
+       s.shift_rate = o.shift_rate;
+       s.velX = o.velX;
+       s.velY = o.velY;
+       s.vmass = o.vmass;
+       s.max_strain_rate = o.max_strain_rate;
+       for (int c = 0; c < 4; ++c) s.stress[c] = o.stress[c];
+       s.scale_x = o.scale_x;
+       s.scale_y = o.scale_y;
+       s.ke = o.ke;
+       s.dt = o.dt;
+       s.g = o.g;
+       s.kn = o.kn;
+       s.kt = o.kt;
+       s.mu = o.mu;
+       s.factor = o.factor;
+     }));
+  if (nc > 0) {
+    xdem_contacts c{};
+    c.count = nc;
+    c.capacity = nc;
+    c.id_i = ci.data();
+    c.id_j = cj.data();
+    double** fields[19] = {&c.normal_x, &c.normal_y, &c.point_x, &c.point_y, &c.branch_x,
+                           &c.branch_y, &c.bv1_x,    &c.bv1_y,   &c.bv2_x,   &c.bv2_y,
+                           &c.shear_x,  &c.shear_y,  &c.fn_x,    &c.fn_y,    &c.ft_x,
+                           &c.ft_y,     &c.torque_i, &c.torque_j, &c.damping};
+    for (int k = 0; k < 19; ++k) *fields[k] = cd[k].data();
+    st = xdem_set_contacts(w, &c);
+    if (st) return st;
+  }
   return XDEM_OK;
 }
 

@@ -237,6 +237,17 @@ class World(WorldBase):
         self._check(self.lib.xdem_batch_set_particles(self.h, nsys, arr, boxes.ctypes.data_as(d),
                                                       dts_p), "batch_set_particles")
 
+    def save_snapshot(self, path):
+        """Writes the whole world (particles, contact history, scalars) to a
+        binary file."""
+        self._check(self.lib.xdem_save_snapshot(self.h, str(path).encode()), "save_snapshot")
+
+    def load_snapshot(self, path):
+        """Replaces this world's state with a saved one (same world kind)."""
+        self._check(self.lib.xdem_load_snapshot(self.h, str(path).encode()), "load_snapshot")
+        k, first = self.batch_info()
+        self.n = int(first[-1])
+
     def quadron_z_phi(self):
         """Rattler-free (Z, solid fraction) as QuadronAnalysis computes them."""
         out = np.zeros(2)
