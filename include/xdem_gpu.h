@@ -66,11 +66,17 @@ enum xdem_world_kind {
 };
 
 /* Particle shapes: CircularParticle.h:10, EllipticParticle.h:10,
-   GluedParticle.h:5 */
+   GluedParticle.h:5, SegmentObject.h:13.  A segment is a fixed wall between
+   two vertices (xdem_particles.seg_*): radius = outer_radius = half its
+   length, (x, y) = the vertices' midpoint, rot = the direction's angle, and
+   SKIP_TIME_INTEGRAL set, as the reference constructor leaves them
+   (SegmentObject.h:24-40).  Segments touch circles only; a segment meeting an
+   ellipse raises XDEM_ERR_UNSUPPORTED_PAIR (the reference exits). */
 enum xdem_shape {
   XDEM_SHAPE_CIRCLE = 0,
   XDEM_SHAPE_ELLIPSE = 1,
-  XDEM_SHAPE_CLUMP = 2
+  XDEM_SHAPE_CLUMP = 2,
+  XDEM_SHAPE_SEGMENT = 3
 };
 
 /* SETTING bit flags, same values as BaseParticle.h:19-24 */
@@ -152,7 +158,8 @@ typedef struct xdem_control {
 } xdem_control;
 
 /* Particle arrays (length n).  For xdem_set_particles every pointer must be
-   non-NULL except num_sub/branch_x/branch_y (NULL = no clumps) and
+   non-NULL except num_sub/branch_x/branch_y (NULL = no clumps), seg_* (NULL =
+   no segments) and
    is_rattler (NULL = all rattlers, as before the first collect).  For
    xdem_get_particles, NULL pointers are skipped. */
 typedef struct xdem_particles {
@@ -165,6 +172,9 @@ typedef struct xdem_particles {
   double *volume, *mass, *inv_mass, *inertia, *inv_inertia;
   int32_t *num_sub;          /* clump: number of sub-particles whose ids follow it */
   double *branch_x, *branch_y; /* sub-particle: GluedParticle::_branchVectors entry */
+  /* segment: SegmentObject::_vertex1, _vertex2 (NULL when there are no
+     segments; entries of other shapes are ignored) */
+  double *seg_x1, *seg_y1, *seg_x2, *seg_y2;
 } xdem_particles;
 
 /* Contact records, sorted by (id_i, id_j); the fields of ContactInformation
@@ -508,8 +518,9 @@ int64_t xdem_total_stress_noalloc_max_contacts(void);
 int32_t xdem_rsa_positions(int32_t n, const double* radius, const double box[4], uint64_t seed,
                            int64_t max_attempts, double* x, double* y);
 
-/* CircularParticle/EllipticParticle::calculateParticleProperties(density)
-   (CircularParticle.cpp:16-23, EllipticParticle.cpp:7-14) */
+/* CircularParticle/EllipticParticle/SegmentObject::calculateParticleProperties
+   (density) (CircularParticle.cpp:16-23, EllipticParticle.cpp:7-14,
+   SegmentObject.cpp:4-10; a segment's radius is half its length) */
 int32_t xdem_particle_properties(int32_t n, const int32_t* shape, const double* radius,
                                  const double* aspect_ratio, double density, double* volume,
                                  double* mass, double* inv_mass, double* inertia,

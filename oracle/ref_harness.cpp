@@ -119,15 +119,21 @@ void* refh_create(const xdem_params* prm, int32_t num_threads) {
 
 void refh_destroy(void* hp) { delete static_cast<Harness*>(hp); }
 
-// calculateParticleProperties(density) for circles/ellipses
-// (CircularParticle.cpp:16-23, EllipticParticle.cpp:7-14).
+// calculateParticleProperties(density) for circles/ellipses/segments
+// (CircularParticle.cpp:16-23, EllipticParticle.cpp:7-14,
+// SegmentObject.cpp:4-10); a segment of radius r spans (-r, 0)..(r, 0).
 void refh_particle_properties(int32_t n, const int32_t* shape, const double* radius,
                               const double* aspect, double density, double* volume,
                               double* mass, double* inv_mass, double* inertia,
                               double* inv_inertia) {
   ContactModel m;
   for (int i = 0; i < n; ++i) {
-    auto p = make_particle(shape[i], 0, i, radius[i], aspect[i], 0, 0, 0, 0, 0, 0, &m);
+    std::unique_ptr<BaseParticle> p;
+    if (shape[i] == XDEM_SHAPE_SEGMENT)
+      p.reset(new SegmentObject(i, vector2d(-radius[i], 0.0), vector2d(radius[i], 0.0),
+                                vector2d(0.0, 0.0), 0.0, &m));
+    else
+      p = make_particle(shape[i], 0, i, radius[i], aspect[i], 0, 0, 0, 0, 0, 0, &m);
     p->calculateParticleProperties(density);
     volume[i] = p->_volume;
     mass[i] = p->_mass;
@@ -175,9 +181,18 @@ int32_t refh_set_particles(void* hp, const xdem_particles* P) {
   h->handlers.clear();
   ContactModel* m = h->model.get();
   for (int i = 0; i < P->n; ++i) {
-    auto p = make_particle(P->shape[i], h->prm.ellipse_method, i, P->radius[i],
-                           P->aspect_ratio[i], P->x[i], P->y[i], P->vx[i], P->vy[i], P->rot[i],
-                           P->rot_vel[i], m);
+    std::unique_ptr<BaseParticle> p;
+    if (P->shape[i] == XDEM_SHAPE_SEGMENT) {
+      // the wall constructor derives position, radii, rotation and direction
+      // from the vertices (SegmentObject.h:24-40)
+      if (!P->seg_x1 || !P->seg_y1 || !P->seg_x2 || !P->seg_y2) return XDEM_ERR_ARGUMENT;
+      p.reset(new SegmentObject(i, vector2d(P->seg_x1[i], P->seg_y1[i]),
+                                vector2d(P->seg_x2[i], P->seg_y2[i]),
+                                vector2d(P->vx[i], P->vy[i]), P->rot_vel[i], m));
+    } else {
+      p = make_particle(P->shape[i], h->prm.ellipse_method, i, P->radius[i], P->aspect_ratio[i],
+                        P->x[i], P->y[i], P->vx[i], P->vy[i], P->rot[i], P->rot_vel[i], m);
+    }
     p->_upLevel = P->up_level[i];
     p->_setting = static_cast<SETTING>(P->setting[i]);
     p->_outerRadius = P->outer_radius[i];
@@ -249,6 +264,12 @@ int32_t refh_get_particles(void* hp, xdem_particles* P) {
     if (P->branch_x || P->branch_y) {
       if (P->branch_x) P->branch_x[i] = 0.0;
       if (P->branch_y) P->branch_y[i] = 0.0;
+    }
+    if (SegmentObject* s = dynamic_cast<SegmentObject*>(p)) {
+      if (P->seg_x1) P->seg_x1[i] = s->_vertex1.x();
+      if (P->seg_y1) P->seg_y1[i] = s->_vertex1.y();
+      if (P->seg_x2) P->seg_x2[i] = s->_vertex2.x();
+      if (P->seg_y2) P->seg_y2[i] = s->_vertex2.y();
     }
   }
   if (P->branch_x || P->branch_y) {

@@ -97,6 +97,7 @@ typedef struct {
 typedef struct {
   int shape;
   double r, asp, x, y, vx, vy, rot, w;
+  v2 s1, s2; /* segment: _vertex1, _vertex2 */
 } pstate_t;
 
 /* BaseParticle::calculateRelativeVelocityAtContactPoint (BaseParticle.cpp:11-25) */
@@ -433,14 +434,76 @@ static int ellipse_intersection(const pstate_t* A_, const pstate_t* B_, v2 off, 
   if (!isfinite(g->overlap)) { g->contacted = 0; return 0; }
   return 1;
 }
+/* SegmentObject::_dirVector = (v2 - v1).getUnitVector() (SegmentObject.h:37,
+   MathVector.h:169-178) */
+static v2 seg_dir(const pstate_t* s) { return vunit(vsub(s->s2, s->s1)); }
+
+/* the point of the segment nearest to q along its direction: a vertex beyond
+   either end, else the projection (SegmentObject.cpp:51-62,
+   CircularParticle.cpp:99-108) */
+static v2 seg_ref(const pstate_t* s, v2 dir, double proj) {
+  if (proj > s->r) return s->s2;
+  if (proj < -s->r) return s->s1;
+  return vadd(V(s->x, s->y), vmul(dir, proj));
+}
+
+/* CircularParticle::contactWithSegmentObject (CircularParticle.cpp:94-129):
+   the circle is P1.  The reference adds the offset to the circle's own
+   position when projecting and again to the reference point (the segment's
+   image would take the offset once); restated as written. */
+static int circle_segment(const pstate_t* a, const pstate_t* b, v2 off, v2 ovel, geom_t* g) {
+  v2 dir = seg_dir(b);
+  double proj = vdot(vsub(vadd(V(a->x, a->y), off), V(b->x, b->y)), dir);
+  v2 ref = seg_ref(b, dir, proj);
+  v2 branch = vsub(vadd(ref, off), V(a->x, a->y));
+  double distance = vlen(branch);
+  double sumR = a->r;
+  g->overlap = sumR - distance;
+  if (g->overlap < 0.0) { g->contacted = 0; return 0; }
+  g->contacted = 1;
+  g->n = vunit(branch);
+  g->cp = ref;
+  g->bv1 = vsub(g->cp, V(a->x, a->y));
+  g->bv2 = vsub(g->cp, vadd(ref, off));
+  relative_velocity(a, b, ovel, g);
+  return 1;
+}
+
+/* SegmentObject::contactWithCircularParticle (SegmentObject.cpp:45-80): the
+   segment is P1; its branch vector to the contact point is zero. */
+static int segment_circle(const pstate_t* a, const pstate_t* b, v2 off, v2 ovel, geom_t* g) {
+  v2 dir = seg_dir(a);
+  v2 pb = vadd(V(b->x, b->y), off);
+  double proj = vdot(vsub(pb, V(a->x, a->y)), dir);
+  v2 ref = seg_ref(a, dir, proj);
+  v2 branch = vsub(pb, ref);
+  double distance = vlen(branch);
+  double sumR = b->r;
+  g->overlap = sumR - distance;
+  if (g->overlap < 0.0) { g->contacted = 0; return 0; }
+  g->contacted = 1;
+  g->n = vunit(branch);
+  g->cp = ref;
+  g->bv1 = vsub(g->cp, ref);
+  g->bv2 = vsub(g->cp, pb);
+  relative_velocity(a, b, ovel, g);
+  return 1;
+}
 
 /* BaseParticle::calculateContactGeometry dispatch (CircularParticle.cpp:25-40,
-   EllipticParticle.cpp:16-32, GluedParticle.cpp:133-140) */
+   EllipticParticle.cpp:16-32, GluedParticle.cpp:133-140,
+   SegmentObject.cpp:12-27) */
 static int contact_geometry(int method, const pstate_t* a, const pstate_t* b, double orad_a,
                             double orad_b, v2 off, v2 ovel, geom_t* g, uint32_t* st) {
   memset(g, 0, sizeof(*g));
   if (a->shape == XDEM_SHAPE_CLUMP || b->shape == XDEM_SHAPE_CLUMP) return 0;
+  if (a->shape == XDEM_SHAPE_SEGMENT) {
+    if (b->shape == XDEM_SHAPE_SEGMENT) return 0;
+    if (b->shape != XDEM_SHAPE_CIRCLE) { *st |= XDEM_ERR_UNSUPPORTED_PAIR; return 0; }
+    return segment_circle(a, b, off, ovel, g);
+  }
   if (a->shape == XDEM_SHAPE_CIRCLE) {
+    if (b->shape == XDEM_SHAPE_SEGMENT) return circle_segment(a, b, off, ovel, g);
     if (b->shape != XDEM_SHAPE_CIRCLE) { *st |= XDEM_ERR_UNSUPPORTED_PAIR; return 0; }
     return circle_circle(a, b, off, ovel, g);
   }
@@ -458,8 +521,8 @@ int32_t xo_pair_geometry(int32_t npairs, int32_t method, const double* pi, const
   for (int k = 0; k < npairs; ++k) {
     const double* a = pi + 9 * k;
     const double* b = pj + 9 * k;
-    pstate_t A = {(int)a[0], a[1], a[2], a[3], a[4], a[5], a[6], a[7], a[8]};
-    pstate_t B = {(int)b[0], b[1], b[2], b[3], b[4], b[5], b[6], b[7], b[8]};
+    pstate_t A = {(int)a[0], a[1], a[2], a[3], a[4], a[5], a[6], a[7], a[8], {0, 0}, {0, 0}};
+    pstate_t B = {(int)b[0], b[1], b[2], b[3], b[4], b[5], b[6], b[7], b[8], {0, 0}, {0, 0}};
     geom_t g;
     int c = contact_geometry(method, &A, &B, a[1], b[1], V(off[4 * k], off[4 * k + 1]),
                              V(off[4 * k + 2], off[4 * k + 3]), &g, &st);
@@ -492,6 +555,7 @@ struct xo_world {
   int n;
   int *shape, *up, *setting, *rattler, *num_sub;
   double *orad, *rad, *asp, *x, *y, *vx, *vy, *rot, *w, *vol, *m, *im, *I, *iI, *bx, *by;
+  double *s1x, *s1y, *s2x, *s2y; /* segment vertices (zero for other shapes) */
   /* contacts: CSR by owner, partners ascending */
   int64_t *cstart;
   contact_t* con;
@@ -539,7 +603,7 @@ static void free_particles(xo_world* w) {
   void* ps[] = {w->shape, w->up, w->setting, w->rattler, w->num_sub, w->orad, w->rad, w->asp,
                 w->x, w->y, w->vx, w->vy, w->rot, w->w, w->vol, w->m, w->im, w->I, w->iI,
                 w->bx, w->by, w->cstart, w->con, w->fx, w->fy, w->tq, w->ncp, w->cand_n,
-                w->cand, w->cand_kind};
+                w->cand, w->cand_kind, w->s1x, w->s1y, w->s2x, w->s2y};
   for (size_t k = 0; k < sizeof(ps) / sizeof(ps[0]); ++k) free(ps[k]);
 }
 
@@ -566,6 +630,7 @@ int32_t xo_set_particles(xo_world* w, const xdem_particles* P) {
   ALLOC(w->x, n); ALLOC(w->y, n); ALLOC(w->vx, n); ALLOC(w->vy, n); ALLOC(w->rot, n);
   ALLOC(w->w, n); ALLOC(w->vol, n); ALLOC(w->m, n); ALLOC(w->im, n); ALLOC(w->I, n);
   ALLOC(w->iI, n); ALLOC(w->bx, n); ALLOC(w->by, n);
+  ALLOC(w->s1x, n); ALLOC(w->s1y, n); ALLOC(w->s2x, n); ALLOC(w->s2y, n);
   ALLOC(w->cstart, n + 1); ALLOC(w->con, 1); w->ncon = 0;
   ALLOC(w->fx, n); ALLOC(w->fy, n); ALLOC(w->tq, n); ALLOC(w->ncp, n);
   ALLOC(w->cand_n, n); ALLOC(w->cand, (size_t)n * XO_CANDIDATE_CAP * 3);
@@ -582,6 +647,11 @@ int32_t xo_set_particles(xo_world* w, const xdem_particles* P) {
     w->I[i] = P->inertia[i]; w->iI[i] = P->inv_inertia[i];
     w->bx[i] = P->branch_x ? P->branch_x[i] : 0.0;
     w->by[i] = P->branch_y ? P->branch_y[i] : 0.0;
+    if (w->shape[i] == XDEM_SHAPE_SEGMENT) {
+      if (!P->seg_x1 || !P->seg_y1 || !P->seg_x2 || !P->seg_y2) return XDEM_ERR_ARGUMENT;
+      w->s1x[i] = P->seg_x1[i]; w->s1y[i] = P->seg_y1[i];
+      w->s2x[i] = P->seg_x2[i]; w->s2y[i] = P->seg_y2[i];
+    }
     /* updateMaximumParticleSize (BaseWorld.cpp:201-219) */
     if (w->orad[i] > maxr) maxr = w->orad[i];
     /* updateTotalParticleVolume (BaseWorld.cpp:188-199) */
@@ -606,6 +676,10 @@ int32_t xo_get_particles(xo_world* w, xdem_particles* P) {
     if (P->inertia) P->inertia[i] = w->I[i];
     if (P->branch_x) P->branch_x[i] = w->bx[i];
     if (P->branch_y) P->branch_y[i] = w->by[i];
+    if (P->seg_x1) P->seg_x1[i] = w->s1x[i];
+    if (P->seg_y1) P->seg_y1[i] = w->s1y[i];
+    if (P->seg_x2) P->seg_x2[i] = w->s2x[i];
+    if (P->seg_y2) P->seg_y2[i] = w->s2y[i];
   }
   return XDEM_OK;
 }
@@ -892,7 +966,8 @@ static void candidate_offset(const xo_world* w, int i, int j, int kind, v2* off,
 
 static inline pstate_t pstate(const xo_world* w, int i) {
   pstate_t p = {w->shape[i], w->rad[i], w->asp[i], w->x[i], w->y[i],
-                w->vx[i], w->vy[i], w->rot[i], w->w[i]};
+                w->vx[i], w->vy[i], w->rot[i], w->w[i],
+                {w->s1x[i], w->s1y[i]}, {w->s2x[i], w->s2y[i]}};
   return p;
 }
 

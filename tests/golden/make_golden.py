@@ -3,7 +3,9 @@
 oracle/ref_harness.cpp).  Run from the repository root where the reference
 sources were available at build time:
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [fixture names, e.g. world_discs_segments_periodic]
+
+(with names, only those fixtures are written)
 
 Every fixture holds seeded inputs and the reference's outputs:
   pairs_<law>.npz    single-pair contact geometry (BaseParticle::
@@ -27,7 +29,7 @@ sys.path.insert(0, os.path.dirname(HERE))
 import oracle  # noqa: E402
 from xdem_b200 import abi  # noqa: E402
 
-from helpers import clump_case, controls, disc_case, ellipse_case  # noqa: E402
+from helpers import clump_case, controls, disc_case, ellipse_case, segment_case  # noqa: E402
 
 
 def random_pairs(seed, N, shape, b_range, asp_range, near):
@@ -50,6 +52,13 @@ def random_pairs(seed, N, shape, b_range, asp_range, near):
     return pi, pj, off
 
 
+ONLY = set(sys.argv[1:])
+
+
+def wanted(name):
+    return not ONLY or name in ONLY
+
+
 def make_pairs():
     cases = {
         "circle": (0, 0, (0.3, 0.7), (1.0, 1.0), (0.8, 1.02)),
@@ -57,6 +66,8 @@ def make_pairs():
         "intersection": (1, abi.ELLIPSE_INTERSECTION, (0.4, 0.7), (1.0, 3.0), (0.5, 1.05)),
     }
     for name, (shape, method, br, ar, near) in cases.items():
+        if not wanted(f"pairs_{name}"):
+            continue
         pi, pj, off = random_pairs(1000 + len(name), 600, shape, br, ar, near)
         if shape == 1:
             pi[:40, 7] = pj[:40, 7] = 0.0
@@ -73,6 +84,8 @@ def make_pairs():
 
 
 def save_world(name, p, prm, ctl, nsteps, mass=None):
+    if not wanted(f"world_{name}"):
+        return
     w = oracle.RefWorld(prm)
     w.set_particles(p)
     if prm.world_kind == abi.WORLD_PERIODIC_CONTROL:
@@ -110,6 +123,10 @@ def make_worlds():
     save_world("ellipses_intersection_control_strain", p, prm, ctl["strain"], 20)
     p, prm = clump_case(nfree=60, nclump=15, seed=35)
     save_world("clumps_periodic", p, prm, ctl["stress"], 20)
+    p, prm = segment_case(n=220, seed=36)
+    save_world("discs_segments_periodic", p, prm, ctl["stress"], 25)
+    p, prm = segment_case(n=220, seed=37, kind=abi.WORLD_LEES_EDWARDS, shift_strain_rate=0.1)
+    save_world("discs_segments_lees_edwards", p, prm, ctl["stress"], 25)
 
 
 if __name__ == "__main__":

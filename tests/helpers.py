@@ -238,3 +238,77 @@ def dense_ellipse_case(n=3000, seed=21, kind=abi.WORLD_LEES_EDWARDS, phi=0.85, a
     prm = make_params(kind, dt, b, inputs.KN, inputs.KT, inputs.RESTITUTION, inputs.FRICTION,
                       shift_strain_rate=shift_rate if kind == abi.WORLD_LEES_EDWARDS else 0.0)
     return q, contacts, prm
+
+
+def _point_segment_nearest(px, py, x1, y1, x2, y2):
+    dx, dy = x2 - x1, y2 - y1
+    t = np.clip(((px - x1) * dx + (py - y1) * dy) / (dx * dx + dy * dy), 0.0, 1.0)
+    qx, qy = x1 + t * dx, y1 + t * dy
+    return np.hypot(px - qx, py - qy), qx, qy
+
+
+def _point_segment_distance(px, py, x1, y1, x2, y2):
+    return _point_segment_nearest(px, py, x1, y1, x2, y2)[0]
+
+
+def segment_case(n=400, phi=0.80, seed=31, kind=abi.WORLD_PERIODIC, nfront=3, vel_sigma=0.05,
+                 long_walls=False, **kw):
+    """Bidisperse discs with fixed wall segments: a horizontal chain inside the
+    box, a tilted chain, and single segments next to the periodic edges (their
+    pairs with discs across the edge are image pairs).  Discs near a segment
+    are moved out to an overlap of 10% of their radius, so that the first
+    steps start with many mild wall contacts.  The first `nfront` segments take the
+    lowest ids (they own their contacts, SegmentObject.cpp:45-80), the others
+    the highest (the discs own theirs, CircularParticle.cpp:94-129)."""
+    p, box = inputs.disc_system(n, phi=phi, seed=seed, vel_sigma=vel_sigma)
+    L = box[1] - box[0]
+    piece = 3.0 if long_walls else 1.2
+    xs = np.arange(-0.35 * L, 0.35 * L - piece, piece)
+    x1 = list(xs)
+    y1 = [0.1 * L] * len(xs)
+    x2 = list(xs + piece)
+    y2 = [0.1 * L] * len(xs)
+    ang = 0.6
+    for k in range(4):  # tilted chain
+        sx = -0.2 * L + k * piece * np.cos(ang)
+        sy = -0.3 * L + k * piece * np.sin(ang)
+        x1.append(sx)
+        y1.append(sy)
+        x2.append(sx + piece * np.cos(ang))
+        y2.append(sy + piece * np.sin(ang))
+    for (cx, cy, a) in ((box[1] - 0.3, 0.0, 1.4), (box[0] + 0.2, -0.25 * L, 0.3),
+                        (0.3 * L, box[3] - 0.25, 0.05), (-0.1 * L, box[2] + 0.3, 2.0)):
+        x1.append(cx - 0.5 * piece * np.cos(a))
+        y1.append(cy - 0.5 * piece * np.sin(a))
+        x2.append(cx + 0.5 * piece * np.cos(a))
+        y2.append(cy + 0.5 * piece * np.sin(a))
+    x1, y1, x2, y2 = (np.asarray(v, np.float64) for v in (x1, y1, x2, y2))
+    # discs closer than 0.9 r to a segment move out to 0.9 r (along the
+    # segment's normal when the centre lies on it); those still closer than
+    # 0.75 r to some segment afterwards are removed
+    for k in range(len(x1)):
+        d, qx, qy = _point_segment_nearest(p["x"], p["y"], x1[k], y1[k], x2[k], y2[k])
+        near = d < 0.9 * p["radius"]
+        ux, uy = p["x"] - qx, p["y"] - qy
+        nx, ny = -(y2[k] - y1[k]), x2[k] - x1[k]
+        nn = np.hypot(nx, ny)
+        tiny = d < 1e-9
+        ux = np.where(tiny, nx / nn, ux / np.maximum(d, 1e-300))
+        uy = np.where(tiny, ny / nn, uy / np.maximum(d, 1e-300))
+        p["x"] = np.where(near, qx + ux * 0.9 * p["radius"], p["x"])
+        p["y"] = np.where(near, qy + uy * 0.9 * p["radius"], p["y"])
+    keep = np.ones(len(p["x"]), bool)
+    for k in range(len(x1)):
+        d = _point_segment_distance(p["x"], p["y"], x1[k], y1[k], x2[k], y2[k])
+        keep &= d >= 0.75 * p["radius"]
+    discs = {k: np.ascontiguousarray(v[keep]) for k, v in p.items()}
+    discs["up_level"] = np.arange(int(keep.sum()), dtype=np.int32)
+    dt = inputs.time_step(discs)
+    seg = inputs.segments(x1, y1, x2, y2)
+    front = {k: v[:nfront] for k, v in seg.items()}
+    back = {k: v[nfront:] for k, v in seg.items()}
+    for part in (front, back):
+        part["up_level"] = np.arange(len(part["x"]), dtype=np.int32)
+    q = inputs.concatenate(front, discs, back)
+    prm = make_params(kind, dt, box, inputs.KN, inputs.KT, inputs.RESTITUTION, inputs.FRICTION, **kw)
+    return q, prm

@@ -18,7 +18,7 @@ import oracle
 from xdem_b200 import abi, inputs
 
 from helpers import (clump_case, compare_contacts, compare_states, controls, disc_case,
-                     ellipse_case, rel_err, same_pairs)
+                     ellipse_case, rel_err, same_pairs, segment_case)
 
 pytestmark = [pytest.mark.reference,
               pytest.mark.skipif(not oracle.ref_available(), reason="compiled reference absent")]
@@ -150,6 +150,40 @@ def test_clumps_trajectory():
     assert rel_err(r.getStress(), c.getStress()) <= 1e-10
 
 
+@pytest.mark.parametrize("kind", [abi.WORLD_PERIODIC, abi.WORLD_PERIODIC_CONTROL,
+                                  abi.WORLD_LEES_EDWARDS])
+def test_segments_one_step(kind):
+    """Disc-segment contacts of both orders (CircularParticle.cpp:94-129,
+    SegmentObject.cpp:45-80), image pairs included."""
+    p, prm = segment_case(kind=kind, seed=31, shift_strain_rate=0.05)
+    r, c = _worlds(p, prm)
+    r.takeTimeStep()
+    c.takeTimeStep()
+    cr = r.get_contacts()
+    seg = np.flatnonzero(p["shape"] == abi.SHAPE_SEGMENT)
+    first = np.isin(cr["id_i"], seg)
+    second = np.isin(cr["id_j"], seg)
+    assert first.sum() >= 2 and second.sum() >= 10
+    compare_contacts(cr, c.get_contacts(), 0.0)
+    compare_states(r.get_state(), c.get_state(), 1e-15)
+
+
+@pytest.mark.parametrize("name", ["stress", "strain"])
+def test_segments_trajectory(name):
+    kind = abi.WORLD_PERIODIC_CONTROL if name == "strain" else abi.WORLD_PERIODIC
+    p, prm = segment_case(kind=kind, seed=32, long_walls=(name == "stress"))
+    r, c = _worlds(p, prm)
+    ctl = controls()[name]
+    assert r.run(40, ctl) == c.run(40, ctl) == 40
+    compare_contacts(r.get_contacts(), c.get_contacts(), 1e-10)
+    sr, sc = r.get_state(), c.get_state()
+    compare_states(sr, sc, 1e-10)
+    seg = p["shape"] == abi.SHAPE_SEGMENT
+    for key in ("vx", "vy", "rot_vel"):  # walls never move (SKIP_TIME_INTEGRAL)
+        np.testing.assert_array_equal(sr[key][seg], p[key][seg])
+    assert rel_err(r.getStress(), c.getStress()) <= 1e-10
+
+
 def test_clump_properties_match_reference():
     """xdem_clump_properties restates GluedParticle::calculateParticleProperties."""
     import ctypes as C
@@ -181,6 +215,7 @@ def test_clump_properties_match_reference():
 def test_particle_properties_match_reference():
     rng = np.random.default_rng(4)
     shape = rng.integers(0, 2, 100).astype(np.int32)
+    shape[::7] = abi.SHAPE_SEGMENT
     r = rng.uniform(0.3, 1.5, 100)
     asp = np.where(shape == 1, rng.uniform(1, 3, 100), 1.0)
     a = inputs.particle_properties(shape, r, asp, 1.7)

@@ -28,7 +28,7 @@ STATUS_NAMES = {
 }
 
 WORLD_PERIODIC, WORLD_PERIODIC_CONTROL, WORLD_LEES_EDWARDS = 0, 1, 2
-SHAPE_CIRCLE, SHAPE_ELLIPSE, SHAPE_CLUMP = 0, 1, 2
+SHAPE_CIRCLE, SHAPE_ELLIPSE, SHAPE_CLUMP, SHAPE_SEGMENT = 0, 1, 2, 3
 SKIP_TIME_INTEGRAL, SKIP_CONTACT_DETECTION, SKIP_MACRO_SUM = 1, 2, 4
 ELLIPSE_CLOSEST_APPROACH, ELLIPSE_INTERSECTION = 0, 1
 PRECISION_FP64, PRECISION_MIXED = 0, 1
@@ -79,10 +79,14 @@ PARTICLE_DOUBLE_FIELDS = ("outer_radius", "radius", "aspect_ratio", "x", "y", "v
                           "rot_vel", "volume", "mass", "inv_mass", "inertia", "inv_inertia")
 
 
+SEGMENT_FIELDS = ("seg_x1", "seg_y1", "seg_x2", "seg_y2")
+
+
 class Particles(C.Structure):
     _fields_ = ([("n", C.c_int32)] + [(f, _i) for f in PARTICLE_INT_FIELDS]
                 + [(f, _d) for f in PARTICLE_DOUBLE_FIELDS]
-                + [("num_sub", _i), ("branch_x", _d), ("branch_y", _d)])
+                + [("num_sub", _i), ("branch_x", _d), ("branch_y", _d)]
+                + [(f, _d) for f in SEGMENT_FIELDS])
 
 
 CONTACT_DOUBLE_FIELDS = ("normal_x", "normal_y", "point_x", "point_y", "branch_x", "branch_y",
@@ -101,7 +105,8 @@ def _ptr(a, ctype):
 
 def particles_struct(p):
     """Particles struct over a dict of numpy arrays (kept alive by the caller).
-    Optional keys: is_rattler, num_sub, branch_x, branch_y."""
+    Optional keys: is_rattler, num_sub, branch_x, branch_y, seg_x1, seg_y1,
+    seg_x2, seg_y2."""
     s = Particles()
     n = len(p["x"])
     s.n = n
@@ -116,6 +121,10 @@ def particles_struct(p):
     for f, ct in (("num_sub", C.c_int32), ("branch_x", C.c_double), ("branch_y", C.c_double)):
         if f in p and p[f] is not None:
             setattr(s, f, _ptr(p[f], ct))
+    for f in SEGMENT_FIELDS:
+        if f in p and p[f] is not None:
+            assert p[f].dtype == np.float64 and p[f].flags.c_contiguous and len(p[f]) == n, f
+            setattr(s, f, _ptr(p[f], C.c_double))
     return s
 
 

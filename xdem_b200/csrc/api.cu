@@ -30,6 +30,9 @@ constexpr int kDefaultSlots = 24;
 // re-sort + kResortEvery steps) swaps the slot sets an even number of times
 constexpr int kResortEvery = 31;
 constexpr double kPi = 3.14159265358979323846;
+// screening radius of a wall segment: above any box size, and small enough
+// that the squared sum of two stays finite in FP32
+constexpr double kWallScreen = 1e18;
 
 inline int blocks_for(int n, int b) { return (n + b - 1) / b; }
 
@@ -563,7 +566,9 @@ int32_t set_particles_impl(xdem_world_s* w, const xdem_particles* P, const std::
     br[i] = make_double2(P->branch_x ? P->branch_x[i] : 0.0, P->branch_y ? P->branch_y[i] : 0.0);
     if (P->num_sub) ns[i] = P->num_sub[i];
     if (P->is_rattler) rat[i] = P->is_rattler[i];
-    if (P->shape[i] < 0 || P->shape[i] > 2) return XDEM_ERR_ARGUMENT;
+    if (P->shape[i] < 0 || P->shape[i] > 3) return XDEM_ERR_ARGUMENT;
+    if (P->shape[i] == XDEM_SHAPE_SEGMENT && (!P->seg_x1 || !P->seg_y1 || !P->seg_x2 || !P->seg_y2))
+      return XDEM_ERR_ARGUMENT;
     if (P->shape[i] == XDEM_SHAPE_CLUMP && (ns[i] < 0 || i + ns[i] >= n)) return XDEM_ERR_ARGUMENT;
   }
   // per system: largest outer radius (updateMaximumParticleSize,
@@ -614,12 +619,13 @@ int32_t set_particles_impl(xdem_world_s* w, const xdem_particles* P, const std::
   for (int k = 0; k < nsys; ++k)  // setVirtualBoundaryMass (PeriodicControlWorld.cpp:58-66)
     w->control_mass[k] = sys_mass[k] / ((double)sys[k].count * 10.0);
   // one contact law for the whole world when every non-clump body has one shape
-  bool any_circle = false, any_ellipse = false;
+  bool any_circle = false, any_ellipse = false, any_segment = false;
   for (int i = 0; i < n; ++i) {
     any_circle |= P->shape[i] == XDEM_SHAPE_CIRCLE;
     any_ellipse |= P->shape[i] == XDEM_SHAPE_ELLIPSE;
+    any_segment |= P->shape[i] == XDEM_SHAPE_SEGMENT;
   }
-  if (any_circle && any_ellipse) w->law = LAW_ANY;
+  if ((any_circle && any_ellipse) || any_segment) w->law = LAW_ANY;
   else if (any_ellipse)
     w->law = w->prm.ellipse_method == XDEM_ELLIPSE_INTERSECTION ? LAW_INTERSECTION : LAW_CLOSEST;
   else w->law = LAW_CIRCLE;
@@ -693,6 +699,26 @@ int32_t set_particles_impl(xdem_world_s* w, const xdem_particles* P, const std::
   CK(w, B.alloc(&d.cell_up, 2 * (size_t)n));
   CK(w, B.alloc(&d.cs, n));
   d.screen_r = w->law == LAW_CIRCLE ? d.rad : d.orad;
+  // wall segments: vertices by id, and a screening radius that passes every
+  // pair, so that a segment's candidates are all bodies of the neighbouring
+  // cells, as in the reference's cell search (its outer radius would not
+  // bound it once a box law has moved its midpoint but not its vertices)
+  d.seg = nullptr;
+  double* wall_screen = nullptr;
+  if (any_segment) {
+    std::vector<double4> sv(n, double4{0.0, 0.0, 0.0, 0.0});
+    std::vector<double> scr(P->outer_radius, P->outer_radius + n);
+    for (int i = 0; i < n; ++i)
+      if (P->shape[i] == XDEM_SHAPE_SEGMENT) {
+        sv[i] = double4{P->seg_x1[i], P->seg_y1[i], P->seg_x2[i], P->seg_y2[i]};
+        scr[i] = kWallScreen;
+      }
+    CK(w, B.alloc(&d.seg, n));
+    CK(w, upload(d.seg, sv.data(), n, s));
+    CK(w, B.alloc(&wall_screen, n));
+    CK(w, upload(wall_screen, scr.data(), n, s));
+    d.screen_r = wall_screen;
+  }
   CK(w, B.alloc(&d.pcell, n));
   CK(w, B.alloc(&d.prank, n));
   CK(w, B.alloc(&d.gcell, n));
@@ -792,6 +818,7 @@ int32_t set_particles_impl(xdem_world_s* w, const xdem_particles* P, const std::
   add(d.force, 16);
   add(d.pcell, 4);  // read by the candidate scan's history test after a re-sort
   add(d.gcell, 4);
+  if (wall_screen) add(wall_screen, 8);
   size_t off = 0;
   for (int a = 0; a < L.count; ++a) {
     L.offset[a] = off;
@@ -982,6 +1009,19 @@ int32_t xdem_get_particles(xdem_world w, xdem_particles* P) {
   if (P->shape) CK(w, download_by_id(w, P->shape, (const int32_t*)d.shape, id_of));
   if (P->setting) CK(w, download_by_id(w, P->setting, (const int32_t*)d.setting, id_of));
   if (P->up_level) CK(w, download_by_id(w, P->up_level, (const int32_t*)d.up, id_of));
+  if (P->seg_x1 || P->seg_y1 || P->seg_x2 || P->seg_y2) {
+    std::vector<double4> sv(n, double4{0.0, 0.0, 0.0, 0.0});
+    if (d.seg) {
+      CK(w, download(sv.data(), d.seg, n, w->stream));
+      CK(w, cudaStreamSynchronize(w->stream));
+    }
+    for (int i = 0; i < n; ++i) {
+      if (P->seg_x1) P->seg_x1[i] = sv[i].x;
+      if (P->seg_y1) P->seg_y1[i] = sv[i].y;
+      if (P->seg_x2) P->seg_x2[i] = sv[i].z;
+      if (P->seg_y2) P->seg_y2[i] = sv[i].w;
+    }
+  }
   P->n = n;
   for (int i = 0; i < n; ++i) {
     if (P->x) P->x[i] = pos[i].x;
@@ -1331,8 +1371,9 @@ namespace {
 
 // file layout (native byte order): SnapHeader, nsys WorldScalars, the
 // particles in id order (5 int32 arrays, then 16 double arrays), the memory
-// order (the id at each memory position), the contacts (id_i, id_j, then 19
-// double arrays, in xdem_contacts field order).  The memory order and the
+// order (the id at each memory position), the wall-segment vertices when
+// has_seg (4 double arrays by id), the contacts (id_i, id_j, then 19 double
+// arrays, in xdem_contacts field order).  The memory order and the
 // steps since the last re-sort come along because block sums (the stress)
 // run in memory order: with both restored, a loaded world repeats the saved
 // one bit for bit.
@@ -1342,7 +1383,7 @@ struct SnapHeader {
   int32_t n, K;
   int64_t ncontacts;
   uint32_t scalars_bytes, params_bytes;
-  int32_t since_resort, pad_;
+  int32_t since_resort, has_seg;
   xdem_params prm;
 };
 constexpr char kSnapMagic[8] = {'X', 'D', 'E', 'M', 'S', 'N', 'P', '1'};
@@ -1446,11 +1487,26 @@ int32_t xdem_save_snapshot(xdem_world w, const char* path) {
   h.scalars_bytes = sizeof(WorldScalars);
   h.params_bytes = sizeof(xdem_params);
   h.since_resort = w->since_resort;
+  h.has_seg = d.seg ? 1 : 0;
   h.prm = w->prm;
+  std::vector<double> segv[4];
+  if (d.seg) {
+    std::vector<double4> sv(n);
+    CK(w, download(sv.data(), d.seg, n, w->stream));
+    CK(w, cudaStreamSynchronize(w->stream));
+    for (int k = 0; k < 4; ++k) segv[k].resize(n);
+    for (int i = 0; i < n; ++i) {
+      segv[0][i] = sv[i].x;
+      segv[1][i] = sv[i].y;
+      segv[2][i] = sv[i].z;
+      segv[3][i] = sv[i].w;
+    }
+  }
   bool ok = put(fc.f, &h, 1) && put(fc.f, all.data(), all.size());
   for (int k = 0; k < 5 && ok; ++k) ok = put(fc.f, ints[k].data(), n);
   for (int k = 0; k < 16 && ok; ++k) ok = put(fc.f, dbl[k].data(), n);
   ok = ok && put(fc.f, id_of.data(), n);
+  for (int k = 0; k < 4 && ok && h.has_seg; ++k) ok = put(fc.f, segv[k].data(), n);
   ok = ok && put(fc.f, ci.data(), nc) && put(fc.f, cj.data(), nc);
   for (int k = 0; k < 19 && ok; ++k) ok = put(fc.f, cd[k].data(), nc);
   return ok ? XDEM_OK : XDEM_ERR_ARGUMENT;
@@ -1481,6 +1537,11 @@ int32_t xdem_load_snapshot(xdem_world w, const char* path) {
   }
   std::vector<int32_t> mem_id(n);
   ok = ok && get(fc.f, mem_id.data(), n);
+  std::vector<double> segv[4];
+  for (int k = 0; k < 4 && ok && h.has_seg; ++k) {
+    segv[k].resize(n);
+    ok = get(fc.f, segv[k].data(), n);
+  }
   const int64_t nc = h.ncontacts;
   std::vector<int32_t> ci(nc), cj(nc);
   std::vector<std::vector<double>> cd(19, std::vector<double>(nc));
@@ -1513,6 +1574,12 @@ int32_t xdem_load_snapshot(xdem_world w, const char* path) {
   P.inv_inertia = dbl[13].data();
   P.branch_x = dbl[14].data();
   P.branch_y = dbl[15].data();
+  if (h.has_seg) {
+    P.seg_x1 = segv[0].data();
+    P.seg_y1 = segv[1].data();
+    P.seg_x2 = segv[2].data();
+    P.seg_y2 = segv[3].data();
+  }
   std::vector<SysDesc> sys(nsys);
   for (int k = 0; k < nsys; ++k) {
     sys[k].first = all[k].first;

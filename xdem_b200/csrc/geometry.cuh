@@ -24,7 +24,7 @@ enum : uint32_t {
   ST_GRID = 1u << 7
 };
 
-enum : int { SHAPE_CIRCLE = 0, SHAPE_ELLIPSE = 1, SHAPE_CLUMP = 2 };
+enum : int { SHAPE_CIRCLE = 0, SHAPE_ELLIPSE = 1, SHAPE_CLUMP = 2, SHAPE_SEGMENT = 3 };
 enum : int { ELLIPSE_CLOSEST = 0, ELLIPSE_INTERSECTION = 1 };
 
 struct PState {
@@ -72,6 +72,72 @@ __device__ __forceinline__ bool circle_circle(const PState& a, const PState& b, 
   vec2<double> p2 = pb - g.n * b.r;
   g.cp = (p1 + p2) / 2.0;
   g.bv1 = g.cp - pa;
+  g.bv2 = g.cp - pb;
+  relative_velocity(a, b, ovel, g);
+  return true;
+}
+
+// A fixed wall segment (SegmentObject.h:13-41): its vertices come as
+// (x1, y1, x2, y2); PState holds its (possibly moved) position and its radius
+// (half the vertex distance).  _dirVector = (v2 - v1).getUnitVector().
+__device__ __forceinline__ vec2<double> seg_dir(double4 s) { return unit(V(s.z, s.w) - V(s.x, s.y)); }
+
+// the segment's point of reference for a projection: a vertex beyond either
+// end, else the projection itself (SegmentObject.cpp:51-62,
+// CircularParticle.cpp:99-108)
+__device__ __forceinline__ vec2<double> seg_ref(const PState& s, double4 v, vec2<double> dir,
+                                                double proj) {
+  if (proj > s.r) return V(v.z, v.w);
+  if (proj < -s.r) return V(v.x, v.y);
+  return V(s.x, s.y) + dir * proj;
+}
+
+// CircularParticle::contactWithSegmentObject (CircularParticle.cpp:94-129),
+// the circle a is P1.  The reference adds the offset to the circle's own
+// position when projecting and again to the reference point; kept as written.
+__device__ __forceinline__ bool circle_segment(const PState& a, const PState& b, double4 vb,
+                                               vec2<double> off, vec2<double> ovel, Geom& g) {
+  const vec2<double> pa = V(a.x, a.y);
+  const vec2<double> dir = seg_dir(vb);
+  const double proj = dot((pa + off) - V(b.x, b.y), dir);
+  const vec2<double> ref = seg_ref(b, vb, dir, proj);
+  const vec2<double> branch = (ref + off) - pa;
+  const double distance = len(branch);
+  const double sumR = a.r;
+  g.overlap = sumR - distance;
+  if (g.overlap < 0.0) {
+    g.contacted = 0;
+    return false;
+  }
+  g.contacted = 1;
+  g.n = unit(branch);
+  g.cp = ref;
+  g.bv1 = g.cp - pa;
+  g.bv2 = g.cp - (ref + off);
+  relative_velocity(a, b, ovel, g);
+  return true;
+}
+
+// SegmentObject::contactWithCircularParticle (SegmentObject.cpp:45-80), the
+// segment a is P1 (its branch vector to the contact point is zero)
+__device__ __forceinline__ bool segment_circle(const PState& a, double4 va, const PState& b,
+                                               vec2<double> off, vec2<double> ovel, Geom& g) {
+  const vec2<double> dir = seg_dir(va);
+  const vec2<double> pb = V(b.x, b.y) + off;
+  const double proj = dot(pb - V(a.x, a.y), dir);
+  const vec2<double> ref = seg_ref(a, va, dir, proj);
+  const vec2<double> branch = pb - ref;
+  const double distance = len(branch);
+  const double sumR = b.r;
+  g.overlap = sumR - distance;
+  if (g.overlap < 0.0) {
+    g.contacted = 0;
+    return false;
+  }
+  g.contacted = 1;
+  g.n = unit(branch);
+  g.cp = ref;
+  g.bv1 = g.cp - ref;
   g.bv2 = g.cp - pb;
   relative_velocity(a, b, ovel, g);
   return true;
@@ -474,15 +540,26 @@ __device__ __forceinline__ bool contact_geometry_law(const PState& a, const PSta
 }
 
 // BaseParticle::calculateContactGeometry dispatch (CircularParticle.cpp:25-40,
-// EllipticParticle.cpp:16-32 with its coarse bounding-circle test, and
-// GluedParticle.cpp:133-140).  cs_a/cs_b: (cos, sin) of each orientation.
+// EllipticParticle.cpp:16-32 with its coarse bounding-circle test,
+// GluedParticle.cpp:133-140, SegmentObject.cpp:12-27).  cs_a/cs_b: (cos, sin)
+// of each orientation; va/vb: the vertices of a segment.
 __device__ __forceinline__ bool contact_geometry(int method, const PState& a, const PState& b,
                                                  double orad_a, double orad_b, vec2<double> off,
                                                  vec2<double> ovel, double2 cs_a, double2 cs_b,
-                                                 Geom& g, uint32_t& st) {
+                                                 Geom& g, uint32_t& st,
+                                                 double4 va = double4{}, double4 vb = double4{}) {
   g = Geom{};
   if (a.shape == SHAPE_CLUMP || b.shape == SHAPE_CLUMP) return false;
+  if (a.shape == SHAPE_SEGMENT) {
+    if (b.shape == SHAPE_SEGMENT) return false;  // SegmentObject.cpp:20-22
+    if (b.shape != SHAPE_CIRCLE) {
+      st |= ST_UNSUPPORTED;
+      return false;
+    }
+    return segment_circle(a, va, b, off, ovel, g);
+  }
   if (a.shape == SHAPE_CIRCLE) {
+    if (b.shape == SHAPE_SEGMENT) return circle_segment(a, b, vb, off, ovel, g);
     if (b.shape != SHAPE_CIRCLE) {
       st |= ST_UNSUPPORTED;
       return false;

@@ -96,8 +96,9 @@ int32_t xdem_rsa_positions(int32_t n, const double* radius, const double box[4],
   return XDEM_OK;
 }
 
-// CircularParticle::calculateParticleProperties (CircularParticle.cpp:16-23)
-// and EllipticParticle::calculateParticleProperties (EllipticParticle.cpp:7-14)
+// CircularParticle::calculateParticleProperties (CircularParticle.cpp:16-23),
+// EllipticParticle::calculateParticleProperties (EllipticParticle.cpp:7-14)
+// and SegmentObject::calculateParticleProperties (SegmentObject.cpp:4-10)
 int32_t xdem_particle_properties(int32_t n, const int32_t* shape, const double* radius,
                                  const double* aspect, double density, double* volume,
                                  double* mass, double* inv_mass, double* inertia,
@@ -119,6 +120,14 @@ int32_t xdem_particle_properties(int32_t n, const int32_t* shape, const double* 
       mass[i] = volume[i] * density;
       inv_mass[i] = 1.0 / mass[i];
       inertia[i] = mass[i] * (r * r + r * r / k / k) / 4.0;
+      inv_inertia[i] = 1.0 / inertia[i];
+    } else if (shape[i] == XDEM_SHAPE_SEGMENT) {
+      // SegmentObject::calculateParticleProperties (SegmentObject.cpp:4-10):
+      // linear volume, a rod's inertia
+      volume[i] = r * 2.0;
+      mass[i] = volume[i] * density;
+      inv_mass[i] = 1.0 / mass[i];
+      inertia[i] = mass[i] * r * r / 3.0;
       inv_inertia[i] = 1.0 / inertia[i];
     } else {
       return XDEM_ERR_ARGUMENT;

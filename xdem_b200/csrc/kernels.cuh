@@ -355,6 +355,11 @@ __device__ __forceinline__ double damping_constant(const DevWorld& w, double fac
   return sqrt((a * b) / (a + b)) * factor;
 }
 
+// vertices of the wall segment at memory position m (zero for other shapes)
+__device__ __forceinline__ double4 seg_at(const DevWorld& w, int shape, int m) {
+  return shape == SHAPE_SEGMENT ? w.seg[w.id_of[m]] : double4{};
+}
+
 template <bool FOLD_BG>
 __device__ __forceinline__ PState load_state(const DevWorld& w, const WorldScalars& ws, int m) {
   PState p;

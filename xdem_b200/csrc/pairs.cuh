@@ -317,7 +317,8 @@ __global__ void __launch_bounds__(128, 4) k_pair_forces(DevWorld w, int par, int
         csa = make_double2(cos(a.rot), sin(a.rot));
         csb = make_double2(cos(b.rot), sin(b.rot));
       }
-      touching = contact_geometry(w.method, a, b, w.orad[m], w.orad[mj], off, ovel, csa, csb, g, st);
+      touching = contact_geometry(w.method, a, b, w.orad[m], w.orad[mj], off, ovel, csa, csb, g, st,
+                                  seg_at(w, a.shape, m), seg_at(w, b.shape, mj));
     } else {
       // the scan has applied the coarse test of this pair
       double2 csa = make_double2(0.0, 0.0), csb = make_double2(0.0, 0.0);

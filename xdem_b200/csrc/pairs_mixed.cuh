@@ -172,7 +172,8 @@ __global__ void __launch_bounds__(128, 4) k_pair_forces_m(DevWorld w, int par, i
       if (LAW == LAW_INTERSECTION)
         touching = contact_geometry_law<LAW_INTERSECTION, true>(a, b, 0.0, 0.0, off, ovel, csa, csb, gd, st);
       else
-        touching = contact_geometry(w.method, a, b, w.orad[m], w.orad[mj], off, ovel, csa, csb, gd, st);
+        touching = contact_geometry(w.method, a, b, w.orad[m], w.orad[mj], off, ovel, csa, csb, gd, st,
+                                    seg_at(w, a.shape, m), seg_at(w, b.shape, mj));
       if (touching) geom_to_m(gd, a, g);
       res = touching ? PW_CONTACT : PW_NONE;
     }

@@ -118,6 +118,7 @@ struct DevWorld {
   double* rot;
   double* w;
   double2* branch;
+  double4* seg;  // [id] wall segment vertices (x1, y1, x2, y2); NULL without segments
   int32_t* rattler;
   double2* force;
   double* torque;
@@ -136,7 +137,7 @@ struct DevWorld {
   float4* cell_scr;
   int32_t* cell_up;       // [2n] upLevel of each cell entry
   double2* cs;            // [n] (cos, sin) of the orientation, this step
-  const double* screen_r; // rad for an all-circle world, orad otherwise
+  const double* screen_r; // rad for an all-circle world, orad otherwise (segments: kWallScreen)
   int32_t* pcell;  // [n] regular cell of the particle at m
   int32_t* prank;  // [n] rank within the cell
   int32_t* gcell;  // [n] ghost cell or -1

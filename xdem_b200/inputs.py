@@ -87,6 +87,48 @@ def assemble(shape, radius, aspect, x, y, vx, vy, rot, rot_vel, density=1.0):
     return p
 
 
+def segments(x1, y1, x2, y2, vx=0.0, vy=0.0, rot_vel=0.0, density=1.0):
+    """Fixed wall segments from their vertices, with the fields the reference
+    constructor derives (SegmentObject.h:24-40): radius = outer radius = half
+    the vertex distance, position = the midpoint, rotation = the direction's
+    angle, SKIP_TIME_INTEGRAL set; volume, mass and inertia as
+    SegmentObject::calculateParticleProperties gives them."""
+    x1, y1, x2, y2 = (np.ascontiguousarray(np.atleast_1d(v), np.float64) for v in (x1, y1, x2, y2))
+    n = len(x1)
+    half = np.sqrt((x1 - x2) * (x1 - x2) + (y1 - y2) * (y1 - y2)) / 2.0
+    shape = np.full(n, abi.SHAPE_SEGMENT, np.int32)
+    p = assemble(shape, half, np.ones(n), (x1 + x2) / 2.0, (y1 + y2) / 2.0,
+                 np.broadcast_to(vx, (n,)).copy(), np.broadcast_to(vy, (n,)).copy(),
+                 np.arctan2(y2 - y1, x2 - x1), np.broadcast_to(rot_vel, (n,)).copy(), density)
+    p["setting"][:] = abi.SKIP_TIME_INTEGRAL
+    p["seg_x1"], p["seg_y1"], p["seg_x2"], p["seg_y2"] = x1.copy(), y1.copy(), x2.copy(), y2.copy()
+    return p
+
+
+def concatenate(*parts):
+    """One particle dict from several, ids in the order given (clump
+    sub-particle ids must stay right after their clump, so a part holding
+    clumps goes in whole)."""
+    n = [len(q["x"]) for q in parts]
+    out = {}
+    keys = set().union(*[q.keys() for q in parts])
+    for k in keys:
+        arrs = []
+        for q, m in zip(parts, n):
+            if k in q and q[k] is not None:
+                arrs.append(np.asarray(q[k]))
+            else:
+                dt = np.int32 if k in ("shape", "up_level", "setting", "is_rattler", "num_sub") \
+                    else np.float64
+                arrs.append(np.zeros(m, dt))
+        out[k] = np.ascontiguousarray(np.concatenate(arrs))
+    # up levels point at ids: shift them with their part
+    first = np.cumsum([0] + n[:-1])
+    out["up_level"] = np.ascontiguousarray(np.concatenate(
+        [np.asarray(q["up_level"], np.int32) + f for q, f in zip(parts, first)]).astype(np.int32))
+    return out
+
+
 def box_for(area, phi):
     half = 0.5 * math.sqrt(area / phi)
     return np.array([-half, half, -half, half])
