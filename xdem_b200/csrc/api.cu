@@ -30,9 +30,6 @@ constexpr int kDefaultSlots = 24;
 // re-sort + kResortEvery steps) swaps the slot sets an even number of times
 constexpr int kResortEvery = 31;
 constexpr double kPi = 3.14159265358979323846;
-// screening radius of a wall segment: above any box size, and small enough
-// that the squared sum of two stays finite in FP32
-constexpr double kWallScreen = 1e18;
 
 inline int blocks_for(int n, int b) { return (n + b - 1) / b; }
 
@@ -699,25 +696,16 @@ int32_t set_particles_impl(xdem_world_s* w, const xdem_particles* P, const std::
   CK(w, B.alloc(&d.cell_up, 2 * (size_t)n));
   CK(w, B.alloc(&d.cs, n));
   d.screen_r = w->law == LAW_CIRCLE ? d.rad : d.orad;
-  // wall segments: vertices by id, and a screening radius that passes every
-  // pair, so that a segment's candidates are all bodies of the neighbouring
-  // cells, as in the reference's cell search (its outer radius would not
-  // bound it once a box law has moved its midpoint but not its vertices)
+  // wall segments: vertices by id (their screening radius follows from the
+  // vertices and the position, screen_radius in kernels.cuh)
   d.seg = nullptr;
-  double* wall_screen = nullptr;
   if (any_segment) {
     std::vector<double4> sv(n, double4{0.0, 0.0, 0.0, 0.0});
-    std::vector<double> scr(P->outer_radius, P->outer_radius + n);
     for (int i = 0; i < n; ++i)
-      if (P->shape[i] == XDEM_SHAPE_SEGMENT) {
+      if (P->shape[i] == XDEM_SHAPE_SEGMENT)
         sv[i] = double4{P->seg_x1[i], P->seg_y1[i], P->seg_x2[i], P->seg_y2[i]};
-        scr[i] = kWallScreen;
-      }
     CK(w, B.alloc(&d.seg, n));
     CK(w, upload(d.seg, sv.data(), n, s));
-    CK(w, B.alloc(&wall_screen, n));
-    CK(w, upload(wall_screen, scr.data(), n, s));
-    d.screen_r = wall_screen;
   }
   CK(w, B.alloc(&d.pcell, n));
   CK(w, B.alloc(&d.prank, n));
@@ -818,7 +806,6 @@ int32_t set_particles_impl(xdem_world_s* w, const xdem_particles* P, const std::
   add(d.force, 16);
   add(d.pcell, 4);  // read by the candidate scan's history test after a re-sort
   add(d.gcell, 4);
-  if (wall_screen) add(wall_screen, 8);
   size_t off = 0;
   for (int a = 0; a < L.count; ++a) {
     L.offset[a] = off;

@@ -136,9 +136,16 @@ __global__ void k_scale_positions(DevWorld w) {
   if (i >= w.n) return;
   const WorldScalars& ws = w.ws[sys_at(w, i)];
   double2 p = w.pos[i];
+  const double2 old = p;
   p.x *= ws.scale_x;
   p.y *= ws.scale_y;
   w.pos[i] = p;
+  // the lists' travel budget covers relative moves between bodies; a wall
+  // segment's reach also changes with its own move (screen_radius)
+  if (w.V && w.seg && w.shape[i] == SHAPE_SEGMENT) {
+    const double ex = p.x - old.x, ey = p.y - old.y;
+    w.vl_disp[i] += 2.0 * sqrt(ex * ex + ey * ey);
+  }
 }
 
 // a6: LeesEdwardsBoundaryWorld::apply/removeBackgroudVelocity (:508-530)
@@ -290,6 +297,28 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_apply(DevWorld w) {
   }
 }
 
+// Radius of the coarse FP32 screen of the body at m: its screening radius, or
+// for a wall segment the farthest point it can touch from its position (its
+// half length, or more once a box law has moved its midpoint but not its
+// vertices), with a relative margin of 1e-6.  The candidate lists count a
+// segment's moves twice (its reach grows with them), see seg_path_factor.
+__device__ __forceinline__ float screen_radius(const DevWorld& w, int m) {
+  if (w.seg && w.shape[m] == SHAPE_SEGMENT) {
+    const double4 v = w.seg[w.id_of[m]];
+    const double2 p = w.pos[m];
+    const double a = sqrt((v.x - p.x) * (v.x - p.x) + (v.y - p.y) * (v.y - p.y));
+    const double b = sqrt((v.z - p.x) * (v.z - p.x) + (v.w - p.y) * (v.w - p.y));
+    return (float)(fmax(w.rad[m], fmax(a, b)) * (1.0 + 1e-6));
+  }
+  return (float)w.screen_r[m];
+}
+
+// path-length weight of the body at m for the candidate lists: 2 for a wall
+// segment (its position and its reach both move), 1 otherwise
+__device__ __forceinline__ double seg_path_factor(const DevWorld& w, int m) {
+  return (w.seg && w.shape[m] == SHAPE_SEGMENT) ? 2.0 : 1.0;
+}
+
 // also clears cell_count (already consumed by the scan) for the next binning
 __global__ void k_scatter(DevWorld w) {
   if (stopped(w)) return;
@@ -306,7 +335,7 @@ __global__ void k_scatter(DevWorld w) {
   const int ix = local % G.nx, iy = local / G.nx;
   // position relative to the cell's corner; y is the same in a ghost row
   const float ry = (float)(p.y - (ws.ymin + iy * G.ly));
-  const float sr = (float)w.screen_r[i];
+  const float sr = screen_radius(w, i);
   const float idb = __int_as_float((w.setting[i] & SKIP_CONTACT_DETECTION) ? -1 : w.id_of[i]);
   const int up = w.up[i];
   int q = w.cell_start[pc] + w.prank[i];
@@ -542,7 +571,7 @@ __global__ void k_integrate(DevWorld w, int reset_rattlers) {
   p.x += vv.x * dt;
   p.y += vv.y * dt;
   om = (om * (1.0 - g * dt) + w.torque[i] * w.iI[i] * dt) / (1.0 + g * dt);
-  if (w.V) w.vl_disp[i] += sqrt(vv.x * vv.x + vv.y * vv.y) * dt;  // for the candidate lists
+  if (w.V) w.vl_disp[i] += sqrt(vv.x * vv.x + vv.y * vv.y) * dt * seg_path_factor(w, i);  // candidate lists
   w.pos[i] = p;
   w.rot[i] = w.rot[i] + om * dt;
   if (reset_rattlers && !(set & SKIP_MACRO_SUM) && w.rattler[i]) {
@@ -848,7 +877,7 @@ __global__ void k_stage(DevWorld w, int to_world) {
     if (w.V) {  // the host's move counts toward the candidate lists' skin
       const double2 op = w.pos[m];
       const double ex = s[id] - op.x, ey = s[n + id] - op.y;
-      w.vl_disp[m] += sqrt(ex * ex + ey * ey);
+      w.vl_disp[m] += sqrt(ex * ex + ey * ey) * seg_path_factor(w, m);
     }
     w.pos[m] = make_double2(s[id], s[n + id]);
     w.vel[m] = make_double2(s[2 * n + id], s[3 * n + id]);

@@ -123,7 +123,7 @@ __device__ __forceinline__ void scan_cells(const DevWorld& w, const WorldScalars
   const float rxi = (float)(pi.x - (ws.xmin + ix * G.lx));
   const float ryi = (float)(pi.y - (ws.ymin + iy * G.ly));
   const float flx = (float)G.lx, fly = (float)G.ly;
-  const float sr_i = (float)w.screen_r[m];
+  const float sr_i = screen_radius(w, m);
   int ncand0 = 0, ncand1 = 0, ncand2 = 0;
 #pragma unroll 1
   for (int k = 0; k < 9; ++k) {

@@ -89,7 +89,7 @@ __global__ void __launch_bounds__(128) k_vl_build(DevWorld w) {
     const float rxi = (float)(pi.x - (ws.xmin + ix * G.lx));
     const float ryi = (float)(pi.y - (ws.ymin + iy * G.ly));
     const float flx = (float)G.lx, fly = (float)G.ly;
-    const float sr_i = (float)w.screen_r[m] + (float)w.skin;
+    const float sr_i = screen_radius(w, m) + (float)w.skin;
 #pragma unroll 1
     for (int k = 0; k < 9; ++k) {
       const int dx = k / 3 - 1, dy = k % 3 - 1;

@@ -137,7 +137,7 @@ struct DevWorld {
   float4* cell_scr;
   int32_t* cell_up;       // [2n] upLevel of each cell entry
   double2* cs;            // [n] (cos, sin) of the orientation, this step
-  const double* screen_r; // rad for an all-circle world, orad otherwise (segments: kWallScreen)
+  const double* screen_r; // rad for an all-circle world, orad otherwise (segments: screen_radius)
   int32_t* pcell;  // [n] regular cell of the particle at m
   int32_t* prank;  // [n] rank within the cell
   int32_t* gcell;  // [n] ghost cell or -1
