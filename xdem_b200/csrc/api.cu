@@ -688,6 +688,8 @@ int32_t set_particles_impl(xdem_world_s* w, const xdem_particles* P, const std::
     CK(w, upload(d.sys_of, sys_of.data(), n, s));
   }
   CK(w, B.alloc(&d.cell_count, cells + 1));
+  CK(w, B.alloc(&d.cell_max, 1));
+  CK(w, cudaMemsetAsync(d.cell_max, 0, sizeof(int32_t), s));
   CK(w, B.alloc(&d.cell_start, cells + 1));
   CK(w, B.alloc(&d.tile_sum, cells / kScanTile + 2));
   CK(w, B.alloc(&d.cell_mem, 2 * (size_t)n));

@@ -172,6 +172,7 @@ __global__ void k_background_velocity(DevWorld w, int apply) {
 __global__ void k_bin(DevWorld w) {
   if (stopped(w)) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0) *w.cell_max = 0;  // k_scan_tiles takes the maximum
   if (i >= w.n) return;
   const WorldScalars& ws = w.ws[sys_at(w, i)];
   Grid G = grid_of(ws);
@@ -242,10 +243,16 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_tiles(DevWorld w) {
   __shared__ int32_t sh_warp[kScanThreads / 32];
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     int base = tile * kScanTile + threadIdx.x * kScanPer;
-    int32_t s = 0;
+    int32_t s = 0, mx = 0;
 #pragma unroll
     for (int k = 0; k < kScanPer; ++k)
-      if (base + k < total) s += w.cell_count[base + k];
+      if (base + k < total) {
+        const int32_t c = w.cell_count[base + k];
+        s += c;
+        mx = max(mx, c);
+      }
+    mx = __reduce_max_sync(0xffffffffu, mx);
+    if ((threadIdx.x & 31) == 0 && mx > 0) atomicMax(w.cell_max, mx);
     int32_t inc = block_inclusive_scan(s, sh_warp);
     if (threadIdx.x == kScanThreads - 1) w.tile_sum[tile] = inc;
     __syncthreads();

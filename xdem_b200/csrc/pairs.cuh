@@ -109,15 +109,18 @@ __device__ __forceinline__ int neighbour_cell(const Grid& G, int world_kind, int
 // The reference's 3x3 scan for the owner at m (cell ix, iy): every candidate
 // j with a larger id and another upLevel, counted per image kind against the
 // 200-candidate cap, and the ones passing the coarse test appended to
-// (list_mj, list_code).  The distance screen runs in FP32 on positions
-// relative to the cell corners; only candidates within its rounding margin of
-// the threshold take the reference's FP64 test.
+// (list_mj, list_code); `matched` receives the old slots of the listed pairs
+// (all of them candidates, so their old slots count as seen).  The distance
+// screen runs in FP32 on positions relative to the cell corners; only
+// candidates within its rounding margin of the threshold take the
+// reference's FP64 test.
 template <int LAW>
 __device__ __forceinline__ void scan_cells(const DevWorld& w, const WorldScalars& ws, const Grid& G,
                                            int m, int ix, int iy, double2 pi, int id_i, int up_i,
                                            int shape_i, double r_i, double orad_i,
                                            const Slots& old, int nold, int& nlist,
-                                           int32_t* list_mj, int32_t* list_code, uint32_t& st) {
+                                           int32_t* list_mj, int32_t* list_code, uint32_t& st,
+                                           uint32_t& matched) {
   const int n = w.n, K = w.K;
   // the owner relative to its cell's corner, in FP32 (see k_scatter)
   const float rxi = (float)(pi.x - (ws.xmin + ix * G.lx));
@@ -170,6 +173,7 @@ __device__ __forceinline__ void scan_cells(const DevWorld& w, const WorldScalars
       int oslot = kNoOldSlot;
       for (int z = 0; z < nold; ++z)
         if (old.partner[(size_t)z * n + m] == id_j) oslot = z;
+      if (oslot != kNoOldSlot) matched |= 1u << oslot;
       list_mj[nlist] = w.cell_mem[q];
       list_code[nlist] = kind | (nlist << 8) | (oslot << 16);
       ++nlist;
@@ -215,10 +219,14 @@ __global__ void __launch_bounds__(128) k_candidates(DevWorld w, int par) {
       const double r_i = w.rad[m], orad_i = w.orad[m];
       const int ix = cell_of(pi.x, ws.xmin, G.lx, G.nx);
       const int iy = cell_of(pi.y, ws.ymin, G.ly, G.ny);
+      uint32_t matched = 0;
       scan_cells<LAW>(w, ws, G, m, ix, iy, pi, id_i, up_i, shape_i, r_i, orad_i, old, nold, nlist,
-                      list_mj, list_code, st);
-      // old partners among the candidates
+                      list_mj, list_code, st, matched);
+      // old partners among the candidates: the listed ones are; the others
+      // are looked up in the nine cells
+      seen = matched;
       for (int z = 0; z < nold; ++z) {
+        if (matched & (1u << z)) continue;
         const int p = old.partner[(size_t)z * n + m];
         if (p < 0) continue;
         const int mj = w.mpos[p];

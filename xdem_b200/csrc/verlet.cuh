@@ -149,16 +149,20 @@ __global__ void __launch_bounds__(128) k_candidates_vl(DevWorld w, int par) {
       const int ix = cell_of(pi.x, ws.xmin, G.lx, G.nx);
       const int iy = cell_of(pi.y, ws.ymin, G.ly, G.ny);
       const int cnt = w.vl_cnt[m];
+      // old slots of listed pairs known to be candidates now (see below)
+      uint32_t matched = 0;
       if (cnt < 0) {  // the list overflowed at its build: the full scan
         scan_cells<LAW>(w, ws, G, m, ix, iy, pi, id_i, up_i, shape_i, r_i, orad_i, old, nold,
-                        nlist, list_mj, list_code, st);
+                        nlist, list_mj, list_code, st, matched);
       } else {
         // the 200-candidate cap (PeriodicBoundaryWorld.cpp:75-78): the nine
         // cells' record counts bound each kind's candidates; where a bound
         // reaches the cap, the candidates are counted as the full scan does
+        // (skipped when no nine cells can hold that many records)
         int tot0 = 0, tot1 = 0, tot2 = 0;
+        const bool cap_reachable = 9 * *w.cell_max + 1 >= kCandidateCap;
 #pragma unroll
-        for (int k = 0; k < 9; ++k) {
+        for (int k = 0; k < 9 && cap_reachable; ++k) {
           int kind;
           const int c = neighbour_cell(G, w.kind, ix, iy, k / 3 - 1, k % 3 - 1, kind);
           const int cc = w.cell_start[c + 1] - w.cell_start[c];
@@ -201,13 +205,22 @@ __global__ void __launch_bounds__(128) k_candidates_vl(DevWorld w, int par) {
           int oslot = kNoOldSlot;
           for (int z = 0; z < nold; ++z)
             if (old.partner[(size_t)z * n + m] == id_j) oslot = z;
+          // a pair that passed a distance test lies within one cell size,
+          // so it is a candidate of the 3x3 scan (LAW_ANY's other pairs pass
+          // without one and take the cell test below)
+          const bool near = LAW != LAW_ANY ||
+                            (shape_i == w.shape[mj] &&
+                             (shape_i == SHAPE_CIRCLE || shape_i == SHAPE_ELLIPSE));
+          if (oslot != kNoOldSlot && near) matched |= 1u << oslot;
           list_mj[nlist] = mj;
           list_code[nlist] = kind | (nlist << 8) | (oslot << 16);
           ++nlist;
         }
       }
       // old partners among the candidates
+      seen = matched;
       for (int z = 0; z < nold; ++z) {
+        if (matched & (1u << z)) continue;
         const int p = old.partner[(size_t)z * n + m];
         if (p < 0) continue;
         const int mj = w.mpos[p];

@@ -126,6 +126,7 @@ struct DevWorld {
   // cell grid: regular cells, then two ghost rows of nx (Lees-Edwards images);
   // cell_mem holds memory positions
   int32_t* cell_count;
+  int32_t* cell_max;  // largest cell count of this step's binning (all systems)
   int32_t* cell_start;
   int32_t* tile_sum;  // scan tile sums
   int32_t* cell_mem;
