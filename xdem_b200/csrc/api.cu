@@ -696,7 +696,7 @@ int32_t set_particles_impl(xdem_world_s* w, const xdem_particles* P, const std::
   CK(w, B.alloc(&d.cell_pos, 2 * (size_t)n));
   CK(w, B.alloc(&d.cell_scr, 2 * (size_t)n));
   CK(w, B.alloc(&d.cell_up, 2 * (size_t)n));
-  CK(w, B.alloc(&d.cs, n));
+  CK(w, B.alloc(&d.body, n));
   d.screen_r = w->law == LAW_CIRCLE ? d.rad : d.orad;
   // wall segments: vertices by id (their screening radius follows from the
   // vertices and the position, screen_radius in kernels.cuh)

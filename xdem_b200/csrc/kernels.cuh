@@ -381,20 +381,6 @@ __global__ void k_scatter(DevWorld w) {
 // FOLD_BG adds the Lees-Edwards background velocity on the fly, bit for bit the
 // value applyBackgroudVelocity would have stored.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ double damping_constant(const DevWorld& w, double factor, int mi, int mj) {
-  // calculateDampingConstact (ContactModel_LinearDissipativeFrictional.cpp:73-82)
-  // selected by SKIP_TIME_INTEGRAL (BaseParticle.cpp:53-64)
-  int si = w.setting[mi] & SKIP_TIME_INTEGRAL, sj = w.setting[mj] & SKIP_TIME_INTEGRAL;
-  double a = w.mass[mi], b = w.mass[mj];
-  if (!si && sj) return sqrt(a) * factor;
-  if (si && !sj) return sqrt(b) * factor;
-  return sqrt((a * b) / (a + b)) * factor;
-}
-
-// vertices of the wall segment at memory position m (zero for other shapes)
-__device__ __forceinline__ double4 seg_at(const DevWorld& w, int shape, int m) {
-  return shape == SHAPE_SEGMENT ? w.seg[w.id_of[m]] : double4{};
-}
 
 template <bool FOLD_BG>
 __device__ __forceinline__ PState load_state(const DevWorld& w, const WorldScalars& ws, int m) {
@@ -411,6 +397,57 @@ __device__ __forceinline__ PState load_state(const DevWorld& w, const WorldScala
   p.rot = w.rot[m];
   p.w = w.w[m];
   return p;
+}
+
+// the record of the body at m for this step's pair kernels; cs = (cos, sin)
+// of its orientation for an ellipse
+__device__ __forceinline__ void write_body(const DevWorld& w, int m, double2 cs) {
+  BodyRec b;
+  b.pos = w.pos[m];
+  b.vel = w.vel[m];
+  b.rot = w.rot[m];
+  b.w = w.w[m];
+  b.r = w.rad[m];
+  b.asp = w.asp[m];
+  b.cs = cs;
+  b.shape = w.shape[m];
+  b.id = w.id_of[m];
+  b.setting = w.setting[m];
+  b.pad = 0;
+  w.body[m] = b;
+}
+
+// the state load_state gives, from a body record
+template <bool FOLD_BG>
+__device__ __forceinline__ PState body_state(const BodyRec& b, const WorldScalars& ws) {
+  PState p;
+  p.shape = b.shape;
+  p.r = b.r;
+  p.asp = b.asp;
+  p.x = b.pos.x;
+  p.y = b.pos.y;
+  p.vx = FOLD_BG ? b.vel.x + ws.shift_rate * b.pos.y : b.vel.x;
+  p.vy = b.vel.y;
+  p.rot = b.rot;
+  p.w = b.w;
+  return p;
+}
+
+// vertices of a wall segment from its record (zero for other shapes)
+__device__ __forceinline__ double4 seg_of(const DevWorld& w, const BodyRec& b) {
+  return b.shape == SHAPE_SEGMENT ? w.seg[b.id] : double4{};
+}
+
+// damping constant of a new contact (the records carry the settings)
+__device__ __forceinline__ double damping_of(const DevWorld& w, double factor, const BodyRec& bi,
+                                             const BodyRec& bj, int mi, int mj) {
+  // calculateDampingConstact (ContactModel_LinearDissipativeFrictional.cpp:73-82)
+  // selected by SKIP_TIME_INTEGRAL (BaseParticle.cpp:53-64)
+  const int si = bi.setting & SKIP_TIME_INTEGRAL, sj = bj.setting & SKIP_TIME_INTEGRAL;
+  const double a = w.mass[mi], b = w.mass[mj];
+  if (!si && sj) return sqrt(a) * factor;
+  if (si && !sj) return sqrt(b) * factor;
+  return sqrt((a * b) / (a + b)) * factor;
 }
 
 // small insertion sorts of keys held in local arrays

@@ -46,8 +46,8 @@ __global__ void __launch_bounds__(128) k_mlp_warm(DevWorld w, MlpDev net, const 
         const PairEntry e = w.pairs[list ? list[i] : i];
         double2 csa, csb;
         if (LAW == LAW_CLOSEST) {
-          csa = w.cs[e.m];
-          csb = w.cs[e.mj];
+          csa = w.body[e.m].cs;
+          csb = w.body[e.mj].cs;
         } else {
           csa = make_double2(cos(w.rot[e.m]), sin(w.rot[e.m]));
           csb = make_double2(cos(w.rot[e.mj]), sin(w.rot[e.mj]));

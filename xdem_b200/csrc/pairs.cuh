@@ -204,9 +204,16 @@ __global__ void __launch_bounds__(128) k_candidates(DevWorld w, int par) {
   int32_t list_mj[kMaxSlots];
   int32_t list_code[kMaxSlots];
   if (valid) {
-    if (LAW == LAW_CLOSEST || LAW == LAW_INTERSECTION) {
-      const double r = w.rot[m];
-      w.cs[m] = make_double2(cos(r), sin(r));
+    {
+      // this step's record of the body for the pair kernels; an ellipse's
+      // (cos, sin) is computed once per body instead of once per pair
+      double2 cs = make_double2(0.0, 0.0);
+      if (LAW == LAW_CLOSEST || LAW == LAW_INTERSECTION ||
+          (LAW == LAW_ANY && w.shape[m] == SHAPE_ELLIPSE)) {
+        const double r = w.rot[m];
+        cs = make_double2(cos(r), sin(r));
+      }
+      write_body(w, m, cs);
     }
     Grid G = grid_of(ws);
     const int id_i = w.id_of[m];
@@ -313,8 +320,9 @@ __global__ void __launch_bounds__(128, 4) k_pair_forces(DevWorld w, int par, int
     if (WARM && LAW == LAW_CLOSEST) wp = w.warm[t];
     const int kind = e.code & 0xff, slot = (e.code >> 8) & 0xff, o = (e.code >> 16) & 0xff;
     const size_t ci = (size_t)slot * n + m;
-    PState a = load_state<FOLD_BG>(w, ws, m);
-    PState b = load_state<FOLD_BG>(w, ws, mj);
+    const BodyRec ba = w.body[m], bb = w.body[mj];
+    PState a = body_state<FOLD_BG>(ba, ws);
+    PState b = body_state<FOLD_BG>(bb, ws);
     vec2<double> off, ovel;
     image_offset(ws, kind, make_double2(a.x, a.y), make_double2(b.x, b.y), off, ovel);
     Geom g;
@@ -322,17 +330,17 @@ __global__ void __launch_bounds__(128, 4) k_pair_forces(DevWorld w, int par, int
     if (LAW == LAW_ANY) {
       double2 csa = make_double2(0.0, 0.0), csb = make_double2(0.0, 0.0);
       if (a.shape == SHAPE_ELLIPSE && b.shape == SHAPE_ELLIPSE) {
-        csa = make_double2(cos(a.rot), sin(a.rot));
-        csb = make_double2(cos(b.rot), sin(b.rot));
+        csa = ba.cs;
+        csb = bb.cs;
       }
       touching = contact_geometry(w.method, a, b, w.orad[m], w.orad[mj], off, ovel, csa, csb, g, st,
-                                  seg_at(w, a.shape, m), seg_at(w, b.shape, mj));
+                                  seg_of(w, ba), seg_of(w, bb));
     } else {
       // the scan has applied the coarse test of this pair
       double2 csa = make_double2(0.0, 0.0), csb = make_double2(0.0, 0.0);
       if (LAW != LAW_CIRCLE) {
-        csa = w.cs[m];
-        csb = w.cs[mj];
+        csa = ba.cs;
+        csb = bb.cs;
       }
       touching = contact_geometry_law<LAW, true, WARM && LAW == LAW_CLOSEST>(
           a, b, 0.0, 0.0, off, ovel, csa, csb, g, st, wp.x);
@@ -353,7 +361,7 @@ __global__ void __launch_bounds__(128, 4) k_pair_forces(DevWorld w, int par, int
       cur.partner[ci] = -1;
       continue;
     }
-    const int id_j = w.id_of[mj];
+    const int id_j = bb.id;
     // BaseParticle::calculateContactForceAndTorque (BaseParticle.cpp:27-98)
     vec2<double> sh, nn = g.n;
     double damp;
@@ -361,7 +369,7 @@ __global__ void __launch_bounds__(128, 4) k_pair_forces(DevWorld w, int par, int
       double rvn = dot(g.rv, g.n);
       if (!is_normal(rvn)) sh = g.srv * dt;
       else sh = g.srv * std_min(dt, g.overlap / rvn);
-      damp = damping_constant(w, factor, m, mj);
+      damp = damping_of(w, factor, ba, bb, m, mj);
     } else {
       size_t oi = (size_t)o * n + m;
       double2 on = old.n[oi], os = old.s[oi];

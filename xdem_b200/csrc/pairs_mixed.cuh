@@ -26,7 +26,8 @@ __device__ __forceinline__ bool is_normal_f(float x) {
 
 // history, force and torques of one touching pair, written to its slot
 __device__ __forceinline__ void write_contact_m(const DevWorld& w, const WorldScalars& ws,
-                                                const PairEntry& e, const PState& a,
+                                                const PairEntry& e, const BodyRec& ba,
+                                                const BodyRec& bb, const PState& a,
                                                 const PState& b, vec2<double> off,
                                                 const GeomM& g, int par, int record,
                                                 uint32_t& st) {
@@ -45,7 +46,7 @@ __device__ __forceinline__ void write_contact_m(const DevWorld& w, const WorldSc
     if (is_normal_f(rvn)) tt = std_min(dt, g.overlap / (double)rvn);
     sx = (double)g.srv.x * tt;
     sy = (double)g.srv.y * tt;
-    damp = damping_constant(w, ws.factor, m, mj);
+    damp = damping_of(w, ws.factor, ba, bb, m, mj);
   } else {
     const size_t oi = (size_t)o * n + m;
     const double2 on = old.n[oi], os = old.s[oi];
@@ -81,7 +82,7 @@ __device__ __forceinline__ void write_contact_m(const DevWorld& w, const WorldSc
     }
   }
   const float Fx = fnx + fsx, Fy = fny + fsy;
-  const int id_j = w.id_of[mj];
+  const int id_j = bb.id;
   cur.partner[ci] = id_j;
   cur.n[ci] = make_double2((double)g.n.x, (double)g.n.y);
   cur.s[ci] = make_double2(sx, sy);
@@ -121,8 +122,9 @@ __global__ void __launch_bounds__(128, 4) k_pair_forces_m(DevWorld w, int par, i
     const WorldScalars& ws = w.ws[sys_at(w, m)];
     const int kind = e.code & 0xff, slot = (e.code >> 8) & 0xff;
     const size_t ci = (size_t)slot * n + m;
-    const PState a = load_state<FOLD_BG>(w, ws, m);
-    const PState b = load_state<FOLD_BG>(w, ws, mj);
+    const BodyRec ba = w.body[m], bb = w.body[mj];
+    const PState a = body_state<FOLD_BG>(ba, ws);
+    const PState b = body_state<FOLD_BG>(bb, ws);
     vec2<double> off, ovel;
     image_offset(ws, kind, make_double2(a.x, a.y), make_double2(b.x, b.y), off, ovel);
     GeomM g;
@@ -135,15 +137,7 @@ __global__ void __launch_bounds__(128, 4) k_pair_forces_m(DevWorld w, int par, i
     if (circles) {
       res = circle_circle_m(a, b, off, ovel, g) ? PW_CONTACT : PW_NONE;
     } else if (closest) {
-      double2 csa, csb;
-      if (LAW == LAW_CLOSEST) {
-        csa = w.cs[m];
-        csb = w.cs[mj];
-      } else {
-        csa = make_double2(cos(a.rot), sin(a.rot));
-        csb = make_double2(cos(b.rot), sin(b.rot));
-      }
-      res = ellipse_closest_m(a, b, off, ovel, csa, csb, g);
+      res = ellipse_closest_m(a, b, off, ovel, ba.cs, bb.cs, g);
       // deferred pairs take consecutive list entries, one atomic per warp
       const unsigned act = __activemask();
       const unsigned defer = __ballot_sync(act, res == PW_FALLBACK);
@@ -160,12 +154,9 @@ __global__ void __launch_bounds__(128, 4) k_pair_forces_m(DevWorld w, int par, i
       // intersection law (kept FP64: near tangency its quartic has a near
       // double root), clumps and unsupported pairs: the FP64 dispatcher
       double2 csa = make_double2(0.0, 0.0), csb = make_double2(0.0, 0.0);
-      if (LAW == LAW_INTERSECTION) {
-        csa = w.cs[m];
-        csb = w.cs[mj];
-      } else if (a.shape == SHAPE_ELLIPSE && b.shape == SHAPE_ELLIPSE) {
-        csa = make_double2(cos(a.rot), sin(a.rot));
-        csb = make_double2(cos(b.rot), sin(b.rot));
+      if (LAW == LAW_INTERSECTION || (a.shape == SHAPE_ELLIPSE && b.shape == SHAPE_ELLIPSE)) {
+        csa = ba.cs;
+        csb = bb.cs;
       }
       Geom gd;
       bool touching;
@@ -173,7 +164,7 @@ __global__ void __launch_bounds__(128, 4) k_pair_forces_m(DevWorld w, int par, i
         touching = contact_geometry_law<LAW_INTERSECTION, true>(a, b, 0.0, 0.0, off, ovel, csa, csb, gd, st);
       else
         touching = contact_geometry(w.method, a, b, w.orad[m], w.orad[mj], off, ovel, csa, csb, gd, st,
-                                    seg_at(w, a.shape, m), seg_at(w, b.shape, mj));
+                                    seg_of(w, ba), seg_of(w, bb));
       if (touching) geom_to_m(gd, a, g);
       res = touching ? PW_CONTACT : PW_NONE;
     }
@@ -181,7 +172,7 @@ __global__ void __launch_bounds__(128, 4) k_pair_forces_m(DevWorld w, int par, i
       cur.partner[ci] = -1;
       continue;
     }
-    write_contact_m(w, ws, e, a, b, off, g, par, record, st);
+    write_contact_m(w, ws, e, ba, bb, a, b, off, g, par, record, st);
   }
   flush_warp(w, st, n_solves, n_iters, n_capped);
 }
@@ -202,18 +193,12 @@ __global__ void __launch_bounds__(128) k_pair_fallback_m(DevWorld w, int par, in
     const WorldScalars& ws = w.ws[sys_at(w, m)];
     const int kind = e.code & 0xff, slot = (e.code >> 8) & 0xff;
     const size_t ci = (size_t)slot * n + m;
-    const PState a = load_state<FOLD_BG>(w, ws, m);
-    const PState b = load_state<FOLD_BG>(w, ws, mj);
+    const BodyRec ba = w.body[m], bb = w.body[mj];
+    const PState a = body_state<FOLD_BG>(ba, ws);
+    const PState b = body_state<FOLD_BG>(bb, ws);
     vec2<double> off, ovel;
     image_offset(ws, kind, make_double2(a.x, a.y), make_double2(b.x, b.y), off, ovel);
-    double2 csa, csb;
-    if (LAW == LAW_CLOSEST) {
-      csa = w.cs[m];
-      csb = w.cs[mj];
-    } else {
-      csa = make_double2(cos(a.rot), sin(a.rot));
-      csb = make_double2(cos(b.rot), sin(b.rot));
-    }
+    const double2 csa = ba.cs, csb = bb.cs;
     Geom gd = Geom{};
     const float2 wp = WARM ? w.warm[f] : make_float2(0.0f, 0.0f);
     const bool touching =
@@ -236,7 +221,7 @@ __global__ void __launch_bounds__(128) k_pair_fallback_m(DevWorld w, int par, in
     }
     GeomM g;
     geom_to_m(gd, a, g);
-    write_contact_m(w, ws, e, a, b, off, g, par, record, st);
+    write_contact_m(w, ws, e, ba, bb, a, b, off, g, par, record, st);
   }
   flush_warp(w, st, n_solves, n_iters, n_capped);
   if (WARM) flush_warm(w, w_off, w_used, w_rej, w_rest, w_right);

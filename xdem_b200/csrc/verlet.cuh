@@ -133,9 +133,16 @@ __global__ void __launch_bounds__(128) k_candidates_vl(DevWorld w, int par) {
   int32_t list_mj[kMaxSlots];
   int32_t list_code[kMaxSlots];
   if (valid) {
-    if (LAW == LAW_CLOSEST || LAW == LAW_INTERSECTION) {
-      const double r = w.rot[m];
-      w.cs[m] = make_double2(cos(r), sin(r));
+    {
+      // this step's record of the body for the pair kernels; an ellipse's
+      // (cos, sin) is computed once per body instead of once per pair
+      double2 cs = make_double2(0.0, 0.0);
+      if (LAW == LAW_CLOSEST || LAW == LAW_INTERSECTION ||
+          (LAW == LAW_ANY && w.shape[m] == SHAPE_ELLIPSE)) {
+        const double r = w.rot[m];
+        cs = make_double2(cos(r), sin(r));
+      }
+      write_body(w, m, cs);
     }
     const Grid G = grid_of(ws);
     const int id_i = w.id_of[m];

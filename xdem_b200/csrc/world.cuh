@@ -72,6 +72,18 @@ struct WorldScalars {
   unsigned long long vl_builds;  // candidate-list rebuilds since the last reset
 };
 
+// One body as the pair kernels read it: every field of a contact
+// construction in one 96-byte record (three 32-byte sectors per gather,
+// against eight scattered arrays).  The candidate kernels rewrite it each
+// step, after the last position move of the step's first half.
+struct alignas(32) BodyRec {
+  double2 pos, vel;
+  double rot, w, r, asp;
+  double2 cs;  // (cos, sin) of rot for an ellipse, zero otherwise
+  int32_t shape, id, setting, pad;
+};
+static_assert(sizeof(BodyRec) == 96, "BodyRec is three sectors");
+
 // one pair listed by the candidate scan: owner position, partner position,
 // and packed in `code` the image kind (bits 0-7), the owner's new slot for the
 // pair (bits 8-15) and its slot in the old set, 255 when the pair is new
@@ -137,7 +149,7 @@ struct DevWorld {
   // contact detection, so that one comparison applies both filters)
   float4* cell_scr;
   int32_t* cell_up;       // [2n] upLevel of each cell entry
-  double2* cs;            // [n] (cos, sin) of the orientation, this step
+  BodyRec* body;          // [n] this step's pair-kernel record of each body
   const double* screen_r; // rad for an all-circle world, orad otherwise (segments: screen_radius)
   int32_t* pcell;  // [n] regular cell of the particle at m
   int32_t* prank;  // [n] rank within the cell
