@@ -54,7 +54,10 @@ enum xdem_status_bits {
   XDEM_ERR_ARGUMENT = 1 << 6,
   /* cell grid has fewer than 3 cells along an axis (the reference's 3x3
      neighbour scan would visit a cell twice) */
-  XDEM_ERR_GRID = 1 << 7
+  XDEM_ERR_GRID = 1 << 7,
+  /* a device-side wait (tensor-core completion barrier) ran out of its
+     iteration limit; the kernel freed its resources and stopped */
+  XDEM_ERR_TIMEOUT = 1 << 8
 };
 
 /* World kinds: PeriodicBoundaryWorld.h:8, PeriodicControlWorld.h:5,

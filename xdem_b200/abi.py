@@ -21,10 +21,11 @@ ERR_ZERO_VECTOR = 1 << 4
 ERR_CUDA = 1 << 5
 ERR_ARGUMENT = 1 << 6
 ERR_GRID = 1 << 7
+ERR_TIMEOUT = 1 << 8
 STATUS_NAMES = {
     ERR_CAPACITY: "CAPACITY", ERR_NEWTON: "NEWTON", ERR_NONFINITE: "NONFINITE",
     ERR_UNSUPPORTED_PAIR: "UNSUPPORTED_PAIR", ERR_ZERO_VECTOR: "ZERO_VECTOR",
-    ERR_CUDA: "CUDA", ERR_ARGUMENT: "ARGUMENT", ERR_GRID: "GRID",
+    ERR_CUDA: "CUDA", ERR_ARGUMENT: "ARGUMENT", ERR_GRID: "GRID", ERR_TIMEOUT: "TIMEOUT",
 }
 
 WORLD_PERIODIC, WORLD_PERIODIC_CONTROL, WORLD_LEES_EDWARDS = 0, 1, 2

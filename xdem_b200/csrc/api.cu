@@ -241,7 +241,7 @@ void launch_update_phases(xdem_world_s* w, int record) {
     }
   } else if (warm) {
     LAUNCH(w, KK_WARM,
-           k_mlp_warm<LAW><<<148 * 8, 128, 0, w->stream>>>(w->dw, w->mlp->dev(), w->dw.npairs, nullptr));
+           k_mlp_warm<LAW><<<148 * 4, 128, 0, w->stream>>>(w->dw, w->mlp->dev(), w->dw.npairs, nullptr));
     LAUNCH(w, KK_PAIRS,
            k_pair_forces<FOLD_BG, LAW, true><<<pb, 128, 0, w->stream>>>(w->dw, w->par, record));
   } else {
@@ -395,6 +395,7 @@ const char* xdem_status_string(int32_t bit) {
     case XDEM_ERR_CUDA: return "CUDA runtime error";
     case XDEM_ERR_ARGUMENT: return "invalid argument";
     case XDEM_ERR_GRID: return "cell grid has fewer than 3 cells along an axis";
+    case XDEM_ERR_TIMEOUT: return "a device-side wait ran out of its iteration limit";
     default: return "unknown status";
   }
 }

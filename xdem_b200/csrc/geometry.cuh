@@ -21,7 +21,8 @@ enum : uint32_t {
   ST_ZERO_VECTOR = 1u << 4,
   ST_CUDA = 1u << 5,
   ST_ARGUMENT = 1u << 6,
-  ST_GRID = 1u << 7
+  ST_GRID = 1u << 7,
+  ST_TIMEOUT = 1u << 8
 };
 
 enum : int { SHAPE_CIRCLE = 0, SHAPE_ELLIPSE = 1, SHAPE_CLUMP = 2, SHAPE_SEGMENT = 3 };

@@ -13,6 +13,7 @@
 
 #include "../../include/xdem_gpu.h"
 #include "mlp_host.h"
+#include "mlp_tc.cuh"
 
 using namespace xdem;
 
@@ -38,29 +39,30 @@ __global__ void k_mlp_publish(const float* theta, __nv_bfloat16* wb) {
 }
 
 // ---- evaluation ---------------------------------------------------------------------
+// rows of x through the network on the tensor cores (mlp_tc.cuh), 128 per
+// tile; *failed = 1 when a completion barrier timed out
 __global__ void __launch_bounds__(128) k_mlp_forward(MlpDev net, int64_t n, const float* x,
-                                                     float* y) {
-  __shared__ float feat[4][16 * 16];
-  __shared__ float out[4][16 * 2];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int64_t tiles = (n + 15) / 16;
-  for (int64_t tile = (int64_t)blockIdx.x * 4 + warp; tile < tiles; tile += (int64_t)gridDim.x * 4) {
-    for (int e = lane; e < 256; e += 32) {
-      const int r = e >> 4, c = e & 15;
-      const int64_t row = tile * 16 + r;
-      feat[warp][e] = (c < kMlpIn && row < n) ? x[row * kMlpIn + c] * net.scale[c] : 0.0f;
+                                                     float* y, int32_t* failed) {
+  __shared__ MlpTcSmem s;
+  mlp_tc_setup(s, net);
+  uint32_t phase = 0;
+  const int64_t tiles = (n + kTcRows - 1) / kTcRows;
+  for (int64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+    const int64_t row = tile * kTcRows + threadIdx.x;
+    float f[kMlpIn];
+#pragma unroll
+    for (int c = 0; c < kMlpIn; ++c) f[c] = row < n ? x[row * kMlpIn + c] * net.scale[c] : 0.0f;
+    float o0, o1;
+    if (!mlp_tc_tile(s, f, phase, o0, o1)) {
+      if (threadIdx.x == 0) *failed = 1;
+      break;
     }
-    __syncwarp();
-    mlp_forward_tile(net, feat[warp], out[warp]);
-    if (lane < 16) {
-      const int64_t row = tile * 16 + lane;
-      if (row < n) {
-        y[row * 2] = out[warp][lane * 2];
-        y[row * 2 + 1] = out[warp][lane * 2 + 1];
-      }
+    if (row < n) {
+      y[row * 2] = o0;
+      y[row * 2 + 1] = o1;
     }
-    __syncwarp();
   }
+  mlp_tc_teardown(s);
 }
 
 // ---- training ----------------------------------------------------------------------------
@@ -503,21 +505,29 @@ int32_t xdem_mlp_set_params(xdem_mlp m, const float* theta, const float* scale) 
 int32_t xdem_mlp_forward(xdem_mlp m, int64_t n, const float* x, float* y) {
   if (!m || n <= 0 || !x || !y) return XDEM_ERR_ARGUMENT;
   float *dx = nullptr, *dy = nullptr;
+  int32_t* dfail = nullptr;
+  int32_t failed = 0;
   cudaError_t e = cudaMalloc(&dx, sizeof(float) * kMlpIn * n);
   if (e == cudaSuccess) e = cudaMalloc(&dy, sizeof(float) * 2 * n);
+  if (e == cudaSuccess) e = cudaMalloc(&dfail, sizeof(int32_t));
+  if (e == cudaSuccess) e = cudaMemsetAsync(dfail, 0, sizeof(int32_t), m->stream);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(dx, x, sizeof(float) * kMlpIn * n, cudaMemcpyHostToDevice, m->stream);
   if (e == cudaSuccess) {
-    const int64_t tiles = (n + 15) / 16;
-    const int blocks = (int)std::min<int64_t>((tiles + 3) / 4, 148 * 8);
-    k_mlp_forward<<<blocks, 128, 0, m->stream>>>(m->dev(), n, dx, dy);
+    const int64_t tiles = (n + kTcRows - 1) / kTcRows;
+    const int blocks = (int)std::min<int64_t>(tiles, 148 * 4);
+    k_mlp_forward<<<blocks, 128, 0, m->stream>>>(m->dev(), n, dx, dy, dfail);
     e = cudaGetLastError();
   }
   if (e == cudaSuccess) e = cudaMemcpyAsync(y, dy, sizeof(float) * 2 * n, cudaMemcpyDeviceToHost, m->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(&failed, dfail, sizeof(int32_t), cudaMemcpyDeviceToHost, m->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(m->stream);
   cudaFree(dx);
   cudaFree(dy);
-  return e == cudaSuccess ? XDEM_OK : XDEM_ERR_CUDA;
+  cudaFree(dfail);
+  if (e != cudaSuccess) return XDEM_ERR_CUDA;
+  return failed ? XDEM_ERR_TIMEOUT : XDEM_OK;
 }
 
 int32_t xdem_mlp_gradient(xdem_mlp m, int64_t n, const float* x, const float* target,

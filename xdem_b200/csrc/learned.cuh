@@ -1,67 +1,52 @@
 // learned.cuh — the world side of the learned warm start (mlp.cuh):
 //
-//   k_mlp_warm    one warp per 16 listed closest-approach pairs: the pair's
+//   k_mlp_warm    tiles of 128 listed closest-approach pairs: the pair's
 //                 features from the FP64 state, the network on the tensor
-//                 cores, and (root fraction, contact logit) into w.warm for
-//                 the pair kernel that follows;
+//                 cores (tcgen05, mlp_tc.cuh), and (root fraction, contact
+//                 logit) into w.warm for the pair kernel that follows;
 //   k_harvest     training pairs from the last candidate list: features, the
 //                 root the plain FP64 Newton iteration converges to (as a
 //                 fraction of its analytic start) and whether the pair touches.
 #pragma once
-#include "mlp.cuh"
+#include "mlp_tc.cuh"
 #include "pairs.cuh"
 
 namespace xdem {
 
-// features of listed pair e (d = p_j + offset - p_i in ellipse i's frame)
-template <bool FOLD_BG>
-__device__ __forceinline__ void pair_features(const DevWorld& w, const MlpDev& net, const PairEntry& e,
-                                              double2 csa, double2 csb, float* f) {
-  const WorldScalars& ws = w.ws[sys_at(w, e.m)];
-  const double2 pa = w.pos[e.m], pb = w.pos[e.mj];
-  vec2<double> off, ovel;
-  image_offset(ws, e.code & 0xff, pa, pb, off, ovel);
-  const double dx = (pb.x + off.x) - pa.x, dy = (pb.y + off.y) - pa.y;
-  mlp_features(net, dx, dy, csa.x, csa.y, csb.x, csb.y, w.rad[e.m], w.asp[e.m], w.rad[e.mj],
-               w.asp[e.mj], f);
-}
-
 // warm starts of the entries [0, *count) of a pair list: entry i is pair
-// list ? list[i] : i.  LAW_CLOSEST worlds read the orientation cosines of
-// k_candidates.
+// list ? list[i] : i.  Tiles of 128 entries go through the network on the
+// tensor cores (mlp_tc.cuh); the features come from the pair's body records.
 template <int LAW>
 __global__ void __launch_bounds__(128) k_mlp_warm(DevWorld w, MlpDev net, const int32_t* count,
                                                   const int32_t* list) {
   if (stopped(w)) return;
-  __shared__ float feat[4][16 * 16];
-  __shared__ float out[4][16 * 2];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  __shared__ MlpTcSmem s;
+  mlp_tc_setup(s, net);
+  uint32_t phase = 0;
   const int n = *count;
-  const int tiles = (n + 15) / 16;
-  for (int tile = blockIdx.x * 4 + warp; tile < tiles; tile += gridDim.x * 4) {
-    const int i = tile * 16 + lane;
-    if (lane < 16) {
-      float f[kMlpIn] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
-      if (i < n) {
-        const PairEntry e = w.pairs[list ? list[i] : i];
-        double2 csa, csb;
-        if (LAW == LAW_CLOSEST) {
-          csa = w.body[e.m].cs;
-          csb = w.body[e.mj].cs;
-        } else {
-          csa = make_double2(cos(w.rot[e.m]), sin(w.rot[e.m]));
-          csb = make_double2(cos(w.rot[e.mj]), sin(w.rot[e.mj]));
-        }
-        pair_features<false>(w, net, e, csa, csb, f);
-      }
-#pragma unroll
-      for (int k = 0; k < 16; ++k) feat[warp][lane * 16 + k] = k < kMlpIn ? f[k] : 0.0f;
+  const int tiles = (n + kTcRows - 1) / kTcRows;
+  bool failed = false;
+  for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+    const int i = tile * kTcRows + threadIdx.x;
+    float f[kMlpIn] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+    if (i < n) {
+      const PairEntry e = w.pairs[list ? list[i] : i];
+      const BodyRec ba = w.body[e.m], bb = w.body[e.mj];
+      const WorldScalars& ws = w.ws[sys_at(w, e.m)];
+      vec2<double> off, ovel;
+      image_offset(ws, e.code & 0xff, ba.pos, bb.pos, off, ovel);
+      const double dx = (bb.pos.x + off.x) - ba.pos.x, dy = (bb.pos.y + off.y) - ba.pos.y;
+      mlp_features(net, dx, dy, ba.cs.x, ba.cs.y, bb.cs.x, bb.cs.y, ba.r, ba.asp, bb.r, bb.asp, f);
     }
-    __syncwarp();
-    mlp_forward_tile(net, feat[warp], out[warp]);
-    if (lane < 16 && i < n) w.warm[i] = make_float2(out[warp][lane * 2], out[warp][lane * 2 + 1]);
-    __syncwarp();
+    float o0, o1;
+    if (!mlp_tc_tile(s, f, phase, o0, o1)) {
+      failed = true;
+      break;
+    }
+    if (i < n) w.warm[i] = make_float2(o0, o1);
   }
+  mlp_tc_teardown(s);
+  if (failed && threadIdx.x == 0) raise(w.status, ST_TIMEOUT);
 }
 
 // Training pairs: every `stride`-th entry of the last candidate list whose two

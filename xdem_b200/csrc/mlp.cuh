@@ -7,11 +7,14 @@
 //   y0  the root of the reference's quartic (EllipticParticle.cpp:92-100,163)
 //       as a fraction of Newton's analytic start sqrt(δ + 1),
 //   y1  a contact logit.
-// Weights are BF16 and every product accumulates in FP32 on the tensor cores
-// (mma.sync m16n8k16): a warp evaluates 16 pairs at a time, and a layer's
-// accumulator fragments (rows = pairs, columns = units) are exactly the
-// A-operand fragments of the next layer, so activations never leave the
-// registers between layers.
+// Weights are BF16 and every product accumulates in FP32 on the tensor cores.
+// Inference (the world's warm start and xdem_mlp_forward) runs tcgen05 MMAs
+// with the accumulator in tensor memory, 128 rows per CTA (mlp_tc.cuh).  The
+// training kernels (learn.cu) keep a warp-level form built from the helpers
+// below (mma.sync m16n8k16): a warp evaluates 16 samples at a time, and a
+// layer's accumulator fragments (rows = samples, columns = units) are exactly
+// the A-operand fragments of the next layer, so the backward pass finds every
+// activation it needs in registers.
 //
 // Parameters live in one FP32 vector (the training master copy) with the
 // layout of MlpLayout; BF16 copies of the weight matrices, row-major
@@ -119,57 +122,6 @@ __device__ __forceinline__ void act_to_a(const float (&acc)[8][4], uint32_t (&A)
     A[s][2] = pack_bf16(silu(acc[2 * s + 1][0]), silu(acc[2 * s + 1][1]));
     A[s][3] = pack_bf16(silu(acc[2 * s + 1][2]), silu(acc[2 * s + 1][3]));
   }
-}
-
-// Forward pass of 16 rows held by one warp.  feat: the warp's [16][16] FP32
-// inputs in shared memory (columns 7..15 zero, already scaled); out: [16][2].
-// Every lane of the warp must call it.
-__device__ __forceinline__ void mlp_forward_tile(const MlpDev& net, const float* feat, float* out) {
-  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-  uint32_t A1[4];
-  A1[0] = pack_bf16(feat[g * 16 + 2 * t], feat[g * 16 + 2 * t + 1]);
-  A1[1] = pack_bf16(feat[(g + 8) * 16 + 2 * t], feat[(g + 8) * 16 + 2 * t + 1]);
-  A1[2] = pack_bf16(feat[g * 16 + 2 * t + 8], feat[g * 16 + 2 * t + 9]);
-  A1[3] = pack_bf16(feat[(g + 8) * 16 + 2 * t + 8], feat[(g + 8) * 16 + 2 * t + 9]);
-  float acc[8][4];
-  const float* th = net.theta;
-  // layer 1: K = 16 (one k-step)
-#pragma unroll
-  for (int j = 0; j < 8; ++j) {
-    const float b0 = th[MlpLayout::B1 + 8 * j + 2 * t], b1 = th[MlpLayout::B1 + 8 * j + 2 * t + 1];
-    acc[j][0] = b0;
-    acc[j][1] = b1;
-    acc[j][2] = b0;
-    acc[j][3] = b1;
-    uint32_t w0, w1;
-    load_b(net.wb + MlpBf16Layout::W1, kMlpK1, j, 0, g, t, w0, w1);
-    mma_bf16(acc[j], A1, w0, w1);
-  }
-  uint32_t A[4][4];
-  act_to_a(acc, A);
-  mlp_hidden(net.wb + MlpBf16Layout::W2, th + MlpLayout::B2, A, g, t, acc);
-  act_to_a(acc, A);
-  mlp_hidden(net.wb + MlpBf16Layout::W3, th + MlpLayout::B3, A, g, t, acc);
-  act_to_a(acc, A);
-  // layer 4: one n-tile of 8 outputs (2 used), K = 64
-  float o[4];
-  o[0] = th[MlpLayout::B4 + 2 * t];
-  o[1] = th[MlpLayout::B4 + 2 * t + 1];
-  o[2] = o[0];
-  o[3] = o[1];
-#pragma unroll
-  for (int s = 0; s < 4; ++s) {
-    uint32_t w0, w1;
-    load_b(net.wb + MlpBf16Layout::W4, kMlpH, 0, s, g, t, w0, w1);
-    mma_bf16(o, A[s], w0, w1);
-  }
-  if (t == 0) {  // columns 0 and 1
-    out[g * 2 + 0] = o[0];
-    out[g * 2 + 1] = o[1];
-    out[(g + 8) * 2 + 0] = o[2];
-    out[(g + 8) * 2 + 1] = o[3];
-  }
-  __syncwarp();
 }
 
 // The features of a closest-approach pair (see the file comment), FP32,
