@@ -465,6 +465,11 @@ int32_t xdem_mlp_get_params(xdem_mlp m, float* theta, float* scale);
 int32_t xdem_mlp_set_params(xdem_mlp m, const float* theta, const float* scale);
 /* forward pass of n rows of 7 features (host arrays; y: 2 per row) */
 int32_t xdem_mlp_forward(xdem_mlp m, int64_t n, const float* x, float* y);
+/* Self-test of the tensor-core kernels' bounded waits (no reference
+   counterpart): one CTA waits on a completion barrier that nothing arrives
+   on; returns XDEM_ERR_TIMEOUT once the wait limit has passed, with the
+   kernel's elapsed milliseconds in *ms. */
+int32_t xdem_selftest_bounded_wait(double* ms);
 /* gradient of the mean loss over n samples (host arrays: x 7 per row,
    target root fraction or NaN where no root exists, contact 0/1):
    (y0 - target)^2 where the target exists + 0.1 * BCE(y1, contact) */

@@ -130,3 +130,18 @@ def test_warm_start_same_results_fewer_iterations(trained, precision):
         # only the few pairs the mixed path hands to the FP64 construction
         # take the warm start
         assert i1 <= i0, (i0, i1)
+
+
+def test_tensor_core_barrier_wait_is_bounded():
+    """A completion barrier that nothing arrives on: the kernels' wait gives up
+    after its limit and reports a timeout instead of hanging."""
+    import ctypes as C
+    from xdem_b200 import abi
+    lib = abi.load_library()
+    ms = C.c_double(0.0)
+    assert lib.xdem_selftest_bounded_wait(C.byref(ms)) == abi.ERR_TIMEOUT
+    assert 0.0 < ms.value < 5000.0
+    # the context stays usable
+    net = Mlp(seed=3)
+    x = _samples(200, 4)[0]
+    assert np.all(np.isfinite(net.forward(x)))

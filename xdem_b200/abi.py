@@ -263,6 +263,7 @@ def load_library(path=LIB_PATH):
         "xdem_mlp_get_params": (C.c_int32, [W, _f, _f]),
         "xdem_mlp_set_params": (C.c_int32, [W, _f, _f]),
         "xdem_mlp_forward": (C.c_int32, [W, C.c_int64, _f, _f]),
+        "xdem_selftest_bounded_wait": (C.c_int32, [_d]),
         "xdem_mlp_gradient": (C.c_int32, [W, C.c_int64, _f, _f, _f, _f, _f]),
         "xdem_mlp_add_samples": (C.c_int32, [W, C.c_int64, _f, _f, _f]),
         "xdem_mlp_dataset": (C.c_int32, [W, P(C.c_int64), _f, _f, _f]),

@@ -65,6 +65,18 @@ __global__ void __launch_bounds__(128) k_mlp_forward(MlpDev net, int64_t n, cons
   mlp_tc_teardown(s);
 }
 
+// a completion barrier that nothing arrives on: the bounded wait gives up
+__global__ void k_selftest_wait(int32_t* timed_out) {
+  __shared__ uint64_t bar;
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  const bool ok = mbar_wait(&bar, 0);
+  if (threadIdx.x == 0) *timed_out = ok ? 0 : 1;
+}
+
 // ---- training ----------------------------------------------------------------------------
 // shared memory of one training block (4 warps x 16 samples)
 struct TrainSmem {
@@ -528,6 +540,30 @@ int32_t xdem_mlp_forward(xdem_mlp m, int64_t n, const float* x, float* y) {
   cudaFree(dfail);
   if (e != cudaSuccess) return XDEM_ERR_CUDA;
   return failed ? XDEM_ERR_TIMEOUT : XDEM_OK;
+}
+
+int32_t xdem_selftest_bounded_wait(double* ms) {
+  int32_t* d = nullptr;
+  int32_t h = 0;
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  cudaError_t e = cudaMalloc(&d, sizeof(int32_t));
+  if (e == cudaSuccess) e = cudaEventCreate(&ev[0]);
+  if (e == cudaSuccess) e = cudaEventCreate(&ev[1]);
+  if (e == cudaSuccess) e = cudaEventRecord(ev[0]);
+  if (e == cudaSuccess) {
+    k_selftest_wait<<<1, 32>>>(d);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaEventRecord(ev[1]);
+  if (e == cudaSuccess) e = cudaMemcpy(&h, d, sizeof(int32_t), cudaMemcpyDeviceToHost);
+  float t = 0.0f;
+  if (e == cudaSuccess) e = cudaEventElapsedTime(&t, ev[0], ev[1]);
+  if (ms) *ms = t;
+  for (cudaEvent_t x : ev)
+    if (x) cudaEventDestroy(x);
+  cudaFree(d);
+  if (e != cudaSuccess) return XDEM_ERR_CUDA;
+  return h ? XDEM_ERR_TIMEOUT : XDEM_OK;
 }
 
 int32_t xdem_mlp_gradient(xdem_mlp m, int64_t n, const float* x, const float* target,
