@@ -154,7 +154,7 @@ enum KernelKind {
 };
 const char* const kKindNames[KK_COUNT] = {
     "k_modify_position", "k_bin", "k_scan", "k_scatter", "k_candidates", "k_pair_forces",
-    "k_finish_slots", "k_collect", "k_integrate", "k_rattlers", "k_stress_partial",
+    "k_pairs_done", "k_collect", "k_integrate", "k_rattlers", "k_stress_partial",
     "k_stress_final", "k_end_of_step", "k_scale_positions", "k_background_velocity",
     "k_kinetic_energy", "k_resort", "k_stage", "k_pair_fallback", "k_mlp_warm", "k_vl_check",
     "k_vl_build"};
@@ -248,7 +248,7 @@ void launch_update_phases(xdem_world_s* w, int record) {
     LAUNCH(w, KK_PAIRS,
            k_pair_forces<FOLD_BG, LAW><<<pb, 128, 0, w->stream>>>(w->dw, w->par, record));
   }
-  LAUNCH(w, KK_FINISH, k_finish_slots<<<nb, 128, 0, w->stream>>>(w->dw, w->par));
+  LAUNCH(w, KK_FINISH, k_pairs_done<<<1, 32, 0, w->stream>>>(w->dw));
 }
 
 template <bool FOLD_BG>

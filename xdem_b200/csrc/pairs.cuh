@@ -4,14 +4,14 @@
 //                   (PeriodicBoundaryWorld.cpp:47-84, LeesEdwardsBoundaryWorld.cpp:
 //                   128-204) with its filters and 200-candidate cap, a cheap
 //                   coarse test, and a compact list of the pairs that pass;
+//                   it also carries over the history of old contacts whose
+//                   pair was not a candidate this step, as the reference's map
+//                   entries survive;
 //   k_pair_forces   one thread per listed pair: image offset, contact geometry,
 //                   history, contact force and torques (BaseParticle.cpp:27-98),
 //                   written to the owner's slot for that pair;
-//   k_finish_slots  one thread per owner: carries over the history of pairs
-//                   that were not candidates this step, as the reference's map
-//                   entries survive, and registers every contact with its
-//                   partner for the partner's force sum (kept out of the heavy
-//                   pair kernel, whose warps would otherwise wait on the atomic).
+// both register every contact they write with its partner (an atomic slot in
+// the partner's incoming list) for the partner's force sum.
 // Splitting the light scan from the heavy geometry keeps warps full on the
 // FP64 ellipse solvers.  A candidate rejected by the coarse test is still a
 // candidate: its history is dropped, as the reference erases it
@@ -181,13 +181,59 @@ __device__ __forceinline__ void scan_cells(const DevWorld& w, const WorldScalars
   }
 }
 
+// Registers the contact in the owner's slot (m, slot) with its partner at
+// memory position mj, for the partner's force sum.  The arrival order is
+// free: k_collect orders the references by owner id.
+__device__ __forceinline__ void register_contact(const DevWorld& w, int mj, int m, int slot,
+                                                 uint32_t& st) {
+  const int pos = atomicAdd(&w.incnt[mj], 1);
+  if (pos < w.K) w.inref[(size_t)pos * w.n + mj] = (uint32_t)m * (uint32_t)w.K + (uint32_t)slot;
+  else st |= ST_CAPACITY;
+}
+
+// The history of the owner's old contacts whose pair was not a candidate this
+// step survives unchanged, as the reference's map entries do: copied to the
+// slots after the k listed ones (which only the pair kernels write) and
+// registered with the partner.  Returns the owner's slot count.
+__device__ __forceinline__ int carry_over(const DevWorld& w, const Slots& old, const Slots& cur,
+                                          int m, int nold, uint32_t seen, int k, uint32_t& st) {
+  const int n = w.n, K = w.K;
+  for (int o = 0; o < nold; ++o) {
+    const size_t oi = (size_t)o * n + m;
+    const int partner = old.partner[oi];
+    if (partner < 0 || (seen & (1u << o))) continue;
+    if (k >= K) {
+      st |= ST_CAPACITY;
+      break;
+    }
+    const size_t ci = (size_t)k * n + m;
+    cur.partner[ci] = partner;
+    cur.n[ci] = old.n[oi];
+    cur.s[ci] = old.s[oi];
+    cur.damp[ci] = old.damp[oi];
+    cur.f[ci] = old.f[oi];
+    cur.t1[ci] = old.t1[oi];
+    cur.t2[ci] = old.t2[oi];
+    cur.b[ci] = old.b[oi];
+    cur.cp[ci] = old.cp[oi];
+    cur.bv1[ci] = old.bv1[oi];
+    cur.bv2[ci] = old.bv2[oi];
+    cur.fn[ci] = old.fn[oi];
+    cur.ft[ci] = old.ft[oi];
+    register_contact(w, w.mpos[partner], m, k, st);
+    ++k;
+  }
+  return k;
+}
+
 // One thread per owner m.  Cell entries are read from the cell-ordered
 // screening records (cell_scr, cell_up), so a neighbour cell is one
 // contiguous run of 20-byte records; the distance screen runs in FP32 on
 // positions relative to the cell corners, and only candidates within its
 // rounding margin of the threshold take the reference's FP64 test.  Old slots whose partner sits in one of the nine
 // cells (and passes the same filters) are marked seen: such a pair was a
-// candidate, so its history is replaced or dropped rather than carried over.
+// candidate, so its history is replaced or dropped; the others are carried
+// over here.
 // For an all-ellipse world the thread also leaves (cos, sin) of its
 // orientation for the pair kernel, computed once per body instead of per pair.
 template <int LAW>
@@ -250,8 +296,7 @@ __global__ void __launch_bounds__(128) k_candidates(DevWorld w, int par) {
         if (hit) seen |= 1u << z;
       }
     }
-    cur.count[m] = nlist;
-    w.seen[m] = seen;
+    cur.count[m] = carry_over(w, old, cur, m, nold, seen, nlist, st);
   }
   // reserve room in the pair list for the whole block at once (one atomic
   // per block on the shared counter)
@@ -412,67 +457,20 @@ __global__ void __launch_bounds__(128, 4) k_pair_forces(DevWorld w, int par, int
       cur.fn[ci] = make_double2(fn.x, fn.y);
       cur.ft[ci] = make_double2(fs.x, fs.y);
     }
+    register_contact(w, mj, m, slot, st);
   }
   flush_warp(w, st, n_solves, n_iters, n_capped);
   if (WARM) flush_warm(w, w_off, w_used, w_rej, w_rest, w_right);
 }
 
-// ---- phase C --------------------------------------------------------------------
-__global__ void __launch_bounds__(128) k_finish_slots(DevWorld w, int par) {
+// ---- end of the update ----------------------------------------------------------
+// The pair kernels have consumed this step's lists: the counters start again
+// from zero for the next update.
+__global__ void k_pairs_done(DevWorld w) {
   if (stopped(w)) return;
-  const int m = blockIdx.x * blockDim.x + threadIdx.x;
-  if (m == 0) {  // phase B has consumed the lists
-    w.ws->last_pairs = *w.npairs;
-    *w.npairs = 0;
-    *w.nfallback = 0;
-  }
-  if (m >= w.n) return;
-  const int n = w.n, K = w.K;
-  const Slots& old = w.slots[par];
-  const Slots& cur = w.slots[par ^ 1];
-  uint32_t st = 0;
-  const uint32_t seen = w.seen[m];
-  const int nold = min(old.count[m], K);
-  int k = cur.count[m];
-  // the contacts listed this step
-  for (int s = 0; s < k; ++s) {
-    const int partner = cur.partner[(size_t)s * n + m];
-    if (partner < 0) continue;
-    const int mj = w.mpos[partner];
-    const int pos = atomicAdd(&w.incnt[mj], 1);
-    if (pos < K) w.inref[(size_t)pos * n + mj] = (uint32_t)m * (uint32_t)K + (uint32_t)s;
-    else st |= ST_CAPACITY;
-  }
-  for (int o = 0; o < nold; ++o) {
-    size_t oi = (size_t)o * n + m;
-    int partner = old.partner[oi];
-    if (partner < 0 || (seen & (1u << o))) continue;
-    if (k >= K) {
-      st |= ST_CAPACITY;
-      break;
-    }
-    size_t ci = (size_t)k * n + m;
-    cur.partner[ci] = partner;
-    cur.n[ci] = old.n[oi];
-    cur.s[ci] = old.s[oi];
-    cur.damp[ci] = old.damp[oi];
-    cur.f[ci] = old.f[oi];
-    cur.t1[ci] = old.t1[oi];
-    cur.t2[ci] = old.t2[oi];
-    cur.b[ci] = old.b[oi];
-    cur.cp[ci] = old.cp[oi];
-    cur.bv1[ci] = old.bv1[oi];
-    cur.bv2[ci] = old.bv2[oi];
-    cur.fn[ci] = old.fn[oi];
-    cur.ft[ci] = old.ft[oi];
-    int mj = w.mpos[partner];
-    int pos = atomicAdd(&w.incnt[mj], 1);
-    if (pos < K) w.inref[(size_t)pos * n + mj] = (uint32_t)m * (uint32_t)K + (uint32_t)k;
-    else st |= ST_CAPACITY;
-    ++k;
-  }
-  cur.count[m] = k;
-  raise(w.status, st);
+  w.ws->last_pairs = *w.npairs;
+  *w.npairs = 0;
+  *w.nfallback = 0;
 }
 
 }  // namespace xdem

@@ -24,7 +24,8 @@ __device__ __forceinline__ bool is_normal_f(float x) {
   return a >= 1.17549435e-38f && a <= 3.40282347e38f;
 }
 
-// history, force and torques of one touching pair, written to its slot
+// history, force and torques of one touching pair, written to its slot and
+// registered with the partner
 __device__ __forceinline__ void write_contact_m(const DevWorld& w, const WorldScalars& ws,
                                                 const PairEntry& e, const BodyRec& ba,
                                                 const BodyRec& bb, const PState& a,
@@ -98,7 +99,7 @@ __device__ __forceinline__ void write_contact_m(const DevWorld& w, const WorldSc
     cur.fn[ci] = make_double2((double)fnx, (double)fny);
     cur.ft[ci] = make_double2((double)fsx, (double)fsy);
   }
-  (void)st;
+  register_contact(w, mj, m, slot, st);
 }
 
 __device__ __forceinline__ void count_solve(uint32_t it, uint32_t& n_solves, uint32_t& n_iters) {

@@ -117,8 +117,9 @@ __global__ void __launch_bounds__(128) k_vl_build(DevWorld w) {
   w.vl_cnt[m] = cnt;
 }
 
-// k_candidates with the lists: same outputs (slot counts, seen masks, the
-// compact pair list, orientation cosines), the same filters and tests.
+// k_candidates with the lists: same outputs (slot counts, carried-over
+// history, the compact pair list, orientation cosines), the same filters and
+// tests.
 template <int LAW>
 __global__ void __launch_bounds__(128) k_candidates_vl(DevWorld w, int par) {
   if (stopped(w)) return;
@@ -244,8 +245,7 @@ __global__ void __launch_bounds__(128) k_candidates_vl(DevWorld w, int par) {
         if (hit) seen |= 1u << z;
       }
     }
-    cur.count[m] = nlist;
-    w.seen[m] = seen;
+    cur.count[m] = carry_over(w, old, cur, m, nold, seen, nlist, st);
   }
   // reserve room in the pair list for the whole block at once
   const unsigned full = 0xffffffffu;
