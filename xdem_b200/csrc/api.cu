@@ -737,7 +737,6 @@ int32_t set_particles_impl(xdem_world_s* w, const xdem_particles* P, const std::
   CK(w, B.alloc(&d.incnt, n));
   CK(w, B.alloc(&d.inref, ks));
   CK(w, cudaMemsetAsync(d.incnt, 0, sizeof(int32_t) * n, s));
-  CK(w, B.alloc(&d.seen, n));
   CK(w, B.alloc(&d.pairs, ks));
   CK(w, B.alloc(&d.npairs, 1));
   CK(w, cudaMemsetAsync(d.npairs, 0, sizeof(int32_t), s));

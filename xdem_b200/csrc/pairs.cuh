@@ -85,6 +85,65 @@ __device__ __forceinline__ bool coarse_pass(int shape_i, int shape_j, double r_i
   return true;
 }
 
+// Shape of a body for the centre-line screen of two ellipses: (cos, sin) of
+// its major axis and its semi-axes, FP32.
+struct AxisShape {
+  float c, s, a, b;
+};
+
+// the screen's record of the ellipse at m; the orientation is reduced to
+// [-pi, pi] in FP64 before the FP32 sine and cosine
+__device__ __forceinline__ AxisShape axis_shape(const DevWorld& w, int m) {
+  double r = w.rot[m];
+  r -= 6.283185307179586 * rint(r * 0.15915494309189535);
+  AxisShape e;
+  __sincosf((float)r, &e.s, &e.c);
+  const double a = w.rad[m];
+  e.a = (float)a;
+  e.b = (float)(a / w.asp[m]);
+  return e;
+}
+
+// True when two ellipses are separated along the line of their centres: the
+// centre distance |d| exceeds the sum of their half-widths along d̂, so their
+// projections on that line are disjoint.  The exact distance of closest
+// approach along d̂ is at most that sum, and two disjoint ellipses do not
+// intersect, so neither law has a contact there and the pair's history is
+// erased (BaseParticle.cpp:95), as it is for a candidate that is not listed.
+// The screen serves the mixed-precision path only: the reference's own
+// construction can report a contact for such a pair when its Newton result
+// is not finite (it then takes d' = 1 + a2', EllipticParticle.cpp:168-170),
+// and the FP64 path reproduces the reference pair for pair.  With
+// H = half-width * |d| = sqrt(a²(d·k)² + b²(d×k)²) the test is
+// |d|² > H_i + H_j; the 1e-3 relative margin is far above the FP32 rounding
+// of d, the angles and the axes (below 1e-5 relative).
+__device__ __forceinline__ bool separated_on_centre_line(float dx, float dy, const AxisShape& i,
+                                                         const AxisShape& j) {
+  const float pi = dx * i.c + dy * i.s, qi = dx * i.s - dy * i.c;
+  const float pj = dx * j.c + dy * j.s, qj = dx * j.s - dy * j.c;
+  const float hi = sqrtf(i.a * i.a * pi * pi + i.b * i.b * qi * qi);
+  const float hj = sqrtf(j.a * j.a * pj * pj + j.b * j.b * qj * qj);
+  return dx * dx + dy * dy > (hi + hj) * 1.001f;
+}
+
+// the centre-line screen applies to mixed-precision worlds of ellipses under
+// one law
+template <int LAW>
+__device__ __forceinline__ bool centre_line_screen(const DevWorld& w) {
+  return (LAW == LAW_CLOSEST || LAW == LAW_INTERSECTION) && w.precision == XDEM_PRECISION_MIXED;
+}
+
+// the owner's record for the screen, from the (cos, sin) of its body record
+template <int LAW>
+__device__ __forceinline__ AxisShape owner_axis_shape(const DevWorld& w, int m, double2 cs) {
+  AxisShape e{0.0f, 0.0f, 0.0f, 0.0f};
+  if (centre_line_screen<LAW>(w)) {
+    const double a = w.rad[m];
+    e = AxisShape{(float)cs.x, (float)cs.y, (float)a, (float)(a / w.asp[m])};
+  }
+  return e;
+}
+
 // ---- phase A --------------------------------------------------------------------
 // Cell (ix+dx, iy+dy) of the reference's 3x3 scan with its image kind
 // (PeriodicBoundaryWorld.cpp:47-84; LeesEdwardsBoundaryWorld.cpp:128-204 for
@@ -120,7 +179,7 @@ __device__ __forceinline__ void scan_cells(const DevWorld& w, const WorldScalars
                                            int shape_i, double r_i, double orad_i,
                                            const Slots& old, int nold, int& nlist,
                                            int32_t* list_mj, int32_t* list_code, uint32_t& st,
-                                           uint32_t& matched) {
+                                           uint32_t& matched, const AxisShape& shape_ax) {
   const int n = w.n, K = w.K;
   // the owner relative to its cell's corner, in FP32 (see k_scatter)
   const float rxi = (float)(pi.x - (ws.xmin + ix * G.lx));
@@ -165,6 +224,15 @@ __device__ __forceinline__ void scan_cells(const DevWorld& w, const WorldScalars
         else
           pass = coarse_pass<LAW>(0, 0, r_i, w.screen_r[mj], orad_i, w.screen_r[mj], pi, pj, off);
         if (!pass) continue;
+      }
+      if (centre_line_screen<LAW>(w)) {
+        // the same FP64 image offset as the candidate lists' test (verlet.cuh)
+        const double2 pj = w.cell_pos[q];
+        vec2<double> off, ovel;
+        image_offset(ws, kind, pi, pj, off, ovel);
+        if (separated_on_centre_line((float)((pj.x + off.x) - pi.x), (float)((pj.y + off.y) - pi.y),
+                                     shape_ax, axis_shape(w, w.cell_mem[q])))
+          continue;
       }
       if (nlist >= K) {
         st |= ST_CAPACITY;
@@ -250,17 +318,16 @@ __global__ void __launch_bounds__(128) k_candidates(DevWorld w, int par) {
   int32_t list_mj[kMaxSlots];
   int32_t list_code[kMaxSlots];
   if (valid) {
-    {
-      // this step's record of the body for the pair kernels; an ellipse's
-      // (cos, sin) is computed once per body instead of once per pair
-      double2 cs = make_double2(0.0, 0.0);
-      if (LAW == LAW_CLOSEST || LAW == LAW_INTERSECTION ||
-          (LAW == LAW_ANY && w.shape[m] == SHAPE_ELLIPSE)) {
-        const double r = w.rot[m];
-        cs = make_double2(cos(r), sin(r));
-      }
-      write_body(w, m, cs);
+    // this step's record of the body for the pair kernels; an ellipse's
+    // (cos, sin) is computed once per body instead of once per pair
+    double2 cs = make_double2(0.0, 0.0);
+    if (LAW == LAW_CLOSEST || LAW == LAW_INTERSECTION ||
+        (LAW == LAW_ANY && w.shape[m] == SHAPE_ELLIPSE)) {
+      const double r = w.rot[m];
+      cs = make_double2(cos(r), sin(r));
     }
+    write_body(w, m, cs);
+    const AxisShape shape_ax = owner_axis_shape<LAW>(w, m, cs);
     Grid G = grid_of(ws);
     const int id_i = w.id_of[m];
     const int nold = min(old.count[m], K);
@@ -274,7 +341,7 @@ __global__ void __launch_bounds__(128) k_candidates(DevWorld w, int par) {
       const int iy = cell_of(pi.y, ws.ymin, G.ly, G.ny);
       uint32_t matched = 0;
       scan_cells<LAW>(w, ws, G, m, ix, iy, pi, id_i, up_i, shape_i, r_i, orad_i, old, nold, nlist,
-                      list_mj, list_code, st, matched);
+                      list_mj, list_code, st, matched, shape_ax);
       // old partners among the candidates: the listed ones are; the others
       // are looked up in the nine cells
       seen = matched;

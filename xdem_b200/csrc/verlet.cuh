@@ -121,7 +121,7 @@ __global__ void __launch_bounds__(128) k_vl_build(DevWorld w) {
 // history, the compact pair list, orientation cosines), the same filters and
 // tests.
 template <int LAW>
-__global__ void __launch_bounds__(128) k_candidates_vl(DevWorld w, int par) {
+__global__ void __launch_bounds__(128, 7) k_candidates_vl(DevWorld w, int par) {
   if (stopped(w)) return;
   const int m = blockIdx.x * blockDim.x + threadIdx.x;
   const bool valid = m < w.n;
@@ -134,17 +134,16 @@ __global__ void __launch_bounds__(128) k_candidates_vl(DevWorld w, int par) {
   int32_t list_mj[kMaxSlots];
   int32_t list_code[kMaxSlots];
   if (valid) {
-    {
-      // this step's record of the body for the pair kernels; an ellipse's
-      // (cos, sin) is computed once per body instead of once per pair
-      double2 cs = make_double2(0.0, 0.0);
-      if (LAW == LAW_CLOSEST || LAW == LAW_INTERSECTION ||
-          (LAW == LAW_ANY && w.shape[m] == SHAPE_ELLIPSE)) {
-        const double r = w.rot[m];
-        cs = make_double2(cos(r), sin(r));
-      }
-      write_body(w, m, cs);
+    // this step's record of the body for the pair kernels; an ellipse's
+    // (cos, sin) is computed once per body instead of once per pair
+    double2 cs = make_double2(0.0, 0.0);
+    if (LAW == LAW_CLOSEST || LAW == LAW_INTERSECTION ||
+        (LAW == LAW_ANY && w.shape[m] == SHAPE_ELLIPSE)) {
+      const double r = w.rot[m];
+      cs = make_double2(cos(r), sin(r));
     }
+    write_body(w, m, cs);
+    const AxisShape shape_ax = owner_axis_shape<LAW>(w, m, cs);
     const Grid G = grid_of(ws);
     const int id_i = w.id_of[m];
     const int nold = min(old.count[m], K);
@@ -161,7 +160,7 @@ __global__ void __launch_bounds__(128) k_candidates_vl(DevWorld w, int par) {
       uint32_t matched = 0;
       if (cnt < 0) {  // the list overflowed at its build: the full scan
         scan_cells<LAW>(w, ws, G, m, ix, iy, pi, id_i, up_i, shape_i, r_i, orad_i, old, nold,
-                        nlist, list_mj, list_code, st, matched);
+                        nlist, list_mj, list_code, st, matched, shape_ax);
       } else {
         // the 200-candidate cap (PeriodicBoundaryWorld.cpp:75-78): the nine
         // cells' record counts bound each kind's candidates; where a bound
@@ -205,6 +204,10 @@ __global__ void __launch_bounds__(128) k_candidates_vl(DevWorld w, int par) {
             pass = coarse_pass<LAW>(0, 0, r_i, w.screen_r[mj], orad_i, w.screen_r[mj], pi, pj,
                                     off);
           if (!pass) continue;
+          if (centre_line_screen<LAW>(w) &&
+              separated_on_centre_line((float)((pj.x + off.x) - pi.x), (float)((pj.y + off.y) - pi.y),
+                                       shape_ax, axis_shape(w, mj)))
+            continue;
           if (nlist >= K) {
             st |= ST_CAPACITY;
             continue;

@@ -160,7 +160,6 @@ struct DevWorld {
   Slots slots[2];
   int32_t* incnt;   // [n] contacts owned by lower ids
   uint32_t* inref;  // [K*n] owner position*K + slot of those contacts
-  uint32_t* seen;   // [n] old slots whose pair was a candidate this step
   PairEntry* pairs; // [K*n] pairs that passed the candidate scan
   int32_t* npairs;  // number of listed pairs
   int32_t* fallback;   // [K*n] mixed precision: listed pairs deferred to the FP64 construction
