@@ -505,6 +505,11 @@ def measure(work, precision, args, dist, full=True, net=None):
            "done": done, "contacts": contacts, "launches": int(launches), "clocks": clk,
            "newton": {"solves_per_step": solves / max(done, 1),
                       "iterations_per_solve": iters / max(solves, 1), "capped_solves": capped}}
+    lists = w.candidate_list_stats()
+    if lists["capacity"] > 0:
+        out["candidate_lists"] = {"builds_per_step": lists["builds"] / max(done, 1),
+                                  "entries_per_particle": lists["entries"] / n,
+                                  "longest": lists["longest"], "capacity": lists["capacity"]}
     if net is not None:
         ws = warm_stats(w)
         off = max(ws["offered"], 1)
@@ -688,6 +693,8 @@ def main():
         "clocks": head["clocks"], "status": head["status"], "newton": head["newton"],
         "cpu_baseline": cpu,
     }
+    if "candidate_lists" in head:
+        line["candidate_lists"] = head["candidate_lists"]
     if loop is not None:
         line["per_system_loop"] = {"value": loop["value"], "ms_per_step": loop["ms_per_step"],
                                    "what": "one world per system, each run for the K steps in "

@@ -208,3 +208,37 @@ def test_mixed_lees_edwards_history_and_mean_shear_stress():
     # the perturbation
     own = len(keys[0] ^ keys[1])
     assert len(keys[0] ^ keys[2]) <= max(0.01 * len(keys[0]), 2.0 * own), (own, len(keys[0] ^ keys[2]))
+
+
+def test_deep_pairs_beside_the_other_pairs_are_bit_identical():
+    """A mixed closest-approach step evaluates the pairs that the centre-line
+    screen classed deep (centre distance below 0.7 of the half-width sum) on
+    a second stream, beside the other pairs and their deferred FP64 pass.
+    With per-kernel profiling on, the same kernels run one after another on
+    one stream.  Both orders give the same state, contacts, stress and Newton
+    counters bit for bit, through direct steps and through the CUDA-graph
+    chunks of a run, and the deep pass ran."""
+    p, contacts, prm = dense_ellipse_case(n=4000, seed=35, kind=abi.WORLD_LEES_EDWARDS,
+                                          shift_rate=0.1)
+    worlds = [World(_mixed(prm)), World(_mixed(prm))]
+    worlds[1].set_profiling(True)
+    for w in worlds:
+        w.raise_mask = ~abi.ERR_NEWTON
+        w.set_particles(p)
+        w.set_contacts(contacts)
+        w.reset_newton_stats()
+    ctl = make_control(update_stress=True)
+    for w in worlds:
+        for _ in range(3):
+            w.takeTimeStep()
+        w.run(70, ctl)
+    assert worlds[1].profile()["k_pair_deep"][0] == 73
+    s0, s1 = worlds[0].get_state(), worlds[1].get_state()
+    for k in s0:
+        np.testing.assert_array_equal(s0[k], s1[k], err_msg=k)
+    c0, c1 = worlds[0].get_contacts(), worlds[1].get_contacts()
+    for k in c0:
+        np.testing.assert_array_equal(c0[k], c1[k], err_msg=k)
+    assert len(c0["id_i"]) > 4000
+    np.testing.assert_array_equal(worlds[0].getStress(), worlds[1].getStress())
+    assert worlds[0].newton_stats() == worlds[1].newton_stats()

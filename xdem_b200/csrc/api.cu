@@ -56,6 +56,11 @@ struct xdem_world_s {
   xdem_params prm{};
   cudaStream_t stream = nullptr;
   bool own_stream = false;
+  // second stream of the contact update (mixed precision, closest approach):
+  // the deep pairs run on it beside the other pairs; fork/join events order
+  // it with `stream`
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
   DevWorld dw{};
   DeviceBuffers particle_bufs;
   WorldScalars* ws = nullptr;
@@ -150,14 +155,14 @@ enum KernelKind {
   KK_MODIFY = 0, KK_BIN, KK_SCAN, KK_SCATTER, KK_CANDIDATES, KK_PAIRS, KK_FINISH, KK_COLLECT,
   KK_INTEGRATE, KK_RATTLERS, KK_STRESS_PARTIAL, KK_STRESS_FINAL, KK_END_OF_STEP, KK_SCALE,
   KK_BACKGROUND, KK_KE, KK_RESORT, KK_STAGE, KK_FALLBACK, KK_WARM, KK_VL_CHECK, KK_VL_BUILD,
-  KK_COUNT
+  KK_DEEP, KK_COUNT
 };
 const char* const kKindNames[KK_COUNT] = {
     "k_modify_position", "k_bin", "k_scan", "k_scatter", "k_candidates", "k_pair_forces",
     "k_pairs_done", "k_collect", "k_integrate", "k_rattlers", "k_stress_partial",
     "k_stress_final", "k_end_of_step", "k_scale_positions", "k_background_velocity",
     "k_kinetic_energy", "k_resort", "k_stage", "k_pair_fallback", "k_mlp_warm", "k_vl_check",
-    "k_vl_build"};
+    "k_vl_build", "k_pair_deep"};
 
 void prof_begin(xdem_world_s* w, int kind) {
   if (!w->prof_on) return;
@@ -225,7 +230,22 @@ void launch_update_phases(xdem_world_s* w, int record) {
   } else {
     LAUNCH(w, KK_CANDIDATES, k_candidates<LAW><<<nb, 128, 0, w->stream>>>(w->dw, w->par));
   }
-  if (w->prm.precision == XDEM_PRECISION_MIXED) {
+  if (w->prm.precision == XDEM_PRECISION_MIXED && LAW == LAW_CLOSEST && !warm) {
+    // the deep pairs on the side stream, beside the others and their deferred
+    // pairs (serial on one stream while the kernels are timed one by one)
+    cudaStream_t ds = w->prof_on ? w->stream : w->side;
+    if (!w->prof_on) {
+      cuda_check(w, cudaEventRecord(w->fork_ev, w->stream));
+      cuda_check(w, cudaStreamWaitEvent(w->side, w->fork_ev, 0));
+    }
+    LAUNCH(w, KK_DEEP, k_pair_deep_m<FOLD_BG, LAW><<<148 * 2, 128, 0, ds>>>(w->dw, w->par, record));
+    if (!w->prof_on) cuda_check(w, cudaEventRecord(w->join_ev, w->side));
+    LAUNCH(w, KK_PAIRS, k_pair_forces_m<FOLD_BG, LAW, PASS_REGULAR><<<pb, 128, 0, w->stream>>>(
+                            w->dw, w->par, record));
+    LAUNCH(w, KK_FALLBACK, k_pair_fallback_m<FOLD_BG, LAW><<<148 * 4, 128, 0, w->stream>>>(
+                               w->dw, w->par, record));
+    if (!w->prof_on) cuda_check(w, cudaStreamWaitEvent(w->stream, w->join_ev, 0));
+  } else if (w->prm.precision == XDEM_PRECISION_MIXED) {
     LAUNCH(w, KK_PAIRS,
            k_pair_forces_m<FOLD_BG, LAW><<<pb, 128, 0, w->stream>>>(w->dw, w->par, record));
     if (LAW == LAW_CLOSEST || LAW == LAW_ANY) {
@@ -422,6 +442,14 @@ int32_t xdem_create(const xdem_params* prm, xdem_world* out) {
     return XDEM_ERR_CUDA;
   }
   w->own_stream = true;
+  int lo = 0, hi = 0;
+  if (cudaDeviceGetStreamPriorityRange(&lo, &hi) != cudaSuccess ||
+      cudaStreamCreateWithPriority(&w->side, cudaStreamNonBlocking, hi) != cudaSuccess ||
+      cudaEventCreateWithFlags(&w->fork_ev, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&w->join_ev, cudaEventDisableTiming) != cudaSuccess) {
+    xdem_destroy(w);
+    return XDEM_ERR_CUDA;
+  }
   if (cudaMalloc(&w->ws, sizeof(WorldScalars)) != cudaSuccess ||
       cudaMalloc(&w->status, sizeof(uint32_t)) != cudaSuccess) {
     xdem_destroy(w);
@@ -461,6 +489,7 @@ int32_t xdem_create(const xdem_params* prm, xdem_world* out) {
 int32_t xdem_destroy(xdem_world w) {
   if (!w) return XDEM_OK;
   if (w->stream) cudaStreamSynchronize(w->stream);
+  if (w->side) cudaStreamSynchronize(w->side);
   w->particle_bufs.release();
   for (cudaEvent_t e : w->prof_events) cudaEventDestroy(e);
   for (cudaEvent_t e : w->timer)
@@ -468,6 +497,9 @@ int32_t xdem_destroy(xdem_world w) {
   if (w->ws) cudaFree(w->ws);
   if (w->status) cudaFree(w->status);
   if (w->own_stream && w->stream) cudaStreamDestroy(w->stream);
+  if (w->side) cudaStreamDestroy(w->side);
+  if (w->fork_ev) cudaEventDestroy(w->fork_ev);
+  if (w->join_ev) cudaEventDestroy(w->join_ev);
   delete w;
   return XDEM_OK;
 }
@@ -481,6 +513,7 @@ int32_t xdem_get_stream(xdem_world w, void** s) {
 int32_t xdem_set_stream(xdem_world w, void* s) {
   if (!w) return XDEM_ERR_ARGUMENT;
   cudaStreamSynchronize(w->stream);
+  cudaStreamSynchronize(w->side);
   if (w->own_stream) cudaStreamDestroy(w->stream);
   if (s) {
     w->stream = static_cast<cudaStream_t>(s);
@@ -743,6 +776,9 @@ int32_t set_particles_impl(xdem_world_s* w, const xdem_particles* P, const std::
   CK(w, B.alloc(&d.fallback, w->prm.precision == XDEM_PRECISION_MIXED ? ks : 1));
   CK(w, B.alloc(&d.nfallback, 1));
   CK(w, cudaMemsetAsync(d.nfallback, 0, sizeof(int32_t), s));
+  CK(w, B.alloc(&d.deep, w->prm.precision == XDEM_PRECISION_MIXED ? ks : 1));
+  CK(w, B.alloc(&d.ndeep, 1));
+  CK(w, cudaMemsetAsync(d.ndeep, 0, sizeof(int32_t), s));
   d.warm = nullptr;
   if (w->mlp) CK(w, B.alloc(&d.warm, ks));
   // candidate lists: rebuilt by the first step (vl_valid starts at 0)

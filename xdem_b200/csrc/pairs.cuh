@@ -104,27 +104,41 @@ __device__ __forceinline__ AxisShape axis_shape(const DevWorld& w, int m) {
   return e;
 }
 
-// True when two ellipses are separated along the line of their centres: the
-// centre distance |d| exceeds the sum of their half-widths along d̂, so their
-// projections on that line are disjoint.  The exact distance of closest
-// approach along d̂ is at most that sum, and two disjoint ellipses do not
-// intersect, so neither law has a contact there and the pair's history is
-// erased (BaseParticle.cpp:95), as it is for a candidate that is not listed.
+// Class of a pair of ellipses on the line of their centres, from the centre
+// distance |d| and the sum S of their half-widths along d̂:
+//   CL_SEPARATED  |d| > 1.001 S: the projections on that line are disjoint.
+//                 The exact distance of closest approach along d̂ is at most
+//                 S, and two disjoint ellipses do not intersect, so neither
+//                 law has a contact there and the pair's history is erased
+//                 (BaseParticle.cpp:95), as it is for a candidate that is not
+//                 listed: the pair is dropped.
+//   CL_DEEP       |d| < 0.7 S: a deep overlap.  The closest-approach Newton
+//                 iterations that run to their cap come from such pairs; they
+//                 are listed apart and evaluated beside the other pairs, so
+//                 that their long serial solve starts first.
+//   CL_REGULAR    otherwise.
 // The screen serves the mixed-precision path only: the reference's own
-// construction can report a contact for such a pair when its Newton result
-// is not finite (it then takes d' = 1 + a2', EllipticParticle.cpp:168-170),
-// and the FP64 path reproduces the reference pair for pair.  With
-// H = half-width * |d| = sqrt(a²(d·k)² + b²(d×k)²) the test is
-// |d|² > H_i + H_j; the 1e-3 relative margin is far above the FP32 rounding
+// construction can report a contact for a separated pair when its Newton
+// result is not finite (it then takes d' = 1 + a2', EllipticParticle.cpp:
+// 168-170), and the FP64 path reproduces the reference pair for pair.  With
+// H = half-width * |d| = sqrt(a²(d·k)² + b²(d×k)²) the tests compare |d|²
+// with (H_i + H_j); the 1e-3 relative margin is far above the FP32 rounding
 // of d, the angles and the axes (below 1e-5 relative).
-__device__ __forceinline__ bool separated_on_centre_line(float dx, float dy, const AxisShape& i,
-                                                         const AxisShape& j) {
+enum { CL_SEPARATED = 0, CL_REGULAR = 1, CL_DEEP = 2 };
+
+__device__ __forceinline__ int centre_line_class(float dx, float dy, const AxisShape& i,
+                                                 const AxisShape& j) {
   const float pi = dx * i.c + dy * i.s, qi = dx * i.s - dy * i.c;
   const float pj = dx * j.c + dy * j.s, qj = dx * j.s - dy * j.c;
   const float hi = sqrtf(i.a * i.a * pi * pi + i.b * i.b * qi * qi);
   const float hj = sqrtf(j.a * j.a * pj * pj + j.b * j.b * qj * qj);
-  return dx * dx + dy * dy > (hi + hj) * 1.001f;
+  const float d2 = dx * dx + dy * dy, S = hi + hj;
+  return d2 > S * 1.001f ? CL_SEPARATED : (d2 < S * 0.7f ? CL_DEEP : CL_REGULAR);
 }
+
+// flag of a listed pair (bit 24 of its list code, PairEntry::pad in the pair
+// list) that the centre-line screen classed deep
+constexpr int kDeepFlag = 1 << 24;
 
 // the centre-line screen applies to mixed-precision worlds of ellipses under
 // one law
@@ -225,14 +239,15 @@ __device__ __forceinline__ void scan_cells(const DevWorld& w, const WorldScalars
           pass = coarse_pass<LAW>(0, 0, r_i, w.screen_r[mj], orad_i, w.screen_r[mj], pi, pj, off);
         if (!pass) continue;
       }
+      int cls = CL_REGULAR;
       if (centre_line_screen<LAW>(w)) {
         // the same FP64 image offset as the candidate lists' test (verlet.cuh)
         const double2 pj = w.cell_pos[q];
         vec2<double> off, ovel;
         image_offset(ws, kind, pi, pj, off, ovel);
-        if (separated_on_centre_line((float)((pj.x + off.x) - pi.x), (float)((pj.y + off.y) - pi.y),
-                                     shape_ax, axis_shape(w, w.cell_mem[q])))
-          continue;
+        cls = centre_line_class((float)((pj.x + off.x) - pi.x), (float)((pj.y + off.y) - pi.y),
+                                shape_ax, axis_shape(w, w.cell_mem[q]));
+        if (cls == CL_SEPARATED) continue;
       }
       if (nlist >= K) {
         st |= ST_CAPACITY;
@@ -243,7 +258,8 @@ __device__ __forceinline__ void scan_cells(const DevWorld& w, const WorldScalars
         if (old.partner[(size_t)z * n + m] == id_j) oslot = z;
       if (oslot != kNoOldSlot) matched |= 1u << oslot;
       list_mj[nlist] = w.cell_mem[q];
-      list_code[nlist] = kind | (nlist << 8) | (oslot << 16);
+      list_code[nlist] =
+          kind | (nlist << 8) | (oslot << 16) | (LAW == LAW_CLOSEST && cls == CL_DEEP ? kDeepFlag : 0);
       ++nlist;
     }
   }
@@ -292,6 +308,36 @@ __device__ __forceinline__ int carry_over(const DevWorld& w, const Slots& old, c
     ++k;
   }
   return k;
+}
+
+// Writes the owner's listed pairs from index `at` of the pair list; a pair
+// classed deep (kDeepFlag) carries pad = 1 and its index is appended to the
+// deep-pair list (one atomic per warp).  Every lane of the warp calls.
+__device__ __forceinline__ void write_pairs(const DevWorld& w, int m, int at, int nlist,
+                                            const int32_t* list_mj, const int32_t* list_code) {
+  int ndeep = 0;
+  for (int s = 0; s < nlist; ++s) {
+    const int c = list_code[s];
+    const int deep = (c & kDeepFlag) ? 1 : 0;
+    ndeep += deep;
+    w.pairs[at + s] = PairEntry{m, list_mj[s], c & ~kDeepFlag, deep};
+  }
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  int incl = ndeep;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int v = __shfl_up_sync(full, incl, o);
+    if (lane >= o) incl += v;
+  }
+  const int tot = __shfl_sync(full, incl, 31);
+  if (tot == 0) return;
+  int base = 0;
+  if (lane == 31) base = atomicAdd(w.ndeep, tot);
+  base = __shfl_sync(full, base, 31);
+  int k = base + incl - ndeep;
+  for (int s = 0; s < nlist && ndeep > 0; ++s)
+    if (list_code[s] & kDeepFlag) w.deep[k++] = at + s;
 }
 
 // One thread per owner m.  Cell entries are read from the cell-ordered
@@ -386,7 +432,7 @@ __global__ void __launch_bounds__(128) k_candidates(DevWorld w, int par) {
   int base = block_base;
   for (int k = 0; k < warp; ++k) base += warp_total[k];
   int at = base + incl - nlist;
-  for (int s = 0; s < nlist; ++s) w.pairs[at + s] = PairEntry{m, list_mj[s], list_code[s], 0};
+  write_pairs(w, m, at, nlist, list_mj, list_code);
   raise(w.status, st);
 }
 
@@ -538,6 +584,7 @@ __global__ void k_pairs_done(DevWorld w) {
   w.ws->last_pairs = *w.npairs;
   *w.npairs = 0;
   *w.nfallback = 0;
+  *w.ndeep = 0;
 }
 
 }  // namespace xdem

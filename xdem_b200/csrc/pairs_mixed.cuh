@@ -110,35 +110,67 @@ __device__ __forceinline__ void count_solve(uint32_t it, uint32_t& n_solves, uin
 }
 
 
-template <bool FOLD_BG, int LAW>
-__global__ void __launch_bounds__(128, 4) k_pair_forces_m(DevWorld w, int par, int record) {
-  if (stopped(w)) return;
+// Which listed pairs a launch of k_pair_forces_m evaluates:
+//   PASS_ALL      every listed pair; closest-approach pairs that need the FP64
+//                 construction are deferred to k_pair_fallback_m;
+//   PASS_REGULAR  every listed pair but the deep ones (PairEntry::pad), with
+//                 the same deferral;
+//   PASS_DEEP     the deep pairs (the deep-pair list), on a second stream
+//                 beside PASS_REGULAR; the FP64 construction runs in place, so
+//                 that the closest-approach Newton iterations that run to their
+//                 cap (deep overlaps) start with the step's other pairs
+//                 instead of after them.
+// Every pair is evaluated by the same operations whichever pass takes it.
+enum { PASS_ALL = 0, PASS_REGULAR = 1, PASS_DEEP = 2 };
+
+template <bool FOLD_BG, int LAW, int PASS>
+__device__ __forceinline__ void pair_forces_m(const DevWorld& w, int par, int record, int t,
+                                              uint32_t& st, uint32_t& n_solves, uint32_t& n_iters,
+                                              uint32_t& n_capped) {
   const int n = w.n;
   const Slots& cur = w.slots[par ^ 1];
-  const int npairs = *w.npairs;
-  uint32_t st = 0, n_solves = 0, n_iters = 0, n_capped = 0;
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < npairs; t += gridDim.x * blockDim.x) {
-    const PairEntry e = w.pairs[t];
-    const int m = e.m, mj = e.mj;
-    const WorldScalars& ws = w.ws[sys_at(w, m)];
-    const int kind = e.code & 0xff, slot = (e.code >> 8) & 0xff;
-    const size_t ci = (size_t)slot * n + m;
-    const BodyRec ba = w.body[m], bb = w.body[mj];
-    const PState a = body_state<FOLD_BG>(ba, ws);
-    const PState b = body_state<FOLD_BG>(bb, ws);
-    vec2<double> off, ovel;
-    image_offset(ws, kind, make_double2(a.x, a.y), make_double2(b.x, b.y), off, ovel);
-    GeomM g;
-    int res = PW_NONE;
-    const bool circles = LAW == LAW_CIRCLE ||
-                         (LAW == LAW_ANY && a.shape == SHAPE_CIRCLE && b.shape == SHAPE_CIRCLE);
-    const bool closest = LAW == LAW_CLOSEST ||
-                         (LAW == LAW_ANY && w.method == ELLIPSE_CLOSEST &&
-                          a.shape == SHAPE_ELLIPSE && b.shape == SHAPE_ELLIPSE);
-    if (circles) {
-      res = circle_circle_m(a, b, off, ovel, g) ? PW_CONTACT : PW_NONE;
-    } else if (closest) {
-      res = ellipse_closest_m(a, b, off, ovel, ba.cs, bb.cs, g);
+  const PairEntry e = w.pairs[t];
+  if (PASS == PASS_REGULAR && e.pad) return;
+  const int m = e.m, mj = e.mj;
+  const WorldScalars& ws = w.ws[sys_at(w, m)];
+  const int kind = e.code & 0xff, slot = (e.code >> 8) & 0xff;
+  const size_t ci = (size_t)slot * n + m;
+  const BodyRec ba = w.body[m], bb = w.body[mj];
+  const PState a = body_state<FOLD_BG>(ba, ws);
+  const PState b = body_state<FOLD_BG>(bb, ws);
+  vec2<double> off, ovel;
+  image_offset(ws, kind, make_double2(a.x, a.y), make_double2(b.x, b.y), off, ovel);
+  GeomM g;
+  int res = PW_NONE;
+  const bool circles = LAW == LAW_CIRCLE ||
+                       (LAW == LAW_ANY && a.shape == SHAPE_CIRCLE && b.shape == SHAPE_CIRCLE);
+  const bool closest = LAW == LAW_CLOSEST ||
+                       (LAW == LAW_ANY && w.method == ELLIPSE_CLOSEST &&
+                        a.shape == SHAPE_ELLIPSE && b.shape == SHAPE_ELLIPSE);
+  if (circles) {
+    res = circle_circle_m(a, b, off, ovel, g) ? PW_CONTACT : PW_NONE;
+  } else if (closest) {
+    res = ellipse_closest_m(a, b, off, ovel, ba.cs, bb.cs, g);
+    if (PASS == PASS_DEEP) {
+      if (res == PW_FALLBACK) {
+        // the reference's FP64 construction in place (as k_pair_fallback_m)
+        Geom gd = Geom{};
+        const bool touching =
+            ellipse_closest<false>(a, b, off, ovel, ba.cs.x, ba.cs.y, bb.cs.x, bb.cs.y, gd, st, 0.0f);
+        if (gd.iters > 0) {
+          n_solves++;
+          n_iters += gd.iters;
+          n_capped += gd.iters >= kNewtonCap ? 1u : 0u;
+        }
+        res = PW_NONE;
+        if (touching) {
+          geom_to_m(gd, a, g);
+          res = PW_CONTACT;
+        }
+      } else {
+        count_solve(g.iters, n_solves, n_iters);
+      }
+    } else {
       // deferred pairs take consecutive list entries, one atomic per warp
       const unsigned act = __activemask();
       const unsigned defer = __ballot_sync(act, res == PW_FALLBACK);
@@ -148,33 +180,54 @@ __global__ void __launch_bounds__(128, 4) k_pair_forces_m(DevWorld w, int par, i
         if (lane == leader) base = atomicAdd(w.nfallback, __popc(defer));
         base = __shfl_sync(defer, base, leader);
         w.fallback[base + __popc(defer & ((1u << lane) - 1u))] = t;
-        continue;
+        return;
       }
       count_solve(g.iters, n_solves, n_iters);
-    } else {
-      // intersection law (kept FP64: near tangency its quartic has a near
-      // double root), clumps and unsupported pairs: the FP64 dispatcher
-      double2 csa = make_double2(0.0, 0.0), csb = make_double2(0.0, 0.0);
-      if (LAW == LAW_INTERSECTION || (a.shape == SHAPE_ELLIPSE && b.shape == SHAPE_ELLIPSE)) {
-        csa = ba.cs;
-        csb = bb.cs;
-      }
-      Geom gd;
-      bool touching;
-      if (LAW == LAW_INTERSECTION)
-        touching = contact_geometry_law<LAW_INTERSECTION, true>(a, b, 0.0, 0.0, off, ovel, csa, csb, gd, st);
-      else
-        touching = contact_geometry(w.method, a, b, w.orad[m], w.orad[mj], off, ovel, csa, csb, gd, st,
-                                    seg_of(w, ba), seg_of(w, bb));
-      if (touching) geom_to_m(gd, a, g);
-      res = touching ? PW_CONTACT : PW_NONE;
     }
-    if (res != PW_CONTACT) {
-      cur.partner[ci] = -1;
-      continue;
+  } else {
+    // intersection law (kept FP64: near tangency its quartic has a near
+    // double root), clumps and unsupported pairs: the FP64 dispatcher
+    double2 csa = make_double2(0.0, 0.0), csb = make_double2(0.0, 0.0);
+    if (LAW == LAW_INTERSECTION || (a.shape == SHAPE_ELLIPSE && b.shape == SHAPE_ELLIPSE)) {
+      csa = ba.cs;
+      csb = bb.cs;
     }
-    write_contact_m(w, ws, e, ba, bb, a, b, off, g, par, record, st);
+    Geom gd;
+    bool touching;
+    if (LAW == LAW_INTERSECTION)
+      touching = contact_geometry_law<LAW_INTERSECTION, true>(a, b, 0.0, 0.0, off, ovel, csa, csb, gd, st);
+    else
+      touching = contact_geometry(w.method, a, b, w.orad[m], w.orad[mj], off, ovel, csa, csb, gd, st,
+                                  seg_of(w, ba), seg_of(w, bb));
+    if (touching) geom_to_m(gd, a, g);
+    res = touching ? PW_CONTACT : PW_NONE;
   }
+  if (res != PW_CONTACT) {
+    cur.partner[ci] = -1;
+    return;
+  }
+  write_contact_m(w, ws, e, ba, bb, a, b, off, g, par, record, st);
+}
+
+template <bool FOLD_BG, int LAW, int PASS = PASS_ALL>
+__global__ void __launch_bounds__(128, 4) k_pair_forces_m(DevWorld w, int par, int record) {
+  if (stopped(w)) return;
+  uint32_t st = 0, n_solves = 0, n_iters = 0, n_capped = 0;
+  const int npairs = *w.npairs;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < npairs; t += gridDim.x * blockDim.x)
+    pair_forces_m<FOLD_BG, LAW, PASS>(w, par, record, t, st, n_solves, n_iters, n_capped);
+  flush_warp(w, st, n_solves, n_iters, n_capped);
+}
+
+// PASS_DEEP: a few blocks, registers as the FP64 construction needs them
+template <bool FOLD_BG, int LAW>
+__global__ void __launch_bounds__(128) k_pair_deep_m(DevWorld w, int par, int record) {
+  if (stopped(w)) return;
+  uint32_t st = 0, n_solves = 0, n_iters = 0, n_capped = 0;
+  const int ndeep = *w.ndeep;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ndeep; t += gridDim.x * blockDim.x)
+    pair_forces_m<FOLD_BG, LAW, PASS_DEEP>(w, par, record, w.deep[t], st, n_solves, n_iters,
+                                           n_capped);
   flush_warp(w, st, n_solves, n_iters, n_capped);
 }
 

@@ -204,10 +204,12 @@ __global__ void __launch_bounds__(128, 7) k_candidates_vl(DevWorld w, int par) {
             pass = coarse_pass<LAW>(0, 0, r_i, w.screen_r[mj], orad_i, w.screen_r[mj], pi, pj,
                                     off);
           if (!pass) continue;
-          if (centre_line_screen<LAW>(w) &&
-              separated_on_centre_line((float)((pj.x + off.x) - pi.x), (float)((pj.y + off.y) - pi.y),
-                                       shape_ax, axis_shape(w, mj)))
-            continue;
+          int cls = CL_REGULAR;
+          if (centre_line_screen<LAW>(w)) {
+            cls = centre_line_class((float)((pj.x + off.x) - pi.x), (float)((pj.y + off.y) - pi.y),
+                                    shape_ax, axis_shape(w, mj));
+            if (cls == CL_SEPARATED) continue;
+          }
           if (nlist >= K) {
             st |= ST_CAPACITY;
             continue;
@@ -224,7 +226,8 @@ __global__ void __launch_bounds__(128, 7) k_candidates_vl(DevWorld w, int par) {
                              (shape_i == SHAPE_CIRCLE || shape_i == SHAPE_ELLIPSE));
           if (oslot != kNoOldSlot && near) matched |= 1u << oslot;
           list_mj[nlist] = mj;
-          list_code[nlist] = kind | (nlist << 8) | (oslot << 16);
+          list_code[nlist] = kind | (nlist << 8) | (oslot << 16) |
+                             (LAW == LAW_CLOSEST && cls == CL_DEEP ? kDeepFlag : 0);
           ++nlist;
         }
       }
@@ -270,7 +273,7 @@ __global__ void __launch_bounds__(128, 7) k_candidates_vl(DevWorld w, int par) {
   int base = block_base;
   for (int k = 0; k < warp; ++k) base += warp_total[k];
   const int at = base + incl - nlist;
-  for (int s = 0; s < nlist; ++s) w.pairs[at + s] = PairEntry{m, list_mj[s], list_code[s], 0};
+  write_pairs(w, m, at, nlist, list_mj, list_code);
   raise(w.status, st);
 }
 
