@@ -771,14 +771,16 @@ int32_t set_particles_impl(xdem_world_s* w, const xdem_particles* P, const std::
   CK(w, B.alloc(&d.inref, ks));
   CK(w, cudaMemsetAsync(d.incnt, 0, sizeof(int32_t) * n, s));
   CK(w, B.alloc(&d.pairs, ks));
-  CK(w, B.alloc(&d.npairs, 1));
-  CK(w, cudaMemsetAsync(d.npairs, 0, sizeof(int32_t), s));
+  // the pair and deep-pair counts are the low and high halves of one 64-bit
+  // word, so that a warp reserves room in both lists with one atomic
+  CK(w, B.alloc(&d.pair_counts, 1));
+  CK(w, cudaMemsetAsync(d.pair_counts, 0, sizeof(unsigned long long), s));
+  d.npairs = reinterpret_cast<int32_t*>(d.pair_counts);
+  d.ndeep = d.npairs + 1;
   CK(w, B.alloc(&d.fallback, w->prm.precision == XDEM_PRECISION_MIXED ? ks : 1));
   CK(w, B.alloc(&d.nfallback, 1));
   CK(w, cudaMemsetAsync(d.nfallback, 0, sizeof(int32_t), s));
   CK(w, B.alloc(&d.deep, w->prm.precision == XDEM_PRECISION_MIXED ? ks : 1));
-  CK(w, B.alloc(&d.ndeep, 1));
-  CK(w, cudaMemsetAsync(d.ndeep, 0, sizeof(int32_t), s));
   d.warm = nullptr;
   if (w->mlp) CK(w, B.alloc(&d.warm, ks));
   // candidate lists: rebuilt by the first step (vl_valid starts at 0)

@@ -310,34 +310,63 @@ __device__ __forceinline__ int carry_over(const DevWorld& w, const Slots& old, c
   return k;
 }
 
-// Writes the owner's listed pairs from index `at` of the pair list; a pair
-// classed deep (kDeepFlag) carries pad = 1 and its index is appended to the
-// deep-pair list (one atomic per warp).  Every lane of the warp calls.
-__device__ __forceinline__ void write_pairs(const DevWorld& w, int m, int at, int nlist,
+// Reserves room for a block's listed pairs (nlist per thread) and deep-pair
+// indices (ndeep per thread) with one atomic on the packed counter of the two
+// lists (pairs in the low 32 bits, deep pairs in the high 32 bits); returns
+// each thread's first index in both.  A block's pairs stay together in the
+// list, in owner order, which keeps the pair kernel's gathers local.  Every
+// thread of the block (of 128) calls.
+__device__ __forceinline__ void reserve_pairs(const DevWorld& w, int nlist, int ndeep, int& at,
+                                              int& deep_at) {
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int a = nlist, b = ndeep;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int va = __shfl_up_sync(full, a, o), vb = __shfl_up_sync(full, b, o);
+    if (lane >= o) {
+      a += va;
+      b += vb;
+    }
+  }
+  __shared__ int warp_a[4], warp_b[4];
+  __shared__ unsigned long long block_base;
+  if (lane == 31) {
+    warp_a[warp] = a;
+    warp_b[warp] = b;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const unsigned ta = warp_a[0] + warp_a[1] + warp_a[2] + warp_a[3];
+    const unsigned tb = warp_b[0] + warp_b[1] + warp_b[2] + warp_b[3];
+    block_base = (ta | tb) ? atomicAdd(w.pair_counts, ((unsigned long long)tb << 32) | ta) : 0ull;
+  }
+  __syncthreads();
+  int ba = (int)(uint32_t)block_base, bb = (int)(uint32_t)(block_base >> 32);
+  for (int k = 0; k < warp; ++k) {
+    ba += warp_a[k];
+    bb += warp_b[k];
+  }
+  at = ba + a - nlist;
+  deep_at = bb + b - ndeep;
+}
+
+// Writes the owner's listed pairs to the pair list, after reserving their
+// room (reserve_pairs); a pair classed deep (kDeepFlag) carries pad = 1 and
+// its index also goes to the deep-pair list.  Every thread of the block
+// calls.
+__device__ __forceinline__ void write_pairs(const DevWorld& w, int m, int nlist,
                                             const int32_t* list_mj, const int32_t* list_code) {
   int ndeep = 0;
+  for (int s = 0; s < nlist; ++s) ndeep += (list_code[s] & kDeepFlag) ? 1 : 0;
+  int at, k;
+  reserve_pairs(w, nlist, ndeep, at, k);
   for (int s = 0; s < nlist; ++s) {
     const int c = list_code[s];
     const int deep = (c & kDeepFlag) ? 1 : 0;
-    ndeep += deep;
     w.pairs[at + s] = PairEntry{m, list_mj[s], c & ~kDeepFlag, deep};
+    if (deep) w.deep[k++] = at + s;
   }
-  const unsigned full = 0xffffffffu;
-  const int lane = threadIdx.x & 31;
-  int incl = ndeep;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const int v = __shfl_up_sync(full, incl, o);
-    if (lane >= o) incl += v;
-  }
-  const int tot = __shfl_sync(full, incl, 31);
-  if (tot == 0) return;
-  int base = 0;
-  if (lane == 31) base = atomicAdd(w.ndeep, tot);
-  base = __shfl_sync(full, base, 31);
-  int k = base + incl - ndeep;
-  for (int s = 0; s < nlist && ndeep > 0; ++s)
-    if (list_code[s] & kDeepFlag) w.deep[k++] = at + s;
 }
 
 // One thread per owner m.  Cell entries are read from the cell-ordered
@@ -411,28 +440,7 @@ __global__ void __launch_bounds__(128) k_candidates(DevWorld w, int par) {
     }
     cur.count[m] = carry_over(w, old, cur, m, nold, seen, nlist, st);
   }
-  // reserve room in the pair list for the whole block at once (one atomic
-  // per block on the shared counter)
-  const unsigned full = 0xffffffffu;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  int incl = nlist;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    int v = __shfl_up_sync(full, incl, o);
-    if (lane >= o) incl += v;
-  }
-  __shared__ int warp_total[4], block_base;
-  if (lane == 31) warp_total[warp] = incl;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    const int tot = warp_total[0] + warp_total[1] + warp_total[2] + warp_total[3];
-    block_base = tot > 0 ? atomicAdd(w.npairs, tot) : 0;
-  }
-  __syncthreads();
-  int base = block_base;
-  for (int k = 0; k < warp; ++k) base += warp_total[k];
-  int at = base + incl - nlist;
-  write_pairs(w, m, at, nlist, list_mj, list_code);
+  write_pairs(w, m, nlist, list_mj, list_code);
   raise(w.status, st);
 }
 

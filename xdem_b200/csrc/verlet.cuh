@@ -253,27 +253,7 @@ __global__ void __launch_bounds__(128, 7) k_candidates_vl(DevWorld w, int par) {
     }
     cur.count[m] = carry_over(w, old, cur, m, nold, seen, nlist, st);
   }
-  // reserve room in the pair list for the whole block at once
-  const unsigned full = 0xffffffffu;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  int incl = nlist;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    int v = __shfl_up_sync(full, incl, o);
-    if (lane >= o) incl += v;
-  }
-  __shared__ int warp_total[4], block_base;
-  if (lane == 31) warp_total[warp] = incl;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    const int tot = warp_total[0] + warp_total[1] + warp_total[2] + warp_total[3];
-    block_base = tot > 0 ? atomicAdd(w.npairs, tot) : 0;
-  }
-  __syncthreads();
-  int base = block_base;
-  for (int k = 0; k < warp; ++k) base += warp_total[k];
-  const int at = base + incl - nlist;
-  write_pairs(w, m, at, nlist, list_mj, list_code);
+  write_pairs(w, m, nlist, list_mj, list_code);
   raise(w.status, st);
 }
 

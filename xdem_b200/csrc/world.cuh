@@ -161,13 +161,14 @@ struct DevWorld {
   int32_t* incnt;   // [n] contacts owned by lower ids
   uint32_t* inref;  // [K*n] owner position*K + slot of those contacts
   PairEntry* pairs; // [K*n] pairs that passed the candidate scan
-  int32_t* npairs;  // number of listed pairs
+  int32_t* npairs;  // number of listed pairs (low half of pair_counts)
   int32_t* fallback;   // [K*n] mixed precision: listed pairs deferred to the FP64 construction
   int32_t* nfallback;  // number of deferred pairs
   // mixed precision, closest approach: listed pairs classed deep by the
   // centre-line screen (indices into pairs), evaluated beside the others
   int32_t* deep;   // [K*n]
-  int32_t* ndeep;  // number of deep pairs
+  int32_t* ndeep;  // number of deep pairs (high half of pair_counts)
+  unsigned long long* pair_counts;  // the two counts, reserved together
   float2* warm;        // [K*n] learned warm start of each listed pair: (root fraction, contact logit)
   // candidate lists kept across steps (verlet.cuh); V == 0: full scan each step
   int V;
