@@ -123,10 +123,37 @@ __device__ __forceinline__ void count_solve(uint32_t it, uint32_t& n_solves, uin
 // Every pair is evaluated by the same operations whichever pass takes it.
 enum { PASS_ALL = 0, PASS_REGULAR = 1, PASS_DEEP = 2 };
 
+__device__ __forceinline__ void prefetch_l2(const void* p) {
+  asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+
+// Asks the L2 for what the pair at index t will read: its two body records
+// (96 bytes each, two lines) and the owner's old history slot.  Issued while
+// the thread's current pair is computed, so that the next pair's gathers find
+// their data on chip.
+__device__ __forceinline__ void prefetch_pair(const DevWorld& w, int par, int t) {
+  const PairEntry e = w.pairs[t];
+  const char* ba = reinterpret_cast<const char*>(w.body + e.m);
+  const char* bb = reinterpret_cast<const char*>(w.body + e.mj);
+  prefetch_l2(ba);
+  prefetch_l2(ba + sizeof(BodyRec) - 1);
+  prefetch_l2(bb);
+  prefetch_l2(bb + sizeof(BodyRec) - 1);
+  const int o = (e.code >> 16) & 0xff;
+  if (o != kNoOldSlot) {
+    const Slots& old = w.slots[par];
+    const size_t oi = (size_t)o * w.n + e.m;
+    prefetch_l2(old.n + oi);
+    prefetch_l2(old.s + oi);
+    prefetch_l2(old.damp + oi);
+  }
+}
+
+// tn: the index of the thread's next pair (prefetched), or -1
 template <bool FOLD_BG, int LAW, int PASS>
 __device__ __forceinline__ void pair_forces_m(const DevWorld& w, int par, int record, int t,
                                               uint32_t& st, uint32_t& n_solves, uint32_t& n_iters,
-                                              uint32_t& n_capped) {
+                                              uint32_t& n_capped, int tn = -1) {
   const int n = w.n;
   const Slots& cur = w.slots[par ^ 1];
   const PairEntry e = w.pairs[t];
@@ -136,6 +163,7 @@ __device__ __forceinline__ void pair_forces_m(const DevWorld& w, int par, int re
   const int kind = e.code & 0xff, slot = (e.code >> 8) & 0xff;
   const size_t ci = (size_t)slot * n + m;
   const BodyRec ba = w.body[m], bb = w.body[mj];
+  if (tn >= 0) prefetch_pair(w, par, tn);
   const PState a = body_state<FOLD_BG>(ba, ws);
   const PState b = body_state<FOLD_BG>(bb, ws);
   vec2<double> off, ovel;
@@ -214,8 +242,10 @@ __global__ void __launch_bounds__(128, 4) k_pair_forces_m(DevWorld w, int par, i
   if (stopped(w)) return;
   uint32_t st = 0, n_solves = 0, n_iters = 0, n_capped = 0;
   const int npairs = *w.npairs;
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < npairs; t += gridDim.x * blockDim.x)
-    pair_forces_m<FOLD_BG, LAW, PASS>(w, par, record, t, st, n_solves, n_iters, n_capped);
+  const int stride = gridDim.x * blockDim.x;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < npairs; t += stride)
+    pair_forces_m<FOLD_BG, LAW, PASS>(w, par, record, t, st, n_solves, n_iters, n_capped,
+                                      t + stride < npairs ? t + stride : -1);
   flush_warp(w, st, n_solves, n_iters, n_capped);
 }
 
