@@ -212,10 +212,10 @@ def test_mixed_lees_edwards_history_and_mean_shear_stress():
 
 def test_deep_pairs_beside_the_other_pairs_are_bit_identical():
     """A mixed closest-approach step evaluates the pairs that the centre-line
-    screen classed deep (centre distance below 0.7 of the half-width sum) on
-    a second stream, beside the other pairs and their deferred FP64 pass.
-    With per-kernel profiling on, the same kernels run one after another on
-    one stream.  Both orders give the same state, contacts, stress and Newton
+    screen classed deep (centre distance below 0.7 of the half-width sum) in
+    a kernel launched ahead of the regular pair pass, which starts as a
+    programmatic dependent launch and runs beside it.  With per-kernel
+    profiling on, the regular pass is an ordinary launch after it.  Both orders give the same state, contacts, stress and Newton
     counters bit for bit, through direct steps and through the CUDA-graph
     chunks of a run, and the deep pass ran."""
     p, contacts, prm = dense_ellipse_case(n=4000, seed=35, kind=abi.WORLD_LEES_EDWARDS,

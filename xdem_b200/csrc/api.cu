@@ -56,11 +56,6 @@ struct xdem_world_s {
   xdem_params prm{};
   cudaStream_t stream = nullptr;
   bool own_stream = false;
-  // second stream of the contact update (mixed precision, closest approach):
-  // the deep pairs run on it beside the other pairs; fork/join events order
-  // it with `stream`
-  cudaStream_t side = nullptr;
-  cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
   DevWorld dw{};
   DeviceBuffers particle_bufs;
   WorldScalars* ws = nullptr;
@@ -231,20 +226,35 @@ void launch_update_phases(xdem_world_s* w, int record) {
     LAUNCH(w, KK_CANDIDATES, k_candidates<LAW><<<nb, 128, 0, w->stream>>>(w->dw, w->par));
   }
   if (w->prm.precision == XDEM_PRECISION_MIXED && LAW == LAW_CLOSEST && !warm) {
-    // the deep pairs on the side stream, beside the others and their deferred
-    // pairs (serial on one stream while the kernels are timed one by one)
-    cudaStream_t ds = w->prof_on ? w->stream : w->side;
-    if (!w->prof_on) {
-      cuda_check(w, cudaEventRecord(w->fork_ev, w->stream));
-      cuda_check(w, cudaStreamWaitEvent(w->side, w->fork_ev, 0));
+    // The deep pairs first, then the regular pair pass as a programmatic
+    // dependent launch: every block of k_pair_deep_m signals at its start, so
+    // the regular pass starts once the deep pass is on the GPU and runs
+    // beside it (in whatever order the blocks would otherwise be dispatched).
+    // The regular pass uses nothing the deep pass writes; the deferred pass
+    // after it is an ordinary launch and waits for both.  While the kernels
+    // are timed one by one the regular pass is an ordinary launch too.
+    LAUNCH(w, KK_DEEP,
+           k_pair_deep_m<FOLD_BG, LAW><<<148 * 2, 128, 0, w->stream>>>(w->dw, w->par, record));
+    if (w->prof_on) {
+      LAUNCH(w, KK_PAIRS, k_pair_forces_m<FOLD_BG, LAW, PASS_REGULAR><<<pb, 128, 0, w->stream>>>(
+                              w->dw, w->par, record));
+    } else {
+      cudaLaunchAttribute attr[1];
+      attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+      attr[0].val.programmaticStreamSerializationAllowed = 1;
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3(pb);
+      cfg.blockDim = dim3(128);
+      cfg.dynamicSmemBytes = 0;
+      cfg.stream = w->stream;
+      cfg.attrs = attr;
+      cfg.numAttrs = 1;
+      cuda_check(w, cudaLaunchKernelEx(&cfg, k_pair_forces_m<FOLD_BG, LAW, PASS_REGULAR>, w->dw,
+                                       w->par, record));
+      w->launches++;
     }
-    LAUNCH(w, KK_DEEP, k_pair_deep_m<FOLD_BG, LAW><<<148 * 2, 128, 0, ds>>>(w->dw, w->par, record));
-    if (!w->prof_on) cuda_check(w, cudaEventRecord(w->join_ev, w->side));
-    LAUNCH(w, KK_PAIRS, k_pair_forces_m<FOLD_BG, LAW, PASS_REGULAR><<<pb, 128, 0, w->stream>>>(
-                            w->dw, w->par, record));
     LAUNCH(w, KK_FALLBACK, k_pair_fallback_m<FOLD_BG, LAW><<<148 * 4, 128, 0, w->stream>>>(
                                w->dw, w->par, record));
-    if (!w->prof_on) cuda_check(w, cudaStreamWaitEvent(w->stream, w->join_ev, 0));
   } else if (w->prm.precision == XDEM_PRECISION_MIXED) {
     LAUNCH(w, KK_PAIRS,
            k_pair_forces_m<FOLD_BG, LAW><<<pb, 128, 0, w->stream>>>(w->dw, w->par, record));
@@ -442,14 +452,6 @@ int32_t xdem_create(const xdem_params* prm, xdem_world* out) {
     return XDEM_ERR_CUDA;
   }
   w->own_stream = true;
-  int lo = 0, hi = 0;
-  if (cudaDeviceGetStreamPriorityRange(&lo, &hi) != cudaSuccess ||
-      cudaStreamCreateWithPriority(&w->side, cudaStreamNonBlocking, hi) != cudaSuccess ||
-      cudaEventCreateWithFlags(&w->fork_ev, cudaEventDisableTiming) != cudaSuccess ||
-      cudaEventCreateWithFlags(&w->join_ev, cudaEventDisableTiming) != cudaSuccess) {
-    xdem_destroy(w);
-    return XDEM_ERR_CUDA;
-  }
   if (cudaMalloc(&w->ws, sizeof(WorldScalars)) != cudaSuccess ||
       cudaMalloc(&w->status, sizeof(uint32_t)) != cudaSuccess) {
     xdem_destroy(w);
@@ -489,7 +491,6 @@ int32_t xdem_create(const xdem_params* prm, xdem_world* out) {
 int32_t xdem_destroy(xdem_world w) {
   if (!w) return XDEM_OK;
   if (w->stream) cudaStreamSynchronize(w->stream);
-  if (w->side) cudaStreamSynchronize(w->side);
   w->particle_bufs.release();
   for (cudaEvent_t e : w->prof_events) cudaEventDestroy(e);
   for (cudaEvent_t e : w->timer)
@@ -497,9 +498,6 @@ int32_t xdem_destroy(xdem_world w) {
   if (w->ws) cudaFree(w->ws);
   if (w->status) cudaFree(w->status);
   if (w->own_stream && w->stream) cudaStreamDestroy(w->stream);
-  if (w->side) cudaStreamDestroy(w->side);
-  if (w->fork_ev) cudaEventDestroy(w->fork_ev);
-  if (w->join_ev) cudaEventDestroy(w->join_ev);
   delete w;
   return XDEM_OK;
 }
@@ -513,7 +511,6 @@ int32_t xdem_get_stream(xdem_world w, void** s) {
 int32_t xdem_set_stream(xdem_world w, void* s) {
   if (!w) return XDEM_ERR_ARGUMENT;
   cudaStreamSynchronize(w->stream);
-  cudaStreamSynchronize(w->side);
   if (w->own_stream) cudaStreamDestroy(w->stream);
   if (s) {
     w->stream = static_cast<cudaStream_t>(s);
@@ -1102,11 +1099,15 @@ int32_t xdem_set_contacts(xdem_world w, const xdem_contacts* C) {
   // incoming references, so that a collect without an update sums these
   // contacts as the reference would
   std::vector<int32_t> inc(n, 0);
-  std::vector<uint32_t> inref(ks, 0);
+  std::vector<int32_t> id_at(n);
+  for (int i = 0; i < n; ++i) id_at[mpos[i]] = i;
+  std::vector<uint64_t> inref(ks, 0);
   for (int m = 0; m < n; ++m)
     for (int s = 0; s < cnt[m]; ++s) {
       int mj = mpos[partner[(size_t)s * n + m]];
-      if (inc[mj] < K) inref[(size_t)inc[mj] * n + mj] = (uint32_t)m * K + s;
+      if (inc[mj] < K)
+        inref[(size_t)inc[mj] * n + mj] =
+            ((uint64_t)(uint32_t)id_at[m] << 32) | (uint32_t)((uint32_t)m * K + s);
       else st |= XDEM_ERR_CAPACITY;
       inc[mj]++;
     }

@@ -482,10 +482,7 @@ __global__ void __launch_bounds__(128) k_collect(DevWorld w, int par) {
   double fx = 0.0, fy = 0.0, t = 0.0;
   {
     uint64_t key[kMaxSlots];  // owner id << 32 | reference
-    for (int a = 0; a < ninc; ++a) {
-      uint32_t ref = w.inref[(size_t)a * n + p];
-      key[a] = ((uint64_t)(uint32_t)w.id_of[ref / K] << 32) | ref;
-    }
+    for (int a = 0; a < ninc; ++a) key[a] = w.inref[(size_t)a * n + p];
     isort(key, ninc);
     for (int a = 0; a < ninc; ++a) {
       uint32_t ref = (uint32_t)key[a];

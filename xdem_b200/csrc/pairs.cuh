@@ -268,10 +268,12 @@ __device__ __forceinline__ void scan_cells(const DevWorld& w, const WorldScalars
 // Registers the contact in the owner's slot (m, slot) with its partner at
 // memory position mj, for the partner's force sum.  The arrival order is
 // free: k_collect orders the references by owner id.
-__device__ __forceinline__ void register_contact(const DevWorld& w, int mj, int m, int slot,
-                                                 uint32_t& st) {
+__device__ __forceinline__ void register_contact(const DevWorld& w, int mj, int owner_id, int m,
+                                                 int slot, uint32_t& st) {
   const int pos = atomicAdd(&w.incnt[mj], 1);
-  if (pos < w.K) w.inref[(size_t)pos * w.n + mj] = (uint32_t)m * (uint32_t)w.K + (uint32_t)slot;
+  if (pos < w.K)
+    w.inref[(size_t)pos * w.n + mj] = ((uint64_t)(uint32_t)owner_id << 32) |
+                                      ((uint32_t)m * (uint32_t)w.K + (uint32_t)slot);
   else st |= ST_CAPACITY;
 }
 
@@ -304,7 +306,7 @@ __device__ __forceinline__ int carry_over(const DevWorld& w, const Slots& old, c
     cur.bv2[ci] = old.bv2[oi];
     cur.fn[ci] = old.fn[oi];
     cur.ft[ci] = old.ft[oi];
-    register_contact(w, w.mpos[partner], m, k, st);
+    register_contact(w, w.mpos[partner], w.id_of[m], m, k, st);
     ++k;
   }
   return k;
@@ -578,7 +580,7 @@ __global__ void __launch_bounds__(128, 4) k_pair_forces(DevWorld w, int par, int
       cur.fn[ci] = make_double2(fn.x, fn.y);
       cur.ft[ci] = make_double2(fs.x, fs.y);
     }
-    register_contact(w, mj, m, slot, st);
+    register_contact(w, mj, ba.id, m, slot, st);
   }
   flush_warp(w, st, n_solves, n_iters, n_capped);
   if (WARM) flush_warm(w, w_off, w_used, w_rej, w_rest, w_right);

@@ -99,7 +99,7 @@ __device__ __forceinline__ void write_contact_m(const DevWorld& w, const WorldSc
     cur.fn[ci] = make_double2((double)fnx, (double)fny);
     cur.ft[ci] = make_double2((double)fsx, (double)fsy);
   }
-  register_contact(w, mj, m, slot, st);
+  register_contact(w, mj, ba.id, m, slot, st);
 }
 
 __device__ __forceinline__ void count_solve(uint32_t it, uint32_t& n_solves, uint32_t& n_iters) {
@@ -115,8 +115,9 @@ __device__ __forceinline__ void count_solve(uint32_t it, uint32_t& n_solves, uin
 //                 construction are deferred to k_pair_fallback_m;
 //   PASS_REGULAR  every listed pair but the deep ones (PairEntry::pad), with
 //                 the same deferral;
-//   PASS_DEEP     the deep pairs (the deep-pair list), on a second stream
-//                 beside PASS_REGULAR; the FP64 construction runs in place, so
+//   PASS_DEEP     the deep pairs (the deep-pair list), in k_pair_deep_m,
+//                 which runs beside PASS_REGULAR; the FP64 construction runs
+//                 in place, so
 //                 that the closest-approach Newton iterations that run to their
 //                 cap (deep overlaps) start with the step's other pairs
 //                 instead of after them.
@@ -249,12 +250,16 @@ __global__ void __launch_bounds__(128, 4) k_pair_forces_m(DevWorld w, int par, i
   flush_warp(w, st, n_solves, n_iters, n_capped);
 }
 
-// PASS_DEEP: a few blocks, registers as the FP64 construction needs them
+// PASS_DEEP: a few blocks, registers as the FP64 construction needs them;
+// launched ahead of the regular pass, which it lets start at once
 template <bool FOLD_BG, int LAW>
 __global__ void __launch_bounds__(128) k_pair_deep_m(DevWorld w, int par, int record) {
   if (stopped(w)) return;
   uint32_t st = 0, n_solves = 0, n_iters = 0, n_capped = 0;
   const int ndeep = *w.ndeep;
+  // the regular pair pass, launched after this kernel as a programmatic
+  // dependent launch, may start now
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ndeep; t += gridDim.x * blockDim.x)
     pair_forces_m<FOLD_BG, LAW, PASS_DEEP>(w, par, record, w.deep[t], st, n_solves, n_iters,
                                            n_capped);

@@ -159,7 +159,9 @@ struct DevWorld {
   // contacts
   Slots slots[2];
   int32_t* incnt;   // [n] contacts owned by lower ids
-  uint32_t* inref;  // [K*n] owner position*K + slot of those contacts
+  // [K*n] those contacts: owner id << 32 | owner position*K + slot (the
+  // force sum orders them by owner id without looking it up)
+  uint64_t* inref;
   PairEntry* pairs; // [K*n] pairs that passed the candidate scan
   int32_t* npairs;  // number of listed pairs (low half of pair_counts)
   int32_t* fallback;   // [K*n] mixed precision: listed pairs deferred to the FP64 construction
