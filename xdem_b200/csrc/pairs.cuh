@@ -98,9 +98,8 @@ __device__ __forceinline__ AxisShape axis_shape(const DevWorld& w, int m) {
   r -= 6.283185307179586 * rint(r * 0.15915494309189535);
   AxisShape e;
   __sincosf((float)r, &e.s, &e.c);
-  const double a = w.rad[m];
-  e.a = (float)a;
-  e.b = (float)(a / w.asp[m]);
+  e.a = (float)w.rad[m];
+  e.b = __fdividef(e.a, (float)w.asp[m]);
   return e;
 }
 
@@ -152,8 +151,8 @@ template <int LAW>
 __device__ __forceinline__ AxisShape owner_axis_shape(const DevWorld& w, int m, double2 cs) {
   AxisShape e{0.0f, 0.0f, 0.0f, 0.0f};
   if (centre_line_screen<LAW>(w)) {
-    const double a = w.rad[m];
-    e = AxisShape{(float)cs.x, (float)cs.y, (float)a, (float)(a / w.asp[m])};
+    const float a = (float)w.rad[m];
+    e = AxisShape{(float)cs.x, (float)cs.y, a, __fdividef(a, (float)w.asp[m])};
   }
   return e;
 }

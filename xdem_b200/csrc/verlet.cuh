@@ -190,6 +190,11 @@ __global__ void __launch_bounds__(128, 7) k_candidates_vl(DevWorld w, int par) {
             }
           }
         }
+        // the first four old partners in registers (the usual case); the
+        // others are read where they are
+        int op[4];
+#pragma unroll
+        for (int z = 0; z < 4; ++z) op[z] = z < nold ? old.partner[(size_t)z * n + m] : -1;
         for (int v = 0; v < cnt; ++v) {
           const int e = w.vl[(size_t)v * n + m];
           const int mj = e >> 2, kind = e & 3;
@@ -216,7 +221,10 @@ __global__ void __launch_bounds__(128, 7) k_candidates_vl(DevWorld w, int par) {
           }
           const int id_j = w.id_of[mj];
           int oslot = kNoOldSlot;
-          for (int z = 0; z < nold; ++z)
+#pragma unroll
+          for (int z = 0; z < 4; ++z)
+            if (op[z] == id_j) oslot = z;
+          for (int z = 4; z < nold; ++z)
             if (old.partner[(size_t)z * n + m] == id_j) oslot = z;
           // a pair that passed a distance test lies within one cell size,
           // so it is a candidate of the 3x3 scan (LAW_ANY's other pairs pass
