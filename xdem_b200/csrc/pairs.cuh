@@ -413,8 +413,9 @@ __global__ void __launch_bounds__(128) k_candidates(DevWorld w, int par) {
       const int up_i = w.up[m];
       const int shape_i = (LAW == LAW_ANY) ? w.shape[m] : 0;
       const double r_i = w.rad[m], orad_i = w.orad[m];
-      const int ix = cell_of(pi.x, ws.xmin, G.lx, G.nx);
-      const int iy = cell_of(pi.y, ws.ymin, G.ly, G.ny);
+      // the owner's cell from this step's binning (k_bin, the same cell_of)
+      const int cell_local = w.pcell[m] - G.base;
+      const int ix = cell_local % G.nx, iy = cell_local / G.nx;
       uint32_t matched = 0;
       scan_cells<LAW>(w, ws, G, m, ix, iy, pi, id_i, up_i, shape_i, r_i, orad_i, old, nold, nlist,
                       list_mj, list_code, st, matched, shape_ax);

@@ -84,8 +84,9 @@ __global__ void __launch_bounds__(128) k_vl_build(DevWorld w) {
   if (G.nx >= 3 && G.ny >= 3 && !(w.setting[m] & SKIP_CONTACT_DETECTION)) {
     const double2 pi = w.pos[m];
     const int id_i = w.id_of[m], up_i = w.up[m];
-    const int ix = cell_of(pi.x, ws.xmin, G.lx, G.nx);
-    const int iy = cell_of(pi.y, ws.ymin, G.ly, G.ny);
+    // the owner's cell from this step's binning (k_bin, the same cell_of)
+    const int cell_local = w.pcell[m] - G.base;
+    const int ix = cell_local % G.nx, iy = cell_local / G.nx;
     const float rxi = (float)(pi.x - (ws.xmin + ix * G.lx));
     const float ryi = (float)(pi.y - (ws.ymin + iy * G.ly));
     const float flx = (float)G.lx, fly = (float)G.ly;
@@ -153,8 +154,9 @@ __global__ void __launch_bounds__(128, 7) k_candidates_vl(DevWorld w, int par) {
       const int up_i = w.up[m];
       const int shape_i = (LAW == LAW_ANY) ? w.shape[m] : 0;
       const double r_i = w.rad[m], orad_i = w.orad[m];
-      const int ix = cell_of(pi.x, ws.xmin, G.lx, G.nx);
-      const int iy = cell_of(pi.y, ws.ymin, G.ly, G.ny);
+      // the owner's cell from this step's binning (k_bin, the same cell_of)
+      const int cell_local = w.pcell[m] - G.base;
+      const int ix = cell_local % G.nx, iy = cell_local / G.nx;
       const int cnt = w.vl_cnt[m];
       // old slots of listed pairs known to be candidates now (see below)
       uint32_t matched = 0;
