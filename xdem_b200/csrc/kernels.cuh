@@ -471,6 +471,23 @@ __device__ __forceinline__ void isort(T* key, int cnt) {
 // torqueOnP1), starting from zero as the reference's per-thread arrays do.
 // Particles with no contact are rattlers (BaseWorld.cpp:25,44-45).
 // ---------------------------------------------------------------------------
+template <class T>
+__device__ __forceinline__ void cmp_swap(T& a, T& b) {
+  const T lo = a < b ? a : b, hi = a < b ? b : a;
+  a = lo;
+  b = hi;
+}
+
+// ascending sort of eight keys held in registers (a 19-comparator network)
+template <class T>
+__device__ __forceinline__ void sort8(T* k) {
+  cmp_swap(k[0], k[1]); cmp_swap(k[2], k[3]); cmp_swap(k[4], k[5]); cmp_swap(k[6], k[7]);
+  cmp_swap(k[0], k[2]); cmp_swap(k[1], k[3]); cmp_swap(k[4], k[6]); cmp_swap(k[5], k[7]);
+  cmp_swap(k[1], k[2]); cmp_swap(k[5], k[6]); cmp_swap(k[0], k[4]); cmp_swap(k[3], k[7]);
+  cmp_swap(k[1], k[5]); cmp_swap(k[2], k[6]); cmp_swap(k[1], k[4]); cmp_swap(k[3], k[6]);
+  cmp_swap(k[2], k[4]); cmp_swap(k[3], k[5]); cmp_swap(k[3], k[4]);
+}
+
 __global__ void __launch_bounds__(128) k_collect(DevWorld w, int par) {
   if (stopped(w)) return;
   int p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -480,6 +497,48 @@ __global__ void __launch_bounds__(128) k_collect(DevWorld w, int par) {
   int nown = min(cur.count[p], K);
   int ninc = min(w.incnt[p], K);
   double fx = 0.0, fy = 0.0, t = 0.0;
+  if (ninc <= 8 && nown <= 8) {
+    // the usual case: both key sets sorted in registers, every load of a set
+    // in flight at once; the same order and operations as below
+    uint64_t ki[8];
+    uint32_t ko[8];
+#pragma unroll
+    for (int a = 0; a < 8; ++a) {
+      ki[a] = a < ninc ? w.inref[(size_t)a * n + p] : ~0ull;
+      const int partner = a < nown ? cur.partner[(size_t)a * n + p] : -1;
+      ko[a] = partner >= 0 ? (((uint32_t)partner << 5) | (uint32_t)a) : 0xffffffffu;
+    }
+    sort8(ki);
+    sort8(ko);
+#pragma unroll
+    for (int a = 0; a < 8; ++a) {
+      if (a < ninc) {
+        const uint32_t ref = (uint32_t)ki[a];
+        const size_t ci = (size_t)(ref % K) * n + ref / K;
+        const double2 F = cur.f[ci];
+        fx += -F.x;
+        fy += -F.y;
+        t += cur.t2[ci];
+      }
+    }
+    int nk = 0;
+#pragma unroll
+    for (int a = 0; a < 8; ++a) {
+      if (ko[a] != 0xffffffffu) {
+        const size_t ci = (size_t)(ko[a] & 31u) * n + p;
+        const double2 F = cur.f[ci];
+        fx += F.x;
+        fy += F.y;
+        t += cur.t1[ci];
+        ++nk;
+      }
+    }
+    w.force[p] = make_double2(fx, fy);
+    w.torque[p] = t;
+    w.ncp[p] = nk + ninc;
+    w.rattler[p] = (nk + ninc) == 0 ? 1 : 0;
+    return;
+  }
   {
     uint64_t key[kMaxSlots];  // owner id << 32 | reference
     for (int a = 0; a < ninc; ++a) key[a] = w.inref[(size_t)a * n + p];
