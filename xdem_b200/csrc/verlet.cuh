@@ -22,6 +22,7 @@
 namespace xdem {
 
 constexpr int kVlBlock = 256;
+constexpr int kVlGroup = 2;  // list entries whose loads k_candidates_vl issues together
 
 // block maxima of the path lengths since the last build
 __global__ void __launch_bounds__(kVlBlock) k_vl_maxdisp(DevWorld w) {
@@ -197,10 +198,28 @@ __global__ void __launch_bounds__(128, 7) k_candidates_vl(DevWorld w, int par) {
         int op[4];
 #pragma unroll
         for (int z = 0; z < 4; ++z) op[z] = z < nold ? old.partner[(size_t)z * n + m] : -1;
-        for (int v = 0; v < cnt; ++v) {
-          const int e = w.vl[(size_t)v * n + m];
+        // the list in groups of kVlGroup entries: the group's entries,
+        // positions and screening radii are loaded together (all in flight at
+        // once), then tested one by one as before
+        for (int v0 = 0; v0 < cnt; v0 += kVlGroup) {
+          int eg[kVlGroup];
+          double2 pg[kVlGroup];
+          double sg[kVlGroup];
+#pragma unroll
+          for (int u = 0; u < kVlGroup; ++u)
+            eg[u] = v0 + u < cnt ? w.vl[(size_t)(v0 + u) * n + m] : 0;
+#pragma unroll
+          for (int u = 0; u < kVlGroup; ++u) {
+            const bool in = v0 + u < cnt;
+            pg[u] = in ? w.pos[eg[u] >> 2] : make_double2(0.0, 0.0);
+            sg[u] = (in && LAW != LAW_ANY) ? w.screen_r[eg[u] >> 2] : 0.0;
+          }
+#pragma unroll
+          for (int u = 0; u < kVlGroup; ++u) {
+          if (v0 + u >= cnt) break;
+          const int e = eg[u];
           const int mj = e >> 2, kind = e & 3;
-          const double2 pj = w.pos[mj];
+          const double2 pj = pg[u];
           vec2<double> off, ovel;
           image_offset(ws, kind, pi, pj, off, ovel);
           bool pass;
@@ -208,8 +227,7 @@ __global__ void __launch_bounds__(128, 7) k_candidates_vl(DevWorld w, int par) {
             pass = coarse_pass<LAW>(shape_i, w.shape[mj], r_i, w.rad[mj], orad_i, w.orad[mj], pi,
                                     pj, off);
           else
-            pass = coarse_pass<LAW>(0, 0, r_i, w.screen_r[mj], orad_i, w.screen_r[mj], pi, pj,
-                                    off);
+            pass = coarse_pass<LAW>(0, 0, r_i, sg[u], orad_i, sg[u], pi, pj, off);
           if (!pass) continue;
           int cls = CL_REGULAR;
           if (centre_line_screen<LAW>(w)) {
@@ -239,6 +257,7 @@ __global__ void __launch_bounds__(128, 7) k_candidates_vl(DevWorld w, int par) {
           list_code[nlist] = kind | (nlist << 8) | (oslot << 16) |
                              (LAW == LAW_CLOSEST && cls == CL_DEEP ? kDeepFlag : 0);
           ++nlist;
+          }
         }
       }
       // old partners among the candidates
