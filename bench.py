@@ -271,15 +271,15 @@ def ncu_traffic_per_particle(kernel):
     return None
 
 
-def kernel_bytes(kernel, n, contacts, pairs):
+def kernel_bytes(kernel, n, contacts, pairs, entries=0):
     """Algorithmic DRAM bytes of one launch of a contact-update kernel, with
     every particle's data counted once (neighbour re-reads hit L2).
-    k_candidates: per particle the owner's data (position 16, id 4, setting 4,
-      up-level 4, radius 8, outer radius 8, screening radius 8, orientation 8,
-      old slot count 4) and its 20-byte screening record read by its
-      neighbours = 84 B, written: slot count 4, seen mask 4, orientation
-      cosines 16 = 24 B; per contact the old partner id 4 B; per listed pair a
-      16 B entry.
+    k_candidates (with candidate lists): per particle the owner's data
+      (position 16, velocity 16, orientation 8, spin 8, radius 8, aspect 8,
+      outer radius 8, shape 4, id 4, setting 4, up-level 4, cell 4, old slot
+      count 4, list length 4) = 100 B, written: its body record 96 B and its
+      slot count 4 B = 200 B; per list entry 4 B; per contact the old partner
+      id 4 B; per listed pair a 16 B entry.
     k_pair_forces: per particle the state the geometry reads (position 16,
       velocity 16, orientation 8, spin 8, radius 8, aspect 8, outer radius 8,
       shape 4, mass 8, setting 4, id 4) = 92 B; per listed pair its entry 16 B;
@@ -288,7 +288,7 @@ def kernel_bytes(kernel, n, contacts, pairs):
       damping 8, force 16, torques 16, branch vector 16 = 92 B); per listed
       pair that does not touch, an empty-slot mark (4 B)."""
     if kernel == "k_candidates":
-        return 108.0 * n + 4.0 * contacts + 16.0 * pairs
+        return 200.0 * n + 4.0 * entries + 4.0 * contacts + 16.0 * pairs
     return 92.0 * n + 16.0 * pairs + 136.0 * contacts + 4.0 * max(pairs - contacts, 0)
 
 
@@ -531,7 +531,8 @@ def measure(work, precision, args, dist, full=True, net=None):
     kname = max(("k_candidates", "k_pair_forces"), key=lambda k: prof.get(k, (1, 0.0))[1])
     upd = prof[kname]
     avg_s = upd[1] / upd[0] / 1e3
-    alg_bytes = kernel_bytes(kname, n, contacts, pairs)
+    lists = w.candidate_list_stats()
+    alg_bytes = kernel_bytes(kname, n, contacts, pairs, lists["entries"])
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / avg_s / 1e9
     traffic_pp = ncu_traffic_per_particle(kname)
