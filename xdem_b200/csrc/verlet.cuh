@@ -121,7 +121,8 @@ __global__ void __launch_bounds__(128) k_vl_build(DevWorld w) {
 
 // k_candidates with the lists: same outputs (slot counts, carried-over
 // history, the compact pair list, orientation cosines), the same filters and
-// tests.
+// tests.  Seven blocks per SM (72 registers): the kernel is latency-bound on
+// its partner gathers, and six blocks with more registers measured slower.
 template <int LAW>
 __global__ void __launch_bounds__(128, 7) k_candidates_vl(DevWorld w, int par) {
   if (stopped(w)) return;
