@@ -38,8 +38,10 @@ enum xdem_status_bits {
      (PeriodicBoundaryWorld.cpp:75-78 exits with -2), or a particle ran out of
      history slots (no reference counterpart: its hash map grows) */
   XDEM_ERR_CAPACITY = 1 << 0,
-  /* closest-approach Newton iteration hit its cap (EllipticParticle.cpp:621
-     has no cap and can loop forever) */
+  /* a closest-approach Newton iteration did not terminate: it repeated an
+     earlier iterate (it would cycle forever) or reached 1,000 iterations
+     (EllipticParticle.cpp:621 has no cap and never returns there); the
+     quartic's root between the analytic start and 1 was taken by bisection */
   XDEM_ERR_NEWTON = 1 << 1,
   /* non-finite position/velocity/force detected */
   XDEM_ERR_NONFINITE = 1 << 2,
@@ -300,7 +302,7 @@ int32_t xdem_set_max_strain_rate(xdem_world w, double rate);
 /* kinetic energy (BaseWorld.cpp:302-310) */
 int32_t xdem_get_kinetic_energy(xdem_world w, double* out);
 /* closest-approach Newton statistics since creation or the last reset:
-   out = {solves, iterations, solves stopped by the iteration cap}
+   out = {solves, iterations, solves that did not terminate (a repeated iterate or the cap)}
    (NewtonRaphsonForQuartic, EllipticParticle.cpp:613-626) */
 int32_t xdem_get_newton_stats(xdem_world w, int64_t out[3]);
 int32_t xdem_reset_newton_stats(xdem_world w);
@@ -320,6 +322,17 @@ int32_t xdem_get_pair_count(xdem_world w, int64_t* out);
    library's build (native byte order, structure sizes checked). */
 int32_t xdem_save_snapshot(xdem_world w, const char* path);
 int32_t xdem_load_snapshot(xdem_world w, const char* path);
+/* Host only (no device needed): reads and checks a snapshot file as
+   xdem_load_snapshot does before it touches the device (sizes against the
+   file length, systems covering ids [0, n) in order, the saved memory order a
+   permutation within each system, contact ids in range); out = {n, systems,
+   contacts, world kind}.  XDEM_ERR_ARGUMENT for a missing, truncated or
+   inconsistent file. */
+int32_t xdem_snapshot_info(const char* path, int64_t out[4]);
+/* Byte layout of this build's snapshot files: {header size, size of one
+   system's scalar record, offset of its first-id field, offset of its
+   particle-count field}. */
+int32_t xdem_snapshot_layout(int64_t out[4]);
 
 /* ---- observables ---------------------------------------------------------- */
 /* QuadronAnalysis's rattler-free coordination number and solid fraction
@@ -420,6 +433,12 @@ int32_t xdem_get_launch_config(xdem_world w, int32_t* pair_blocks_per_sm, double
    build); skin_fraction in
    (0, 1] (default 0.1).  Call before xdem_set_particles. */
 int32_t xdem_set_candidate_lists(xdem_world w, int32_t capacity, double skin_fraction);
+/* Steps between refreshes of the particles' memory order on the device (no
+   counterpart in the reference, whose particles stay in id order).  The
+   arrays are re-sorted by cell every `interval` steps so that neighbours sit
+   at nearby addresses; results do not depend on it.  interval: odd, or 0 =
+   never re-sort; default 31. */
+int32_t xdem_set_memory_order_refresh(xdem_world w, int32_t interval);
 /* out = {list rebuilds since the last xdem_reset_newton_stats, longest list,
    total entries, capacity} */
 int32_t xdem_get_candidate_list_stats(xdem_world w, int64_t out[4]);
@@ -513,7 +532,9 @@ int32_t xdem_get_warm_stats(xdem_world w, int64_t out[5]);
    contacts per call (4,194,304; more returns XDEM_ERR_CAPACITY), and calls
    that may overlap on the GPU race on that array and must be ordered by the
    caller.  The first call on a device looks the array up for that device:
-   make it with the device current and before any stream capture begins. */
+   make it with the device current and before any stream capture begins.  The
+   address is kept for the life of the process, so the entry point must not be
+   used on a device after a cudaDeviceReset there. */
 int32_t xdem_total_stress_noalloc(int64_t ncontacts, const double* fx, const double* fy,
                                   const double* bx, const double* by, double area,
                                   double* stress, void* cuda_stream);

@@ -28,9 +28,15 @@ _port = None
 _ref = None
 
 
-def build(ref_src="/root/reference/src"):
-    """make -C oracle (the restatement always; the reference when its sources exist)."""
-    subprocess.run(["make", "-s", "-C", HERE, f"REF_SRC={ref_src}"], check=True)
+def build(ref_src=None):
+    """make -C oracle (the restatement always; the reference when its sources
+    exist).  ref_src: the reference's src/ folder; default the environment
+    variable XDEM_REFERENCE_SRC, else the Makefile's own default."""
+    ref_src = ref_src or os.environ.get("XDEM_REFERENCE_SRC")
+    cmd = ["make", "-s", "-C", HERE]
+    if ref_src:
+        cmd.append(f"REF_SRC={ref_src}")
+    subprocess.run(cmd, check=True)
 
 
 def ref_available():
@@ -80,7 +86,10 @@ def port_lib():
         lib.xo_status.restype = C.c_uint32
         lib.xo_status.argtypes = [C.c_void_p]
         lib.xo_newton_quartic.restype = C.c_double
-        lib.xo_newton_quartic.argtypes = [C.c_double] * 6 + [_i]
+        lib.xo_newton_quartic.argtypes = [C.c_double] * 6 + [_i, _i]
+        lib.xo_bisect_quartic.restype = C.c_double
+        lib.xo_bisect_quartic.argtypes = [C.c_double] * 7
+        _port["bisect_quartic"] = lib.xo_bisect_quartic
         _port["status"] = lib.xo_status
         _port["newton_quartic"] = lib.xo_newton_quartic
     return _port
@@ -231,6 +240,12 @@ def ref_particle_properties(shape, radius, aspect, density=1.0):
 
 
 def newton_quartic(A, B, Cc, D, E, init):
+    """(iterate, iterations, stuck) of the checker's Newton iteration."""
     it = C.c_int32(0)
-    r = port_lib()["newton_quartic"](A, B, Cc, D, E, init, C.byref(it))
-    return r, it.value
+    stuck = C.c_int32(0)
+    r = port_lib()["newton_quartic"](A, B, Cc, D, E, init, C.byref(it), C.byref(stuck))
+    return r, it.value, bool(stuck.value)
+
+
+def bisect_quartic(A, B, Cc, D, E, s, q):
+    return port_lib()["bisect_quartic"](A, B, Cc, D, E, s, q)

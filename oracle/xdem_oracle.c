@@ -129,10 +129,16 @@ static int circle_circle(const pstate_t* a, const pstate_t* b, v2 off, v2 ovel, 
   return 1;
 }
 
-/* EllipticParticle::NewtonRaphsonForQuartic (EllipticParticle.cpp:613-626),
-   with an iteration cap the reference lacks. */
+/* EllipticParticle::NewtonRaphsonForQuartic (EllipticParticle.cpp:613-626).
+   The reference's loop has no cap and never ends on some deeply overlapping
+   pairs.  Its iteration is a function of the iterate alone, so an iterate
+   equal to an earlier one (and not within the tolerance of its predecessor)
+   means the loop cycles forever; Brent's test (compare each iterate with the
+   one saved at the last power-of-two step) finds the repeat.  *stuck is set on
+   a repeat or at XO_NEWTON_CAP iterations; otherwise the result is the
+   reference's. */
 double xo_newton_quartic(double A, double B, double C, double D, double E, double init,
-                         int32_t* iters) {
+                         int32_t* iters, int32_t* stuck) {
   double A0 = 4.0 * A;
   double B0 = 3.0 * B;
   double C0 = 2.0 * C;
@@ -140,15 +146,61 @@ double xo_newton_quartic(double A, double B, double C, double D, double E, doubl
   double r = 0.0;
   double tol = 1e-10;
   int it = 0;
+  double saved = init;
+  int power = 1, lam = 0;
+  int st = 0;
   while (fabs(r0 - r) > tol) {
-    if (it >= XO_NEWTON_CAP) break;
+    if (it >= XO_NEWTON_CAP) {
+      st = 1;
+      break;
+    }
     r = r0;
     r0 -= (A * (r0 * r0 * r0 * r0) + B * (r0 * r0 * r0) + C * (r0 * r0) + D * r0 + E) /
           (A0 * (r0 * r0 * r0) + B0 * (r0 * r0) + C0 * r0 + D);
     ++it;
+    if (r0 == saved && fabs(r0 - r) > tol) {
+      st = 1;
+      break;
+    }
+    if (++lam == power) {
+      saved = r0;
+      power <<= 1;
+      lam = 0;
+    }
   }
   if (iters) *iters = it;
+  if (stuck) *stuck = st;
   return r0;
+}
+
+static double quartic_at(double A, double B, double C, double D, double E, double q) {
+  return A * (q * q * q * q) + B * (q * q * q) + C * (q * q) + D * q + E;
+}
+
+/* Where the Newton iteration never ends: the quartic's root in
+   [min(1, s), max(1, s)] (s = sqrt(δ+1), the analytic start) by bisection to
+   adjacent doubles; without a sign change there the iterate q is kept. */
+double xo_bisect_quartic(double A, double B, double C, double D, double E, double s, double q) {
+  double lo = fmin(1.0, s), hi = fmax(1.0, s);
+  if (!(lo < hi)) return q;
+  double flo = quartic_at(A, B, C, D, E, lo);
+  double fhi = quartic_at(A, B, C, D, E, hi);
+  if (flo == 0.0) return lo;
+  if (fhi == 0.0) return hi;
+  if (!((flo < 0.0) != (fhi < 0.0))) return q;
+  for (int k = 0; k < 80; ++k) {
+    double mid = 0.5 * (lo + hi);
+    if (!(mid > lo && mid < hi)) break;
+    double fm = quartic_at(A, B, C, D, E, mid);
+    if (fm == 0.0) return mid;
+    if ((fm < 0.0) == (flo < 0.0)) {
+      lo = mid;
+      flo = fm;
+    } else {
+      hi = mid;
+    }
+  }
+  return 0.5 * (lo + hi);
 }
 
 /* EllipticParticle::contactWithEllipticParticle, closest approach
@@ -205,10 +257,14 @@ static int ellipse_closest(const pstate_t* a, const pstate_t* b, v2 off, v2 ovel
   double C = -tanPhi2 - (1.0 + delta) * (1.0 + delta) + (1.0 + (1.0 + delta) * tanPhi2) / (b2p * b2p);
   double D = 2.0 * (1.0 + tanPhi2) * (1.0 + delta) / b2p;
   double E = (1.0 + tanPhi2 + delta) * (1.0 + delta);
-  int32_t it = 0;
-  double q = xo_newton_quartic(A, B, C, D, E, sqrt(delta + 1.0), &it);
+  int32_t it = 0, stuck = 0;
+  double start = sqrt(delta + 1.0);
+  double q = xo_newton_quartic(A, B, C, D, E, start, &it, &stuck);
+  if (stuck) {
+    q = xo_bisect_quartic(A, B, C, D, E, start, q);
+    *st |= XDEM_ERR_NEWTON;
+  }
   g->iters = it;
-  if (it >= XO_NEWTON_CAP) *st |= XDEM_ERR_NEWTON;
   double temp = (q * q - 1.0) / delta;
   double d_prime = 0.0;
   if (temp < 0) temp = 0.0;

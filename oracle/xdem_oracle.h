@@ -11,8 +11,11 @@
  *     ids (ascending owner), then own contacts (ascending partner); the
  *     reference's single-thread order is the same except that own contacts
  *     follow unordered_map iteration order (BaseWorld.cpp:26-56);
- *   - the closest-approach Newton loop stops after XO_NEWTON_CAP iterations
- *     and raises XDEM_ERR_NEWTON (EllipticParticle.cpp:621 has no cap);
+ *   - the closest-approach Newton loop stops when it repeats an earlier
+ *     iterate (it would cycle forever) or after XO_NEWTON_CAP iterations,
+ *     takes the quartic's root on [min(1, s), max(1, s)] by bisection, and
+ *     raises XDEM_ERR_NEWTON (EllipticParticle.cpp:621 has no cap and does
+ *     not return there);
  *   - errors that exit() in the reference raise status bits instead.
  */
 #ifndef XDEM_ORACLE_H
@@ -47,9 +50,12 @@ void xo_quadron_z_phi(xo_world* w, double* out);
 
 int32_t xo_pair_geometry(int32_t npairs, int32_t method, const double* pi, const double* pj,
                          const double* off, double* out);
-/* Newton on A r^4 + B r^3 + C r^2 + D r + E from init; *iters gets the count
-   (XO_NEWTON_CAP when it did not converge). */
+/* Newton on A r^4 + B r^3 + C r^2 + D r + E from init; *iters gets the count,
+   *stuck 1 when the iteration repeated an earlier iterate or reached
+   XO_NEWTON_CAP (either may be NULL). */
 double xo_newton_quartic(double A, double B, double C, double D, double E, double init,
-                         int32_t* iters);
+                         int32_t* iters, int32_t* stuck);
+/* the root on [min(1, s), max(1, s)] by bisection (q if no sign change) */
+double xo_bisect_quartic(double A, double B, double C, double D, double E, double s, double q);
 
 #endif

@@ -223,7 +223,25 @@ def controls():
                                   scale_rattlers=0.99, sequence=abi.SEQ_SUBSTEPS),
         "uniform": make_control(update_stress=True, box_law=abi.BOX_STRESS_UNIFORM, p0=5.0,
                                 reset_rattlers=True),
+        # updatePeriodicBoundary_stressControlUniform_strainLimit
+        # (PeriodicControlWorld.cpp:215-237); needs setup_control (max strain rate)
+        "uniform_limit": make_control(update_stress=True, box_law=abi.BOX_STRESS_UNIFORM_LIMIT,
+                                      p0=5.0, reset_rattlers=True),
     }
+
+
+# max strain rate of the "uniform_limit" control: the box velocity grows by
+# (p0 - p) L dt per step, so the limit (rate * L / 2) binds after a few tens of
+# steps and the law runs both branches within a short trajectory
+UNIFORM_LIMIT_MAX_STRAIN_RATE = 0.05
+
+
+def setup_control(name, *worlds):
+    """World settings a control of controls() needs (setMaxStrainRate,
+    PeriodicControlWorld.cpp:69-71, for the strain-limited law)."""
+    if name == "uniform_limit":
+        for w in worlds:
+            w.setMaxStrainRate(UNIFORM_LIMIT_MAX_STRAIN_RATE)
 
 
 def dense_ellipse_case(n=3000, seed=21, kind=abi.WORLD_LEES_EDWARDS, phi=0.85, aspect=inputs.c4_aspect,

@@ -22,7 +22,7 @@ import oracle
 from xdem_b200 import abi
 from xdem_b200.world import World, make_control, pair_geometry
 
-from helpers import (clump_case, compare_contacts, compare_pair_geometry, compare_states, controls,
+from helpers import (setup_control, clump_case, compare_contacts, compare_pair_geometry, compare_states, controls,
                      disc_case, ellipse_case, rel_err, same_pairs)
 
 pytestmark = pytest.mark.gpu
@@ -112,16 +112,6 @@ def test_pair_geometry_circles():
     assert og[:10, 0].all()
 
 
-def test_newton_cap_raises_status():
-    """The input that cycles forever in the reference's uncapped Newton loop
-    (EllipticParticle.cpp:621) stops at the cap on the host restatement, and
-    the product reports XDEM_ERR_NEWTON rather than hanging."""
-    A, B, C, D, E = (-0.26036636837902971, -0.32298145246944276, 0.12112405448664837,
-                     0.28164745468898272, 0.087345098145840058)
-    r, it = oracle.newton_quartic(A, B, C, D, E, 0.51812102010664518)
-    assert it == 1000
-
-
 @pytest.mark.parametrize("kind", [abi.WORLD_PERIODIC, abi.WORLD_PERIODIC_CONTROL,
                                   abi.WORLD_LEES_EDWARDS])
 def test_discs_one_step(kind):
@@ -144,11 +134,13 @@ def test_ellipses_one_step(kind, method):
     _compare_worlds(g, c, ONE_STEP_TOL)
 
 
-@pytest.mark.parametrize("name", ["plain", "stress", "strain", "stress_xy", "uniform"])
+@pytest.mark.parametrize("name", ["plain", "stress", "strain", "stress_xy", "uniform",
+                                  "uniform_limit"])
 def test_discs_trajectory_controls(name):
     kind = abi.WORLD_PERIODIC_CONTROL if name != "plain" else abi.WORLD_PERIODIC
     p, prm = disc_case(n=300, phi=0.80, seed=4, kind=kind)
     g, c = _pair(p, prm)
+    setup_control(name, g, c)
     ctl = controls()[name]
     assert g.run(50, ctl) == 50
     assert c.run(50, ctl) == 50

@@ -17,7 +17,7 @@ import pytest
 import oracle
 from xdem_b200 import abi, inputs
 
-from helpers import (clump_case, compare_contacts, compare_states, controls, disc_case,
+from helpers import (setup_control, clump_case, compare_contacts, compare_states, controls, disc_case,
                      ellipse_case, rel_err, same_pairs, segment_case)
 
 pytestmark = [pytest.mark.reference,
@@ -112,11 +112,13 @@ def test_ellipses_one_step(kind, method):
     compare_states(r.get_state(), c.get_state(), 1e-15)
 
 
-@pytest.mark.parametrize("name", ["plain", "stress", "strain", "stress_xy", "uniform"])
+@pytest.mark.parametrize("name", ["plain", "stress", "strain", "stress_xy", "uniform",
+                                  "uniform_limit"])
 def test_discs_trajectory_controls(name):
     kind = abi.WORLD_PERIODIC_CONTROL if name != "plain" else abi.WORLD_PERIODIC
     p, prm = disc_case(n=250, phi=0.80, seed=23, kind=kind)
     r, c = _worlds(p, prm)
+    setup_control(name, r, c)
     ctl = controls()[name]
     assert r.run(40, ctl) == c.run(40, ctl) == 40
     compare_contacts(r.get_contacts(), c.get_contacts(), 1e-10)

@@ -91,3 +91,38 @@ def test_noalloc_limits():
                                          C.c_void_p(out.data_ptr()), None) == abi.OK
     torch.cuda.synchronize()
     assert np.all(out.cpu().numpy() == 0.0)
+
+
+def _stress_sum_bound(fx, fy, bx, by, area):
+    """numpy's sum and the sum of |terms| that bounds any summation order's
+    rounding (relative 1e-12 of it is far above 4M terms times one ulp)."""
+    terms = [fx * bx, fx * by, fy * bx, fy * by]
+    ref = np.array([t.sum() for t in terms]) / area
+    mag = np.array([np.abs(t).sum() for t in terms]) / area
+    return ref, mag
+
+
+@pytest.mark.parametrize("ncontacts", [300_000, 4 * 1024 * 1024])
+def test_noalloc_many_blocks_and_the_cap_on_a_stream(ncontacts):
+    """Synthetic contacts: about 300k (the final pass loops over more than
+    256 block partials) and exactly the stated maximum, queued on a torch
+    stream rather than the default one; each compared with numpy's sum."""
+    torch = pytest.importorskip("torch")
+    lib = abi.load_library()
+    assert ncontacts <= lib.xdem_total_stress_noalloc_max_contacts()
+    rng = np.random.default_rng(ncontacts)
+    fx, fy, bx, by = (rng.normal(0.0, 1.0, ncontacts) for _ in range(4))
+    area = 1234.5
+    ref, mag = _stress_sum_bound(fx, fy, bx, by, area)
+    stream = torch.cuda.Stream()
+    with torch.cuda.stream(stream):
+        dev = [torch.tensor(a, dtype=torch.float64, device="cuda") for a in (fx, fy, bx, by)]
+        out = torch.full((4,), float("nan"), dtype=torch.float64, device="cuda")
+    stream.synchronize()
+    for _ in range(2):
+        st = lib.xdem_total_stress_noalloc(ncontacts, *[C.c_void_p(t.data_ptr()) for t in dev], area,
+                                           C.c_void_p(out.data_ptr()), C.c_void_p(stream.cuda_stream))
+        assert st == abi.OK
+        stream.synchronize()
+        s = out.cpu().numpy()
+        assert np.all(np.abs(s - ref) <= 1e-12 * mag), (s, ref)

@@ -255,6 +255,9 @@ def load_library(path=LIB_PATH):
         "xdem_set_launch_config": (C.c_int32, [W, C.c_int32, C.c_double]),
         "xdem_set_candidate_lists": (C.c_int32, [W, C.c_int32, C.c_double]),
         "xdem_get_candidate_list_stats": (C.c_int32, [W, P(C.c_int64)]),
+        "xdem_set_memory_order_refresh": (C.c_int32, [W, C.c_int32]),
+        "xdem_snapshot_info": (C.c_int32, [C.c_char_p, P(C.c_int64)]),
+        "xdem_snapshot_layout": (C.c_int32, [P(C.c_int64)]),
         "xdem_get_launch_config": (C.c_int32, [W, P(C.c_int32), P(C.c_double)]),
         "xdem_autotune": (C.c_int32, [W, P(Control), C.c_int32, _d]),
         "xdem_mlp_create": (C.c_int32, [C.c_uint64, P(W)]),

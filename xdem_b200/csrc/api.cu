@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstddef>
 #include <cmath>
 #include <cstdio>
 #include <cstdint>
@@ -26,9 +27,12 @@ namespace {
 
 constexpr int kBlock = 128;
 constexpr int kDefaultSlots = 24;
-// steps between memory-order refreshes; odd, so that a captured chunk (one
-// re-sort + kResortEvery steps) swaps the slot sets an even number of times
+// default steps between memory-order refreshes; odd, so that a captured
+// chunk (one re-sort + kResortEvery steps) swaps the slot sets an even number
+// of times
 constexpr int kResortEvery = 31;
+// since_resort value that makes the next step refresh the memory order
+constexpr int kResortDue = 1 << 30;
 constexpr double kPi = 3.14159265358979323846;
 
 inline int blocks_for(int n, int b) { return (n + b - 1) / b; }
@@ -73,7 +77,10 @@ struct xdem_world_s {
   size_t prof_used = 0;                  // pairs recorded
   int64_t launches = 0;
   cudaEvent_t timer[2] = {nullptr, nullptr};
-  int since_resort = kResortEvery;  // steps since the memory order was refreshed
+  int since_resort = kResortDue;  // steps since the memory order was refreshed
+  // steps between memory-order refreshes (odd), 0 = never
+  // (xdem_set_memory_order_refresh)
+  int resort_every = kResortEvery;
   int law = LAW_ANY;                // contact-kernel specialisation for the shapes present
   xdem_mlp_s* mlp = nullptr;        // learned warm start of the closest-approach Newton iteration
   PermList perm{};                  // particle arrays moved by a re-sort
@@ -208,6 +215,25 @@ void launch_find(xdem_world_s* w) {
   LAUNCH(w, KK_SCATTER, k_scatter<<<nb, kBlock, 0, w->stream>>>(w->dw));
 }
 
+// A pair kernel (DevWorld, slot-set parity, record) on the world's stream as
+// a programmatic dependent launch: it may start while the kernel before it
+// (which signals with griddepcontrol.launch_dependents) still runs.  The
+// launch after it is an ordinary one and waits for both.
+void launch_dependent(xdem_world_s* w, int blocks, void (*kernel)(DevWorld, int, int), int record) {
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(blocks);
+  cfg.blockDim = dim3(128);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = w->stream;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cuda_check(w, cudaLaunchKernelEx(&cfg, kernel, w->dw, w->par, record));
+  w->launches++;
+}
+
 // updateContacts as candidate scan, per-pair forces, and history carry-over
 // (pairs.cuh); the pair kernel runs a grid-stride loop over the listed pairs
 template <bool FOLD_BG, int LAW>
@@ -239,19 +265,7 @@ void launch_update_phases(xdem_world_s* w, int record) {
       LAUNCH(w, KK_PAIRS, k_pair_forces_m<FOLD_BG, LAW, PASS_REGULAR><<<pb, 128, 0, w->stream>>>(
                               w->dw, w->par, record));
     } else {
-      cudaLaunchAttribute attr[1];
-      attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-      attr[0].val.programmaticStreamSerializationAllowed = 1;
-      cudaLaunchConfig_t cfg = {};
-      cfg.gridDim = dim3(pb);
-      cfg.blockDim = dim3(128);
-      cfg.dynamicSmemBytes = 0;
-      cfg.stream = w->stream;
-      cfg.attrs = attr;
-      cfg.numAttrs = 1;
-      cuda_check(w, cudaLaunchKernelEx(&cfg, k_pair_forces_m<FOLD_BG, LAW, PASS_REGULAR>, w->dw,
-                                       w->par, record));
-      w->launches++;
+      launch_dependent(w, pb, k_pair_forces_m<FOLD_BG, LAW, PASS_REGULAR>, record);
     }
     LAUNCH(w, KK_FALLBACK, k_pair_fallback_m<FOLD_BG, LAW><<<148 * 4, 128, 0, w->stream>>>(
                                w->dw, w->par, record));
@@ -274,6 +288,17 @@ void launch_update_phases(xdem_world_s* w, int record) {
            k_mlp_warm<LAW><<<148 * 4, 128, 0, w->stream>>>(w->dw, w->mlp->dev(), w->dw.npairs, nullptr));
     LAUNCH(w, KK_PAIRS,
            k_pair_forces<FOLD_BG, LAW, true><<<pb, 128, 0, w->stream>>>(w->dw, w->par, record));
+  } else if (LAW == LAW_CLOSEST) {
+    // as in mixed precision: the deep pairs first, the regular pass beside
+    // them as a programmatic dependent launch (an ordinary launch while the
+    // kernels are timed one by one)
+    LAUNCH(w, KK_DEEP, k_pair_deep<FOLD_BG, LAW><<<148 * 2, 128, 0, w->stream>>>(w->dw, w->par, record));
+    if (w->prof_on) {
+      LAUNCH(w, KK_PAIRS, k_pair_forces<FOLD_BG, LAW, false, PASS64_REGULAR><<<pb, 128, 0, w->stream>>>(
+                              w->dw, w->par, record));
+    } else {
+      launch_dependent(w, pb, k_pair_forces<FOLD_BG, LAW, false, PASS64_REGULAR>, record);
+    }
   } else {
     LAUNCH(w, KK_PAIRS,
            k_pair_forces<FOLD_BG, LAW><<<pb, 128, 0, w->stream>>>(w->dw, w->par, record));
@@ -370,9 +395,9 @@ void enqueue_step(xdem_world_s* w, const xdem_control* ctl, int record, bool res
 }
 
 // a step with the re-sort policy: the memory order is refreshed every
-// kResortEvery steps
+// resort_every steps (never when it is 0)
 void policy_step(xdem_world_s* w, const xdem_control* ctl, int record) {
-  bool resort = w->since_resort >= kResortEvery;
+  bool resort = w->resort_every > 0 && w->since_resort >= w->resort_every;
   if (resort) w->since_resort = 0;
   enqueue_step(w, ctl, record, resort);
   w->since_resort++;
@@ -777,7 +802,8 @@ int32_t set_particles_impl(xdem_world_s* w, const xdem_particles* P, const std::
   CK(w, B.alloc(&d.fallback, w->prm.precision == XDEM_PRECISION_MIXED ? ks : 1));
   CK(w, B.alloc(&d.nfallback, 1));
   CK(w, cudaMemsetAsync(d.nfallback, 0, sizeof(int32_t), s));
-  CK(w, B.alloc(&d.deep, w->prm.precision == XDEM_PRECISION_MIXED ? ks : 1));
+  // the deep-pair list serves closest-approach worlds of both precisions
+  CK(w, B.alloc(&d.deep, ks));
   d.warm = nullptr;
   if (w->mlp) CK(w, B.alloc(&d.warm, ks));
   // candidate lists: rebuilt by the first step (vl_valid starts at 0)
@@ -851,7 +877,7 @@ int32_t set_particles_impl(xdem_world_s* w, const xdem_particles* P, const std::
   }
   CK(w, B.alloc(&d.scratch, off));
   w->par = 0;
-  w->since_resort = kResortEvery;
+  w->since_resort = kResortDue;
   CK(w, cudaStreamSynchronize(s));
   return XDEM_OK;
 }
@@ -1439,6 +1465,87 @@ cudaError_t by_id(xdem_world_s* w, const T* src, const std::vector<int32_t>& id_
   return download_by_id(w, out.data(), src, id_of);
 }
 
+// A snapshot file read into host memory and checked in full before any of
+// it reaches the device: the header's sizes against the file's length, the
+// systems (in order, each non-empty, together covering ids [0, n) with no gap
+// or overlap), and the saved memory order (a permutation that keeps every
+// system in its own id range).  Any failure is XDEM_ERR_ARGUMENT.
+struct SnapData {
+  SnapHeader h{};
+  std::vector<WorldScalars> all;
+  std::vector<int32_t> ints[5];
+  std::vector<double> dbl[16];
+  std::vector<int32_t> mem_id;
+  std::vector<double> segv[4];
+  std::vector<int32_t> ci, cj;
+  std::vector<std::vector<double>> cd;
+};
+
+int32_t read_snapshot(const char* path, SnapData& d) {
+  FileCloser fc{fopen(path, "rb")};
+  if (!fc.f) return XDEM_ERR_ARGUMENT;
+  if (fseek(fc.f, 0, SEEK_END) != 0) return XDEM_ERR_ARGUMENT;
+  const long long fsize = (long long)ftell(fc.f);
+  if (fsize < 0 || fseek(fc.f, 0, SEEK_SET) != 0) return XDEM_ERR_ARGUMENT;
+  SnapHeader& h = d.h;
+  if (!get(fc.f, &h, 1) || std::memcmp(h.magic, kSnapMagic, 8) != 0 || h.version != 1 ||
+      h.scalars_bytes != sizeof(WorldScalars) || h.params_bytes != sizeof(xdem_params) ||
+      h.n <= 0 || h.nsys == 0 || h.nsys > (uint32_t)h.n || h.ncontacts < 0 ||
+      (h.has_seg != 0 && h.has_seg != 1))
+    return XDEM_ERR_ARGUMENT;
+  const long long n = h.n, nsys = h.nsys, nc = h.ncontacts;
+  // the exact length the header implies (checked before anything is sized by it)
+  const long long per_particle = 5 * 4 + 16 * 8 + 4 + (h.has_seg ? 4 * 8 : 0);
+  if (nc > (fsize / 8)) return XDEM_ERR_ARGUMENT;
+  const long long want = (long long)sizeof(SnapHeader) + nsys * (long long)sizeof(WorldScalars) +
+                         n * per_particle + nc * (2 * 4 + 19 * 8);
+  if (want != fsize) return XDEM_ERR_ARGUMENT;
+  d.all.resize(nsys);
+  bool ok = get(fc.f, d.all.data(), nsys);
+  for (int k = 0; k < 5 && ok; ++k) {
+    d.ints[k].resize(n);
+    ok = get(fc.f, d.ints[k].data(), n);
+  }
+  for (int k = 0; k < 16 && ok; ++k) {
+    d.dbl[k].resize(n);
+    ok = get(fc.f, d.dbl[k].data(), n);
+  }
+  d.mem_id.resize(n);
+  ok = ok && get(fc.f, d.mem_id.data(), n);
+  for (int k = 0; k < 4 && ok && h.has_seg; ++k) {
+    d.segv[k].resize(n);
+    ok = get(fc.f, d.segv[k].data(), n);
+  }
+  d.ci.resize(nc);
+  d.cj.resize(nc);
+  d.cd.assign(19, std::vector<double>(nc));
+  ok = ok && get(fc.f, d.ci.data(), nc) && get(fc.f, d.cj.data(), nc);
+  for (int k = 0; k < 19 && ok; ++k) ok = get(fc.f, d.cd[k].data(), nc);
+  if (!ok) return XDEM_ERR_ARGUMENT;
+  // systems: consecutive, non-empty, covering [0, n)
+  long long next = 0;
+  for (long long k = 0; k < nsys; ++k) {
+    const WorldScalars& o = d.all[k];
+    if (o.first != next || o.count <= 0 || (long long)o.first + o.count > n) return XDEM_ERR_ARGUMENT;
+    next = (long long)o.first + o.count;
+  }
+  if (next != n) return XDEM_ERR_ARGUMENT;
+  // memory order: a permutation of each system's id range
+  std::vector<char> taken(n, 0);
+  for (long long k = 0; k < nsys; ++k) {
+    const int lo = d.all[k].first, hi = d.all[k].first + d.all[k].count;
+    for (int m = lo; m < hi; ++m) {
+      const int id = d.mem_id[m];
+      if (id < lo || id >= hi || taken[id]) return XDEM_ERR_ARGUMENT;
+      taken[id] = 1;
+    }
+  }
+  // contact ids inside the world (xdem_set_contacts checks the rest)
+  for (long long c = 0; c < nc; ++c)
+    if (d.ci[c] < 0 || d.ci[c] >= n || d.cj[c] < 0 || d.cj[c] >= n) return XDEM_ERR_ARGUMENT;
+  return XDEM_OK;
+}
+
 }  // namespace
 extern "C" {
 
@@ -1542,40 +1649,21 @@ int32_t xdem_save_snapshot(xdem_world w, const char* path) {
 
 int32_t xdem_load_snapshot(xdem_world w, const char* path) {
   if (!w || !path) return XDEM_ERR_ARGUMENT;
-  FileCloser fc{fopen(path, "rb")};
-  if (!fc.f) return XDEM_ERR_ARGUMENT;
-  SnapHeader h{};
-  if (!get(fc.f, &h, 1) || std::memcmp(h.magic, kSnapMagic, 8) != 0 || h.version != 1 ||
-      h.scalars_bytes != sizeof(WorldScalars) || h.params_bytes != sizeof(xdem_params) ||
-      h.n <= 0 || h.nsys == 0 || h.ncontacts < 0 || h.prm.world_kind != w->prm.world_kind)
-    return XDEM_ERR_ARGUMENT;
+  SnapData sd;
+  if (int32_t e = read_snapshot(path, sd)) return e;
+  SnapHeader& h = sd.h;
+  if (h.prm.world_kind != w->prm.world_kind) return XDEM_ERR_ARGUMENT;
   const int n = h.n;
   const int nsys = (int)h.nsys;
-  std::vector<WorldScalars> all(nsys);
-  std::vector<int32_t> ints[5];
-  std::vector<double> dbl[16];
-  bool ok = get(fc.f, all.data(), nsys);
-  for (int k = 0; k < 5 && ok; ++k) {
-    ints[k].resize(n);
-    ok = get(fc.f, ints[k].data(), n);
-  }
-  for (int k = 0; k < 16 && ok; ++k) {
-    dbl[k].resize(n);
-    ok = get(fc.f, dbl[k].data(), n);
-  }
-  std::vector<int32_t> mem_id(n);
-  ok = ok && get(fc.f, mem_id.data(), n);
-  std::vector<double> segv[4];
-  for (int k = 0; k < 4 && ok && h.has_seg; ++k) {
-    segv[k].resize(n);
-    ok = get(fc.f, segv[k].data(), n);
-  }
+  std::vector<WorldScalars>& all = sd.all;
+  std::vector<int32_t>* ints = sd.ints;
+  std::vector<double>* dbl = sd.dbl;
+  std::vector<int32_t>& mem_id = sd.mem_id;
+  std::vector<double>* segv = sd.segv;
   const int64_t nc = h.ncontacts;
-  std::vector<int32_t> ci(nc), cj(nc);
-  std::vector<std::vector<double>> cd(19, std::vector<double>(nc));
-  ok = ok && get(fc.f, ci.data(), nc) && get(fc.f, cj.data(), nc);
-  for (int k = 0; k < 19 && ok; ++k) ok = get(fc.f, cd[k].data(), nc);
-  if (!ok) return XDEM_ERR_ARGUMENT;
+  std::vector<int32_t>& ci = sd.ci;
+  std::vector<int32_t>& cj = sd.cj;
+  std::vector<std::vector<double>>& cd = sd.cd;
   // the particles (the snapshot's contact-model and run settings are restored
   // below; its precision, ellipse law and slot count are the world's own)
   w->prm.dt = h.prm.dt;
@@ -1618,15 +1706,10 @@ int32_t xdem_load_snapshot(xdem_world w, const char* path) {
     sys[k].box[3] = all[k].ymax;
     sys[k].dt = all[k].dt;
   }
-  // the memory order: a permutation keeping every system in its id range
+  // the memory order (read_snapshot checked it is a permutation keeping
+  // every system in its id range)
   std::vector<int32_t> newpos(n, -1);
-  for (int k = 0; k < nsys; ++k)
-    for (int m = sys[k].first; m < sys[k].first + sys[k].count; ++m) {
-      const int id = mem_id[m];
-      if (id < sys[k].first || id >= sys[k].first + sys[k].count || newpos[id] >= 0)
-        return XDEM_ERR_ARGUMENT;
-      newpos[id] = m;
-    }
+  for (int m = 0; m < n; ++m) newpos[mem_id[m]] = m;
   int32_t st = set_particles_impl(w, &P, sys);
   if (st) return st;
   // set_particles leaves memory order = id order: move every particle array
@@ -1636,7 +1719,7 @@ int32_t xdem_load_snapshot(xdem_world w, const char* path) {
   CK(w, cudaGetLastError());
   k_copy_back<<<blocks_for(n, kBlock), kBlock, 0, w->stream>>>(w->dw, w->perm);
   CK(w, cudaGetLastError());
-  w->since_resort = std::max(0, std::min(h.since_resort, kResortEvery));
+  w->since_resort = std::max(0, std::min(h.since_resort, kResortDue));
   // the world scalars of every system: box, time step, contact model,
   // Lees-Edwards and box-law state, the last stress
   CK(w, modify_all(w, [&](WorldScalars& s, int k) {
@@ -1680,6 +1763,26 @@ int32_t xdem_load_snapshot(xdem_world w, const char* path) {
     st = xdem_set_contacts(w, &c);
     if (st) return st;
   }
+  return XDEM_OK;
+}
+
+int32_t xdem_snapshot_info(const char* path, int64_t out[4]) {
+  if (!path || !out) return XDEM_ERR_ARGUMENT;
+  SnapData sd;
+  if (int32_t e = read_snapshot(path, sd)) return e;
+  out[0] = sd.h.n;
+  out[1] = sd.h.nsys;
+  out[2] = sd.h.ncontacts;
+  out[3] = sd.h.prm.world_kind;
+  return XDEM_OK;
+}
+
+int32_t xdem_snapshot_layout(int64_t out[4]) {
+  if (!out) return XDEM_ERR_ARGUMENT;
+  out[0] = (int64_t)sizeof(SnapHeader);
+  out[1] = (int64_t)sizeof(WorldScalars);
+  out[2] = (int64_t)offsetof(WorldScalars, first);
+  out[3] = (int64_t)offsetof(WorldScalars, count);
   return XDEM_OK;
 }
 
@@ -1776,6 +1879,15 @@ int32_t xdem_set_candidate_lists(xdem_world w, int32_t capacity, double skin_fra
   if (w->dw.n > 0) return XDEM_ERR_ARGUMENT;  // before xdem_set_particles
   w->vl_capacity = capacity;
   w->skin_fraction = skin_fraction;
+  return XDEM_OK;
+}
+
+int32_t xdem_set_memory_order_refresh(xdem_world w, int32_t interval) {
+  // odd: a captured chunk (one re-sort and `interval` steps) must swap the
+  // slot sets an even number of times
+  if (!w || interval < 0 || (interval > 0 && (interval % 2) == 0) || interval > (1 << 20))
+    return XDEM_ERR_ARGUMENT;
+  w->resort_every = interval;
   return XDEM_OK;
 }
 
@@ -2017,18 +2129,20 @@ int32_t xdem_run(xdem_world w, int32_t nsteps, const xdem_control* ctl, int32_t*
   const int rec_all = ctl->stop_on_pressure ? 1 : 0;
   int body = nsteps - 1;
   // direct steps until a re-sort is due, then whole chunks (one re-sort and
-  // kResortEvery steps) captured once in a CUDA graph and replayed
-  while (body > 0 && w->since_resort < kResortEvery) {
+  // resort_every steps, or 32 steps without re-sorts) captured once in a
+  // CUDA graph and replayed
+  const int chunk = w->resort_every > 0 ? w->resort_every : 32;
+  while (w->resort_every > 0 && body > 0 && w->since_resort < w->resort_every) {
     policy_step(w, ctl, rec_all);
     --body;
   }
-  if (body >= kResortEvery && !w->prof_on) {
+  if (body >= chunk && !w->prof_on) {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     const int par0 = w->par;
     const int64_t launches_before = w->launches;
     CK(w, cudaStreamBeginCapture(w->stream, cudaStreamCaptureModeThreadLocal));
-    for (int k = 0; k < kResortEvery; ++k) policy_step(w, ctl, rec_all);
+    for (int k = 0; k < chunk; ++k) policy_step(w, ctl, rec_all);
     cudaError_t e = cudaStreamEndCapture(w->stream, &graph);
     if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
     if (e != cudaSuccess) {
@@ -2037,11 +2151,11 @@ int32_t xdem_run(xdem_world w, int32_t nsteps, const xdem_control* ctl, int32_t*
     }
     // a chunk swaps the slot sets an even number of times: parity unchanged
     w->par = par0;
-    const int reps = body / kResortEvery;
+    const int reps = body / chunk;
     const int64_t per_chunk = w->launches - launches_before;
     w->launches += per_chunk * (reps - 1);
     for (int r = 0; r < reps && e == cudaSuccess; ++r) e = cudaGraphLaunch(exec, w->stream);
-    body -= reps * kResortEvery;
+    body -= reps * chunk;
     cudaGraphExecDestroy(exec);
     cudaGraphDestroy(graph);
     CK(w, e);

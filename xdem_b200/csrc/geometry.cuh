@@ -8,9 +8,12 @@
 
 namespace xdem {
 
-// The reference loop (EllipticParticle.cpp:621) has no cap and cycles forever
-// on some deeply overlapping pairs; some converging pairs of dense packings
-// need several hundred iterations from the analytic start.
+// The reference loop (EllipticParticle.cpp:621) has no cap and never ends on
+// some deeply overlapping pairs (δ < 0, the iterate wanders among negative
+// values where the quartic has no root); some converging pairs of dense
+// packings need several hundred iterations from the analytic start.  The
+// iteration here stops when it repeats an earlier iterate exactly (it would
+// then cycle forever) or at this cap.
 constexpr int kNewtonCap = 1000;
 
 enum : uint32_t {
@@ -38,6 +41,8 @@ struct Geom {
   int iters;
   int warm;  // learned warm start: 0 not offered, 1 used, 2 rejected by the residual test,
              // 3 used but the root left its interval (the plain start decided)
+  int stuck;  // closest approach: Newton did not terminate (repeat or cap); the root
+              // was then found by bisection (newton_quartic, bisect_quartic)
   vec2<double> cp, n, bv1, bv2;
   double overlap;
   vec2<double> rv, nrv, srv;
@@ -144,10 +149,16 @@ __device__ __forceinline__ bool segment_circle(const PState& a, double4 va, cons
   return true;
 }
 
-// EllipticParticle::NewtonRaphsonForQuartic (EllipticParticle.cpp:613-626),
-// capped at kNewtonCap iterations.
+// EllipticParticle::NewtonRaphsonForQuartic (EllipticParticle.cpp:613-626).
+// The reference's iteration is a function of the iterate alone, so an iterate
+// equal to an earlier one (not within the tolerance of its predecessor) means
+// the loop would cycle forever there; Brent's cycle test (compare each
+// iterate with the one saved at the last power-of-two step) finds such a
+// repeat within twice the cycle's length after its start.  `stuck` is set
+// on a repeat or at kNewtonCap iterations; the operations are the
+// reference's, so wherever the reference returns, the result is its own.
 __device__ __forceinline__ double newton_quartic(double A, double B, double C, double D, double E,
-                                                 double init, int& iters) {
+                                                 double init, int& iters, bool& stuck) {
   double A0 = 4.0 * A;
   double B0 = 3.0 * B;
   double C0 = 2.0 * C;
@@ -155,17 +166,70 @@ __device__ __forceinline__ double newton_quartic(double A, double B, double C, d
   double r = 0.0;
   const double tol = 1e-10;
   int it = 0;
+  double saved = init;
+  int power = 1, lam = 0;
+  stuck = false;
   while (fabs(r0 - r) > tol) {
-    if (it >= kNewtonCap) break;
+    if (it >= kNewtonCap) {
+      stuck = true;
+      break;
+    }
     r = r0;
     double p2 = r0 * r0;
     double p3 = p2 * r0;
     double p4 = p3 * r0;
     r0 -= (A * p4 + B * p3 + C * p2 + D * r0 + E) / (A0 * p3 + B0 * p2 + C0 * r0 + D);
     ++it;
+    if (r0 == saved && fabs(r0 - r) > tol) {
+      stuck = true;
+      break;
+    }
+    if (++lam == power) {
+      saved = r0;
+      power <<= 1;
+      lam = 0;
+    }
   }
   iters = it;
   return r0;
+}
+
+// the quartic A q^4 + B q^3 + C q^2 + D q + E, Horner-free as in the Newton step
+__device__ __forceinline__ double quartic_at(double A, double B, double C, double D, double E,
+                                             double q) {
+  double p2 = q * q;
+  double p3 = p2 * q;
+  double p4 = p3 * q;
+  return A * p4 + B * p3 + C * p2 + D * q + E;
+}
+
+// Where the reference's Newton iteration never ends (newton_quartic's
+// `stuck`), the root it is meant to find: the quartic's root in
+// [min(1, s), max(1, s)], s = sqrt(δ+1) the analytic start, by bisection to
+// adjacent doubles (no division, a fixed sequence of operations).  Without a
+// sign change on that interval the iterate q is kept.
+__device__ __forceinline__ double bisect_quartic(double A, double B, double C, double D, double E,
+                                                 double s, double q) {
+  double lo = fmin(1.0, s), hi = fmax(1.0, s);
+  if (!(lo < hi)) return q;
+  double flo = quartic_at(A, B, C, D, E, lo);
+  const double fhi = quartic_at(A, B, C, D, E, hi);
+  if (flo == 0.0) return lo;
+  if (fhi == 0.0) return hi;
+  if (!((flo < 0.0) != (fhi < 0.0))) return q;
+  for (int k = 0; k < 80; ++k) {
+    const double mid = 0.5 * (lo + hi);
+    if (!(mid > lo && mid < hi)) break;
+    const double fm = quartic_at(A, B, C, D, E, mid);
+    if (fm == 0.0) return mid;
+    if ((fm < 0.0) == (flo < 0.0)) {
+      lo = mid;
+      flo = fm;
+    } else {
+      hi = mid;
+    }
+  }
+  return 0.5 * (lo + hi);
 }
 
 // Largest Newton step accepted at a learned warm start, relative to the start
@@ -265,17 +329,22 @@ __device__ __forceinline__ bool ellipse_closest(const PState& a, const PState& b
       }
     }
   }
-  double q = newton_quartic(A, B, C, D, E, init, it);
-  if (WARM && g.warm == 1 && !(q >= lo * (1.0 - 1e-9) && q <= hi * (1.0 + 1e-9))) {
+  bool stuck = false;
+  double q = newton_quartic(A, B, C, D, E, init, it, stuck);
+  if (WARM && g.warm == 1 && (stuck || !(q >= lo * (1.0 - 1e-9) && q <= hi * (1.0 + 1e-9)))) {
     int it2 = 0;
-    q = newton_quartic(A, B, C, D, E, start, it2);
+    q = newton_quartic(A, B, C, D, E, start, it2, stuck);
     it += it2;
     g.warm = 3;
   }
+  if (stuck) {
+    q = bisect_quartic(A, B, C, D, E, start, q);
+    st |= ST_NEWTON;
+  }
   g.iters = it;
+  g.stuck = stuck ? 1 : 0;
   g.q = q;
   g.q_start = start;
-  if (it >= kNewtonCap) st |= ST_NEWTON;
   double temp = (q * q - 1.0) / delta;
   double d_prime = 0.0;
   if (temp < 0) temp = 0.0;

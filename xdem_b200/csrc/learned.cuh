@@ -84,7 +84,7 @@ __global__ void __launch_bounds__(128) k_harvest(DevWorld w, MlpDev net, int str
         // a target exists when Newton ran, converged, and its root lies in the
         // interval between 1 and the analytic start that the warm start uses
         const double lo = fmin(1.0, g.q_start), hi = fmax(1.0, g.q_start);
-        const bool root = g.iters > 0 && g.iters < kNewtonCap && g.q_start > 0.0 &&
+        const bool root = g.iters > 0 && !g.stuck && g.q_start > 0.0 &&
                           g.q >= lo * (1.0 - 1e-9) && g.q <= hi * (1.0 + 1e-9);
         tg = root ? (float)(g.q / g.q_start) : __int_as_float(0x7fc00000);
         ct = touching ? 1.0f : 0.0f;

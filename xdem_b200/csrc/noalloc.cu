@@ -24,7 +24,12 @@
 //     same call;
 //   - the first call on a device looks up the scratch address for that device,
 //     which needs that device to be current; make that first call before any
-//     stream capture begins.
+//     stream capture begins;
+//   - the address is kept for the life of the process: a cudaDeviceReset (or
+//     anything else that destroys the device's primary context) unloads the
+//     array, so this entry point must not be called on that device after one;
+//   - the status reports this call's own launches only (each launch's return
+//     code), never an error an earlier, unrelated runtime call left behind.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -125,12 +130,21 @@ extern "C" int32_t xdem_total_stress_noalloc(int64_t ncontacts, const double* fx
   if (scratch_address(&partials) != cudaSuccess) return XDEM_ERR_CUDA;
   cudaStream_t s = static_cast<cudaStream_t>(cuda_stream);
   int nblocks = (int)((ncontacts + kNoallocPerBlock - 1) / kNoallocPerBlock);
-  if (nblocks > 0)
-    k_noalloc_stress_blocks<<<nblocks, kNoallocThreads, 0, s>>>(ncontacts, fx, fy, bx, by,
-                                                                 partials, nblocks);
+  long long nc = ncontacts;
+  // launched through cudaLaunchKernel, whose return code is this launch's own
+  if (nblocks > 0) {
+    void* args[] = {&nc, &fx, &fy, &bx, &by, &partials, &nblocks};
+    if (cudaLaunchKernel((const void*)k_noalloc_stress_blocks, dim3(nblocks), dim3(kNoallocThreads),
+                         args, 0, s) != cudaSuccess)
+      return XDEM_ERR_CUDA;
+  }
   // with no contacts the final pass reads no partials and writes zeros
-  k_noalloc_stress_final<<<1, kNoallocThreads, 0, s>>>(partials, nblocks, area, stress);
-  return cudaGetLastError() == cudaSuccess ? XDEM_OK : XDEM_ERR_CUDA;
+  const double* cpartials = partials;
+  void* fargs[] = {&cpartials, &nblocks, &area, &stress};
+  if (cudaLaunchKernel((const void*)k_noalloc_stress_final, dim3(1), dim3(kNoallocThreads), fargs, 0,
+                       s) != cudaSuccess)
+    return XDEM_ERR_CUDA;
+  return XDEM_OK;
 }
 
 extern "C" int64_t xdem_total_stress_noalloc_max_contacts(void) { return kNoallocMaxContacts; }

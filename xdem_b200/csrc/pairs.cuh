@@ -139,18 +139,27 @@ __device__ __forceinline__ int centre_line_class(float dx, float dy, const AxisS
 // list) that the centre-line screen classed deep
 constexpr int kDeepFlag = 1 << 24;
 
-// the centre-line screen applies to mixed-precision worlds of ellipses under
-// one law
+// the centre-line screen (dropping separated pairs) applies to
+// mixed-precision worlds of ellipses under one law
 template <int LAW>
 __device__ __forceinline__ bool centre_line_screen(const DevWorld& w) {
   return (LAW == LAW_CLOSEST || LAW == LAW_INTERSECTION) && w.precision == XDEM_PRECISION_MIXED;
+}
+
+// the centre-line class is computed for those worlds and for every
+// closest-approach world, whose deep pairs are evaluated in a pass of their
+// own in both precisions (the FP64 path drops nothing: the class only orders
+// the evaluation)
+template <int LAW>
+__device__ __forceinline__ bool centre_line_classes(const DevWorld& w) {
+  return LAW == LAW_CLOSEST || centre_line_screen<LAW>(w);
 }
 
 // the owner's record for the screen, from the (cos, sin) of its body record
 template <int LAW>
 __device__ __forceinline__ AxisShape owner_axis_shape(const DevWorld& w, int m, double2 cs) {
   AxisShape e{0.0f, 0.0f, 0.0f, 0.0f};
-  if (centre_line_screen<LAW>(w)) {
+  if (centre_line_classes<LAW>(w)) {
     const float a = (float)w.rad[m];
     e = AxisShape{(float)cs.x, (float)cs.y, a, __fdividef(a, (float)w.asp[m])};
   }
@@ -239,14 +248,14 @@ __device__ __forceinline__ void scan_cells(const DevWorld& w, const WorldScalars
         if (!pass) continue;
       }
       int cls = CL_REGULAR;
-      if (centre_line_screen<LAW>(w)) {
+      if (centre_line_classes<LAW>(w)) {
         // the same FP64 image offset as the candidate lists' test (verlet.cuh)
         const double2 pj = w.cell_pos[q];
         vec2<double> off, ovel;
         image_offset(ws, kind, pi, pj, off, ovel);
         cls = centre_line_class((float)((pj.x + off.x) - pi.x), (float)((pj.y + off.y) - pi.y),
                                 shape_ax, axis_shape(w, w.cell_mem[q]));
-        if (cls == CL_SEPARATED) continue;
+        if (cls == CL_SEPARATED && centre_line_screen<LAW>(w)) continue;
       }
       if (nlist >= K) {
         st |= ST_CAPACITY;
@@ -467,19 +476,30 @@ __device__ __forceinline__ void flush_warm(const DevWorld& w, uint32_t offered, 
   }
 }
 
-// WARM: closest-approach pairs start Newton from the learned warm start of
-// their list entry (w.warm, written by k_mlp_warm)
-template <bool FOLD_BG, int LAW, bool WARM = false>
-__global__ void __launch_bounds__(128, 4) k_pair_forces(DevWorld w, int par, int record) {
-  if (stopped(w)) return;
-  const int n = w.n;
-  const Slots& old = w.slots[par];
-  const Slots& cur = w.slots[par ^ 1];
-  const int npairs = *w.npairs;
+// Counters of one thread of a pair kernel, flushed per warp at its end.
+struct PairCounters {
   uint32_t st = 0;
   uint32_t n_solves = 0, n_iters = 0, n_capped = 0;
   uint32_t w_off = 0, w_used = 0, w_rej = 0, w_rest = 0, w_right = 0;
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < npairs; t += gridDim.x * blockDim.x) {
+};
+
+// Which listed pairs a launch of the FP64 pair kernel evaluates: all of them,
+// or all but the deep ones (PairEntry::pad), which k_pair_deep evaluates
+// beside it.  Every pair is evaluated by the same operations whichever pass
+// takes it.
+enum { PASS64_ALL = 0, PASS64_REGULAR = 1 };
+
+// One listed pair t: image offset, contact geometry, history and force,
+// written to the owner's slot.  WARM: a closest-approach pair starts Newton
+// from the learned warm start of its list entry (w.warm, k_mlp_warm).
+template <bool FOLD_BG, int LAW, bool WARM>
+__device__ __forceinline__ void pair_forces_fp64(const DevWorld& w, int par, int record, int t,
+                                                 PairCounters& pc) {
+  const int n = w.n;
+  const Slots& old = w.slots[par];
+  const Slots& cur = w.slots[par ^ 1];
+  uint32_t& st = pc.st;
+  {
     const PairEntry e = w.pairs[t];
     const int m = e.m, mj = e.mj;
     const WorldScalars& ws = w.ws[sys_at(w, m)];
@@ -514,20 +534,20 @@ __global__ void __launch_bounds__(128, 4) k_pair_forces(DevWorld w, int par, int
           a, b, 0.0, 0.0, off, ovel, csa, csb, g, st, wp.x);
     }
     if (WARM && LAW == LAW_CLOSEST && g.warm) {
-      w_off++;
-      w_used += g.warm == 1 || g.warm == 3;
-      w_rej += g.warm == 2;
-      w_rest += g.warm == 3;
-      w_right += (wp.y > 0.0f) == touching;
+      pc.w_off++;
+      pc.w_used += g.warm == 1 || g.warm == 3;
+      pc.w_rej += g.warm == 2;
+      pc.w_rest += g.warm == 3;
+      pc.w_right += (wp.y > 0.0f) == touching;
     }
     if (LAW != LAW_CIRCLE && g.iters > 0) {
-      n_solves++;
-      n_iters += g.iters;
-      n_capped += g.iters >= kNewtonCap ? 1u : 0u;
+      pc.n_solves++;
+      pc.n_iters += g.iters;
+      pc.n_capped += g.stuck ? 1u : 0u;
     }
     if (!touching) {
       cur.partner[ci] = -1;
-      continue;
+      return;
     }
     const int id_j = bb.id;
     // BaseParticle::calculateContactForceAndTorque (BaseParticle.cpp:27-98)
@@ -582,8 +602,35 @@ __global__ void __launch_bounds__(128, 4) k_pair_forces(DevWorld w, int par, int
     }
     register_contact(w, mj, ba.id, m, slot, st);
   }
-  flush_warp(w, st, n_solves, n_iters, n_capped);
-  if (WARM) flush_warm(w, w_off, w_used, w_rej, w_rest, w_right);
+}
+
+template <bool FOLD_BG, int LAW, bool WARM = false, int PASS = PASS64_ALL>
+__global__ void __launch_bounds__(128, 4) k_pair_forces(DevWorld w, int par, int record) {
+  if (stopped(w)) return;
+  const int npairs = *w.npairs;
+  PairCounters pc;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < npairs; t += gridDim.x * blockDim.x) {
+    if (PASS == PASS64_REGULAR && w.pairs[t].pad) continue;
+    pair_forces_fp64<FOLD_BG, LAW, WARM>(w, par, record, t, pc);
+  }
+  flush_warp(w, pc.st, pc.n_solves, pc.n_iters, pc.n_capped);
+  if (WARM) flush_warm(w, pc.w_off, pc.w_used, pc.w_rej, pc.w_rest, pc.w_right);
+}
+
+// The deep pairs of a closest-approach world (the deep-pair list written by
+// the candidate kernels), launched ahead of the regular pass, which may start
+// at once (a programmatic dependent launch): the Newton iterations that run
+// long (deep overlaps) then start with the step's other pairs instead of
+// ending the pair phase as a serial tail.
+template <bool FOLD_BG, int LAW>
+__global__ void __launch_bounds__(128) k_pair_deep(DevWorld w, int par, int record) {
+  if (stopped(w)) return;
+  const int ndeep = *w.ndeep;
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  PairCounters pc;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ndeep; t += gridDim.x * blockDim.x)
+    pair_forces_fp64<FOLD_BG, LAW, false>(w, par, record, w.deep[t], pc);
+  flush_warp(w, pc.st, pc.n_solves, pc.n_iters, pc.n_capped);
 }
 
 // ---- end of the update ----------------------------------------------------------

@@ -189,7 +189,7 @@ __device__ __forceinline__ void pair_forces_m(const DevWorld& w, int par, int re
         if (gd.iters > 0) {
           n_solves++;
           n_iters += gd.iters;
-          n_capped += gd.iters >= kNewtonCap ? 1u : 0u;
+          n_capped += gd.stuck ? 1u : 0u;
         }
         res = PW_NONE;
         if (touching) {
@@ -302,7 +302,7 @@ __global__ void __launch_bounds__(128) k_pair_fallback_m(DevWorld w, int par, in
     if (gd.iters > 0) {
       n_solves++;
       n_iters += gd.iters;
-      n_capped += gd.iters >= kNewtonCap ? 1u : 0u;
+      n_capped += gd.stuck ? 1u : 0u;
     }
     if (!touching) {
       cur.partner[ci] = -1;

@@ -231,10 +231,10 @@ __global__ void __launch_bounds__(128, 7) k_candidates_vl(DevWorld w, int par) {
             pass = coarse_pass<LAW>(0, 0, r_i, sg[u], orad_i, sg[u], pi, pj, off);
           if (!pass) continue;
           int cls = CL_REGULAR;
-          if (centre_line_screen<LAW>(w)) {
+          if (centre_line_classes<LAW>(w)) {
             cls = centre_line_class((float)((pj.x + off.x) - pi.x), (float)((pj.y + off.y) - pi.y),
                                     shape_ax, axis_shape(w, mj));
-            if (cls == CL_SEPARATED) continue;
+            if (cls == CL_SEPARATED && centre_line_screen<LAW>(w)) continue;
           }
           if (nlist >= K) {
             st |= ST_CAPACITY;

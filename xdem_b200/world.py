@@ -421,6 +421,11 @@ class World(WorldBase):
         self._check(self.lib.xdem_set_candidate_lists(self.h, capacity, skin_fraction),
                     "set_candidate_lists")
 
+    def set_memory_order_refresh(self, interval):
+        """Steps between re-sorts of the device memory order (odd; 0 = never)."""
+        self._check(self.lib.xdem_set_memory_order_refresh(self.h, interval),
+                    "set_memory_order_refresh")
+
     def candidate_list_stats(self):
         """{builds, longest, entries, capacity} of the candidate lists"""
         out = (C.c_int64 * 4)()
