@@ -61,6 +61,17 @@ def log(*a):
 # ---------------------------------------------------------------------------
 # workloads
 # ---------------------------------------------------------------------------
+def config_le_ellipses(n):
+    """The workload's description, the same in both arms (values that depend
+    on the random sample are reported beside it, in workload_numbers)."""
+    return {"workload": f"lees_edwards_shear_ellipses_{n}", "n_particles": n,
+            "world": "LeesEdwardsBoundaryWorld",
+            "contact_law": "closest approach (Zheng-Palffy-Muhoray quartic, Newton)",
+            "aspect_ratio": "U[1,3]", "b": "{0.5,0.7}", "solid_fraction": 0.85,
+            "shear_rate": "1e-3*sqrt(kn/m_min)", "dt": "0.02*sqrt(m_min/kn)",
+            "l2": "inputs larger than L2 (state + contact history resident in HBM)"}
+
+
 def workload_le_ellipses(n, seed):
     """Lees-Edwards shear of ellipses, a/b ~ U[1,3], b in {0.5,0.7}, phi 0.85."""
     from xdem_b200 import abi, inputs, packing
@@ -74,22 +85,20 @@ def workload_le_ellipses(n, seed):
     q, contacts, b, info = packing.compress(p, box, 0.85, dt, steps=4000, relax=2000)
     log(f"setup: compressed phi {info['phi0']:.3f} -> {info['phi']:.4f} in {info['steps']} steps "
         f"+ {info['relax']} relaxation steps, {time.time() - t:.1f}s, "
-        f"{info['capped_newton']} capped Newton solves")
+        f"{info['capped_newton']} non-terminating Newton solves")
     prm = make_params(abi.WORLD_LEES_EDWARDS, dt, b, inputs.KN, inputs.KT, inputs.RESTITUTION,
                       inputs.FRICTION, shift_strain_rate=rate)
     return {"particles": q, "contacts": contacts, "params": prm, "control": make_control(),
             # the compiled reference's Newton loop (EllipticParticle.cpp:621) has no
             # iteration cap and never returns on the few deeply overlapping pairs of
-            # this packing that cycle (the GPU run counts them as capped solves), so
-            # the CPU leg runs the C restatement, identical but for that cap
+            # this packing that cycle, so the full-size CPU leg runs the C
+            # restatement, identical but for stopping those
             "cpu_kind": "port",
-            "cpu_note": "C restatement of the reference (capped Newton; the compiled reference "
-                        "does not return on this packing's cycling Newton pairs)",
-            "config": {"workload": f"lees_edwards_shear_ellipses_{n}", "n_particles": n,
-                       "world": "LeesEdwardsBoundaryWorld",
-                       "contact_law": "closest approach (Zheng-Palffy-Muhoray quartic, Newton)",
-                       "aspect_ratio": "U[1,3]", "b": "{0.5,0.7}",
-                       "solid_fraction": round(info["phi"], 4), "shear_rate": rate, "dt": dt}}
+            "cpu_note": "C restatement of the reference (it stops the Newton iterations the "
+                        "compiled reference never returns from)",
+            "config": config_le_ellipses(n),
+            "numbers": {"solid_fraction_reached": round(info["phi"], 5), "shear_rate": rate,
+                        "dt": dt}}
 
 
 def train_warm_start(seed, n=262144, target_pairs=10_000_000, epochs=12):
@@ -131,6 +140,12 @@ def train_warm_start(seed, n=262144, target_pairs=10_000_000, epochs=12):
     return net, info
 
 
+def config_periodic_discs(n):
+    return {"workload": f"periodic_discs_{n}", "n_particles": n, "world": "PeriodicBoundaryWorld",
+            "contact_law": "disc-disc", "radii": "{0.5,0.7}", "solid_fraction": 0.70,
+            "dt": "0.02*sqrt(m_min/kn)"}
+
+
 def workload_periodic_discs(n, seed):
     """Bidisperse discs r 0.5/0.7 at phi 0.70, PeriodicBoundaryWorld (config-0 recipe at size n)."""
     from xdem_b200 import abi, inputs
@@ -141,9 +156,7 @@ def workload_periodic_discs(n, seed):
                       inputs.FRICTION)
     return {"particles": p, "contacts": None, "params": prm, "control": make_control(),
             "cpu_kind": "reference", "cpu_note": "compiled reference sources (oracle/_ref)",
-            "config": {"workload": f"periodic_discs_{n}", "n_particles": n,
-                       "world": "PeriodicBoundaryWorld", "contact_law": "disc-disc",
-                       "radii": "{0.5,0.7}", "solid_fraction": 0.70, "dt": dt}}
+            "config": config_periodic_discs(n), "numbers": {"dt": dt}}
 
 
 def workload_batch_ensemble(n_systems, seed):
@@ -191,6 +204,76 @@ def workload_batch_ensemble(n_systems, seed):
                        "n_particles": n, "world": "PeriodicBoundaryWorld (batched)",
                        "system_kinds": counts, "particles_per_system": "log-uniform [1000, 50000]",
                        "solid_fraction": "U[0.6, 0.8]"}}
+
+
+def cpu_sample_le_ellipses(n_sample, seed, threads):
+    """A bounded sample of the Lees-Edwards ellipse shear made on the CPU only
+    (no product library): n_sample ellipses of the workload's shapes, RSA,
+    compression to solid fraction 0.85 by the C restatement, and the
+    workload's shear rate."""
+    import oracle
+    from xdem_b200 import abi, inputs
+    from xdem_b200.world import make_control, make_params
+    q, contacts, box, dt = oracle.ellipse_sample(n_sample, seed, threads=threads, steps=2500,
+                                                 relax=800)
+    rate = 1e-3 * math.sqrt(inputs.KN / float(np.min(q["mass"])))
+    prm = make_params(abi.WORLD_LEES_EDWARDS, dt, box, inputs.KN, inputs.KT, inputs.RESTITUTION,
+                      inputs.FRICTION, shift_strain_rate=rate)
+    return {"particles": q, "contacts": contacts, "params": prm, "control": make_control(),
+            "cpu_kind": "reference",
+            "cpu_note": f"{n_sample}-ellipse sample of the workload made on the CPU (RSA, C "
+                        f"restatement compression to 0.85, same shapes and shear rate)"}
+
+
+def cpu_sample_c0(seed, threads, n=1024):
+    """The disc configuration on the CPU only: n bidisperse discs (r 0.5/0.7,
+    50:50), RSA at 0.50, the C restatement's strain control to 0.70 and a
+    relaxation, velocities N(0, 0.01^2), PeriodicBoundaryWorld."""
+    import oracle
+    from xdem_b200 import abi, inputs
+    from xdem_b200.world import make_control, make_params
+    rng = np.random.default_rng(seed)
+    r = np.where(rng.permutation(n) < n // 2, 0.5, 0.7).astype(np.float64)
+    box = inputs.box_for(float(np.sum(np.pi * r * r)), 0.50)
+    x, y = oracle.rsa_discs(r, box, seed + 1)
+    shape = np.zeros(n, np.int32)
+    zero = np.zeros(n)
+    p = {"shape": shape, "up_level": np.arange(n, dtype=np.int32), "setting": np.zeros(n, np.int32),
+         "is_rattler": np.zeros(n, np.int32), "outer_radius": r, "radius": r.copy(),
+         "aspect_ratio": np.ones(n), "x": x, "y": y, "vx": zero.copy(), "vy": zero.copy(),
+         "rot": zero.copy(), "rot_vel": zero.copy()}
+    p.update(oracle.particle_properties(shape, r, np.ones(n)))
+    dt = 0.02 * math.sqrt(float(np.min(p["mass"])) / inputs.KN)
+    q, _, box = oracle.strain_compress(oracle.PortWorld, p, box, dt, 0.70, 2000, 500,
+                                       threads=threads)
+    q["vx"] = rng.normal(0.0, 0.01, n)
+    q["vy"] = rng.normal(0.0, 0.01, n)
+    q["rot_vel"] = np.zeros(n)
+    prm = make_params(abi.WORLD_PERIODIC, dt, box, inputs.KN, inputs.KT, inputs.RESTITUTION,
+                      inputs.FRICTION)
+    return {"particles": q, "contacts": None, "params": prm, "control": make_control(),
+            "cpu_kind": "reference", "cpu_note": f"{n} discs at 0.70 made on the CPU"}
+
+
+def reference_vs_restatement(threads, seed):
+    """Speed of the compiled reference and of the C restatement on the same
+    CPU-made inputs, both with `threads` threads: the disc configuration
+    (1,024 discs) and a 4,096-ellipse sample of the shear workload.  The
+    restatement is what the full-size CPU leg times; this relates it to the
+    reference's own code where both return."""
+    out = {}
+    for name, make in (("discs_1024", lambda: cpu_sample_c0(seed, threads)),
+                       ("ellipses_4096", lambda: cpu_sample_le_ellipses(4096, seed, threads))):
+        work = make()
+        ref = run_cpu(work, 400, 1, threads, budget_s=8.0, timeout_s=120, kind="reference")
+        port = run_cpu(work, 400, 1, threads, budget_s=8.0, timeout_s=120, kind="port")
+        entry = {"reference": ref.get("value"), "restatement": port.get("value")}
+        if ref.get("kind") != "reference" or "error" in ref:
+            entry["reference_note"] = ref.get("error", "compiled reference not available")
+        if entry["reference"] and entry["restatement"]:
+            entry["restatement_over_reference"] = entry["restatement"] / entry["reference"]
+        out[name] = entry
+    return out
 
 
 WORKLOADS = {"le_ellipses": workload_le_ellipses, "periodic_discs": workload_periodic_discs,
@@ -345,10 +428,12 @@ def _system_params(work, sy):
     return prm
 
 
-def run_cpu(work, steps, warmup, threads, budget_s=25.0, timeout_s=300, max_particles=150000):
-    """Times the CPU implementation named by work["cpu_kind"] in a child
-    process with a watchdog (a batch: its first systems, up to max_particles).
-    Returns the child's result dict or {"error": ...}."""
+def run_cpu(work, steps, warmup, threads, budget_s=25.0, timeout_s=300, max_particles=150000,
+            kind=None):
+    """Times the CPU implementation named by `kind` (default work["cpu_kind"])
+    in a child process with a watchdog (a batch: its first systems, up to
+    max_particles).  Returns the child's result dict or {"error": ...}."""
+    kind = kind or work["cpu_kind"]
     import tempfile
     if "systems" in work:
         items, total = [], 0
@@ -372,7 +457,7 @@ def run_cpu(work, steps, warmup, threads, budget_s=25.0, timeout_s=300, max_part
     path = ",".join(paths)
     cmd = [sys.executable, os.path.abspath(__file__), "--cpu-child", path, "--steps", str(steps),
            "--warmup", str(warmup), "--threads", str(threads), "--budget", str(budget_s),
-           "--cpu-kind", work["cpu_kind"]]
+           "--cpu-kind", kind]
     env = dict(os.environ, OMP_NUM_THREADS=str(threads))
     try:
         r = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout_s, env=env)
@@ -483,31 +568,43 @@ def measure(work, precision, args, dist, full=True, net=None):
 
     w.run(max(args.warmup, 3), ctl)
 
-    # ---- value: device time of K steps ----------------------------------
-    barrier()
-    w.synchronize()
+    # ---- value: device time of K steps, repeated ---------------------------
+    # Each repeat times exactly K steps (CUDA events on the library's stream,
+    # a barrier and a synchronisation on both sides); the repeats continue
+    # until they cover a second of device time (at least five), so that the
+    # clock sampler (every 100 ms) sees the timed region; the value is the
+    # median repeat.
     clocks = ClockSampler(0)
     w.reset_newton_stats()
     clocks.start()
-    l0 = w.launch_count()
-    lib.xdem_range_push(b"bench_value")
-    lib.xdem_timer_start(w.h)
-    done = w.run(args.steps, ctl)
-    ms = C.c_double(0.0)
-    lib.xdem_timer_stop(w.h, C.byref(ms))
-    lib.xdem_range_pop()
-    launches = w.launch_count() - l0
+    reps, launches, done_total = [], 0, 0
+    while len(reps) < 5 or (sum(reps) < 1000.0 and len(reps) < 400):
+        barrier()
+        w.synchronize()
+        l0 = w.launch_count()
+        lib.xdem_range_push(b"bench_value")
+        lib.xdem_timer_start(w.h)
+        done = w.run(args.steps, ctl)
+        ms = C.c_double(0.0)
+        lib.xdem_timer_stop(w.h, C.byref(ms))
+        lib.xdem_range_pop()
+        launches = w.launch_count() - l0
+        done_total += done
+        reps.append(max_over_ranks(ms.value))
     clk = clocks.stop()
-    ms_total = max_over_ranks(ms.value)
+    ms_total = statistics.median(reps)
     contacts = w.count_contacts()
     solves, iters, capped = w.newton_stats()
     out = {"value": n * done * WORLD / (ms_total / 1e3), "ms_per_step": ms_total / max(done, 1),
            "done": done, "contacts": contacts, "launches": int(launches), "clocks": clk,
-           "newton": {"solves_per_step": solves / max(done, 1),
-                      "iterations_per_solve": iters / max(solves, 1), "capped_solves": capped}}
+           "repeats": {"count": len(reps), "ms_min": min(reps), "ms_median": ms_total,
+                       "ms_max": max(reps)},
+           "newton": {"solves_per_step": solves / max(done_total, 1),
+                      "iterations_per_solve": iters / max(solves, 1),
+                      "nonterminating_solves_per_step": capped / max(done_total, 1)}}
     lists = w.candidate_list_stats()
     if lists["capacity"] > 0:
-        out["candidate_lists"] = {"builds_per_step": lists["builds"] / max(done, 1),
+        out["candidate_lists"] = {"builds_per_step": lists["builds"] / max(done_total, 1),
                                   "entries_per_particle": lists["entries"] / n,
                                   "longest": lists["longest"], "capacity": lists["capacity"]}
     if net is not None:
@@ -576,6 +673,60 @@ def measure(work, precision, args, dist, full=True, net=None):
     return out
 
 
+def accuracy(work, steps=2000, sample_every=100):
+    """Mixed precision against FP64 on the workload's packing: (1) one step
+    from the same state and history, the largest per-contact force difference
+    over the largest FP64 contact force; (2) the mean shear stress (xy) over
+    `steps` steps of each path, sampled every `sample_every` steps, and its
+    relative difference.  The FP64 path is the one the parity tests pin to the
+    reference (1e-10 per contact); the stated bars are 1e-5 and 0.5 %."""
+    from xdem_b200 import abi
+    from xdem_b200.world import World, make_control
+
+    def world(prec):
+        prm = abi.Params()
+        C.memmove(C.byref(prm), C.byref(work["params"]), C.sizeof(abi.Params))
+        prm.precision = prec
+        w = World(prm)
+        w.raise_mask = ~abi.ERR_NEWTON
+        w.set_particles(work["particles"])
+        if work["contacts"] is not None and len(work["contacts"]["id_i"]):
+            w.set_contacts(work["contacts"])
+        return w
+
+    t0 = time.time()
+    w64, wmx = world(abi.PRECISION_FP64), world(abi.PRECISION_MIXED)
+    w64.run(1, work["control"])
+    wmx.run(1, work["control"])
+    c64, cmx = w64.get_contacts(), wmx.get_contacts()
+    k64 = c64["id_i"].astype(np.int64) << 32 | c64["id_j"].astype(np.int64)
+    kmx = cmx["id_i"].astype(np.int64) << 32 | cmx["id_j"].astype(np.int64)
+    common, i64, imx = np.intersect1d(k64, kmx, assume_unique=True, return_indices=True)
+    f64 = np.stack([c64["fn_x"] + c64["ft_x"], c64["fn_y"] + c64["ft_y"]], 1)
+    fmx = np.stack([cmx["fn_x"] + cmx["ft_x"], cmx["fn_y"] + cmx["ft_y"]], 1)
+    scale = float(np.max(np.hypot(f64[:, 0], f64[:, 1])))
+    err = np.hypot(*(fmx[imx] - f64[i64]).T) / scale
+    one_step = {"max_force_error": float(err.max()), "p99_99_force_error": float(np.quantile(err, 0.9999)),
+                "contacts_over_1e-5": int(np.sum(err > 1e-5)), "contacts": int(len(k64)),
+                "contacts_only_fp64": int(len(k64) - len(common)),
+                "contacts_only_mixed": int(len(kmx) - len(common)), "bar": 1e-5}
+    ctl = make_control(update_stress=True)
+    s64, smx = [], []
+    for _ in range(steps // sample_every):
+        w64.run(sample_every, ctl)
+        wmx.run(sample_every, ctl)
+        s64.append(w64.getStress()[1])
+        smx.append(wmx.getStress()[1])
+    m64, mmx = float(np.mean(s64)), float(np.mean(smx))
+    shear = {"steps": steps, "samples": len(s64), "mean_shear_stress_fp64": m64,
+             "mean_shear_stress_mixed": mmx, "relative_difference": abs(mmx - m64) / abs(m64),
+             "bar": 5e-3}
+    w64.close()
+    wmx.close()
+    log(f"accuracy: {one_step}, {shear}, {time.time() - t0:.1f}s")
+    return {"one_step_forces": one_step, "mean_shear_stress": shear}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -611,14 +762,30 @@ def main():
         dist = dist_mod
 
     if args.impl == "reference":
+        # The reference's CPU implementation of the path, on the host cores,
+        # on a bounded sample of the workload built without the product
+        # library: the compiled reference where it returns within the
+        # watchdog, else the C restatement.
         if RANK != 0:
             if dist:
                 dist.destroy_process_group()
             return
-        size = args.n if args.workload != "batch_ensemble" else args.systems
-        work = WORKLOADS[args.workload](size, args.seed)
         threads = os.cpu_count() or 1
-        res = run_cpu(work, args.steps, 1, threads, budget_s=60.0)
+        if args.workload == "le_ellipses":
+            work = cpu_sample_le_ellipses(4096, args.seed, threads)
+            config = config_le_ellipses(args.n)
+        elif args.workload == "periodic_discs":
+            work = cpu_sample_c0(args.seed, threads, n=args.n)
+            config = config_periodic_discs(args.n)
+        else:
+            work = WORKLOADS[args.workload](args.systems, args.seed)
+            config = work["config"]
+        config = dict(config, parallelism="single")
+        res = run_cpu(work, args.steps, 1, threads, budget_s=40.0, timeout_s=150, kind="reference")
+        if "error" in res:
+            note = res["error"]
+            res = run_cpu(work, args.steps, 1, threads, budget_s=40.0, timeout_s=150, kind="port")
+            work["cpu_note"] += f"; the compiled reference gave no result ({note})"
         if "error" in res:
             print(json.dumps({"impl": "reference", "unavailable": res["error"]}), flush=True)
         else:
@@ -627,9 +794,9 @@ def main():
                       f"after 1 warm-up step, {threads} threads; {work['cpu_note']}")
             line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT,
                     "n_gpus": args.gpus, "steps": k, "warmup": 1,
-                    "ms_per_step": 1e3 * work["config"]["n_particles"] / v,
+                    "ms_per_step": 1e3 * config["n_particles"] / v,
                     "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-                    "data": "synthetic", "config": work["config"],
+                    "data": "synthetic", "config": config,
                     "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": res["kind"],
                                      "sample": sample},
                     "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0,
@@ -676,24 +843,36 @@ def main():
                              f"{res['systems']} system(s) after 1 warm-up step "
                              f"({res['one_step_s']:.2f} s per step); {work['cpu_note']}"}
 
+    acc = None
+    if args.workload == "le_ellipses" and not args.no_compare and args.precision == "mixed":
+        acc = accuracy(work)
+    cpu_cmp = None
+    if RANK == 0 and WORLD == 1 and not args.no_cpu_baseline:
+        cpu_cmp = reference_vs_restatement(os.cpu_count() or 1, args.seed)
+        if cpu is not None:
+            cpu["reference_vs_restatement"] = cpu_cmp
+
     cfg = dict(work["config"])
-    cfg["precision"] = args.precision
-    cfg["l2"] = "inputs larger than L2 (state + contact history resident in HBM)"
+    cfg.setdefault("l2", "inputs larger than L2 (state + contact history resident in HBM)")
     cfg["parallelism"] = f"replicas{WORLD}" if WORLD > 1 else "single"
-    cfg["contacts"] = head["contacts"]
+    numbers = dict(work.get("numbers", {}))
+    numbers["contacts"] = head["contacts"]
     line = {
         "metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": WORLD,
         "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": head["ms_per_step"],
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32+f64" if args.precision == "mixed" else "f64",
-        "data": "synthetic", "config": cfg,
+        "data": "synthetic", "config": cfg, "precision": args.precision,
+        "workload_numbers": numbers,
         "contacts_per_s": head["contacts"] * head["done"] * WORLD / (head["ms_per_step"] * head["done"] / 1e3),
         "e2e": head["e2e"], "gpu_launches": head["launches"], "roofline": head["roofline"],
         "kernel_share": head["kernel_share"], "kernel_ms_per_step": head["kernel_ms_per_step"],
         "profiled_ms_per_step": head["profiled_ms_per_step"],
-        "clocks": head["clocks"], "status": head["status"], "newton": head["newton"],
-        "cpu_baseline": cpu,
+        "clocks": head["clocks"], "repeats": head["repeats"], "status": head["status"],
+        "newton": head["newton"], "cpu_baseline": cpu,
     }
+    if acc is not None:
+        line["accuracy_mixed_vs_fp64"] = acc
     if "candidate_lists" in head:
         line["candidate_lists"] = head["candidate_lists"]
     if loop is not None:

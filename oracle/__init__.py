@@ -249,3 +249,133 @@ def newton_quartic(A, B, Cc, D, E, init):
 
 def bisect_quartic(A, B, Cc, D, E, s, q):
     return port_lib()["bisect_quartic"](A, B, Cc, D, E, s, q)
+
+
+# ---- CPU-only inputs (no product library): the reference arm of bench.py ----
+
+def particle_properties(shape, radius, aspect, density=1.0):
+    """calculateParticleProperties of circles and ellipses: the compiled
+    reference's own when it is built here, else its formulas
+    (CircularParticle.cpp:16-23, EllipticParticle.cpp:7-14) in numpy."""
+    if ref_available():
+        return ref_particle_properties(shape, radius, aspect, density)
+    r = np.asarray(radius, np.float64)
+    k = np.asarray(aspect, np.float64)
+    ell = np.asarray(shape) == abi.SHAPE_ELLIPSE
+    vol = np.where(ell, np.pi * r * r / k, np.pi * r * r)
+    mass = vol * density
+    inertia = np.where(ell, mass * (r * r + r * r / k / k) / 4.0, mass * r * r / 2.0)
+    return {"volume": vol, "mass": mass, "inv_mass": 1.0 / mass, "inertia": inertia,
+            "inv_inertia": 1.0 / inertia}
+
+
+def rsa_discs(radius, box, seed, max_attempts=100000):
+    """Random sequential addition of discs (largest first) into the periodic
+    box without overlap, with a cell grid; numpy only, seeded."""
+    rng = np.random.default_rng(seed)
+    r = np.asarray(radius, np.float64)
+    n = len(r)
+    L = box[1] - box[0]
+    H = box[3] - box[2]
+    cell = 2.0 * float(r.max())
+    nx, ny = max(1, int(L // cell)), max(1, int(H // cell))
+    grid = {}
+    x = np.zeros(n)
+    y = np.zeros(n)
+    for i in np.argsort(-r, kind="stable"):
+        for _ in range(max_attempts):
+            px, py = rng.uniform(box[0], box[1]), rng.uniform(box[2], box[3])
+            cx, cy = int((px - box[0]) / L * nx) % nx, int((py - box[2]) / H * ny) % ny
+            ok = True
+            for dx in (-1, 0, 1):
+                for dy in (-1, 0, 1):
+                    for j in grid.get(((cx + dx) % nx, (cy + dy) % ny), ()):
+                        ddx = px - x[j]
+                        ddy = py - y[j]
+                        ddx -= L * round(ddx / L)
+                        ddy -= H * round(ddy / H)
+                        if ddx * ddx + ddy * ddy < (r[i] + r[j]) ** 2:
+                            ok = False
+                            break
+                    if not ok:
+                        break
+                if not ok:
+                    break
+            if ok:
+                x[i], y[i] = px, py
+                grid.setdefault((cx, cy), []).append(i)
+                break
+        else:
+            raise RuntimeError("RSA did not place every disc")
+    return x, y
+
+
+def strain_compress(world_cls, p, box, dt, phi_target, steps, relax, damping=0.1,
+                    method=abi.ELLIPSE_CLOSEST_APPROACH, threads=1):
+    """Strain-controlled compression (updatePeriodicBoundary_strainControl,
+    PeriodicControlWorld.cpp:124-135) of the particle dict p to phi_target in
+    about `steps` steps, then `relax` steps at the final box, by a CPU world;
+    returns (particles with the new state, contacts, box)."""
+    import math
+    from xdem_b200 import inputs
+    from xdem_b200.world import make_control, make_params
+    prm = make_params(abi.WORLD_PERIODIC_CONTROL, dt, box, inputs.KN, inputs.KT,
+                      inputs.RESTITUTION, inputs.FRICTION, global_damping=damping,
+                      ellipse_method=method)
+    w = world_cls(prm, threads)
+    w.raise_mask = ~abi.ERR_NEWTON
+    w.set_particles(p)
+    vol = float(p["volume"].sum())
+    phi0 = vol / ((box[1] - box[0]) * (box[3] - box[2]))
+    s_step = math.sqrt(phi0 / phi_target) ** (1.0 / steps)
+    ctl = make_control(box_law=abi.BOX_STRAIN, reset_rattlers=False)
+    done = 0
+    while done < 3 * steps:
+        b = w.getBoundary()
+        L = b[1] - b[0]
+        s_rem = math.sqrt(vol / (L * (b[3] - b[2])) / phi_target)
+        if s_rem >= 1.0 - 1e-12:
+            break
+        left = max(1, int(math.ceil(math.log(s_rem) / math.log(s_step))))
+        chunk = min(200, left)
+        per = s_rem ** (1.0 / chunk) if chunk == left else s_step
+        ctl.p0 = ctl.p1 = (per - 1.0) / (L * dt)
+        w.run(chunk, ctl)
+        done += chunk
+    if relax:
+        w.run(relax, make_control())
+    st = w.get_state()
+    q = dict(p)
+    for k in ("x", "y", "vx", "vy", "rot", "rot_vel"):
+        q[k] = st[k].copy()
+    contacts = w.get_contacts()
+    b = np.array(w.getBoundary())
+    w.close()
+    return q, contacts, b
+
+
+def ellipse_sample(n, seed, aspect_hi=3.0, phi=0.85, threads=1, steps=3000, relax=1000):
+    """A CPU-made sample of the ellipse shear workloads: n ellipses with
+    b in {0.5, 0.7} (50:50) and a/b ~ U[1, aspect_hi], orientations U[0, pi),
+    RSA of their bounding discs at fraction 0.40, then the C restatement's
+    strain-controlled compression to solid fraction phi and a relaxation.
+    Returns (particles, contacts, box, dt)."""
+    from xdem_b200 import inputs
+    rng = np.random.default_rng(seed)
+    b = np.where(rng.permutation(n) < n // 2, 0.5, 0.7).astype(np.float64)
+    k = rng.uniform(1.0, aspect_hi, n)
+    a = k * b
+    box = inputs.box_for(float(np.sum(np.pi * a * a)), 0.40)
+    x, y = rsa_discs(a, box, seed + 1)
+    rot = rng.uniform(0.0, np.pi, n)
+    shape = np.ones(n, np.int32)
+    props = particle_properties(shape, a, k)
+    zero = np.zeros(n)
+    p = {"shape": shape, "up_level": np.arange(n, dtype=np.int32), "setting": np.zeros(n, np.int32),
+         "is_rattler": np.zeros(n, np.int32), "outer_radius": a, "radius": a.copy(),
+         "aspect_ratio": k, "x": x, "y": y, "vx": zero.copy(), "vy": zero.copy(), "rot": rot,
+         "rot_vel": zero.copy()}
+    p.update(props)
+    dt = 0.02 * float(np.sqrt(np.min(p["mass"]) / inputs.KN))
+    q, contacts, box = strain_compress(PortWorld, p, box, dt, phi, steps, relax, threads=threads)
+    return q, contacts, box, dt

@@ -137,8 +137,16 @@ def _converged(p, cc, prm):
     off = np.zeros((len(i), 4))
     off[:, 0] = p["x"][i] - p["x"][j] - cc["branch_x"]
     off[:, 1] = p["y"][i] - p["y"][j] - cc["branch_y"]
-    out, _ = oracle.pair_geometry(rows(i), rows(j), off, abi.ELLIPSE_CLOSEST_APPROACH, "port")
-    return out[:, 16] < 1000
+    pi, pj = rows(i), rows(j)
+    out, _ = oracle.pair_geometry(pi, pj, off, abi.ELLIPSE_CLOSEST_APPROACH, "port")
+    keep = np.ones(len(i), bool)
+    # a solve that stopped on a repeated iterate or the cap raises
+    # XDEM_ERR_NEWTON; only long ones can have
+    for k in np.nonzero(out[:, 16] >= 50)[0]:
+        _, st = oracle.pair_geometry(pi[k:k + 1], pj[k:k + 1], off[k:k + 1],
+                                     abi.ELLIPSE_CLOSEST_APPROACH, "port")
+        keep[k] = not (st & abi.ERR_NEWTON)
+    return keep
 
 
 def _force_err(cm, cc, keep=None):

@@ -91,16 +91,10 @@ struct AxisShape {
   float c, s, a, b;
 };
 
-// the screen's record of the ellipse at m; the orientation is reduced to
-// [-pi, pi] in FP64 before the FP32 sine and cosine
+// the screen's record of the ellipse at m (k_bodies wrote it this step)
 __device__ __forceinline__ AxisShape axis_shape(const DevWorld& w, int m) {
-  double r = w.rot[m];
-  r -= 6.283185307179586 * rint(r * 0.15915494309189535);
-  AxisShape e;
-  __sincosf((float)r, &e.s, &e.c);
-  e.a = (float)w.rad[m];
-  e.b = __fdividef(e.a, (float)w.asp[m]);
-  return e;
+  const float4 r = w.axis[m];
+  return AxisShape{r.x, r.y, r.z, r.w};
 }
 
 // Class of a pair of ellipses on the line of their centres, from the centre
@@ -155,14 +149,11 @@ __device__ __forceinline__ bool centre_line_classes(const DevWorld& w) {
   return LAW == LAW_CLOSEST || centre_line_screen<LAW>(w);
 }
 
-// the owner's record for the screen, from the (cos, sin) of its body record
+// the owner's record for the screen
 template <int LAW>
-__device__ __forceinline__ AxisShape owner_axis_shape(const DevWorld& w, int m, double2 cs) {
+__device__ __forceinline__ AxisShape owner_axis_shape(const DevWorld& w, int m) {
   AxisShape e{0.0f, 0.0f, 0.0f, 0.0f};
-  if (centre_line_classes<LAW>(w)) {
-    const float a = (float)w.rad[m];
-    e = AxisShape{(float)cs.x, (float)cs.y, a, __fdividef(a, (float)w.asp[m])};
-  }
+  if (centre_line_classes<LAW>(w)) e = axis_shape(w, m);
   return e;
 }
 
@@ -387,8 +378,6 @@ __device__ __forceinline__ void write_pairs(const DevWorld& w, int m, int nlist,
 // cells (and passes the same filters) are marked seen: such a pair was a
 // candidate, so its history is replaced or dropped; the others are carried
 // over here.
-// For an all-ellipse world the thread also leaves (cos, sin) of its
-// orientation for the pair kernel, computed once per body instead of per pair.
 template <int LAW>
 __global__ void __launch_bounds__(128) k_candidates(DevWorld w, int par) {
   if (stopped(w)) return;
@@ -403,16 +392,7 @@ __global__ void __launch_bounds__(128) k_candidates(DevWorld w, int par) {
   int32_t list_mj[kMaxSlots];
   int32_t list_code[kMaxSlots];
   if (valid) {
-    // this step's record of the body for the pair kernels; an ellipse's
-    // (cos, sin) is computed once per body instead of once per pair
-    double2 cs = make_double2(0.0, 0.0);
-    if (LAW == LAW_CLOSEST || LAW == LAW_INTERSECTION ||
-        (LAW == LAW_ANY && w.shape[m] == SHAPE_ELLIPSE)) {
-      const double r = w.rot[m];
-      cs = make_double2(cos(r), sin(r));
-    }
-    write_body(w, m, cs);
-    const AxisShape shape_ax = owner_axis_shape<LAW>(w, m, cs);
+    const AxisShape shape_ax = owner_axis_shape<LAW>(w, m);
     Grid G = grid_of(ws);
     const int id_i = w.id_of[m];
     const int nold = min(old.count[m], K);

@@ -24,12 +24,33 @@ namespace xdem {
 constexpr int kVlBlock = 256;
 constexpr int kVlGroup = 2;  // list entries whose loads k_candidates_vl issues together
 
-// block maxima of the path lengths since the last build
-__global__ void __launch_bounds__(kVlBlock) k_vl_maxdisp(DevWorld w) {
+// The bodies' records for this step's contact update, written after the
+// step's last position move and memory-order refresh, so that the candidate
+// and pair kernels only read them: the pair kernels' 96-byte record with
+// (cos, sin) of an ellipse's orientation in FP64, and the FP32 axis record of
+// the centre-line class.  With candidate lists, also the block maxima of the
+// path lengths since the last list build.
+template <int LAW>
+__global__ void __launch_bounds__(kVlBlock) k_bodies(DevWorld w) {
   if (stopped(w)) return;
   __shared__ double sh[kVlBlock / 32];
   const int m = blockIdx.x * blockDim.x + threadIdx.x;
-  double v = m < w.n ? w.vl_disp[m] : 0.0;
+  double v = 0.0;
+  if (m < w.n) {
+    double2 cs = make_double2(0.0, 0.0);
+    if (LAW == LAW_CLOSEST || LAW == LAW_INTERSECTION ||
+        (LAW == LAW_ANY && w.shape[m] == SHAPE_ELLIPSE)) {
+      const double r = w.rot[m];
+      cs = make_double2(cos(r), sin(r));
+    }
+    write_body(w, m, cs);
+    if (centre_line_classes<LAW>(w)) {
+      const double a = w.rad[m];
+      w.axis[m] = make_float4((float)cs.x, (float)cs.y, (float)a, (float)(a / w.asp[m]));
+    }
+    if (w.V) v = w.vl_disp[m];
+  }
+  if (!w.V) return;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
   if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
@@ -120,7 +141,7 @@ __global__ void __launch_bounds__(128) k_vl_build(DevWorld w) {
 }
 
 // k_candidates with the lists: same outputs (slot counts, carried-over
-// history, the compact pair list, orientation cosines), the same filters and
+// history, the compact pair list), the same filters and
 // tests.  Seven blocks per SM (72 registers): the kernel is latency-bound on
 // its partner gathers, and six blocks with more registers measured slower.
 template <int LAW>
@@ -137,16 +158,7 @@ __global__ void __launch_bounds__(128, 7) k_candidates_vl(DevWorld w, int par) {
   int32_t list_mj[kMaxSlots];
   int32_t list_code[kMaxSlots];
   if (valid) {
-    // this step's record of the body for the pair kernels; an ellipse's
-    // (cos, sin) is computed once per body instead of once per pair
-    double2 cs = make_double2(0.0, 0.0);
-    if (LAW == LAW_CLOSEST || LAW == LAW_INTERSECTION ||
-        (LAW == LAW_ANY && w.shape[m] == SHAPE_ELLIPSE)) {
-      const double r = w.rot[m];
-      cs = make_double2(cos(r), sin(r));
-    }
-    write_body(w, m, cs);
-    const AxisShape shape_ax = owner_axis_shape<LAW>(w, m, cs);
+    const AxisShape shape_ax = owner_axis_shape<LAW>(w, m);
     const Grid G = grid_of(ws);
     const int id_i = w.id_of[m];
     const int nold = min(old.count[m], K);
