@@ -522,9 +522,10 @@ def measure_loop(work, precision, args):
     return {"value": n * args.steps / (ms.value / 1e3), "ms_per_step": ms.value / args.steps}
 
 
-def measure(work, precision, args, dist, full=True, net=None):
+def measure(work, precision, args, dist, full=True, net=None, kernels=False):
     """Times `args.steps` steps of the workload at the given precision.
     full: also the per-kernel roofline pass and the end-to-end pass;
+    kernels: (without full) the per-kernel pass alone;
     net: the learned warm start to attach."""
     from xdem_b200 import abi
     from xdem_b200.learned import warm_stats
@@ -615,6 +616,13 @@ def measure(work, precision, args, dist, full=True, net=None):
                              "fallback_fraction": (ws["rejected"] + ws["restarted"]) / off,
                              "contact_logit_accuracy": ws["logit_right"] / off}
     if not full:
+        if kernels:
+            w.set_profiling(True)
+            w.run(args.steps, ctl)
+            prof = w.profile()
+            w.set_profiling(False)
+            out["kernel_ms_per_step"] = {k: round(v[1] / args.steps, 5) for k, v in prof.items()}
+            out["pairs_per_step"] = w.pair_count()
         out["status"] = w.synchronize()
         w.close()
         return out
@@ -814,7 +822,8 @@ def main():
     work = WORKLOADS[args.workload](size, args.seed + RANK)
     n = work["config"]["n_particles"]
     head = measure(work, prec[args.precision], args, dist, full=True)
-    cmp_ = None if args.no_compare else measure(work, prec[other], args, dist, full=False)
+    cmp_ = None if args.no_compare else measure(work, prec[other], args, dist, full=False,
+                                                kernels=True)
     loop = None
     if "systems" in work:
         loop = measure_loop(work, prec[args.precision], args)
@@ -823,9 +832,11 @@ def main():
         net, tinfo = train_warm_start(args.seed)
         learned = {"training": tinfo}
         for name, pr in (("fp64_warm", abi.PRECISION_FP64), ("mixed_warm", abi.PRECISION_MIXED)):
-            r = measure(work, pr, args, dist, full=False, net=net)
+            r = measure(work, pr, args, dist, full=False, net=net, kernels=True)
             learned[name] = {"value": r["value"], "ms_per_step": r["ms_per_step"],
                              "newton": r["newton"], "warm_start": r["warm_start"],
+                             "kernel_ms_per_step": r["kernel_ms_per_step"],
+                             "pairs_per_step": r["pairs_per_step"],
                              "status": r["status"], "clocks": r["clocks"]}
         net.close()
 
@@ -885,6 +896,7 @@ def main():
     if cmp_ is not None:
         line[other] = {"value": cmp_["value"], "ms_per_step": cmp_["ms_per_step"],
                        "contacts": cmp_["contacts"], "newton": cmp_["newton"],
+                       "kernel_ms_per_step": cmp_["kernel_ms_per_step"],
                        "clocks": cmp_["clocks"], "status": cmp_["status"]}
         line[f"speedup_vs_{other}"] = head["value"] / cmp_["value"]
     if RANK == 0:

@@ -24,10 +24,16 @@ configurations' shapes and sizes:
       and box at the stop, the stress sampled along the way, and the final
       Z and phi.
 
-Each fixture also holds the C restatement's (oracle/liboracle.so) result of
-the same run, and the spread of the reference's own observables over runs
-whose initial velocities differ by one ulp, which sizes the tolerances of the
-tests (stated in tests/test_long_runs.py).  Run from the repository root:
+The disc fixture also holds the C restatement's (oracle/liboracle.so) run
+and three reference runs whose initial velocities differ by one ulp.  The
+compiled reference stops returning during the closest-approach compression
+(a Newton iteration without end between steps 10,000 and 20,000), so that
+fixture pins the restatement to the reference on the first 10,000 steps and
+records the restatement's full run and two runs with one orientation moved by
+one ulp, which size the tolerances of tests/test_long_runs.py.  The
+intersection-law compression stops at its first step in the reference
+(spurious contacts on the overlap-free packing); its fixture holds that step.
+Run from the repository root:
 
     python tests/golden/make_long_runs.py [c0] [c1]
 """

@@ -250,3 +250,52 @@ def test_deep_pairs_beside_the_other_pairs_are_bit_identical():
     assert len(c0["id_i"]) > 4000
     np.testing.assert_array_equal(worlds[0].getStress(), worlds[1].getStress())
     assert worlds[0].newton_stats() == worlds[1].newton_stats()
+
+
+def test_mixed_accuracy_at_the_shear_configuration_size():
+    """The mixed-precision configuration at its size: 262,144 ellipses with
+    a/b ~ U[1,2] and b in {0.5, 0.7}, compressed to solid fraction 0.85 and
+    sheared in a LeesEdwardsBoundaryWorld at 1e-3 sqrt(kn/m_min).  Against the
+    FP64 path on the same packing and history (the FP64 path reproduces the
+    checker to 1e-10 per contact at smaller sizes, tests above), with fixed
+    bars: (1) after one step, every contact both paths hold has a force within
+    1e-5 of the largest FP64 contact force, the contact sets agree but for at
+    most 1e-5 of the contacts (pairs within rounding of tangency); (2) the
+    mean shear stress over 2,000 steps (sampled every 100) agrees within
+    0.5 %."""
+    import math
+    from xdem_b200 import inputs, packing
+    from xdem_b200.world import make_params
+    n = 262144
+    p, box = inputs.ellipse_system(n, b=inputs.c2_b, aspect=inputs.c2_aspect, phi_rsa_circle=0.40,
+                                   phi=None, seed=62, vel_sigma=0.01)
+    dt = inputs.time_step(p)
+    q, contacts, b, _ = packing.compress(p, box, 0.85, dt, steps=3000, relax=1000)
+    rate = 1e-3 * math.sqrt(inputs.KN / float(np.min(p["mass"])))
+    prm = make_params(abi.WORLD_LEES_EDWARDS, dt, b, inputs.KN, inputs.KT, inputs.RESTITUTION,
+                      inputs.FRICTION, shift_strain_rate=rate)
+    worlds = [World(prm), World(_mixed(prm))]
+    for w in worlds:
+        w.raise_mask = ~abi.ERR_NEWTON
+        w.set_particles(q)
+        w.set_contacts(contacts)
+        w.takeTimeStep()
+    c64, cmx = worlds[0].get_contacts(), worlds[1].get_contacts()
+    k64 = c64["id_i"].astype(np.int64) << 32 | c64["id_j"].astype(np.int64)
+    kmx = cmx["id_i"].astype(np.int64) << 32 | cmx["id_j"].astype(np.int64)
+    common, i64, imx = np.intersect1d(k64, kmx, assume_unique=True, return_indices=True)
+    assert len(k64) > n
+    assert len(k64) + len(kmx) - 2 * len(common) <= 1e-5 * len(k64)
+    f64 = np.stack([c64["fn_x"] + c64["ft_x"], c64["fn_y"] + c64["ft_y"]], 1)
+    fmx = np.stack([cmx["fn_x"] + cmx["ft_x"], cmx["fn_y"] + cmx["ft_y"]], 1)
+    scale = np.max(np.hypot(f64[:, 0], f64[:, 1]))
+    err = np.hypot(*(fmx[imx] - f64[i64]).T) / scale
+    assert err.max() <= FORCE_TOL, float(err.max())
+    ctl = make_control(update_stress=True)
+    series = [[], []]
+    for _ in range(20):
+        for w, s in zip(worlds, series):
+            w.run(100, ctl)
+            s.append(w.getStress()[1])
+    m64, mmx = float(np.mean(series[0])), float(np.mean(series[1]))
+    assert abs(mmx - m64) <= 5e-3 * abs(m64), (m64, mmx)

@@ -25,8 +25,12 @@ C restatement to it over the first 10,000 steps (bit for bit) and records the
 restatement's full run and two runs with one orientation moved by one ulp.
 CUDA's cos/sin may differ from glibc's in the last bit, so after ~450,000
 steps through jamming the trajectories have decorrelated and only the
-observables compare; the tolerances (C1_*_TOL below) are fixed, set above
-the spread those one-ulp runs show.
+observables compare.  The stop is a jamming transient of a small system (the
+pressure jumps from below 1 to above 10 within one 20,000-step sample), and
+runs one ulp apart stop at 432,134-474,978 steps, solid fraction
+0.799-0.832 and rattler-free Z 2.36-2.58 (the fixture's three runs); the
+fixed tolerances below are that range widened by its own width, around the
+fixture's central run.
 
 long_c1_intersection.npz — the same compression with Strobach's intersection
 law: the reference finds spurious contacts on the overlap-free RSA packing
@@ -50,10 +54,12 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 GOLD = os.path.join(HERE, "golden")
 STATE_KEYS = ("x", "y", "vx", "vy", "rot", "rot_vel")
 
-# C1 observables at the stop, GPU against the restatement's run
-C1_PHI_TOL = 2e-3
-C1_Z_TOL = 0.25
-C1_STEPS_REL_TOL = 0.01
+# C1 observables at the stop, GPU against the restatement's central run
+# (runs one ulp apart: steps within 5.6 %, solid fraction within 0.02, Z
+# within 0.21 of it)
+C1_PHI_TOL = 0.035
+C1_Z_TOL = 0.45
+C1_STEPS_REL_TOL = 0.10
 
 
 def _load(name):
