@@ -43,7 +43,8 @@ enum xdem_status_bits {
      (EllipticParticle.cpp:621 has no cap and never returns there); the
      quartic's root between the analytic start and 1 was taken by bisection */
   XDEM_ERR_NEWTON = 1 << 1,
-  /* non-finite position/velocity/force detected */
+  /* a time integral produced a non-finite position, velocity or spin (the
+     reference carries NaN on silently) */
   XDEM_ERR_NONFINITE = 1 << 2,
   /* pair of shapes without a contact law, e.g. circle-ellipse
      (CircularParticle.cpp:38, EllipticParticle.cpp:30 exit with -1) */

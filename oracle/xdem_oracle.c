@@ -1233,6 +1233,13 @@ static void take_time_integral(xo_world* w) {
     w->w[i] = (w->w[i] * (1.0 - g * dt) + w->tq[i] * w->iI[i] * dt) / (1.0 + g * dt);
     w->rot[i] += w->w[i] * dt;
   }
+  /* a non-finite state (the reference carries NaN on without a word) */
+  for (int i = 0; i < w->n; ++i)
+    if (!isfinite(w->x[i]) || !isfinite(w->y[i]) || !isfinite(w->vx[i]) || !isfinite(w->vy[i]) ||
+        !isfinite(w->rot[i]) || !isfinite(w->w[i])) {
+      w->status |= XDEM_ERR_NONFINITE;
+      break;
+    }
 }
 
 /* BaseWorld::resetVelocityOfRattlers / scaleVelocityOfRattlers (BaseWorld.cpp:79-106) */

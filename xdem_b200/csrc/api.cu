@@ -292,8 +292,10 @@ void launch_update_phases(xdem_world_s* w, int record) {
   } else if (LAW == LAW_CLOSEST) {
     // as in mixed precision: the deep pairs first, the regular pass beside
     // them as a programmatic dependent launch (an ordinary launch while the
-    // kernels are timed one by one)
-    LAUNCH(w, KK_DEEP, k_pair_deep<FOLD_BG, LAW><<<148 * 2, 128, 0, w->stream>>>(w->dw, w->par, record));
+    // kernels are timed one by one).  Every deep pair is an FP64 solve here,
+    // so the deep pass gets the pair kernel's grid; the regular pass's blocks
+    // take the SMs as the deep pass's blocks retire.
+    LAUNCH(w, KK_DEEP, k_pair_deep<FOLD_BG, LAW><<<pb, 128, 0, w->stream>>>(w->dw, w->par, record));
     if (w->prof_on) {
       LAUNCH(w, KK_PAIRS, k_pair_forces<FOLD_BG, LAW, false, PASS64_REGULAR><<<pb, 128, 0, w->stream>>>(
                               w->dw, w->par, record));

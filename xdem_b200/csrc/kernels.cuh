@@ -654,6 +654,8 @@ __global__ void k_integrate(DevWorld w, int reset_rattlers) {
       w.rot[sk] += angle;
     }
     if (w.V) w.vl_disp[i] += sqrt(vv.x * vv.x + vv.y * vv.y) * dt;
+    if (!(isfinite(p.x) && isfinite(p.y) && isfinite(vv.x) && isfinite(vv.y) && isfinite(om)))
+      raise(w.status, ST_NONFINITE);
     w.pos[i] = p;
     w.rot[i] = rot;
     if (reset_rattlers && !(set & SKIP_MACRO_SUM) && is_rattler(w, i)) {
@@ -672,6 +674,10 @@ __global__ void k_integrate(DevWorld w, int reset_rattlers) {
   p.y += vv.y * dt;
   om = (om * (1.0 - g * dt) + w.torque[i] * w.iI[i] * dt) / (1.0 + g * dt);
   if (w.V) w.vl_disp[i] += sqrt(vv.x * vv.x + vv.y * vv.y) * dt * seg_path_factor(w, i);  // candidate lists
+  // a non-finite state raises XDEM_ERR_NONFINITE (the reference carries NaN
+  // on without a word)
+  if (!(isfinite(p.x) && isfinite(p.y) && isfinite(vv.x) && isfinite(vv.y) && isfinite(om)))
+    raise(w.status, ST_NONFINITE);
   w.pos[i] = p;
   w.rot[i] = w.rot[i] + om * dt;
   if (reset_rattlers && !(set & SKIP_MACRO_SUM) && w.rattler[i]) {
