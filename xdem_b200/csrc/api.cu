@@ -157,14 +157,14 @@ enum KernelKind {
   KK_MODIFY = 0, KK_BIN, KK_SCAN, KK_SCATTER, KK_CANDIDATES, KK_PAIRS, KK_FINISH, KK_COLLECT,
   KK_INTEGRATE, KK_RATTLERS, KK_STRESS_PARTIAL, KK_STRESS_FINAL, KK_END_OF_STEP, KK_SCALE,
   KK_BACKGROUND, KK_KE, KK_RESORT, KK_STAGE, KK_FALLBACK, KK_WARM, KK_VL_CHECK, KK_VL_BUILD,
-  KK_DEEP, KK_BODIES, KK_COUNT
+  KK_DEEP, KK_COUNT
 };
 const char* const kKindNames[KK_COUNT] = {
     "k_modify_position", "k_bin", "k_scan", "k_scatter", "k_candidates", "k_pair_forces",
     "k_pairs_done", "k_collect", "k_integrate", "k_rattlers", "k_stress_partial",
     "k_stress_final", "k_end_of_step", "k_scale_positions", "k_background_velocity",
     "k_kinetic_energy", "k_resort", "k_stage", "k_pair_fallback", "k_mlp_warm", "k_vl_check",
-    "k_vl_build", "k_pair_deep", "k_bodies"};
+    "k_vl_build", "k_pair_deep"};
 
 void prof_begin(xdem_world_s* w, int kind) {
   if (!w->prof_on) return;
@@ -242,10 +242,9 @@ void launch_update_phases(xdem_world_s* w, int record) {
   const int pb = 148 * w->pair_blocks_per_sm;
   // the learned warm start applies to closest-approach worlds
   const bool warm = w->mlp != nullptr && w->dw.warm != nullptr && LAW == LAW_CLOSEST;
-  const int vb = blocks_for(w->dw.n, kVlBlock);
-  // this step's body and axis records (and the lists' path-length maxima)
-  LAUNCH(w, KK_BODIES, k_bodies<LAW><<<vb, kVlBlock, 0, w->stream>>>(w->dw));
   if (w->dw.V > 0) {
+    const int vb = blocks_for(w->dw.n, kVlBlock);
+    LAUNCH(w, KK_VL_CHECK, k_vl_maxdisp<<<vb, kVlBlock, 0, w->stream>>>(w->dw));
     LAUNCH(w, KK_VL_CHECK, k_vl_check<<<1, 1024, 0, w->stream>>>(w->dw, vb));
     LAUNCH(w, KK_VL_BUILD, k_vl_build<LAW><<<nb, 128, 0, w->stream>>>(w->dw));
     LAUNCH(w, KK_CANDIDATES, k_candidates_vl<LAW><<<nb, 128, 0, w->stream>>>(w->dw, w->par));
@@ -289,19 +288,6 @@ void launch_update_phases(xdem_world_s* w, int record) {
            k_mlp_warm<LAW><<<148 * 4, 128, 0, w->stream>>>(w->dw, w->mlp->dev(), w->dw.npairs, nullptr));
     LAUNCH(w, KK_PAIRS,
            k_pair_forces<FOLD_BG, LAW, true><<<pb, 128, 0, w->stream>>>(w->dw, w->par, record));
-  } else if (LAW == LAW_CLOSEST) {
-    // as in mixed precision: the deep pairs first, the regular pass beside
-    // them as a programmatic dependent launch (an ordinary launch while the
-    // kernels are timed one by one).  Every deep pair is an FP64 solve here,
-    // so the deep pass gets the pair kernel's grid; the regular pass's blocks
-    // take the SMs as the deep pass's blocks retire.
-    LAUNCH(w, KK_DEEP, k_pair_deep<FOLD_BG, LAW><<<pb, 128, 0, w->stream>>>(w->dw, w->par, record));
-    if (w->prof_on) {
-      LAUNCH(w, KK_PAIRS, k_pair_forces<FOLD_BG, LAW, false, PASS64_REGULAR><<<pb, 128, 0, w->stream>>>(
-                              w->dw, w->par, record));
-    } else {
-      launch_dependent(w, pb, k_pair_forces<FOLD_BG, LAW, false, PASS64_REGULAR>, record);
-    }
   } else {
     LAUNCH(w, KK_PAIRS,
            k_pair_forces<FOLD_BG, LAW><<<pb, 128, 0, w->stream>>>(w->dw, w->par, record));
@@ -756,7 +742,9 @@ int32_t set_particles_impl(xdem_world_s* w, const xdem_particles* P, const std::
   CK(w, B.alloc(&d.cell_scr, 2 * (size_t)n));
   CK(w, B.alloc(&d.cell_up, 2 * (size_t)n));
   CK(w, B.alloc(&d.body, n));
-  CK(w, B.alloc(&d.axis, n));
+  // the centre-line screen's axis records (mixed precision only)
+  d.axis = nullptr;
+  if (w->prm.precision == XDEM_PRECISION_MIXED) CK(w, B.alloc(&d.axis, n));
   d.screen_r = w->law == LAW_CIRCLE ? d.rad : d.orad;
   // wall segments: vertices by id (their screening radius follows from the
   // vertices and the position, screen_radius in kernels.cuh)
@@ -806,8 +794,7 @@ int32_t set_particles_impl(xdem_world_s* w, const xdem_particles* P, const std::
   CK(w, B.alloc(&d.fallback, w->prm.precision == XDEM_PRECISION_MIXED ? ks : 1));
   CK(w, B.alloc(&d.nfallback, 1));
   CK(w, cudaMemsetAsync(d.nfallback, 0, sizeof(int32_t), s));
-  // the deep-pair list serves closest-approach worlds of both precisions
-  CK(w, B.alloc(&d.deep, ks));
+  CK(w, B.alloc(&d.deep, w->prm.precision == XDEM_PRECISION_MIXED ? ks : 1));
   d.warm = nullptr;
   if (w->mlp) CK(w, B.alloc(&d.warm, ks));
   // candidate lists: rebuilt by the first step (vl_valid starts at 0)
@@ -873,6 +860,7 @@ int32_t set_particles_impl(xdem_world_s* w, const xdem_particles* P, const std::
   add(d.force, 16);
   add(d.pcell, 4);  // read by the candidate scan's history test after a re-sort
   add(d.gcell, 4);
+  if (d.axis) add(d.axis, 16);  // written by k_scatter before the re-sort
   size_t off = 0;
   for (int a = 0; a < L.count; ++a) {
     L.offset[a] = off;

@@ -345,6 +345,16 @@ __global__ void k_scatter(DevWorld w) {
   const float sr = screen_radius(w, i);
   const float idb = __int_as_float((w.setting[i] & SKIP_CONTACT_DETECTION) ? -1 : w.id_of[i]);
   const int up = w.up[i];
+  if (w.axis && w.shape[i] == SHAPE_ELLIPSE) {
+    // the centre-line screen's record (pairs.cuh, axis_shape): the
+    // orientation reduced to [-pi, pi] in FP64 before the FP32 sine and cosine
+    double r = w.rot[i];
+    r -= 6.283185307179586 * rint(r * 0.15915494309189535);
+    float sn, cs;
+    __sincosf((float)r, &sn, &cs);
+    const float a = (float)w.rad[i];
+    w.axis[i] = make_float4(cs, sn, a, __fdividef(a, (float)w.asp[i]));
+  }
   int q = w.cell_start[pc] + w.prank[i];
   w.cell_mem[q] = i;
   w.cell_pos[q] = p;

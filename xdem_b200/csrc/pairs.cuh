@@ -91,7 +91,7 @@ struct AxisShape {
   float c, s, a, b;
 };
 
-// the screen's record of the ellipse at m (k_bodies wrote it this step)
+// the screen's record of the ellipse at m (k_scatter wrote it this step)
 __device__ __forceinline__ AxisShape axis_shape(const DevWorld& w, int m) {
   const float4 r = w.axis[m];
   return AxisShape{r.x, r.y, r.z, r.w};
@@ -133,28 +133,32 @@ __device__ __forceinline__ int centre_line_class(float dx, float dy, const AxisS
 // list) that the centre-line screen classed deep
 constexpr int kDeepFlag = 1 << 24;
 
-// the centre-line screen (dropping separated pairs) applies to
-// mixed-precision worlds of ellipses under one law
+// the centre-line screen applies to mixed-precision worlds of ellipses under
+// one law
 template <int LAW>
 __device__ __forceinline__ bool centre_line_screen(const DevWorld& w) {
   return (LAW == LAW_CLOSEST || LAW == LAW_INTERSECTION) && w.precision == XDEM_PRECISION_MIXED;
-}
-
-// the centre-line class is computed for those worlds and for every
-// closest-approach world, whose deep pairs are evaluated in a pass of their
-// own in both precisions (the FP64 path drops nothing: the class only orders
-// the evaluation)
-template <int LAW>
-__device__ __forceinline__ bool centre_line_classes(const DevWorld& w) {
-  return LAW == LAW_CLOSEST || centre_line_screen<LAW>(w);
 }
 
 // the owner's record for the screen
 template <int LAW>
 __device__ __forceinline__ AxisShape owner_axis_shape(const DevWorld& w, int m) {
   AxisShape e{0.0f, 0.0f, 0.0f, 0.0f};
-  if (centre_line_classes<LAW>(w)) e = axis_shape(w, m);
+  if (centre_line_screen<LAW>(w)) e = axis_shape(w, m);
   return e;
+}
+
+// this step's record of the owner's body for the pair kernels; an ellipse's
+// (cos, sin) is computed once per body instead of once per pair
+template <int LAW>
+__device__ __forceinline__ void write_owner_body(const DevWorld& w, int m) {
+  double2 cs = make_double2(0.0, 0.0);
+  if (LAW == LAW_CLOSEST || LAW == LAW_INTERSECTION ||
+      (LAW == LAW_ANY && w.shape[m] == SHAPE_ELLIPSE)) {
+    const double r = w.rot[m];
+    cs = make_double2(cos(r), sin(r));
+  }
+  write_body(w, m, cs);
 }
 
 // ---- phase A --------------------------------------------------------------------
@@ -239,14 +243,14 @@ __device__ __forceinline__ void scan_cells(const DevWorld& w, const WorldScalars
         if (!pass) continue;
       }
       int cls = CL_REGULAR;
-      if (centre_line_classes<LAW>(w)) {
+      if (centre_line_screen<LAW>(w)) {
         // the same FP64 image offset as the candidate lists' test (verlet.cuh)
         const double2 pj = w.cell_pos[q];
         vec2<double> off, ovel;
         image_offset(ws, kind, pi, pj, off, ovel);
         cls = centre_line_class((float)((pj.x + off.x) - pi.x), (float)((pj.y + off.y) - pi.y),
                                 shape_ax, axis_shape(w, w.cell_mem[q]));
-        if (cls == CL_SEPARATED && centre_line_screen<LAW>(w)) continue;
+        if (cls == CL_SEPARATED) continue;
       }
       if (nlist >= K) {
         st |= ST_CAPACITY;
@@ -392,6 +396,7 @@ __global__ void __launch_bounds__(128) k_candidates(DevWorld w, int par) {
   int32_t list_mj[kMaxSlots];
   int32_t list_code[kMaxSlots];
   if (valid) {
+    write_owner_body<LAW>(w, m);
     const AxisShape shape_ax = owner_axis_shape<LAW>(w, m);
     Grid G = grid_of(ws);
     const int id_i = w.id_of[m];
@@ -462,12 +467,6 @@ struct PairCounters {
   uint32_t n_solves = 0, n_iters = 0, n_capped = 0;
   uint32_t w_off = 0, w_used = 0, w_rej = 0, w_rest = 0, w_right = 0;
 };
-
-// Which listed pairs a launch of the FP64 pair kernel evaluates: all of them,
-// or all but the deep ones (PairEntry::pad), which k_pair_deep evaluates
-// beside it.  Every pair is evaluated by the same operations whichever pass
-// takes it.
-enum { PASS64_ALL = 0, PASS64_REGULAR = 1 };
 
 // One listed pair t: image offset, contact geometry, history and force,
 // written to the owner's slot.  WARM: a closest-approach pair starts Newton
@@ -584,33 +583,16 @@ __device__ __forceinline__ void pair_forces_fp64(const DevWorld& w, int par, int
   }
 }
 
-template <bool FOLD_BG, int LAW, bool WARM = false, int PASS = PASS64_ALL>
+// one thread per listed pair (grid-stride loop)
+template <bool FOLD_BG, int LAW, bool WARM = false>
 __global__ void __launch_bounds__(128, 4) k_pair_forces(DevWorld w, int par, int record) {
   if (stopped(w)) return;
   const int npairs = *w.npairs;
   PairCounters pc;
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < npairs; t += gridDim.x * blockDim.x) {
-    if (PASS == PASS64_REGULAR && w.pairs[t].pad) continue;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < npairs; t += gridDim.x * blockDim.x)
     pair_forces_fp64<FOLD_BG, LAW, WARM>(w, par, record, t, pc);
-  }
   flush_warp(w, pc.st, pc.n_solves, pc.n_iters, pc.n_capped);
   if (WARM) flush_warm(w, pc.w_off, pc.w_used, pc.w_rej, pc.w_rest, pc.w_right);
-}
-
-// The deep pairs of a closest-approach world (the deep-pair list written by
-// the candidate kernels), launched ahead of the regular pass, which may start
-// at once (a programmatic dependent launch): the Newton iterations that run
-// long (deep overlaps) then start with the step's other pairs instead of
-// ending the pair phase as a serial tail.
-template <bool FOLD_BG, int LAW>
-__global__ void __launch_bounds__(128) k_pair_deep(DevWorld w, int par, int record) {
-  if (stopped(w)) return;
-  const int ndeep = *w.ndeep;
-  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-  PairCounters pc;
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ndeep; t += gridDim.x * blockDim.x)
-    pair_forces_fp64<FOLD_BG, LAW, false>(w, par, record, w.deep[t], pc);
-  flush_warp(w, pc.st, pc.n_solves, pc.n_iters, pc.n_capped);
 }
 
 // ---- end of the update ----------------------------------------------------------

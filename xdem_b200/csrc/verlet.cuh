@@ -24,33 +24,12 @@ namespace xdem {
 constexpr int kVlBlock = 256;
 constexpr int kVlGroup = 2;  // list entries whose loads k_candidates_vl issues together
 
-// The bodies' records for this step's contact update, written after the
-// step's last position move and memory-order refresh, so that the candidate
-// and pair kernels only read them: the pair kernels' 96-byte record with
-// (cos, sin) of an ellipse's orientation in FP64, and the FP32 axis record of
-// the centre-line class.  With candidate lists, also the block maxima of the
-// path lengths since the last list build.
-template <int LAW>
-__global__ void __launch_bounds__(kVlBlock) k_bodies(DevWorld w) {
+// block maxima of the path lengths since the last build
+__global__ void __launch_bounds__(kVlBlock) k_vl_maxdisp(DevWorld w) {
   if (stopped(w)) return;
   __shared__ double sh[kVlBlock / 32];
   const int m = blockIdx.x * blockDim.x + threadIdx.x;
-  double v = 0.0;
-  if (m < w.n) {
-    double2 cs = make_double2(0.0, 0.0);
-    if (LAW == LAW_CLOSEST || LAW == LAW_INTERSECTION ||
-        (LAW == LAW_ANY && w.shape[m] == SHAPE_ELLIPSE)) {
-      const double r = w.rot[m];
-      cs = make_double2(cos(r), sin(r));
-    }
-    write_body(w, m, cs);
-    if (centre_line_classes<LAW>(w)) {
-      const double a = w.rad[m];
-      w.axis[m] = make_float4((float)cs.x, (float)cs.y, (float)a, (float)(a / w.asp[m]));
-    }
-    if (w.V) v = w.vl_disp[m];
-  }
-  if (!w.V) return;
+  double v = m < w.n ? w.vl_disp[m] : 0.0;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
   if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
@@ -140,8 +119,8 @@ __global__ void __launch_bounds__(128) k_vl_build(DevWorld w) {
   w.vl_cnt[m] = cnt;
 }
 
-// k_candidates with the lists: same outputs (slot counts, carried-over
-// history, the compact pair list), the same filters and
+// k_candidates with the lists: same outputs (body records, slot counts,
+// carried-over history, the compact pair list), the same filters and
 // tests.  Seven blocks per SM (72 registers): the kernel is latency-bound on
 // its partner gathers, and six blocks with more registers measured slower.
 template <int LAW>
@@ -158,6 +137,7 @@ __global__ void __launch_bounds__(128, 7) k_candidates_vl(DevWorld w, int par) {
   int32_t list_mj[kMaxSlots];
   int32_t list_code[kMaxSlots];
   if (valid) {
+    write_owner_body<LAW>(w, m);
     const AxisShape shape_ax = owner_axis_shape<LAW>(w, m);
     const Grid G = grid_of(ws);
     const int id_i = w.id_of[m];
@@ -243,10 +223,10 @@ __global__ void __launch_bounds__(128, 7) k_candidates_vl(DevWorld w, int par) {
             pass = coarse_pass<LAW>(0, 0, r_i, sg[u], orad_i, sg[u], pi, pj, off);
           if (!pass) continue;
           int cls = CL_REGULAR;
-          if (centre_line_classes<LAW>(w)) {
+          if (centre_line_screen<LAW>(w)) {
             cls = centre_line_class((float)((pj.x + off.x) - pi.x), (float)((pj.y + off.y) - pi.y),
                                     shape_ax, axis_shape(w, mj));
-            if (cls == CL_SEPARATED && centre_line_screen<LAW>(w)) continue;
+            if (cls == CL_SEPARATED) continue;
           }
           if (nlist >= K) {
             st |= ST_CAPACITY;

@@ -74,8 +74,8 @@ struct WorldScalars {
 
 // One body as the pair kernels read it: every field of a contact
 // construction in one 96-byte record (three 32-byte sectors per gather,
-// against eight scattered arrays).  k_bodies rewrites it each step, after the
-// last position move of the step's first half.
+// against eight scattered arrays).  The candidate kernels rewrite it each
+// step, after the last position move of the step's first half.
 struct alignas(32) BodyRec {
   double2 pos, vel;
   double rot, w, r, asp;
@@ -151,8 +151,8 @@ struct DevWorld {
   int32_t* cell_up;       // [2n] upLevel of each cell entry
   BodyRec* body;          // [n] this step's pair-kernel record of each body
   // [n] FP32 (cos, sin) of each ellipse's orientation and its semi-axes (a, b),
-  // for the centre-line class of the candidate kernels; written with the
-  // body records
+  // for the centre-line screen of the mixed-precision candidate kernels;
+  // written by k_scatter, moved by a re-sort (NULL in FP64 worlds)
   float4* axis;
   const double* screen_r; // rad for an all-circle world, orad otherwise (segments: screen_radius)
   int32_t* pcell;  // [n] regular cell of the particle at m
