@@ -735,6 +735,37 @@ def accuracy(work, steps=2000, sample_every=100):
     return {"one_step_forces": one_step, "mean_shear_stress": shear}
 
 
+def mlp_kernels():
+    """A few launches of the learned warm start's kernels, for a profiler:
+    training (k_mlp_train) on 262,144 synthetic samples, 2 epochs, then
+    inference (k_mlp_warm) in a Lees-Edwards world of 65,536 ellipses
+    (a/b ~ U[1,3], b in {0.5, 0.7}) with the network attached, 8 steps."""
+    from xdem_b200 import abi, inputs
+    from xdem_b200.learned import Mlp
+    from xdem_b200.world import World, make_control, make_params
+    net = Mlp(seed=3)
+    rng = np.random.default_rng(0)
+    n = 262144
+    net.add_samples(rng.normal(0, 1, (n, 7)).astype(np.float32),
+                    rng.uniform(0.5, 1.0, n).astype(np.float32),
+                    (rng.uniform(0, 1, n) > 0.5).astype(np.float32))
+    net.train(2, batch=8192, lr=1e-3, seed=1)
+    p, box = inputs.ellipse_system(65536, b=inputs.c2_b, aspect=inputs.c4_aspect,
+                                   phi_rsa_circle=0.40, phi=None, seed=5)
+    area = (box[1] - box[0]) * (box[3] - box[2])
+    box = inputs.scale_to_fraction(p, box, p["volume"].sum(), p["volume"].sum() / area * 1.6)
+    prm = make_params(abi.WORLD_LEES_EDWARDS, inputs.time_step(p), box, inputs.KN, inputs.KT,
+                      inputs.RESTITUTION, inputs.FRICTION, shift_strain_rate=0.1)
+    w = World(prm)
+    w.raise_mask = ~(abi.ERR_NEWTON | abi.ERR_NONFINITE)
+    w.set_particles(p)
+    net.attach(w)
+    w.run(8, make_control())
+    log(f"mlp kernels: {w.pair_count()} listed pairs in the last step")
+    w.close()
+    net.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -751,11 +782,16 @@ def main():
     ap.add_argument("--no-learned", action="store_true",
                     help="skip training and timing the learned warm start")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--mlp-kernels", action="store_true",
+                    help="only launch the learned warm start's kernels a few times (profiling)")
     ap.add_argument("--cpu-child", default=None, help=argparse.SUPPRESS)
     ap.add_argument("--cpu-kind", default="port", help=argparse.SUPPRESS)
     ap.add_argument("--threads", type=int, default=0, help=argparse.SUPPRESS)
     ap.add_argument("--budget", type=float, default=20.0, help=argparse.SUPPRESS)
     args = ap.parse_args()
+    if args.mlp_kernels:
+        mlp_kernels()
+        return
     if args.cpu_child:
         _cpu_child(args.cpu_child, args.steps, args.warmup, args.threads or os.cpu_count(),
                    args.budget, args.cpu_kind)
