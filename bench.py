@@ -255,19 +255,38 @@ def cpu_sample_c0(seed, threads, n=1024):
             "cpu_kind": "reference", "cpu_note": f"{n} discs at 0.70 made on the CPU"}
 
 
+def cpu_sample_c1_prefix(steps=4000):
+    """The ellipse compression's start (tests/golden/long_c1_closest.npz: 512
+    ellipses, b ~ U[0.4, 0.6], a = 1.5 b, an overlap-free RSA at 0.50, strain
+    control at -1e-4), over a prefix on which the compiled reference returns
+    (it stops returning after ~10,000 steps of this run)."""
+    from xdem_b200 import abi, inputs
+    from xdem_b200.world import make_control, make_params
+    z = np.load(os.path.join(ROOT, "tests", "golden", "long_c1_closest.npz"))
+    p = {k[2:]: z[k] for k in z.files if k.startswith("p_")}
+    prm = make_params(abi.WORLD_PERIODIC_CONTROL, float(z["dt"]), z["box0"], inputs.KN, inputs.KT,
+                      inputs.RESTITUTION, inputs.FRICTION)
+    rate = float(z["rate"])
+    return {"particles": p, "contacts": None, "params": prm, "steps": steps,
+            "control": make_control(update_stress=True, box_law=abi.BOX_STRAIN, p0=rate, p1=rate),
+            "cpu_kind": "reference", "cpu_note": "512-ellipse compression prefix"}
+
+
 def reference_vs_restatement(threads, seed):
     """Speed of the compiled reference and of the C restatement on the same
-    CPU-made inputs, both with `threads` threads: the disc configuration
-    (1,024 discs) and a 4,096-ellipse sample of the shear workload.  The
-    restatement is what the full-size CPU leg times; this relates it to the
-    reference's own code where both return."""
+    CPU-made inputs where the reference returns: the disc configuration
+    (1,024 discs, `threads` threads each) and the first steps of the ellipse
+    compression (512 ellipses, one thread each).  The restatement is what the
+    full-size CPU leg times; this relates it to the reference's own code."""
     out = {}
-    for name, make in (("discs_1024", lambda: cpu_sample_c0(seed, threads)),
-                       ("ellipses_4096", lambda: cpu_sample_le_ellipses(4096, seed, threads))):
+    cases = (("discs_1024", lambda: cpu_sample_c0(seed, threads), threads),
+             ("ellipses_512_compression", cpu_sample_c1_prefix, 1))
+    for name, make, th in cases:
         work = make()
-        ref = run_cpu(work, 400, 1, threads, budget_s=8.0, timeout_s=120, kind="reference")
-        port = run_cpu(work, 400, 1, threads, budget_s=8.0, timeout_s=120, kind="port")
-        entry = {"reference": ref.get("value"), "restatement": port.get("value")}
+        steps = work.get("steps", 400)
+        ref = run_cpu(work, steps, 1, th, budget_s=8.0, timeout_s=120, kind="reference")
+        port = run_cpu(work, steps, 1, th, budget_s=8.0, timeout_s=120, kind="port")
+        entry = {"threads": th, "reference": ref.get("value"), "restatement": port.get("value")}
         if ref.get("kind") != "reference" or "error" in ref:
             entry["reference_note"] = ref.get("error", "compiled reference not available")
         if entry["reference"] and entry["restatement"]:

@@ -438,7 +438,7 @@ int32_t xdem_set_candidate_lists(xdem_world w, int32_t capacity, double skin_fra
    counterpart in the reference, whose particles stay in id order).  The
    arrays are re-sorted by cell every `interval` steps so that neighbours sit
    at nearby addresses; results do not depend on it.  interval: odd, or 0 =
-   never re-sort; default 31. */
+   never re-sort; default 63. */
 int32_t xdem_set_memory_order_refresh(xdem_world w, int32_t interval);
 /* out = {list rebuilds since the last xdem_reset_newton_stats, longest list,
    total entries, capacity} */
