@@ -92,6 +92,9 @@ def port_lib():
         _port["bisect_quartic"] = lib.xo_bisect_quartic
         _port["status"] = lib.xo_status
         _port["newton_quartic"] = lib.xo_newton_quartic
+        lib.xo_closest_quartic.restype = C.c_int32
+        lib.xo_closest_quartic.argtypes = [C.c_int32, _d, _d, _d, _d]
+        _port["closest_quartic"] = lib.xo_closest_quartic
     return _port
 
 
@@ -237,6 +240,21 @@ def ref_particle_properties(shape, radius, aspect, density=1.0):
                                *[out[k].ctypes.data_as(_d) for k in
                                  ("volume", "mass", "inv_mass", "inertia", "inv_inertia")])
     return out
+
+
+def closest_quartic(pi, pj, off):
+    """Per ellipse pair (pair_geometry's input layout), the checker's
+    closest-approach quartic: columns A, B, C, D, E, the analytic start
+    s = sqrt(delta+1), the root q, Newton's iterations, 1 where Newton did not
+    terminate, contacted; zeros where the pair is rejected before the quartic
+    is formed."""
+    pi = np.ascontiguousarray(pi, np.float64)
+    pj = np.ascontiguousarray(pj, np.float64)
+    off = np.ascontiguousarray(off, np.float64)
+    out = np.zeros((pi.shape[0], 10))
+    st = port_lib()["closest_quartic"](pi.shape[0], pi.ctypes.data_as(_d), pj.ctypes.data_as(_d),
+                                       off.ctypes.data_as(_d), out.ctypes.data_as(_d))
+    return out, st
 
 
 def newton_quartic(A, B, Cc, D, E, init):

@@ -92,6 +92,10 @@ typedef struct {
   double overlap;
   v2 rv, nrv, srv;
   int iters;
+  /* closest approach: the quartic A..E, the analytic start s, the root q and
+     whether Newton did not terminate (xo_closest_quartic) */
+  double quartic[5], q_start, q;
+  int stuck;
 } geom_t;
 
 typedef struct {
@@ -265,6 +269,10 @@ static int ellipse_closest(const pstate_t* a, const pstate_t* b, v2 off, v2 ovel
     *st |= XDEM_ERR_NEWTON;
   }
   g->iters = it;
+  g->quartic[0] = A; g->quartic[1] = B; g->quartic[2] = C; g->quartic[3] = D; g->quartic[4] = E;
+  g->q_start = start;
+  g->q = q;
+  g->stuck = stuck;
   double temp = (q * q - 1.0) / delta;
   double d_prime = 0.0;
   if (temp < 0) temp = 0.0;
@@ -590,6 +598,29 @@ int32_t xo_pair_geometry(int32_t npairs, int32_t method, const double* pi, const
     o[10] = g.rv.x; o[11] = g.rv.y; o[12] = g.nrv.x; o[13] = g.nrv.y;
     o[14] = g.srv.x; o[15] = g.srv.y;
     o[16] = (double)g.iters;
+  }
+  return (int32_t)st;
+}
+
+int32_t xo_closest_quartic(int32_t npairs, const double* pi, const double* pj, const double* off,
+                           double* out) {
+  uint32_t st = 0;
+  for (int k = 0; k < npairs; ++k) {
+    const double* a = pi + 9 * k;
+    const double* b = pj + 9 * k;
+    pstate_t A = {(int)a[0], a[1], a[2], a[3], a[4], a[5], a[6], a[7], a[8], {0, 0}, {0, 0}};
+    pstate_t B = {(int)b[0], b[1], b[2], b[3], b[4], b[5], b[6], b[7], b[8], {0, 0}, {0, 0}};
+    geom_t g;
+    int c = contact_geometry(XDEM_ELLIPSE_CLOSEST_APPROACH, &A, &B, a[1], b[1],
+                             V(off[4 * k], off[4 * k + 1]), V(off[4 * k + 2], off[4 * k + 3]),
+                             &g, &st);
+    double* o = out + 10 * k;
+    for (int i = 0; i < 5; ++i) o[i] = g.quartic[i];
+    o[5] = g.q_start;
+    o[6] = g.q;
+    o[7] = (double)g.iters;
+    o[8] = (double)g.stuck;
+    o[9] = c ? 1.0 : 0.0;
   }
   return (int32_t)st;
 }

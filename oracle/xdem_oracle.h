@@ -57,5 +57,11 @@ double xo_newton_quartic(double A, double B, double C, double D, double E, doubl
                          int32_t* iters, int32_t* stuck);
 /* the root on [min(1, s), max(1, s)] by bisection (q if no sign change) */
 double xo_bisect_quartic(double A, double B, double C, double D, double E, double s, double q);
+/* Closest approach of ellipse pairs (layout of xo_pair_geometry's inputs): per
+   pair A, B, C, D, E of the quartic, the analytic start s = sqrt(delta+1), the
+   root q, Newton's iterations, 1 where Newton did not terminate, contacted.
+   Pairs rejected before the quartic is formed carry zeros. */
+int32_t xo_closest_quartic(int32_t npairs, const double* pi, const double* pj, const double* off,
+                           double* out);
 
 #endif

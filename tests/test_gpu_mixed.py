@@ -14,10 +14,12 @@ the stated error of the mixed path:
   - forces after one step from an identical state: within 1e-5 of the
     largest contact force, per contact (the force tolerance the mixed mode
     promises), torques likewise;
-  - mean shear stress of a Lees-Edwards shear run: within 0.5 %, or within
-    the spread that a 1e-12 perturbation of the initial state produces in
-    the FP64 path itself, whichever is larger (a short run of a small system
-    is chaotic enough for the two to be comparable).
+  - shear stress of a Lees-Edwards shear run: at the benchmark size, the
+    first step's within 1e-6 and the 2,000-step mean within 5 % (the FP64
+    path's own 2,000-step mean moves by 1.4 % when the initial positions move
+    by one part in 1e15); in a small system, within 0.5 % or within the
+    spread that a 1e-12 perturbation of the initial state produces in the FP64
+    path itself, whichever is larger.
 Pairs whose FP64 closest-approach Newton iteration does not converge (the
 reference's loop never returns on them, EllipticParticle.cpp:621; the
 checker stops it at its cap) have no FP64 answer to compare with and are
@@ -255,14 +257,28 @@ def test_deep_pairs_beside_the_other_pairs_are_bit_identical():
 def test_mixed_accuracy_at_the_shear_configuration_size():
     """The mixed-precision configuration at its size: 262,144 ellipses with
     a/b ~ U[1,2] and b in {0.5, 0.7}, compressed to solid fraction 0.85 and
-    sheared in a LeesEdwardsBoundaryWorld at 1e-3 sqrt(kn/m_min).  Against the
+    sheared in a LeesEdwardsBoundaryWorld at 1e-3 sqrt(kn/m_min), against the
     FP64 path on the same packing and history (the FP64 path reproduces the
-    checker to 1e-10 per contact at smaller sizes, tests above), with fixed
-    bars: (1) after one step, every contact both paths hold has a force within
-    1e-5 of the largest FP64 contact force, the contact sets agree but for at
-    most 1e-5 of the contacts (pairs within rounding of tangency); (2) the
-    mean shear stress over 2,000 steps (sampled every 100) agrees within
-    0.5 %."""
+    checker to 1e-10 per contact, tests above).  Fixed bars:
+      (1) after one step, every contact both paths hold has a force within
+          1e-5 of the largest FP64 contact force, and the contact sets agree
+          but for at most 1e-5 of the contacts (pairs within rounding of
+          tangency);
+      (2) the shear stress of that step within 1e-6 (relative; the two
+          paths hold the same contacts there and their sums differ by about
+          1e-10);
+      (3) the mean shear stress over 2,000 steps (sampled every 100) within
+          5 %.
+    Beyond the first steps the two paths hold different sets of a few deep
+    contacts: the closest-approach Newton iteration can end at different
+    roots of the quartic for inputs one rounding apart (long solves wander
+    before converging, and the root decides contact or no contact), so on
+    this packing four deep contacts worth 0.6 % of the shear stress are in
+    the FP64 path's second step and not in the mixed one's, and the FP64 path
+    started from positions scaled by (1 + 1e-15) gains one by step 5.  Its
+    2,000-step mean then lies 1.4 % away from the unperturbed run's (4.7 %
+    from 1 + 1e-12).  A 0.5 % bar on one run's mean is below that floor;
+    bars (1) and (2) are where the precision shows."""
     import math
     from xdem_b200 import inputs, packing
     from xdem_b200.world import make_params
@@ -275,11 +291,15 @@ def test_mixed_accuracy_at_the_shear_configuration_size():
     prm = make_params(abi.WORLD_LEES_EDWARDS, dt, b, inputs.KN, inputs.KT, inputs.RESTITUTION,
                       inputs.FRICTION, shift_strain_rate=rate)
     worlds = [World(prm), World(_mixed(prm))]
+    ctl = make_control(update_stress=True)
+    first = []
     for w in worlds:
         w.raise_mask = ~abi.ERR_NEWTON
         w.set_particles(q)
         w.set_contacts(contacts)
-        w.takeTimeStep()
+        w.run(1, ctl)
+        first.append(w.getStress()[1])
+    assert abs(first[1] - first[0]) <= 1e-6 * abs(first[0]), first
     c64, cmx = worlds[0].get_contacts(), worlds[1].get_contacts()
     k64 = c64["id_i"].astype(np.int64) << 32 | c64["id_j"].astype(np.int64)
     kmx = cmx["id_i"].astype(np.int64) << 32 | cmx["id_j"].astype(np.int64)
@@ -291,11 +311,10 @@ def test_mixed_accuracy_at_the_shear_configuration_size():
     scale = np.max(np.hypot(f64[:, 0], f64[:, 1]))
     err = np.hypot(*(fmx[imx] - f64[i64]).T) / scale
     assert err.max() <= FORCE_TOL, float(err.max())
-    ctl = make_control(update_stress=True)
     series = [[], []]
     for _ in range(20):
         for w, s in zip(worlds, series):
             w.run(100, ctl)
             s.append(w.getStress()[1])
     m64, mmx = float(np.mean(series[0])), float(np.mean(series[1]))
-    assert abs(mmx - m64) <= 5e-3 * abs(m64), (m64, mmx)
+    assert abs(mmx - m64) <= 5e-2 * abs(m64), (m64, mmx)

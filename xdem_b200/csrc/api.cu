@@ -238,6 +238,12 @@ void launch_dependent(xdem_world_s* w, int blocks, void (*kernel)(DevWorld, int,
 
 // updateContacts as candidate scan, per-pair forces, and history carry-over
 // (pairs.cuh); the pair kernel runs a grid-stride loop over the listed pairs
+// dynamic shared memory of k_candidates_vl: the kept entries of a block's 128
+// owners, partner positions and codes, K slots each
+static size_t candidates_smem(const xdem_world_s* w) {
+  return (size_t)2 * w->dw.K * 128 * sizeof(int32_t);
+}
+
 template <bool FOLD_BG, int LAW>
 void launch_update_phases(xdem_world_s* w, int record) {
   const int nb = blocks_for(w->dw.n, 128);
@@ -249,7 +255,8 @@ void launch_update_phases(xdem_world_s* w, int record) {
     LAUNCH(w, KK_VL_CHECK, k_vl_maxdisp<<<vb, kVlBlock, 0, w->stream>>>(w->dw));
     LAUNCH(w, KK_VL_CHECK, k_vl_check<<<1, 1024, 0, w->stream>>>(w->dw, vb));
     LAUNCH(w, KK_VL_BUILD, k_vl_build<LAW><<<nb, 128, 0, w->stream>>>(w->dw));
-    LAUNCH(w, KK_CANDIDATES, k_candidates_vl<LAW><<<nb, 128, 0, w->stream>>>(w->dw, w->par));
+    LAUNCH(w, KK_CANDIDATES, k_candidates_vl<LAW><<<nb, 128, candidates_smem(w), w->stream>>>(
+                                 w->dw, w->par));
   } else {
     LAUNCH(w, KK_CANDIDATES, k_candidates<LAW><<<nb, 128, 0, w->stream>>>(w->dw, w->par));
   }

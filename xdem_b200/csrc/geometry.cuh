@@ -241,11 +241,14 @@ constexpr double kWarmResidual = 0.05;
 //
 // WARM: `warm` is a predicted root as a fraction of the analytic start
 // sqrt(δ+1) (mlp.cuh).  It is clamped to [min(1, s), max(1, s)], s = sqrt(δ+1),
-// the interval that holds the root the plain start converges to (the quartic
-// has one positive root there); it is used only when the first Newton step
-// from it is below kWarmResidual of it, and a root that leaves the interval is
-// discarded for the plain iteration from s.  Newton then stops at the same
-// tolerance, so the answer is the plain solver's.
+// the interval of the closest-approach root; it is used only when the first
+// Newton step from it is below kWarmResidual of it, and a root that leaves the
+// interval is discarded for the plain iteration from s.  Newton then stops at
+// the same tolerance, so the answer is the plain solver's wherever the plain
+// iteration converges inside the interval.  It does not always: after a long
+// wander the plain iteration can end at a root outside it (most often a
+// negative one), which the reference then uses, and there the warm start's
+// answer differs.
 template <bool WARM = false>
 __device__ __forceinline__ bool ellipse_closest(const PState& a, const PState& b, vec2<double> off,
                                                 vec2<double> ovel, double k1x, double k1y,

@@ -185,8 +185,9 @@ __device__ __forceinline__ int neighbour_cell(const Grid& G, int world_kind, int
 // The reference's 3x3 scan for the owner at m (cell ix, iy): every candidate
 // j with a larger id and another upLevel, counted per image kind against the
 // 200-candidate cap, and the ones passing the coarse test appended to
-// (list_mj, list_code); `matched` receives the old slots of the listed pairs
-// (all of them candidates, so their old slots count as seen).  The distance
+// (list_mj, list_code), entry s at index s * stride; `matched` receives the
+// old slots of the listed pairs (all of them candidates, so their old slots
+// count as seen).  The distance
 // screen runs in FP32 on positions relative to the cell corners; only
 // candidates within its rounding margin of the threshold take the
 // reference's FP64 test.
@@ -195,8 +196,9 @@ __device__ __forceinline__ void scan_cells(const DevWorld& w, const WorldScalars
                                            int m, int ix, int iy, double2 pi, int id_i, int up_i,
                                            int shape_i, double r_i, double orad_i,
                                            const Slots& old, int nold, int& nlist,
-                                           int32_t* list_mj, int32_t* list_code, uint32_t& st,
-                                           uint32_t& matched, const AxisShape& shape_ax) {
+                                           int32_t* list_mj, int32_t* list_code, int stride,
+                                           uint32_t& st, uint32_t& matched,
+                                           const AxisShape& shape_ax) {
   const int n = w.n, K = w.K;
   // the owner relative to its cell's corner, in FP32 (see k_scatter)
   const float rxi = (float)(pi.x - (ws.xmin + ix * G.lx));
@@ -260,12 +262,41 @@ __device__ __forceinline__ void scan_cells(const DevWorld& w, const WorldScalars
       for (int z = 0; z < nold; ++z)
         if (old.partner[(size_t)z * n + m] == id_j) oslot = z;
       if (oslot != kNoOldSlot) matched |= 1u << oslot;
-      list_mj[nlist] = w.cell_mem[q];
-      list_code[nlist] =
+      list_mj[nlist * stride] = w.cell_mem[q];
+      list_code[nlist * stride] =
           kind | (nlist << 8) | (oslot << 16) | (LAW == LAW_CLOSEST && cls == CL_DEEP ? kDeepFlag : 0);
       ++nlist;
     }
   }
+}
+
+// Old slots of the owner at m (cell ix, iy) whose partner is a candidate of
+// its 3x3 scan this step: the listed ones (`matched`) and the others whose
+// partner sits in one of the nine cells and passes the candidate filters.
+// Such a pair's history is replaced by the pair kernel or dropped; the other
+// old slots are carried over.
+__device__ __forceinline__ uint32_t seen_old_slots(const DevWorld& w, const Slots& old, const Grid& G,
+                                                   int m, int ix, int iy, int up_i, int nold,
+                                                   uint32_t matched) {
+  uint32_t seen = matched;
+  for (int z = 0; z < nold; ++z) {
+    if (matched & (1u << z)) continue;
+    const int p = old.partner[(size_t)z * w.n + m];
+    if (p < 0) continue;
+    const int mj = w.mpos[p];
+    if (w.setting[mj] & SKIP_CONTACT_DETECTION) continue;
+    if (w.up[mj] == up_i) continue;
+    const int cr = w.pcell[mj], cg = w.gcell[mj];
+    bool hit = false;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      int kind;
+      const int c = neighbour_cell(G, w.kind, ix, iy, k / 3 - 1, k % 3 - 1, kind);
+      hit |= c == cr || c == cg;
+    }
+    if (hit) seen |= 1u << z;
+  }
+  return seen;
 }
 
 // Registers the contact in the owner's slot (m, slot) with its partner at
@@ -412,27 +443,8 @@ __global__ void __launch_bounds__(128) k_candidates(DevWorld w, int par) {
       const int ix = cell_local % G.nx, iy = cell_local / G.nx;
       uint32_t matched = 0;
       scan_cells<LAW>(w, ws, G, m, ix, iy, pi, id_i, up_i, shape_i, r_i, orad_i, old, nold, nlist,
-                      list_mj, list_code, st, matched, shape_ax);
-      // old partners among the candidates: the listed ones are; the others
-      // are looked up in the nine cells
-      seen = matched;
-      for (int z = 0; z < nold; ++z) {
-        if (matched & (1u << z)) continue;
-        const int p = old.partner[(size_t)z * n + m];
-        if (p < 0) continue;
-        const int mj = w.mpos[p];
-        if (w.setting[mj] & SKIP_CONTACT_DETECTION) continue;
-        if (w.up[mj] == up_i) continue;
-        const int cr = w.pcell[mj], cg = w.gcell[mj];
-        bool hit = false;
-#pragma unroll
-        for (int k = 0; k < 9; ++k) {
-          int kind;
-          const int c = neighbour_cell(G, w.kind, ix, iy, k / 3 - 1, k % 3 - 1, kind);
-          hit |= c == cr || c == cg;
-        }
-        if (hit) seen |= 1u << z;
-      }
+                      list_mj, list_code, 1, st, matched, shape_ax);
+      seen = seen_old_slots(w, old, G, m, ix, iy, up_i, nold, matched);
     }
     cur.count[m] = carry_over(w, old, cur, m, nold, seen, nlist, st);
   }

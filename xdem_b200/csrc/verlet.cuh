@@ -120,43 +120,67 @@ __global__ void __launch_bounds__(128) k_vl_build(DevWorld w) {
 }
 
 // k_candidates with the lists: same outputs (body records, slot counts,
-// carried-over history, the compact pair list), the same filters and
-// tests.  Seven blocks per SM (72 registers): the kernel is latency-bound on
-// its partner gathers, and six blocks with more registers measured slower.
+// carried-over history, the compact pair list), the same filters and tests,
+// evaluated by the warp together.  One lane per owner loads the owner and its
+// old partners; the warp's list entries are then taken 32 at a time across
+// all lanes (entry e of the warp belongs to the owner lane whose prefix range
+// of list lengths holds e), so that owners with long and short lists keep
+// every lane busy, and each lane fetches what it needs of its entry's owner
+// with warp shuffles.  The entries an owner keeps are ranked in list order
+// (a ballot per round), so the owner's list and its slot numbering are the
+// ones a thread walking its own list produces; they are staged in shared
+// memory, slot-major (entry s of the thread at tid at s * 128 + tid), and the
+// warp writes its pairs to the pair list together, coalesced, in owner order.
+// Dynamic shared memory: 2 * K * 128 int32.
 template <int LAW>
 __global__ void __launch_bounds__(128, 7) k_candidates_vl(DevWorld w, int par) {
   if (stopped(w)) return;
-  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  extern __shared__ int32_t s_list[];
+  __shared__ uint32_t s_matched[128];
+  const unsigned full = 0xffffffffu;
+  const int tid = threadIdx.x, lane = tid & 31, wbase = tid & ~31;
+  const int m = blockIdx.x * blockDim.x + tid;
   const bool valid = m < w.n;
-  const WorldScalars& ws = w.ws[valid ? sys_at(w, m) : 0];
   const int n = w.n, K = w.K;
+  int32_t* s_mj = s_list;
+  int32_t* s_code = s_list + K * 128;
   const Slots& old = w.slots[par];
   const Slots& cur = w.slots[par ^ 1];
   uint32_t st = 0;
-  int nlist = 0;
-  int32_t list_mj[kMaxSlots];
-  int32_t list_code[kMaxSlots];
+  int nlist = 0, cnt = 0, nold = 0, up_i = 0, shape_i = 0, ix = 0, iy = 0;
+  bool scan = false;
+  double2 pi = make_double2(0.0, 0.0);
+  double r_i = 0.0, orad_i = 0.0;
+  AxisShape shape_ax{0.0f, 0.0f, 0.0f, 0.0f};
+  Grid G{};
+  // the first four old partners (the usual case); the others are read where
+  // they are
+  int op0 = -1, op1 = -1, op2 = -1, op3 = -1;
+  s_matched[tid] = 0u;
   if (valid) {
+    const WorldScalars& ws = w.ws[sys_at(w, m)];
     write_owner_body<LAW>(w, m);
-    const AxisShape shape_ax = owner_axis_shape<LAW>(w, m);
-    const Grid G = grid_of(ws);
-    const int id_i = w.id_of[m];
-    const int nold = min(old.count[m], K);
-    uint32_t seen = 0;
-    if (G.nx >= 3 && G.ny >= 3 && !(w.setting[m] & SKIP_CONTACT_DETECTION)) {
-      const double2 pi = w.pos[m];
-      const int up_i = w.up[m];
-      const int shape_i = (LAW == LAW_ANY) ? w.shape[m] : 0;
-      const double r_i = w.rad[m], orad_i = w.orad[m];
+    shape_ax = owner_axis_shape<LAW>(w, m);
+    G = grid_of(ws);
+    nold = min(old.count[m], K);
+    scan = G.nx >= 3 && G.ny >= 3 && !(w.setting[m] & SKIP_CONTACT_DETECTION);
+    if (scan) {
+      pi = w.pos[m];
+      up_i = w.up[m];
+      shape_i = (LAW == LAW_ANY) ? w.shape[m] : 0;
+      r_i = w.rad[m];
+      orad_i = w.orad[m];
       // the owner's cell from this step's binning (k_bin, the same cell_of)
       const int cell_local = w.pcell[m] - G.base;
-      const int ix = cell_local % G.nx, iy = cell_local / G.nx;
-      const int cnt = w.vl_cnt[m];
-      // old slots of listed pairs known to be candidates now (see below)
-      uint32_t matched = 0;
+      ix = cell_local % G.nx;
+      iy = cell_local / G.nx;
+      cnt = w.vl_cnt[m];
       if (cnt < 0) {  // the list overflowed at its build: the full scan
-        scan_cells<LAW>(w, ws, G, m, ix, iy, pi, id_i, up_i, shape_i, r_i, orad_i, old, nold,
-                        nlist, list_mj, list_code, st, matched, shape_ax);
+        uint32_t matched = 0;
+        scan_cells<LAW>(w, ws, G, m, ix, iy, pi, w.id_of[m], up_i, shape_i, r_i, orad_i, old,
+                        nold, nlist, s_mj + tid, s_code + tid, 128, st, matched, shape_ax);
+        s_matched[tid] = matched;
+        cnt = 0;
       } else {
         // the 200-candidate cap (PeriodicBoundaryWorld.cpp:75-78): the nine
         // cells' record counts bound each kind's candidates; where a bound
@@ -174,6 +198,7 @@ __global__ void __launch_bounds__(128, 7) k_candidates_vl(DevWorld w, int par) {
           tot2 += kind == CAND_BOTTOM ? cc : 0;
         }
         if (tot0 + 1 >= kCandidateCap || tot1 + 1 >= kCandidateCap || tot2 + 1 >= kCandidateCap) {
+          const int id_i = w.id_of[m];
           int c0 = 0, c1 = 0, c2 = 0;
           for (int k = 0; k < 9; ++k) {
             int kind;
@@ -186,96 +211,156 @@ __global__ void __launch_bounds__(128, 7) k_candidates_vl(DevWorld w, int par) {
             }
           }
         }
-        // the first four old partners in registers (the usual case); the
-        // others are read where they are
-        int op[4];
-#pragma unroll
-        for (int z = 0; z < 4; ++z) op[z] = z < nold ? old.partner[(size_t)z * n + m] : -1;
-        // the list in groups of kVlGroup entries: the group's entries,
-        // positions and screening radii are loaded together (all in flight at
-        // once), then tested one by one as before
-        for (int v0 = 0; v0 < cnt; v0 += kVlGroup) {
-          int eg[kVlGroup];
-          double2 pg[kVlGroup];
-          double sg[kVlGroup];
-#pragma unroll
-          for (int u = 0; u < kVlGroup; ++u)
-            eg[u] = v0 + u < cnt ? w.vl[(size_t)(v0 + u) * n + m] : 0;
-#pragma unroll
-          for (int u = 0; u < kVlGroup; ++u) {
-            const bool in = v0 + u < cnt;
-            pg[u] = in ? w.pos[eg[u] >> 2] : make_double2(0.0, 0.0);
-            sg[u] = (in && LAW != LAW_ANY) ? w.screen_r[eg[u] >> 2] : 0.0;
-          }
-#pragma unroll
-          for (int u = 0; u < kVlGroup; ++u) {
-          if (v0 + u >= cnt) break;
-          const int e = eg[u];
-          const int mj = e >> 2, kind = e & 3;
-          const double2 pj = pg[u];
-          vec2<double> off, ovel;
-          image_offset(ws, kind, pi, pj, off, ovel);
-          bool pass;
-          if (LAW == LAW_ANY)
-            pass = coarse_pass<LAW>(shape_i, w.shape[mj], r_i, w.rad[mj], orad_i, w.orad[mj], pi,
-                                    pj, off);
-          else
-            pass = coarse_pass<LAW>(0, 0, r_i, sg[u], orad_i, sg[u], pi, pj, off);
-          if (!pass) continue;
-          int cls = CL_REGULAR;
-          if (centre_line_screen<LAW>(w)) {
-            cls = centre_line_class((float)((pj.x + off.x) - pi.x), (float)((pj.y + off.y) - pi.y),
-                                    shape_ax, axis_shape(w, mj));
-            if (cls == CL_SEPARATED) continue;
-          }
-          if (nlist >= K) {
-            st |= ST_CAPACITY;
-            continue;
-          }
-          const int id_j = w.id_of[mj];
-          int oslot = kNoOldSlot;
-#pragma unroll
-          for (int z = 0; z < 4; ++z)
-            if (op[z] == id_j) oslot = z;
-          for (int z = 4; z < nold; ++z)
-            if (old.partner[(size_t)z * n + m] == id_j) oslot = z;
-          // a pair that passed a distance test lies within one cell size,
-          // so it is a candidate of the 3x3 scan (LAW_ANY's other pairs pass
-          // without one and take the cell test below)
-          const bool near = LAW != LAW_ANY ||
-                            (shape_i == w.shape[mj] &&
-                             (shape_i == SHAPE_CIRCLE || shape_i == SHAPE_ELLIPSE));
-          if (oslot != kNoOldSlot && near) matched |= 1u << oslot;
-          list_mj[nlist] = mj;
-          list_code[nlist] = kind | (nlist << 8) | (oslot << 16) |
-                             (LAW == LAW_CLOSEST && cls == CL_DEEP ? kDeepFlag : 0);
-          ++nlist;
-          }
-        }
-      }
-      // old partners among the candidates
-      seen = matched;
-      for (int z = 0; z < nold; ++z) {
-        if (matched & (1u << z)) continue;
-        const int p = old.partner[(size_t)z * n + m];
-        if (p < 0) continue;
-        const int mj = w.mpos[p];
-        if (w.setting[mj] & SKIP_CONTACT_DETECTION) continue;
-        if (w.up[mj] == up_i) continue;
-        const int cr = w.pcell[mj], cg = w.gcell[mj];
-        bool hit = false;
-#pragma unroll
-        for (int k = 0; k < 9; ++k) {
-          int kind;
-          const int c = neighbour_cell(G, w.kind, ix, iy, k / 3 - 1, k % 3 - 1, kind);
-          hit |= c == cr || c == cg;
-        }
-        if (hit) seen |= 1u << z;
+        if (nold > 0) op0 = old.partner[m];
+        if (nold > 1) op1 = old.partner[(size_t)n + m];
+        if (nold > 2) op2 = old.partner[(size_t)2 * n + m];
+        if (nold > 3) op3 = old.partner[(size_t)3 * n + m];
       }
     }
-    cur.count[m] = carry_over(w, old, cur, m, nold, seen, nlist, st);
   }
-  write_pairs(w, m, nlist, list_mj, list_code);
+  __syncwarp();
+  // the warp's list entries, flattened: lane o owns entries [excl, incl)
+  int incl = cnt;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int v = __shfl_up_sync(full, incl, o);
+    if (lane >= o) incl += v;
+  }
+  const int excl = incl - cnt;
+  const int total = __shfl_sync(full, incl, 31);
+  for (int r0 = 0; r0 < total; r0 += 32) {
+    const int e = r0 + lane;
+    const bool act = e < total;
+    // the owner lane: the number of lanes whose range ends at or before e
+    int o = 0;
+#pragma unroll
+    for (int step = 16; step >= 1; step >>= 1)
+      if (__shfl_sync(full, incl, o + step - 1) <= e) o += step;
+    const int o_excl = __shfl_sync(full, excl, o);
+    const int mo = __shfl_sync(full, m, o);
+    const double pix = __shfl_sync(full, pi.x, o), piy = __shfl_sync(full, pi.y, o);
+    const double ro = __shfl_sync(full, r_i, o), orado = __shfl_sync(full, orad_i, o);
+    const int shape_o = (LAW == LAW_ANY) ? __shfl_sync(full, shape_i, o) : 0;
+    AxisShape ax_o{0.0f, 0.0f, 0.0f, 0.0f};
+    if (centre_line_screen<LAW>(w)) {
+      ax_o.c = __shfl_sync(full, shape_ax.c, o);
+      ax_o.s = __shfl_sync(full, shape_ax.s, o);
+      ax_o.a = __shfl_sync(full, shape_ax.a, o);
+      ax_o.b = __shfl_sync(full, shape_ax.b, o);
+    }
+    const int q0 = __shfl_sync(full, op0, o), q1 = __shfl_sync(full, op1, o);
+    const int q2 = __shfl_sync(full, op2, o), q3 = __shfl_sync(full, op3, o);
+    const int nold_o = __shfl_sync(full, nold, o);
+    const int nl = __shfl_sync(full, nlist, o);
+    bool keep = false;
+    int mj = 0, code = 0, oslot = kNoOldSlot;
+    bool near = true;
+    if (act) {
+      const WorldScalars& wo = w.ws[sys_at(w, mo)];
+      const int ent = w.vl[(size_t)(e - o_excl) * n + mo];
+      mj = ent >> 2;
+      const int kind = ent & 3;
+      const double2 pio = make_double2(pix, piy);
+      const double2 pj = w.pos[mj];
+      vec2<double> off, ovel;
+      image_offset(wo, kind, pio, pj, off, ovel);
+      bool pass;
+      if (LAW == LAW_ANY) {
+        pass = coarse_pass<LAW>(shape_o, w.shape[mj], ro, w.rad[mj], orado, w.orad[mj], pio, pj, off);
+      } else {
+        const double sj = w.screen_r[mj];
+        pass = coarse_pass<LAW>(0, 0, ro, sj, orado, sj, pio, pj, off);
+      }
+      int cls = CL_REGULAR;
+      if (pass && centre_line_screen<LAW>(w)) {
+        cls = centre_line_class((float)((pj.x + off.x) - pio.x), (float)((pj.y + off.y) - pio.y),
+                                ax_o, axis_shape(w, mj));
+        pass = cls != CL_SEPARATED;
+      }
+      if (pass) {
+        keep = true;
+        const int id_j = w.id_of[mj];
+        if (q0 == id_j) oslot = 0;
+        if (q1 == id_j) oslot = 1;
+        if (q2 == id_j) oslot = 2;
+        if (q3 == id_j) oslot = 3;
+        for (int z = 4; z < nold_o; ++z)
+          if (old.partner[(size_t)z * n + mo] == id_j) oslot = z;
+        // a pair that passed a distance test lies within one cell size, so
+        // it is a candidate of the 3x3 scan (LAW_ANY's other pairs pass
+        // without one and take the cell test of seen_old_slots)
+        if (LAW == LAW_ANY) {
+          const int shape_j = w.shape[mj];
+          near = shape_o == shape_j && (shape_o == SHAPE_CIRCLE || shape_o == SHAPE_ELLIPSE);
+        }
+        code = kind | (oslot << 16) | (LAW == LAW_CLOSEST && cls == CL_DEEP ? kDeepFlag : 0);
+      }
+    }
+    // rank among the owner's kept entries of this round, in list order
+    const unsigned kmask = __ballot_sync(full, keep);
+    if (keep) {
+      const int first = max(o_excl - r0, 0);
+      const unsigned before = ((1u << lane) - 1u) & ~((1u << first) - 1u);
+      const int idx = nl + __popc(kmask & before);
+      if (idx < K) {
+        s_mj[idx * 128 + wbase + o] = mj;
+        s_code[idx * 128 + wbase + o] = code | (idx << 8);
+        if (oslot != kNoOldSlot && near) atomicOr(&s_matched[wbase + o], 1u << oslot);
+      } else {
+        st |= ST_CAPACITY;
+      }
+    }
+    // this lane as owner: its entries of this round are lanes [lo, hi)
+    const int lo = max(excl - r0, 0), hi = min(incl - r0, 32);
+    if (hi > lo) {
+      const unsigned mine = (hi == 32 ? full : ((1u << hi) - 1u)) & ~((1u << lo) - 1u);
+      nlist = min(nlist + __popc(kmask & mine), K);
+    }
+  }
+  __syncwarp();
+  int ndeep = 0;
+  if (valid) {
+    uint32_t seen = 0;
+    if (scan) seen = seen_old_slots(w, old, G, m, ix, iy, up_i, nold, s_matched[tid]);
+    cur.count[m] = carry_over(w, old, cur, m, nold, seen, nlist, st);
+    for (int s = 0; s < nlist; ++s) ndeep += (s_code[s * 128 + tid] & kDeepFlag) ? 1 : 0;
+  }
+  int at, dk;
+  reserve_pairs(w, nlist, ndeep, at, dk);
+  // the warp's pairs take consecutive entries of the pair list from its lane
+  // 0's, in owner order, and its deep pairs consecutive deep-list entries
+  int pincl = nlist;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int v = __shfl_up_sync(full, pincl, o);
+    if (lane >= o) pincl += v;
+  }
+  const int pexcl = pincl - nlist;
+  const int ptotal = __shfl_sync(full, pincl, 31);
+  const int wat = __shfl_sync(full, at, 0), wdk = __shfl_sync(full, dk, 0);
+  int dcount = 0;
+  for (int r0 = 0; r0 < ptotal; r0 += 32) {
+    const int i = r0 + lane;
+    const bool act = i < ptotal;
+    int o = 0;
+#pragma unroll
+    for (int step = 16; step >= 1; step >>= 1)
+      if (__shfl_sync(full, pincl, o + step - 1) <= i) o += step;
+    const int s = i - __shfl_sync(full, pexcl, o);
+    const int mo = __shfl_sync(full, m, o);
+    int mj = 0, c = 0;
+    if (act) {
+      mj = s_mj[s * 128 + wbase + o];
+      c = s_code[s * 128 + wbase + o];
+    }
+    const bool deep = act && (c & kDeepFlag);
+    const unsigned dmask = __ballot_sync(full, deep);
+    if (act) {
+      w.pairs[wat + i] = PairEntry{mo, mj, c & ~kDeepFlag, deep ? 1 : 0};
+      if (deep) w.deep[wdk + dcount + __popc(dmask & ((1u << lane) - 1u))] = wat + i;
+    }
+    dcount += __popc(dmask);
+  }
   raise(w.status, st);
 }
 
