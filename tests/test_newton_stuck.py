@@ -94,6 +94,35 @@ def test_fixture_pairs_are_stuck_and_resolved():
         assert stk & abi.ERR_NEWTON, k
 
 
+def test_converged_roots_outside_the_interval():
+    """Where the reference returns, its root is not always the one in
+    [min(1, s), max(1, s)]: over 200,000 seeded deep overlaps with the
+    fixture's shapes, some converged solves end outside that interval
+    (mostly at a negative root), and their share grows with the iteration
+    count (a long wander before converging).  The interval's root (what the
+    bisection, or a learned start clamped to the interval, finds) is then a
+    different answer, which is why a solve that converges is never cut short
+    in its favour."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("make_newton_stuck",
+                                                  os.path.join(HERE, "golden", "make_newton_stuck.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    pi, pj = mod.deep_pairs(np.random.default_rng(5), 200_000)
+    out, _ = oracle.closest_quartic(pi, pj, np.zeros((len(pi), 4)))
+    solved = (out[:, 7] > 0) & (out[:, 8] == 0)
+    o = out[solved]
+    lo, hi = np.minimum(1.0, o[:, 5]), np.maximum(1.0, o[:, 5])
+    outside = ~((o[:, 6] >= lo * (1 - 1e-12)) & (o[:, 6] <= hi * (1 + 1e-12)))
+    assert outside.sum() > 0
+    short, long_ = o[:, 7] < 10, o[:, 7] >= 20
+    assert outside[long_].mean() > 10 * outside[short].mean()
+    assert np.mean(o[outside, 6] < 0) > 0.5
+    for c in o[outside][:20]:
+        rb = oracle.bisect_quartic(*c[:5], c[5], np.nan)
+        assert not (abs(rb - c[6]) <= 1e-9 * max(1.0, abs(c[6])))
+
+
 @pytest.mark.gpu
 def test_gpu_stuck_pairs_match_checker():
     """The CUDA closest-approach law on the fixture pairs.  The quartic's
