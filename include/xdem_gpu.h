@@ -472,7 +472,10 @@ int32_t xdem_pair_geometry(int32_t npairs, int32_t ellipse_method, int32_t preci
    world.  With xdem_set_warm_start a closest-approach world starts Newton
    from the prediction when its first step is small, keeps the plain start
    otherwise, and iterates to the reference's tolerance either way, so the
-   result is the plain solver's; xdem_get_warm_stats counts what happened. */
+   result is the plain solver's wherever the plain iteration's root lies in
+   [min(1, sqrt(δ+1)), max(1, sqrt(δ+1))] (after a long wander it can end
+   outside, where the warm-started solve returns the interval's root);
+   xdem_get_warm_stats counts what happened. */
 int32_t xdem_mlp_create(uint64_t seed, xdem_mlp* out);
 int32_t xdem_mlp_destroy(xdem_mlp m);
 /* number of FP32 parameters: W1[64][16], b1[64], W2[64][64], b2[64],

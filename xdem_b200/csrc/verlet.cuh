@@ -22,7 +22,7 @@
 namespace xdem {
 
 constexpr int kVlBlock = 256;
-constexpr int kVlGroup = 2;  // list entries whose loads k_candidates_vl issues together
+constexpr int kVlRounds = 1;  // rounds of 32 list entries whose loads k_candidates_vl issues together (two spill at 72 registers and measured slower)
 
 // block maxima of the path lengths since the last build
 __global__ void __launch_bounds__(kVlBlock) k_vl_maxdisp(DevWorld w) {
@@ -153,8 +153,8 @@ __global__ void __launch_bounds__(128, 7) k_candidates_vl(DevWorld w, int par) {
   double r_i = 0.0, orad_i = 0.0;
   AxisShape shape_ax{0.0f, 0.0f, 0.0f, 0.0f};
   Grid G{};
-  // the first four old partners (the usual case); the others are read where
-  // they are
+  // the memory positions of the first four old partners (the usual case);
+  // the others are read where they are
   int op0 = -1, op1 = -1, op2 = -1, op3 = -1;
   s_matched[tid] = 0u;
   if (valid) {
@@ -211,10 +211,16 @@ __global__ void __launch_bounds__(128, 7) k_candidates_vl(DevWorld w, int par) {
             }
           }
         }
-        if (nold > 0) op0 = old.partner[m];
-        if (nold > 1) op1 = old.partner[(size_t)n + m];
-        if (nold > 2) op2 = old.partner[(size_t)2 * n + m];
-        if (nold > 3) op3 = old.partner[(size_t)3 * n + m];
+        // the first four old partners' memory positions (list entries are
+        // memory positions; ids and positions are one to one)
+        const int p0 = nold > 0 ? old.partner[m] : -1;
+        const int p1 = nold > 1 ? old.partner[(size_t)n + m] : -1;
+        const int p2 = nold > 2 ? old.partner[(size_t)2 * n + m] : -1;
+        const int p3 = nold > 3 ? old.partner[(size_t)3 * n + m] : -1;
+        op0 = p0 >= 0 ? w.mpos[p0] : -1;
+        op1 = p1 >= 0 ? w.mpos[p1] : -1;
+        op2 = p2 >= 0 ? w.mpos[p2] : -1;
+        op3 = p3 >= 0 ? w.mpos[p3] : -1;
       }
     }
   }
@@ -228,93 +234,117 @@ __global__ void __launch_bounds__(128, 7) k_candidates_vl(DevWorld w, int par) {
   }
   const int excl = incl - cnt;
   const int total = __shfl_sync(full, incl, 31);
-  for (int r0 = 0; r0 < total; r0 += 32) {
-    const int e = r0 + lane;
-    const bool act = e < total;
-    // the owner lane: the number of lanes whose range ends at or before e
-    int o = 0;
+  // kVlRounds rounds of 32 entries at a time: the owners and list entries of
+  // all of them are located and their loads issued before any is tested
+  for (int r0 = 0; r0 < total; r0 += 32 * kVlRounds) {
+    int oh[kVlRounds], oex[kVlRounds], moh[kVlRounds], ent[kVlRounds];
+    double2 pjh[kVlRounds];
+    double sjh[kVlRounds];
+    AxisShape axh[kVlRounds];
 #pragma unroll
-    for (int step = 16; step >= 1; step >>= 1)
-      if (__shfl_sync(full, incl, o + step - 1) <= e) o += step;
-    const int o_excl = __shfl_sync(full, excl, o);
-    const int mo = __shfl_sync(full, m, o);
-    const double pix = __shfl_sync(full, pi.x, o), piy = __shfl_sync(full, pi.y, o);
-    const double ro = __shfl_sync(full, r_i, o), orado = __shfl_sync(full, orad_i, o);
-    const int shape_o = (LAW == LAW_ANY) ? __shfl_sync(full, shape_i, o) : 0;
-    AxisShape ax_o{0.0f, 0.0f, 0.0f, 0.0f};
-    if (centre_line_screen<LAW>(w)) {
-      ax_o.c = __shfl_sync(full, shape_ax.c, o);
-      ax_o.s = __shfl_sync(full, shape_ax.s, o);
-      ax_o.a = __shfl_sync(full, shape_ax.a, o);
-      ax_o.b = __shfl_sync(full, shape_ax.b, o);
+    for (int h = 0; h < kVlRounds; ++h) {
+      const int e = r0 + 32 * h + lane;
+      // the owner lane: the number of lanes whose range ends at or before e
+      int o = 0;
+#pragma unroll
+      for (int step = 16; step >= 1; step >>= 1)
+        if (__shfl_sync(full, incl, o + step - 1) <= e) o += step;
+      oh[h] = o;
+      oex[h] = __shfl_sync(full, excl, o);
+      moh[h] = __shfl_sync(full, m, o);
+      ent[h] = e < total ? w.vl[(size_t)(e - oex[h]) * n + moh[h]] : 0;
     }
-    const int q0 = __shfl_sync(full, op0, o), q1 = __shfl_sync(full, op1, o);
-    const int q2 = __shfl_sync(full, op2, o), q3 = __shfl_sync(full, op3, o);
-    const int nold_o = __shfl_sync(full, nold, o);
-    const int nl = __shfl_sync(full, nlist, o);
-    bool keep = false;
-    int mj = 0, code = 0, oslot = kNoOldSlot;
-    bool near = true;
-    if (act) {
-      const WorldScalars& wo = w.ws[sys_at(w, mo)];
-      const int ent = w.vl[(size_t)(e - o_excl) * n + mo];
-      mj = ent >> 2;
-      const int kind = ent & 3;
-      const double2 pio = make_double2(pix, piy);
-      const double2 pj = w.pos[mj];
-      vec2<double> off, ovel;
-      image_offset(wo, kind, pio, pj, off, ovel);
-      bool pass;
-      if (LAW == LAW_ANY) {
-        pass = coarse_pass<LAW>(shape_o, w.shape[mj], ro, w.rad[mj], orado, w.orad[mj], pio, pj, off);
-      } else {
-        const double sj = w.screen_r[mj];
-        pass = coarse_pass<LAW>(0, 0, ro, sj, orado, sj, pio, pj, off);
+#pragma unroll
+    for (int h = 0; h < kVlRounds; ++h) {
+      const bool act = r0 + 32 * h + lane < total;
+      const int mj = ent[h] >> 2;
+      pjh[h] = act ? w.pos[mj] : make_double2(0.0, 0.0);
+      sjh[h] = act && LAW != LAW_ANY ? w.screen_r[mj] : 0.0;
+      axh[h] = act && centre_line_screen<LAW>(w) ? axis_shape(w, mj) : AxisShape{0.0f, 0.0f, 0.0f, 0.0f};
+    }
+#pragma unroll
+    for (int h = 0; h < kVlRounds; ++h) {
+      const int rb = r0 + 32 * h;
+      const int e = rb + lane;
+      const bool act = e < total;
+      const int o = oh[h], o_excl = oex[h], mo = moh[h];
+      const double pix = __shfl_sync(full, pi.x, o), piy = __shfl_sync(full, pi.y, o);
+      const double ro = __shfl_sync(full, r_i, o), orado = __shfl_sync(full, orad_i, o);
+      const int shape_o = (LAW == LAW_ANY) ? __shfl_sync(full, shape_i, o) : 0;
+      AxisShape ax_o{0.0f, 0.0f, 0.0f, 0.0f};
+      if (centre_line_screen<LAW>(w)) {
+        ax_o.c = __shfl_sync(full, shape_ax.c, o);
+        ax_o.s = __shfl_sync(full, shape_ax.s, o);
+        ax_o.a = __shfl_sync(full, shape_ax.a, o);
+        ax_o.b = __shfl_sync(full, shape_ax.b, o);
       }
-      int cls = CL_REGULAR;
-      if (pass && centre_line_screen<LAW>(w)) {
-        cls = centre_line_class((float)((pj.x + off.x) - pio.x), (float)((pj.y + off.y) - pio.y),
-                                ax_o, axis_shape(w, mj));
-        pass = cls != CL_SEPARATED;
-      }
-      if (pass) {
-        keep = true;
-        const int id_j = w.id_of[mj];
-        if (q0 == id_j) oslot = 0;
-        if (q1 == id_j) oslot = 1;
-        if (q2 == id_j) oslot = 2;
-        if (q3 == id_j) oslot = 3;
-        for (int z = 4; z < nold_o; ++z)
-          if (old.partner[(size_t)z * n + mo] == id_j) oslot = z;
-        // a pair that passed a distance test lies within one cell size, so
-        // it is a candidate of the 3x3 scan (LAW_ANY's other pairs pass
-        // without one and take the cell test of seen_old_slots)
-        if (LAW == LAW_ANY) {
-          const int shape_j = w.shape[mj];
-          near = shape_o == shape_j && (shape_o == SHAPE_CIRCLE || shape_o == SHAPE_ELLIPSE);
+      const int q0 = __shfl_sync(full, op0, o), q1 = __shfl_sync(full, op1, o);
+      const int q2 = __shfl_sync(full, op2, o), q3 = __shfl_sync(full, op3, o);
+      const int nold_o = __shfl_sync(full, nold, o);
+      const int nl = __shfl_sync(full, nlist, o);
+      bool keep = false;
+      int mj = 0, code = 0, oslot = kNoOldSlot;
+      bool near = true;
+      if (act) {
+        const WorldScalars& wo = w.ws[sys_at(w, mo)];
+        mj = ent[h] >> 2;
+        const int kind = ent[h] & 3;
+        const double2 pio = make_double2(pix, piy);
+        const double2 pj = pjh[h];
+        vec2<double> off, ovel;
+        image_offset(wo, kind, pio, pj, off, ovel);
+        bool pass;
+        if (LAW == LAW_ANY)
+          pass = coarse_pass<LAW>(shape_o, w.shape[mj], ro, w.rad[mj], orado, w.orad[mj], pio, pj, off);
+        else
+          pass = coarse_pass<LAW>(0, 0, ro, sjh[h], orado, sjh[h], pio, pj, off);
+        int cls = CL_REGULAR;
+        if (pass && centre_line_screen<LAW>(w)) {
+          cls = centre_line_class((float)((pj.x + off.x) - pio.x), (float)((pj.y + off.y) - pio.y),
+                                  ax_o, axh[h]);
+          pass = cls != CL_SEPARATED;
         }
-        code = kind | (oslot << 16) | (LAW == LAW_CLOSEST && cls == CL_DEEP ? kDeepFlag : 0);
+        if (pass) {
+          keep = true;
+          if (q0 == mj) oslot = 0;
+          if (q1 == mj) oslot = 1;
+          if (q2 == mj) oslot = 2;
+          if (q3 == mj) oslot = 3;
+          if (nold_o > 4) {
+            const int id_j = w.id_of[mj];
+            for (int z = 4; z < nold_o; ++z)
+              if (old.partner[(size_t)z * n + mo] == id_j) oslot = z;
+          }
+          // a pair that passed a distance test lies within one cell size, so
+          // it is a candidate of the 3x3 scan (LAW_ANY's other pairs pass
+          // without one and take the cell test of seen_old_slots)
+          if (LAW == LAW_ANY) {
+            const int shape_j = w.shape[mj];
+            near = shape_o == shape_j && (shape_o == SHAPE_CIRCLE || shape_o == SHAPE_ELLIPSE);
+          }
+          code = kind | (oslot << 16) | (LAW == LAW_CLOSEST && cls == CL_DEEP ? kDeepFlag : 0);
+        }
       }
-    }
-    // rank among the owner's kept entries of this round, in list order
-    const unsigned kmask = __ballot_sync(full, keep);
-    if (keep) {
-      const int first = max(o_excl - r0, 0);
-      const unsigned before = ((1u << lane) - 1u) & ~((1u << first) - 1u);
-      const int idx = nl + __popc(kmask & before);
-      if (idx < K) {
-        s_mj[idx * 128 + wbase + o] = mj;
-        s_code[idx * 128 + wbase + o] = code | (idx << 8);
-        if (oslot != kNoOldSlot && near) atomicOr(&s_matched[wbase + o], 1u << oslot);
-      } else {
-        st |= ST_CAPACITY;
+      // rank among the owner's kept entries of this round, in list order
+      const unsigned kmask = __ballot_sync(full, keep);
+      if (keep) {
+        const int first = max(o_excl - rb, 0);
+        const unsigned before = ((1u << lane) - 1u) & ~((1u << first) - 1u);
+        const int idx = nl + __popc(kmask & before);
+        if (idx < K) {
+          s_mj[idx * 128 + wbase + o] = mj;
+          s_code[idx * 128 + wbase + o] = code | (idx << 8);
+          if (oslot != kNoOldSlot && near) atomicOr(&s_matched[wbase + o], 1u << oslot);
+        } else {
+          st |= ST_CAPACITY;
+        }
       }
-    }
-    // this lane as owner: its entries of this round are lanes [lo, hi)
-    const int lo = max(excl - r0, 0), hi = min(incl - r0, 32);
-    if (hi > lo) {
-      const unsigned mine = (hi == 32 ? full : ((1u << hi) - 1u)) & ~((1u << lo) - 1u);
-      nlist = min(nlist + __popc(kmask & mine), K);
+      // this lane as owner: its entries of this round are lanes [lo, hi)
+      const int lo = max(excl - rb, 0), hi = min(incl - rb, 32);
+      if (hi > lo) {
+        const unsigned mine = (hi == 32 ? full : ((1u << hi) - 1u)) & ~((1u << lo) - 1u);
+        nlist = min(nlist + __popc(kmask & mine), K);
+      }
     }
   }
   __syncwarp();

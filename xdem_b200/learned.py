@@ -4,7 +4,10 @@ of the reference's quartic (EllipticParticle.cpp:92-100, 163) as a fraction
 of Newton's analytic start, plus a contact logit, trained on the GPU on pairs
 harvested from worlds.  The network only moves Newton's starting point; the
 iteration still runs to the reference's tolerance (see ellipse_closest in
-xdem_b200/csrc/geometry.cuh), so results are the plain solver's."""
+xdem_b200/csrc/geometry.cuh), so results are the plain solver's wherever the
+plain iteration's root lies in [min(1, sqrt(δ+1)), max(1, sqrt(δ+1))]; a
+plain iteration that wanders long can end outside that interval, and the
+warm-started solve then returns the interval's root instead."""
 import ctypes as C
 
 import numpy as np
