@@ -12,7 +12,7 @@
 
 namespace xdem {
 
-// every contact of the current slot set starts active; each end counts it
+// every contact of the current record set starts active; each end counts it
 // (deg must start at zero)
 __global__ void k_core_init(DevWorld w, int par, int32_t* deg, uint8_t* eact) {
   const int m = blockIdx.x * blockDim.x + threadIdx.x;
@@ -20,14 +20,17 @@ __global__ void k_core_init(DevWorld w, int par, int32_t* deg, uint8_t* eact) {
   const int n = w.n, K = w.K;
   const Slots& cur = w.slots[par];
   const int cnt = min(cur.count[m], K);
+  const int base = cnt > 0 ? cur.base[m] : 0;
   int own = 0;
+  // eact: one flag per (slot, owner), slot-major scratch
   for (int s = 0; s < K; ++s) {
     const size_t e = (size_t)s * n + m;
-    const bool on = s < cnt && cur.partner[e] >= 0;
+    const int partner = s < cnt ? cur.partner[base + s] : -1;
+    const bool on = partner >= 0;
     eact[e] = on ? 1 : 0;
     if (on) {
       own++;
-      atomicAdd(&deg[w.mpos[cur.partner[e]]], 1);
+      atomicAdd(&deg[w.mpos[partner]], 1);
     }
   }
   if (own) atomicAdd(&deg[m], own);
@@ -59,10 +62,11 @@ __global__ void k_core_edges(DevWorld w, int par, int32_t* deg, const uint8_t* l
   const int n = w.n, K = w.K;
   const Slots& cur = w.slots[par];
   const int cnt = min(cur.count[m], K);
+  const int base = cnt > 0 ? cur.base[m] : 0;
   for (int s = 0; s < cnt; ++s) {
     const size_t e = (size_t)s * n + m;
     if (!eact[e]) continue;
-    const int p = w.mpos[cur.partner[e]];
+    const int p = w.mpos[cur.partner[base + s]];
     if (!leave[m] && !leave[p]) continue;
     eact[e] = 0;
     if (!leave[m]) atomicSub(&deg[m], 1);

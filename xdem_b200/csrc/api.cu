@@ -28,7 +28,7 @@ namespace {
 constexpr int kBlock = 128;
 constexpr int kDefaultSlots = 24;
 // default steps between memory-order refreshes; odd, so that a captured
-// chunk (one re-sort + kResortEvery steps) swaps the slot sets an even number
+// chunk (one re-sort + kResortEvery steps) swaps the record sets an even number
 // of times.  On the 1M shear a re-sort costs ~1.5 ms and every 63 steps keeps
 // the neighbour gathers as local as every 31 (0.863 against 0.909 ms/step;
 // 127: 0.859)
@@ -66,7 +66,7 @@ struct xdem_world_s {
   DeviceBuffers particle_bufs;
   WorldScalars* ws = nullptr;
   uint32_t* status = nullptr;
-  int par = 0;            // slot set holding the latest contacts
+  int par = 0;            // record set holding the latest contacts
   int nsys = 1;           // systems (batched worlds: more than one)
   int partial_blocks = 0;
   uint32_t host_status = 0;
@@ -775,6 +775,7 @@ int32_t set_particles_impl(xdem_world_s* w, const xdem_particles* P, const std::
   for (int b = 0; b < 2; ++b) {
     Slots& S = d.slots[b];
     CK(w, B.alloc(&S.count, n));
+    CK(w, B.alloc(&S.base, n));
     CK(w, B.alloc(&S.partner, ks));
     CK(w, B.alloc(&S.n, ks));
     CK(w, B.alloc(&S.s, ks));
@@ -789,6 +790,7 @@ int32_t set_particles_impl(xdem_world_s* w, const xdem_particles* P, const std::
     CK(w, B.alloc(&S.fn, ks));
     CK(w, B.alloc(&S.ft, ks));
     CK(w, cudaMemsetAsync(S.count, 0, sizeof(int32_t) * n, s));
+    CK(w, cudaMemsetAsync(S.base, 0, sizeof(int32_t) * n, s));
   }
   CK(w, B.alloc(&d.incnt, n));
   CK(w, B.alloc(&d.inref, ks));
@@ -1025,17 +1027,18 @@ int32_t xdem_batch_count_contacts(xdem_world w, int64_t* counts) {
   if (!w || !counts || w->dw.n <= 0) return XDEM_ERR_ARGUMENT;
   const int n = w->dw.n, K = w->dw.K;
   std::vector<WorldScalars> all(w->nsys);
-  std::vector<int32_t> cnt(n), partner((size_t)K * n);
+  std::vector<int32_t> cnt(n), base(n), partner((size_t)K * n);
   CK(w, cudaMemcpyAsync(all.data(), w->ws, sizeof(WorldScalars) * w->nsys, cudaMemcpyDeviceToHost,
                         w->stream));
   CK(w, download(cnt.data(), w->dw.slots[w->par].count, n, w->stream));
+  CK(w, download(base.data(), w->dw.slots[w->par].base, n, w->stream));
   CK(w, download(partner.data(), w->dw.slots[w->par].partner, (size_t)K * n, w->stream));
   CK(w, cudaStreamSynchronize(w->stream));
   // a system's particles keep its memory range [first, first + count)
   for (int k = 0; k < w->nsys; ++k) {
     int64_t t = 0;
     for (int m = all[k].first; m < all[k].first + all[k].count; ++m)
-      for (int s = 0; s < std::min(cnt[m], K); ++s) t += partner[(size_t)s * n + m] >= 0;
+      for (int s = 0; s < std::min(cnt[m], K); ++s) t += partner[(size_t)base[m] + s] >= 0;
     counts[k] = t;
   }
   return XDEM_OK;
@@ -1092,21 +1095,28 @@ int32_t xdem_set_contacts(xdem_world w, const xdem_contacts* C) {
   std::vector<int32_t> mpos(n);
   CK(w, download(mpos.data(), w->dw.mpos, n, w->stream));
   CK(w, cudaStreamSynchronize(w->stream));
-  std::vector<int32_t> cnt(n, 0), partner(ks, 0);
+  std::vector<int32_t> cnt(n, 0), base(n, 0), fill(n, 0), partner(ks, 0);
   std::vector<double2> nn(ks), sh(ks), f(ks), b(ks), cp(ks), bv1(ks), bv2(ks), fn(ks), ft(ks);
   std::vector<double> damp(ks), t1(ks), t2(ks);
   uint32_t st = 0;
+  // records per owner (the first K in input order), then each owner's
+  // consecutive records in memory order
   for (int64_t k = 0; k < C->count; ++k) {
     int i = C->id_i[k], j = C->id_j[k];
     if (i < 0 || i >= n || j < 0 || j >= n || i >= j) return XDEM_ERR_ARGUMENT;
     int m = mpos[i];
-    int s = cnt[m];
-    if (s >= K) {
+    if (cnt[m] >= K) {
       st |= XDEM_ERR_CAPACITY;
       continue;
     }
     cnt[m]++;
-    size_t ci = (size_t)s * n + m;
+  }
+  for (int m = 1; m < n; ++m) base[m] = base[m - 1] + cnt[m - 1];
+  for (int64_t k = 0; k < C->count; ++k) {
+    int i = C->id_i[k], j = C->id_j[k];
+    int m = mpos[i];
+    if (fill[m] >= cnt[m]) continue;
+    size_t ci = (size_t)base[m] + fill[m]++;
     partner[ci] = j;
     nn[ci] = make_double2(C->normal_x[k], C->normal_y[k]);
     sh[ci] = make_double2(C->shear_x[k], C->shear_y[k]);
@@ -1131,16 +1141,17 @@ int32_t xdem_set_contacts(xdem_world w, const xdem_contacts* C) {
   std::vector<uint64_t> inref(ks, 0);
   for (int m = 0; m < n; ++m)
     for (int s = 0; s < cnt[m]; ++s) {
-      int mj = mpos[partner[(size_t)s * n + m]];
+      const size_t ci = (size_t)base[m] + s;
+      int mj = mpos[partner[ci]];
       if (inc[mj] < K)
-        inref[(size_t)inc[mj] * n + mj] =
-            ((uint64_t)(uint32_t)id_at[m] << 32) | (uint32_t)((uint32_t)m * K + s);
+        inref[(size_t)inc[mj] * n + mj] = ((uint64_t)(uint32_t)id_at[m] << 32) | (uint32_t)ci;
       else st |= XDEM_ERR_CAPACITY;
       inc[mj]++;
     }
   const Slots& S = w->dw.slots[w->par];
   cudaStream_t q = w->stream;
   CK(w, upload(S.count, cnt.data(), n, q));
+  CK(w, upload(S.base, base.data(), n, q));
   CK(w, upload(S.partner, partner.data(), ks, q));
   CK(w, upload(S.n, nn.data(), ks, q));
   CK(w, upload(S.s, sh.data(), ks, q));
@@ -1167,15 +1178,16 @@ int32_t xdem_get_contacts(xdem_world w, xdem_contacts* C) {
   const size_t ks = (size_t)K * n;
   const Slots& S = w->dw.slots[w->par];
   cudaStream_t q = w->stream;
-  std::vector<int32_t> cnt(n), partner(ks), id_of(n), mpos(n);
+  std::vector<int32_t> cnt(n), base(n), partner(ks), id_of(n), mpos(n);
   CK(w, download(cnt.data(), S.count, n, q));
+  CK(w, download(base.data(), S.base, n, q));
   CK(w, download(partner.data(), S.partner, ks, q));
   CK(w, download(id_of.data(), w->dw.id_of, n, q));
   CK(w, download(mpos.data(), w->dw.mpos, n, q));
   CK(w, cudaStreamSynchronize(q));
   int64_t total = 0;
   for (int m = 0; m < n; ++m)
-    for (int s = 0; s < std::min(cnt[m], K); ++s) total += partner[(size_t)s * n + m] >= 0;
+    for (int s = 0; s < std::min(cnt[m], K); ++s) total += partner[(size_t)base[m] + s] >= 0;
   C->count = total;
   if (C->capacity < total) return XDEM_ERR_CAPACITY;
   std::vector<double2> nn(ks), sh(ks), b(ks), cp(ks), bv1(ks), bv2(ks), fn(ks), ft(ks);
@@ -1199,10 +1211,10 @@ int32_t xdem_get_contacts(xdem_world w, xdem_contacts* C) {
     const int c = std::min(cnt[m], K);
     order.clear();
     for (int s = 0; s < c; ++s)
-      if (partner[(size_t)s * n + m] >= 0) order.push_back({partner[(size_t)s * n + m], s});
+      if (partner[(size_t)base[m] + s] >= 0) order.push_back({partner[(size_t)base[m] + s], s});
     std::sort(order.begin(), order.end());
     for (auto& o : order) {
-      size_t ci = (size_t)o.second * n + m;
+      size_t ci = (size_t)base[m] + o.second;
       C->id_i[k] = i;
       C->id_j[k] = o.first;
       C->normal_x[k] = nn[ci].x;
@@ -1250,13 +1262,14 @@ int32_t xdem_get_force_and_torque(xdem_world w, double* fx, double* fy, double* 
 int32_t xdem_count_contacts(xdem_world w, int64_t* out) {
   if (!w || !out || w->dw.n <= 0) return XDEM_ERR_ARGUMENT;
   const int n = w->dw.n, K = w->dw.K;
-  std::vector<int32_t> cnt(n), partner((size_t)K * n);
+  std::vector<int32_t> cnt(n), base(n), partner((size_t)K * n);
   CK(w, download(cnt.data(), w->dw.slots[w->par].count, n, w->stream));
+  CK(w, download(base.data(), w->dw.slots[w->par].base, n, w->stream));
   CK(w, download(partner.data(), w->dw.slots[w->par].partner, (size_t)K * n, w->stream));
   CK(w, cudaStreamSynchronize(w->stream));
   int64_t t = 0;
   for (int m = 0; m < n; ++m)
-    for (int s = 0; s < std::min(cnt[m], K); ++s) t += partner[(size_t)s * n + m] >= 0;
+    for (int s = 0; s < std::min(cnt[m], K); ++s) t += partner[(size_t)base[m] + s] >= 0;
   *out = t;
   return XDEM_OK;
 }
@@ -1885,7 +1898,7 @@ int32_t xdem_set_candidate_lists(xdem_world w, int32_t capacity, double skin_fra
 
 int32_t xdem_set_memory_order_refresh(xdem_world w, int32_t interval) {
   // odd: a captured chunk (one re-sort and `interval` steps) must swap the
-  // slot sets an even number of times
+  // record sets an even number of times
   if (!w || interval < 0 || (interval > 0 && (interval % 2) == 0) || interval > (1 << 20))
     return XDEM_ERR_ARGUMENT;
   w->resort_every = interval;
@@ -2150,7 +2163,7 @@ int32_t xdem_run(xdem_world w, int32_t nsteps, const xdem_control* ctl, int32_t*
       if (graph) cudaGraphDestroy(graph);
       return (int32_t)(cuda_check(w, e) | fetch_status(w));
     }
-    // a chunk swaps the slot sets an even number of times: parity unchanged
+    // a chunk swaps the record sets an even number of times: parity unchanged
     w->par = par0;
     const int reps = body / chunk;
     const int64_t per_chunk = w->launches - launches_before;

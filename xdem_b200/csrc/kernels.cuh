@@ -382,7 +382,7 @@ __global__ void k_scatter(DevWorld w) {
 // LeesEdwardsBoundaryWorld.cpp:128-204), evaluates every candidate with a
 // larger id at its image offset (PeriodicBoundaryWorld.cpp:97-101,
 // LeesEdwardsBoundaryWorld.cpp:233-279), and writes the contacts into its
-// slots of the new slot set:
+// records of the new record set:
 //   - new contact: initial shear overlap and damping constant (BaseParticle.cpp:38-65)
 //   - old contact: shear overlap rotated with the normal (BaseParticle.cpp:67-82)
 //   - candidate not in contact: dropped (BaseParticle.cpp:95)
@@ -505,6 +505,7 @@ __global__ void __launch_bounds__(128) k_collect(DevWorld w, int par) {
   const int n = w.n, K = w.K;
   const Slots& cur = w.slots[par];
   int nown = min(cur.count[p], K);
+  const int base = nown > 0 ? cur.base[p] : 0;
   int ninc = min(w.incnt[p], K);
   double fx = 0.0, fy = 0.0, t = 0.0;
   if (ninc <= 8 && nown <= 8) {
@@ -515,7 +516,7 @@ __global__ void __launch_bounds__(128) k_collect(DevWorld w, int par) {
 #pragma unroll
     for (int a = 0; a < 8; ++a) {
       ki[a] = a < ninc ? w.inref[(size_t)a * n + p] : ~0ull;
-      const int partner = a < nown ? cur.partner[(size_t)a * n + p] : -1;
+      const int partner = a < nown ? cur.partner[base + a] : -1;
       ko[a] = partner >= 0 ? (((uint32_t)partner << 5) | (uint32_t)a) : 0xffffffffu;
     }
     sort8(ki);
@@ -523,8 +524,7 @@ __global__ void __launch_bounds__(128) k_collect(DevWorld w, int par) {
 #pragma unroll
     for (int a = 0; a < 8; ++a) {
       if (a < ninc) {
-        const uint32_t ref = (uint32_t)ki[a];
-        const size_t ci = (size_t)(ref % K) * n + ref / K;
+        const size_t ci = (uint32_t)ki[a];
         const double2 F = cur.f[ci];
         fx += -F.x;
         fy += -F.y;
@@ -535,7 +535,7 @@ __global__ void __launch_bounds__(128) k_collect(DevWorld w, int par) {
 #pragma unroll
     for (int a = 0; a < 8; ++a) {
       if (ko[a] != 0xffffffffu) {
-        const size_t ci = (size_t)(ko[a] & 31u) * n + p;
+        const size_t ci = (size_t)base + (ko[a] & 31u);
         const double2 F = cur.f[ci];
         fx += F.x;
         fy += F.y;
@@ -554,8 +554,7 @@ __global__ void __launch_bounds__(128) k_collect(DevWorld w, int par) {
     for (int a = 0; a < ninc; ++a) key[a] = w.inref[(size_t)a * n + p];
     isort(key, ninc);
     for (int a = 0; a < ninc; ++a) {
-      uint32_t ref = (uint32_t)key[a];
-      size_t ci = (size_t)(ref % K) * n + ref / K;
+      size_t ci = (uint32_t)key[a];
       double2 F = cur.f[ci];
       fx += -F.x;
       fy += -F.y;
@@ -566,13 +565,13 @@ __global__ void __launch_bounds__(128) k_collect(DevWorld w, int par) {
     uint32_t key[kMaxSlots];  // partner id << 5 | slot; empty slots skipped
     int nk = 0;
     for (int a = 0; a < nown; ++a) {
-      int partner = cur.partner[(size_t)a * n + p];
+      int partner = cur.partner[base + a];
       if (partner >= 0) key[nk++] = ((uint32_t)partner << 5) | a;
     }
     nown = nk;
     isort(key, nown);
     for (int a = 0; a < nown; ++a) {
-      size_t ci = (size_t)(key[a] & 31u) * n + p;
+      size_t ci = (size_t)base + (key[a] & 31u);
       double2 F = cur.f[ci];
       fx += F.x;
       fy += F.y;
@@ -727,16 +726,18 @@ constexpr int kReduceBlock = 256;
 
 __device__ __forceinline__ void own_stress(const DevWorld& w, const Slots& cur, int p, bool sub,
                                            double2 bvo, mat2<double>& s) {
-  const int n = w.n, K = w.K;
+  const int K = w.K;
   int c0 = min(cur.count[p], K), cnt = 0;
+  if (c0 <= 0) return;
+  const int base = cur.base[p];
   uint32_t key[kMaxSlots];
   for (int a = 0; a < c0; ++a) {
-    int partner = cur.partner[(size_t)a * n + p];
+    int partner = cur.partner[base + a];
     if (partner >= 0) key[cnt++] = ((uint32_t)partner << 5) | a;
   }
   isort(key, cnt);
   for (int a = 0; a < cnt; ++a) {
-    size_t ci = (size_t)(key[a] & 31u) * n + p;
+    size_t ci = (size_t)base + (key[a] & 31u);
     double2 F = cur.f[ci], b = cur.b[ci];
     vec2<double> bb = V(b.x, b.y);
     if (sub) bb = bb + V(bvo.x, bvo.y);

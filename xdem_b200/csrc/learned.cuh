@@ -64,7 +64,9 @@ __global__ void __launch_bounds__(128) k_harvest(DevWorld w, MlpDev net, int str
     float tg = 0.0f, ct = 0.0f;
     if (t < n && t % stride == 0) {
       const PairEntry e = w.pairs[t];
-      if (w.shape[e.m] == SHAPE_ELLIPSE && w.shape[e.mj] == SHAPE_ELLIPSE) {
+      // carried-over records are no candidate pairs
+      if (!(e.code & kCarryFlag) && w.shape[e.m] == SHAPE_ELLIPSE &&
+          w.shape[e.mj] == SHAPE_ELLIPSE) {
         const WorldScalars& ws = w.ws[sys_at(w, e.m)];
         const PState a = load_state<false>(w, ws, e.m);
         const PState b = load_state<false>(w, ws, e.mj);

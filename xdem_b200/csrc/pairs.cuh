@@ -9,14 +9,14 @@
 //                   entries survive;
 //   k_pair_forces   one thread per listed pair: image offset, contact geometry,
 //                   history, contact force and torques (BaseParticle.cpp:27-98),
-//                   written to the owner's slot for that pair;
-// both register every contact they write with its partner (an atomic slot in
+//                   written to the pair's record (its pair-list index);
+// both register every contact they write with its partner (an atomic entry in
 // the partner's incoming list) for the partner's force sum.
 // Splitting the light scan from the heavy geometry keeps warps full on the
 // FP64 ellipse solvers.  A candidate rejected by the coarse test is still a
 // candidate: its history is dropped, as the reference erases it
 // (BaseParticle.cpp:95).  A listed pair that turns out not to touch leaves an
-// empty slot (partner -1) that every reader skips.
+// empty record (partner -1) that every reader skips.
 #pragma once
 #include "kernels.cuh"
 
@@ -129,9 +129,6 @@ __device__ __forceinline__ int centre_line_class(float dx, float dy, const AxisS
   return d2 > S * 1.001f ? CL_SEPARATED : (d2 < S * 0.7f ? CL_DEEP : CL_REGULAR);
 }
 
-// flag of a listed pair (bit 24 of its list code, PairEntry::pad in the pair
-// list) that the centre-line screen classed deep
-constexpr int kDeepFlag = 1 << 24;
 
 // the centre-line screen applies to mixed-precision worlds of ellipses under
 // one law
@@ -199,7 +196,8 @@ __device__ __forceinline__ void scan_cells(const DevWorld& w, const WorldScalars
                                            int32_t* list_mj, int32_t* list_code, int stride,
                                            uint32_t& st, uint32_t& matched,
                                            const AxisShape& shape_ax) {
-  const int n = w.n, K = w.K;
+  const int K = w.K;
+  const int ob = nold > 0 ? old.base[m] : 0;  // the owner's first old record
   // the owner relative to its cell's corner, in FP32 (see k_scatter)
   const float rxi = (float)(pi.x - (ws.xmin + ix * G.lx));
   const float ryi = (float)(pi.y - (ws.ymin + iy * G.ly));
@@ -260,7 +258,7 @@ __device__ __forceinline__ void scan_cells(const DevWorld& w, const WorldScalars
       }
       int oslot = kNoOldSlot;
       for (int z = 0; z < nold; ++z)
-        if (old.partner[(size_t)z * n + m] == id_j) oslot = z;
+        if (old.partner[ob + z] == id_j) oslot = z;
       if (oslot != kNoOldSlot) matched |= 1u << oslot;
       list_mj[nlist * stride] = w.cell_mem[q];
       list_code[nlist * stride] =
@@ -270,80 +268,97 @@ __device__ __forceinline__ void scan_cells(const DevWorld& w, const WorldScalars
   }
 }
 
-// Old slots of the owner at m (cell ix, iy) whose partner is a candidate of
-// its 3x3 scan this step: the listed ones (`matched`) and the others whose
-// partner sits in one of the nine cells and passes the candidate filters.
-// Such a pair's history is replaced by the pair kernel or dropped; the other
-// old slots are carried over.
-__device__ __forceinline__ uint32_t seen_old_slots(const DevWorld& w, const Slots& old, const Grid& G,
-                                                   int m, int ix, int iy, int up_i, int nold,
-                                                   uint32_t matched) {
-  uint32_t seen = matched;
+// Old slots of the owner at m (cell ix, iy) to carry over: a valid old
+// contact whose partner is not a candidate of the 3x3 scan this step.  A
+// candidate's history is replaced by the pair kernel or dropped: the listed
+// pairs (`matched`) are candidates, and so is a partner that sits in one of
+// the nine cells and passes the candidate filters.  The history of the other
+// old contacts survives unchanged, as the reference's map entries do.  At
+// most `room` slots are kept (the first ones); more raise ST_CAPACITY.
+__device__ __forceinline__ uint32_t carry_mask(const DevWorld& w, const Slots& old, const Grid& G,
+                                               int m, int ix, int iy, int up_i, int nold,
+                                               uint32_t matched, int room, uint32_t& st) {
+  uint32_t carry = 0;
+  if (nold <= 0) return 0;
+  const int ob = old.base[m];
+  int kept = 0;
   for (int z = 0; z < nold; ++z) {
     if (matched & (1u << z)) continue;
-    const int p = old.partner[(size_t)z * w.n + m];
+    const int p = old.partner[ob + z];
     if (p < 0) continue;
     const int mj = w.mpos[p];
-    if (w.setting[mj] & SKIP_CONTACT_DETECTION) continue;
-    if (w.up[mj] == up_i) continue;
-    const int cr = w.pcell[mj], cg = w.gcell[mj];
-    bool hit = false;
+    if (!(w.setting[mj] & SKIP_CONTACT_DETECTION) && w.up[mj] != up_i) {
+      const int cr = w.pcell[mj], cg = w.gcell[mj];
+      bool hit = false;
 #pragma unroll
-    for (int k = 0; k < 9; ++k) {
-      int kind;
-      const int c = neighbour_cell(G, w.kind, ix, iy, k / 3 - 1, k % 3 - 1, kind);
-      hit |= c == cr || c == cg;
+      for (int k = 0; k < 9; ++k) {
+        int kind;
+        const int c = neighbour_cell(G, w.kind, ix, iy, k / 3 - 1, k % 3 - 1, kind);
+        hit |= c == cr || c == cg;
+      }
+      if (hit) continue;
     }
-    if (hit) seen |= 1u << z;
-  }
-  return seen;
-}
-
-// Registers the contact in the owner's slot (m, slot) with its partner at
-// memory position mj, for the partner's force sum.  The arrival order is
-// free: k_collect orders the references by owner id.
-__device__ __forceinline__ void register_contact(const DevWorld& w, int mj, int owner_id, int m,
-                                                 int slot, uint32_t& st) {
-  const int pos = atomicAdd(&w.incnt[mj], 1);
-  if (pos < w.K)
-    w.inref[(size_t)pos * w.n + mj] = ((uint64_t)(uint32_t)owner_id << 32) |
-                                      ((uint32_t)m * (uint32_t)w.K + (uint32_t)slot);
-  else st |= ST_CAPACITY;
-}
-
-// The history of the owner's old contacts whose pair was not a candidate this
-// step survives unchanged, as the reference's map entries do: copied to the
-// slots after the k listed ones (which only the pair kernels write) and
-// registered with the partner.  Returns the owner's slot count.
-__device__ __forceinline__ int carry_over(const DevWorld& w, const Slots& old, const Slots& cur,
-                                          int m, int nold, uint32_t seen, int k, uint32_t& st) {
-  const int n = w.n, K = w.K;
-  for (int o = 0; o < nold; ++o) {
-    const size_t oi = (size_t)o * n + m;
-    const int partner = old.partner[oi];
-    if (partner < 0 || (seen & (1u << o))) continue;
-    if (k >= K) {
+    if (kept >= room) {
       st |= ST_CAPACITY;
       break;
     }
-    const size_t ci = (size_t)k * n + m;
-    cur.partner[ci] = partner;
-    cur.n[ci] = old.n[oi];
-    cur.s[ci] = old.s[oi];
-    cur.damp[ci] = old.damp[oi];
-    cur.f[ci] = old.f[oi];
-    cur.t1[ci] = old.t1[oi];
-    cur.t2[ci] = old.t2[oi];
-    cur.b[ci] = old.b[oi];
-    cur.cp[ci] = old.cp[oi];
-    cur.bv1[ci] = old.bv1[oi];
-    cur.bv2[ci] = old.bv2[oi];
-    cur.fn[ci] = old.fn[oi];
-    cur.ft[ci] = old.ft[oi];
-    register_contact(w, w.mpos[partner], w.id_of[m], m, k, st);
-    ++k;
+    carry |= 1u << z;
+    ++kept;
   }
-  return k;
+  return carry;
+}
+
+// Old slots to carry over of an owner that takes no part in this step's
+// contact detection (an invalid grid, SKIP_CONTACT_DETECTION): all valid
+// ones, up to K.
+__device__ __forceinline__ uint32_t carry_all(const DevWorld& w, const Slots& old, int m, int nold,
+                                              uint32_t& st) {
+  uint32_t carry = 0;
+  if (nold <= 0) return 0;
+  const int ob = old.base[m];
+  int kept = 0;
+  for (int z = 0; z < nold; ++z) {
+    if (old.partner[ob + z] < 0) continue;
+    if (kept >= w.K) {
+      st |= ST_CAPACITY;
+      break;
+    }
+    carry |= 1u << z;
+    ++kept;
+  }
+  return carry;
+}
+
+// Registers the contact of record r (owner id owner_id) with its partner at
+// memory position mj, for the partner's force sum.  The arrival order is
+// free: k_collect orders the references by owner id.
+__device__ __forceinline__ void register_contact(const DevWorld& w, int mj, int owner_id, int r,
+                                                 uint32_t& st) {
+  const int pos = atomicAdd(&w.incnt[mj], 1);
+  if (pos < w.K)
+    w.inref[(size_t)pos * w.n + mj] = ((uint64_t)(uint32_t)owner_id << 32) | (uint32_t)r;
+  else st |= ST_CAPACITY;
+}
+
+// A carried-over contact: old record ro copied to record r of this step and
+// registered with its partner.
+__device__ __forceinline__ void carry_record(const DevWorld& w, const Slots& old, const Slots& cur,
+                                             int owner_id, int ro, int r, uint32_t& st) {
+  const int partner = old.partner[ro];
+  cur.partner[r] = partner;
+  cur.n[r] = old.n[ro];
+  cur.s[r] = old.s[ro];
+  cur.damp[r] = old.damp[ro];
+  cur.f[r] = old.f[ro];
+  cur.t1[r] = old.t1[ro];
+  cur.t2[r] = old.t2[ro];
+  cur.b[r] = old.b[ro];
+  cur.cp[r] = old.cp[ro];
+  cur.bv1[r] = old.bv1[ro];
+  cur.bv2[r] = old.bv2[ro];
+  cur.fn[r] = old.fn[ro];
+  cur.ft[r] = old.ft[ro];
+  register_contact(w, w.mpos[partner], owner_id, r, st);
 }
 
 // Reserves room for a block's listed pairs (nlist per thread) and deep-pair
@@ -387,21 +402,35 @@ __device__ __forceinline__ void reserve_pairs(const DevWorld& w, int nlist, int 
   deep_at = bb + b - ndeep;
 }
 
-// Writes the owner's listed pairs to the pair list, after reserving their
-// room (reserve_pairs); a pair classed deep (kDeepFlag) carries pad = 1 and
-// its index also goes to the deep-pair list.  Every thread of the block
-// calls.
-__device__ __forceinline__ void write_pairs(const DevWorld& w, int m, int nlist,
-                                            const int32_t* list_mj, const int32_t* list_code) {
+// Writes the owner's records to the pair list, after reserving their room
+// (reserve_pairs): its listed pairs, with last step's record of each (old
+// base + old slot, -1 for a new pair), then the old contacts it carries over
+// (`carry`, a mask of old slots), whose records it copies here.  A pair
+// classed deep (kDeepFlag) also goes to the deep-pair list.  Records the
+// owner's first record and count.  Every thread of the block calls.
+__device__ __forceinline__ void write_pairs(const DevWorld& w, const Slots& old, const Slots& cur,
+                                            int m, bool valid, int nlist, const int32_t* list_mj,
+                                            const int32_t* list_code, uint32_t carry,
+                                            uint32_t& st) {
   int ndeep = 0;
   for (int s = 0; s < nlist; ++s) ndeep += (list_code[s] & kDeepFlag) ? 1 : 0;
+  const int ncarry = __popc(carry);
   int at, k;
-  reserve_pairs(w, nlist, ndeep, at, k);
+  reserve_pairs(w, nlist + ncarry, ndeep, at, k);
+  if (!valid) return;
+  cur.base[m] = at;
+  cur.count[m] = nlist + ncarry;
+  const int ob = old.base[m];  // used only where the owner has old records
   for (int s = 0; s < nlist; ++s) {
-    const int c = list_code[s];
-    const int deep = (c & kDeepFlag) ? 1 : 0;
-    w.pairs[at + s] = PairEntry{m, list_mj[s], c & ~kDeepFlag, deep};
-    if (deep) w.deep[k++] = at + s;
+    const int c = list_code[s], oslot = (c >> 16) & 0xff;
+    w.pairs[at + s] = PairEntry{m, list_mj[s], c, oslot != kNoOldSlot ? ob + oslot : -1};
+    if (c & kDeepFlag) w.deep[k++] = at + s;
+  }
+  int s = nlist;
+  for (uint32_t cm = carry; cm; cm &= cm - 1, ++s) {
+    const int z = __ffs(cm) - 1, ro = ob + z;
+    w.pairs[at + s] = PairEntry{m, w.mpos[old.partner[ro]], kCarryFlag | (s << 8) | (z << 16), ro};
+    carry_record(w, old, cur, w.id_of[m], ro, at + s, st);
   }
 }
 
@@ -409,21 +438,22 @@ __device__ __forceinline__ void write_pairs(const DevWorld& w, int m, int nlist,
 // screening records (cell_scr, cell_up), so a neighbour cell is one
 // contiguous run of 20-byte records; the distance screen runs in FP32 on
 // positions relative to the cell corners, and only candidates within its
-// rounding margin of the threshold take the reference's FP64 test.  Old slots whose partner sits in one of the nine
-// cells (and passes the same filters) are marked seen: such a pair was a
-// candidate, so its history is replaced or dropped; the others are carried
-// over here.
+// rounding margin of the threshold take the reference's FP64 test.  Old
+// slots whose partner sits in one of the nine cells (and passes the same
+// filters) belong to candidates, so their history is replaced or dropped;
+// the others are carried over (carry_mask).
 template <int LAW>
 __global__ void __launch_bounds__(128) k_candidates(DevWorld w, int par) {
   if (stopped(w)) return;
   const int m = blockIdx.x * blockDim.x + threadIdx.x;
   const bool valid = m < w.n;
   const WorldScalars& ws = w.ws[valid ? sys_at(w, m) : 0];
-  const int n = w.n, K = w.K;
+  const int K = w.K;
   const Slots& old = w.slots[par];
   const Slots& cur = w.slots[par ^ 1];
   uint32_t st = 0;
   int nlist = 0;
+  uint32_t carry = 0;
   int32_t list_mj[kMaxSlots];
   int32_t list_code[kMaxSlots];
   if (valid) {
@@ -432,7 +462,6 @@ __global__ void __launch_bounds__(128) k_candidates(DevWorld w, int par) {
     Grid G = grid_of(ws);
     const int id_i = w.id_of[m];
     const int nold = min(old.count[m], K);
-    uint32_t seen = 0;
     if (G.nx >= 3 && G.ny >= 3 && !(w.setting[m] & SKIP_CONTACT_DETECTION)) {
       const double2 pi = w.pos[m];
       const int up_i = w.up[m];
@@ -444,11 +473,12 @@ __global__ void __launch_bounds__(128) k_candidates(DevWorld w, int par) {
       uint32_t matched = 0;
       scan_cells<LAW>(w, ws, G, m, ix, iy, pi, id_i, up_i, shape_i, r_i, orad_i, old, nold, nlist,
                       list_mj, list_code, 1, st, matched, shape_ax);
-      seen = seen_old_slots(w, old, G, m, ix, iy, up_i, nold, matched);
+      carry = carry_mask(w, old, G, m, ix, iy, up_i, nold, matched, K - nlist, st);
+    } else {
+      carry = carry_all(w, old, m, nold, st);
     }
-    cur.count[m] = carry_over(w, old, cur, m, nold, seen, nlist, st);
   }
-  write_pairs(w, m, nlist, list_mj, list_code);
+  write_pairs(w, old, cur, m, valid, nlist, list_mj, list_code, carry, st);
   raise(w.status, st);
 }
 
@@ -481,24 +511,24 @@ struct PairCounters {
 };
 
 // One listed pair t: image offset, contact geometry, history and force,
-// written to the owner's slot.  WARM: a closest-approach pair starts Newton
-// from the learned warm start of its list entry (w.warm, k_mlp_warm).
+// written to record t.  WARM: a closest-approach pair starts Newton from the
+// learned warm start of its list entry (w.warm, k_mlp_warm).
 template <bool FOLD_BG, int LAW, bool WARM>
 __device__ __forceinline__ void pair_forces_fp64(const DevWorld& w, int par, int record, int t,
                                                  PairCounters& pc) {
-  const int n = w.n;
   const Slots& old = w.slots[par];
   const Slots& cur = w.slots[par ^ 1];
   uint32_t& st = pc.st;
   {
     const PairEntry e = w.pairs[t];
+    if (e.code & kCarryFlag) return;  // a carried-over record, copied by the candidate kernel
     const int m = e.m, mj = e.mj;
     const WorldScalars& ws = w.ws[sys_at(w, m)];
     const double dt = ws.dt, kn = ws.kn, kt = ws.kt, mu = ws.mu, factor = ws.factor;
     float2 wp = make_float2(0.0f, 0.0f);
     if (WARM && LAW == LAW_CLOSEST) wp = w.warm[t];
-    const int kind = e.code & 0xff, slot = (e.code >> 8) & 0xff, o = (e.code >> 16) & 0xff;
-    const size_t ci = (size_t)slot * n + m;
+    const int kind = e.code & 0xff;
+    const size_t ci = (size_t)t;
     const BodyRec ba = w.body[m], bb = w.body[mj];
     PState a = body_state<FOLD_BG>(ba, ws);
     PState b = body_state<FOLD_BG>(bb, ws);
@@ -544,13 +574,13 @@ __device__ __forceinline__ void pair_forces_fp64(const DevWorld& w, int par, int
     // BaseParticle::calculateContactForceAndTorque (BaseParticle.cpp:27-98)
     vec2<double> sh, nn = g.n;
     double damp;
-    if (o == kNoOldSlot) {
+    if (e.old < 0) {
       double rvn = dot(g.rv, g.n);
       if (!is_normal(rvn)) sh = g.srv * dt;
       else sh = g.srv * std_min(dt, g.overlap / rvn);
       damp = damping_of(w, factor, ba, bb, m, mj);
     } else {
-      size_t oi = (size_t)o * n + m;
+      size_t oi = (size_t)e.old;
       double2 on = old.n[oi], os = old.s[oi];
       damp = old.damp[oi];
       vec2<double> no = V(on.x, on.y);
@@ -591,7 +621,7 @@ __device__ __forceinline__ void pair_forces_fp64(const DevWorld& w, int par, int
       cur.fn[ci] = make_double2(fn.x, fn.y);
       cur.ft[ci] = make_double2(fs.x, fs.y);
     }
-    register_contact(w, mj, ba.id, m, slot, st);
+    register_contact(w, mj, ba.id, t, st);
   }
 }
 

@@ -1,5 +1,5 @@
 // pairs_mixed.cuh — phase B of updateContacts for the mixed-precision path
-// (XDEM_PRECISION_MIXED).  Same candidate list, slots and history carry-over
+// (XDEM_PRECISION_MIXED).  Same candidate list, records and history carry-over
 // as the FP64 path (pairs.cuh); per listed pair:
 //   geometry   geometry_mixed.cuh (FP32 with the FP64 overlap);
 //   history    the tangential spring stays FP64: its rotation with the normal
@@ -8,7 +8,7 @@
 //              (the same numbers, without the transcendental calls), and the
 //              increment v_t dt is added in FP64;
 //   force      ContactModel_LinearDissipativeFrictioanl (…Frictional.cpp:3-46)
-//              in FP32, written to the FP64 slot arrays.
+//              in FP32, written to the FP64 history records.
 // Closest-approach pairs that need the reference's FP64 construction (see
 // geometry_mixed.cuh) are appended to a fallback list and evaluated by
 // k_pair_fallback_m after the main pass, so that both passes run converged
@@ -24,23 +24,21 @@ __device__ __forceinline__ bool is_normal_f(float x) {
   return a >= 1.17549435e-38f && a <= 3.40282347e38f;
 }
 
-// history, force and torques of one touching pair, written to its slot and
-// registered with the partner
+// history, force and torques of one touching pair, written to its record t
+// (its pair-list index) and registered with the partner
 __device__ __forceinline__ void write_contact_m(const DevWorld& w, const WorldScalars& ws,
-                                                const PairEntry& e, const BodyRec& ba,
+                                                const PairEntry& e, int t, const BodyRec& ba,
                                                 const BodyRec& bb, const PState& a,
                                                 const PState& b, vec2<double> off,
                                                 const GeomM& g, int par, int record,
                                                 uint32_t& st) {
-  const int n = w.n;
   const Slots& old = w.slots[par];
   const Slots& cur = w.slots[par ^ 1];
   const int m = e.m, mj = e.mj;
-  const int slot = (e.code >> 8) & 0xff, o = (e.code >> 16) & 0xff;
-  const size_t ci = (size_t)slot * n + m;
+  const size_t ci = (size_t)t;
   const double dt = ws.dt;
   double sx, sy, damp;
-  if (o == kNoOldSlot) {
+  if (e.old < 0) {
     // new contact (BaseParticle.cpp:38-65)
     const float rvn = g.rv.x * g.n.x + g.rv.y * g.n.y;
     double tt = dt;
@@ -49,7 +47,7 @@ __device__ __forceinline__ void write_contact_m(const DevWorld& w, const WorldSc
     sy = (double)g.srv.y * tt;
     damp = damping_of(w, ws.factor, ba, bb, m, mj);
   } else {
-    const size_t oi = (size_t)o * n + m;
+    const size_t oi = (size_t)e.old;
     const double2 on = old.n[oi], os = old.s[oi];
     damp = old.damp[oi];
     const float nox = (float)on.x, noy = (float)on.y;
@@ -99,7 +97,7 @@ __device__ __forceinline__ void write_contact_m(const DevWorld& w, const WorldSc
     cur.fn[ci] = make_double2((double)fnx, (double)fny);
     cur.ft[ci] = make_double2((double)fsx, (double)fsy);
   }
-  register_contact(w, mj, ba.id, m, slot, st);
+  register_contact(w, mj, ba.id, t, st);
 }
 
 __device__ __forceinline__ void count_solve(uint32_t it, uint32_t& n_solves, uint32_t& n_iters) {
@@ -129,7 +127,7 @@ __device__ __forceinline__ void prefetch_l2(const void* p) {
 }
 
 // Asks the L2 for what the pair at index t will read: its two body records
-// (96 bytes each, two lines) and the owner's old history slot.  Issued while
+// (96 bytes each, two lines) and last step's history record.  Issued while
 // the thread's current pair is computed, so that the next pair's gathers find
 // their data on chip.
 __device__ __forceinline__ void prefetch_pair(const DevWorld& w, int par, int t) {
@@ -140,13 +138,11 @@ __device__ __forceinline__ void prefetch_pair(const DevWorld& w, int par, int t)
   prefetch_l2(ba + sizeof(BodyRec) - 1);
   prefetch_l2(bb);
   prefetch_l2(bb + sizeof(BodyRec) - 1);
-  const int o = (e.code >> 16) & 0xff;
-  if (o != kNoOldSlot) {
+  if (e.old >= 0) {
     const Slots& old = w.slots[par];
-    const size_t oi = (size_t)o * w.n + e.m;
-    prefetch_l2(old.n + oi);
-    prefetch_l2(old.s + oi);
-    prefetch_l2(old.damp + oi);
+    prefetch_l2(old.n + e.old);
+    prefetch_l2(old.s + e.old);
+    prefetch_l2(old.damp + e.old);
   }
 }
 
@@ -155,14 +151,16 @@ template <bool FOLD_BG, int LAW, int PASS>
 __device__ __forceinline__ void pair_forces_m(const DevWorld& w, int par, int record, int t,
                                               uint32_t& st, uint32_t& n_solves, uint32_t& n_iters,
                                               uint32_t& n_capped, int tn = -1) {
-  const int n = w.n;
   const Slots& cur = w.slots[par ^ 1];
   const PairEntry e = w.pairs[t];
-  if (PASS == PASS_REGULAR && e.pad) return;
+  // carried-over records are copied by the candidate kernel; the regular
+  // pass leaves the deep pairs to k_pair_deep_m
+  if (e.code & kCarryFlag) return;
+  if (PASS == PASS_REGULAR && (e.code & kDeepFlag)) return;
   const int m = e.m, mj = e.mj;
   const WorldScalars& ws = w.ws[sys_at(w, m)];
-  const int kind = e.code & 0xff, slot = (e.code >> 8) & 0xff;
-  const size_t ci = (size_t)slot * n + m;
+  const int kind = e.code & 0xff;
+  const size_t ci = (size_t)t;
   const BodyRec ba = w.body[m], bb = w.body[mj];
   if (tn >= 0) prefetch_pair(w, par, tn);
   const PState a = body_state<FOLD_BG>(ba, ws);
@@ -235,7 +233,7 @@ __device__ __forceinline__ void pair_forces_m(const DevWorld& w, int par, int re
     cur.partner[ci] = -1;
     return;
   }
-  write_contact_m(w, ws, e, ba, bb, a, b, off, g, par, record, st);
+  write_contact_m(w, ws, e, t, ba, bb, a, b, off, g, par, record, st);
 }
 
 template <bool FOLD_BG, int LAW, int PASS = PASS_ALL>
@@ -271,17 +269,17 @@ __global__ void __launch_bounds__(128) k_pair_deep_m(DevWorld w, int par, int re
 template <bool FOLD_BG, int LAW, bool WARM = false>
 __global__ void __launch_bounds__(128) k_pair_fallback_m(DevWorld w, int par, int record) {
   if (stopped(w)) return;
-  const int n = w.n;
   const Slots& cur = w.slots[par ^ 1];
   const int nfb = *w.nfallback;
   uint32_t st = 0, n_solves = 0, n_iters = 0, n_capped = 0;
   uint32_t w_off = 0, w_used = 0, w_rej = 0, w_rest = 0, w_right = 0;
   for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < nfb; f += gridDim.x * blockDim.x) {
-    const PairEntry e = w.pairs[w.fallback[f]];
+    const int t = w.fallback[f];
+    const PairEntry e = w.pairs[t];
     const int m = e.m, mj = e.mj;
     const WorldScalars& ws = w.ws[sys_at(w, m)];
-    const int kind = e.code & 0xff, slot = (e.code >> 8) & 0xff;
-    const size_t ci = (size_t)slot * n + m;
+    const int kind = e.code & 0xff;
+    const size_t ci = (size_t)t;
     const BodyRec ba = w.body[m], bb = w.body[mj];
     const PState a = body_state<FOLD_BG>(ba, ws);
     const PState b = body_state<FOLD_BG>(bb, ws);
@@ -310,7 +308,7 @@ __global__ void __launch_bounds__(128) k_pair_fallback_m(DevWorld w, int par, in
     }
     GeomM g;
     geom_to_m(gd, a, g);
-    write_contact_m(w, ws, e, ba, bb, a, b, off, g, par, record, st);
+    write_contact_m(w, ws, e, t, ba, bb, a, b, off, g, par, record, st);
   }
   flush_warp(w, st, n_solves, n_iters, n_capped);
   if (WARM) flush_warm(w, w_off, w_used, w_rej, w_rest, w_right);

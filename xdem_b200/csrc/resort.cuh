@@ -3,9 +3,9 @@
 // Runs after a step's binning: particles are ordered by regular cell, ties by
 // id (k_sort_cells, deterministic), every particle array is moved to its new
 // position through a scratch slab and copied back (array addresses stay fixed,
-// so captured graphs stay valid), the contact history moves into the other
-// slot set (which the next update overwrites anyway), and the cell lists are
-// renumbered.  Nothing the reference computes depends on the memory order.
+// so captured graphs stay valid), each owner's record count and first record
+// move with it into the other record set (the records keep their indices; the
+// next update overwrites them anyway), and the cell lists are renumbered.  Nothing the reference computes depends on the memory order.
 #pragma once
 #include "kernels.cuh"
 
@@ -113,9 +113,10 @@ __global__ void k_copy_back(DevWorld w, PermList L) {
   }
 }
 
-// history of the owner at m -> slot set par^1 at newpos[m]; counts one swap.
-// With an invalid grid the particles did not move and the history is copied
-// in place, so that the slot-set parity stays what the host expects.
+// history of the owner at m -> record set par^1: its count and first record
+// go to newpos[m], its records keep their indices; counts one swap.  With an
+// invalid grid the particles did not move and the history is copied in
+// place, so that the record-set parity stays what the host expects.
 __global__ void k_permute_history(DevWorld w, int par) {
   if (stopped(w)) return;
   int m = blockIdx.x * blockDim.x + threadIdx.x;
@@ -123,27 +124,29 @@ __global__ void k_permute_history(DevWorld w, int par) {
   if (m >= w.n) return;
   const Grid G = grid_of(w.ws[sys_at(w, m)]);
   const bool moved = G.nx >= 3 && G.ny >= 3;
-  const int n = w.n, K = w.K;
+  const int K = w.K;
   const Slots& src = w.slots[par];
   const Slots& dst = w.slots[par ^ 1];
   int t = moved ? w.newpos[m] : m;
   int c = min(src.count[m], K);
+  const int base = c > 0 ? src.base[m] : 0;
   dst.count[t] = c;
+  dst.base[t] = base;
   for (int s = 0; s < c; ++s) {
-    size_t a = (size_t)s * n + m, b = (size_t)s * n + t;
-    dst.partner[b] = src.partner[a];
-    dst.n[b] = src.n[a];
-    dst.s[b] = src.s[a];
-    dst.damp[b] = src.damp[a];
-    dst.f[b] = src.f[a];
-    dst.t1[b] = src.t1[a];
-    dst.t2[b] = src.t2[a];
-    dst.b[b] = src.b[a];
-    dst.cp[b] = src.cp[a];
-    dst.bv1[b] = src.bv1[a];
-    dst.bv2[b] = src.bv2[a];
-    dst.fn[b] = src.fn[a];
-    dst.ft[b] = src.ft[a];
+    const size_t a = (size_t)base + s;
+    dst.partner[a] = src.partner[a];
+    dst.n[a] = src.n[a];
+    dst.s[a] = src.s[a];
+    dst.damp[a] = src.damp[a];
+    dst.f[a] = src.f[a];
+    dst.t1[a] = src.t1[a];
+    dst.t2[a] = src.t2[a];
+    dst.b[a] = src.b[a];
+    dst.cp[a] = src.cp[a];
+    dst.bv1[a] = src.bv1[a];
+    dst.bv2[a] = src.bv2[a];
+    dst.fn[a] = src.fn[a];
+    dst.ft[a] = src.ft[a];
   }
 }
 

@@ -147,7 +147,7 @@ __global__ void __launch_bounds__(128, 7) k_candidates_vl(DevWorld w, int par) {
   const Slots& old = w.slots[par];
   const Slots& cur = w.slots[par ^ 1];
   uint32_t st = 0;
-  int nlist = 0, cnt = 0, nold = 0, up_i = 0, shape_i = 0, ix = 0, iy = 0;
+  int nlist = 0, cnt = 0, nold = 0, ob = 0, up_i = 0, shape_i = 0, ix = 0, iy = 0;
   bool scan = false;
   double2 pi = make_double2(0.0, 0.0);
   double r_i = 0.0, orad_i = 0.0;
@@ -163,6 +163,7 @@ __global__ void __launch_bounds__(128, 7) k_candidates_vl(DevWorld w, int par) {
     shape_ax = owner_axis_shape<LAW>(w, m);
     G = grid_of(ws);
     nold = min(old.count[m], K);
+    ob = nold > 0 ? old.base[m] : 0;  // the owner's first old record
     scan = G.nx >= 3 && G.ny >= 3 && !(w.setting[m] & SKIP_CONTACT_DETECTION);
     if (scan) {
       pi = w.pos[m];
@@ -213,10 +214,10 @@ __global__ void __launch_bounds__(128, 7) k_candidates_vl(DevWorld w, int par) {
         }
         // the first four old partners' memory positions (list entries are
         // memory positions; ids and positions are one to one)
-        const int p0 = nold > 0 ? old.partner[m] : -1;
-        const int p1 = nold > 1 ? old.partner[(size_t)n + m] : -1;
-        const int p2 = nold > 2 ? old.partner[(size_t)2 * n + m] : -1;
-        const int p3 = nold > 3 ? old.partner[(size_t)3 * n + m] : -1;
+        const int p0 = nold > 0 ? old.partner[ob] : -1;
+        const int p1 = nold > 1 ? old.partner[ob + 1] : -1;
+        const int p2 = nold > 2 ? old.partner[ob + 2] : -1;
+        const int p3 = nold > 3 ? old.partner[ob + 3] : -1;
         op0 = p0 >= 0 ? w.mpos[p0] : -1;
         op1 = p1 >= 0 ? w.mpos[p1] : -1;
         op2 = p2 >= 0 ? w.mpos[p2] : -1;
@@ -280,7 +281,7 @@ __global__ void __launch_bounds__(128, 7) k_candidates_vl(DevWorld w, int par) {
       }
       const int q0 = __shfl_sync(full, op0, o), q1 = __shfl_sync(full, op1, o);
       const int q2 = __shfl_sync(full, op2, o), q3 = __shfl_sync(full, op3, o);
-      const int nold_o = __shfl_sync(full, nold, o);
+      const int nold_o = __shfl_sync(full, nold, o), ob_o = __shfl_sync(full, ob, o);
       const int nl = __shfl_sync(full, nlist, o);
       bool keep = false;
       int mj = 0, code = 0, oslot = kNoOldSlot;
@@ -313,11 +314,11 @@ __global__ void __launch_bounds__(128, 7) k_candidates_vl(DevWorld w, int par) {
           if (nold_o > 4) {
             const int id_j = w.id_of[mj];
             for (int z = 4; z < nold_o; ++z)
-              if (old.partner[(size_t)z * n + mo] == id_j) oslot = z;
+              if (old.partner[ob_o + z] == id_j) oslot = z;
           }
           // a pair that passed a distance test lies within one cell size, so
           // it is a candidate of the 3x3 scan (LAW_ANY's other pairs pass
-          // without one and take the cell test of seen_old_slots)
+          // without one and take the cell test of carry_mask)
           if (LAW == LAW_ANY) {
             const int shape_j = w.shape[mj];
             near = shape_o == shape_j && (shape_o == SHAPE_CIRCLE || shape_o == SHAPE_ELLIPSE);
@@ -349,23 +350,29 @@ __global__ void __launch_bounds__(128, 7) k_candidates_vl(DevWorld w, int par) {
   }
   __syncwarp();
   int ndeep = 0;
+  uint32_t carry = 0;
   if (valid) {
-    uint32_t seen = 0;
-    if (scan) seen = seen_old_slots(w, old, G, m, ix, iy, up_i, nold, s_matched[tid]);
-    cur.count[m] = carry_over(w, old, cur, m, nold, seen, nlist, st);
+    carry = scan ? carry_mask(w, old, G, m, ix, iy, up_i, nold, s_matched[tid], K - nlist, st)
+                 : carry_all(w, old, m, nold, st);
     for (int s = 0; s < nlist; ++s) ndeep += (s_code[s * 128 + tid] & kDeepFlag) ? 1 : 0;
   }
+  const int nrec = nlist + __popc(carry);  // the owner's records: listed pairs, then carried
   int at, dk;
-  reserve_pairs(w, nlist, ndeep, at, dk);
-  // the warp's pairs take consecutive entries of the pair list from its lane
-  // 0's, in owner order, and its deep pairs consecutive deep-list entries
-  int pincl = nlist;
+  reserve_pairs(w, nrec, ndeep, at, dk);
+  if (valid) {
+    cur.base[m] = at;
+    cur.count[m] = nrec;
+  }
+  // the warp's records take consecutive entries of the pair list from its
+  // lane 0's, in owner order, and its deep pairs consecutive deep-list
+  // entries
+  int pincl = nrec;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
     const int v = __shfl_up_sync(full, pincl, o);
     if (lane >= o) pincl += v;
   }
-  const int pexcl = pincl - nlist;
+  const int pexcl = pincl - nrec;
   const int ptotal = __shfl_sync(full, pincl, 31);
   const int wat = __shfl_sync(full, at, 0), wdk = __shfl_sync(full, dk, 0);
   int dcount = 0;
@@ -378,16 +385,24 @@ __global__ void __launch_bounds__(128, 7) k_candidates_vl(DevWorld w, int par) {
       if (__shfl_sync(full, pincl, o + step - 1) <= i) o += step;
     const int s = i - __shfl_sync(full, pexcl, o);
     const int mo = __shfl_sync(full, m, o);
-    int mj = 0, c = 0;
-    if (act) {
-      mj = s_mj[s * 128 + wbase + o];
-      c = s_code[s * 128 + wbase + o];
-    }
+    const int nl_o = __shfl_sync(full, nlist, o), ob_o = __shfl_sync(full, ob, o);
+    const uint32_t carry_o = __shfl_sync(full, carry, o);
+    int c = 0;
+    if (act && s < nl_o) c = s_code[s * 128 + wbase + o];
     const bool deep = act && (c & kDeepFlag);
     const unsigned dmask = __ballot_sync(full, deep);
-    if (act) {
-      w.pairs[wat + i] = PairEntry{mo, mj, c & ~kDeepFlag, deep ? 1 : 0};
+    if (act && s < nl_o) {
+      const int oslot = (c >> 16) & 0xff;
+      w.pairs[wat + i] = PairEntry{mo, s_mj[s * 128 + wbase + o], c,
+                                   oslot != kNoOldSlot ? ob_o + oslot : -1};
       if (deep) w.deep[wdk + dcount + __popc(dmask & ((1u << lane) - 1u))] = wat + i;
+    } else if (act) {
+      // the (s - nl_o)-th carried old slot
+      uint32_t cm = carry_o;
+      for (int q = nl_o; q < s; ++q) cm &= cm - 1;
+      const int z = __ffs(cm) - 1, ro = ob_o + z;
+      w.pairs[wat + i] = PairEntry{mo, w.mpos[old.partner[ro]], kCarryFlag | (s << 8) | (z << 16), ro};
+      carry_record(w, old, cur, w.id_of[mo], ro, wat + i, st);
     }
     dcount += __popc(dmask);
   }

@@ -9,11 +9,14 @@
 // orders by id (contact ownership, force-sum order, clump sub-particles) is
 // ordered by id here too, so results do not depend on the memory order.
 //
-// Contact history lives in per-owner slots: slot s of the particle at m is
-// element s*n + m of each slot array (slot-major, so consecutive particles
-// touch consecutive addresses); the owner is the lower id, as in the
-// reference's per-particle maps.  Two slot sets alternate: one holds the
-// previous history while the other receives the new contacts.
+// Contact history lives in records kept in pair-list order: the contacts of
+// the particle at m (the owner is the lower id, as in the reference's
+// per-particle maps) are the `count[m]` consecutive records from `base[m]`,
+// slot s being record base[m] + s.  Each step the candidate kernel reserves
+// the owner's records in the pair list (its listed pairs, then the old
+// contacts it carries over), so the pair kernels read last step's record of
+// a pair and write this step's in pair order.  Two record sets alternate: one
+// holds the previous history while the other receives the new contacts.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -23,8 +26,10 @@ namespace xdem {
 constexpr int kMaxSlots = 32;  // upper bound of history slots per particle
 
 struct Slots {
-  int32_t* count;    // [n] contacts owned by the particle at m
-  int32_t* partner;  // [K*n] partner id j (> owner id)
+  int32_t* count;    // [n] records owned by the particle at m
+  int32_t* base;     // [n] its first record
+  // records [K*n], indexed by record (pair-list) index
+  int32_t* partner;  // partner id j (> owner id), -1 for a listed pair without contact
   double2* n;        // contact normal
   double2* s;        // tangential spring (shear overlap)
   double* damp;      // damping constant, fixed at creation
@@ -84,14 +89,20 @@ struct alignas(32) BodyRec {
 };
 static_assert(sizeof(BodyRec) == 96, "BodyRec is three sectors");
 
-// one pair listed by the candidate scan: owner position, partner position,
-// and packed in `code` the image kind (bits 0-7), the owner's new slot for the
-// pair (bits 8-15) and its slot in the old set, 255 when the pair is new
-// (bits 16-23)
+// one entry of the pair list (and the index of its history record): owner
+// position, partner position, last step's record of the pair (-1 when the
+// pair is new), and packed in `code` the image kind (bits 0-7), the owner's
+// slot (bits 8-15), its slot in the old set, 255 when the pair is new (bits
+// 16-23), and the flags kDeepFlag and kCarryFlag
 struct PairEntry {
-  int32_t m, mj, code, pad;
+  int32_t m, mj, code, old;
 };
 constexpr int kNoOldSlot = 255;
+// a listed pair that the centre-line screen classed deep (mixed precision)
+constexpr int kDeepFlag = 1 << 24;
+// an old contact carried over without a candidate pair: its record is copied
+// by the candidate kernel and the pair kernels skip the entry
+constexpr int kCarryFlag = 1 << 25;
 
 
 // A world holds one system or, batched, nsys independent systems of the same
@@ -163,8 +174,8 @@ struct DevWorld {
   // contacts
   Slots slots[2];
   int32_t* incnt;   // [n] contacts owned by lower ids
-  // [K*n] those contacts: owner id << 32 | owner position*K + slot (the
-  // force sum orders them by owner id without looking it up)
+  // [K*n] those contacts: owner id << 32 | record (the force sum orders them
+  // by owner id without looking it up)
   uint64_t* inref;
   PairEntry* pairs; // [K*n] pairs that passed the candidate scan
   int32_t* npairs;  // number of listed pairs (low half of pair_counts)
