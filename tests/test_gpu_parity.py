@@ -269,6 +269,56 @@ def test_contact_upload_roundtrip():
     _compare_worlds(g, c, ONE_STEP_TOL)
 
 
+def test_history_of_non_candidates_carried_over():
+    """An old contact whose pair is not a candidate any more keeps its history
+    (the reference's map entry survives, BaseParticle.cpp:95 erases only
+    candidates) and its force still enters the force sum.  Contacts of a
+    settled packing plus three entries between particles far apart are
+    uploaded to the GPU world and to the checker; after five steps both hold
+    the same contacts (the three carried over unchanged) and the same state."""
+    p, prm = disc_case(n=300, phi=0.82, seed=12)
+    c = oracle.PortWorld(prm)
+    c.set_particles(p)
+    c.run(20)
+    st = c.get_state()
+    q = dict(p)
+    for k in ("x", "y", "vx", "vy", "rot", "rot_vel"):
+        q[k] = st[k].copy()
+    cont = c.get_contacts()
+    existing = set(zip(cont["id_i"].tolist(), cont["id_j"].tolist()))
+    box = prm.xmax - prm.xmin
+    far = []
+    for i in range(len(q["x"])):
+        for j in range(i + 1, len(q["x"])):
+            dx = abs(q["x"][i] - q["x"][j])
+            dy = abs(q["y"][i] - q["y"][j])
+            dx, dy = min(dx, box - dx), min(dy, (prm.ymax - prm.ymin) - dy)
+            if dx > 0.3 * box and dy > 0.3 * box and (i, j) not in existing:
+                far.append((i, j))
+                break
+        if len(far) == 3:
+            break
+    assert len(far) == 3
+    extra = {k: np.concatenate([v, v[:3]]) for k, v in cont.items()}
+    extra["id_i"][-3:] = [f[0] for f in far]
+    extra["id_j"][-3:] = [f[1] for f in far]
+    g = World(prm)
+    g.set_particles(q)
+    g.set_contacts(extra)
+    c2 = oracle.PortWorld(prm)
+    c2.set_particles(q)
+    c2.set_contacts(extra)
+    g.run(5)
+    c2.run(5)
+    _compare_worlds(g, c2, TRAJ_TOL)
+    gc = g.get_contacts()
+    keys = list(zip(gc["id_i"].tolist(), gc["id_j"].tolist()))
+    for (i, j), k in zip(far, range(len(extra["id_i"]) - 3, len(extra["id_i"]))):
+        at = keys.index((i, j))
+        for f in ("shear_x", "shear_y", "fn_x", "fn_y", "ft_x", "ft_y", "damping"):
+            assert gc[f][at] == extra[f][k], (i, j, f)
+
+
 def test_stop_on_pressure():
     p, prm = disc_case(n=300, phi=0.75, seed=13, kind=abi.WORLD_PERIODIC_CONTROL)
     g, c = _pair(p, prm)

@@ -84,6 +84,7 @@ struct xdem_world_s {
   // (xdem_set_memory_order_refresh)
   int resort_every = kResortEvery;
   int law = LAW_ANY;                // contact-kernel specialisation for the shapes present
+  bool has_clumps = false;          // a clump's time integral reads its sub-particles' sums
   xdem_mlp_s* mlp = nullptr;        // learned warm start of the closest-approach Newton iteration
   PermList perm{};                  // particle arrays moved by a re-sort
   // launch configuration (xdem_set_launch_config / xdem_autotune): blocks per
@@ -156,14 +157,14 @@ cudaError_t download(T* dst, const T* src, size_t count, cudaStream_t s) {
 
 // ---- per-kernel timing ------------------------------------------------------
 enum KernelKind {
-  KK_MODIFY = 0, KK_BIN, KK_SCAN, KK_SCATTER, KK_CANDIDATES, KK_PAIRS, KK_FINISH, KK_COLLECT,
+  KK_MODIFY = 0, KK_BIN, KK_SCAN, KK_SCATTER, KK_CANDIDATES, KK_PAIRS, KK_COLLECT_INTEGRATE, KK_COLLECT,
   KK_INTEGRATE, KK_RATTLERS, KK_STRESS_PARTIAL, KK_STRESS_FINAL, KK_END_OF_STEP, KK_SCALE,
   KK_BACKGROUND, KK_KE, KK_RESORT, KK_STAGE, KK_FALLBACK, KK_WARM, KK_VL_CHECK, KK_VL_BUILD,
   KK_DEEP, KK_COUNT
 };
 const char* const kKindNames[KK_COUNT] = {
     "k_modify_position", "k_bin", "k_scan", "k_scatter", "k_candidates", "k_pair_forces",
-    "k_pairs_done", "k_collect", "k_integrate", "k_rattlers", "k_stress_partial",
+    "k_collect_integrate", "k_collect", "k_integrate", "k_rattlers", "k_stress_partial",
     "k_stress_final", "k_end_of_step", "k_scale_positions", "k_background_velocity",
     "k_kinetic_energy", "k_resort", "k_stage", "k_pair_fallback", "k_mlp_warm", "k_vl_check",
     "k_vl_build", "k_pair_deep"};
@@ -205,13 +206,17 @@ void launch_modify(xdem_world_s* w) {
   LAUNCH(w, KK_MODIFY, k_modify_position<<<blocks_for(n, kBlock), kBlock, 0, w->stream>>>(w->dw));
 }
 
-void launch_find(xdem_world_s* w) {
+// findPossibleContacts' binning; modify: the step's position move first, in
+// the binning kernel
+void launch_find(xdem_world_s* w, bool modify = false) {
   int n = w->dw.n;
-  LAUNCH(w, KK_BIN, k_bin<<<blocks_for(n, kBlock), kBlock, 0, w->stream>>>(w->dw));
+  if (modify)
+    LAUNCH(w, KK_BIN, k_bin<true><<<blocks_for(n, kBlock), kBlock, 0, w->stream>>>(w->dw));
+  else
+    LAUNCH(w, KK_BIN, k_bin<false><<<blocks_for(n, kBlock), kBlock, 0, w->stream>>>(w->dw));
   int cells = w->dw.ncell_total;
   int tiles = std::min(blocks_for(cells, kScanTile), 2 * 148 * 8);
   LAUNCH(w, KK_SCAN, k_scan_tiles<<<tiles, kScanThreads, 0, w->stream>>>(w->dw));
-  LAUNCH(w, KK_SCAN, k_scan_sums<<<1, kScanThreads, 0, w->stream>>>(w->dw));
   LAUNCH(w, KK_SCAN, k_scan_apply<<<tiles, kScanThreads, 0, w->stream>>>(w->dw));
   int nb = std::max(blocks_for(n, kBlock), std::min(blocks_for(cells, kBlock), 1184));
   LAUNCH(w, KK_SCATTER, k_scatter<<<nb, kBlock, 0, w->stream>>>(w->dw));
@@ -221,7 +226,8 @@ void launch_find(xdem_world_s* w) {
 // a programmatic dependent launch: it may start while the kernel before it
 // (which signals with griddepcontrol.launch_dependents) still runs.  The
 // launch after it is an ordinary one and waits for both.
-void launch_dependent(xdem_world_s* w, int blocks, void (*kernel)(DevWorld, int, int), int record) {
+void launch_dependent(xdem_world_s* w, int blocks, void (*kernel)(DevWorld, int, int, int),
+                      int record) {
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
   attr[0].val.programmaticStreamSerializationAllowed = 1;
@@ -232,7 +238,7 @@ void launch_dependent(xdem_world_s* w, int blocks, void (*kernel)(DevWorld, int,
   cfg.stream = w->stream;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  cuda_check(w, cudaLaunchKernelEx(&cfg, kernel, w->dw, w->par, record));
+  cuda_check(w, cudaLaunchKernelEx(&cfg, kernel, w->dw, w->par, record, 0));
   w->launches++;
 }
 
@@ -253,13 +259,14 @@ void launch_update_phases(xdem_world_s* w, int record) {
   if (w->dw.V > 0) {
     const int vb = blocks_for(w->dw.n, kVlBlock);
     LAUNCH(w, KK_VL_CHECK, k_vl_maxdisp<<<vb, kVlBlock, 0, w->stream>>>(w->dw));
-    LAUNCH(w, KK_VL_CHECK, k_vl_check<<<1, 1024, 0, w->stream>>>(w->dw, vb));
     LAUNCH(w, KK_VL_BUILD, k_vl_build<LAW><<<nb, 128, 0, w->stream>>>(w->dw));
     LAUNCH(w, KK_CANDIDATES, k_candidates_vl<LAW><<<nb, 128, candidates_smem(w), w->stream>>>(
                                  w->dw, w->par));
   } else {
     LAUNCH(w, KK_CANDIDATES, k_candidates<LAW><<<nb, 128, 0, w->stream>>>(w->dw, w->par));
   }
+  // the launch that ends the pair phase (finish = 1) also resets the pair
+  // counters for the next update (finish_pairs)
   if (w->prm.precision == XDEM_PRECISION_MIXED && LAW == LAW_CLOSEST && !warm) {
     // The deep pairs first, then the regular pair pass as a programmatic
     // dependent launch: every block of k_pair_deep_m signals at its start, so
@@ -272,36 +279,36 @@ void launch_update_phases(xdem_world_s* w, int record) {
            k_pair_deep_m<FOLD_BG, LAW><<<148 * 2, 128, 0, w->stream>>>(w->dw, w->par, record));
     if (w->prof_on) {
       LAUNCH(w, KK_PAIRS, k_pair_forces_m<FOLD_BG, LAW, PASS_REGULAR><<<pb, 128, 0, w->stream>>>(
-                              w->dw, w->par, record));
+                              w->dw, w->par, record, 0));
     } else {
       launch_dependent(w, pb, k_pair_forces_m<FOLD_BG, LAW, PASS_REGULAR>, record);
     }
     LAUNCH(w, KK_FALLBACK, k_pair_fallback_m<FOLD_BG, LAW><<<148 * 4, 128, 0, w->stream>>>(
-                               w->dw, w->par, record));
+                               w->dw, w->par, record, 1));
   } else if (w->prm.precision == XDEM_PRECISION_MIXED) {
-    LAUNCH(w, KK_PAIRS,
-           k_pair_forces_m<FOLD_BG, LAW><<<pb, 128, 0, w->stream>>>(w->dw, w->par, record));
-    if (LAW == LAW_CLOSEST || LAW == LAW_ANY) {
+    const bool deferred = LAW == LAW_CLOSEST || LAW == LAW_ANY;
+    LAUNCH(w, KK_PAIRS, k_pair_forces_m<FOLD_BG, LAW><<<pb, 128, 0, w->stream>>>(
+                            w->dw, w->par, record, deferred ? 0 : 1));
+    if (deferred) {
       if (warm) {
         LAUNCH(w, KK_WARM, k_mlp_warm<LAW><<<148 * 4, 128, 0, w->stream>>>(
                                w->dw, w->mlp->dev(), w->dw.nfallback, w->dw.fallback));
         LAUNCH(w, KK_FALLBACK, k_pair_fallback_m<FOLD_BG, LAW, true><<<148 * 4, 128, 0, w->stream>>>(
-                                   w->dw, w->par, record));
+                                   w->dw, w->par, record, 1));
       } else {
         LAUNCH(w, KK_FALLBACK, k_pair_fallback_m<FOLD_BG, LAW><<<148 * 4, 128, 0, w->stream>>>(
-                                   w->dw, w->par, record));
+                                   w->dw, w->par, record, 1));
       }
     }
   } else if (warm) {
     LAUNCH(w, KK_WARM,
            k_mlp_warm<LAW><<<148 * 4, 128, 0, w->stream>>>(w->dw, w->mlp->dev(), w->dw.npairs, nullptr));
     LAUNCH(w, KK_PAIRS,
-           k_pair_forces<FOLD_BG, LAW, true><<<pb, 128, 0, w->stream>>>(w->dw, w->par, record));
+           k_pair_forces<FOLD_BG, LAW, true><<<pb, 128, 0, w->stream>>>(w->dw, w->par, record, 1));
   } else {
     LAUNCH(w, KK_PAIRS,
-           k_pair_forces<FOLD_BG, LAW><<<pb, 128, 0, w->stream>>>(w->dw, w->par, record));
+           k_pair_forces<FOLD_BG, LAW><<<pb, 128, 0, w->stream>>>(w->dw, w->par, record, 1));
   }
-  LAUNCH(w, KK_FINISH, k_pairs_done<<<1, 32, 0, w->stream>>>(w->dw));
 }
 
 template <bool FOLD_BG>
@@ -331,6 +338,17 @@ void launch_integrate(xdem_world_s* w, bool fold_bg, int reset) {
     LAUNCH(w, KK_INTEGRATE, k_integrate<true><<<blocks_for(n, kBlock), kBlock, 0, w->stream>>>(w->dw, reset));
   else
     LAUNCH(w, KK_INTEGRATE, k_integrate<false><<<blocks_for(n, kBlock), kBlock, 0, w->stream>>>(w->dw, reset));
+}
+
+// the force sum and the time integral of a world without clumps in one pass
+void launch_collect_integrate(xdem_world_s* w, bool fold_bg, int reset) {
+  int n = w->dw.n;
+  if (fold_bg)
+    LAUNCH(w, KK_COLLECT_INTEGRATE, k_collect_integrate<true><<<blocks_for(n, 128), 128, 0,
+                                                                 w->stream>>>(w->dw, w->par, reset));
+  else
+    LAUNCH(w, KK_COLLECT_INTEGRATE, k_collect_integrate<false><<<blocks_for(n, 128), 128, 0,
+                                                                  w->stream>>>(w->dw, w->par, reset));
 }
 
 void launch_stress(xdem_world_s* w) {
@@ -380,12 +398,15 @@ void enqueue_step(xdem_world_s* w, const xdem_control* ctl, int record, bool res
   bool own = ctl->sequence == XDEM_SEQ_TAKE_TIME_STEP;
   bool le = own && kind == XDEM_WORLD_LEES_EDWARDS;
   if (ctl->scale_rattlers) launch_rattlers(w, 0, ctl->rattler_scale);
-  launch_modify(w);
-  launch_find(w);
+  launch_find(w, true);
   if (resort) launch_resort(w);
   launch_update(w, le, record);
-  launch_collect(w);
-  launch_integrate(w, le, own && kind == XDEM_WORLD_PERIODIC_CONTROL);
+  if (w->has_clumps) {
+    launch_collect(w);
+    launch_integrate(w, le, own && kind == XDEM_WORLD_PERIODIC_CONTROL);
+  } else {
+    launch_collect_integrate(w, le, own && kind == XDEM_WORLD_PERIODIC_CONTROL);
+  }
   if (ctl->reset_rattlers) launch_rattlers(w, 1, 0.0);
   if (ctl->update_stress) launch_stress(w);
   launch_end_of_step(w, ctl->box_law, ctl->p0, ctl->p1, le ? 1 : 0, ctl->stop_on_pressure,
@@ -670,12 +691,14 @@ int32_t set_particles_impl(xdem_world_s* w, const xdem_particles* P, const std::
   for (int k = 0; k < nsys; ++k)  // setVirtualBoundaryMass (PeriodicControlWorld.cpp:58-66)
     w->control_mass[k] = sys_mass[k] / ((double)sys[k].count * 10.0);
   // one contact law for the whole world when every non-clump body has one shape
-  bool any_circle = false, any_ellipse = false, any_segment = false;
+  bool any_circle = false, any_ellipse = false, any_segment = false, any_clump = false;
   for (int i = 0; i < n; ++i) {
     any_circle |= P->shape[i] == XDEM_SHAPE_CIRCLE;
     any_ellipse |= P->shape[i] == XDEM_SHAPE_ELLIPSE;
     any_segment |= P->shape[i] == XDEM_SHAPE_SEGMENT;
+    any_clump |= P->shape[i] == XDEM_SHAPE_CLUMP;
   }
+  w->has_clumps = any_clump;
   if ((any_circle && any_ellipse) || any_segment) w->law = LAW_ANY;
   else if (any_ellipse)
     w->law = w->prm.ellipse_method == XDEM_ELLIPSE_INTERSECTION ? LAW_INTERSECTION : LAW_CLOSEST;
@@ -746,6 +769,8 @@ int32_t set_particles_impl(xdem_world_s* w, const xdem_particles* P, const std::
   CK(w, cudaMemsetAsync(d.cell_max, 0, sizeof(int32_t), s));
   CK(w, B.alloc(&d.cell_start, cells + 1));
   CK(w, B.alloc(&d.tile_sum, cells / kScanTile + 2));
+  CK(w, B.alloc(&d.done, 3));
+  CK(w, cudaMemsetAsync(d.done, 0, 3 * sizeof(uint32_t), s));
   CK(w, B.alloc(&d.cell_mem, 2 * (size_t)n));
   CK(w, B.alloc(&d.cell_pos, 2 * (size_t)n));
   CK(w, B.alloc(&d.cell_scr, 2 * (size_t)n));

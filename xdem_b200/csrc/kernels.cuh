@@ -102,11 +102,8 @@ __device__ __forceinline__ void flush_warp(const DevWorld& w, uint32_t st, uint3
 // a2: modifyParticlePosition (PeriodicBoundaryWorld.cpp:129-142,
 //     LeesEdwardsBoundaryWorld.cpp:304-333)
 // ---------------------------------------------------------------------------
-__global__ void k_modify_position(DevWorld w) {
-  if (stopped(w)) return;
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= w.n) return;
-  const WorldScalars& ws = w.ws[sys_at(w, i)];
+__device__ __forceinline__ double2 modify_position_at(const DevWorld& w, const WorldScalars& ws,
+                                                      int i) {
   double2 p = w.pos[i];
   if (w.kind == WORLD_LE) {
     if (p.y < ws.ymin) {
@@ -127,6 +124,14 @@ __global__ void k_modify_position(DevWorld w) {
     else if (p.y > ws.ymax) p.y += -ws.ylen;
   }
   w.pos[i] = p;
+  return p;
+}
+
+__global__ void k_modify_position(DevWorld w) {
+  if (stopped(w)) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= w.n) return;
+  modify_position_at(w, w.ws[sys_at(w, i)], i);
 }
 
 // scaleAllParticlePosition(scale_x, scale_y) (BaseWorld.cpp:119-124); after a
@@ -169,19 +174,22 @@ __global__ void k_background_velocity(DevWorld w, int apply) {
 // ncell+nx+[0,nx) top-row particles shifted by -shift (boxLE_bottom, :82-88).
 // The order inside a cell is not fixed; nothing downstream depends on it.
 // ---------------------------------------------------------------------------
+// MODIFY: k_modify_position's wrap first, in the same thread (a step's
+// position move followed by the binning)
+template <bool MODIFY = false>
 __global__ void k_bin(DevWorld w) {
   if (stopped(w)) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i == 0) *w.cell_max = 0;  // k_scan_tiles takes the maximum
   if (i >= w.n) return;
   const WorldScalars& ws = w.ws[sys_at(w, i)];
+  const double2 p = MODIFY ? modify_position_at(w, ws, i) : w.pos[i];
   Grid G = grid_of(ws);
   w.incnt[i] = 0;  // incoming-contact counters of this step's update
   if (G.nx < 3 || G.ny < 3) {
     if (i == ws.first) raise(w.status, ST_GRID);
     return;
   }
-  double2 p = w.pos[i];
   int ix = cell_of(p.x, ws.xmin, G.lx, G.nx);
   int iy = cell_of(p.y, ws.ymin, G.ly, G.ny);
   int c = G.base + iy * G.nx + ix;
@@ -236,11 +244,36 @@ __device__ __forceinline__ int32_t block_inclusive_scan(int32_t v, int32_t* sh_w
   return v;
 }
 
+// exclusive scan of the tile sums (one block); cell_start[total] = total
+// count.  The tile sums come from other blocks of the same launch: read past
+// the L1.
+__device__ __forceinline__ void scan_tile_sums(const DevWorld& w, int32_t* sh_warp) {
+  const int total = w.ncell_total;
+  int ntiles = (total + kScanTile - 1) / kScanTile;
+  int32_t carry = 0;
+  for (int base = 0; base < ntiles; base += kScanThreads) {
+    int t = base + threadIdx.x;
+    int32_t v = t < ntiles ? __ldcg(w.tile_sum + t) : 0;
+    int32_t inc = block_inclusive_scan(v, sh_warp);
+    if (t < ntiles) w.tile_sum[t] = carry + inc - v;
+    __syncthreads();
+    if (threadIdx.x == kScanThreads - 1) sh_warp[0] = inc;
+    __syncthreads();
+    carry += sh_warp[0];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) w.cell_start[total] = carry;
+}
+
+// tile sums, and the largest cell count; the last block to finish scans the
+// tile sums (a fence before the count of finished blocks makes every tile
+// sum visible to it; nothing waits)
 __global__ void __launch_bounds__(kScanThreads) k_scan_tiles(DevWorld w) {
   if (stopped(w)) return;
   const int total = w.ncell_total;
   int ntiles = (total + kScanTile - 1) / kScanTile;
   __shared__ int32_t sh_warp[kScanThreads / 32];
+  __shared__ bool last;
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     int base = tile * kScanTile + threadIdx.x * kScanPer;
     int32_t s = 0, mx = 0;
@@ -257,27 +290,15 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_tiles(DevWorld w) {
     if (threadIdx.x == kScanThreads - 1) w.tile_sum[tile] = inc;
     __syncthreads();
   }
-}
-
-// exclusive scan of the tile sums (one block); cell_start[total] = total count
-__global__ void __launch_bounds__(kScanThreads) k_scan_sums(DevWorld w) {
-  if (stopped(w)) return;
-  const int total = w.ncell_total;
-  int ntiles = (total + kScanTile - 1) / kScanTile;
-  __shared__ int32_t sh_warp[kScanThreads / 32];
-  int32_t carry = 0;
-  for (int base = 0; base < ntiles; base += kScanThreads) {
-    int t = base + threadIdx.x;
-    int32_t v = t < ntiles ? w.tile_sum[t] : 0;
-    int32_t inc = block_inclusive_scan(v, sh_warp);
-    if (t < ntiles) w.tile_sum[t] = carry + inc - v;
-    __syncthreads();
-    if (threadIdx.x == kScanThreads - 1) sh_warp[0] = inc;
-    __syncthreads();
-    carry += sh_warp[0];
-    __syncthreads();
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(&w.done[1], 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (last) {
+    __threadfence();
+    scan_tile_sums(w, sh_warp);
+    if (threadIdx.x == 0) w.done[1] = 0;
   }
-  if (threadIdx.x == 0) w.cell_start[total] = carry;
 }
 
 __global__ void __launch_bounds__(kScanThreads) k_scan_apply(DevWorld w) {
@@ -498,10 +519,10 @@ __device__ __forceinline__ void sort8(T* k) {
   cmp_swap(k[2], k[4]); cmp_swap(k[3], k[5]); cmp_swap(k[3], k[4]);
 }
 
-__global__ void __launch_bounds__(128) k_collect(DevWorld w, int par) {
-  if (stopped(w)) return;
-  int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= w.n) return;
+// the force sum of the particle at p: written to force, torque, ncp and
+// rattler, and returned in (Fo, To, rat)
+__device__ __forceinline__ void collect_at(const DevWorld& w, int par, int p, double2& Fo,
+                                           double& To, int& rat) {
   const int n = w.n, K = w.K;
   const Slots& cur = w.slots[par];
   int nown = min(cur.count[p], K);
@@ -543,10 +564,13 @@ __global__ void __launch_bounds__(128) k_collect(DevWorld w, int par) {
         ++nk;
       }
     }
-    w.force[p] = make_double2(fx, fy);
+    Fo = make_double2(fx, fy);
+    To = t;
+    rat = (nk + ninc) == 0 ? 1 : 0;
+    w.force[p] = Fo;
     w.torque[p] = t;
     w.ncp[p] = nk + ninc;
-    w.rattler[p] = (nk + ninc) == 0 ? 1 : 0;
+    w.rattler[p] = rat;
     return;
   }
   {
@@ -578,10 +602,23 @@ __global__ void __launch_bounds__(128) k_collect(DevWorld w, int par) {
       t += cur.t1[ci];
     }
   }
-  w.force[p] = make_double2(fx, fy);
+  Fo = make_double2(fx, fy);
+  To = t;
+  rat = (nown + ninc) == 0 ? 1 : 0;
+  w.force[p] = Fo;
   w.torque[p] = t;
   w.ncp[p] = nown + ninc;
-  w.rattler[p] = (nown + ninc) == 0 ? 1 : 0;
+  w.rattler[p] = rat;
+}
+
+__global__ void __launch_bounds__(128) k_collect(DevWorld w, int par) {
+  if (stopped(w)) return;
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= w.n) return;
+  double2 F;
+  double T;
+  int rat;
+  collect_at(w, par, p, F, T, rat);
 }
 
 // GluedParticle::isRattlerParticle (GluedParticle.cpp:141-147)
@@ -601,11 +638,11 @@ __device__ __forceinline__ bool is_rattler(const DevWorld& w, int m) {
 // (BaseWorld.cpp:79-92).  FOLD_BG first removes the Lees-Edwards background
 // velocity exactly as removeBackgroudVelocity would after applyBackgroudVelocity.
 // ---------------------------------------------------------------------------
-template <bool FOLD_BG>
-__global__ void k_integrate(DevWorld w, int reset_rattlers) {
-  if (stopped(w)) return;
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= w.n) return;
+// SUMS: the particle's force, torque and rattler flag come from the caller
+// (k_collect_integrate, a world without clumps) instead of memory
+template <bool FOLD_BG, bool SUMS>
+__device__ __forceinline__ void integrate_at(const DevWorld& w, int i, int reset_rattlers,
+                                             double2 Fs, double Ts, int rat) {
   const WorldScalars& ws = w.ws[sys_at(w, i)];
   const double dt = ws.dt, g = ws.g;
   const int set = w.setting[i];
@@ -676,12 +713,12 @@ __global__ void k_integrate(DevWorld w, int reset_rattlers) {
     }
     return;
   }
-  double2 F = w.force[i];
+  double2 F = SUMS ? Fs : w.force[i];
   double im = w.im[i];
   vec2<double> vv = (V(v.x, v.y) * (1.0 - g * dt) + (V(F.x, F.y) * im) * dt) / (1.0 + g * dt);
   p.x += vv.x * dt;
   p.y += vv.y * dt;
-  om = (om * (1.0 - g * dt) + w.torque[i] * w.iI[i] * dt) / (1.0 + g * dt);
+  om = (om * (1.0 - g * dt) + (SUMS ? Ts : w.torque[i]) * w.iI[i] * dt) / (1.0 + g * dt);
   if (w.V) w.vl_disp[i] += sqrt(vv.x * vv.x + vv.y * vv.y) * dt * seg_path_factor(w, i);  // candidate lists
   // a non-finite state raises XDEM_ERR_NONFINITE (the reference carries NaN
   // on without a word)
@@ -689,13 +726,36 @@ __global__ void k_integrate(DevWorld w, int reset_rattlers) {
     raise(w.status, ST_NONFINITE);
   w.pos[i] = p;
   w.rot[i] = w.rot[i] + om * dt;
-  if (reset_rattlers && !(set & SKIP_MACRO_SUM) && w.rattler[i]) {
+  if (reset_rattlers && !(set & SKIP_MACRO_SUM) && (SUMS ? rat : w.rattler[i])) {
     w.vel[i] = make_double2(0.0, 0.0);
     w.w[i] = 0.0;
   } else {
     w.vel[i] = make_double2(vv.x, vv.y);
     w.w[i] = om;
   }
+}
+
+template <bool FOLD_BG>
+__global__ void k_integrate(DevWorld w, int reset_rattlers) {
+  if (stopped(w)) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= w.n) return;
+  integrate_at<FOLD_BG, false>(w, i, reset_rattlers, make_double2(0.0, 0.0), 0.0, 0);
+}
+
+// k_collect then k_integrate, one thread per particle, for a world without
+// clumps (a body's time integral then reads only its own sums): the force,
+// torque and rattler flag go from the sum to the integral in registers
+template <bool FOLD_BG>
+__global__ void __launch_bounds__(128) k_collect_integrate(DevWorld w, int par, int reset_rattlers) {
+  if (stopped(w)) return;
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= w.n) return;
+  double2 F;
+  double T;
+  int rat;
+  collect_at(w, par, p, F, T, rat);
+  integrate_at<FOLD_BG, true>(w, p, reset_rattlers, F, T, rat);
 }
 
 // BaseWorld::resetVelocityOfRattlers / scaleVelocityOfRattlers (BaseWorld.cpp:79-106)

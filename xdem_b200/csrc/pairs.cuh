@@ -625,9 +625,33 @@ __device__ __forceinline__ void pair_forces_fp64(const DevWorld& w, int par, int
   }
 }
 
+// ---- end of the update ----------------------------------------------------------
+// The pair kernels have consumed this step's lists: the counters start again
+// from zero for the next update, and the count of listed pairs is kept for
+// the host.  Done by the last block to finish the launch that ends the pair
+// phase (`finish`): a fence before the count of finished blocks orders every
+// block's reads of the counters before the reset; nothing waits.  Every
+// thread of the block calls.
+__device__ __forceinline__ void finish_pairs(const DevWorld& w) {
+  __shared__ bool last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(&w.done[2], 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (last && threadIdx.x == 0) {
+    __threadfence();
+    w.ws->last_pairs = *w.npairs;
+    *w.npairs = 0;
+    *w.nfallback = 0;
+    *w.ndeep = 0;
+    w.done[2] = 0;
+  }
+}
+
 // one thread per listed pair (grid-stride loop)
 template <bool FOLD_BG, int LAW, bool WARM = false>
-__global__ void __launch_bounds__(128, 4) k_pair_forces(DevWorld w, int par, int record) {
+__global__ void __launch_bounds__(128, 4) k_pair_forces(DevWorld w, int par, int record,
+                                                        int finish) {
   if (stopped(w)) return;
   const int npairs = *w.npairs;
   PairCounters pc;
@@ -635,17 +659,7 @@ __global__ void __launch_bounds__(128, 4) k_pair_forces(DevWorld w, int par, int
     pair_forces_fp64<FOLD_BG, LAW, WARM>(w, par, record, t, pc);
   flush_warp(w, pc.st, pc.n_solves, pc.n_iters, pc.n_capped);
   if (WARM) flush_warm(w, pc.w_off, pc.w_used, pc.w_rej, pc.w_rest, pc.w_right);
-}
-
-// ---- end of the update ----------------------------------------------------------
-// The pair kernels have consumed this step's lists: the counters start again
-// from zero for the next update.
-__global__ void k_pairs_done(DevWorld w) {
-  if (stopped(w)) return;
-  w.ws->last_pairs = *w.npairs;
-  *w.npairs = 0;
-  *w.nfallback = 0;
-  *w.ndeep = 0;
+  if (finish) finish_pairs(w);
 }
 
 }  // namespace xdem

@@ -237,7 +237,8 @@ __device__ __forceinline__ void pair_forces_m(const DevWorld& w, int par, int re
 }
 
 template <bool FOLD_BG, int LAW, int PASS = PASS_ALL>
-__global__ void __launch_bounds__(128, 4) k_pair_forces_m(DevWorld w, int par, int record) {
+__global__ void __launch_bounds__(128, 4) k_pair_forces_m(DevWorld w, int par, int record,
+                                                          int finish) {
   if (stopped(w)) return;
   uint32_t st = 0, n_solves = 0, n_iters = 0, n_capped = 0;
   const int npairs = *w.npairs;
@@ -246,6 +247,7 @@ __global__ void __launch_bounds__(128, 4) k_pair_forces_m(DevWorld w, int par, i
     pair_forces_m<FOLD_BG, LAW, PASS>(w, par, record, t, st, n_solves, n_iters, n_capped,
                                       t + stride < npairs ? t + stride : -1);
   flush_warp(w, st, n_solves, n_iters, n_capped);
+  if (finish) finish_pairs(w);
 }
 
 // PASS_DEEP: a few blocks, registers as the FP64 construction needs them;
@@ -267,7 +269,8 @@ __global__ void __launch_bounds__(128) k_pair_deep_m(DevWorld w, int par, int re
 // the closest-approach pairs deferred by k_pair_forces_m: the reference's FP64
 // construction (EllipticParticle.cpp:34-285), then the mixed force
 template <bool FOLD_BG, int LAW, bool WARM = false>
-__global__ void __launch_bounds__(128) k_pair_fallback_m(DevWorld w, int par, int record) {
+__global__ void __launch_bounds__(128) k_pair_fallback_m(DevWorld w, int par, int record,
+                                                         int finish) {
   if (stopped(w)) return;
   const Slots& cur = w.slots[par ^ 1];
   const int nfb = *w.nfallback;
@@ -312,6 +315,7 @@ __global__ void __launch_bounds__(128) k_pair_fallback_m(DevWorld w, int par, in
   }
   flush_warp(w, st, n_solves, n_iters, n_capped);
   if (WARM) flush_warm(w, w_off, w_used, w_rej, w_rest, w_right);
+  if (finish) finish_pairs(w);
 }
 
 // single pairs through the mixed geometry (xdem_pair_geometry with

@@ -24,29 +24,12 @@ namespace xdem {
 constexpr int kVlBlock = 256;
 constexpr int kVlRounds = 1;  // rounds of 32 list entries whose loads k_candidates_vl issues together (two spill at 72 registers and measured slower)
 
-// block maxima of the path lengths since the last build
-__global__ void __launch_bounds__(kVlBlock) k_vl_maxdisp(DevWorld w) {
-  if (stopped(w)) return;
-  __shared__ double sh[kVlBlock / 32];
-  const int m = blockIdx.x * blockDim.x + threadIdx.x;
-  double v = m < w.n ? w.vl_disp[m] : 0.0;
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
-  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double mx = 0.0;
-    for (int k = 0; k < kVlBlock / 32; ++k) mx = fmax(mx, sh[k]);
-    w.vl_part[blockIdx.x] = mx;
-  }
-}
-
-// whether this step rebuilds the lists (system 0's vl_build)
-__global__ void __launch_bounds__(1024) k_vl_check(DevWorld w, int nblocks) {
-  if (stopped(w)) return;
-  __shared__ double sh[32];
+// whether this step rebuilds the lists (system 0's vl_build), from the block
+// maxima of the path lengths (nblocks of them; written by other blocks of the
+// launch, so read past the L1); every thread of the block calls
+__device__ __forceinline__ void vl_decide(const DevWorld& w, int nblocks, double* sh) {
   double v = 0.0;
-  for (int b = threadIdx.x; b < nblocks; b += blockDim.x) v = fmax(v, w.vl_part[b]);
+  for (int b = threadIdx.x; b < nblocks; b += blockDim.x) v = fmax(v, __ldcg(w.vl_part + b));
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
   if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
@@ -64,6 +47,35 @@ __global__ void __launch_bounds__(1024) k_vl_check(DevWorld w, int nblocks) {
       ws[0].vl_valid = 1;
       ws[0].vl_builds += 1;
     }
+  }
+}
+
+// block maxima of the path lengths since the last build; the last block to
+// finish takes the rebuild decision (a fence before the count of finished
+// blocks makes every maximum visible to it; nothing waits)
+__global__ void __launch_bounds__(kVlBlock) k_vl_maxdisp(DevWorld w) {
+  if (stopped(w)) return;
+  __shared__ double sh[kVlBlock / 32];
+  __shared__ bool last;
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  double v = m < w.n ? w.vl_disp[m] : 0.0;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double mx = 0.0;
+    for (int k = 0; k < kVlBlock / 32; ++k) mx = fmax(mx, sh[k]);
+    w.vl_part[blockIdx.x] = mx;
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(&w.done[0], 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (last) {
+    __threadfence();
+    vl_decide(w, gridDim.x, sh);
+    if (threadIdx.x == 0) w.done[0] = 0;
   }
 }
 
