@@ -85,6 +85,7 @@ struct xdem_world_s {
   int resort_every = kResortEvery;
   int law = LAW_ANY;                // contact-kernel specialisation for the shapes present
   bool has_clumps = false;          // a clump's time integral reads its sub-particles' sums
+  bool list_decided = false;        // the step's list-rebuild decision is already enqueued
   xdem_mlp_s* mlp = nullptr;        // learned warm start of the closest-approach Newton iteration
   PermList perm{};                  // particle arrays moved by a re-sort
   // launch configuration (xdem_set_launch_config / xdem_autotune): blocks per
@@ -206,9 +207,18 @@ void launch_modify(xdem_world_s* w) {
   LAUNCH(w, KK_MODIFY, k_modify_position<<<blocks_for(n, kBlock), kBlock, 0, w->stream>>>(w->dw));
 }
 
+// whether this step rebuilds the candidate lists (a grid-stride pass over the
+// path lengths, few blocks, so that the last one has few maxima to combine)
+void launch_list_decision(xdem_world_s* w) {
+  const int vb = std::min(blocks_for(w->dw.n, kVlBlock), 148 * 4);
+  LAUNCH(w, KK_VL_CHECK, k_vl_maxdisp<<<vb, kVlBlock, 0, w->stream>>>(w->dw));
+}
+
 // findPossibleContacts' binning; modify: the step's position move first, in
 // the binning kernel
-void launch_find(xdem_world_s* w, bool modify = false) {
+// decided: the step's list-rebuild decision is taken between the scan and the
+// scatter, which then writes the cell records only where a scan reads them
+void launch_find(xdem_world_s* w, bool modify = false, bool decided = false) {
   int n = w->dw.n;
   if (modify)
     LAUNCH(w, KK_BIN, k_bin<true><<<blocks_for(n, kBlock), kBlock, 0, w->stream>>>(w->dw));
@@ -219,7 +229,8 @@ void launch_find(xdem_world_s* w, bool modify = false) {
   LAUNCH(w, KK_SCAN, k_scan_tiles<<<tiles, kScanThreads, 0, w->stream>>>(w->dw));
   LAUNCH(w, KK_SCAN, k_scan_apply<<<tiles, kScanThreads, 0, w->stream>>>(w->dw));
   int nb = std::max(blocks_for(n, kBlock), std::min(blocks_for(cells, kBlock), 1184));
-  LAUNCH(w, KK_SCATTER, k_scatter<<<nb, kBlock, 0, w->stream>>>(w->dw));
+  if (decided) launch_list_decision(w);
+  LAUNCH(w, KK_SCATTER, k_scatter<<<nb, kBlock, 0, w->stream>>>(w->dw, decided ? 1 : 0));
 }
 
 // A pair kernel (DevWorld, slot-set parity, record) on the world's stream as
@@ -257,8 +268,7 @@ void launch_update_phases(xdem_world_s* w, int record) {
   // the learned warm start applies to closest-approach worlds
   const bool warm = w->mlp != nullptr && w->dw.warm != nullptr && LAW == LAW_CLOSEST;
   if (w->dw.V > 0) {
-    const int vb = blocks_for(w->dw.n, kVlBlock);
-    LAUNCH(w, KK_VL_CHECK, k_vl_maxdisp<<<vb, kVlBlock, 0, w->stream>>>(w->dw));
+    if (!w->list_decided) launch_list_decision(w);
     LAUNCH(w, KK_VL_BUILD, k_vl_build<LAW><<<nb, 128, 0, w->stream>>>(w->dw));
     LAUNCH(w, KK_CANDIDATES, k_candidates_vl<LAW><<<nb, 128, candidates_smem(w), w->stream>>>(
                                  w->dw, w->par));
@@ -340,15 +350,18 @@ void launch_integrate(xdem_world_s* w, bool fold_bg, int reset) {
     LAUNCH(w, KK_INTEGRATE, k_integrate<false><<<blocks_for(n, kBlock), kBlock, 0, w->stream>>>(w->dw, reset));
 }
 
-// the force sum and the time integral of a world without clumps in one pass
-void launch_collect_integrate(xdem_world_s* w, bool fold_bg, int reset) {
+// the force sum and the time integral of a world without clumps in one pass;
+// end_le >= 0: with the step's end (its Lees-Edwards update flag), -1 without
+void launch_collect_integrate(xdem_world_s* w, bool fold_bg, int reset, int end_le) {
   int n = w->dw.n;
   if (fold_bg)
     LAUNCH(w, KK_COLLECT_INTEGRATE, k_collect_integrate<true><<<blocks_for(n, 128), 128, 0,
-                                                                 w->stream>>>(w->dw, w->par, reset));
+                                                                 w->stream>>>(w->dw, w->par, reset,
+                                                                              end_le));
   else
     LAUNCH(w, KK_COLLECT_INTEGRATE, k_collect_integrate<false><<<blocks_for(n, 128), 128, 0,
-                                                                  w->stream>>>(w->dw, w->par, reset));
+                                                                  w->stream>>>(w->dw, w->par, reset,
+                                                                               end_le));
 }
 
 void launch_stress(xdem_world_s* w) {
@@ -398,15 +411,28 @@ void enqueue_step(xdem_world_s* w, const xdem_control* ctl, int record, bool res
   bool own = ctl->sequence == XDEM_SEQ_TAKE_TIME_STEP;
   bool le = own && kind == XDEM_WORLD_LEES_EDWARDS;
   if (ctl->scale_rattlers) launch_rattlers(w, 0, ctl->rattler_scale);
-  launch_find(w, true);
+  // with candidate lists and no re-sort the rebuild decision comes before the
+  // scatter, so that the cell records are written only when a scan reads
+  // them; a re-sort reorders the records and invalidates the lists, so its
+  // step writes them all and decides after it
+  const bool decided = w->dw.V > 0 && !resort;
+  launch_find(w, true, decided);
   if (resort) launch_resort(w);
+  w->list_decided = decided;
   launch_update(w, le, record);
+  w->list_decided = false;
+  // without a rattler reset, stress pass, box law or stop test between them,
+  // the step's end is taken by the last block of the fused sum and integral
+  const bool fold_end = !w->has_clumps && !ctl->reset_rattlers && !ctl->update_stress &&
+                        ctl->box_law == BOX_NONE && !ctl->stop_on_pressure;
   if (w->has_clumps) {
     launch_collect(w);
     launch_integrate(w, le, own && kind == XDEM_WORLD_PERIODIC_CONTROL);
   } else {
-    launch_collect_integrate(w, le, own && kind == XDEM_WORLD_PERIODIC_CONTROL);
+    launch_collect_integrate(w, le, own && kind == XDEM_WORLD_PERIODIC_CONTROL,
+                             fold_end ? (le ? 1 : 0) : -1);
   }
+  if (fold_end) return;
   if (ctl->reset_rattlers) launch_rattlers(w, 1, 0.0);
   if (ctl->update_stress) launch_stress(w);
   launch_end_of_step(w, ctl->box_law, ctl->p0, ctl->p1, le ? 1 : 0, ctl->stop_on_pressure,
@@ -769,8 +795,8 @@ int32_t set_particles_impl(xdem_world_s* w, const xdem_particles* P, const std::
   CK(w, cudaMemsetAsync(d.cell_max, 0, sizeof(int32_t), s));
   CK(w, B.alloc(&d.cell_start, cells + 1));
   CK(w, B.alloc(&d.tile_sum, cells / kScanTile + 2));
-  CK(w, B.alloc(&d.done, 3));
-  CK(w, cudaMemsetAsync(d.done, 0, 3 * sizeof(uint32_t), s));
+  CK(w, B.alloc(&d.done, 4));
+  CK(w, cudaMemsetAsync(d.done, 0, 4 * sizeof(uint32_t), s));
   CK(w, B.alloc(&d.cell_mem, 2 * (size_t)n));
   CK(w, B.alloc(&d.cell_pos, 2 * (size_t)n));
   CK(w, B.alloc(&d.cell_scr, 2 * (size_t)n));

@@ -184,6 +184,16 @@ __global__ void k_bin(DevWorld w) {
   if (i >= w.n) return;
   const WorldScalars& ws = w.ws[sys_at(w, i)];
   const double2 p = MODIFY ? modify_position_at(w, ws, i) : w.pos[i];
+  if (w.axis && w.shape[i] == SHAPE_ELLIPSE) {
+    // the centre-line screen's record (pairs.cuh, axis_shape): the
+    // orientation reduced to [-pi, pi] in FP64 before the FP32 sine and cosine
+    double r = w.rot[i];
+    r -= 6.283185307179586 * rint(r * 0.15915494309189535);
+    float sn, cs;
+    __sincosf((float)r, &sn, &cs);
+    const float a = (float)w.rad[i];
+    w.axis[i] = make_float4(cs, sn, a, __fdividef(a, (float)w.asp[i]));
+  }
   Grid G = grid_of(ws);
   w.incnt[i] = 0;  // incoming-contact counters of this step's update
   if (G.nx < 3 || G.ny < 3) {
@@ -347,12 +357,20 @@ __device__ __forceinline__ double seg_path_factor(const DevWorld& w, int m) {
   return (w.seg && w.shape[m] == SHAPE_SEGMENT) ? 2.0 : 1.0;
 }
 
-// also clears cell_count (already consumed by the scan) for the next binning
-__global__ void k_scatter(DevWorld w) {
+// The cell-ordered records of the 3x3 scan; also clears cell_count (already
+// consumed by the scan) for the next binning.  when_needed: this step's
+// rebuild decision is taken, and the records are written only where a scan
+// reads them: a list rebuild, a list that overflowed at the last build
+// (scanned in full every step), or nine cells that may hold the
+// 200-candidate cap's count (counted from the records).
+__global__ void k_scatter(DevWorld w, int when_needed) {
   if (stopped(w)) return;
   const int total = w.ncell_total;
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < total; c += gridDim.x * blockDim.x)
     w.cell_count[c] = 0;
+  if (when_needed && !w.ws->vl_build && !w.ws->vl_overflow &&
+      9 * *w.cell_max + 1 < kCandidateCap)
+    return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= w.n) return;
   const Grid G = grid_of(w.ws[sys_at(w, i)]);
@@ -366,16 +384,6 @@ __global__ void k_scatter(DevWorld w) {
   const float sr = screen_radius(w, i);
   const float idb = __int_as_float((w.setting[i] & SKIP_CONTACT_DETECTION) ? -1 : w.id_of[i]);
   const int up = w.up[i];
-  if (w.axis && w.shape[i] == SHAPE_ELLIPSE) {
-    // the centre-line screen's record (pairs.cuh, axis_shape): the
-    // orientation reduced to [-pi, pi] in FP64 before the FP32 sine and cosine
-    double r = w.rot[i];
-    r -= 6.283185307179586 * rint(r * 0.15915494309189535);
-    float sn, cs;
-    __sincosf((float)r, &sn, &cs);
-    const float a = (float)w.rad[i];
-    w.axis[i] = make_float4(cs, sn, a, __fdividef(a, (float)w.asp[i]));
-  }
   int q = w.cell_start[pc] + w.prank[i];
   w.cell_mem[q] = i;
   w.cell_pos[q] = p;
@@ -743,20 +751,6 @@ __global__ void k_integrate(DevWorld w, int reset_rattlers) {
   integrate_at<FOLD_BG, false>(w, i, reset_rattlers, make_double2(0.0, 0.0), 0.0, 0);
 }
 
-// k_collect then k_integrate, one thread per particle, for a world without
-// clumps (a body's time integral then reads only its own sums): the force,
-// torque and rattler flag go from the sum to the integral in registers
-template <bool FOLD_BG>
-__global__ void __launch_bounds__(128) k_collect_integrate(DevWorld w, int par, int reset_rattlers) {
-  if (stopped(w)) return;
-  int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= w.n) return;
-  double2 F;
-  double T;
-  int rat;
-  collect_at(w, par, p, F, T, rat);
-  integrate_at<FOLD_BG, true>(w, p, reset_rattlers, F, T, rat);
-}
 
 // BaseWorld::resetVelocityOfRattlers / scaleVelocityOfRattlers (BaseWorld.cpp:79-106)
 __global__ void k_rattlers(DevWorld w, int reset, double scale) {
@@ -976,10 +970,10 @@ __device__ __forceinline__ void box_law(WorldScalars& ws, int law, double p0, do
 // count and the stop test.  After a stop the scales are 1.
 // One thread per system; the run-level counters and the stop test (single
 // systems only) belong to system 0.
-__global__ void k_end_of_step(DevWorld w, int law, double p0, double p1, int le_update,
-                              int stop_on_pressure, double stop_pressure, int count_step) {
-  const int sys = blockIdx.x * blockDim.x + threadIdx.x;
-  if (sys >= w.nsys) return;
+// the end of a step for system sys (k_end_of_step)
+__device__ __forceinline__ void end_of_step_at(const DevWorld& w, int sys, int law, double p0,
+                                               double p1, int le_update, int stop_on_pressure,
+                                               double stop_pressure, int count_step) {
   WorldScalars& ws = w.ws[sys];
   if (stopped(w)) {
     ws.scale_x = 1.0;
@@ -1006,6 +1000,47 @@ __global__ void k_end_of_step(DevWorld w, int law, double p0, double p1, int le_
     ws.flips += 1;
   }
   if (stop_on_pressure && (ws.stress[0] + ws.stress[3]) / 2.0 >= stop_pressure) ws.stop = 1;
+}
+
+__global__ void k_end_of_step(DevWorld w, int law, double p0, double p1, int le_update,
+                              int stop_on_pressure, double stop_pressure, int count_step) {
+  const int sys = blockIdx.x * blockDim.x + threadIdx.x;
+  if (sys >= w.nsys) return;
+  end_of_step_at(w, sys, law, p0, p1, le_update, stop_on_pressure, stop_pressure, count_step);
+}
+
+// k_collect then k_integrate, one thread per particle, for a world without
+// clumps (a body's time integral then reads only its own sums): the force,
+// torque and rattler flag go from the sum to the integral in registers
+//
+// le_update >= 0: the step's end (k_end_of_step without a box law, stop test
+// or stress in between) by the last block to finish, for every system, with
+// that Lees-Edwards update flag (a fence before the count of finished blocks;
+// nothing waits); -1: k_end_of_step follows as its own launch.
+template <bool FOLD_BG>
+__global__ void __launch_bounds__(128) k_collect_integrate(DevWorld w, int par, int reset_rattlers,
+                                                           int le_update) {
+  if (stopped(w)) return;
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < w.n) {
+    double2 F;
+    double T;
+    int rat;
+    collect_at(w, par, p, F, T, rat);
+    integrate_at<FOLD_BG, true>(w, p, reset_rattlers, F, T, rat);
+  }
+  if (le_update < 0) return;
+  __shared__ bool last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(&w.done[3], 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (last) {
+    __threadfence();
+    for (int sys = threadIdx.x; sys < w.nsys; sys += blockDim.x)
+      end_of_step_at(w, sys, BOX_NONE, 0.0, 0.0, le_update, 0, 0.0, 1);
+    if (threadIdx.x == 0) w.done[3] = 0;
+  }
 }
 
 // kinetic energy (BaseWorld.cpp:302-310), fixed-tree sum

@@ -45,6 +45,7 @@ __device__ __forceinline__ void vl_decide(const DevWorld& w, int nblocks, double
     if (rebuild) {
       for (int s = 0; s < w.nsys; ++s) ws[s].vl_travel = 0.0;
       ws[0].vl_valid = 1;
+      ws[0].vl_overflow = 0;
       ws[0].vl_builds += 1;
     }
   }
@@ -57,8 +58,9 @@ __global__ void __launch_bounds__(kVlBlock) k_vl_maxdisp(DevWorld w) {
   if (stopped(w)) return;
   __shared__ double sh[kVlBlock / 32];
   __shared__ bool last;
-  const int m = blockIdx.x * blockDim.x + threadIdx.x;
-  double v = m < w.n ? w.vl_disp[m] : 0.0;
+  double v = 0.0;
+  for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < w.n; m += gridDim.x * blockDim.x)
+    v = fmax(v, w.vl_disp[m]);
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
   if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
@@ -129,6 +131,7 @@ __global__ void __launch_bounds__(128) k_vl_build(DevWorld w) {
     }
   }
   w.vl_cnt[m] = cnt;
+  if (cnt < 0) w.ws->vl_overflow = 1;  // k_scatter then writes the cell records every step
 }
 
 // k_candidates with the lists: same outputs (body records, slot counts,

@@ -65,8 +65,9 @@ struct WorldScalars {
   // arrays; particles (ids and memory positions) [first, first + count)
   int32_t nx_cap, ny_cap, cell_base, first, count;
   // candidate lists (verlet.cuh), system 0: 0 once they must be rebuilt;
-  // 1 while the step's build kernel rebuilds them
-  int32_t vl_valid, vl_build, pad_;
+  // 1 while the step's build kernel rebuilds them; 1 when a list of the last
+  // build overflowed (its owner is scanned in full every step)
+  int32_t vl_valid, vl_build, vl_overflow;
   // closest-approach Newton statistics since the last reset: solves,
   // iterations, solves stopped by the iteration cap
   unsigned long long newton_solves, newton_iters, newton_capped;
@@ -152,9 +153,10 @@ struct DevWorld {
   int32_t* cell_max;  // largest cell count of this step's binning (all systems)
   int32_t* cell_start;
   int32_t* tile_sum;  // scan tile sums
-  // [3] blocks finished of the list check, of the scan's tile pass and of the
-  // launch that ends the pair phase: the last block of each finishes the
-  // pass's work, then resets its counter
+  // [4] blocks finished of the list check, of the scan's tile pass, of the
+  // launch that ends the pair phase and of the fused force sum and time
+  // integral: the last block of each finishes the pass's work, then resets
+  // its counter
   uint32_t* done;
   int32_t* cell_mem;
   double2* cell_pos;      // [2n] position of each cell entry, cell order
