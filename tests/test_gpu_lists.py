@@ -2,12 +2,15 @@
 a world with the lists and a world with the full 3x3 scan every step produce
 the same contacts and state bit for bit — in a Lees-Edwards shear (the shift
 travels, particles cross the sheared edge), under a strain-controlled box law
-(affine scaling), for clumps, after host state uploads, and in a batch."""
+(affine scaling), for clumps, after host state uploads, in a batch, with
+lists that overflow, and where nine cells may hold the 200-candidate cap's
+count (the last two read the cell-ordered records on steps without a list
+rebuild)."""
 import numpy as np
 import pytest
 
 from xdem_b200 import abi
-from xdem_b200.world import World, make_control
+from xdem_b200.world import World, make_control, make_params
 
 from helpers import clump_case, dense_ellipse_case, disc_case
 
@@ -69,3 +72,46 @@ def test_lists_match_full_scan_clumps():
     for w in (a, b):
         w.run(120, make_control())
     assert _same(a, b) > 50
+
+
+def test_lists_match_full_scan_list_overflow():
+    """Lists of three entries overflow for most particles, which then take
+    the full 3x3 scan every step from the cell records (written every step
+    while a list of the last build overflowed); plain steps."""
+    p, prm = disc_case(n=1500, phi=0.80, seed=21)
+    a, b = World(prm), World(prm)
+    a.set_candidate_lists(0)
+    b.set_candidate_lists(3, 0.1)
+    for w in (a, b):
+        w.set_particles(p)
+        w.run(80, make_control())
+    assert _same(a, b) > 1000
+    assert b.candidate_list_stats()["builds"] >= 1
+
+
+def test_lists_match_full_scan_candidate_cap_reachable():
+    """Small discs (r 0.25) with a few large ones (r 1.2, which set the cell
+    size to 2.01 x 1.2) at solid fraction 0.65 put up to 23 records in a
+    cell, so nine cells may hold the 200-candidate cap's count and the bound
+    is counted from the cell records every step (below the cap itself: no
+    capacity error)."""
+    from xdem_b200 import inputs
+    rng = np.random.default_rng(5)
+    n = 3000
+    r = np.where(rng.permutation(n) < 40, 1.2, 0.25)
+    box = inputs.box_for(float(np.sum(np.pi * r * r)), 0.5)
+    x, y = inputs.rsa_positions(r, box, 6)
+    p = inputs.assemble(np.zeros(n, np.int32), r, np.ones(n), x, y, rng.normal(0, 0.05, n),
+                        rng.normal(0, 0.05, n), np.zeros(n), np.zeros(n))
+    box = inputs.scale_to_fraction(p, box, float(np.sum(p["volume"])), 0.65)
+    side = 2.01 * 1.2
+    nx, ny = int((box[1] - box[0]) // side), int((box[3] - box[2]) // side)
+    counts, _, _ = np.histogram2d(p["x"], p["y"], bins=(nx, ny),
+                                  range=((box[0], box[1]), (box[2], box[3])))
+    assert 9 * counts.max() + 1 >= 200
+    prm = make_params(abi.WORLD_PERIODIC, inputs.time_step(p), box, inputs.KN, inputs.KT,
+                      inputs.RESTITUTION, inputs.FRICTION)
+    a, b = _pair_of_worlds(p, prm)
+    for w in (a, b):
+        w.run(60, make_control())
+    assert _same(a, b) > 100
