@@ -202,6 +202,29 @@ void prof_end(xdem_world_s* w) {
   } while (0)
 
 // ---- launch helpers -------------------------------------------------------
+// A step kernel as a programmatic dependent launch: it may become resident
+// while the kernel before it runs and waits in its pdl_begin until that one
+// has completed, so that its launch and its blocks' start overlap the other's
+// tail.  While the kernels are timed one by one it is an ordinary launch.
+template <typename... KArgs, typename... Args>
+void launch_chain(xdem_world_s* w, int kind, void (*kernel)(KArgs...), int grid, int block,
+                  size_t smem, Args... args) {
+  prof_begin(w, kind);
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = w->prof_on ? 0 : 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = w->stream;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cuda_check(w, cudaLaunchKernelEx(&cfg, kernel, args...));
+  prof_end(w);
+  w->launches++;
+}
+
 void launch_modify(xdem_world_s* w) {
   int n = w->dw.n;
   LAUNCH(w, KK_MODIFY, k_modify_position<<<blocks_for(n, kBlock), kBlock, 0, w->stream>>>(w->dw));
@@ -211,7 +234,7 @@ void launch_modify(xdem_world_s* w) {
 // path lengths, few blocks, so that the last one has few maxima to combine)
 void launch_list_decision(xdem_world_s* w) {
   const int vb = std::min(blocks_for(w->dw.n, kVlBlock), 148 * 4);
-  LAUNCH(w, KK_VL_CHECK, k_vl_maxdisp<<<vb, kVlBlock, 0, w->stream>>>(w->dw));
+  launch_chain(w, KK_VL_CHECK, k_vl_maxdisp, vb, kVlBlock, 0, w->dw);
 }
 
 // findPossibleContacts' binning; modify: the step's position move first, in
@@ -221,16 +244,16 @@ void launch_list_decision(xdem_world_s* w) {
 void launch_find(xdem_world_s* w, bool modify = false, bool decided = false) {
   int n = w->dw.n;
   if (modify)
-    LAUNCH(w, KK_BIN, k_bin<true><<<blocks_for(n, kBlock), kBlock, 0, w->stream>>>(w->dw));
+    launch_chain(w, KK_BIN, k_bin<true>, blocks_for(n, kBlock), kBlock, 0, w->dw);
   else
-    LAUNCH(w, KK_BIN, k_bin<false><<<blocks_for(n, kBlock), kBlock, 0, w->stream>>>(w->dw));
+    launch_chain(w, KK_BIN, k_bin<false>, blocks_for(n, kBlock), kBlock, 0, w->dw);
   int cells = w->dw.ncell_total;
   int tiles = std::min(blocks_for(cells, kScanTile), 2 * 148 * 8);
-  LAUNCH(w, KK_SCAN, k_scan_tiles<<<tiles, kScanThreads, 0, w->stream>>>(w->dw));
-  LAUNCH(w, KK_SCAN, k_scan_apply<<<tiles, kScanThreads, 0, w->stream>>>(w->dw));
+  launch_chain(w, KK_SCAN, k_scan_tiles, tiles, kScanThreads, 0, w->dw);
+  launch_chain(w, KK_SCAN, k_scan_apply, tiles, kScanThreads, 0, w->dw);
   int nb = std::max(blocks_for(n, kBlock), std::min(blocks_for(cells, kBlock), 1184));
   if (decided) launch_list_decision(w);
-  LAUNCH(w, KK_SCATTER, k_scatter<<<nb, kBlock, 0, w->stream>>>(w->dw, decided ? 1 : 0));
+  launch_chain(w, KK_SCATTER, k_scatter, nb, kBlock, 0, w->dw, decided ? 1 : 0);
 }
 
 // A pair kernel (DevWorld, slot-set parity, record) on the world's stream as
@@ -269,9 +292,8 @@ void launch_update_phases(xdem_world_s* w, int record) {
   const bool warm = w->mlp != nullptr && w->dw.warm != nullptr && LAW == LAW_CLOSEST;
   if (w->dw.V > 0) {
     if (!w->list_decided) launch_list_decision(w);
-    LAUNCH(w, KK_VL_BUILD, k_vl_build<LAW><<<nb, 128, 0, w->stream>>>(w->dw));
-    LAUNCH(w, KK_CANDIDATES, k_candidates_vl<LAW><<<nb, 128, candidates_smem(w), w->stream>>>(
-                                 w->dw, w->par));
+    launch_chain(w, KK_VL_BUILD, k_vl_build<LAW>, nb, 128, 0, w->dw);
+    launch_chain(w, KK_CANDIDATES, k_candidates_vl<LAW>, nb, 128, candidates_smem(w), w->dw, w->par);
   } else {
     LAUNCH(w, KK_CANDIDATES, k_candidates<LAW><<<nb, 128, 0, w->stream>>>(w->dw, w->par));
   }
@@ -285,8 +307,7 @@ void launch_update_phases(xdem_world_s* w, int record) {
     // The regular pass uses nothing the deep pass writes; the deferred pass
     // after it is an ordinary launch and waits for both.  While the kernels
     // are timed one by one the regular pass is an ordinary launch too.
-    LAUNCH(w, KK_DEEP,
-           k_pair_deep_m<FOLD_BG, LAW><<<148 * 2, 128, 0, w->stream>>>(w->dw, w->par, record));
+    launch_chain(w, KK_DEEP, k_pair_deep_m<FOLD_BG, LAW>, 148 * 2, 128, 0, w->dw, w->par, record);
     if (w->prof_on) {
       LAUNCH(w, KK_PAIRS, k_pair_forces_m<FOLD_BG, LAW, PASS_REGULAR><<<pb, 128, 0, w->stream>>>(
                               w->dw, w->par, record, 0));
@@ -355,13 +376,11 @@ void launch_integrate(xdem_world_s* w, bool fold_bg, int reset) {
 void launch_collect_integrate(xdem_world_s* w, bool fold_bg, int reset, int end_le) {
   int n = w->dw.n;
   if (fold_bg)
-    LAUNCH(w, KK_COLLECT_INTEGRATE, k_collect_integrate<true><<<blocks_for(n, 128), 128, 0,
-                                                                 w->stream>>>(w->dw, w->par, reset,
-                                                                              end_le));
+    launch_chain(w, KK_COLLECT_INTEGRATE, k_collect_integrate<true>, blocks_for(n, 128), 128, 0,
+                 w->dw, w->par, reset, end_le);
   else
-    LAUNCH(w, KK_COLLECT_INTEGRATE, k_collect_integrate<false><<<blocks_for(n, 128), 128, 0,
-                                                                  w->stream>>>(w->dw, w->par, reset,
-                                                                               end_le));
+    launch_chain(w, KK_COLLECT_INTEGRATE, k_collect_integrate<false>, blocks_for(n, 128), 128, 0,
+                 w->dw, w->par, reset, end_le);
 }
 
 void launch_stress(xdem_world_s* w) {

@@ -34,6 +34,18 @@ __device__ __forceinline__ int sys_at(const DevWorld& w, int m) {
 // run-level stop flag (set by a stop condition; ends the kernels of a run)
 __device__ __forceinline__ bool stopped(const DevWorld& w) { return w.ws->stop != 0; }
 
+// Programmatic dependent launch of a step's kernels: a kernel launched with
+// it may become resident while the kernel before it in the stream runs;
+// pdl_begin first waits until that kernel has completed and its writes are
+// visible (a no-op for an ordinary launch), then lets the next kernel launch
+// (it becomes resident once every block of this one has started, and waits
+// in its own pdl_begin).  Every kernel that a step launches this way calls
+// pdl_begin before touching memory.
+__device__ __forceinline__ void pdl_begin() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // Grid of PeriodicBoundaryWorld::findPossibleContacts (PeriodicBoundaryWorld.cpp:17-22):
 // nx = floor(xlen / (2.01 r_max)); clamped to the allocated capacity, which
 // only makes cells larger and leaves the contact set unchanged.  Regular cell
@@ -178,6 +190,7 @@ __global__ void k_background_velocity(DevWorld w, int apply) {
 // position move followed by the binning)
 template <bool MODIFY = false>
 __global__ void k_bin(DevWorld w) {
+  pdl_begin();
   if (stopped(w)) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i == 0) *w.cell_max = 0;  // k_scan_tiles takes the maximum
@@ -279,6 +292,7 @@ __device__ __forceinline__ void scan_tile_sums(const DevWorld& w, int32_t* sh_wa
 // tile sums (a fence before the count of finished blocks makes every tile
 // sum visible to it; nothing waits)
 __global__ void __launch_bounds__(kScanThreads) k_scan_tiles(DevWorld w) {
+  pdl_begin();
   if (stopped(w)) return;
   const int total = w.ncell_total;
   int ntiles = (total + kScanTile - 1) / kScanTile;
@@ -312,6 +326,7 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_tiles(DevWorld w) {
 }
 
 __global__ void __launch_bounds__(kScanThreads) k_scan_apply(DevWorld w) {
+  pdl_begin();
   if (stopped(w)) return;
   const int total = w.ncell_total;
   int ntiles = (total + kScanTile - 1) / kScanTile;
@@ -364,6 +379,7 @@ __device__ __forceinline__ double seg_path_factor(const DevWorld& w, int m) {
 // (scanned in full every step), or nine cells that may hold the
 // 200-candidate cap's count (counted from the records).
 __global__ void k_scatter(DevWorld w, int when_needed) {
+  pdl_begin();
   if (stopped(w)) return;
   const int total = w.ncell_total;
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < total; c += gridDim.x * blockDim.x)
@@ -1020,6 +1036,7 @@ __global__ void k_end_of_step(DevWorld w, int law, double p0, double p1, int le_
 template <bool FOLD_BG>
 __global__ void __launch_bounds__(128) k_collect_integrate(DevWorld w, int par, int reset_rattlers,
                                                            int le_update) {
+  pdl_begin();
   if (stopped(w)) return;
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p < w.n) {

@@ -254,12 +254,13 @@ __global__ void __launch_bounds__(128, 4) k_pair_forces_m(DevWorld w, int par, i
 // launched ahead of the regular pass, which it lets start at once
 template <bool FOLD_BG, int LAW>
 __global__ void __launch_bounds__(128) k_pair_deep_m(DevWorld w, int par, int record) {
+  // the candidate kernel before it has completed; the regular pair pass,
+  // launched after this kernel as a programmatic dependent launch, may start
+  // now (it reads nothing this kernel writes)
+  pdl_begin();
   if (stopped(w)) return;
   uint32_t st = 0, n_solves = 0, n_iters = 0, n_capped = 0;
   const int ndeep = *w.ndeep;
-  // the regular pair pass, launched after this kernel as a programmatic
-  // dependent launch, may start now
-  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ndeep; t += gridDim.x * blockDim.x)
     pair_forces_m<FOLD_BG, LAW, PASS_DEEP>(w, par, record, w.deep[t], st, n_solves, n_iters,
                                            n_capped);

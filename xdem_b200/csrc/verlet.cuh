@@ -55,6 +55,7 @@ __device__ __forceinline__ void vl_decide(const DevWorld& w, int nblocks, double
 // finish takes the rebuild decision (a fence before the count of finished
 // blocks makes every maximum visible to it; nothing waits)
 __global__ void __launch_bounds__(kVlBlock) k_vl_maxdisp(DevWorld w) {
+  pdl_begin();
   if (stopped(w)) return;
   __shared__ double sh[kVlBlock / 32];
   __shared__ bool last;
@@ -88,6 +89,7 @@ __global__ void __launch_bounds__(kVlBlock) k_vl_maxdisp(DevWorld w) {
 // scanned in full every step until the next build.
 template <int LAW>
 __global__ void __launch_bounds__(128) k_vl_build(DevWorld w) {
+  pdl_begin();
   if (stopped(w) || !w.ws->vl_build) return;
   const int m = blockIdx.x * blockDim.x + threadIdx.x;
   if (m >= w.n) return;
@@ -149,6 +151,7 @@ __global__ void __launch_bounds__(128) k_vl_build(DevWorld w) {
 // Dynamic shared memory: 2 * K * 128 int32.
 template <int LAW>
 __global__ void __launch_bounds__(128, 7) k_candidates_vl(DevWorld w, int par) {
+  pdl_begin();
   if (stopped(w)) return;
   extern __shared__ int32_t s_list[];
   __shared__ uint32_t s_matched[128];
