@@ -86,6 +86,7 @@ struct xdem_world_s {
   int law = LAW_ANY;                // contact-kernel specialisation for the shapes present
   bool has_clumps = false;          // a clump's time integral reads its sub-particles' sums
   bool list_decided = false;        // the step's list-rebuild decision is already enqueued
+  bool body_written = false;        // the step's body records are written by its binning
   xdem_mlp_s* mlp = nullptr;        // learned warm start of the closest-approach Newton iteration
   PermList perm{};                  // particle arrays moved by a re-sort
   // launch configuration (xdem_set_launch_config / xdem_autotune): blocks per
@@ -293,7 +294,8 @@ void launch_update_phases(xdem_world_s* w, int record) {
   if (w->dw.V > 0) {
     if (!w->list_decided) launch_list_decision(w);
     launch_chain(w, KK_VL_BUILD, k_vl_build<LAW>, nb, 128, 0, w->dw);
-    launch_chain(w, KK_CANDIDATES, k_candidates_vl<LAW>, nb, 128, candidates_smem(w), w->dw, w->par);
+    launch_chain(w, KK_CANDIDATES, k_candidates_vl<LAW>, nb, 128, candidates_smem(w), w->dw, w->par,
+                 w->body_written ? 0 : 1);
   } else {
     LAUNCH(w, KK_CANDIDATES, k_candidates<LAW><<<nb, 128, 0, w->stream>>>(w->dw, w->par));
   }
@@ -438,8 +440,10 @@ void enqueue_step(xdem_world_s* w, const xdem_control* ctl, int record, bool res
   launch_find(w, true, decided);
   if (resort) launch_resort(w);
   w->list_decided = decided;
+  w->body_written = !resort;  // a re-sort moves the particles after the binning wrote them
   launch_update(w, le, record);
   w->list_decided = false;
+  w->body_written = false;
   // without a rattler reset, stress pass, box law or stop test between them,
   // the step's end is taken by the last block of the fused sum and integral
   const bool fold_end = !w->has_clumps && !ctl->reset_rattlers && !ctl->update_stress &&

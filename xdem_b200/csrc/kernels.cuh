@@ -178,6 +178,24 @@ __global__ void k_background_velocity(DevWorld w, int apply) {
   w.vel[i] = v;
 }
 
+// the record of the body at m for this step's pair kernels; cs = (cos, sin)
+// of its orientation for an ellipse
+__device__ __forceinline__ void write_body(const DevWorld& w, int m, double2 cs) {
+  BodyRec b;
+  b.pos = w.pos[m];
+  b.vel = w.vel[m];
+  b.rot = w.rot[m];
+  b.w = w.w[m];
+  b.r = w.rad[m];
+  b.asp = w.asp[m];
+  b.cs = cs;
+  b.shape = w.shape[m];
+  b.id = w.id_of[m];
+  b.setting = w.setting[m];
+  b.pad = 0;
+  w.body[m] = b;
+}
+
 // ---------------------------------------------------------------------------
 // a3/a4: cell binning.  Counting sort: per-cell counts by atomics, an
 // exclusive scan, and a scatter.  Ghost rows after the regular cells hold the
@@ -197,6 +215,16 @@ __global__ void k_bin(DevWorld w) {
   if (i >= w.n) return;
   const WorldScalars& ws = w.ws[sys_at(w, i)];
   const double2 p = MODIFY ? modify_position_at(w, ws, i) : w.pos[i];
+  if (MODIFY) {
+    // this step's body record for the pair kernels (the candidate kernel
+    // writes it instead after a re-sort, or when the step runs as sub-steps)
+    double2 cs = make_double2(0.0, 0.0);
+    if (w.shape[i] == SHAPE_ELLIPSE) {
+      const double r = w.rot[i];
+      cs = make_double2(cos(r), sin(r));
+    }
+    write_body(w, i, cs);
+  }
   if (w.axis && w.shape[i] == SHAPE_ELLIPSE) {
     // the centre-line screen's record (pairs.cuh, axis_shape): the
     // orientation reduced to [-pi, pi] in FP64 before the FP32 sine and cosine
@@ -452,24 +480,6 @@ __device__ __forceinline__ PState load_state(const DevWorld& w, const WorldScala
   p.rot = w.rot[m];
   p.w = w.w[m];
   return p;
-}
-
-// the record of the body at m for this step's pair kernels; cs = (cos, sin)
-// of its orientation for an ellipse
-__device__ __forceinline__ void write_body(const DevWorld& w, int m, double2 cs) {
-  BodyRec b;
-  b.pos = w.pos[m];
-  b.vel = w.vel[m];
-  b.rot = w.rot[m];
-  b.w = w.w[m];
-  b.r = w.rad[m];
-  b.asp = w.asp[m];
-  b.cs = cs;
-  b.shape = w.shape[m];
-  b.id = w.id_of[m];
-  b.setting = w.setting[m];
-  b.pad = 0;
-  w.body[m] = b;
 }
 
 // the state load_state gives, from a body record

@@ -150,7 +150,9 @@ __global__ void __launch_bounds__(128) k_vl_build(DevWorld w) {
 // warp writes its pairs to the pair list together, coalesced, in owner order.
 // Dynamic shared memory: 2 * K * 128 int32.
 template <int LAW>
-__global__ void __launch_bounds__(128, 7) k_candidates_vl(DevWorld w, int par) {
+// body: write the owners' body records here (after a re-sort, or when the
+// step runs as sub-steps; otherwise the binning kernel has written them)
+__global__ void __launch_bounds__(128, 7) k_candidates_vl(DevWorld w, int par, int body) {
   pdl_begin();
   if (stopped(w)) return;
   extern __shared__ int32_t s_list[];
@@ -177,7 +179,7 @@ __global__ void __launch_bounds__(128, 7) k_candidates_vl(DevWorld w, int par) {
   s_matched[tid] = 0u;
   if (valid) {
     const WorldScalars& ws = w.ws[sys_at(w, m)];
-    write_owner_body<LAW>(w, m);
+    if (body) write_owner_body<LAW>(w, m);
     shape_ax = owner_axis_shape<LAW>(w, m);
     G = grid_of(ws);
     nold = min(old.count[m], K);
