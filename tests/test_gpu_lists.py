@@ -67,11 +67,42 @@ def test_lists_match_full_scan_strain_control_and_uploads():
 
 
 def test_lists_match_full_scan_clumps():
+    """Also: a sub-disc outside the periodic box (its clump's centre inside)
+    is wrapped on its own at each step's start and placed at the clump's
+    centre plus its branch again by the time integral; that jump of one box
+    length is no move, so the lists are not rebuilt every step."""
     p, prm = clump_case(nfree=150, nclump=40, seed=17, phi=0.62)
     a, b = _pair_of_worlds(p, prm)
     for w in (a, b):
         w.run(120, make_control())
     assert _same(a, b) > 50
+    s = b.get_state()
+    xmin, xmax, ymin, ymax = b.getBoundary()
+    sub = np.nonzero(p["up_level"] != np.arange(len(p["up_level"])))[0]
+    outside = (s["x"][sub] < xmin) | (s["x"][sub] > xmax) | (s["y"][sub] < ymin) | (s["y"][sub] > ymax)
+    assert np.any(outside), "no sub-disc outside the box: the case needs one"
+    builds = b.candidate_list_stats()["builds"]
+    assert builds < 30, f"{builds} list builds in 120 steps"
+
+
+@pytest.mark.parametrize("kind", ["compression", "shear"])
+def test_lists_match_full_scan_clumps_moving_box(kind):
+    """Clumps under a strain-controlled compression (the box law scales every
+    position, and the time integral puts each sub-disc back at its clump's
+    centre plus its branch) and in a Lees-Edwards shear (sub-discs cross the
+    sheared edge on their own)."""
+    p, prm = clump_case(nfree=150, nclump=40, seed=23, phi=0.6)
+    if kind == "compression":
+        prm.world_kind = abi.WORLD_PERIODIC_CONTROL
+        ctl = make_control(update_stress=True, box_law=abi.BOX_STRAIN, p0=-2e-3, p1=-2e-3)
+    else:
+        prm.world_kind = abi.WORLD_LEES_EDWARDS
+        prm.shift_strain_rate = 2.0
+        ctl = make_control(update_stress=True)
+    a, b = _pair_of_worlds(p, prm)
+    for w in (a, b):
+        w.run(100, ctl)
+    assert _same(a, b) > 20
 
 
 def test_lists_match_full_scan_list_overflow():

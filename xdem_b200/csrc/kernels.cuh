@@ -725,8 +725,26 @@ __device__ __forceinline__ void integrate_at(const DevWorld& w, int i, int reset
       vec2<double> sv = vv + crossw(b, om);
       w.vel[sk] = make_double2(sv.x, sv.y);
       if (w.V) {  // path length for the candidate lists
+        // the sub-particle's move from its stored position, which a box law
+        // may have scaled apart from the clump's centre plus its branch; the
+        // periodic wrap moves each body on its own, so a wrap of the
+        // sub-particle alone shows here as a jump of one box image, which is
+        // no move and is taken out (a wrap across the sheared edge already
+        // rebuilds the lists)
         const double2 op = w.pos[sk];
-        const double ex = (p.x + b.x) - op.x, ey = (p.y + b.y) - op.y;
+        double ex = (p.x + b.x) - op.x, ey = (p.y + b.y) - op.y;
+        if (w.kind == WORLD_LE) {
+          if (ey > 0.5 * ws.ylen) {
+            ey -= ws.ylen;
+            ex -= ws.shift;
+          } else if (ey < -0.5 * ws.ylen) {
+            ey += ws.ylen;
+            ex += ws.shift;
+          }
+        } else {
+          ey -= ws.ylen * rint(ey / ws.ylen);
+        }
+        ex -= ws.xlen * rint(ex / ws.xlen);
         w.vl_disp[sk] += sqrt(ex * ex + ey * ey);
       }
       w.pos[sk] = make_double2(p.x + b.x, p.y + b.y);

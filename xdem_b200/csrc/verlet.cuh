@@ -26,7 +26,9 @@ constexpr int kVlRounds = 1;  // rounds of 32 list entries whose loads k_candida
 
 // whether this step rebuilds the lists (system 0's vl_build), from the block
 // maxima of the path lengths (nblocks of them; written by other blocks of the
-// launch, so read past the L1); every thread of the block calls
+// launch, so read past the L1) and every system's travel budget (the block's
+// threads read the systems' budgets side by side); every thread of the block
+// calls
 __device__ __forceinline__ void vl_decide(const DevWorld& w, int nblocks, double* sh) {
   double v = 0.0;
   for (int b = threadIdx.x; b < nblocks; b += blockDim.x) v = fmax(v, __ldcg(w.vl_part + b));
@@ -34,16 +36,18 @@ __device__ __forceinline__ void vl_decide(const DevWorld& w, int nblocks, double
   for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
   if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
   __syncthreads();
+  double mx = 0.0;
+  for (int k = 0; k < (int)(blockDim.x >> 5); ++k) mx = fmax(mx, sh[k]);
+  WorldScalars* ws = w.ws;
+  int need = threadIdx.x == 0 && ws[0].vl_valid == 0;
+  for (int s = threadIdx.x; s < w.nsys; s += blockDim.x)
+    if (2.0 * mx + ws[s].vl_travel >= w.skin) need = 1;
+  const bool rebuild = __syncthreads_or(need) != 0;
+  if (rebuild)
+    for (int s = threadIdx.x; s < w.nsys; s += blockDim.x) ws[s].vl_travel = 0.0;
   if (threadIdx.x == 0) {
-    double mx = 0.0;
-    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) mx = fmax(mx, sh[k]);
-    WorldScalars* ws = w.ws;
-    bool rebuild = ws[0].vl_valid == 0;
-    for (int s = 0; s < w.nsys && !rebuild; ++s)
-      if (2.0 * mx + ws[s].vl_travel >= w.skin) rebuild = true;
     ws[0].vl_build = rebuild ? 1 : 0;
     if (rebuild) {
-      for (int s = 0; s < w.nsys; ++s) ws[s].vl_travel = 0.0;
       ws[0].vl_valid = 1;
       ws[0].vl_overflow = 0;
       ws[0].vl_builds += 1;
