@@ -301,7 +301,10 @@ void launch_update_phases(xdem_world_s* w, int record) {
   }
   // the launch that ends the pair phase (finish = 1) also resets the pair
   // counters for the next update (finish_pairs)
-  if (w->prm.precision == XDEM_PRECISION_MIXED && LAW == LAW_CLOSEST && !warm) {
+  // deep pairs are listed apart where the closest-approach law applies
+  const bool deep_lists = LAW == LAW_CLOSEST || (LAW == LAW_ANY && w->prm.ellipse_method ==
+                                                                       XDEM_ELLIPSE_CLOSEST_APPROACH);
+  if (w->prm.precision == XDEM_PRECISION_MIXED && deep_lists && !warm) {
     // The deep pairs first, then the regular pair pass as a programmatic
     // dependent launch: every block of k_pair_deep_m signals at its start, so
     // the regular pass starts once the deep pass is on the GPU and runs
@@ -449,6 +452,9 @@ void enqueue_step(xdem_world_s* w, const xdem_control* ctl, int record, bool res
   const bool fold_end = !w->has_clumps && !ctl->reset_rattlers && !ctl->update_stress &&
                         ctl->box_law == BOX_NONE && !ctl->stop_on_pressure;
   if (w->has_clumps) {
+    // a clump's time integral reads its sub-particles' sums: the sum pass
+    // first (one thread taking a clump's sub-particles serially measured
+    // slower than the two passes)
     launch_collect(w);
     launch_integrate(w, le, own && kind == XDEM_WORLD_PERIODIC_CONTROL);
   } else {

@@ -110,6 +110,20 @@ __device__ __forceinline__ void flush_warp(const DevWorld& w, uint32_t st, uint3
   }
 }
 
+// Whether this block is the last of its launch to get here (the same answer in
+// every thread of the block): every thread fences its writes, then the block
+// counts itself in `counter`; the last block sees what the others wrote.  The
+// caller resets the counter.  Nothing waits.
+__device__ __forceinline__ bool last_block(uint32_t* counter, bool& sh_last) {
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) sh_last = atomicAdd(counter, 1u) == gridDim.x - 1;
+  __syncthreads();
+  const bool last = sh_last;
+  if (last) __threadfence();
+  return last;
+}
+
 // ---------------------------------------------------------------------------
 // a2: modifyParticlePosition (PeriodicBoundaryWorld.cpp:129-142,
 //     LeesEdwardsBoundaryWorld.cpp:304-333)
@@ -204,15 +218,11 @@ __device__ __forceinline__ void write_body(const DevWorld& w, int m, double2 cs)
 // ncell+nx+[0,nx) top-row particles shifted by -shift (boxLE_bottom, :82-88).
 // The order inside a cell is not fixed; nothing downstream depends on it.
 // ---------------------------------------------------------------------------
+// The binning of the body at i.
 // MODIFY: k_modify_position's wrap first, in the same thread (a step's
 // position move followed by the binning)
-template <bool MODIFY = false>
-__global__ void k_bin(DevWorld w) {
-  pdl_begin();
-  if (stopped(w)) return;
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i == 0) *w.cell_max = 0;  // k_scan_tiles takes the maximum
-  if (i >= w.n) return;
+template <bool MODIFY>
+__device__ __forceinline__ void bin_at(const DevWorld& w, int i) {
   const WorldScalars& ws = w.ws[sys_at(w, i)];
   const double2 p = MODIFY ? modify_position_at(w, ws, i) : w.pos[i];
   if (MODIFY) {
@@ -262,6 +272,46 @@ __global__ void k_bin(DevWorld w) {
   }
   w.gcell[i] = gc;
   if (gc >= 0) w.grank[i] = atomicAdd(&w.cell_count[gc], 1);
+}
+
+// Whether this step rebuilds the candidate lists (system 0's vl_build), from
+// mx, the largest path length since the last build, and every system's travel
+// budget (the block's threads read the systems' budgets side by side); every
+// thread of the block calls
+__device__ __forceinline__ void list_rebuild_decision(const DevWorld& w, double mx) {
+  WorldScalars* ws = w.ws;
+  int need = threadIdx.x == 0 && ws[0].vl_valid == 0;
+  for (int s = threadIdx.x; s < w.nsys; s += blockDim.x)
+    if (2.0 * mx + ws[s].vl_travel >= w.skin) need = 1;
+  const bool rebuild = __syncthreads_or(need) != 0;
+  if (rebuild)
+    for (int s = threadIdx.x; s < w.nsys; s += blockDim.x) ws[s].vl_travel = 0.0;
+  if (threadIdx.x == 0) {
+    ws[0].vl_build = rebuild ? 1 : 0;
+    if (rebuild) {
+      ws[0].vl_valid = 1;
+      ws[0].vl_overflow = 0;
+      ws[0].vl_builds += 1;
+    }
+  }
+}
+
+// Whether this step's scan reads the cell records: a list rebuild, a list
+// that overflowed at the last build (scanned in full every step), or nine
+// cells that may hold the 200-candidate cap's count (counted from the
+// records); known once the rebuild decision is taken
+__device__ __forceinline__ bool cells_needed(const DevWorld& w) {
+  return w.ws->vl_build || w.ws->vl_overflow || 9 * *w.cell_max + 1 >= kCandidateCap;
+}
+
+// a3: the binning of every body
+template <bool MODIFY = false>
+__global__ void k_bin(DevWorld w) {
+  pdl_begin();
+  if (stopped(w)) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0) *w.cell_max = 0;  // k_scan_tiles takes the maximum
+  if (i < w.n) bin_at<MODIFY>(w, i);
 }
 
 // Exclusive scan of cell_count[0 .. ncell + 2nx) into cell_start, in three
@@ -342,12 +392,7 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_tiles(DevWorld w) {
     if (threadIdx.x == kScanThreads - 1) w.tile_sum[tile] = inc;
     __syncthreads();
   }
-  __threadfence();
-  __syncthreads();
-  if (threadIdx.x == 0) last = atomicAdd(&w.done[1], 1u) == gridDim.x - 1;
-  __syncthreads();
-  if (last) {
-    __threadfence();
+  if (last_block(&w.done[1], last)) {
     scan_tile_sums(w, sh_warp);
     if (threadIdx.x == 0) w.done[1] = 0;
   }
@@ -403,18 +448,14 @@ __device__ __forceinline__ double seg_path_factor(const DevWorld& w, int m) {
 // The cell-ordered records of the 3x3 scan; also clears cell_count (already
 // consumed by the scan) for the next binning.  when_needed: this step's
 // rebuild decision is taken, and the records are written only where a scan
-// reads them: a list rebuild, a list that overflowed at the last build
-// (scanned in full every step), or nine cells that may hold the
-// 200-candidate cap's count (counted from the records).
+// reads them (cells_needed).
 __global__ void k_scatter(DevWorld w, int when_needed) {
   pdl_begin();
   if (stopped(w)) return;
   const int total = w.ncell_total;
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < total; c += gridDim.x * blockDim.x)
     w.cell_count[c] = 0;
-  if (when_needed && !w.ws->vl_build && !w.ws->vl_overflow &&
-      9 * *w.cell_max + 1 < kCandidateCap)
-    return;
+  if (when_needed && !cells_needed(w)) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= w.n) return;
   const Grid G = grid_of(w.ws[sys_at(w, i)]);
@@ -697,7 +738,8 @@ __device__ __forceinline__ void integrate_at(const DevWorld& w, int i, int reset
   }
   double2 p = w.pos[i];
   double om = w.w[i];
-  if (w.shape[i] == SHAPE_CLUMP) {
+  // (SUMS: a world without clumps; the branch is left out of that kernel)
+  if (!SUMS && w.shape[i] == SHAPE_CLUMP) {
     vec2<double> F = V(0.0, 0.0);
     double T = 0.0;
     const int ns = w.num_sub[i];
@@ -1076,12 +1118,7 @@ __global__ void __launch_bounds__(128) k_collect_integrate(DevWorld w, int par, 
   }
   if (le_update < 0) return;
   __shared__ bool last;
-  __threadfence();
-  __syncthreads();
-  if (threadIdx.x == 0) last = atomicAdd(&w.done[3], 1u) == gridDim.x - 1;
-  __syncthreads();
-  if (last) {
-    __threadfence();
+  if (last_block(&w.done[3], last)) {
     for (int sys = threadIdx.x; sys < w.nsys; sys += blockDim.x)
       end_of_step_at(w, sys, BOX_NONE, 0.0, 0.0, le_update, 0, 0.0, 1);
     if (threadIdx.x == 0) w.done[3] = 0;

@@ -130,18 +130,33 @@ __device__ __forceinline__ int centre_line_class(float dx, float dy, const AxisS
 }
 
 
-// the centre-line screen applies to mixed-precision worlds of ellipses under
-// one law
+// the centre-line screen applies to pairs of ellipses in mixed-precision
+// worlds: under one law every pair, in a world of several shapes (LAW_ANY)
+// the pairs of two ellipses
 template <int LAW>
 __device__ __forceinline__ bool centre_line_screen(const DevWorld& w) {
-  return (LAW == LAW_CLOSEST || LAW == LAW_INTERSECTION) && w.precision == XDEM_PRECISION_MIXED;
+  return (LAW == LAW_CLOSEST || LAW == LAW_INTERSECTION || LAW == LAW_ANY) &&
+         w.precision == XDEM_PRECISION_MIXED;
+}
+template <int LAW>
+__device__ __forceinline__ bool screens_pair(const DevWorld& w, int shape_i, int shape_j) {
+  return centre_line_screen<LAW>(w) &&
+         (LAW != LAW_ANY || (shape_i == SHAPE_ELLIPSE && shape_j == SHAPE_ELLIPSE));
 }
 
-// the owner's record for the screen
+// the deep pairs of the screen are listed apart where the closest-approach
+// law applies
+template <int LAW>
+__device__ __forceinline__ bool lists_deep(const DevWorld& w) {
+  return LAW == LAW_CLOSEST || (LAW == LAW_ANY && w.method == ELLIPSE_CLOSEST);
+}
+
+// the owner's record for the screen (an ellipse's; zeros for other shapes)
 template <int LAW>
 __device__ __forceinline__ AxisShape owner_axis_shape(const DevWorld& w, int m) {
   AxisShape e{0.0f, 0.0f, 0.0f, 0.0f};
-  if (centre_line_screen<LAW>(w)) e = axis_shape(w, m);
+  if (centre_line_screen<LAW>(w) && (LAW != LAW_ANY || w.shape[m] == SHAPE_ELLIPSE))
+    e = axis_shape(w, m);
   return e;
 }
 
@@ -243,7 +258,7 @@ __device__ __forceinline__ void scan_cells(const DevWorld& w, const WorldScalars
         if (!pass) continue;
       }
       int cls = CL_REGULAR;
-      if (centre_line_screen<LAW>(w)) {
+      if (screens_pair<LAW>(w, shape_i, LAW == LAW_ANY ? w.shape[w.cell_mem[q]] : 0)) {
         // the same FP64 image offset as the candidate lists' test (verlet.cuh)
         const double2 pj = w.cell_pos[q];
         vec2<double> off, ovel;
@@ -262,7 +277,7 @@ __device__ __forceinline__ void scan_cells(const DevWorld& w, const WorldScalars
       if (oslot != kNoOldSlot) matched |= 1u << oslot;
       list_mj[nlist * stride] = w.cell_mem[q];
       list_code[nlist * stride] =
-          kind | (nlist << 8) | (oslot << 16) | (LAW == LAW_CLOSEST && cls == CL_DEEP ? kDeepFlag : 0);
+          kind | (nlist << 8) | (oslot << 16) | (lists_deep<LAW>(w) && cls == CL_DEEP ? kDeepFlag : 0);
       ++nlist;
     }
   }
@@ -634,12 +649,7 @@ __device__ __forceinline__ void pair_forces_fp64(const DevWorld& w, int par, int
 // thread of the block calls.
 __device__ __forceinline__ void finish_pairs(const DevWorld& w) {
   __shared__ bool last;
-  __threadfence();
-  __syncthreads();
-  if (threadIdx.x == 0) last = atomicAdd(&w.done[2], 1u) == gridDim.x - 1;
-  __syncthreads();
-  if (last && threadIdx.x == 0) {
-    __threadfence();
+  if (last_block(&w.done[2], last) && threadIdx.x == 0) {
     w.ws->last_pairs = *w.npairs;
     *w.npairs = 0;
     *w.nfallback = 0;

@@ -24,11 +24,9 @@ namespace xdem {
 constexpr int kVlBlock = 256;
 constexpr int kVlRounds = 1;  // rounds of 32 list entries whose loads k_candidates_vl issues together (two spill at 72 registers and measured slower)
 
-// whether this step rebuilds the lists (system 0's vl_build), from the block
-// maxima of the path lengths (nblocks of them; written by other blocks of the
-// launch, so read past the L1) and every system's travel budget (the block's
-// threads read the systems' budgets side by side); every thread of the block
-// calls
+// the step's list-rebuild decision from the block maxima of the path lengths
+// (nblocks of them; written by other blocks of the launch, so read past the
+// L1); every thread of the block calls
 __device__ __forceinline__ void vl_decide(const DevWorld& w, int nblocks, double* sh) {
   double v = 0.0;
   for (int b = threadIdx.x; b < nblocks; b += blockDim.x) v = fmax(v, __ldcg(w.vl_part + b));
@@ -38,21 +36,7 @@ __device__ __forceinline__ void vl_decide(const DevWorld& w, int nblocks, double
   __syncthreads();
   double mx = 0.0;
   for (int k = 0; k < (int)(blockDim.x >> 5); ++k) mx = fmax(mx, sh[k]);
-  WorldScalars* ws = w.ws;
-  int need = threadIdx.x == 0 && ws[0].vl_valid == 0;
-  for (int s = threadIdx.x; s < w.nsys; s += blockDim.x)
-    if (2.0 * mx + ws[s].vl_travel >= w.skin) need = 1;
-  const bool rebuild = __syncthreads_or(need) != 0;
-  if (rebuild)
-    for (int s = threadIdx.x; s < w.nsys; s += blockDim.x) ws[s].vl_travel = 0.0;
-  if (threadIdx.x == 0) {
-    ws[0].vl_build = rebuild ? 1 : 0;
-    if (rebuild) {
-      ws[0].vl_valid = 1;
-      ws[0].vl_overflow = 0;
-      ws[0].vl_builds += 1;
-    }
-  }
+  list_rebuild_decision(w, mx);
 }
 
 // block maxima of the path lengths since the last build; the last block to
@@ -75,12 +59,7 @@ __global__ void __launch_bounds__(kVlBlock) k_vl_maxdisp(DevWorld w) {
     for (int k = 0; k < kVlBlock / 32; ++k) mx = fmax(mx, sh[k]);
     w.vl_part[blockIdx.x] = mx;
   }
-  __threadfence();
-  __syncthreads();
-  if (threadIdx.x == 0) last = atomicAdd(&w.done[0], 1u) == gridDim.x - 1;
-  __syncthreads();
-  if (last) {
-    __threadfence();
+  if (last_block(&w.done[0], last)) {
     vl_decide(w, gridDim.x, sh);
     if (threadIdx.x == 0) w.done[0] = 0;
   }
@@ -285,7 +264,8 @@ __global__ void __launch_bounds__(128, 7) k_candidates_vl(DevWorld w, int par, i
       const int mj = ent[h] >> 2;
       pjh[h] = act ? w.pos[mj] : make_double2(0.0, 0.0);
       sjh[h] = act && LAW != LAW_ANY ? w.screen_r[mj] : 0.0;
-      axh[h] = act && centre_line_screen<LAW>(w) ? axis_shape(w, mj) : AxisShape{0.0f, 0.0f, 0.0f, 0.0f};
+      axh[h] = act && centre_line_screen<LAW>(w) && LAW != LAW_ANY ? axis_shape(w, mj)
+                                                                 : AxisShape{0.0f, 0.0f, 0.0f, 0.0f};
     }
 #pragma unroll
     for (int h = 0; h < kVlRounds; ++h) {
@@ -324,9 +304,12 @@ __global__ void __launch_bounds__(128, 7) k_candidates_vl(DevWorld w, int par, i
         else
           pass = coarse_pass<LAW>(0, 0, ro, sjh[h], orado, sjh[h], pio, pj, off);
         int cls = CL_REGULAR;
-        if (pass && centre_line_screen<LAW>(w)) {
+        if (pass && screens_pair<LAW>(w, shape_o, LAW == LAW_ANY ? w.shape[mj] : 0)) {
+          // (a world of several shapes reads the partner's axis record here,
+          // for the pairs of two ellipses only)
+          const AxisShape ax_j = LAW == LAW_ANY ? axis_shape(w, mj) : axh[h];
           cls = centre_line_class((float)((pj.x + off.x) - pio.x), (float)((pj.y + off.y) - pio.y),
-                                  ax_o, axh[h]);
+                                  ax_o, ax_j);
           pass = cls != CL_SEPARATED;
         }
         if (pass) {
@@ -347,7 +330,7 @@ __global__ void __launch_bounds__(128, 7) k_candidates_vl(DevWorld w, int par, i
             const int shape_j = w.shape[mj];
             near = shape_o == shape_j && (shape_o == SHAPE_CIRCLE || shape_o == SHAPE_ELLIPSE);
           }
-          code = kind | (oslot << 16) | (LAW == LAW_CLOSEST && cls == CL_DEEP ? kDeepFlag : 0);
+          code = kind | (oslot << 16) | (lists_deep<LAW>(w) && cls == CL_DEEP ? kDeepFlag : 0);
         }
       }
       // rank among the owner's kept entries of this round, in list order
