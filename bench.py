@@ -377,11 +377,12 @@ def kernel_bytes(kernel, n, contacts, pairs, entries=0):
     """Algorithmic DRAM bytes of one launch of a contact-update kernel, with
     every particle's data counted once (neighbour re-reads hit L2).
     k_candidates (with candidate lists): per particle the owner's data
-      (position 16, velocity 16, orientation 8, spin 8, radius 8, aspect 8,
-      outer radius 8, shape 4, id 4, setting 4, up-level 4, cell 4, old slot
-      count 4, list length 4) = 100 B, written: its body record 96 B and its
-      slot count 4 B = 200 B; per list entry 4 B; per contact the old partner
-      id 4 B; per listed pair a 16 B entry.
+      (position 16, radius 8, outer radius 8, axis record 16, setting 4,
+      up-level 4, cell 4, list length 4, old record count 4 and first
+      record 4) = 72 B, written: its record count and first record 8 B =
+      80 B (the binning kernel writes the body record); per list entry 4 B;
+      per old contact its partner's id and memory position 8 B; per listed
+      pair a 16 B entry.
     k_pair_forces: per particle the state the geometry reads (position 16,
       velocity 16, orientation 8, spin 8, radius 8, aspect 8, outer radius 8,
       shape 4, mass 8, setting 4, id 4) = 92 B; per listed pair its entry 16 B;
@@ -390,7 +391,7 @@ def kernel_bytes(kernel, n, contacts, pairs, entries=0):
       damping 8, force 16, torques 16, branch vector 16 = 92 B); per listed
       pair that does not touch, an empty-slot mark (4 B)."""
     if kernel == "k_candidates":
-        return 200.0 * n + 4.0 * entries + 4.0 * contacts + 16.0 * pairs
+        return 80.0 * n + 4.0 * entries + 8.0 * contacts + 16.0 * pairs
     return 92.0 * n + 16.0 * pairs + 136.0 * contacts + 4.0 * max(pairs - contacts, 0)
 
 
