@@ -359,8 +359,16 @@ __global__ void __launch_bounds__(128, 7) k_candidates_vl(DevWorld w, int par, i
   int ndeep = 0;
   uint32_t carry = 0;
   if (valid) {
-    carry = scan ? carry_mask(w, old, G, m, ix, iy, up_i, nold, s_matched[tid], K - nlist, st)
-                 : carry_all(w, old, m, nold, st);
+    if (scan) {
+      // the owner's grid, cell and up-level again (reloaded rather than kept
+      // in registers through the entry loop)
+      const Grid G2 = grid_of(w.ws[sys_at(w, m)]);
+      const int cl = w.pcell[m] - G2.base;
+      carry = carry_mask(w, old, G2, m, cl % G2.nx, cl / G2.nx, w.up[m], nold, s_matched[tid],
+                         K - nlist, st);
+    } else {
+      carry = carry_all(w, old, m, nold, st);
+    }
     for (int s = 0; s < nlist; ++s) ndeep += (s_code[s * 128 + tid] & kDeepFlag) ? 1 : 0;
   }
   const int nrec = nlist + __popc(carry);  // the owner's records: listed pairs, then carried
