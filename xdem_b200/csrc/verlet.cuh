@@ -98,19 +98,35 @@ __global__ void __launch_bounds__(128) k_vl_build(DevWorld w) {
       const int c = neighbour_cell(G, w.kind, ix, iy, dx, dy, kind);
       const int q0 = w.cell_start[c], q1 = w.cell_start[c + 1];
       const float ox = dx * flx - rxi, oy = dy * fly - ryi;
-      for (int q = q0; q < q1; ++q) {
-        const float4 rj = w.cell_scr[q];
-        if (__float_as_int(rj.w) <= id_i) continue;
-        if (w.cell_up[q] == up_i) continue;
-        const float ddx = ox + rj.x, ddy = oy + rj.y;
-        const float R = sr_i + rj.z;
-        if (ddx * ddx + ddy * ddy > R * R * (1.0f + 1e-4f) + 1e-4f) continue;
-        if (cnt >= w.V) {
-          cnt = -1;
-          break;
+      // two cell entries at a time, their loads issued together
+      for (int q = q0; q < q1; q += 2) {
+        const bool two = q + 1 < q1;
+        const float4 ra = w.cell_scr[q];
+        const float4 rb = two ? w.cell_scr[q + 1] : make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
+        const int ua = w.cell_up[q], ub = two ? w.cell_up[q + 1] : up_i;
+        const int ma = w.cell_mem[q], mb = two ? w.cell_mem[q + 1] : 0;
+        const bool ka = __float_as_int(ra.w) > id_i && ua != up_i &&
+                        !((ox + ra.x) * (ox + ra.x) + (oy + ra.y) * (oy + ra.y) >
+                          (sr_i + ra.z) * (sr_i + ra.z) * (1.0f + 1e-4f) + 1e-4f);
+        const bool kb = __float_as_int(rb.w) > id_i && ub != up_i &&
+                        !((ox + rb.x) * (ox + rb.x) + (oy + rb.y) * (oy + rb.y) >
+                          (sr_i + rb.z) * (sr_i + rb.z) * (1.0f + 1e-4f) + 1e-4f);
+        if (ka) {
+          if (cnt >= w.V) {
+            cnt = -1;
+            break;
+          }
+          w.vl[(size_t)cnt * n + m] = (ma << 2) | kind;
+          ++cnt;
         }
-        w.vl[(size_t)cnt * n + m] = (w.cell_mem[q] << 2) | kind;
-        ++cnt;
+        if (kb) {
+          if (cnt >= w.V) {
+            cnt = -1;
+            break;
+          }
+          w.vl[(size_t)cnt * n + m] = (mb << 2) | kind;
+          ++cnt;
+        }
       }
       if (cnt < 0) break;
     }
