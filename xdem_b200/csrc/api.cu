@@ -376,16 +376,15 @@ void launch_integrate(xdem_world_s* w, bool fold_bg, int reset) {
     LAUNCH(w, KK_INTEGRATE, k_integrate<false><<<blocks_for(n, kBlock), kBlock, 0, w->stream>>>(w->dw, reset));
 }
 
-// the force sum and the time integral of a world without clumps in one pass;
-// end_le >= 0: with the step's end (its Lees-Edwards update flag), -1 without
-void launch_collect_integrate(xdem_world_s* w, bool fold_bg, int reset, int end_le) {
+// the force sum and the time integral of a world without clumps in one pass
+void launch_collect_integrate(xdem_world_s* w, bool fold_bg, int reset) {
   int n = w->dw.n;
   if (fold_bg)
     launch_chain(w, KK_COLLECT_INTEGRATE, k_collect_integrate<true>, blocks_for(n, 128), 128, 0,
-                 w->dw, w->par, reset, end_le);
+                 w->dw, w->par, reset);
   else
     launch_chain(w, KK_COLLECT_INTEGRATE, k_collect_integrate<false>, blocks_for(n, 128), 128, 0,
-                 w->dw, w->par, reset, end_le);
+                 w->dw, w->par, reset);
 }
 
 void launch_stress(xdem_world_s* w) {
@@ -447,10 +446,6 @@ void enqueue_step(xdem_world_s* w, const xdem_control* ctl, int record, bool res
   launch_update(w, le, record);
   w->list_decided = false;
   w->body_written = false;
-  // without a rattler reset, stress pass, box law or stop test between them,
-  // the step's end is taken by the last block of the fused sum and integral
-  const bool fold_end = !w->has_clumps && !ctl->reset_rattlers && !ctl->update_stress &&
-                        ctl->box_law == BOX_NONE && !ctl->stop_on_pressure;
   if (w->has_clumps) {
     // a clump's time integral reads its sub-particles' sums: the sum pass
     // first (one thread taking a clump's sub-particles serially measured
@@ -458,10 +453,8 @@ void enqueue_step(xdem_world_s* w, const xdem_control* ctl, int record, bool res
     launch_collect(w);
     launch_integrate(w, le, own && kind == XDEM_WORLD_PERIODIC_CONTROL);
   } else {
-    launch_collect_integrate(w, le, own && kind == XDEM_WORLD_PERIODIC_CONTROL,
-                             fold_end ? (le ? 1 : 0) : -1);
+    launch_collect_integrate(w, le, own && kind == XDEM_WORLD_PERIODIC_CONTROL);
   }
-  if (fold_end) return;
   if (ctl->reset_rattlers) launch_rattlers(w, 1, 0.0);
   if (ctl->update_stress) launch_stress(w);
   launch_end_of_step(w, ctl->box_law, ctl->p0, ctl->p1, le ? 1 : 0, ctl->stop_on_pressure,

@@ -153,10 +153,9 @@ struct DevWorld {
   int32_t* cell_max;  // largest cell count of this step's binning (all systems)
   int32_t* cell_start;
   int32_t* tile_sum;  // scan tile sums
-  // [4] blocks finished of the list check, of the scan's tile pass, of the
-  // launch that ends the pair phase and of the fused force sum and time
-  // integral: the last block of each finishes the pass's work, then resets
-  // its counter
+  // [4] blocks finished of the list check, of the scan's tile pass and of the
+  // launch that ends the pair phase (the fourth is unused): the last block of
+  // each finishes the pass's work, then resets its counter
   uint32_t* done;
   int32_t* cell_mem;
   double2* cell_pos;      // [2n] position of each cell entry, cell order
